@@ -1,0 +1,140 @@
+"""Cloth meshes and the synthetic workloads used by the tests and the benchmark.
+
+`grid_mesh` builds the same topology as Bounce's ``b3GridClothMesh``
+(include/bounce/cloth/grid_cloth_mesh.h:26-94): vertices stored row-major,
+``v(i, j) = i * (W + 1) + j``, in the x-z plane centred at the origin, and two
+triangles per cell, ``(v3, v2, v1)`` and ``(v1, v4, v3)``.  The reference
+template has unit spacing; here the grid is scaled to ``size`` metres and can
+carry a seeded Gaussian jitter, applied before the cloth is built so that the
+rest state includes it.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# b3ParticleType (include/bounce/cloth/particle.h:27-32)
+STATIC, KINEMATIC, DYNAMIC = 0, 1, 2
+
+
+@dataclass
+class ClothDef:
+    """b3ClothDef (include/bounce/cloth/cloth.h:56-95)."""
+
+    density: float = 0.0
+    streching: float = 0.0
+    shearing: float = 0.0
+    bending: float = 0.0
+    sewing: float = 0.0
+    damping: float = 0.0
+    thickness: float = 0.0
+    friction: float = 0.2
+
+    def as_array(self) -> np.ndarray:
+        return np.array([self.density, self.streching, self.shearing, self.bending, self.sewing,
+                         self.damping, self.thickness, self.friction], dtype=np.float32)
+
+
+@dataclass
+class Mesh:
+    vertices: np.ndarray            # float32 (N, 3)
+    triangles: np.ndarray           # uint32 (T, 3)
+    sewing: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), np.uint32))  # (s1, s2, v1, v2)
+
+    @property
+    def vertex_count(self) -> int:
+        return int(self.vertices.shape[0])
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.triangles.shape[0])
+
+
+def grid_mesh(side: int, size: float = 1.0, jitter: float = 0.0, seed: int = 0) -> Mesh:
+    """A side x side vertex grid, (side-1)^2 cells, 2 (side-1)^2 triangles."""
+    if side < 2:
+        raise ValueError("a grid needs at least 2 vertices per side")
+    w = side - 1
+    j, i = np.meshgrid(np.arange(side), np.arange(side))
+    verts = np.zeros((side * side, 3), dtype=np.float64)
+    verts[:, 0] = (j.reshape(-1) / w - 0.5) * size
+    verts[:, 2] = (i.reshape(-1) / w - 0.5) * size
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        verts += rng.normal(0.0, jitter, size=verts.shape)
+    ci, cj = np.meshgrid(np.arange(w), np.arange(w), indexing="ij")
+    ci = ci.reshape(-1)
+    cj = cj.reshape(-1)
+    v1 = ci * side + cj
+    v2 = (ci + 1) * side + cj
+    v3 = (ci + 1) * side + cj + 1
+    v4 = ci * side + cj + 1
+    tris = np.empty((2 * w * w, 3), dtype=np.uint32)
+    tris[0::2] = np.stack([v3, v2, v1], axis=1)
+    tris[1::2] = np.stack([v1, v4, v3], axis=1)
+    return Mesh(verts.astype(np.float32), tris)
+
+
+@dataclass
+class Scene:
+    """One cloth with everything a step sequence needs."""
+
+    name: str
+    mesh: Mesh
+    cdef: ClothDef
+    pinned: np.ndarray                      # vertex ids made static
+    gravity: tuple = (0.0, -9.8, 0.0)
+    spheres: list = field(default_factory=list)   # (center (3,), radius, friction)
+    dt: float = 1.0 / 60.0
+    steps: int = 100
+    velocity_iterations: int = 8
+    position_iterations: int = 2
+    tol: float = 1e-4
+    max_iterations: int = 50
+
+
+def plain_scene(side: int = 32, seed: int = 1, steps: int = 100) -> Scene:
+    """Single cloth, no contacts: 1 m x 1 m, 1 kg/m^2, stretch 1e4, shear 1e3,
+    damping 0.05, gravity (0, -9.8, 0), the two corners of row 0 pinned,
+    jitter N(0, 1e-3 m)."""
+    mesh = grid_mesh(side, 1.0, 1e-3, seed)
+    cdef = ClothDef(density=1.0, streching=1e4, shearing=1e3, damping=0.05, friction=0.3)
+    pins = np.array([0, side - 1], dtype=np.uint32)
+    return Scene(f"grid{side}_plain", mesh, cdef, pins, steps=steps)
+
+
+def sphere_scene(side: int = 256, seed: int = 2, steps: int = 200) -> Scene:
+    """Single large cloth: stretch + shear + bending springs (1e2) on every
+    edge-adjacent triangle pair, a static sphere of radius 0.3 m 0.5 m below
+    the cloth centre, friction 0.3, jitter N(0, 1e-3 m)."""
+    mesh = grid_mesh(side, 1.0, 1e-3, seed)
+    cdef = ClothDef(density=1.0, streching=1e4, shearing=1e3, bending=1e2, damping=0.05, friction=0.3)
+    pins = np.array([0, side - 1], dtype=np.uint32)
+    sph = [((0.0, -0.5, 0.0), 0.3, 0.3)]
+    return Scene(f"grid{side}_bend_sphere", mesh, cdef, pins, spheres=sph, steps=steps)
+
+
+def stiff_scene(side: int = 1024, steps: int = 50) -> Scene:
+    """Ill-conditioned large cloth: stretch 1e5, damping 0.1, shear 1e3, no jitter."""
+    mesh = grid_mesh(side, 1.0, 0.0, 0)
+    cdef = ClothDef(density=1.0, streching=1e5, shearing=1e3, damping=0.1, friction=0.3)
+    pins = np.array([0, side - 1], dtype=np.uint32)
+    return Scene(f"grid{side}_stiff", mesh, cdef, pins, steps=steps)
+
+
+def batch_scenes(count: int = 512, seed: int = 3, side_lo: int = 16, side_hi: int = 128,
+                 steps: int = 100) -> list:
+    """Many independent cloths: side ~ U{side_lo..side_hi}, stretch log-U[1e3, 1e5],
+    shear log-U[1e2, 1e4], the whole row 0 pinned."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        side = int(rng.integers(side_lo, side_hi + 1))
+        ks = float(10.0 ** rng.uniform(3.0, 5.0))
+        kh = float(10.0 ** rng.uniform(2.0, 4.0))
+        mesh = grid_mesh(side, 1.0, 1e-3, seed * 100003 + k)
+        cdef = ClothDef(density=1.0, streching=ks, shearing=kh, damping=0.05, friction=0.3)
+        pins = np.arange(side, dtype=np.uint32)
+        out.append(Scene(f"batch{k}_{side}", mesh, cdef, pins, steps=steps))
+    return out

@@ -1,0 +1,356 @@
+"""ctypes front-ends for the two CPU checkers (test infrastructure only).
+
+* `PortCloth` wraps ``_build/liboracle.so``: the C restatement of the
+  reference's cloth step (cloth_oracle.c).
+* `RefCloth` wraps ``_ref/libbounce_ref.so``: the reference library itself,
+  compiled from its unmodified sources by the Makefile next to this file,
+  with ref_harness.cpp.
+
+Only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py use
+this package; the product (bounce_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "_build", "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libbounce_ref.so")
+
+STOP_REFERENCE, STOP_RELATIVE = 0, 1
+DOT_F32, DOT_COMPENSATED, DOT_F64 = 0, 1, 2
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+
+def build(port: bool = True, ref: bool = True) -> None:
+    """Compile the checkers (the reference part needs its sources on disk)."""
+    targets = []
+    if port:
+        targets.append("port")
+    if ref and os.path.isdir("/root/reference/src"):
+        targets.append("ref")
+    if targets:
+        subprocess.run(["make", "-s", "-C", HERE, "-j8"] + targets, check=True)
+
+
+class _OcStepInfo(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("delta0", C.c_double), ("delta", C.c_double),
+                ("b_delta", C.c_double), ("active_contacts", C.c_uint32), ("contacts", C.c_uint32)]
+
+
+_port = None
+_ref = None
+
+
+def port_lib():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_LIB):
+            build(port=True, ref=False)
+        L = C.CDLL(PORT_LIB)
+        L.oc_create.restype = C.c_void_p
+        L.oc_create.argtypes = [_f32p, C.c_uint32, _u32p, C.c_uint32, _u32p, C.c_uint32, _f32p]
+        L.oc_destroy.argtypes = [C.c_void_p]
+        L.oc_set_gravity.argtypes = [C.c_void_p, _f32p]
+        L.oc_set_type.argtypes = [C.c_void_p, C.c_uint32, C.c_int]
+        for name in ("oc_apply_force", "oc_apply_translation", "oc_set_position", "oc_set_velocity"):
+            getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, _f32p]
+        L.oc_add_sphere.argtypes = [C.c_void_p, _f32p, C.c_float, C.c_float]
+        L.oc_set_solver.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_uint32, C.c_int]
+        L.oc_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(_OcStepInfo)]
+        L.oc_get_state.argtypes = [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _u8p]
+        L.oc_energy.restype = C.c_float
+        L.oc_energy.argtypes = [C.c_void_p]
+        L.oc_describe.restype = C.c_uint32
+        L.oc_describe.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oc_get_contacts.restype = C.c_uint32
+        L.oc_get_contacts.argtypes = [C.c_void_p, _u8p, _u8p, _f32p]
+        L.oc_force_count.restype = C.c_uint32
+        L.oc_force_count.argtypes = [C.c_void_p]
+        L.oc_spring_count.restype = C.c_uint32
+        L.oc_spring_count.argtypes = [C.c_void_p]
+        L.oc_get_springs.argtypes = [C.c_void_p, _u32p, _f32p, _f32p]
+        L.oc_build_system.restype = C.c_uint32
+        L.oc_build_system.argtypes = [C.c_void_p, C.c_float]
+        L.oc_get_system.argtypes = [C.c_void_p, _u32p, _u32p, _f32p, _f32p, _f32p, _f32p, _u32p]
+        L.oc_mpcg.restype = C.c_uint32
+        L.oc_mpcg.argtypes = [C.c_uint32, _u32p, _u32p, _f32p, _f32p, _f32p, _f32p, C.c_int, C.c_float,
+                              C.c_uint32, C.c_int, _f32p, _f64p]
+        L.oc_solve_f64.restype = C.c_uint32
+        L.oc_solve_f64.argtypes = [C.c_uint32, _u32p, _u32p, _f32p, _f32p, _f32p, _f32p, C.c_double,
+                                   C.c_uint32, _f64p]
+        _port = L
+    return _port
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_LIB):
+            raise FileNotFoundError(f"{REF_LIB} is not built (make -C oracle ref)")
+        L = C.CDLL(REF_LIB)
+        L.ref_cloth_create.restype = C.c_void_p
+        L.ref_cloth_create.argtypes = [_f32p, C.c_uint32, _u32p, C.c_uint32, _u32p, C.c_uint32, _f32p, C.c_int]
+        L.ref_cloth_destroy.argtypes = [C.c_void_p]
+        L.ref_cloth_set_gravity.argtypes = [C.c_void_p, _f32p]
+        L.ref_cloth_set_type.argtypes = [C.c_void_p, C.c_uint32, C.c_int]
+        for name in ("ref_cloth_apply_force", "ref_cloth_apply_translation", "ref_cloth_set_position",
+                     "ref_cloth_set_velocity"):
+            getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, _f32p]
+        L.ref_cloth_add_sphere.argtypes = [C.c_void_p, _f32p, C.c_float, C.c_float]
+        L.ref_cloth_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_uint32, C.c_int]
+        L.ref_last_iterations.restype = C.c_uint32
+        L.ref_cloth_get_state.argtypes = [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _u8p]
+        L.ref_cloth_energy.restype = C.c_float
+        L.ref_cloth_energy.argtypes = [C.c_void_p]
+        L.ref_cloth_describe.restype = C.c_uint32
+        L.ref_cloth_describe.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_cloth_get_contacts.restype = C.c_uint32
+        L.ref_cloth_get_contacts.argtypes = [C.c_void_p, _u8p, _u8p, _f32p]
+        L.ref_cloth_build_system.restype = C.c_uint32
+        L.ref_cloth_build_system.argtypes = [C.c_void_p, C.c_float]
+        L.ref_cloth_get_system.argtypes = [C.c_void_p, _u32p, _u32p, _f32p, _f32p, _f32p, _f32p, _u32p]
+        L.ref_profile_read.restype = C.c_uint32
+        L.ref_profile_read.argtypes = [C.c_char_p, C.c_uint32, _f64p, np.ctypeslib.ndpointer(np.uint64)]
+        L.ref_profile_reset.argtypes = []
+        _ref = L
+    return _ref
+
+
+class _Base:
+    """Shared state accessors; subclasses bind the library calls."""
+
+    def __init__(self, mesh, cdef):
+        self.n = mesh.vertex_count
+        self.t = mesh.triangle_count
+        self._verts = np.ascontiguousarray(mesh.vertices, np.float32).reshape(-1)
+        self._tris = np.ascontiguousarray(mesh.triangles, np.uint32).reshape(-1)
+        sew = np.ascontiguousarray(mesh.sewing, np.uint32).reshape(-1)
+        self._sew = sew if sew.size else np.zeros(4, np.uint32)
+        self._nsew = int(mesh.sewing.shape[0])
+        self._def = cdef.as_array()
+
+    def state(self):
+        x = np.zeros(3 * self.n, np.float32)
+        v = np.zeros(3 * self.n, np.float32)
+        dv = np.zeros(3 * self.n, np.float32)
+        m = np.zeros(self.n, np.float32)
+        ty = np.zeros(self.n, np.uint8)
+        self._get_state(x, v, dv, m, ty)
+        return {"x": x.reshape(-1, 3), "v": v.reshape(-1, 3), "dv": dv.reshape(-1, 3), "mass": m, "type": ty}
+
+    def describe(self):
+        nf = self._describe(None, None, None)
+        tri = np.zeros(6 * self.t, np.float32)
+        fat = np.zeros(6 * self.n, np.float32)
+        forces = np.zeros(8 * max(nf, 1), np.float32)
+        self._describe(tri.ctypes.data, fat.ctypes.data, forces.ctypes.data)
+        return {"tri_rest": tri.reshape(-1, 6), "fat_aabb": fat.reshape(-1, 6),
+                "forces": forces.reshape(-1, 8)[:nf]}
+
+    def contacts(self):
+        ex = np.zeros(self.n, np.uint8)
+        ac = np.zeros(self.n, np.uint8)
+        imp = np.zeros(3 * self.n, np.float32)
+        cnt = self._get_contacts(ex, ac, imp)
+        return {"count": int(cnt), "exists": ex, "active": ac, "impulses": imp.reshape(-1, 3)}
+
+    def system(self, dt: float):
+        nnz = self._build_system(dt)
+        rowptr = np.zeros(self.n + 1, np.uint32)
+        cols = np.zeros(max(nnz, 1), np.uint32)
+        vals = np.zeros(9 * max(nnz, 1), np.float32)
+        b = np.zeros(3 * self.n, np.float32)
+        S = np.zeros(self.n, np.float32)
+        x0 = np.zeros(3 * self.n, np.float32)
+        vor = np.zeros(self.n, np.uint32)
+        self._get_system(rowptr, cols, vals, b, S, x0, vor)
+        return {"rowptr": rowptr, "cols": cols[:nnz], "vals": vals[:9 * nnz], "b": b, "S": S, "x0": x0,
+                "vertex_of_row": vor}
+
+    # scene helpers
+    def setup(self, scene):
+        self.set_gravity(scene.gravity)
+        for p in scene.pinned:
+            self.set_type(int(p), 0)
+        for (c, r, mu) in scene.spheres:
+            self.add_sphere(c, r, mu)
+        return self
+
+
+class PortCloth(_Base):
+    """The C restatement."""
+
+    def __init__(self, mesh, cdef):
+        super().__init__(mesh, cdef)
+        self.L = port_lib()
+        self.h = self.L.oc_create(self._verts, self.n, self._tris, self.t, self._sew, self._nsew, self._def)
+        self.last = _OcStepInfo()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.oc_destroy(self.h)
+            self.h = None
+
+    def set_gravity(self, g):
+        self.L.oc_set_gravity(self.h, np.asarray(g, np.float32))
+
+    def set_type(self, vertex, ty):
+        self.L.oc_set_type(self.h, vertex, ty)
+
+    def apply_force(self, vertex, f):
+        self.L.oc_apply_force(self.h, vertex, np.asarray(f, np.float32))
+
+    def apply_translation(self, vertex, t):
+        self.L.oc_apply_translation(self.h, vertex, np.asarray(t, np.float32))
+
+    def set_position(self, vertex, x):
+        self.L.oc_set_position(self.h, vertex, np.asarray(x, np.float32))
+
+    def set_velocity(self, vertex, v):
+        self.L.oc_set_velocity(self.h, vertex, np.asarray(v, np.float32))
+
+    def add_sphere(self, center, radius, friction):
+        return self.L.oc_add_sphere(self.h, np.asarray(center, np.float32), radius, friction)
+
+    def set_solver(self, stop_rule=STOP_REFERENCE, tol=0.0, max_iterations=20, dot=DOT_F32):
+        self.L.oc_set_solver(self.h, stop_rule, tol, max_iterations, dot)
+
+    def step(self, dt, vel_iters=8, pos_iters=2):
+        self.L.oc_step(self.h, dt, vel_iters, pos_iters, C.byref(self.last))
+        return {"iterations": self.last.iterations, "delta0": self.last.delta0, "delta": self.last.delta,
+                "b_delta": self.last.b_delta, "active_contacts": self.last.active_contacts,
+                "contacts": self.last.contacts}
+
+    def energy(self):
+        return float(self.L.oc_energy(self.h))
+
+    def springs(self):
+        ns = self.L.oc_spring_count(self.h)
+        pairs = np.zeros(2 * max(ns, 1), np.uint32)
+        rest = np.zeros(max(ns, 1), np.float32)
+        ks = np.zeros(max(ns, 1), np.float32)
+        self.L.oc_get_springs(self.h, pairs, rest, ks)
+        return pairs[:2 * ns].reshape(-1, 2), rest[:ns], ks[:ns]
+
+    def _get_state(self, *a):
+        self.L.oc_get_state(self.h, *a)
+
+    def _describe(self, a, b, c):
+        return self.L.oc_describe(self.h, a, b, c)
+
+    def _get_contacts(self, *a):
+        return self.L.oc_get_contacts(self.h, *a)
+
+    def _build_system(self, dt):
+        return self.L.oc_build_system(self.h, dt)
+
+    def _get_system(self, *a):
+        self.L.oc_get_system(self.h, *a)
+
+
+class RefCloth(_Base):
+    """The reference library (compiled from its sources)."""
+
+    def __init__(self, mesh, cdef, restated: bool = True):
+        super().__init__(mesh, cdef)
+        self.L = ref_lib()
+        self.h = self.L.ref_cloth_create(self._verts, self.n, self._tris, self.t, self._sew, self._nsew,
+                                         self._def, 1 if restated else 0)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.ref_cloth_destroy(self.h)
+            self.h = None
+
+    def set_gravity(self, g):
+        self.L.ref_cloth_set_gravity(self.h, np.asarray(g, np.float32))
+
+    def set_type(self, vertex, ty):
+        self.L.ref_cloth_set_type(self.h, vertex, ty)
+
+    def apply_force(self, vertex, f):
+        self.L.ref_cloth_apply_force(self.h, vertex, np.asarray(f, np.float32))
+
+    def apply_translation(self, vertex, t):
+        self.L.ref_cloth_apply_translation(self.h, vertex, np.asarray(t, np.float32))
+
+    def set_position(self, vertex, x):
+        self.L.ref_cloth_set_position(self.h, vertex, np.asarray(x, np.float32))
+
+    def set_velocity(self, vertex, v):
+        self.L.ref_cloth_set_velocity(self.h, vertex, np.asarray(v, np.float32))
+
+    def add_sphere(self, center, radius, friction):
+        self.L.ref_cloth_add_sphere(self.h, np.asarray(center, np.float32), radius, friction)
+
+    def step(self, dt, vel_iters=8, pos_iters=2, full=False):
+        self.L.ref_cloth_step(self.h, dt, vel_iters, pos_iters, 1 if full else 0)
+        return {"iterations": int(self.L.ref_last_iterations())}
+
+    def energy(self):
+        return float(self.L.ref_cloth_energy(self.h))
+
+    def _get_state(self, *a):
+        self.L.ref_cloth_get_state(self.h, *a)
+
+    def _describe(self, a, b, c):
+        return self.L.ref_cloth_describe(self.h, a, b, c)
+
+    def _get_contacts(self, *a):
+        return self.L.ref_cloth_get_contacts(self.h, *a)
+
+    def _build_system(self, dt):
+        return self.L.ref_cloth_build_system(self.h, dt)
+
+    def _get_system(self, *a):
+        self.L.ref_cloth_get_system(self.h, *a)
+
+
+def ref_profile():
+    """Accumulated reference profile scopes: {name: (seconds, calls)}."""
+    L = ref_lib()
+    k = L.ref_profile_read(None, 0, np.zeros(64, np.float64), np.zeros(64, np.uint64))
+    buf = C.create_string_buffer(4096)
+    secs = np.zeros(max(k, 1), np.float64)
+    calls = np.zeros(max(k, 1), np.uint64)
+    L.ref_profile_read(buf, 4096, secs, calls)
+    names = buf.value.decode().split("\n")[:k]
+    return {nm: (float(secs[i]), int(calls[i])) for i, nm in enumerate(names)}
+
+
+def ref_profile_reset():
+    ref_lib().ref_profile_reset()
+
+
+def mpcg(system, stop_rule=STOP_REFERENCE, tol=0.0, max_iterations=20, dot=DOT_F32):
+    """The oracle's MPCG on an exported system; returns (x (n,3), iterations, stats)."""
+    L = port_lib()
+    n = system["rowptr"].size - 1
+    x = np.zeros(3 * n, np.float32)
+    stats = np.zeros(3, np.float64)
+    it = L.oc_mpcg(n, system["rowptr"], system["cols"], system["vals"], system["b"], system["S"],
+                   system["x0"], stop_rule, tol, max_iterations, dot, x, stats)
+    return x.reshape(-1, 3), int(it), {"delta0": stats[0], "b_delta": stats[1], "delta": stats[2]}
+
+
+def solve_f64(system, tol=1e-12, max_iterations=100000):
+    """FP64 filtered Jacobi-PCG of the same system; returns x (n,3) float64."""
+    L = port_lib()
+    n = system["rowptr"].size - 1
+    x = np.zeros(3 * n, np.float64)
+    it = L.oc_solve_f64(n, system["rowptr"], system["cols"], system["vals"], system["b"], system["S"],
+                        system["x0"], tol, max_iterations, x)
+    return x.reshape(-1, 3), int(it)

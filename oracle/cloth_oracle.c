@@ -1,0 +1,1430 @@
+/*
+ * CPU restatement of Bounce's implicit cloth step -- test infrastructure only
+ * (parity oracle; see cloth_oracle.h).  Every function names the reference
+ * file and lines it follows.  Vector and matrix helpers evaluate in the same
+ * order as the reference's inline operators (include/bounce/common/math/
+ * vec3.h, mat33.h, vec2.h, mat22.h), which is what makes the results
+ * bit-identical to the compiled reference in reference mode.
+ */
+#include "cloth_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------ */
+/* math helpers, same evaluation order as the reference's operators          */
+/* ------------------------------------------------------------------------ */
+
+typedef struct { float x, y, z; } v3;
+typedef struct { v3 x, y, z; } m33; /* column-major, like b3Mat33 */
+typedef struct { float x, y; } v2;
+
+static const float kEps = FLT_EPSILON;         /* B3_EPSILON, settings.h:42 */
+static const float kAabbExtension = 0.2f;       /* settings.h:54 */
+static const float kAabbMultiplier = 2.0f;      /* settings.h:60 */
+static const float kLinearSlop = 0.005f;        /* settings.h:63 */
+static const float kMaxLinearCorrection = 0.2f; /* settings.h:95 */
+static const float kBaumgarte = 0.1f;           /* settings.h:101 */
+
+static inline v3 V(float x, float y, float z) { v3 r = {x, y, z}; return r; }
+static inline v3 vadd(v3 a, v3 b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 vsub(v3 a, v3 b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 vscale(float s, v3 v) { return V(s * v.x, s * v.y, s * v.z); }
+static inline v3 vdiv(v3 v, float s) { return V(v.x / s, v.y / s, v.z / s); }
+static inline v3 vneg(v3 v) { return V(-v.x, -v.y, -v.z); }
+static inline float vdot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline v3 vcross(v3 a, v3 b)
+{
+    return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline float vlength(v3 v) { return sqrtf(v.x * v.x + v.y * v.y + v.z * v.z); }
+static inline v3 vmin(v3 a, v3 b)
+{
+    return V(a.x < b.x ? a.x : b.x, a.y < b.y ? a.y : b.y, a.z < b.z ? a.z : b.z);
+}
+static inline v3 vmax(v3 a, v3 b)
+{
+    return V(a.x > b.x ? a.x : b.x, a.y > b.y ? a.y : b.y, a.z > b.z ? a.z : b.z);
+}
+static inline v3 vzero(void) { return V(0.0f, 0.0f, 0.0f); }
+
+static inline m33 M3(v3 x, v3 y, v3 z) { m33 m = {x, y, z}; return m; }
+static inline m33 mzero(void) { return M3(vzero(), vzero(), vzero()); }
+static inline m33 mident(void)
+{
+    return M3(V(1.0f, 0.0f, 0.0f), V(0.0f, 1.0f, 0.0f), V(0.0f, 0.0f, 1.0f));
+}
+static inline m33 mdiag3(float x, float y, float z)
+{
+    return M3(V(x, 0.0f, 0.0f), V(0.0f, y, 0.0f), V(0.0f, 0.0f, z));
+}
+static inline m33 madd(m33 a, m33 b) { return M3(vadd(a.x, b.x), vadd(a.y, b.y), vadd(a.z, b.z)); }
+static inline m33 msub(m33 a, m33 b) { return M3(vsub(a.x, b.x), vsub(a.y, b.y), vsub(a.z, b.z)); }
+static inline m33 mscale(float s, m33 a) { return M3(vscale(s, a.x), vscale(s, a.y), vscale(s, a.z)); }
+static inline m33 mouter(v3 a, v3 b) { return M3(vscale(b.x, a), vscale(b.y, a), vscale(b.z, a)); }
+/* A * v = v.x * A.x + v.y * A.y + v.z * A.z (mat33.h:129-132) */
+static inline v3 mmul(m33 a, v3 v)
+{
+    return vadd(vadd(vscale(v.x, a.x), vscale(v.y, a.y)), vscale(v.z, a.z));
+}
+static inline void madd_to(m33* a, m33 b)
+{
+    a->x = vadd(a->x, b.x);
+    a->y = vadd(a->y, b.y);
+    a->z = vadd(a->z, b.z);
+}
+static inline void msub_to(m33* a, m33 b)
+{
+    a->x = vsub(a->x, b.x);
+    a->y = vsub(a->y, b.y);
+    a->z = vsub(a->z, b.z);
+}
+
+static inline v2 W(float x, float y) { v2 r = {x, y}; return r; }
+
+/* b3Perp (vec3.h:255-266): unnormalised perpendicular. */
+static inline v3 vperp(v3 v)
+{
+    if (fabsf(v.x) >= 0.57735027f) return V(v.y, -v.x, 0.0f);
+    return V(0.0f, v.z, -v.y);
+}
+
+/* ------------------------------------------------------------------------ */
+/* sparse rows with the reference's list semantics                           */
+/* ------------------------------------------------------------------------ */
+
+/* One sparse row.  Blocks are kept in first-touch (append) order; the
+ * reference's singly linked row (sparse_mat33.h:27-32, :194-216) pushes each
+ * new block to the front, so its list order is the reverse of this array. */
+typedef struct {
+    uint32_t* cols;
+    m33* vals;
+    uint32_t count, cap;
+} lrow;
+
+static m33* lrow_at(lrow* r, uint32_t col)
+{
+    for (uint32_t k = 0; k < r->count; ++k)
+        if (r->cols[k] == col) return r->vals + k;
+    if (r->count == r->cap) {
+        r->cap = r->cap ? 2 * r->cap : 8;
+        r->cols = (uint32_t*)realloc(r->cols, r->cap * sizeof(uint32_t));
+        r->vals = (m33*)realloc(r->vals, r->cap * sizeof(m33));
+    }
+    r->cols[r->count] = col;
+    r->vals[r->count] = mzero();
+    return r->vals + r->count++;
+}
+
+static int lrow_find(const lrow* r, uint32_t col)
+{
+    for (uint32_t k = 0; k < r->count; ++k)
+        if (r->cols[k] == col) return (int)k;
+    return -1;
+}
+
+static void lrows_clear(lrow* rows, uint32_t n)
+{
+    for (uint32_t i = 0; i < n; ++i) rows[i].count = 0;
+}
+
+static void lrows_free(lrow* rows, uint32_t n)
+{
+    if (!rows) return;
+    for (uint32_t i = 0; i < n; ++i) {
+        free(rows[i].cols);
+        free(rows[i].vals);
+    }
+    free(rows);
+}
+
+/* ------------------------------------------------------------------------ */
+/* cloth state                                                               */
+/* ------------------------------------------------------------------------ */
+
+enum { F_STRETCH = 0, F_SHEAR = 1, F_SPRING = 2 };
+
+typedef struct {
+    int type;
+    uint32_t a, b, c;    /* triangle index (a) for stretch/shear; vertices (a, b) for springs */
+    float ks, kd, p0, p1; /* stretch: bu, bv; spring: L0 */
+} force_t;
+
+typedef struct {
+    v3 center;
+    float radius, friction;
+    v3 fat_lo, fat_hi; /* the shape's proxy in the world broadphase */
+} sphere_t;
+
+typedef struct {
+    uint32_t particle, shape;
+    int active;
+    v3 normal1, local_point2, tangent1, tangent2;
+    float normal_impulse;
+    v2 tangent_impulse;
+} contact_t;
+
+struct oc_cloth {
+    uint32_t n, t;
+    float def[8];
+    uint32_t* tris;
+
+    /* particles, by vertex index */
+    v3 *x, *v, *f, *y, *mx;
+    float *mass, *inv_mass, *radius, *friction;
+    uint8_t* type;
+    v3 *fat_lo, *fat_hi;
+    /* particle list (cloth.cpp:319 PushFront): order[k] = vertex of list slot k */
+    uint32_t* order;
+
+    /* triangles rest state (cloth.cpp:155-191) */
+    float *du1, *dv1, *du2, *dv2, *inv_det, *alpha;
+
+    /* forces in list (application) order */
+    force_t* forces;
+    uint32_t nforce;
+    uint32_t nspring;
+
+    v3 gravity;
+    sphere_t* spheres;
+    uint32_t nsphere;
+
+    /* body-contact list stored tail first: element [ncontact-1] is the list head */
+    contact_t* contacts;
+    uint32_t ncontact, contact_cap;
+
+    int stop_rule, dot;
+    float tol;
+    uint32_t max_iter;
+
+    /* solver scratch */
+    lrow *dfdx, *dfdv;
+    uint32_t *a_rowptr, *a_cols;
+    m33* a_vals;
+    uint32_t a_cap;
+    v3 *sx, *sv, *sf, *sy, *sx0, *b, *dvsol;
+    float* Sflag;
+    uint32_t* solver_of_vertex;
+    uint32_t sys_nnz;
+};
+
+/* ------------------------------------------------------------------------ */
+/* construction                                                              */
+/* ------------------------------------------------------------------------ */
+
+typedef struct { uint32_t a, b, tri, slot; } dedge;
+
+static int dedge_cmp(const void* pa, const void* pb)
+{
+    const dedge* x = (const dedge*)pa;
+    const dedge* y = (const dedge*)pb;
+    if (x->a != y->a) return x->a < y->a ? -1 : 1;
+    if (x->b != y->b) return x->b < y->b ? -1 : 1;
+    if (x->tri != y->tri) return x->tri < y->tri ? -1 : 1;
+    if (x->slot != y->slot) return x->slot < y->slot ? -1 : 1;
+    return 0;
+}
+
+static void push_force(oc_cloth* c, force_t f)
+{
+    c->forces[c->nforce++] = f;
+}
+
+/* b3Cloth::b3Cloth (cloth.cpp:96-266) with b3FindSharedEdges (:40-94)
+ * restated over a sorted directed-edge table: same pairs, same order. */
+oc_cloth* oc_create(const float* vertices, uint32_t n, const uint32_t* triangles, uint32_t t,
+                    const uint32_t* sewing, uint32_t nsew, const float* def)
+{
+    oc_cloth* c = (oc_cloth*)calloc(1, sizeof(oc_cloth));
+    c->n = n;
+    c->t = t;
+    memcpy(c->def, def, sizeof(c->def));
+    c->tris = (uint32_t*)malloc(3 * (size_t)t * sizeof(uint32_t));
+    memcpy(c->tris, triangles, 3 * (size_t)t * sizeof(uint32_t));
+
+    c->x = (v3*)calloc(n, sizeof(v3));
+    c->v = (v3*)calloc(n, sizeof(v3));
+    c->f = (v3*)calloc(n, sizeof(v3));
+    c->y = (v3*)calloc(n, sizeof(v3));
+    c->mx = (v3*)calloc(n, sizeof(v3));
+    c->mass = (float*)calloc(n, sizeof(float));
+    c->inv_mass = (float*)calloc(n, sizeof(float));
+    c->radius = (float*)calloc(n, sizeof(float));
+    c->friction = (float*)calloc(n, sizeof(float));
+    c->type = (uint8_t*)calloc(n, 1);
+    c->fat_lo = (v3*)calloc(n, sizeof(v3));
+    c->fat_hi = (v3*)calloc(n, sizeof(v3));
+    c->order = (uint32_t*)calloc(n, sizeof(uint32_t));
+    c->solver_of_vertex = (uint32_t*)calloc(n, sizeof(uint32_t));
+
+    float thickness = def[6], fric = def[7];
+    /* particles: mass 1 -> dynamic (particle.cpp:24-44), proxy fattened by
+     * B3_AABB_EXTENSION (cloth.cpp:312-317, broad_phase.cpp:78-82) */
+    for (uint32_t i = 0; i < n; ++i) {
+        c->x[i] = V(vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]);
+        c->type[i] = OC_DYNAMIC;
+        c->radius[i] = thickness;
+        c->friction[i] = fric;
+        v3 r = V(thickness, thickness, thickness);
+        v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
+        c->fat_lo[i] = vsub(vsub(c->x[i], r), ext);
+        c->fat_hi[i] = vadd(vadd(c->x[i], r), ext);
+        /* PushFront: the newest particle heads the list */
+        c->order[n - 1 - i] = i;
+    }
+
+    /* ComputeMass (cloth.cpp:388-427) */
+    const float inv3 = 1.0f / 3.0f;
+    const float rho = def[0];
+    for (uint32_t k = 0; k < t; ++k) {
+        v3 a = c->x[triangles[3 * k]], b = c->x[triangles[3 * k + 1]], cc = c->x[triangles[3 * k + 2]];
+        float area = 0.5f * vlength(vcross(vsub(b, a), vsub(cc, a)));
+        float m = rho * area;
+        c->mass[triangles[3 * k]] += inv3 * m;
+        c->mass[triangles[3 * k + 1]] += inv3 * m;
+        c->mass[triangles[3 * k + 2]] += inv3 * m;
+    }
+    for (uint32_t i = 0; i < n; ++i) c->inv_mass[i] = 1.0f / c->mass[i];
+
+    /* triangles (cloth.cpp:129-215) */
+    c->du1 = (float*)malloc(t * sizeof(float));
+    c->dv1 = (float*)malloc(t * sizeof(float));
+    c->du2 = (float*)malloc(t * sizeof(float));
+    c->dv2 = (float*)malloc(t * sizeof(float));
+    c->inv_det = (float*)malloc(t * sizeof(float));
+    c->alpha = (float*)malloc(t * sizeof(float));
+
+    /* forces are created in this order and pushed to the front of the force
+     * list (cloth.cpp:353-358); we build the creation order first. */
+    size_t fcap = 2 * (size_t)t + 3 * (size_t)t + nsew + 1;
+    force_t* created = (force_t*)calloc(fcap, sizeof(force_t));
+    uint32_t ncreated = 0;
+
+    for (uint32_t k = 0; k < t; ++k) {
+        v3 A = c->x[triangles[3 * k]], B = c->x[triangles[3 * k + 1]], C = c->x[triangles[3 * k + 2]];
+        v3 AB = vsub(B, A), AC = vsub(C, A);
+        float u1 = 0.0f, v1 = 0.0f;
+        float u2 = vlength(AB), v2_ = 0.0f;
+        v3 n_AB = vdiv(AB, u2);
+        float A2 = vlength(vcross(AB, AC));
+        float u3 = vdot(AC, n_AB);
+        float v3_ = A2 / u2;
+        float du1 = u2 - u1, dv1 = v2_ - v1, du2 = u3 - u1, dv2 = v3_ - v1;
+        c->du1[k] = du1;
+        c->dv1[k] = dv1;
+        c->du2[k] = du2;
+        c->dv2[k] = dv2;
+        float det = du1 * dv2 - du2 * dv1;
+        c->inv_det[k] = 1.0f / det;
+        c->alpha[k] = 0.5f * A2;
+        if (def[1] > 0.0f) {
+            force_t f = {F_STRETCH, k, 0, 0, def[1], def[5], 1.0f, 1.0f};
+            created[ncreated++] = f;
+        }
+        if (def[2] > 0.0f) {
+            force_t f = {F_SHEAR, k, 0, 0, def[2], def[5], 0.0f, 0.0f};
+            created[ncreated++] = f;
+        }
+    }
+
+    /* bending springs between non-shared vertices (cloth.cpp:218-245) */
+    dedge* edges = (dedge*)malloc(3 * (size_t)t * sizeof(dedge) + 1);
+    for (uint32_t k = 0; k < t; ++k) {
+        for (uint32_t e = 0; e < 3; ++e) {
+            dedge d = {triangles[3 * k + e], triangles[3 * k + (e + 1) % 3], k, e};
+            edges[3 * k + e] = d;
+        }
+    }
+    qsort(edges, 3 * (size_t)t, sizeof(dedge), dedge_cmp);
+    c->nspring = 0;
+    for (uint32_t i = 0; i < t; ++i) {
+        const uint32_t* t1 = triangles + 3 * i;
+        for (uint32_t j1 = 0; j1 < 3; ++j1) {
+            uint32_t k1 = j1 + 1 < 3 ? j1 + 1 : 0;
+            uint32_t a = t1[j1], b = t1[k1];
+            /* lower bound of (b, a, i + 1, 0) */
+            size_t lo = 0, hi = 3 * (size_t)t;
+            dedge key = {b, a, i + 1, 0};
+            while (lo < hi) {
+                size_t mid = (lo + hi) / 2;
+                if (dedge_cmp(edges + mid, &key) < 0) lo = mid + 1;
+                else hi = mid;
+            }
+            uint32_t last = UINT32_MAX;
+            for (size_t q = lo; q < 3 * (size_t)t && edges[q].a == b && edges[q].b == a; ++q) {
+                if (edges[q].tri == last) continue;
+                last = edges[q].tri;
+                const uint32_t* t2 = triangles + 3 * edges[q].tri;
+                uint32_t k2 = edges[q].slot + 1 < 3 ? edges[q].slot + 1 : 0;
+                uint32_t k3 = k1 + 1 < 3 ? k1 + 1 : 0;
+                uint32_t k4 = k2 + 1 < 3 ? k2 + 1 : 0;
+                uint32_t p3 = t1[k3], p4 = t2[k4];
+                /* b3SpringForceDef::Initialize (spring_force.cpp:25-35) */
+                float L0 = vlength(vsub(c->x[p3], c->x[p4]));
+                if (def[3] > 0.0f) {
+                    force_t f = {F_SPRING, p3, p4, 0, def[3], def[5], L0, 0.0f};
+                    if (ncreated == fcap) {
+                        fcap *= 2;
+                        created = (force_t*)realloc(created, fcap * sizeof(force_t));
+                    }
+                    created[ncreated++] = f;
+                    c->nspring++;
+                }
+            }
+        }
+    }
+    free(edges);
+
+    /* sewing springs (cloth.cpp:248-262) */
+    for (uint32_t s = 0; s < nsew; ++s) {
+        uint32_t p1 = sewing[4 * s + 2], p2 = sewing[4 * s + 3];
+        float L0 = vlength(vsub(c->x[p1], c->x[p2]));
+        if (def[4] > 0.0f) {
+            force_t f = {F_SPRING, p1, p2, 0, def[4], def[5], L0, 0.0f};
+            if (ncreated == fcap) {
+                fcap *= 2;
+                created = (force_t*)realloc(created, fcap * sizeof(force_t));
+            }
+            created[ncreated++] = f;
+            c->nspring++;
+        }
+    }
+
+    c->forces = (force_t*)malloc((ncreated + 1) * sizeof(force_t));
+    c->nforce = 0;
+    for (uint32_t k = ncreated; k-- > 0;) push_force(c, created[k]);
+    free(created);
+
+    c->gravity = vzero();
+    c->stop_rule = OC_STOP_REFERENCE;
+    c->tol = 0.0f;
+    c->max_iter = 20;
+    c->dot = OC_DOT_F32;
+
+    c->dfdx = (lrow*)calloc(n, sizeof(lrow));
+    c->dfdv = (lrow*)calloc(n, sizeof(lrow));
+    c->a_rowptr = (uint32_t*)calloc(n + 1, sizeof(uint32_t));
+    c->sx = (v3*)calloc(n, sizeof(v3));
+    c->sv = (v3*)calloc(n, sizeof(v3));
+    c->sf = (v3*)calloc(n, sizeof(v3));
+    c->sy = (v3*)calloc(n, sizeof(v3));
+    c->sx0 = (v3*)calloc(n, sizeof(v3));
+    c->b = (v3*)calloc(n, sizeof(v3));
+    c->dvsol = (v3*)calloc(n, sizeof(v3));
+    c->Sflag = (float*)calloc(n, sizeof(float));
+    return c;
+}
+
+void oc_destroy(oc_cloth* c)
+{
+    if (!c) return;
+    free(c->tris);
+    free(c->x); free(c->v); free(c->f); free(c->y); free(c->mx);
+    free(c->mass); free(c->inv_mass); free(c->radius); free(c->friction); free(c->type);
+    free(c->fat_lo); free(c->fat_hi); free(c->order); free(c->solver_of_vertex);
+    free(c->du1); free(c->dv1); free(c->du2); free(c->dv2); free(c->inv_det); free(c->alpha);
+    free(c->forces); free(c->spheres); free(c->contacts);
+    lrows_free(c->dfdx, c->n);
+    lrows_free(c->dfdv, c->n);
+    free(c->a_rowptr); free(c->a_cols); free(c->a_vals);
+    free(c->sx); free(c->sv); free(c->sf); free(c->sy); free(c->sx0); free(c->b); free(c->dvsol);
+    free(c->Sflag);
+    free(c);
+}
+
+/* ------------------------------------------------------------------------ */
+/* particle API (particle.cpp, particle.h)                                   */
+/* ------------------------------------------------------------------------ */
+
+/* b3BroadPhase::MoveProxy (broad_phase.cpp:99-149) for a particle proxy. */
+static void move_proxy(oc_cloth* c, uint32_t i, v3 displacement)
+{
+    v3 r = V(c->radius[i], c->radius[i], c->radius[i]);
+    v3 lo = vsub(c->x[i], r), hi = vadd(c->x[i], r);
+    v3 flo = c->fat_lo[i], fhi = c->fat_hi[i];
+    int contains = flo.x <= lo.x && lo.x <= fhi.x && flo.y <= lo.y && lo.y <= fhi.y &&
+                   flo.z <= lo.z && lo.z <= fhi.z && flo.x <= hi.x && hi.x <= fhi.x &&
+                   flo.y <= hi.y && hi.y <= fhi.y && flo.z <= hi.z && hi.z <= fhi.z;
+    if (contains) return;
+    v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
+    lo = vsub(lo, ext);
+    hi = vadd(hi, ext);
+    v3 d = vscale(kAabbMultiplier, displacement);
+    if (d.x < 0.0f) lo.x += d.x; else hi.x += d.x;
+    if (d.y < 0.0f) lo.y += d.y; else hi.y += d.y;
+    if (d.z < 0.0f) lo.z += d.z; else hi.z += d.z;
+    c->fat_lo[i] = lo;
+    c->fat_hi[i] = hi;
+}
+
+/* Remove every body contact of particle i (particle.cpp:66-83). */
+static void destroy_particle_contacts(oc_cloth* c, uint32_t i)
+{
+    uint32_t w = 0;
+    for (uint32_t k = 0; k < c->ncontact; ++k)
+        if (c->contacts[k].particle != i) c->contacts[w++] = c->contacts[k];
+    c->ncontact = w;
+}
+
+void oc_set_gravity(oc_cloth* c, const float* g) { c->gravity = V(g[0], g[1], g[2]); }
+
+/* b3Particle::SetType (particle.cpp:121-143) */
+void oc_set_type(oc_cloth* c, uint32_t i, int type)
+{
+    if (c->type[i] == type) return;
+    c->type[i] = (uint8_t)type;
+    c->f[i] = vzero();
+    if (type == OC_STATIC) {
+        c->v[i] = vzero();
+        c->y[i] = vzero();
+        move_proxy(c, i, vzero());
+    }
+    destroy_particle_contacts(c, i);
+}
+
+/* b3Particle::ApplyForce / ApplyTranslation / SetPosition / SetVelocity (particle.h:205-271) */
+void oc_apply_force(oc_cloth* c, uint32_t i, const float* f)
+{
+    if (c->type[i] != OC_DYNAMIC) return;
+    c->f[i] = vadd(c->f[i], V(f[0], f[1], f[2]));
+}
+
+void oc_apply_translation(oc_cloth* c, uint32_t i, const float* t)
+{
+    c->y[i] = vadd(c->y[i], V(t[0], t[1], t[2]));
+}
+
+void oc_set_position(oc_cloth* c, uint32_t i, const float* x)
+{
+    v3 p = V(x[0], x[1], x[2]);
+    v3 d = vsub(p, c->x[i]);
+    c->x[i] = p;
+    c->y[i] = vzero();
+    move_proxy(c, i, d);
+}
+
+void oc_set_velocity(oc_cloth* c, uint32_t i, const float* v)
+{
+    if (c->type[i] == OC_STATIC) return;
+    c->v[i] = V(v[0], v[1], v[2]);
+}
+
+/* A static body at `center` with one sphere shape: the shape proxy is the
+ * sphere's AABB (sphere_shape.cpp:53-59) fattened by B3_AABB_EXTENSION. */
+int oc_add_sphere(oc_cloth* c, const float* center, float radius, float friction)
+{
+    c->spheres = (sphere_t*)realloc(c->spheres, (c->nsphere + 1) * sizeof(sphere_t));
+    sphere_t* s = c->spheres + c->nsphere;
+    s->center = V(center[0], center[1], center[2]);
+    s->radius = radius;
+    s->friction = friction;
+    v3 r = V(radius, radius, radius);
+    v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
+    s->fat_lo = vsub(vsub(s->center, r), ext);
+    s->fat_hi = vadd(vadd(s->center, r), ext);
+    return (int)c->nsphere++;
+}
+
+void oc_set_solver(oc_cloth* c, int stop_rule, float tol, uint32_t max_iterations, int dot)
+{
+    c->stop_rule = stop_rule;
+    c->tol = tol;
+    c->max_iter = max_iterations;
+    c->dot = dot;
+}
+
+/* ------------------------------------------------------------------------ */
+/* force elements                                                            */
+/* ------------------------------------------------------------------------ */
+
+static void add9(lrow* rows, const uint32_t* ids, m33 K[3][3])
+{
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) madd_to(lrow_at(rows + ids[i], ids[j]), K[i][j]);
+}
+
+/* b3StrechForce::Apply (strech_force.cpp:59-329) */
+static void apply_stretch(oc_cloth* c, const force_t* fo)
+{
+    uint32_t t = fo->a;
+    float alpha = c->alpha[t], du1 = c->du1[t], dv1 = c->dv1[t], du2 = c->du2[t], dv2 = c->dv2[t];
+    float inv_det = c->inv_det[t];
+    uint32_t ids[3] = {c->solver_of_vertex[c->tris[3 * t]], c->solver_of_vertex[c->tris[3 * t + 1]],
+                       c->solver_of_vertex[c->tris[3 * t + 2]]};
+    float ks = fo->ks, kd = fo->kd, bu = fo->p0, bv = fo->p1;
+    v3 x1 = c->sx[ids[0]], x2 = c->sx[ids[1]], x3 = c->sx[ids[2]];
+    v3 vs[3] = {c->sv[ids[0]], c->sv[ids[1]], c->sv[ids[2]]};
+    m33 I = mident();
+    v3 dx1 = vsub(x2, x1), dx2 = vsub(x3, x1);
+    v3 wu = vscale(inv_det, vsub(vscale(dv2, dx1), vscale(dv1, dx2)));
+    float len_wu = vlength(wu);
+    v3 wv = vscale(inv_det, vadd(vscale(-du2, dx1), vscale(du1, dx2)));
+    float len_wv = vlength(wv);
+    float dwudx[3] = {inv_det * (dv1 - dv2), inv_det * dv2, -inv_det * dv1};
+    float dwvdx[3] = {inv_det * (du2 - du1), -inv_det * du2, inv_det * du1};
+    v3 f[3] = {vzero(), vzero(), vzero()};
+    m33 K[3][3];
+
+    for (int dir = 0; dir < 2; ++dir) {
+        v3 w = dir == 0 ? wu : wv;
+        float len = dir == 0 ? len_wu : len_wv;
+        const float* dw = dir == 0 ? dwudx : dwvdx;
+        float bdir = dir == 0 ? bu : bv;
+        if (!(len > 0.0f)) continue;
+        float inv_len = 1.0f / len;
+        v3 nw = vscale(inv_len, w);
+        v3 dC[3];
+        for (int i = 0; i < 3; ++i) dC[i] = vscale(alpha * dw[i], nw);
+        if (ks > 0.0f && len > bdir) {
+            float C = alpha * (len - bdir);
+            for (int i = 0; i < 3; ++i) f[i] = vadd(f[i], vscale(-ks * C, dC[i]));
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    m33 d2 = mscale(alpha * inv_len * dw[i] * dw[j], msub(I, mouter(nw, nw)));
+                    K[i][j] = mscale(-ks, madd(mouter(dC[i], dC[j]), mscale(C, d2)));
+                }
+            add9(c->dfdx, ids, K);
+        }
+        if (kd > 0.0f) {
+            float dCdt = 0.0f;
+            for (int i = 0; i < 3; ++i) dCdt += vdot(dC[i], vs[i]);
+            for (int i = 0; i < 3; ++i) f[i] = vadd(f[i], vscale(-kd * dCdt, dC[i]));
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) K[i][j] = mscale(-kd, mouter(dC[i], dC[j]));
+            add9(c->dfdv, ids, K);
+        }
+    }
+    for (int i = 0; i < 3; ++i) c->sf[ids[i]] = vadd(c->sf[ids[i]], f[i]);
+}
+
+/* b3ShearForce::Apply (shear_force.cpp:57-212); the second-derivative term
+ * is left out as in the reference (:142-144). */
+static void apply_shear(oc_cloth* c, const force_t* fo)
+{
+    uint32_t t = fo->a;
+    float alpha = c->alpha[t], du1 = c->du1[t], dv1 = c->dv1[t], du2 = c->du2[t], dv2 = c->dv2[t];
+    float inv_det = c->inv_det[t];
+    uint32_t ids[3] = {c->solver_of_vertex[c->tris[3 * t]], c->solver_of_vertex[c->tris[3 * t + 1]],
+                       c->solver_of_vertex[c->tris[3 * t + 2]]};
+    float ks = fo->ks, kd = fo->kd;
+    v3 x1 = c->sx[ids[0]], x2 = c->sx[ids[1]], x3 = c->sx[ids[2]];
+    v3 vs[3] = {c->sv[ids[0]], c->sv[ids[1]], c->sv[ids[2]]};
+    v3 dx1 = vsub(x2, x1), dx2 = vsub(x3, x1);
+    v3 wu = vscale(inv_det, vsub(vscale(dv2, dx1), vscale(dv1, dx2)));
+    v3 wv = vscale(inv_det, vadd(vscale(-du2, dx1), vscale(du1, dx2)));
+    float dwudx[3] = {inv_det * (dv1 - dv2), inv_det * dv2, -inv_det * dv1};
+    float dwvdx[3] = {inv_det * (du2 - du1), -inv_det * du2, inv_det * du1};
+    v3 f[3] = {vzero(), vzero(), vzero()};
+    m33 K[3][3];
+    v3 dC[3];
+    for (int i = 0; i < 3; ++i) dC[i] = vscale(alpha, vadd(vscale(dwudx[i], wv), vscale(dwvdx[i], wu)));
+    if (ks > 0.0f) {
+        float C = alpha * vdot(wu, wv);
+        for (int i = 0; i < 3; ++i) f[i] = vadd(f[i], vscale(-ks * C, dC[i]));
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) K[i][j] = mscale(-ks, mouter(dC[i], dC[j]));
+        add9(c->dfdx, ids, K);
+    }
+    if (kd > 0.0f) {
+        float dCdt = 0.0f;
+        for (int i = 0; i < 3; ++i) dCdt += vdot(dC[i], vs[i]);
+        for (int i = 0; i < 3; ++i) f[i] = vadd(f[i], vscale(-kd * dCdt, dC[i]));
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) K[i][j] = mscale(-kd, mouter(dC[i], dC[j]));
+        add9(c->dfdv, ids, K);
+    }
+    for (int i = 0; i < 3; ++i) c->sf[ids[i]] = vadd(c->sf[ids[i]], f[i]);
+}
+
+/* b3SpringForce::Apply (spring_force.cpp:53-120), including the reference's
+ * unnormalised outer product in K11 (:88). */
+static void apply_spring(oc_cloth* c, const force_t* fo)
+{
+    uint32_t i1 = c->solver_of_vertex[fo->a], i2 = c->solver_of_vertex[fo->b];
+    float ks = fo->ks, kd = fo->kd, L0 = fo->p0;
+    v3 x1 = c->sx[i1], v1 = c->sv[i1], x2 = c->sx[i2], v2_ = c->sv[i2];
+    m33 I = mident();
+    v3 f = vzero();
+    if (ks > 0.0f) {
+        v3 dx = vsub(x1, x2);
+        float L = vlength(dx);
+        if (L > L0) {
+            v3 dCdx = vdiv(dx, L);
+            f = vadd(f, vscale(-ks * (L - L0), dCdx));
+            m33 K11 = mscale(-ks, madd(mouter(dx, dx), mscale(1.0f - L0 / L, msub(I, mouter(dx, dx)))));
+            m33 K12 = mscale(-1.0f, K11);
+            madd_to(lrow_at(c->dfdx + i1, i1), K11);
+            madd_to(lrow_at(c->dfdx + i1, i2), K12);
+            madd_to(lrow_at(c->dfdx + i2, i1), K12);
+            madd_to(lrow_at(c->dfdx + i2, i2), K11);
+        }
+    }
+    if (kd > 0.0f) {
+        v3 dv = vsub(v1, v2_);
+        f = vadd(f, vscale(-kd, dv));
+        m33 K11 = mscale(-kd, I);
+        m33 K12 = mscale(-1.0f, K11);
+        madd_to(lrow_at(c->dfdv + i1, i1), K11);
+        madd_to(lrow_at(c->dfdv + i1, i2), K12);
+        madd_to(lrow_at(c->dfdv + i2, i1), K12);
+        madd_to(lrow_at(c->dfdv + i2, i2), K11);
+    }
+    c->sf[i1] = vadd(c->sf[i1], f);
+    c->sf[i2] = vsub(c->sf[i2], f);
+}
+
+/* ------------------------------------------------------------------------ */
+/* system formation                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* out = A * v over rows stored in append order, summed in the reference's
+ * list order (reverse of append), sparse_mat33.h:264-282. */
+static void lrows_mul(const lrow* rows, uint32_t n, const v3* v, v3* out)
+{
+    for (uint32_t i = 0; i < n; ++i) {
+        v3 acc = vzero();
+        for (uint32_t k = rows[i].count; k-- > 0;) acc = vadd(acc, mmul(rows[i].vals[k], v[rows[i].cols[k]]));
+        out[i] = acc;
+    }
+}
+
+/* Gather + forces + A and b (cloth_force_solver.cpp:142-204).  A is left in
+ * a_rowptr / a_cols / a_vals in the order its linked rows end up in after
+ * `M - h * dfdv - (h * h) * dfdx`: blocks that only dfdx touches (in reverse
+ * first-touch order), the diagonal, then the dfdv blocks in first-touch
+ * order (sparse_mat33.h:153-174 copies reverse a row; :194-216 and :235-250
+ * push new blocks to the front). */
+static void form_system(oc_cloth* c, float h)
+{
+    uint32_t n = c->n;
+    for (uint32_t k = 0; k < n; ++k) c->solver_of_vertex[c->order[k]] = k;
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t i = c->order[k];
+        c->sx[k] = c->x[i];
+        c->sv[k] = c->v[i];
+        c->sf[k] = c->f[i];
+        if (c->type[i] == OC_DYNAMIC) {
+            c->sf[k] = vadd(c->sf[k], vscale(c->mass[i], c->gravity));
+            c->Sflag[k] = 1.0f;
+        } else {
+            c->Sflag[k] = 0.0f;
+        }
+        c->sy[k] = c->y[i];
+        c->sx0[k] = c->mx[i];
+    }
+    lrows_clear(c->dfdx, n);
+    lrows_clear(c->dfdv, n);
+    for (uint32_t q = 0; q < c->nforce; ++q) {
+        const force_t* fo = c->forces + q;
+        if (fo->type == F_STRETCH) apply_stretch(c, fo);
+        else if (fo->type == F_SHEAR) apply_shear(c, fo);
+        else apply_spring(c, fo);
+    }
+
+    /* A */
+    uint32_t nnz = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t cnt = 1;
+        for (uint32_t e = 0; e < c->dfdv[k].count; ++e) cnt += c->dfdv[k].cols[e] != k;
+        for (uint32_t e = 0; e < c->dfdx[k].count; ++e) {
+            uint32_t j = c->dfdx[k].cols[e];
+            if (j != k && lrow_find(c->dfdv + k, j) < 0) ++cnt;
+        }
+        nnz += cnt;
+    }
+    if (nnz > c->a_cap) {
+        c->a_cap = nnz;
+        c->a_cols = (uint32_t*)realloc(c->a_cols, nnz * sizeof(uint32_t));
+        c->a_vals = (m33*)realloc(c->a_vals, nnz * sizeof(m33));
+    }
+    float hh = h * h;
+    uint32_t w = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        c->a_rowptr[k] = w;
+        const lrow* D = c->dfdv + k;
+        const lrow* K = c->dfdx + k;
+        /* dfdx-only blocks, newest first */
+        for (uint32_t e = K->count; e-- > 0;) {
+            uint32_t j = K->cols[e];
+            if (j == k || lrow_find(D, j) >= 0) continue;
+            m33 val = mzero();
+            msub_to(&val, mscale(hh, K->vals[e]));
+            c->a_cols[w] = j;
+            c->a_vals[w++] = val;
+        }
+        /* diagonal */
+        {
+            m33 val = mdiag3(c->mass[c->order[k]], c->mass[c->order[k]], c->mass[c->order[k]]);
+            int d = lrow_find(D, k);
+            if (d >= 0) msub_to(&val, mscale(h, D->vals[d]));
+            int kk = lrow_find(K, k);
+            if (kk >= 0) msub_to(&val, mscale(hh, K->vals[kk]));
+            c->a_cols[w] = k;
+            c->a_vals[w++] = val;
+        }
+        /* dfdv blocks in first-touch order */
+        for (uint32_t e = 0; e < D->count; ++e) {
+            uint32_t j = D->cols[e];
+            if (j == k) continue;
+            m33 val = mzero();
+            msub_to(&val, mscale(h, D->vals[e]));
+            int kk = lrow_find(K, j);
+            if (kk >= 0) msub_to(&val, mscale(hh, K->vals[kk]));
+            c->a_cols[w] = j;
+            c->a_vals[w++] = val;
+        }
+    }
+    c->a_rowptr[n] = w;
+    c->sys_nnz = w;
+
+    /* b = h * (f + h * (dfdx * v) + dfdx * y) */
+    v3* t1 = (v3*)malloc(n * sizeof(v3));
+    v3* t2 = (v3*)malloc(n * sizeof(v3));
+    lrows_mul(c->dfdx, n, c->sv, t1);
+    lrows_mul(c->dfdx, n, c->sy, t2);
+    for (uint32_t k = 0; k < n; ++k) {
+        v3 s = vadd(vadd(c->sf[k], vscale(h, t1[k])), t2[k]);
+        c->b[k] = vscale(h, s);
+    }
+    free(t1);
+    free(t2);
+}
+
+/* ------------------------------------------------------------------------ */
+/* MPCG                                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* Accumulator for a dot product in one of the three precisions. */
+typedef struct {
+    int mode;
+    float s32, c32;
+    double s64;
+} dacc;
+
+static inline void dacc_init(dacc* a, int mode)
+{
+    a->mode = mode;
+    a->s32 = 0.0f;
+    a->c32 = 0.0f;
+    a->s64 = 0.0;
+}
+
+static inline void dacc_add(dacc* a, v3 x, v3 y)
+{
+    if (a->mode == OC_DOT_F64) {
+        a->s64 += (double)x.x * (double)y.x + (double)x.y * (double)y.y + (double)x.z * (double)y.z;
+    } else if (a->mode == OC_DOT_COMPENSATED) {
+        /* Neumaier's variant of Kahan summation over the per-row terms */
+        float term = vdot(x, y);
+        float t = a->s32 + term;
+        if (fabsf(a->s32) >= fabsf(term)) a->c32 += (a->s32 - t) + term;
+        else a->c32 += (term - t) + a->s32;
+        a->s32 = t;
+    } else {
+        a->s32 += vdot(x, y);
+    }
+}
+
+static inline double dacc_get(const dacc* a)
+{
+    if (a->mode == OC_DOT_F64) return a->s64;
+    if (a->mode == OC_DOT_COMPENSATED) return (double)(a->s32 + a->c32);
+    return (double)a->s32;
+}
+
+static void csr_mul(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const m33* vals, const v3* v,
+                    v3* out)
+{
+    for (uint32_t i = 0; i < n; ++i) {
+        v3 acc = vzero();
+        for (uint32_t k = rowptr[i]; k < rowptr[i + 1]; ++k) acc = vadd(acc, mmul(vals[k], v[cols[k]]));
+        out[i] = acc;
+    }
+}
+
+static uint32_t mpcg(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const m33* vals, const v3* b,
+                     const float* Sflag, const v3* y, int stop_rule, float tol, uint32_t max_iter, int dot,
+                     v3* x, double* stats)
+{
+    m33* S = (m33*)malloc(n * sizeof(m33));
+    m33* IS = (m33*)malloc(n * sizeof(m33));
+    m33* invP = (m33*)malloc(n * sizeof(m33));
+    v3* r = (v3*)malloc(n * sizeof(v3));
+    v3* p = (v3*)malloc(n * sizeof(v3));
+    v3* s = (v3*)malloc(n * sizeof(v3));
+    v3* hv = (v3*)malloc(n * sizeof(v3));
+    v3* tmp = (v3*)calloc(n + 1, sizeof(v3));
+    v3* tmp2 = (v3*)malloc(n * sizeof(v3));
+    v3* bhat = (v3*)malloc(n * sizeof(v3));
+
+    /* Jacobi preconditioner from the diagonal blocks (:70-88) */
+    for (uint32_t i = 0; i < n; ++i) {
+        m33 a = mzero();
+        for (uint32_t k = rowptr[i]; k < rowptr[i + 1]; ++k)
+            if (cols[k] == i) { a = vals[k]; break; }
+        invP[i] = mdiag3(1.0f / a.x.x, 1.0f / a.y.y, 1.0f / a.z.z);
+        S[i] = Sflag[i] != 0.0f ? mident() : mzero();
+        IS[i] = msub(mident(), S[i]);
+    }
+    /* x = S y + (I - S) z with z = 0 (:90) */
+    for (uint32_t i = 0; i < n; ++i) {
+        tmp[i] = mmul(IS[i], vzero());
+        x[i] = vadd(mmul(S[i], y[i]), tmp[i]);
+    }
+    /* b_hat = S (b - A (I - S) z) (:92) */
+    csr_mul(n, rowptr, cols, vals, tmp, tmp2);
+    for (uint32_t i = 0; i < n; ++i) bhat[i] = mmul(S[i], vsub(b[i], tmp2[i]));
+    dacc acc;
+    dacc_init(&acc, dot);
+    for (uint32_t i = 0; i < n; ++i) dacc_add(&acc, bhat[i], mmul(invP[i], bhat[i]));
+    double b_delta = dacc_get(&acc);
+    /* r = S (b - A x), p = S P^-1 r, delta = r.p (:96-100) */
+    csr_mul(n, rowptr, cols, vals, x, tmp2);
+    for (uint32_t i = 0; i < n; ++i) r[i] = mmul(S[i], vsub(b[i], tmp2[i]));
+    for (uint32_t i = 0; i < n; ++i) p[i] = mmul(S[i], mmul(invP[i], r[i]));
+    dacc_init(&acc, dot);
+    for (uint32_t i = 0; i < n; ++i) dacc_add(&acc, r[i], p[i]);
+    double delta_new = dacc_get(&acc);
+    if (dot == OC_DOT_F32 || dot == OC_DOT_COMPENSATED) {
+        b_delta = (float)b_delta;
+        delta_new = (float)delta_new;
+    }
+    double delta0 = delta_new;
+
+    uint32_t it = 0;
+    for (;;) {
+        if (it == max_iter) break;
+        if (stop_rule == OC_STOP_REFERENCE) {
+            if (dot == OC_DOT_F64) {
+                if (delta_new <= (double)(kEps * kEps) * b_delta) break;
+            } else if ((float)delta_new <= kEps * kEps * (float)b_delta) {
+                break;
+            }
+        } else if (delta_new <= (double)tol * (double)tol * b_delta) {
+            break;
+        }
+        csr_mul(n, rowptr, cols, vals, p, tmp);
+        for (uint32_t i = 0; i < n; ++i) s[i] = mmul(S[i], tmp[i]);
+        dacc_init(&acc, dot);
+        for (uint32_t i = 0; i < n; ++i) dacc_add(&acc, p[i], s[i]);
+        float alpha;
+        if (dot == OC_DOT_F64) alpha = (float)(delta_new / dacc_get(&acc));
+        else alpha = (float)delta_new / (float)dacc_get(&acc);
+        for (uint32_t i = 0; i < n; ++i) x[i] = vadd(x[i], vscale(alpha, p[i]));
+        for (uint32_t i = 0; i < n; ++i) r[i] = vsub(r[i], vscale(alpha, s[i]));
+        for (uint32_t i = 0; i < n; ++i) hv[i] = mmul(invP[i], r[i]);
+        double delta_old = delta_new;
+        dacc_init(&acc, dot);
+        for (uint32_t i = 0; i < n; ++i) dacc_add(&acc, r[i], hv[i]);
+        delta_new = dacc_get(&acc);
+        float beta;
+        if (dot == OC_DOT_F64) {
+            beta = (float)(delta_new / delta_old);
+        } else {
+            delta_new = (float)delta_new;
+            beta = (float)delta_new / (float)delta_old;
+        }
+        for (uint32_t i = 0; i < n; ++i) p[i] = mmul(S[i], vadd(hv[i], vscale(beta, p[i])));
+        ++it;
+    }
+    if (stats) {
+        stats[0] = delta0;
+        stats[1] = b_delta;
+        stats[2] = delta_new;
+    }
+    free(S); free(IS); free(invP); free(r); free(p); free(s); free(hv); free(tmp); free(tmp2); free(bhat);
+    return it;
+}
+
+uint32_t oc_mpcg(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const float* vals, const float* b,
+                 const float* S, const float* x0, int stop_rule, float tol, uint32_t max_iterations, int dot,
+                 float* x, double* stats)
+{
+    return mpcg(n, rowptr, cols, (const m33*)vals, (const v3*)b, S, (const v3*)x0, stop_rule, tol,
+                max_iterations, dot, (v3*)x, stats);
+}
+
+/* FP64 filtered Jacobi-PCG on the same system, for error reports. */
+uint32_t oc_solve_f64(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const float* vals,
+                      const float* b, const float* S, const float* x0, double tol, uint32_t max_iterations,
+                      double* x)
+{
+    double* A = (double*)malloc((size_t)rowptr[n] * 9 * sizeof(double));
+    for (size_t k = 0; k < (size_t)rowptr[n] * 9; ++k) A[k] = vals[k];
+    double* invP = (double*)malloc(3 * (size_t)n * sizeof(double));
+    double* r = (double*)malloc(3 * (size_t)n * sizeof(double));
+    double* p = (double*)malloc(3 * (size_t)n * sizeof(double));
+    double* s = (double*)malloc(3 * (size_t)n * sizeof(double));
+    double* tmp = (double*)calloc(3 * (size_t)n, sizeof(double));
+    for (uint32_t i = 0; i < n; ++i) {
+        const double* a = NULL;
+        for (uint32_t k = rowptr[i]; k < rowptr[i + 1]; ++k)
+            if (cols[k] == i) { a = A + 9 * (size_t)k; break; }
+        for (int d = 0; d < 3; ++d) invP[3 * i + d] = a ? 1.0 / a[4 * d] : 0.0;
+        for (int d = 0; d < 3; ++d) x[3 * i + d] = S[i] != 0.0f ? (double)x0[3 * i + d] : 0.0;
+    }
+#define SPMV(in, out)                                                                  \
+    for (uint32_t i = 0; i < n; ++i) {                                                 \
+        double a0 = 0, a1 = 0, a2 = 0;                                                 \
+        for (uint32_t k = rowptr[i]; k < rowptr[i + 1]; ++k) {                         \
+            const double* m = A + 9 * (size_t)k;                                       \
+            const double* v = in + 3 * (size_t)cols[k];                                \
+            a0 += m[0] * v[0] + m[3] * v[1] + m[6] * v[2];                             \
+            a1 += m[1] * v[0] + m[4] * v[1] + m[7] * v[2];                             \
+            a2 += m[2] * v[0] + m[5] * v[1] + m[8] * v[2];                             \
+        }                                                                              \
+        out[3 * i] = a0; out[3 * i + 1] = a1; out[3 * i + 2] = a2;                     \
+    }
+    double b_delta = 0.0;
+    for (uint32_t i = 0; i < n; ++i)
+        if (S[i] != 0.0f)
+            for (int d = 0; d < 3; ++d) b_delta += (double)b[3 * i + d] * b[3 * i + d] * invP[3 * i + d];
+    SPMV(x, tmp);
+    double delta = 0.0;
+    for (uint32_t i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            size_t q = 3 * (size_t)i + d;
+            r[q] = S[i] != 0.0f ? (double)b[q] - tmp[q] : 0.0;
+            p[q] = invP[q] * r[q];
+            delta += r[q] * p[q];
+        }
+    uint32_t it = 0;
+    while (it < max_iterations && delta > tol * tol * b_delta) {
+        SPMV(p, s);
+        double ps = 0.0;
+        for (uint32_t i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d) {
+                size_t q = 3 * (size_t)i + d;
+                if (S[i] == 0.0f) s[q] = 0.0;
+                ps += p[q] * s[q];
+            }
+        double alpha = delta / ps;
+        double dn = 0.0;
+        for (size_t q = 0; q < 3 * (size_t)n; ++q) {
+            x[q] += alpha * p[q];
+            r[q] -= alpha * s[q];
+            dn += r[q] * r[q] * invP[q];
+        }
+        double beta = dn / delta;
+        delta = dn;
+        for (uint32_t i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d) {
+                size_t q = 3 * (size_t)i + d;
+                p[q] = S[i] != 0.0f ? invP[q] * r[q] + beta * p[q] : 0.0;
+            }
+        ++it;
+    }
+#undef SPMV
+    free(A); free(invP); free(r); free(p); free(s); free(tmp);
+    return it;
+}
+
+/* ------------------------------------------------------------------------ */
+/* body contacts                                                             */
+/* ------------------------------------------------------------------------ */
+
+static inline int aabb_overlap(v3 alo, v3 ahi, v3 blo, v3 bhi)
+{
+    /* b3TestOverlap (aabb3.h:247-251) */
+    return alo.x <= bhi.x && alo.y <= bhi.y && alo.z <= bhi.z && ahi.x >= blo.x && ahi.y >= blo.y &&
+           ahi.z >= blo.z;
+}
+
+/* b3ParticleBodyContact::Update (cloth_particle_body_contact.cpp:24-47) with
+ * b3SphereShape::TestSphere (sphere_shape.cpp:71-95) for a static body whose
+ * frame is the identity rotation at the sphere centre. */
+static void contact_update(oc_cloth* c, contact_t* k)
+{
+    const sphere_t* sp = c->spheres + k->shape;
+    uint32_t i = k->particle;
+    float radius = sp->radius + c->radius[i];
+    float rr = radius * radius;
+    v3 d = vsub(c->x[i], sp->center);
+    float dd = vdot(d, d);
+    if (!(dd <= rr)) {
+        k->active = 0;
+        return;
+    }
+    float d_len = sqrtf(dd);
+    v3 normal = V(0.0f, 1.0f, 0.0f);
+    if (d_len > kEps) normal = vdiv(d, d_len);
+    k->active = 1;
+    k->normal1 = vneg(normal);
+    k->local_point2 = vzero();
+    k->tangent1 = vperp(k->normal1);
+    k->tangent2 = vcross(k->tangent1, k->normal1);
+}
+
+/* UpdateBodyContacts (cloth_contact_manager.cpp:277-315). */
+static void update_body_contacts(oc_cloth* c)
+{
+    /* walk the list from its head (the array's end) and compact */
+    uint32_t n = c->ncontact;
+    uint8_t* keep = (uint8_t*)malloc(n + 1);
+    for (uint32_t q = n; q-- > 0;) {
+        contact_t* k = c->contacts + q;
+        keep[q] = 0;
+        if (c->type[k->particle] != OC_DYNAMIC) continue; /* the body is static too */
+        const sphere_t* sp = c->spheres + k->shape;
+        if (!aabb_overlap(c->fat_lo[k->particle], c->fat_hi[k->particle], sp->fat_lo, sp->fat_hi)) continue;
+        contact_update(c, k);
+        keep[q] = 1;
+    }
+    uint32_t w = 0;
+    for (uint32_t q = 0; q < n; ++q)
+        if (keep[q]) c->contacts[w++] = c->contacts[q];
+    c->ncontact = w;
+    free(keep);
+}
+
+/* FindNewBodyContacts + AddPSPair (cloth_contact_manager.cpp:64-123).  The
+ * world broadphase reports every shape whose fat AABB overlaps the
+ * particle's; a new contact is pushed to the list front. */
+static void find_new_body_contacts(oc_cloth* c)
+{
+    if (c->nsphere == 0) return;
+    /* which (particle, shape) pairs already have a contact */
+    uint8_t* has = (uint8_t*)calloc((size_t)c->n * c->nsphere, 1);
+    for (uint32_t q = 0; q < c->ncontact; ++q)
+        has[(size_t)c->contacts[q].particle * c->nsphere + c->contacts[q].shape] = 1;
+    for (uint32_t k = 0; k < c->n; ++k) {
+        uint32_t i = c->order[k];
+        if (c->type[i] != OC_DYNAMIC) continue;
+        for (uint32_t s = 0; s < c->nsphere; ++s) {
+            const sphere_t* sp = c->spheres + s;
+            if (!aabb_overlap(c->fat_lo[i], c->fat_hi[i], sp->fat_lo, sp->fat_hi)) continue;
+            if (has[(size_t)i * c->nsphere + s]) continue;
+            has[(size_t)i * c->nsphere + s] = 1;
+            if (c->ncontact == c->contact_cap) {
+                c->contact_cap = c->contact_cap ? 2 * c->contact_cap : 1024;
+                c->contacts = (contact_t*)realloc(c->contacts, c->contact_cap * sizeof(contact_t));
+            }
+            contact_t* nk = c->contacts + c->ncontact++;
+            memset(nk, 0, sizeof(*nk));
+            nk->particle = i;
+            nk->shape = s;
+            nk->active = 0;
+        }
+    }
+    free(has);
+}
+
+typedef struct {
+    uint32_t index;     /* solver row */
+    float inv_mass, friction, normal_mass;
+    float tm_xx, tm_xy, tm_yx, tm_yy; /* tangent mass (mat22, column-major x=(xx,xy), y=(yx,yy)) */
+    v3 normal, tangent1, tangent2;
+    float normal_impulse;
+    v2 tangent_impulse;
+    /* position constraint */
+    v3 normal_a, center_b;
+    float radius_a, radius_b;
+    contact_t* src;
+} bc_t;
+
+/* b3ClothSolver::Solve contact part (cloth_solver.cpp:103-182) with the
+ * body-contact functions of cloth_contact_solver.cpp, for static bodies
+ * (inverse mass and inertia 0, zero velocity). */
+static void solve_contacts(oc_cloth* c, float h, uint32_t vel_iters, uint32_t pos_iters, v3* pos, v3* vel,
+                           uint32_t* nactive)
+{
+    uint32_t na = 0;
+    for (uint32_t q = c->ncontact; q-- > 0;) na += c->contacts[q].active != 0;
+    *nactive = na;
+    bc_t* bc = (bc_t*)calloc(na + 1, sizeof(bc_t));
+    uint32_t w = 0;
+    /* contacts enter the solver in list order (cloth.cpp:539-545) */
+    for (uint32_t q = c->ncontact; q-- > 0;) {
+        contact_t* k = c->contacts + q;
+        if (!k->active) continue;
+        bc_t* x = bc + w++;
+        const sphere_t* sp = c->spheres + k->shape;
+        uint32_t i = k->particle;
+        x->src = k;
+        x->index = c->solver_of_vertex[i];
+        x->inv_mass = c->type[i] == OC_STATIC ? 0.0f : c->inv_mass[i];
+        x->friction = sqrtf(c->friction[i] * sp->friction); /* b3MixFriction */
+        x->normal_a = k->normal1;
+        x->center_b = sp->center;
+        x->radius_a = c->radius[i];
+        x->radius_b = sp->radius;
+        /* InitializeBodyContactConstraints (:54-177) */
+        x->normal = k->normal1;
+        x->tangent1 = k->tangent1;
+        x->tangent2 = k->tangent2;
+        x->normal_impulse = k->normal_impulse;
+        x->tangent_impulse = k->tangent_impulse;
+        float mA = x->inv_mass, mB = 0.0f;
+        float K = mA + mB + 0.0f + 0.0f;
+        x->normal_mass = K > 0.0f ? 1.0f / K : 0.0f;
+        /* b3Inverse(b3Mat22) (math.cpp:77-93) of [[k11, k12], [k12, k22]] */
+        float k11 = mA + mB + 0.0f + 0.0f, k12 = 0.0f + 0.0f, k22 = mA + mB + 0.0f + 0.0f;
+        float det = k11 * k22 - k12 * k12;
+        if (det != 0.0f) det = 1.0f / det;
+        x->tm_xx = det * k22;
+        x->tm_yx = -det * k12;
+        x->tm_xy = -det * k12;
+        x->tm_yy = det * k11;
+    }
+    /* WarmStartBodyContactConstraints (:264-307) */
+    for (uint32_t q = 0; q < na; ++q) {
+        bc_t* x = bc + q;
+        v3 vA = vel[x->index];
+        float mA = x->inv_mass;
+        v3 P = vscale(x->normal_impulse, x->normal);
+        vA = vsub(vA, vscale(mA, P));
+        v3 P1 = vscale(x->tangent_impulse.x, x->tangent1);
+        v3 P2 = vscale(x->tangent_impulse.y, x->tangent2);
+        vA = vsub(vA, vscale(mA, vadd(P1, P2)));
+        vel[x->index] = vA;
+    }
+    /* SolveBodyContactVelocityConstraints (:388-472) */
+    for (uint32_t it = 0; it < vel_iters; ++it) {
+        for (uint32_t q = 0; q < na; ++q) {
+            bc_t* x = bc + q;
+            v3 vA = vel[x->index];
+            float mA = x->inv_mass;
+            {
+                /* dv = vB + wB x rB - vA - wA x rA with vB = wB = wA = 0 */
+                v3 dv = vsub(vzero(), vA);
+                float Cdot = vdot(x->normal, dv);
+                float impulse = x->normal_mass * (-Cdot + 0.0f);
+                float old = x->normal_impulse;
+                float ni = old + impulse;
+                x->normal_impulse = ni > 0.0f ? ni : 0.0f;
+                impulse = x->normal_impulse - old;
+                v3 P = vscale(impulse, x->normal);
+                vA = vsub(vA, vscale(mA, P));
+            }
+            {
+                v3 dv = vsub(vzero(), vA);
+                v2 Cdot = W(vdot(dv, x->tangent1), vdot(dv, x->tangent2));
+                v2 nc = W(-Cdot.x, -Cdot.y);
+                /* Mat22 * Vec2 = v.x * A.x + v.y * A.y (mat22.h:56-59) */
+                v2 impulse = W(nc.x * x->tm_xx + nc.y * x->tm_yx, nc.x * x->tm_xy + nc.y * x->tm_yy);
+                v2 old = x->tangent_impulse;
+                x->tangent_impulse.x += impulse.x;
+                x->tangent_impulse.y += impulse.y;
+                float maxImpulse = x->friction * x->normal_impulse;
+                v2 ti = x->tangent_impulse;
+                if (ti.x * ti.x + ti.y * ti.y > maxImpulse * maxImpulse) {
+                    float sl = sqrtf(ti.x * ti.x + ti.y * ti.y);
+                    if (sl > kEps) {
+                        ti.x /= sl;
+                        ti.y /= sl;
+                    }
+                    ti.x *= maxImpulse;
+                    ti.y *= maxImpulse;
+                    x->tangent_impulse = ti;
+                }
+                impulse = W(x->tangent_impulse.x - old.x, x->tangent_impulse.y - old.y);
+                v3 P1 = vscale(impulse.x, x->tangent1);
+                v3 P2 = vscale(impulse.y, x->tangent2);
+                v3 P = vadd(P1, P2);
+                vA = vsub(vA, vscale(mA, P));
+            }
+            vel[x->index] = vA;
+        }
+    }
+    /* StoreImpulses (:598-607) */
+    for (uint32_t q = 0; q < na; ++q) {
+        bc[q].src->normal_impulse = bc[q].normal_impulse;
+        bc[q].src->tangent_impulse = bc[q].tangent_impulse;
+    }
+    /* integrate positions (cloth_solver.cpp:143-147) */
+    for (uint32_t k = 0; k < c->n; ++k) pos[k] = vadd(pos[k], vscale(h, vel[k]));
+    /* SolveBodyContactPositionConstraints (:620-718), early out (cloth_solver.cpp:151-164) */
+    for (uint32_t it = 0; it < pos_iters; ++it) {
+        float minSeparation = 0.0f;
+        for (uint32_t q = 0; q < na; ++q) {
+            bc_t* x = bc + q;
+            v3 cA = pos[x->index];
+            v3 cB = x->center_b;
+            v3 nA = x->normal_a;
+            float separation = vdot(vsub(cB, cA), nA) - x->radius_a - x->radius_b;
+            minSeparation = minSeparation < separation ? minSeparation : separation;
+            float Cv = kBaumgarte * (separation + kLinearSlop);
+            float C = Cv < 0.0f ? Cv : 0.0f;
+            C = -kMaxLinearCorrection > C ? -kMaxLinearCorrection : C;
+            float mA = x->inv_mass;
+            float K = mA + 0.0f + 0.0f + 0.0f;
+            float impulse = K > 0.0f ? -C / K : 0.0f;
+            v3 P = vscale(impulse, nA);
+            cA = vsub(cA, vscale(mA, P));
+            pos[x->index] = cA;
+        }
+        if (minSeparation >= -3.0f * kLinearSlop) break;
+    }
+    free(bc);
+}
+
+/* ------------------------------------------------------------------------ */
+/* step                                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* b3Cloth::Step (cloth.cpp:551-601) without the self-collision pass, with
+ * b3Cloth::Solve (:507-549), b3ClothSolver::Solve (cloth_solver.cpp:78-193)
+ * and b3ClothForceSolver::Solve (cloth_force_solver.cpp:138-222). */
+void oc_step(oc_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, oc_step_info* info)
+{
+    uint32_t n = c->n;
+    oc_step_info local;
+    memset(&local, 0, sizeof(local));
+
+    update_body_contacts(c);
+
+    if (dt > 0.0f) {
+        float h = dt;
+        form_system(c, h);
+        double stats[3];
+        local.iterations = mpcg(n, c->a_rowptr, c->a_cols, c->a_vals, c->b, c->Sflag, c->sx0, c->stop_rule, c->tol,
+                                c->max_iter, c->dot, c->dvsol, stats);
+        local.delta0 = stats[0];
+        local.b_delta = stats[1];
+        local.delta = stats[2];
+        /* sv = sv + x; sx = sx + sy; copy back (:211-222) */
+        v3* pos = (v3*)malloc(n * sizeof(v3));
+        v3* vel = (v3*)malloc(n * sizeof(v3));
+        for (uint32_t k = 0; k < n; ++k) {
+            uint32_t i = c->order[k];
+            vel[k] = vadd(c->sv[k], c->dvsol[k]);
+            pos[k] = vadd(c->sx[k], c->sy[k]);
+            c->mx[i] = c->dvsol[k];
+        }
+        solve_contacts(c, h, vel_iters, pos_iters, pos, vel, &local.active_contacts);
+        for (uint32_t k = 0; k < n; ++k) {
+            uint32_t i = c->order[k];
+            c->x[i] = pos[k];
+            c->v[i] = vel[k];
+        }
+        free(pos);
+        free(vel);
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        c->f[i] = vzero();
+        c->y[i] = vzero();
+    }
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t i = c->order[k];
+        move_proxy(c, i, vscale(dt, c->v[i]));
+    }
+    find_new_body_contacts(c);
+    local.contacts = c->ncontact;
+    if (info) *info = local;
+}
+
+/* ------------------------------------------------------------------------ */
+/* queries                                                                   */
+/* ------------------------------------------------------------------------ */
+
+void oc_get_state(const oc_cloth* c, float* x, float* v, float* dv, float* mass, uint8_t* type)
+{
+    for (uint32_t i = 0; i < c->n; ++i) {
+        if (x) { x[3 * i] = c->x[i].x; x[3 * i + 1] = c->x[i].y; x[3 * i + 2] = c->x[i].z; }
+        if (v) { v[3 * i] = c->v[i].x; v[3 * i + 1] = c->v[i].y; v[3 * i + 2] = c->v[i].z; }
+        if (dv) { dv[3 * i] = c->mx[i].x; dv[3 * i + 1] = c->mx[i].y; dv[3 * i + 2] = c->mx[i].z; }
+        if (mass) mass[i] = c->mass[i];
+        if (type) type[i] = c->type[i];
+    }
+}
+
+/* b3Cloth::GetEnergy (cloth.cpp:366-374), summed in particle-list order */
+float oc_energy(const oc_cloth* c)
+{
+    float E = 0.0f;
+    for (uint32_t k = 0; k < c->n; ++k) {
+        uint32_t i = c->order[k];
+        E += c->mass[i] * vdot(c->v[i], c->v[i]);
+    }
+    return 0.5f * E;
+}
+
+uint32_t oc_describe(const oc_cloth* c, float* tri_rest, float* fat_aabb, float* force_desc)
+{
+    if (tri_rest)
+        for (uint32_t k = 0; k < c->t; ++k) {
+            float* o = tri_rest + 6 * k;
+            o[0] = c->du1[k]; o[1] = c->dv1[k]; o[2] = c->du2[k]; o[3] = c->dv2[k];
+            o[4] = c->inv_det[k]; o[5] = c->alpha[k];
+        }
+    if (fat_aabb)
+        for (uint32_t i = 0; i < c->n; ++i) {
+            float* o = fat_aabb + 6 * i;
+            o[0] = c->fat_lo[i].x; o[1] = c->fat_lo[i].y; o[2] = c->fat_lo[i].z;
+            o[3] = c->fat_hi[i].x; o[4] = c->fat_hi[i].y; o[5] = c->fat_hi[i].z;
+        }
+    if (force_desc)
+        for (uint32_t q = 0; q < c->nforce; ++q) {
+            const force_t* f = c->forces + q;
+            float* o = force_desc + 8 * q;
+            memset(o, 0, 8 * sizeof(float));
+            o[0] = (float)f->type;
+            if (f->type == F_SPRING) {
+                o[1] = (float)f->a; o[2] = (float)f->b; o[3] = -1.0f;
+                o[4] = f->ks; o[5] = f->kd; o[6] = f->p0;
+            } else {
+                o[1] = (float)c->tris[3 * f->a]; o[2] = (float)c->tris[3 * f->a + 1];
+                o[3] = (float)c->tris[3 * f->a + 2];
+                o[4] = f->ks; o[5] = f->kd;
+                if (f->type == F_STRETCH) { o[6] = f->p0; o[7] = f->p1; }
+            }
+        }
+    return c->nforce;
+}
+
+uint32_t oc_force_count(const oc_cloth* c) { return c->nforce; }
+uint32_t oc_spring_count(const oc_cloth* c) { return c->nspring; }
+
+void oc_get_springs(const oc_cloth* c, uint32_t* pairs, float* rest_length, float* stiffness)
+{
+    /* the force list holds springs newest first; report creation order */
+    uint32_t w = 0;
+    for (uint32_t q = c->nforce; q-- > 0;) {
+        const force_t* f = c->forces + q;
+        if (f->type != F_SPRING) continue;
+        if (pairs) { pairs[2 * w] = f->a; pairs[2 * w + 1] = f->b; }
+        if (rest_length) rest_length[w] = f->p0;
+        if (stiffness) stiffness[w] = f->ks;
+        ++w;
+    }
+}
+
+uint32_t oc_get_contacts(const oc_cloth* c, uint8_t* exists, uint8_t* active, float* impulses)
+{
+    if (exists) memset(exists, 0, c->n);
+    if (active) memset(active, 0, c->n);
+    if (impulses) memset(impulses, 0, 3 * (size_t)c->n * sizeof(float));
+    for (uint32_t q = 0; q < c->ncontact; ++q) {
+        const contact_t* k = c->contacts + q;
+        uint32_t i = k->particle;
+        if (exists) exists[i] = 1;
+        if (active) active[i] = (uint8_t)(k->active != 0);
+        if (impulses) {
+            impulses[3 * i] = k->normal_impulse;
+            impulses[3 * i + 1] = k->tangent_impulse.x;
+            impulses[3 * i + 2] = k->tangent_impulse.y;
+        }
+    }
+    return c->ncontact;
+}
+
+uint32_t oc_build_system(oc_cloth* c, float dt)
+{
+    form_system(c, dt);
+    return c->sys_nnz;
+}
+
+void oc_get_system(const oc_cloth* c, uint32_t* rowptr, uint32_t* cols, float* vals, float* b, float* S,
+                   float* x0, uint32_t* vertex_of_row)
+{
+    uint32_t n = c->n;
+    memcpy(rowptr, c->a_rowptr, (n + 1) * sizeof(uint32_t));
+    memcpy(cols, c->a_cols, c->sys_nnz * sizeof(uint32_t));
+    memcpy(vals, c->a_vals, (size_t)c->sys_nnz * sizeof(m33));
+    memcpy(b, c->b, n * sizeof(v3));
+    memcpy(S, c->Sflag, n * sizeof(float));
+    memcpy(x0, c->sx0, n * sizeof(v3));
+    memcpy(vertex_of_row, c->order, n * sizeof(uint32_t));
+}
