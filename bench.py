@@ -1,0 +1,325 @@
+"""Benchmark of the implicit cloth step on B200.
+
+Workload (default): one 256 x 256 cloth (65,536 vertices, 130,050 triangles,
+194,565 bending springs) with a static sphere collider, dt = 1/60 s, 8
+velocity / 2 position contact iterations, CG to relative residual 1e-4 (at
+most 50 iterations, FP64 inner products).  Metric: cloth vertex-steps per
+second, whole job.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one independent cloth per rank (replicas: a single cloth's step
+has no exchange to shard), launched by torch.distributed.run; the reported
+value is all ranks' vertex-steps over the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cloth vertex-steps/s"
+UNIT = "vertex-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--side", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([s.strip() for s in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(info: dict, kernel: str) -> float:
+    """Bytes one launch of a kernel must move at least (FP32, full block pattern)."""
+    n, blocks, t, s = info["vertices"], info["blocks"], info["triangles"], info["springs"]
+    if kernel == "cg_spmv":
+        # A values + column ids, p gathered once, s written, filter and degree bytes
+        return 40.0 * blocks + 12 * n + 12 * n + 2 * n
+    if kernel == "cg_update":
+        return (5 * 12 + 2 * 12) * n
+    if kernel == "cg_direction":
+        return (3 * 12 + 12 + 1) * n
+    if kernel == "cg_init":
+        return 40.0 * blocks + (12 * 3 + 1 + 3 * 12) * n
+    if kernel == "assemble":
+        inc = 3 * t + 2 * s
+        return 36.0 * blocks + (24 + 24 + 4 + 1 + 24) * n + 40.0 * t + 24.0 * s + 8.0 * inc
+    return 0.0
+
+
+def run_ours(args, rank, world):
+    import bounce_b200 as b3g
+    import torch
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    scene = b3g.sphere_scene(args.side, seed=2 + rank)
+    opts = b3g.SolverOptions.relative(1e-4, 50, b3g.DOT_F64)
+    cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene, opts)
+    info = cloth.info()
+    n = info["vertices"]
+    # L2 flush buffer (> 126 MB L2), written between timed steps
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
+
+    for _ in range(args.warmup):
+        cloth.step(scene.dt, scene.velocity_iterations, scene.position_iterations)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = b3g.kernel_launch_count()
+    step_ms, iters, contacts = [], [], []
+    with ClockSampler(dev) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            st = cloth.step(scene.dt, scene.velocity_iterations, scene.position_iterations)
+            step_ms.append(st["step_ms"])
+            iters.append(st["iterations"])
+            contacts.append(st["active_contacts"])
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    launches = b3g.kernel_launch_count() - launches0
+    dev_s = sum(step_ms) / 1000.0
+    if world > 1:
+        t = torch.tensor([dev_s], dtype=torch.float64, device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+        dev_s = float(t.item())
+    value = world * n * args.steps / dev_s
+
+    # end to end through the public API with host buffers: per step the
+    # external forces go host->device, the positions come back device->host
+    forces = np.zeros((n, 3), np.float32)
+    pos = np.zeros((n, 3), np.float32)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cloth.apply_forces(forces)
+        cloth.step(scene.dt, scene.velocity_iterations, scene.position_iterations)
+        cloth.positions(pos)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * n * args.steps / e2e_s
+
+    # per-kernel device times for the roofline
+    prof = []
+    for _ in range(args.profile_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        prof.append(cloth.step_profiled(scene.dt, scene.velocity_iterations, scene.position_iterations))
+    it_total = sum(p["cg_iterations"] for p in prof)
+    kern = {
+        "assemble": (sum(p["assemble_ms"] for p in prof), len(prof)),
+        "cg_init": (sum(p["cg_init_ms"] for p in prof), len(prof)),
+        "cg_spmv": (sum(p["cg_spmv_ms"] for p in prof), max(it_total, 1)),
+        "cg_update": (sum(p["cg_update_ms"] for p in prof), max(it_total, 1)),
+        "cg_direction": (sum(p["cg_direction_ms"] for p in prof), max(it_total, 1)),
+        "finalize": (sum(p["finalize_ms"] for p in prof), len(prof)),
+        "post": (sum(p["post_ms"] for p in prof), len(prof)),
+        "contacts_update": (sum(p["contacts_update_ms"] for p in prof), len(prof)),
+    }
+    total = sum(v[0] for v in kern.values())
+    dom = max(kern, key=lambda k: kern[k][0])
+    avg_ms = kern[dom][0] / kern[dom][1]
+    alg = algorithmic_bytes(info, dom)
+    peak, peak_kind = peaks()
+    achieved = alg / (avg_ms / 1000.0) / 1e9
+    cloth.close()
+    return {
+        "value": value, "ms_per_step": 1000.0 * dev_s / args.steps, "wall_s": wall, "e2e": e2e,
+        "iterations_mean": float(np.mean(iters)), "active_contacts_mean": float(np.mean(contacts)),
+        "launches": launches, "clocks": clocks.summary(), "info": info,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
+                     "share": kern[dom][0] / total if total else None},
+        "kernel_ms": {k: v[0] / v[1] for k, v in kern.items()},
+    }
+
+
+def cpu_reference_sample(side: int, steps: int, warm: int):
+    """The reference (compiled from its sources) stepping the same cloth on one host core."""
+    import oracle
+
+    import bounce_b200 as b3g
+
+    scene = b3g.sphere_scene(side, seed=2)
+    t0 = time.perf_counter()
+    ref = oracle.RefCloth(scene.mesh, scene.cdef, restated=True).setup(scene)
+    build_s = time.perf_counter() - t0
+    for _ in range(warm):
+        ref.step(scene.dt, scene.velocity_iterations, scene.position_iterations)
+    oracle.ref_profile_reset()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ref.step(scene.dt, scene.velocity_iterations, scene.position_iterations)
+    dt = time.perf_counter() - t0
+    prof = oracle.ref_profile()
+    solve = prof.get("Cloth Solve", (0.0, 0))[0]
+    n = scene.mesh.vertex_count
+    return {"value": n * steps / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": (f"{steps} steps (after {warm} warm-up) of the same {side}x{side} cloth with the reference "
+                       f"b3Cloth::Step minus the inert self-collision pass, CG at the reference's own 20-iteration "
+                       f"rule; {dt / steps:.2f} s/step, of which 'Cloth Solve' {solve / steps:.2f} s/step "
+                       f"({n * steps / max(solve, 1e-9):.3g} vertex-steps/s for the solve alone); "
+                       f"constructor {build_s:.1f} s"),
+            "seconds": dt}
+
+
+def host_cpu():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps = max(1, min(args.steps, 3))
+        warm = min(args.warmup, 1)
+        base = cpu_reference_sample(args.side, steps, warm)
+        line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+                "warmup": warm, "ms_per_step": 1000.0 * base["seconds"] / steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+                "config": {"workload": f"grid{args.side}x{args.side}_bending_sphere", "vertices": args.side ** 2,
+                           "host_cpu": host_cpu()},
+                "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import torch
+
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    r = run_ours(args, rank, world)
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            base = cpu_reference_sample(args.side, 2, 0)
+            base = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as e:  # the reference library was not built here
+            base = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    n = r["info"]["vertices"]
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"grid{args.side}x{args.side}_bending_sphere", "vertices": n,
+                   "triangles": r["info"]["triangles"], "springs": r["info"]["springs"],
+                   "blocks": r["info"]["blocks"], "cg": "relative residual 1e-4, max 50, fp64 dots",
+                   "contact_iterations": [8, 2], "parallelism": f"replicas{world}",
+                   "l2": "flushed (256 MB write) before every timed step",
+                   "cg_iterations_mean": r["iterations_mean"], "active_contacts_mean": r["active_contacts_mean"]},
+        "clocks": r["clocks"],
+        "e2e": {"value": r["e2e"], "unit": UNIT, "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 12 * n},
+        "gpu_launches": r["launches"],
+        "roofline": r["roofline"],
+        "kernel_ms": r["kernel_ms"],
+        "cpu_baseline": base,
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,1 +1,361 @@
-"""B200-native implicit cloth step for Bounce (placeholder)."""
+"""B200-native implicit cloth step with Bounce's ``b3Cloth`` semantics.
+
+The compute path is libb3g.so (hand-written CUDA for sm_100a behind the C ABI
+in include/b3g.h).  This module is a thin ctypes front-end with the shape of
+the reference's C++ classes:
+
+* ``Cloth``       ~ ``b3Cloth``  (include/bounce/cloth/cloth.h:99-158)
+* ``Particle``    ~ ``b3Particle`` (include/bounce/cloth/particle.h:63-111)
+* ``SolverOptions``  the CG stop rule / iteration cap / dot precision
+
+There is no CPU fallback: if libb3g.so is missing the import of the native
+library raises, and without a CUDA device ``Cloth(...)`` raises B3gError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from .meshes import (DYNAMIC, KINEMATIC, STATIC, ClothDef, Mesh, Scene, batch_scenes, grid_mesh,  # noqa: F401
+                     plain_scene, sphere_scene, stiff_scene)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libb3g.so")
+
+STOP_REFERENCE, STOP_RELATIVE = 0, 1
+DOT_F32, DOT_COMPENSATED, DOT_F64 = 0, 1, 2
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "degenerate mesh", 3: "no CUDA device", 4: "out of memory",
+          5: "CUDA error", 6: "numerical breakdown in CG", 7: "device wait timed out", 8: "capacity exceeded",
+          9: "unsupported mesh"}
+
+
+class B3gError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({status})")
+        self.status = status
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("vertex_count", C.c_uint32), ("vertices", C.c_void_p), ("triangle_count", C.c_uint32),
+                ("triangles", C.c_void_p), ("sewing_line_count", C.c_uint32), ("sewing_lines", C.c_void_p)]
+
+
+class ClothDefC(C.Structure):
+    _fields_ = [(k, C.c_float) for k in ("density", "streching", "shearing", "bending", "sewing", "damping",
+                                          "thickness", "friction")]
+
+
+class SolverOptsC(C.Structure):
+    _fields_ = [("stop_rule", C.c_int), ("tolerance", C.c_float), ("max_iterations", C.c_uint32), ("dot", C.c_int)]
+
+
+class StepStatsC(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("delta0", C.c_double), ("delta", C.c_double), ("b_delta", C.c_double),
+                ("active_contacts", C.c_uint32), ("contacts", C.c_uint32), ("step_ms", C.c_float)]
+
+
+class PhaseTimesC(C.Structure):
+    _fields_ = [(k, C.c_float) for k in ("contacts_update_ms", "assemble_ms", "cg_init_ms", "cg_spmv_ms",
+                                          "cg_update_ms", "cg_direction_ms", "finalize_ms",
+                                          "contact_position_ms", "post_ms")] + \
+               [("cg_iterations", C.c_uint32), ("contact_position_launches", C.c_uint32)]
+
+
+class ClothInfoC(C.Structure):
+    _fields_ = [(k, C.c_uint32) for k in ("vertices", "triangles", "springs", "blocks", "sell_entries",
+                                           "max_degree")]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libb3g.so (fails loudly when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m bounce_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp, u32, f32, i32 = C.c_void_p, C.c_uint32, C.c_float, C.c_int
+        sig = {
+            "b3g_cloth_create": [C.POINTER(MeshDesc), C.POINTER(ClothDefC), i32, C.POINTER(vp)],
+            "b3g_cloth_destroy": [vp],
+            "b3g_cloth_set_gravity": [vp, vp],
+            "b3g_cloth_get_gravity": [vp, vp],
+            "b3g_cloth_set_solver": [vp, C.POINTER(SolverOptsC)],
+            "b3g_cloth_add_static_sphere": [vp, vp, f32, f32, C.POINTER(u32)],
+            "b3g_cloth_clear_colliders": [vp],
+            "b3g_particle_set_type": [vp, u32, i32],
+            "b3g_particle_get_type": [vp, u32, C.POINTER(i32)],
+            "b3g_particle_set_position": [vp, u32, vp],
+            "b3g_particle_get_position": [vp, u32, vp],
+            "b3g_particle_set_velocity": [vp, u32, vp],
+            "b3g_particle_get_velocity": [vp, u32, vp],
+            "b3g_particle_get_mass": [vp, u32, C.POINTER(f32)],
+            "b3g_particle_apply_force": [vp, u32, vp],
+            "b3g_particle_apply_translation": [vp, u32, vp],
+            "b3g_cloth_set_types": [vp, vp],
+            "b3g_cloth_apply_forces": [vp, vp],
+            "b3g_cloth_apply_translations": [vp, vp],
+            "b3g_cloth_step": [vp, f32, u32, u32, C.POINTER(StepStatsC)],
+            "b3g_cloth_assemble": [vp, f32],
+            "b3g_cloth_read_state": [vp, vp, vp, vp],
+            "b3g_cloth_write_state": [vp, vp, vp, vp],
+            "b3g_cloth_read_masses": [vp, vp],
+            "b3g_cloth_get_energy": [vp, C.POINTER(f32)],
+            "b3g_cloth_read_contacts": [vp, vp, vp, vp],
+            "b3g_cloth_last_stats": [vp, C.POINTER(StepStatsC)],
+            "b3g_cloth_read_system": [vp, C.POINTER(u32), vp, vp, vp, vp, vp, vp],
+            "b3g_cloth_step_profiled": [vp, f32, u32, u32, C.POINTER(PhaseTimesC), C.POINTER(StepStatsC)],
+            "b3g_cloth_get_info": [vp, C.POINTER(ClothInfoC)],
+            "b3g_mpcg_solve": [u32, vp, vp, vp, vp, vp, vp, C.POINTER(SolverOptsC), vp, C.POINTER(u32),
+                               C.POINTER(StepStatsC), vp],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.b3g_cloth_vertex_count.argtypes = [vp]
+        L.b3g_cloth_vertex_count.restype = u32
+        L.b3g_status_string.argtypes = [C.c_int]
+        L.b3g_status_string.restype = C.c_char_p
+        L.b3g_kernel_launch_count.argtypes = []
+        L.b3g_kernel_launch_count.restype = C.c_uint64
+        _lib = L
+    return _lib
+
+
+def check(status: int, what: str) -> None:
+    if status != 0:
+        raise B3gError(status, what)
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _f3(v) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(v, dtype=np.float32).reshape(3))
+
+
+@dataclass
+class SolverOptions:
+    stop_rule: int = STOP_REFERENCE
+    tolerance: float = 0.0
+    max_iterations: int = 20
+    dot: int = DOT_F32
+
+    @staticmethod
+    def reference() -> "SolverOptions":
+        """b3SolveMPCG's own rule: 20 iterations, delta <= FLT_EPSILON^2 b_delta."""
+        return SolverOptions(STOP_REFERENCE, 0.0, 20, DOT_F32)
+
+    @staticmethod
+    def relative(tol: float = 1e-4, max_iterations: int = 50, dot: int = DOT_F64) -> "SolverOptions":
+        return SolverOptions(STOP_RELATIVE, tol, max_iterations, dot)
+
+    def as_c(self) -> SolverOptsC:
+        return SolverOptsC(self.stop_rule, self.tolerance, self.max_iterations, self.dot)
+
+
+class Particle:
+    """One particle of a Cloth (b3Particle)."""
+
+    def __init__(self, cloth: "Cloth", vertex: int):
+        self.cloth = cloth
+        self.vertex = vertex
+
+    def set_type(self, t: int) -> None:
+        check(lib().b3g_particle_set_type(self.cloth.h, self.vertex, t), "set_type")
+
+    def get_type(self) -> int:
+        out = C.c_int(0)
+        check(lib().b3g_particle_get_type(self.cloth.h, self.vertex, C.byref(out)), "get_type")
+        return out.value
+
+    def set_position(self, x) -> None:
+        check(lib().b3g_particle_set_position(self.cloth.h, self.vertex, _ptr(_f3(x))), "set_position")
+
+    def get_position(self) -> np.ndarray:
+        out = np.zeros(3, np.float32)
+        check(lib().b3g_particle_get_position(self.cloth.h, self.vertex, _ptr(out)), "get_position")
+        return out
+
+    def set_velocity(self, v) -> None:
+        check(lib().b3g_particle_set_velocity(self.cloth.h, self.vertex, _ptr(_f3(v))), "set_velocity")
+
+    def get_velocity(self) -> np.ndarray:
+        out = np.zeros(3, np.float32)
+        check(lib().b3g_particle_get_velocity(self.cloth.h, self.vertex, _ptr(out)), "get_velocity")
+        return out
+
+    def get_mass(self) -> float:
+        out = C.c_float(0)
+        check(lib().b3g_particle_get_mass(self.cloth.h, self.vertex, C.byref(out)), "get_mass")
+        return out.value
+
+    def apply_force(self, f) -> None:
+        check(lib().b3g_particle_apply_force(self.cloth.h, self.vertex, _ptr(_f3(f))), "apply_force")
+
+    def apply_translation(self, t) -> None:
+        check(lib().b3g_particle_apply_translation(self.cloth.h, self.vertex, _ptr(_f3(t))), "apply_translation")
+
+
+class Cloth:
+    """A cloth on one GPU (b3Cloth)."""
+
+    def __init__(self, mesh: Mesh, cdef: ClothDef, device: int = 0):
+        L = lib()
+        self._verts = np.ascontiguousarray(mesh.vertices, np.float32)
+        self._tris = np.ascontiguousarray(mesh.triangles, np.uint32)
+        self._sew = np.ascontiguousarray(mesh.sewing, np.uint32)
+        md = MeshDesc(mesh.vertex_count, _ptr(self._verts), mesh.triangle_count, _ptr(self._tris),
+                      int(self._sew.shape[0]), _ptr(self._sew) if self._sew.size else None)
+        d = ClothDefC(cdef.density, cdef.streching, cdef.shearing, cdef.bending, cdef.sewing, cdef.damping,
+                      cdef.thickness, cdef.friction)
+        h = C.c_void_p()
+        check(L.b3g_cloth_create(C.byref(md), C.byref(d), device, C.byref(h)), "b3g_cloth_create")
+        self.h = h
+        self.n = mesh.vertex_count
+        self.nsph = 0
+        self.stats = StepStatsC()
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().b3g_cloth_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    # b3Cloth API
+    def set_gravity(self, g) -> None:
+        check(lib().b3g_cloth_set_gravity(self.h, _ptr(_f3(g))), "set_gravity")
+
+    def get_gravity(self) -> np.ndarray:
+        out = np.zeros(3, np.float32)
+        check(lib().b3g_cloth_get_gravity(self.h, _ptr(out)), "get_gravity")
+        return out
+
+    def set_solver(self, opts: SolverOptions) -> None:
+        o = opts.as_c()
+        check(lib().b3g_cloth_set_solver(self.h, C.byref(o)), "set_solver")
+
+    def add_sphere(self, center, radius: float, friction: float) -> int:
+        sid = C.c_uint32(0)
+        check(lib().b3g_cloth_add_static_sphere(self.h, _ptr(_f3(center)), radius, friction, C.byref(sid)),
+              "add_static_sphere")
+        self.nsph += 1
+        return sid.value
+
+    def clear_colliders(self) -> None:
+        check(lib().b3g_cloth_clear_colliders(self.h), "clear_colliders")
+        self.nsph = 0
+
+    def particle(self, i: int) -> Particle:
+        return Particle(self, i)
+
+    get_particle = particle
+
+    def set_types(self, types) -> None:
+        t = np.ascontiguousarray(types, np.uint8)
+        check(lib().b3g_cloth_set_types(self.h, _ptr(t)), "set_types")
+
+    def apply_forces(self, f) -> None:
+        a = np.ascontiguousarray(f, np.float32)
+        check(lib().b3g_cloth_apply_forces(self.h, _ptr(a)), "apply_forces")
+
+    def apply_translations(self, t) -> None:
+        a = np.ascontiguousarray(t, np.float32)
+        check(lib().b3g_cloth_apply_translations(self.h, _ptr(a)), "apply_translations")
+
+    def step(self, dt: float, velocity_iterations: int = 8, position_iterations: int = 2) -> dict:
+        check(lib().b3g_cloth_step(self.h, dt, velocity_iterations, position_iterations, C.byref(self.stats)),
+              "step")
+        s = self.stats
+        return {"iterations": s.iterations, "delta0": s.delta0, "delta": s.delta, "b_delta": s.b_delta,
+                "active_contacts": s.active_contacts, "contacts": s.contacts, "step_ms": s.step_ms}
+
+    def step_profiled(self, dt: float, velocity_iterations: int = 8, position_iterations: int = 2) -> dict:
+        t = PhaseTimesC()
+        check(lib().b3g_cloth_step_profiled(self.h, dt, velocity_iterations, position_iterations, C.byref(t),
+                                            C.byref(self.stats)), "step_profiled")
+        out = {k: getattr(t, k) for k, _ in PhaseTimesC._fields_}
+        out["iterations"] = self.stats.iterations
+        return out
+
+    def info(self) -> dict:
+        i = ClothInfoC()
+        check(lib().b3g_cloth_get_info(self.h, C.byref(i)), "get_info")
+        return {k: getattr(i, k) for k, _ in ClothInfoC._fields_}
+
+    def assemble(self, dt: float) -> None:
+        check(lib().b3g_cloth_assemble(self.h, dt), "assemble")
+
+    def state(self) -> dict:
+        x = np.zeros((self.n, 3), np.float32)
+        v = np.zeros((self.n, 3), np.float32)
+        dv = np.zeros((self.n, 3), np.float32)
+        check(lib().b3g_cloth_read_state(self.h, _ptr(x), _ptr(v), _ptr(dv)), "read_state")
+        return {"x": x, "v": v, "dv": dv}
+
+    def positions(self, out: np.ndarray | None = None) -> np.ndarray:
+        x = out if out is not None else np.zeros((self.n, 3), np.float32)
+        check(lib().b3g_cloth_read_state(self.h, _ptr(x), None, None), "read_state")
+        return x
+
+    def write_state(self, x=None, v=None, dv=None) -> None:
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (x, v, dv)]
+        check(lib().b3g_cloth_write_state(self.h, *[None if a is None else _ptr(a) for a in arrs]), "write_state")
+
+    def masses(self) -> np.ndarray:
+        m = np.zeros(self.n, np.float32)
+        check(lib().b3g_cloth_read_masses(self.h, _ptr(m)), "read_masses")
+        return m
+
+    def energy(self) -> float:
+        e = C.c_float(0)
+        check(lib().b3g_cloth_get_energy(self.h, C.byref(e)), "get_energy")
+        return e.value
+
+    def contacts(self) -> dict:
+        k = max(self.nsph, 1)
+        ex = np.zeros(k * self.n, np.uint8)
+        ac = np.zeros(k * self.n, np.uint8)
+        imp = np.zeros((k * self.n, 3), np.float32)
+        check(lib().b3g_cloth_read_contacts(self.h, _ptr(ex), _ptr(ac), _ptr(imp)), "read_contacts")
+        return {"exists": ex[: self.nsph * self.n], "active": ac[: self.nsph * self.n],
+                "impulses": imp[: self.nsph * self.n]}
+
+    def system(self) -> dict:
+        nnz = C.c_uint32(0)
+        L = lib()
+        check(L.b3g_cloth_read_system(self.h, C.byref(nnz), None, None, None, None, None, None), "read_system")
+        rowptr = np.zeros(self.n + 1, np.uint32)
+        cols = np.zeros(nnz.value, np.uint32)
+        vals = np.zeros(9 * nnz.value, np.float32)
+        b = np.zeros(3 * self.n, np.float32)
+        S = np.zeros(self.n, np.float32)
+        x0 = np.zeros(3 * self.n, np.float32)
+        check(L.b3g_cloth_read_system(self.h, C.byref(nnz), _ptr(rowptr), _ptr(cols), _ptr(vals), _ptr(b), _ptr(S),
+                                      _ptr(x0)), "read_system")
+        return {"rowptr": rowptr, "cols": cols, "vals": vals, "b": b, "S": S, "x0": x0}
+
+    def setup(self, scene: Scene, opts: SolverOptions | None = None) -> "Cloth":
+        """Gravity, pinned vertices and colliders of a Scene."""
+        self.set_gravity(scene.gravity)
+        types = np.full(self.n, DYNAMIC, np.uint8)
+        types[np.asarray(scene.pinned, np.int64)] = STATIC
+        self.set_types(types)
+        for (c, r, mu) in scene.spheres:
+            self.add_sphere(c, r, mu)
+        if opts is not None:
+            self.set_solver(opts)
+        return self
+
+
+def kernel_launch_count() -> int:
+    return int(lib().b3g_kernel_launch_count())

@@ -1,0 +1,919 @@
+// C ABI of libb3g.so (include/b3g.h): cloth handles, device memory, the
+// per-step CUDA graph, particle edits and state transfers.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/b3g.h"
+#include "cloth_dev.cuh"
+#include "topology.h"
+
+using namespace b3g;
+
+namespace {
+
+// One device arena per cloth, carved into 256-byte aligned buffers.
+struct Arena {
+    char* base = nullptr;
+    size_t size = 0, used = 0;
+    template <class T> T* take(size_t count)
+    {
+        size_t off = (used + 255) & ~size_t(255);
+        used = off + count * sizeof(T);
+        return reinterpret_cast<T*>(base + off);
+    }
+};
+
+b3g_status from_cuda(cudaError_t e)
+{
+    if (e == cudaSuccess) return B3G_OK;
+    if (e == cudaErrorMemoryAllocation) return B3G_ERR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorInvalidDevice)
+        return B3G_ERR_NO_DEVICE;
+    return B3G_ERR_CUDA;
+}
+
+#define B3G_TRY(expr)                               \
+    do {                                            \
+        cudaError_t e_ = (expr);                    \
+        if (e_ != cudaSuccess) return from_cuda(e_); \
+    } while (0)
+
+}  // namespace
+
+struct b3g_cloth {
+    int device = 0;
+    cudaStream_t stream = nullptr, body_stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    Arena arena;
+    ClothDev dev{};
+    ClothTopology topo;
+    float gravity[3] = {0.0f, 0.0f, 0.0f};
+    b3g_solver_opts opts{B3G_STOP_REFERENCE, 0.0f, 20u, B3G_DOT_F32};
+    uint32_t step_index = 0;
+    int assemble_block = 128;
+
+    // pinned staging
+    StepScalars* h_sc = nullptr;
+    ParticleOp* h_ops = nullptr;
+    uint32_t ops_cap = 0;
+    std::vector<ParticleOp> pending;
+    ParticleOp* d_ops = nullptr;
+    uint32_t d_ops_cap = 0;
+    float* d_stage = nullptr;  // 3 n floats for array uploads
+    uint8_t* d_stage_u8 = nullptr;
+
+    // graph cache
+    cudaGraphExec_t exec = nullptr;
+    int graph_dot = -1;
+    uint32_t graph_pos_iters = UINT32_MAX;
+    uint32_t graph_nsph = UINT32_MAX;
+    bool graph_ok = true;
+
+    b3g_step_stats last{};
+};
+
+namespace {
+
+b3g_status flush_ops(b3g_cloth* c)
+{
+    if (c->pending.empty()) return B3G_OK;
+    uint32_t cnt = (uint32_t)c->pending.size();
+    if (cnt > c->ops_cap) {
+        if (c->h_ops) cudaFreeHost(c->h_ops);
+        c->ops_cap = std::max<uint32_t>(cnt, 256);
+        B3G_TRY(cudaMallocHost(&c->h_ops, c->ops_cap * sizeof(ParticleOp)));
+    }
+    if (cnt > c->d_ops_cap) {
+        if (c->d_ops) cudaFree(c->d_ops);
+        c->d_ops_cap = std::max<uint32_t>(cnt, 256);
+        B3G_TRY(cudaMalloc(&c->d_ops, c->d_ops_cap * sizeof(ParticleOp)));
+    }
+    // The pinned buffer may still be read by an earlier copy.
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    std::memcpy(c->h_ops, c->pending.data(), cnt * sizeof(ParticleOp));
+    B3G_TRY(cudaMemcpyAsync(c->d_ops, c->h_ops, cnt * sizeof(ParticleOp), cudaMemcpyHostToDevice, c->stream));
+    B3G_TRY(launch_particle_ops(c->dev, c->d_ops, cnt, c->stream));
+    c->pending.clear();
+    return B3G_OK;
+}
+
+void destroy_graph(b3g_cloth* c)
+{
+    if (c->exec) cudaGraphExecDestroy(c->exec);
+    c->exec = nullptr;
+}
+
+// Captures one step: [contacts_update] assemble cg_init while{cg iteration}
+// finalize [contact_position x (pos_iters - 1)] post.
+b3g_status build_graph(b3g_cloth* c, uint32_t pos_iters)
+{
+    destroy_graph(c);
+    const int dot = (int)c->opts.dot;
+    cudaStream_t st = c->stream;
+    cudaGraph_t graph = nullptr;
+    // launches recorded while capturing are not executions
+    const uint64_t launches_before = kernel_launches();
+    B3G_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t err = cudaSuccess;
+    do {
+        if ((err = launch_contacts_update(c->dev, st)) != cudaSuccess) break;
+        if ((err = launch_assemble(c->dev, c->assemble_block, st)) != cudaSuccess) break;
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cap;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        if ((err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cap, &deps, &ndeps)) != cudaSuccess) break;
+        cudaGraphConditionalHandle cond;
+        if ((err = cudaGraphConditionalHandleCreate(&cond, cap, 0, 0)) != cudaSuccess) break;
+        if ((err = launch_cg_init(c->dev, dot, cond, 1, st)) != cudaSuccess) break;
+        if ((err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cap, &deps, &ndeps)) != cudaSuccess) break;
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t wnode;
+        if ((err = cudaGraphAddNode(&wnode, cap, deps, ndeps, &cp)) != cudaSuccess) break;
+        if ((err = cudaStreamUpdateCaptureDependencies(st, &wnode, 1, cudaStreamSetCaptureDependencies)) !=
+            cudaSuccess)
+            break;
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        if ((err = cudaStreamBeginCaptureToGraph(c->body_stream, body, nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+            break;
+        cudaError_t e2 = launch_cg_iteration(c->dev, dot, cond, 1, c->body_stream);
+        cudaGraph_t body_out = nullptr;
+        cudaError_t e3 = cudaStreamEndCapture(c->body_stream, &body_out);
+        if (e2 != cudaSuccess) { err = e2; break; }
+        if (e3 != cudaSuccess) { err = e3; break; }
+        if ((err = launch_finalize(c->dev, st)) != cudaSuccess) break;
+        for (uint32_t k = 1; k < pos_iters; ++k)
+            if ((err = launch_contact_position(c->dev, st)) != cudaSuccess) break;
+        if (err != cudaSuccess) break;
+        if ((err = launch_post(c->dev, st)) != cudaSuccess) break;
+    } while (0);
+    cudaError_t e_end = cudaStreamEndCapture(st, &graph);
+    count_launches(launches_before - kernel_launches());
+    if (err == cudaSuccess) err = e_end;
+    if (err == cudaSuccess) err = cudaGraphInstantiate(&c->exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        c->exec = nullptr;
+        return from_cuda(err);
+    }
+    c->graph_dot = dot;
+    c->graph_pos_iters = pos_iters;
+    c->graph_nsph = c->dev.nsph;
+    return B3G_OK;
+}
+
+// Same sequence without a graph: every CG iteration is launched and returns
+// early on the device once the loop condition is cleared.
+b3g_status launch_step_plain(b3g_cloth* c, uint32_t pos_iters)
+{
+    const int dot = (int)c->opts.dot;
+    cudaStream_t st = c->stream;
+    cudaGraphConditionalHandle none = 0;
+    B3G_TRY(launch_contacts_update(c->dev, st));
+    B3G_TRY(launch_assemble(c->dev, c->assemble_block, st));
+    B3G_TRY(launch_cg_init(c->dev, dot, none, 0, st));
+    for (uint32_t k = 0; k < c->opts.max_iterations; ++k) B3G_TRY(launch_cg_iteration(c->dev, dot, none, 0, st));
+    B3G_TRY(launch_finalize(c->dev, st));
+    for (uint32_t k = 1; k < pos_iters; ++k) B3G_TRY(launch_contact_position(c->dev, st));
+    B3G_TRY(launch_post(c->dev, st));
+    return B3G_OK;
+}
+
+bool valid(const b3g_cloth* c) { return c != nullptr && c->dev.n > 0; }
+
+}  // namespace
+
+extern "C" {
+
+const char* b3g_status_string(b3g_status s)
+{
+    switch (s) {
+        case B3G_OK: return "ok";
+        case B3G_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case B3G_ERR_DEGENERATE_MESH: return "degenerate mesh";
+        case B3G_ERR_NO_DEVICE: return "no CUDA device";
+        case B3G_ERR_OUT_OF_MEMORY: return "out of memory";
+        case B3G_ERR_CUDA: return "CUDA error";
+        case B3G_ERR_NUMERICAL: return "numerical breakdown in CG";
+        case B3G_ERR_TIMEOUT: return "device wait timed out";
+        case B3G_ERR_CAPACITY: return "capacity exceeded";
+        case B3G_ERR_UNSUPPORTED: return "unsupported mesh";
+    }
+    return "unknown status";
+}
+
+uint64_t b3g_kernel_launch_count(void) { return kernel_launches(); }
+
+b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, int device, b3g_cloth** out)
+{
+    if (!mesh || !def || !out || !mesh->vertices || !mesh->triangles || mesh->vertex_count == 0 ||
+        mesh->triangle_count == 0 || (mesh->sewing_line_count && !mesh->sewing_lines))
+        return B3G_ERR_INVALID_ARGUMENT;
+    if (!(def->density > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return B3G_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return B3G_ERR_INVALID_ARGUMENT;
+
+    const float d8[8] = {def->density, def->streching, def->shearing, def->bending,
+                         def->sewing,  def->damping,   def->thickness, def->friction};
+    b3g_cloth* c = new (std::nothrow) b3g_cloth();
+    if (!c) return B3G_ERR_OUT_OF_MEMORY;
+    int rc = build_topology(mesh->vertex_count, mesh->vertices, mesh->triangle_count, mesh->triangles,
+                            mesh->sewing_line_count, mesh->sewing_lines, d8, &c->topo);
+    if (rc != 0) {
+        delete c;
+        return (b3g_status)rc;
+    }
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete c;
+        return from_cuda(e);
+    }
+    const ClothTopology& T = c->topo;
+    const uint32_t n = T.n, t = T.t, ns = T.ns;
+    ClothDev& d = c->dev;
+    d.n = n;
+    d.t = t;
+    d.ns = ns;
+    d.nsph = 0;
+    d.nslices = T.nslices;
+    d.max_deg = T.max_deg;
+    d.E = T.E;
+    d.k_stretch = def->streching;
+    d.k_shear = def->shearing;
+    d.k_damp = def->damping;
+    d.thickness = def->thickness;
+    d.friction = def->friction;
+    d.block = 256;
+    d.grid = std::min<uint32_t>((n + 255) / 256, 148 * 8);
+
+    // sizes
+    const size_t vec = 3 * (size_t)n * sizeof(float);
+    size_t bytes = 0;
+    auto add = [&](size_t b) { bytes += ((b + 255) & ~size_t(255)) + 256; };
+    add((T.nslices + 1) * 4); add(n); add((size_t)T.E * 4); add((size_t)T.E * 36);
+    add((n + 1) * 4); add(T.inc_elem.size() * 4 + 4); add(T.inc_meta.size() * 4 + 4);
+    add((size_t)t * 16); add((size_t)t * 16); add((size_t)t * 8); add((size_t)ns * 8 + 8); add((size_t)ns * 16 + 16);
+    for (int k = 0; k < 11; ++k) add(vec);  // x v fext y mx b dv r p s pinv
+    add((size_t)n * 4); add(n);             // mass, type
+    add(vec); add(vec);                     // fat lo / hi
+    const size_t nn = (size_t)kMaxSpheres * n;
+    add(nn); add(nn); add(nn * 4); add(nn * 12); add(nn * 12); add(nn * 12); add(nn * 12);
+    add(sizeof(StepScalars));
+    add((size_t)d.grid * 32);
+    add(vec); add(n);                       // staging
+    e = cudaMalloc(&c->arena.base, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return B3G_ERR_OUT_OF_MEMORY;
+    }
+    c->arena.size = bytes;
+    Arena& A = c->arena;
+    uint32_t* slice_off = A.take<uint32_t>(T.nslices + 1);
+    uint8_t* row_deg = A.take<uint8_t>(n);
+    uint32_t* cols = A.take<uint32_t>(T.E);
+    d.vals = A.take<float>((size_t)T.E * 9);
+    uint32_t* inc_ptr = A.take<uint32_t>(n + 1);
+    uint32_t* inc_elem = A.take<uint32_t>(T.inc_elem.size() + 1);
+    uint32_t* inc_meta = A.take<uint32_t>(T.inc_meta.size() + 1);
+    uint4* tri = A.take<uint4>(t);
+    float4* tri_rest = A.take<float4>(t);
+    float2* tri_rest2 = A.take<float2>(t);
+    uint2* spr = A.take<uint2>(ns + 1);
+    float4* spr_par = A.take<float4>(ns + 1);
+    d.x = A.take<float>(3 * (size_t)n);
+    d.v = A.take<float>(3 * (size_t)n);
+    d.fext = A.take<float>(3 * (size_t)n);
+    d.y = A.take<float>(3 * (size_t)n);
+    d.mx = A.take<float>(3 * (size_t)n);
+    d.b = A.take<float>(3 * (size_t)n);
+    d.dv = A.take<float>(3 * (size_t)n);
+    d.r = A.take<float>(3 * (size_t)n);
+    d.p = A.take<float>(3 * (size_t)n);
+    d.s = A.take<float>(3 * (size_t)n);
+    d.pinv = A.take<float>(3 * (size_t)n);
+    float* mass = A.take<float>(n);
+    d.type = A.take<uint8_t>(n);
+    d.fat_lo = A.take<float>(3 * (size_t)n);
+    d.fat_hi = A.take<float>(3 * (size_t)n);
+    d.c_exists = A.take<uint8_t>(nn);
+    d.c_active = A.take<uint8_t>(nn);
+    d.c_key = A.take<uint32_t>(nn);
+    d.c_normal = A.take<float>(3 * nn);
+    d.c_t1 = A.take<float>(3 * nn);
+    d.c_t2 = A.take<float>(3 * nn);
+    d.c_imp = A.take<float>(3 * nn);
+    d.sc = A.take<StepScalars>(1);
+    d.partials = A.take<char>((size_t)d.grid * 32);
+    c->d_stage = A.take<float>(3 * (size_t)n);
+    c->d_stage_u8 = A.take<uint8_t>(n);
+    d.slice_off = slice_off;
+    d.row_deg = row_deg;
+    d.cols = cols;
+    d.inc_ptr = inc_ptr;
+    d.inc_elem = inc_elem;
+    d.inc_meta = inc_meta;
+    d.tri = tri;
+    d.tri_rest = tri_rest;
+    d.tri_rest2 = tri_rest2;
+    d.spr = spr;
+    d.spr_par = spr_par;
+    d.mass = mass;
+
+    // host-side images
+    std::vector<uint4> h_tri(t);
+    std::vector<float4> h_rest(t);
+    std::vector<float2> h_rest2(t);
+    for (uint32_t k = 0; k < t; ++k) {
+        h_tri[k] = make_uint4(mesh->triangles[3 * k], mesh->triangles[3 * k + 1], mesh->triangles[3 * k + 2], 0u);
+        const float* r = &T.rest[6 * (size_t)k];
+        h_rest[k] = make_float4(r[0], r[1], r[2], r[3]);
+        h_rest2[k] = make_float2(r[4], r[5]);
+    }
+    std::vector<uint2> h_spr(ns + 1);
+    std::vector<float4> h_sp(ns + 1);
+    for (uint32_t s = 0; s < ns; ++s) {
+        h_spr[s] = make_uint2(T.spring_pairs[2 * s], T.spring_pairs[2 * s + 1]);
+        h_sp[s] = make_float4(T.spring_par[3 * s], T.spring_par[3 * s + 1], T.spring_par[3 * s + 2], 0.0f);
+    }
+    std::vector<float> planes(3 * (size_t)n), lo(3 * (size_t)n), hi(3 * (size_t)n);
+    const float r = def->thickness;
+    for (uint32_t i = 0; i < n; ++i)
+        for (int q = 0; q < 3; ++q) {
+            float x = mesh->vertices[3 * i + q];
+            planes[(size_t)q * n + i] = x;
+            // proxy at creation: [x - r, x + r] fattened by B3_AABB_EXTENSION (cloth.cpp:312-317)
+            lo[(size_t)q * n + i] = (x - r) - 0.2f;
+            hi[(size_t)q * n + i] = (x + r) + 0.2f;
+        }
+    std::vector<uint8_t> types(n, (uint8_t)B3G_DYNAMIC);
+
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess ||
+        (e = cudaMallocHost(&c->h_sc, sizeof(StepScalars))) != cudaSuccess) {
+        b3g_cloth_destroy(c);
+        return from_cuda(e);
+    }
+    cudaStream_t st = c->stream;
+    std::memset(c->h_sc, 0, sizeof(StepScalars));
+    auto up = [&](void* dst, const void* src, size_t b) {
+        if (e == cudaSuccess && b) e = cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, st);
+    };
+    e = cudaMemsetAsync(A.base, 0, A.size, st);
+    up(slice_off, T.slice_off.data(), T.slice_off.size() * 4);
+    up(row_deg, T.row_deg.data(), n);
+    up(cols, T.sell_cols.data(), (size_t)T.E * 4);
+    up(inc_ptr, T.inc_ptr.data(), (n + 1) * 4);
+    up(inc_elem, T.inc_elem.data(), T.inc_elem.size() * 4);
+    up(inc_meta, T.inc_meta.data(), T.inc_meta.size() * 4);
+    up(tri, h_tri.data(), (size_t)t * 16);
+    up(tri_rest, h_rest.data(), (size_t)t * 16);
+    up(tri_rest2, h_rest2.data(), (size_t)t * 8);
+    up(spr, h_spr.data(), (size_t)ns * 8);
+    up(spr_par, h_sp.data(), (size_t)ns * 16);
+    up(d.x, planes.data(), vec);
+    up(mass, T.mass.data(), (size_t)n * 4);
+    up(d.type, types.data(), n);
+    up(d.fat_lo, lo.data(), vec);
+    up(d.fat_hi, hi.data(), vec);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        b3g_cloth_destroy(c);
+        return from_cuda(e);
+    }
+    size_t smem = assemble_smem_bytes(d, c->assemble_block);
+    while (smem > 200 * 1024 && c->assemble_block > 32) {
+        c->assemble_block /= 2;
+        smem = assemble_smem_bytes(d, c->assemble_block);
+    }
+    *out = c;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_destroy(b3g_cloth* c)
+{
+    if (!c) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    destroy_graph(c);
+    if (c->arena.base) cudaFree(c->arena.base);
+    if (c->d_ops) cudaFree(c->d_ops);
+    if (c->h_ops) cudaFreeHost(c->h_ops);
+    if (c->h_sc) cudaFreeHost(c->h_sc);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->body_stream) cudaStreamDestroy(c->body_stream);
+    delete c;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_set_gravity(b3g_cloth* c, const float g[3])
+{
+    if (!valid(c) || !g) return B3G_ERR_INVALID_ARGUMENT;
+    std::memcpy(c->gravity, g, sizeof(c->gravity));
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_get_gravity(const b3g_cloth* c, float g[3])
+{
+    if (!valid(c) || !g) return B3G_ERR_INVALID_ARGUMENT;
+    std::memcpy(g, c->gravity, sizeof(c->gravity));
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_set_solver(b3g_cloth* c, const b3g_solver_opts* o)
+{
+    if (!valid(c) || !o) return B3G_ERR_INVALID_ARGUMENT;
+    if (o->max_iterations < 1 || (o->stop_rule != B3G_STOP_REFERENCE && o->stop_rule != B3G_STOP_RELATIVE) ||
+        (o->dot != B3G_DOT_F32 && o->dot != B3G_DOT_COMPENSATED && o->dot != B3G_DOT_F64) ||
+        (o->stop_rule == B3G_STOP_RELATIVE && !(o->tolerance >= 0.0f)))
+        return B3G_ERR_INVALID_ARGUMENT;
+    c->opts = *o;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_add_static_sphere(b3g_cloth* c, const float center[3], float radius, float friction,
+                                       uint32_t* shape_id)
+{
+    if (!valid(c) || !center || !(radius > 0.0f) || !(friction >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    if (c->dev.nsph >= (uint32_t)kMaxSpheres) return B3G_ERR_CAPACITY;
+    SphereDev& s = c->dev.sph[c->dev.nsph];
+    s.cx = center[0];
+    s.cy = center[1];
+    s.cz = center[2];
+    s.radius = radius;
+    s.friction = friction;
+    // sphere AABB (sphere_shape.cpp:53-59) fattened by B3_AABB_EXTENSION (broad_phase.cpp:78-82)
+    for (int q = 0; q < 3; ++q) {
+        s.lo[q] = (center[q] - radius) - 0.2f;
+        s.hi[q] = (center[q] + radius) + 0.2f;
+    }
+    if (shape_id) *shape_id = c->dev.nsph;
+    c->dev.nsph += 1;
+    destroy_graph(c);
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_clear_colliders(b3g_cloth* c)
+{
+    if (!valid(c)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    B3G_TRY(launch_clear_contacts(c->dev, c->stream));
+    c->dev.nsph = 0;
+    destroy_graph(c);
+    return B3G_OK;
+}
+
+static b3g_status push_op(b3g_cloth* c, uint32_t vertex, uint32_t kind, const float* a)
+{
+    if (!valid(c) || vertex >= c->dev.n) return B3G_ERR_INVALID_ARGUMENT;
+    ParticleOp op;
+    op.vertex = vertex;
+    op.kind = kind;
+    op.a[0] = a ? a[0] : 0.0f;
+    op.a[1] = a ? a[1] : 0.0f;
+    op.a[2] = a ? a[2] : 0.0f;
+    c->pending.push_back(op);
+    return B3G_OK;
+}
+
+b3g_status b3g_particle_set_type(b3g_cloth* c, uint32_t vertex, b3g_particle_type type)
+{
+    if (type != B3G_STATIC && type != B3G_KINEMATIC && type != B3G_DYNAMIC) return B3G_ERR_INVALID_ARGUMENT;
+    float a[3] = {(float)type, 0.0f, 0.0f};
+    return push_op(c, vertex, OP_SET_TYPE, a);
+}
+
+b3g_status b3g_particle_set_position(b3g_cloth* c, uint32_t vertex, const float p[3])
+{
+    if (!p) return B3G_ERR_INVALID_ARGUMENT;
+    return push_op(c, vertex, OP_SET_POSITION, p);
+}
+
+b3g_status b3g_particle_set_velocity(b3g_cloth* c, uint32_t vertex, const float v[3])
+{
+    if (!v) return B3G_ERR_INVALID_ARGUMENT;
+    return push_op(c, vertex, OP_SET_VELOCITY, v);
+}
+
+b3g_status b3g_particle_apply_force(b3g_cloth* c, uint32_t vertex, const float f[3])
+{
+    if (!f) return B3G_ERR_INVALID_ARGUMENT;
+    return push_op(c, vertex, OP_APPLY_FORCE, f);
+}
+
+b3g_status b3g_particle_apply_translation(b3g_cloth* c, uint32_t vertex, const float t[3])
+{
+    if (!t) return B3G_ERR_INVALID_ARGUMENT;
+    return push_op(c, vertex, OP_APPLY_TRANSLATION, t);
+}
+
+static b3g_status read_vertex(const b3g_cloth* cc, uint32_t vertex, const float* planes, float out[3])
+{
+    b3g_cloth* c = const_cast<b3g_cloth*>(cc);
+    if (!valid(c) || vertex >= c->dev.n || !out) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    const uint32_t n = c->dev.n;
+    for (int q = 0; q < 3; ++q)
+        B3G_TRY(cudaMemcpyAsync(out + q, planes + (size_t)q * n + vertex, 4, cudaMemcpyDeviceToHost, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    return B3G_OK;
+}
+
+b3g_status b3g_particle_get_position(const b3g_cloth* c, uint32_t vertex, float p[3])
+{
+    return c ? read_vertex(c, vertex, c->dev.x, p) : B3G_ERR_INVALID_ARGUMENT;
+}
+
+b3g_status b3g_particle_get_velocity(const b3g_cloth* c, uint32_t vertex, float v[3])
+{
+    return c ? read_vertex(c, vertex, c->dev.v, v) : B3G_ERR_INVALID_ARGUMENT;
+}
+
+b3g_status b3g_particle_get_mass(const b3g_cloth* c, uint32_t vertex, float* m)
+{
+    if (!valid(c) || vertex >= c->dev.n || !m) return B3G_ERR_INVALID_ARGUMENT;
+    *m = c->topo.mass[vertex];
+    return B3G_OK;
+}
+
+b3g_status b3g_particle_get_type(const b3g_cloth* cc, uint32_t vertex, b3g_particle_type* type)
+{
+    b3g_cloth* c = const_cast<b3g_cloth*>(cc);
+    if (!valid(c) || vertex >= c->dev.n || !type) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    uint8_t t8 = 0;
+    B3G_TRY(cudaMemcpyAsync(&t8, c->dev.type + vertex, 1, cudaMemcpyDeviceToHost, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    *type = (b3g_particle_type)t8;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_set_types(b3g_cloth* c, const uint8_t* types)
+{
+    if (!valid(c) || !types) return B3G_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < c->dev.n; ++i)
+        if (types[i] > 2) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    B3G_TRY(cudaMemcpyAsync(c->d_stage_u8, types, c->dev.n, cudaMemcpyHostToDevice, c->stream));
+    B3G_TRY(launch_set_types(c->dev, c->d_stage_u8, c->stream));
+    return B3G_OK;
+}
+
+static b3g_status add_array(b3g_cloth* c, float* dst, const float* src, int only_dynamic)
+{
+    if (!valid(c) || !src) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    B3G_TRY(cudaMemcpyAsync(c->d_stage, src, 3 * (size_t)c->dev.n * 4, cudaMemcpyHostToDevice, c->stream));
+    B3G_TRY(launch_add_vectors(c->dev, dst, c->d_stage, only_dynamic, c->stream));
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_apply_forces(b3g_cloth* c, const float* f)
+{
+    return c ? add_array(c, c->dev.fext, f, 1) : B3G_ERR_INVALID_ARGUMENT;
+}
+
+b3g_status b3g_cloth_apply_translations(b3g_cloth* c, const float* t)
+{
+    return c ? add_array(c, c->dev.y, t, 0) : B3G_ERR_INVALID_ARGUMENT;
+}
+
+b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, b3g_step_stats* stats)
+{
+    if (!valid(c)) return B3G_ERR_INVALID_ARGUMENT;
+    if (!(dt >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    cudaStream_t st = c->stream;
+    // step parameters (the pinned buffer is free: the previous step was waited for)
+    StepScalars* h = c->h_sc;
+    std::memset(h, 0, sizeof(StepScalars));
+    h->dt = dt;
+    h->vel_iters = vel_iters;
+    h->pos_iters = pos_iters;
+    h->step_index = ++c->step_index;
+    h->max_iter = c->opts.max_iterations;
+    h->stop_rule = (int)c->opts.stop_rule;
+    h->tol = c->opts.tolerance;
+    h->dot = (int)c->opts.dot;
+    h->gx = c->gravity[0];
+    h->gy = c->gravity[1];
+    h->gz = c->gravity[2];
+    h->pos_solved = 1;
+    B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, st));
+    B3G_TRY(cudaEventRecord(c->ev0, st));
+    if (dt > 0.0f) {
+        if (c->graph_ok && (!c->exec || c->graph_dot != (int)c->opts.dot || c->graph_pos_iters != pos_iters ||
+                            c->graph_nsph != c->dev.nsph)) {
+            if (build_graph(c, pos_iters) != B3G_OK) c->graph_ok = false;
+        }
+        if (c->graph_ok && c->exec) {
+            B3G_TRY(cudaGraphLaunch(c->exec, st));
+        } else {
+            if ((s = launch_step_plain(c, pos_iters)) != B3G_OK) return s;
+        }
+    } else {
+        // Step with dt = 0: contacts update, no solve, clear and AABB sync
+        B3G_TRY(launch_contacts_update(c->dev, st));
+        B3G_TRY(launch_post(c->dev, st));
+    }
+    B3G_TRY(cudaEventRecord(c->ev1, st));
+    B3G_TRY(cudaMemcpyAsync(h, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, st));
+    B3G_TRY(cudaStreamSynchronize(st));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    b3g_step_stats& L = c->last;
+    L.iterations = dt > 0.0f ? h->iter : 0;
+    L.delta0 = h->delta0;
+    L.delta = h->delta;
+    L.b_delta = h->b_delta;
+    L.active_contacts = h->active_contacts;
+    L.contacts = h->contacts;
+    L.step_ms = ms;
+    if (dt > 0.0f && c->graph_ok && c->exec) {
+        // kernel nodes the graph ran: [contacts_update] assemble cg_init,
+        // 3 per CG iteration, finalize, [contact_position x (pos_iters - 1)], post
+        const uint64_t ns = c->dev.nsph ? 1 : 0;
+        count_launches(ns + 2 + 3ull * L.iterations + 1 + (ns && pos_iters > 1 ? pos_iters - 1 : 0) + 1);
+    }
+    if (stats) *stats = L;
+    if (dt > 0.0f && h->status != 0) return (b3g_status)h->status;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_assemble(b3g_cloth* c, float dt)
+{
+    if (!valid(c) || !(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    StepScalars* h = c->h_sc;
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    std::memset(h, 0, sizeof(StepScalars));
+    h->dt = dt;
+    h->gx = c->gravity[0];
+    h->gy = c->gravity[1];
+    h->gz = c->gravity[2];
+    B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, c->stream));
+    B3G_TRY(launch_assemble(c->dev, c->assemble_block, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters,
+                                   b3g_phase_times* times, b3g_step_stats* stats)
+{
+    if (!valid(c) || !times || !(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    cudaStream_t st = c->stream;
+    B3G_TRY(cudaStreamSynchronize(st));
+    StepScalars* h = c->h_sc;
+    std::memset(h, 0, sizeof(StepScalars));
+    h->dt = dt;
+    h->vel_iters = vel_iters;
+    h->pos_iters = pos_iters;
+    h->step_index = ++c->step_index;
+    h->max_iter = c->opts.max_iterations;
+    h->stop_rule = (int)c->opts.stop_rule;
+    h->tol = c->opts.tolerance;
+    h->dot = (int)c->opts.dot;
+    h->gx = c->gravity[0];
+    h->gy = c->gravity[1];
+    h->gz = c->gravity[2];
+    h->pos_solved = 1;
+    B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, st));
+    std::memset(times, 0, sizeof(*times));
+    const int dot = (int)c->opts.dot;
+    float ms = 0.0f;
+    auto timed = [&](float* acc, auto&& fn) -> b3g_status {
+        B3G_TRY(cudaEventRecord(c->ev0, st));
+        B3G_TRY(fn());
+        B3G_TRY(cudaEventRecord(c->ev1, st));
+        B3G_TRY(cudaEventSynchronize(c->ev1));
+        B3G_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        *acc += ms;
+        return B3G_OK;
+    };
+    cudaGraphConditionalHandle none = 0;
+    if (c->dev.nsph && (s = timed(&times->contacts_update_ms, [&] { return launch_contacts_update(c->dev, st); })))
+        return s;
+    if ((s = timed(&times->assemble_ms, [&] { return launch_assemble(c->dev, c->assemble_block, st); }))) return s;
+    if ((s = timed(&times->cg_init_ms, [&] { return launch_cg_init(c->dev, dot, none, 0, st); }))) return s;
+    StepScalars probe;
+    for (;;) {
+        B3G_TRY(cudaMemcpy(&probe, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost));
+        if (!probe.cont) break;
+        if ((s = timed(&times->cg_spmv_ms, [&] { return launch_cg_part(c->dev, dot, 0, st); }))) return s;
+        if ((s = timed(&times->cg_update_ms, [&] { return launch_cg_part(c->dev, dot, 1, st); }))) return s;
+        if ((s = timed(&times->cg_direction_ms, [&] { return launch_cg_part(c->dev, dot, 2, st); }))) return s;
+        times->cg_iterations += 1;
+    }
+    if ((s = timed(&times->finalize_ms, [&] { return launch_finalize(c->dev, st); }))) return s;
+    for (uint32_t k = 1; c->dev.nsph && k < pos_iters; ++k) {
+        if ((s = timed(&times->contact_position_ms, [&] { return launch_contact_position(c->dev, st); }))) return s;
+        times->contact_position_launches += 1;
+    }
+    if ((s = timed(&times->post_ms, [&] { return launch_post(c->dev, st); }))) return s;
+    B3G_TRY(cudaMemcpyAsync(h, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, st));
+    B3G_TRY(cudaStreamSynchronize(st));
+    b3g_step_stats& L = c->last;
+    L.iterations = h->iter;
+    L.delta0 = h->delta0;
+    L.delta = h->delta;
+    L.b_delta = h->b_delta;
+    L.active_contacts = h->active_contacts;
+    L.contacts = h->contacts;
+    L.step_ms = times->contacts_update_ms + times->assemble_ms + times->cg_init_ms + times->cg_spmv_ms +
+                times->cg_update_ms + times->cg_direction_ms + times->finalize_ms + times->contact_position_ms +
+                times->post_ms;
+    if (stats) *stats = L;
+    if (h->status != 0) return (b3g_status)h->status;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_get_info(const b3g_cloth* c, b3g_cloth_info* info)
+{
+    if (!valid(c) || !info) return B3G_ERR_INVALID_ARGUMENT;
+    info->vertices = c->topo.n;
+    info->triangles = c->topo.t;
+    info->springs = c->topo.ns;
+    info->blocks = (uint32_t)c->topo.row_cols.size();
+    info->sell_entries = c->topo.E;
+    info->max_degree = c->topo.max_deg;
+    return B3G_OK;
+}
+
+uint32_t b3g_cloth_vertex_count(const b3g_cloth* c) { return valid(c) ? c->dev.n : 0u; }
+
+static b3g_status read_planes(b3g_cloth* c, const float* planes, float* out)
+{
+    const uint32_t n = c->dev.n;
+    std::vector<float> tmp(3 * (size_t)n);
+    B3G_TRY(cudaMemcpyAsync(tmp.data(), planes, 3 * (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    for (uint32_t i = 0; i < n; ++i)
+        for (int q = 0; q < 3; ++q) out[3 * i + q] = tmp[(size_t)q * n + i];
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_read_state(const b3g_cloth* cc, float* x, float* v, float* mx)
+{
+    b3g_cloth* c = const_cast<b3g_cloth*>(cc);
+    if (!valid(c)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    if (x && (s = read_planes(c, c->dev.x, x)) != B3G_OK) return s;
+    if (v && (s = read_planes(c, c->dev.v, v)) != B3G_OK) return s;
+    if (mx && (s = read_planes(c, c->dev.mx, mx)) != B3G_OK) return s;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_write_state(b3g_cloth* c, const float* x, const float* v, const float* mx)
+{
+    if (!valid(c)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    const uint32_t n = c->dev.n;
+    std::vector<float> tmp(3 * (size_t)n);
+    const float* srcs[3] = {x, v, mx};
+    float* dsts[3] = {c->dev.x, c->dev.v, c->dev.mx};
+    for (int k = 0; k < 3; ++k) {
+        if (!srcs[k]) continue;
+        for (uint32_t i = 0; i < n; ++i)
+            for (int q = 0; q < 3; ++q) tmp[(size_t)q * n + i] = srcs[k][3 * i + q];
+        B3G_TRY(cudaMemcpyAsync(dsts[k], tmp.data(), 3 * (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
+        B3G_TRY(cudaStreamSynchronize(c->stream));
+    }
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_read_masses(const b3g_cloth* c, float* m)
+{
+    if (!valid(c) || !m) return B3G_ERR_INVALID_ARGUMENT;
+    std::memcpy(m, c->topo.mass.data(), c->topo.mass.size() * 4);
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_get_energy(const b3g_cloth* cc, float* energy)
+{
+    b3g_cloth* c = const_cast<b3g_cloth*>(cc);
+    if (!valid(c) || !energy) return B3G_ERR_INVALID_ARGUMENT;
+    const uint32_t n = c->dev.n;
+    std::vector<float> v(3 * (size_t)n);
+    b3g_status s = b3g_cloth_read_state(c, nullptr, v.data(), nullptr);
+    if (s != B3G_OK) return s;
+    // summed in particle-list order (newest particle first), cloth.cpp:366-374
+    float E = 0.0f;
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t i = n - 1 - k;
+        E += c->topo.mass[i] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+    }
+    *energy = 0.5f * E;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_read_contacts(const b3g_cloth* cc, uint8_t* exists, uint8_t* active, float* impulses)
+{
+    b3g_cloth* c = const_cast<b3g_cloth*>(cc);
+    if (!valid(c)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    const size_t nn = (size_t)c->dev.nsph * c->dev.n;
+    if (!nn) return B3G_OK;
+    const size_t nall = (size_t)kMaxSpheres * c->dev.n;
+    if (exists) B3G_TRY(cudaMemcpyAsync(exists, c->dev.c_exists, nn, cudaMemcpyDeviceToHost, c->stream));
+    if (active) B3G_TRY(cudaMemcpyAsync(active, c->dev.c_active, nn, cudaMemcpyDeviceToHost, c->stream));
+    if (impulses) {
+        std::vector<float> tmp(3 * nall);
+        B3G_TRY(cudaMemcpyAsync(tmp.data(), c->dev.c_imp, 3 * nall * 4, cudaMemcpyDeviceToHost, c->stream));
+        B3G_TRY(cudaStreamSynchronize(c->stream));
+        // c_imp planes have stride nsph * n
+        for (size_t q = 0; q < nn; ++q)
+            for (int k = 0; k < 3; ++k) impulses[3 * q + k] = tmp[k * nn + q];
+    }
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_last_stats(const b3g_cloth* c, b3g_step_stats* stats)
+{
+    if (!valid(c) || !stats) return B3G_ERR_INVALID_ARGUMENT;
+    *stats = c->last;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_read_system(const b3g_cloth* cc, uint32_t* nnz, uint32_t* rowptr, uint32_t* cols, float* vals,
+                                 float* b, float* S, float* x0)
+{
+    b3g_cloth* c = const_cast<b3g_cloth*>(cc);
+    if (!valid(c) || !nnz) return B3G_ERR_INVALID_ARGUMENT;
+    const ClothTopology& T = c->topo;
+    const uint32_t n = T.n;
+    *nnz = (uint32_t)T.row_cols.size();
+    if (!vals) return B3G_OK;
+    if (!rowptr || !cols) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    std::vector<float> sv(9 * (size_t)T.E);
+    B3G_TRY(cudaMemcpyAsync(sv.data(), c->dev.vals, 9 * (size_t)T.E * 4, cudaMemcpyDeviceToHost, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    std::memcpy(rowptr, T.row_ptr.data(), (n + 1) * 4);
+    std::memcpy(cols, T.row_cols.data(), T.row_cols.size() * 4);
+    for (uint32_t r = 0; r < n; ++r) {
+        uint32_t q = r / 32, lane = r % 32;
+        for (uint32_t k = 0; k < T.row_deg[r]; ++k) {
+            size_t idx = T.slice_off[q] + 32 * k + lane;
+            for (int m = 0; m < 9; ++m) vals[9 * (size_t)(T.row_ptr[r] + k) + m] = sv[(size_t)m * T.E + idx];
+        }
+    }
+    b3g_status s;
+    if (b && (s = read_planes(c, c->dev.b, b)) != B3G_OK) return s;
+    if (S || x0) {
+        std::vector<uint8_t> ty(n);
+        std::vector<float> mx(3 * (size_t)n);
+        B3G_TRY(cudaMemcpyAsync(ty.data(), c->dev.type, n, cudaMemcpyDeviceToHost, c->stream));
+        if ((s = read_planes(c, c->dev.mx, mx.data())) != B3G_OK) return s;
+        // the system's warm start is the m_x the step began with: after a
+        // step, m_x already holds the new solution; report S and m_x as stored
+        for (uint32_t i = 0; i < n; ++i) {
+            if (S) S[i] = ty[i] == B3G_DYNAMIC ? 1.0f : 0.0f;
+            if (x0)
+                for (int q = 0; q < 3; ++q) x0[3 * i + q] = mx[3 * i + q];
+        }
+    }
+    return B3G_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,142 @@
+// Device-side layout of one cloth and the kernels of one implicit step.
+//
+// Layout (all in HBM, owned by the cloth handle):
+//  * per-vertex state as SoA planes of length n: x, v, f_ext, y (translation),
+//    mx (last CG solution, the warm start), b, dv, r, p, s, pinv (3 planes
+//    each), mass (1 plane), type (u8);
+//  * the block matrix A in sliced ELL (SELL-32): rows in slices of 32, one
+//    slice padded to its widest row; entry (row 32 q + lane, slot k) sits at
+//    slice_off[q] + 32 k + lane, so a warp reading slot k of its 32 rows reads
+//    32 consecutive words per plane.  Values are 9 planes of E floats
+//    (column-major b3Mat33 order), columns one u32 plane.  Slot 0 of every row
+//    is its diagonal block; padding slots point at the row itself with zero
+//    values;
+//  * per-vertex incidence lists (CSR) of the elements touching the vertex, in
+//    the order Bounce applies its forces (force list = reverse creation order,
+//    src/bounce/cloth/cloth.cpp:353-358), each with the SELL slots of the
+//    element's vertices inside the vertex's row.  Assembly is row-centric:
+//    one thread owns one row, recomputes each incident element and
+//    accumulates only its own row -- no atomics, no colouring, deterministic.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace b3g {
+
+constexpr int kMaxSpheres = 4;
+constexpr int kSlice = 32;
+
+// Device scalars of one cloth's step (CG state, reductions, contact flags).
+struct StepScalars {
+    // CG
+    double delta;       // current r.P^-1 r
+    double delta0;
+    double b_delta;
+    double pAp;
+    float alpha, beta;
+    uint32_t iter;
+    uint32_t cont;      // 1 while the CG loop should run another iteration
+    uint32_t status;    // 0 ok, else b3g_status
+    // last-block counters of the grid reductions
+    uint32_t ticket[4];
+    // contacts
+    float min_sep;
+    uint32_t pos_solved;
+    uint32_t active_contacts;
+    uint32_t contacts;
+    // step parameters (written by the host before each step)
+    float dt;
+    uint32_t vel_iters, pos_iters;
+    uint32_t step_index;
+    uint32_t max_iter;
+    int stop_rule;
+    float tol;
+    int dot;
+    float gx, gy, gz;
+};
+
+struct SphereDev {
+    float cx, cy, cz, radius, friction;
+    float lo[3], hi[3];   // fat AABB of the shape proxy
+};
+
+struct ClothDev {
+    uint32_t n, t, ns, nsph;
+    uint32_t nslices, max_deg, E;
+    const uint32_t* slice_off;  // nslices + 1
+    const uint8_t* row_deg;     // n
+    const uint32_t* cols;       // E
+    float* vals;                // 9 E
+
+    const uint32_t* inc_ptr;    // n + 1
+    const uint32_t* inc_elem;   // bit 31 set: spring id, else triangle id
+    const uint32_t* inc_meta;   // corner/end (bits 0-1), slots of element vertices (8 bits each from bit 8)
+
+    const uint4* tri;           // v1, v2, v3, 0
+    const float4* tri_rest;     // du1, dv1, du2, dv2
+    const float2* tri_rest2;    // inv_det, alpha
+    const uint2* spr;           // p1, p2 (vertex ids)
+    const float4* spr_par;      // L0, ks, kd, 0
+
+    float k_stretch, k_shear, k_damp;
+    float thickness, friction;  // particle radius and friction (b3ClothDef)
+
+    float *x, *v, *fext, *y, *mx;
+    const float* mass;
+    uint8_t* type;
+    float *b, *dv, *r, *p, *s, *pinv;
+    float *fat_lo, *fat_hi;
+
+    // contacts, [sphere][vertex]
+    uint8_t* c_exists;
+    uint8_t* c_active;
+    uint32_t* c_key;            // creation key: step index * kMaxSpheres + sphere
+    float* c_normal;            // 3 planes of nsph * n
+    float* c_t1;
+    float* c_t2;
+    float* c_imp;               // normal, tangent x, tangent y
+    SphereDev sph[kMaxSpheres];
+
+    StepScalars* sc;
+    void* partials;             // reduction partials, >= grid blocks * 16 bytes
+    uint32_t grid;              // blocks of the row kernels
+    uint32_t block;             // threads of the row kernels
+};
+
+// Host launchers (cloth_kernels.cu).  The assembly kernel needs
+// assemble_smem_bytes() of dynamic shared memory.
+size_t assemble_smem_bytes(const ClothDev& c, int block);
+cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st);
+cudaError_t launch_assemble(const ClothDev& c, int block, cudaStream_t st);
+// CG kernels: when use_graph is set, the reduction tail of init/update sets
+// the while-node condition `cond`; otherwise every iteration kernel returns
+// early once the device flag StepScalars::cont is 0.
+cudaError_t launch_cg_init(const ClothDev& c, int dot, cudaGraphConditionalHandle cond, int use_graph,
+                           cudaStream_t st);
+cudaError_t launch_cg_iteration(const ClothDev& c, int dot, cudaGraphConditionalHandle cond, int use_graph,
+                                cudaStream_t st);
+// The three kernels of one CG iteration, one at a time (profiling).
+cudaError_t launch_cg_part(const ClothDev& c, int dot, int part, cudaStream_t st);
+cudaError_t launch_finalize(const ClothDev& c, cudaStream_t st);
+cudaError_t launch_contact_position(const ClothDev& c, cudaStream_t st);
+cudaError_t launch_post(const ClothDev& c, cudaStream_t st);
+
+// Sequential particle edits (set type / position / velocity, apply force /
+// translation) in call order, and whole-cloth array forms.
+struct ParticleOp {
+    uint32_t vertex, kind;
+    float a[3];
+};
+enum { OP_SET_TYPE = 0, OP_SET_POSITION = 1, OP_SET_VELOCITY = 2, OP_APPLY_FORCE = 3, OP_APPLY_TRANSLATION = 4 };
+cudaError_t launch_particle_ops(const ClothDev& c, const ParticleOp* ops, uint32_t count, cudaStream_t st);
+cudaError_t launch_set_types(const ClothDev& c, const uint8_t* types, cudaStream_t st);
+cudaError_t launch_add_vectors(const ClothDev& c, float* dst_planes, const float* src_xyz, int only_dynamic,
+                               cudaStream_t st);
+cudaError_t launch_clear_contacts(const ClothDev& c, cudaStream_t st);
+
+uint64_t kernel_launches();
+void count_launches(uint64_t k);
+
+}  // namespace b3g

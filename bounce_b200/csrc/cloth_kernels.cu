@@ -1,0 +1,1136 @@
+// Kernels of one implicit cloth step (single cloth, whole GPU).
+//
+//   contacts_update  b3ClothContactManager::UpdateBodyContacts
+//                    (src/bounce/cloth/cloth_contact_manager.cpp:277-315)
+//   assemble         forces + Jacobians + A, b, P^-1
+//                    (src/bounce/cloth/cloth_force_solver.cpp:164-204,
+//                     src/bounce/cloth/forces/{strech,shear,spring}_force.cpp)
+//   cg_*             b3SolveMPCG (cloth_force_solver.cpp:61-136)
+//   finalize         v += dv, x += y, contact warm start / velocity
+//                    iterations / x += h v / first position iteration
+//                    (cloth_force_solver.cpp:211-222, cloth_solver.cpp:95-164,
+//                     contacts/cloth_contact_solver.cpp body functions)
+//   contact_position later position iterations with the global early out
+//   post             clear f and y, particle AABB sync, new body contacts
+//                    (cloth.cpp:564-577, cloth_contact_manager.cpp:64-123)
+//
+// Everything is compiled with -fmad=false so element arithmetic matches the
+// CPU reference operation for operation.  Grid reductions are deterministic:
+// every block writes one partial, the last block to arrive (ticket counter)
+// sums the partials in index order.
+#include <atomic>
+#include <cfloat>
+#include <cstdio>
+
+#include "cloth_dev.cuh"
+#include "vec.cuh"
+
+namespace b3g {
+
+static std::atomic<uint64_t> g_launches{0};
+uint64_t kernel_launches() { return g_launches.load(); }
+void count_launches(uint64_t k) { g_launches += k; }
+
+namespace {
+
+constexpr float kEps = FLT_EPSILON;              // B3_EPSILON
+constexpr float kAabbExtension = 0.2f;           // B3_AABB_EXTENSION
+constexpr float kAabbMultiplier = 2.0f;          // B3_AABB_MULTIPLIER
+constexpr float kLinearSlop = 0.005f;            // B3_LINEAR_SLOP
+constexpr float kMaxLinearCorrection = 0.2f;     // B3_MAX_LINEAR_CORRECTION
+constexpr float kBaumgarte = 0.1f;               // B3_BAUMGARTE
+constexpr int kStatusNumerical = 6;
+
+// ---------------------------------------------------------------------------
+// reductions
+// ---------------------------------------------------------------------------
+
+// A partial sum in one of the three dot precisions.
+struct CompF {
+    float s, c;
+};
+
+template <int DOT> struct DotT;
+template <> struct DotT<0> {
+    typedef float T;
+    static __device__ T zero() { return 0.0f; }
+    static __device__ T add_term(T a, f3 x, f3 y) { return a + dot(x, y); }
+    static __device__ T combine(T a, T b) { return a + b; }
+    static __device__ double value(T a) { return (double)a; }
+    static __device__ T shfl(T a, int off) { return __shfl_down_sync(0xffffffffu, a, off); }
+    static __device__ T load(const T* p) { return __ldcg(p); }
+};
+template <> struct DotT<1> {
+    typedef CompF T;
+    static __device__ T zero() { return CompF{0.0f, 0.0f}; }
+    // Neumaier step over the per-row terms
+    static __device__ T add_term(T a, f3 x, f3 y)
+    {
+        float term = dot(x, y);
+        float t = a.s + term;
+        if (fabsf(a.s) >= fabsf(term)) a.c += (a.s - t) + term;
+        else a.c += (term - t) + a.s;
+        a.s = t;
+        return a;
+    }
+    // TwoSum of the running sums, compensations added
+    static __device__ T combine(T a, T b)
+    {
+        float s = a.s + b.s;
+        float bp = s - a.s;
+        float err = (a.s - (s - bp)) + (b.s - bp);
+        return CompF{s, (a.c + b.c) + err};
+    }
+    static __device__ double value(T a) { return (double)(a.s + a.c); }
+    static __device__ T shfl(T a, int off)
+    {
+        return CompF{__shfl_down_sync(0xffffffffu, a.s, off), __shfl_down_sync(0xffffffffu, a.c, off)};
+    }
+    static __device__ T load(const T* p) { return CompF{__ldcg(&p->s), __ldcg(&p->c)}; }
+};
+template <> struct DotT<2> {
+    typedef double T;
+    static __device__ T zero() { return 0.0; }
+    static __device__ T add_term(T a, f3 x, f3 y)
+    {
+        return a + ((double)x.x * (double)y.x + (double)x.y * (double)y.y + (double)x.z * (double)y.z);
+    }
+    static __device__ T combine(T a, T b) { return a + b; }
+    static __device__ double value(T a) { return a; }
+    static __device__ T shfl(T a, int off) { return __shfl_down_sync(0xffffffffu, a, off); }
+    static __device__ T load(const T* p) { return __ldcg(p); }
+};
+
+// Block-wide reduction of NV values; result valid in thread 0.
+template <int DOT, int NV>
+__device__ void block_reduce(typename DotT<DOT>::T (&v)[NV])
+{
+    typedef DotT<DOT> D;
+    typedef typename D::T T;
+    __shared__ T sh[NV][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int off = 16; off > 0; off >>= 1) v[k] = D::combine(v[k], D::shfl(v[k], off));
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k][warp] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            v[k] = lane < nwarps ? sh[k][lane] : D::zero();
+            for (int off = 16; off > 0; off >>= 1) v[k] = D::combine(v[k], D::shfl(v[k], off));
+        }
+    }
+    __syncthreads();
+}
+
+// Writes this block's partials; returns true (in every thread) in the last
+// block to arrive, after which `v` holds the grid totals in thread 0.
+template <int DOT, int NV>
+__device__ bool grid_reduce(typename DotT<DOT>::T (&v)[NV], void* partials, uint32_t* ticket)
+{
+    typedef DotT<DOT> D;
+    typedef typename D::T T;
+    __shared__ bool last;
+    block_reduce<DOT, NV>(v);
+    T* part = reinterpret_cast<T*>(partials);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) part[blockIdx.x * NV + k] = v[k];
+        __threadfence();
+        unsigned t = atomicAdd(ticket, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    T acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = D::zero();
+    for (uint32_t bi = threadIdx.x; bi < gridDim.x; bi += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] = D::combine(acc[k], D::load(part + bi * NV + k));
+    block_reduce<DOT, NV>(acc);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = acc[k];
+    if (threadIdx.x == 0) *ticket = 0u;
+    return true;
+}
+
+// CG stop rule (cloth_force_solver.cpp:105-113, or the relative tolerance)
+__device__ bool cg_stop(const StepScalars* sc, double delta, double b_delta)
+{
+    if (sc->stop_rule == 0) {
+        if (sc->dot == 2) return delta <= (double)(kEps * kEps) * b_delta;
+        return (float)delta <= kEps * kEps * (float)b_delta;
+    }
+    return delta <= (double)sc->tol * (double)sc->tol * b_delta;
+}
+
+// ---------------------------------------------------------------------------
+// SELL access
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t row_base(const ClothDev& c, uint32_t row)
+{
+    return c.slice_off[row >> 5] + (row & 31u);
+}
+
+__device__ __forceinline__ m3 load_block(const ClothDev& c, uint32_t idx)
+{
+    const float* v = c.vals;
+    const uint32_t E = c.E;
+    return m3{f3{v[idx], v[E + idx], v[2 * E + idx]}, f3{v[3 * E + idx], v[4 * E + idx], v[5 * E + idx]},
+              f3{v[6 * E + idx], v[7 * E + idx], v[8 * E + idx]}};
+}
+
+__device__ __forceinline__ void store_block(const ClothDev& c, uint32_t idx, const m3& m)
+{
+    float* v = c.vals;
+    const uint32_t E = c.E;
+    v[idx] = m.x.x; v[E + idx] = m.x.y; v[2 * E + idx] = m.x.z;
+    v[3 * E + idx] = m.y.x; v[4 * E + idx] = m.y.y; v[5 * E + idx] = m.y.z;
+    v[6 * E + idx] = m.z.x; v[7 * E + idx] = m.z.y; v[8 * E + idx] = m.z.z;
+}
+
+// (A q)_row for a vector q given as 3 planes.
+__device__ __forceinline__ f3 spmv_row(const ClothDev& c, uint32_t row, const float* q)
+{
+    const uint32_t base = row_base(c, row);
+    const uint32_t deg = c.row_deg[row];
+    f3 acc = zero3();
+    for (uint32_t k = 0; k < deg; ++k) {
+        const uint32_t idx = base + 32u * k;
+        const uint32_t col = c.cols[idx];
+        acc = acc + load_block(c, idx) * ld3(q, c.n, col);
+    }
+    return acc;
+}
+
+__device__ __forceinline__ bool is_dynamic(const ClothDev& c, uint32_t i) { return c.type[i] == 2; }
+
+// ---------------------------------------------------------------------------
+// assembly
+// ---------------------------------------------------------------------------
+
+// Per-thread accumulators for one row in shared memory, laid out
+// [(slot * 18 + component) * B + thread] so that lanes never conflict.
+struct RowAcc {
+    float* base;
+    uint8_t* touch;   // dfdx first-touch order, [k * B + thread]
+    int B, tid;
+    uint64_t touched;
+    int ntouch;
+
+    __device__ void clear(int deg)
+    {
+        for (int k = 0; k < deg; ++k)
+            for (int q = 0; q < 18; ++q) base[(k * 18 + q) * B + tid] = 0.0f;
+        touched = 0ull;
+        ntouch = 0;
+    }
+    __device__ void addK(int slot, const m3& m)
+    {
+        if (!(touched & (1ull << slot))) {
+            touched |= 1ull << slot;
+            touch[ntouch * B + tid] = (uint8_t)slot;
+            ++ntouch;
+        }
+        float* p = base + (slot * 18) * B + tid;
+        p[0 * B] += m.x.x; p[1 * B] += m.x.y; p[2 * B] += m.x.z;
+        p[3 * B] += m.y.x; p[4 * B] += m.y.y; p[5 * B] += m.y.z;
+        p[6 * B] += m.z.x; p[7 * B] += m.z.y; p[8 * B] += m.z.z;
+    }
+    __device__ void addD(int slot, const m3& m)
+    {
+        float* p = base + (slot * 18 + 9) * B + tid;
+        p[0 * B] += m.x.x; p[1 * B] += m.x.y; p[2 * B] += m.x.z;
+        p[3 * B] += m.y.x; p[4 * B] += m.y.y; p[5 * B] += m.y.z;
+        p[6 * B] += m.z.x; p[7 * B] += m.z.y; p[8 * B] += m.z.z;
+    }
+    __device__ m3 getK(int slot) const
+    {
+        const float* p = base + (slot * 18) * B + tid;
+        return m3{f3{p[0], p[B], p[2 * B]}, f3{p[3 * B], p[4 * B], p[5 * B]}, f3{p[6 * B], p[7 * B], p[8 * B]}};
+    }
+    __device__ m3 getD(int slot) const
+    {
+        const float* p = base + (slot * 18 + 9) * B + tid;
+        return m3{f3{p[0], p[B], p[2 * B]}, f3{p[3 * B], p[4 * B], p[5 * B]}, f3{p[6 * B], p[7 * B], p[8 * B]}};
+    }
+};
+
+// b3SpringForce::Apply (spring_force.cpp:53-120) restricted to one end.
+__device__ void spring_row(const ClothDev& c, RowAcc& acc, uint32_t sid, int end, int slot_self, int slot_other,
+                           f3& f_row)
+{
+    const uint2 pr = c.spr[sid];
+    const float4 par = c.spr_par[sid];
+    const float L0 = par.x, ks = par.y, kd = par.z;
+    const uint32_t n = c.n;
+    const f3 x1 = ld3(c.x, n, pr.x), x2 = ld3(c.x, n, pr.y);
+    const f3 v1 = ld3(c.v, n, pr.x), v2 = ld3(c.v, n, pr.y);
+    const m3 I = mident();
+    f3 mf = zero3();
+    if (ks > 0.0f) {
+        const f3 dx = x1 - x2;
+        const float L = length(dx);
+        if (L > L0) {
+            const f3 dCdx = dx / L;
+            mf = mf + (-ks * (L - L0)) * dCdx;
+            const m3 K11 = -ks * (outer(dx, dx) + (1.0f - L0 / L) * (I - outer(dx, dx)));
+            const m3 K12 = -1.0f * K11;
+            if (end == 0) {
+                acc.addK(slot_self, K11);
+                acc.addK(slot_other, K12);
+            } else {
+                acc.addK(slot_other, K12);
+                acc.addK(slot_self, K11);
+            }
+        }
+    }
+    if (kd > 0.0f) {
+        const f3 dv = v1 - v2;
+        mf = mf + (-kd) * dv;
+        const m3 K11 = -kd * I;
+        const m3 K12 = -1.0f * K11;
+        acc.addD(slot_self, K11);
+        acc.addD(slot_other, K12);
+    }
+    f_row = end == 0 ? f_row + mf : f_row - mf;
+}
+
+// b3ShearForce::Apply then b3StrechForce::Apply (the force list holds the
+// shear element of a triangle before its stretch element) for corner `cn`.
+__device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn, const int slot[3], f3& f_row)
+{
+    const uint4 tv = c.tri[t];
+    const float4 rs = c.tri_rest[t];
+    const float2 rs2 = c.tri_rest2[t];
+    const float du1 = rs.x, dv1 = rs.y, du2 = rs.z, dv2 = rs.w, inv_det = rs2.x, alpha = rs2.y;
+    const uint32_t n = c.n;
+    const f3 x1 = ld3(c.x, n, tv.x), x2 = ld3(c.x, n, tv.y), x3 = ld3(c.x, n, tv.z);
+    const f3 vs[3] = {ld3(c.v, n, tv.x), ld3(c.v, n, tv.y), ld3(c.v, n, tv.z)};
+    const f3 dx1 = x2 - x1, dx2 = x3 - x1;
+    const f3 wu = inv_det * (dv2 * dx1 - dv1 * dx2);
+    const f3 wv = inv_det * ((-du2) * dx1 + du1 * dx2);
+    const float dwudx[3] = {inv_det * (dv1 - dv2), inv_det * dv2, -inv_det * dv1};
+    const float dwvdx[3] = {inv_det * (du2 - du1), -inv_det * du2, inv_det * du1};
+    const float kd = c.k_damp;
+
+    if (c.k_shear > 0.0f) {  // shear_force.cpp:57-212
+        const float ks = c.k_shear;
+        f3 dC[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) dC[i] = alpha * (dwudx[i] * wv + dwvdx[i] * wu);
+        f3 fe = zero3();
+        if (ks > 0.0f) {
+            const float C = alpha * dot(wu, wv);
+            fe = fe + (-ks * C) * dC[cn];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc.addK(slot[j], -ks * outer(dC[cn], dC[j]));
+        }
+        if (kd > 0.0f) {
+            float dCdt = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) dCdt += dot(dC[i], vs[i]);
+            fe = fe + (-kd * dCdt) * dC[cn];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc.addD(slot[j], -kd * outer(dC[cn], dC[j]));
+        }
+        f_row = f_row + fe;
+    }
+    if (c.k_stretch > 0.0f) {  // strech_force.cpp:59-329, bu = bv = 1 (cloth.cpp:198-199)
+        const float ks = c.k_stretch;
+        const float len_wu = length(wu);
+        const float len_wv = length(wv);
+        const m3 I = mident();
+        f3 fe = zero3();
+#pragma unroll
+        for (int d = 0; d < 2; ++d) {
+            const f3 w = d == 0 ? wu : wv;
+            const float len = d == 0 ? len_wu : len_wv;
+            const float* dw = d == 0 ? dwudx : dwvdx;
+            if (!(len > 0.0f)) continue;
+            const float inv_len = 1.0f / len;
+            const f3 nw = inv_len * w;
+            f3 dC[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) dC[i] = (alpha * dw[i]) * nw;
+            if (ks > 0.0f && len > 1.0f) {
+                const float C = alpha * (len - 1.0f);
+                fe = fe + (-ks * C) * dC[cn];
+                const m3 P = I - outer(nw, nw);
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const m3 d2 = (alpha * inv_len * dw[cn] * dw[j]) * P;
+                    acc.addK(slot[j], -ks * (outer(dC[cn], dC[j]) + C * d2));
+                }
+            }
+            if (kd > 0.0f) {
+                float dCdt = 0.0f;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) dCdt += dot(dC[i], vs[i]);
+                fe = fe + (-kd * dCdt) * dC[cn];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) acc.addD(slot[j], -kd * outer(dC[cn], dC[j]));
+            }
+        }
+        f_row = f_row + fe;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_assemble(ClothDev c)
+{
+    extern __shared__ float smem[];
+    const int B = blockDim.x, tid = threadIdx.x;
+    const uint32_t row = blockIdx.x * B + tid;
+    if (row >= c.n) return;
+    const StepScalars* sc = c.sc;
+    const float h = sc->dt;
+    const float hh = h * h;
+    const uint32_t n = c.n;
+
+    RowAcc acc;
+    acc.base = smem;
+    acc.touch = reinterpret_cast<uint8_t*>(smem + (size_t)c.max_deg * 18 * B);
+    acc.B = B;
+    acc.tid = tid;
+    const int deg = c.row_deg[row];
+    acc.clear(deg);
+
+    // sf = f_ext (+ m g for dynamic particles), cloth_force_solver.cpp:172-180
+    f3 f = ld3(c.fext, n, row);
+    const float m = c.mass[row];
+    const bool dyn = is_dynamic(c, row);
+    if (dyn) f = f + m * mk(sc->gx, sc->gy, sc->gz);
+
+    for (uint32_t e = c.inc_ptr[row]; e < c.inc_ptr[row + 1]; ++e) {
+        const uint32_t el = c.inc_elem[e];
+        const uint32_t meta = c.inc_meta[e];
+        const int cn = meta & 3u;
+        const int s0 = (meta >> 8) & 0xffu, s1 = (meta >> 16) & 0xffu, s2 = (meta >> 24) & 0xffu;
+        if (el & 0x80000000u) {
+            // springs: slot of p1 in s0, of p2 in s1; cn = end
+            spring_row(c, acc, el & 0x7fffffffu, cn, cn == 0 ? s0 : s1, cn == 0 ? s1 : s0, f);
+        } else {
+            const int slots[3] = {s0, s1, s2};
+            triangle_row(c, acc, el, cn, slots, f);
+        }
+    }
+
+    // A = (M - h dfdv) - h^2 dfdx, one row (cloth_force_solver.cpp:198)
+    const uint32_t base = row_base(c, row);
+    m3 diag = mzero();
+    for (int k = 0; k < deg; ++k) {
+        const m3 M = k == 0 ? m3{f3{m, 0.0f, 0.0f}, f3{0.0f, m, 0.0f}, f3{0.0f, 0.0f, m}} : mzero();
+        const m3 a = (M - h * acc.getD(k)) - hh * acc.getK(k);
+        if (k == 0) diag = a;
+        store_block(c, base + 32u * k, a);
+    }
+    // Jacobi preconditioner (cloth_force_solver.cpp:70-88)
+    st3(c.pinv, n, row, mk(1.0f / diag.x.x, 1.0f / diag.y.y, 1.0f / diag.z.z));
+
+    // b = h (f + h dfdx v + dfdx y), dfdx summed in its row-list order
+    // (reverse first touch, sparse_mat33.h:264-282)
+    f3 t1 = zero3(), t2 = zero3();
+    for (int q = acc.ntouch - 1; q >= 0; --q) {
+        const int k = acc.touch[q * B + tid];
+        const uint32_t col = c.cols[base + 32u * k];
+        const m3 K = acc.getK(k);
+        t1 = t1 + K * ld3(c.v, n, col);
+    }
+    for (int q = acc.ntouch - 1; q >= 0; --q) {
+        const int k = acc.touch[q * B + tid];
+        const uint32_t col = c.cols[base + 32u * k];
+        const m3 K = acc.getK(k);
+        t2 = t2 + K * ld3(c.y, n, col);
+    }
+    st3(c.b, n, row, h * ((f + h * t1) + t2));
+}
+
+// ---------------------------------------------------------------------------
+// MPCG
+// ---------------------------------------------------------------------------
+
+// x0 = S m_x; r = S (b - A x0); p = S P^-1 r; b_delta, delta
+// (cloth_force_solver.cpp:90-100)
+template <int DOT>
+__global__ void k_cg_init(ClothDev c, cudaGraphConditionalHandle cond, int use_graph)
+{
+    typedef DotT<DOT> D;
+    typename D::T v[2] = {D::zero(), D::zero()};
+    const uint32_t n = c.n;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+        const bool Si = is_dynamic(c, row);
+        // A x0 with x0_j = S_j m_x_j gathered on the fly
+        const uint32_t base = row_base(c, row);
+        const uint32_t deg = c.row_deg[row];
+        f3 ax = zero3();
+        for (uint32_t k = 0; k < deg; ++k) {
+            const uint32_t idx = base + 32u * k;
+            const uint32_t col = c.cols[idx];
+            const f3 xj = is_dynamic(c, col) ? ld3(c.mx, n, col) : zero3();
+            ax = ax + load_block(c, idx) * xj;
+        }
+        const f3 bi = ld3(c.b, n, row);
+        const f3 pv = ld3(c.pinv, n, row);
+        const f3 x0 = Si ? ld3(c.mx, n, row) : zero3();
+        const f3 r = Si ? bi - ax : zero3();
+        const f3 p = Si ? mk(r.x * pv.x, r.y * pv.y, r.z * pv.z) : zero3();
+        const f3 bh = Si ? bi : zero3();
+        st3(c.dv, n, row, x0);
+        st3(c.r, n, row, r);
+        st3(c.p, n, row, p);
+        v[0] = D::add_term(v[0], bh, mk(bh.x * pv.x, bh.y * pv.y, bh.z * pv.z));
+        v[1] = D::add_term(v[1], r, p);
+    }
+    if (grid_reduce<DOT, 2>(v, c.partials, &c.sc->ticket[0]) && threadIdx.x == 0) {
+        StepScalars* sc = c.sc;
+        double bd = D::value(v[0]), dl = D::value(v[1]);
+        if (DOT != 2) {
+            bd = (double)(float)bd;
+            dl = (double)(float)dl;
+        }
+        sc->b_delta = bd;
+        sc->delta = dl;
+        sc->delta0 = dl;
+        sc->iter = 0;
+        sc->status = 0;
+        uint32_t cont = (sc->max_iter > 0 && !cg_stop(sc, dl, bd)) ? 1u : 0u;
+        if (!isfinite(dl) || !isfinite(bd)) {
+            sc->status = kStatusNumerical;
+            cont = 0;
+        }
+        sc->cont = cont;
+        if (use_graph) cudaGraphSetConditional(cond, cont);
+    }
+}
+
+// s = S A p, alpha = delta / p.s (cloth_force_solver.cpp:115-117)
+template <int DOT>
+__global__ void k_cg_spmv(ClothDev c)
+{
+    typedef DotT<DOT> D;
+    if (c.sc->cont == 0u) return;
+    typename D::T v[1] = {D::zero()};
+    const uint32_t n = c.n;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+        const f3 ap = spmv_row(c, row, c.p);
+        const f3 s = is_dynamic(c, row) ? ap : zero3();
+        st3(c.s, n, row, s);
+        v[0] = D::add_term(v[0], ld3(c.p, n, row), s);
+    }
+    if (grid_reduce<DOT, 1>(v, c.partials, &c.sc->ticket[1]) && threadIdx.x == 0) {
+        StepScalars* sc = c.sc;
+        const double pAp = D::value(v[0]);
+        sc->pAp = pAp;
+        float alpha;
+        if (DOT == 2) alpha = (float)(sc->delta / pAp);
+        else alpha = (float)sc->delta / (float)pAp;
+        sc->alpha = alpha;
+    }
+}
+
+// x += alpha p; r -= alpha s; h = P^-1 r; delta' = r.h; beta
+// (cloth_force_solver.cpp:119-128); sets the loop condition.
+template <int DOT>
+__global__ void k_cg_update(ClothDev c, cudaGraphConditionalHandle cond, int use_graph)
+{
+    typedef DotT<DOT> D;
+    if (c.sc->cont == 0u) return;
+    typename D::T v[1] = {D::zero()};
+    const uint32_t n = c.n;
+    const float alpha = c.sc->alpha;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+        const f3 p = ld3(c.p, n, row);
+        const f3 s = ld3(c.s, n, row);
+        const f3 x = ld3(c.dv, n, row) + alpha * p;
+        const f3 r = ld3(c.r, n, row) - alpha * s;
+        const f3 pv = ld3(c.pinv, n, row);
+        const f3 hv = mk(r.x * pv.x, r.y * pv.y, r.z * pv.z);
+        st3(c.dv, n, row, x);
+        st3(c.r, n, row, r);
+        v[0] = D::add_term(v[0], r, hv);
+    }
+    if (grid_reduce<DOT, 1>(v, c.partials, &c.sc->ticket[2]) && threadIdx.x == 0) {
+        StepScalars* sc = c.sc;
+        double dn = D::value(v[0]);
+        const double dold = sc->delta;
+        float beta;
+        if (DOT == 2) {
+            beta = (float)(dn / dold);
+        } else {
+            dn = (double)(float)dn;
+            beta = (float)dn / (float)dold;
+        }
+        sc->delta = dn;
+        sc->beta = beta;
+        sc->iter += 1;
+        uint32_t cont = (sc->iter < sc->max_iter && !cg_stop(sc, dn, sc->b_delta)) ? 1u : 0u;
+        if (!isfinite(dn) || !isfinite(sc->alpha) || !isfinite(beta)) {
+            sc->status = kStatusNumerical;
+            cont = 0;
+        }
+        sc->cont = cont;
+        if (use_graph) cudaGraphSetConditional(cond, cont);
+    }
+}
+
+// p = S (P^-1 r + beta p) (cloth_force_solver.cpp:130)
+__global__ void k_cg_direction(ClothDev c)
+{
+    if (c.sc->cont == 0u) return;
+    const uint32_t n = c.n;
+    const float beta = c.sc->beta;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+        const f3 r = ld3(c.r, n, row);
+        const f3 pv = ld3(c.pinv, n, row);
+        const f3 hv = mk(r.x * pv.x, r.y * pv.y, r.z * pv.z);
+        const f3 p = is_dynamic(c, row) ? hv + beta * ld3(c.p, n, row) : zero3();
+        st3(c.p, n, row, p);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// contacts
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ bool overlap(const float* lo, const float* hi, const SphereDev& s)
+{
+    // b3TestOverlap (include/bounce/collision/shapes/aabb3.h:247-251)
+    return lo[0] <= s.hi[0] && lo[1] <= s.hi[1] && lo[2] <= s.hi[2] && hi[0] >= s.lo[0] && hi[1] >= s.lo[1] &&
+           hi[2] >= s.lo[2];
+}
+
+__device__ __forceinline__ void load_fat(const ClothDev& c, uint32_t i, float* lo, float* hi)
+{
+    const uint32_t n = c.n;
+    lo[0] = c.fat_lo[i]; lo[1] = c.fat_lo[n + i]; lo[2] = c.fat_lo[2 * n + i];
+    hi[0] = c.fat_hi[i]; hi[1] = c.fat_hi[n + i]; hi[2] = c.fat_hi[2 * n + i];
+}
+
+// UpdateBodyContacts + b3ParticleBodyContact::Update with TestSphere
+// (cloth_contact_manager.cpp:277-315, cloth_particle_body_contact.cpp:24-47,
+// sphere_shape.cpp:71-95)
+__global__ void k_contacts_update(ClothDev c)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const uint32_t n = c.n, nn = c.nsph * n;
+    float lo[3], hi[3];
+    load_fat(c, i, lo, hi);
+    const f3 xi = ld3(c.x, n, i);
+    for (uint32_t s = 0; s < c.nsph; ++s) {
+        const uint32_t q = s * n + i;
+        if (!c.c_exists[q]) continue;
+        const SphereDev& sp = c.sph[s];
+        if (!is_dynamic(c, i) || !overlap(lo, hi, sp)) {
+            c.c_exists[q] = 0;
+            c.c_active[q] = 0;
+            continue;
+        }
+        const float radius = sp.radius + c.thickness;
+        const float rr = radius * radius;
+        const f3 d = xi - mk(sp.cx, sp.cy, sp.cz);
+        const float dd = dot(d, d);
+        if (!(dd <= rr)) {
+            c.c_active[q] = 0;
+            continue;
+        }
+        const float d_len = sqrtf(dd);
+        f3 normal = mk(0.0f, 1.0f, 0.0f);
+        if (d_len > kEps) normal = d / d_len;
+        const f3 n1 = mk(-normal.x, -normal.y, -normal.z);
+        const f3 t1 = perp(n1);
+        const f3 t2 = cross(t1, n1);
+        c.c_active[q] = 1;
+        st3(c.c_normal, nn, q, n1);
+        st3(c.c_t1, nn, q, t1);
+        st3(c.c_t2, nn, q, t2);
+    }
+}
+
+// Active contacts of vertex i in list order (newest first).
+__device__ int contact_order(const ClothDev& c, uint32_t i, int* order)
+{
+    int k = 0;
+    const uint32_t n = c.n;
+    for (uint32_t s = 0; s < c.nsph; ++s) {
+        const uint32_t q = s * n + i;
+        if (c.c_exists[q] && c.c_active[q]) order[k++] = (int)s;
+    }
+    // insertion sort by descending creation key
+    for (int a = 1; a < k; ++a) {
+        int v = order[a];
+        int b = a - 1;
+        while (b >= 0 && c.c_key[order[b] * n + i] < c.c_key[v * n + i]) {
+            order[b + 1] = order[b];
+            --b;
+        }
+        order[b + 1] = v;
+    }
+    return k;
+}
+
+// One position iteration for vertex i; returns its smallest separation
+// (cloth_contact_solver.cpp:620-718).
+__device__ float position_iteration(const ClothDev& c, uint32_t i, f3& pos, const int* order, int k)
+{
+    const uint32_t n = c.n, nn = c.nsph * n;
+    const float mA = 1.0f / c.mass[i];
+    float min_sep = 0.0f;
+    for (int a = 0; a < k; ++a) {
+        const int s = order[a];
+        const SphereDev& sp = c.sph[s];
+        const f3 nA = ld3(c.c_normal, nn, s * n + i);
+        const f3 cB = mk(sp.cx, sp.cy, sp.cz);
+        const float separation = dot(cB - pos, nA) - c.thickness - sp.radius;
+        min_sep = min_sep < separation ? min_sep : separation;
+        const float Cv = kBaumgarte * (separation + kLinearSlop);
+        float C = Cv < 0.0f ? Cv : 0.0f;
+        C = -kMaxLinearCorrection > C ? -kMaxLinearCorrection : C;
+        const float K = mA + 0.0f + 0.0f + 0.0f;
+        const float impulse = K > 0.0f ? -C / K : 0.0f;
+        const f3 P = impulse * nA;
+        pos = pos - mA * P;
+    }
+    return min_sep;
+}
+
+__device__ void min_reduce_flag(const ClothDev& c, float local_min, uint32_t active)
+{
+    __shared__ float smin[32];
+    __shared__ uint32_t scnt[32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int off = 16; off > 0; off >>= 1) {
+        local_min = fminf(local_min, __shfl_down_sync(0xffffffffu, local_min, off));
+        active += __shfl_down_sync(0xffffffffu, active, off);
+    }
+    if (lane == 0) {
+        smin[warp] = local_min;
+        scnt[warp] = active;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float m = 0.0f;
+        uint32_t a = 0;
+        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) {
+            m = fminf(m, smin[w]);
+            a += scnt[w];
+        }
+        float* part = reinterpret_cast<float*>(c.partials);
+        part[blockIdx.x] = m;
+        if (a) atomicAdd(&c.sc->active_contacts, a);
+        __threadfence();
+        unsigned t = atomicAdd(&c.sc->ticket[3], 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const volatile float* part = reinterpret_cast<const volatile float*>(c.partials);
+        float m = 0.0f;
+        for (uint32_t b = 0; b < gridDim.x; ++b) m = fminf(m, part[b]);
+        c.sc->min_sep = m;
+        // cloth_solver.cpp:151-164: stop once every contact is within 3 slops
+        c.sc->pos_solved = m >= -3.0f * kLinearSlop ? 1u : 0u;
+        c.sc->ticket[3] = 0u;
+    }
+}
+
+// v += dv; x += y; m_x = dv; contact solve (cloth_solver.cpp:95-164)
+__global__ void k_finalize(ClothDev c)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = c.n, nn = c.nsph * n;
+    const StepScalars* sc = c.sc;
+    const float h = sc->dt;
+    float local_min = 0.0f;
+    uint32_t active = 0;
+    if (i < n) {
+        const f3 dv = ld3(c.dv, n, i);
+        f3 vel = ld3(c.v, n, i) + dv;
+        f3 pos = ld3(c.x, n, i) + ld3(c.y, n, i);
+        st3(c.mx, n, i, dv);
+        int order[kMaxSpheres];
+        const int k = c.nsph ? contact_order(c, i, order) : 0;
+        active = (uint32_t)k;
+        if (k > 0) {
+            const float mA = 1.0f / c.mass[i];
+            // InitializeBodyContactConstraints (cloth_contact_solver.cpp:54-177), static body
+            float nmass[kMaxSpheres], tm_xx[kMaxSpheres], tm_xy[kMaxSpheres], tm_yx[kMaxSpheres],
+                tm_yy[kMaxSpheres], fr[kMaxSpheres], ni[kMaxSpheres], tix[kMaxSpheres], tiy[kMaxSpheres];
+            for (int a = 0; a < k; ++a) {
+                const int s = order[a];
+                const uint32_t q = s * n + i;
+                const float K = mA + 0.0f + 0.0f + 0.0f;
+                nmass[a] = K > 0.0f ? 1.0f / K : 0.0f;
+                const float k11 = mA + 0.0f + 0.0f + 0.0f, k12 = 0.0f + 0.0f, k22 = mA + 0.0f + 0.0f + 0.0f;
+                float det = k11 * k22 - k12 * k12;
+                if (det != 0.0f) det = 1.0f / det;
+                tm_xx[a] = det * k22;
+                tm_yx[a] = -det * k12;
+                tm_xy[a] = -det * k12;
+                tm_yy[a] = det * k11;
+                fr[a] = sqrtf(c.friction * c.sph[s].friction);
+                ni[a] = c.c_imp[q];
+                tix[a] = c.c_imp[nn + q];
+                tiy[a] = c.c_imp[2 * nn + q];
+            }
+            // WarmStartBodyContactConstraints (:264-307)
+            for (int a = 0; a < k; ++a) {
+                const uint32_t q = order[a] * n + i;
+                const f3 nrm = ld3(c.c_normal, nn, q), t1 = ld3(c.c_t1, nn, q), t2 = ld3(c.c_t2, nn, q);
+                const f3 P = ni[a] * nrm;
+                vel = vel - mA * P;
+                const f3 P1 = tix[a] * t1, P2 = tiy[a] * t2;
+                vel = vel - mA * (P1 + P2);
+            }
+            // SolveBodyContactVelocityConstraints (:388-472)
+            for (uint32_t it = 0; it < sc->vel_iters; ++it) {
+                for (int a = 0; a < k; ++a) {
+                    const uint32_t q = order[a] * n + i;
+                    const f3 nrm = ld3(c.c_normal, nn, q), t1 = ld3(c.c_t1, nn, q), t2 = ld3(c.c_t2, nn, q);
+                    {
+                        const f3 dvv = zero3() - vel;
+                        const float Cdot = dot(nrm, dvv);
+                        float impulse = nmass[a] * (-Cdot + 0.0f);
+                        const float old = ni[a];
+                        const float sum = old + impulse;
+                        ni[a] = sum > 0.0f ? sum : 0.0f;
+                        impulse = ni[a] - old;
+                        const f3 P = impulse * nrm;
+                        vel = vel - mA * P;
+                    }
+                    {
+                        const f3 dvv = zero3() - vel;
+                        const float cx = dot(dvv, t1), cy = dot(dvv, t2);
+                        const float ncx = -cx, ncy = -cy;
+                        const float ix = ncx * tm_xx[a] + ncy * tm_yx[a];
+                        const float iy = ncx * tm_xy[a] + ncy * tm_yy[a];
+                        const float ox = tix[a], oy = tiy[a];
+                        tix[a] += ix;
+                        tiy[a] += iy;
+                        const float maxImpulse = fr[a] * ni[a];
+                        if (tix[a] * tix[a] + tiy[a] * tiy[a] > maxImpulse * maxImpulse) {
+                            const float sl = sqrtf(tix[a] * tix[a] + tiy[a] * tiy[a]);
+                            if (sl > kEps) {
+                                tix[a] /= sl;
+                                tiy[a] /= sl;
+                            }
+                            tix[a] *= maxImpulse;
+                            tiy[a] *= maxImpulse;
+                        }
+                        const float jx = tix[a] - ox, jy = tiy[a] - oy;
+                        const f3 P = jx * t1 + jy * t2;
+                        vel = vel - mA * P;
+                    }
+                }
+            }
+            // StoreImpulses (:598-607)
+            for (int a = 0; a < k; ++a) {
+                const uint32_t q = order[a] * n + i;
+                c.c_imp[q] = ni[a];
+                c.c_imp[nn + q] = tix[a];
+                c.c_imp[2 * nn + q] = tiy[a];
+            }
+        }
+        // integrate positions (cloth_solver.cpp:143-147)
+        pos = pos + h * vel;
+        if (k > 0 && sc->pos_iters > 0) local_min = position_iteration(c, i, pos, order, k);
+        st3(c.x, n, i, pos);
+        st3(c.v, n, i, vel);
+    }
+    if (c.nsph) min_reduce_flag(c, local_min, active);
+}
+
+// A later position iteration, run only while the previous ones left a
+// contact deeper than 3 slops (cloth_solver.cpp:151-164).
+__global__ void k_contact_position(ClothDev c)
+{
+    if (c.sc->pos_solved) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = c.n;
+    float local_min = 0.0f;
+    if (i < n) {
+        int order[kMaxSpheres];
+        const int k = contact_order(c, i, order);
+        if (k > 0) {
+            f3 pos = ld3(c.x, n, i);
+            local_min = position_iteration(c, i, pos, order, k);
+            st3(c.x, n, i, pos);
+        }
+    }
+    min_reduce_flag(c, local_min, 0u);
+}
+
+__device__ void move_proxy_dev(const ClothDev& c, uint32_t i, f3 disp)
+{
+    const uint32_t n = c.n;
+    const f3 x = ld3(c.x, n, i);
+    float lo[3], hi[3];
+    load_fat(c, i, lo, hi);
+    const float r = c.thickness;
+    float tlo[3] = {x.x - r, x.y - r, x.z - r}, thi[3] = {x.x + r, x.y + r, x.z + r};
+    bool contains = true;
+    for (int d = 0; d < 3; ++d)
+        contains = contains && lo[d] <= tlo[d] && tlo[d] <= hi[d] && lo[d] <= thi[d] && thi[d] <= hi[d];
+    if (contains) return;
+    const float dd[3] = {kAabbMultiplier * disp.x, kAabbMultiplier * disp.y, kAabbMultiplier * disp.z};
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = tlo[d] - kAabbExtension;
+        hi[d] = thi[d] + kAabbExtension;
+        if (dd[d] < 0.0f) lo[d] += dd[d];
+        else hi[d] += dd[d];
+    }
+    c.fat_lo[i] = lo[0]; c.fat_lo[n + i] = lo[1]; c.fat_lo[2 * n + i] = lo[2];
+    c.fat_hi[i] = hi[0]; c.fat_hi[n + i] = hi[1]; c.fat_hi[2 * n + i] = hi[2];
+}
+
+// Clear f and y, sync the particle AABB (b3BroadPhase::MoveProxy,
+// broad_phase.cpp:99-149), new body contacts (cloth_contact_manager.cpp:64-123).
+__global__ void k_post(ClothDev c)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = c.n, nn = c.nsph * n;
+    const StepScalars* sc = c.sc;
+    uint32_t alive = 0;
+    if (i < n) {
+        st3(c.fext, n, i, zero3());
+        st3(c.y, n, i, zero3());
+        move_proxy_dev(c, i, sc->dt * ld3(c.v, n, i));
+        float lo[3], hi[3];
+        load_fat(c, i, lo, hi);
+        const bool dyn = is_dynamic(c, i);
+        for (uint32_t s = 0; s < c.nsph; ++s) {
+            const uint32_t q = s * n + i;
+            if (!c.c_exists[q] && dyn && overlap(lo, hi, c.sph[s])) {
+                c.c_exists[q] = 1;
+                c.c_active[q] = 0;
+                c.c_key[q] = sc->step_index * kMaxSpheres + s;
+                c.c_imp[q] = 0.0f;
+                c.c_imp[nn + q] = 0.0f;
+                c.c_imp[2 * nn + q] = 0.0f;
+            }
+            alive += c.c_exists[q];
+        }
+    }
+    if (c.nsph) {
+        for (int off = 16; off > 0; off >>= 1) alive += __shfl_down_sync(0xffffffffu, alive, off);
+        if ((threadIdx.x & 31) == 0 && alive) atomicAdd(&c.sc->contacts, alive);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// particle edits
+// ---------------------------------------------------------------------------
+
+__device__ void destroy_contacts_dev(const ClothDev& c, uint32_t i)
+{
+    for (uint32_t s = 0; s < c.nsph; ++s) {
+        c.c_exists[s * c.n + i] = 0;
+        c.c_active[s * c.n + i] = 0;
+    }
+}
+
+// b3Particle::SetType (particle.cpp:121-143)
+__device__ void set_type_dev(const ClothDev& c, uint32_t i, uint8_t type)
+{
+    const uint32_t n = c.n;
+    if (c.type[i] == type) return;
+    c.type[i] = type;
+    st3(c.fext, n, i, zero3());
+    if (type == 0) {
+        st3(c.v, n, i, zero3());
+        st3(c.y, n, i, zero3());
+        move_proxy_dev(c, i, zero3());
+    }
+    destroy_contacts_dev(c, i);
+}
+
+__global__ void k_particle_ops(ClothDev c, const ParticleOp* ops, uint32_t count)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const uint32_t n = c.n;
+    for (uint32_t k = 0; k < count; ++k) {
+        const ParticleOp op = ops[k];
+        const uint32_t i = op.vertex;
+        if (i >= n) continue;
+        const f3 a = mk(op.a[0], op.a[1], op.a[2]);
+        switch (op.kind) {
+            case OP_SET_TYPE: set_type_dev(c, i, (uint8_t)op.a[0]); break;
+            case OP_SET_POSITION: {  // particle.h:205-214
+                const f3 d = a - ld3(c.x, n, i);
+                st3(c.x, n, i, a);
+                st3(c.y, n, i, zero3());
+                move_proxy_dev(c, i, d);
+                break;
+            }
+            case OP_SET_VELOCITY:  // particle.h:221-228
+                if (c.type[i] != 0) st3(c.v, n, i, a);
+                break;
+            case OP_APPLY_FORCE:  // particle.h:260-267
+                if (c.type[i] == 2) st3(c.fext, n, i, ld3(c.fext, n, i) + a);
+                break;
+            case OP_APPLY_TRANSLATION:  // particle.h:269-272
+                st3(c.y, n, i, ld3(c.y, n, i) + a);
+                break;
+        }
+    }
+}
+
+__global__ void k_set_types(ClothDev c, const uint8_t* types)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < c.n) set_type_dev(c, i, types[i]);
+}
+
+__global__ void k_add_vectors(ClothDev c, float* dst, const float* src, int only_dynamic)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    if (only_dynamic && c.type[i] != 2) return;
+    const f3 a = mk(src[3 * i], src[3 * i + 1], src[3 * i + 2]);
+    st3(dst, c.n, i, ld3(dst, c.n, i) + a);
+}
+
+__global__ void k_clear_contacts(ClothDev c)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < c.n) destroy_contacts_dev(c, i);
+}
+
+inline uint32_t blocks_for(uint32_t n, uint32_t b) { return (n + b - 1) / b; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+size_t assemble_smem_bytes(const ClothDev& c, int block)
+{
+    return (size_t)c.max_deg * 18 * sizeof(float) * block + (size_t)c.max_deg * block;
+}
+
+cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st)
+{
+    if (!c.nsph) return cudaSuccess;
+    k_contacts_update<<<blocks_for(c.n, 256), 256, 0, st>>>(c);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_assemble(const ClothDev& c, int block, cudaStream_t st)
+{
+    const size_t smem = assemble_smem_bytes(c, block);
+    cudaError_t e = cudaFuncSetAttribute(k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_assemble<<<blocks_for(c.n, block), block, smem, st>>>(c);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cg_init(const ClothDev& c, int dot, cudaGraphConditionalHandle cond, int use_graph,
+                           cudaStream_t st)
+{
+    if (dot == 0) k_cg_init<0><<<c.grid, c.block, 0, st>>>(c, cond, use_graph);
+    else if (dot == 1) k_cg_init<1><<<c.grid, c.block, 0, st>>>(c, cond, use_graph);
+    else k_cg_init<2><<<c.grid, c.block, 0, st>>>(c, cond, use_graph);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cg_iteration(const ClothDev& c, int dot, cudaGraphConditionalHandle cond, int use_graph,
+                                cudaStream_t st)
+{
+    if (dot == 0) {
+        k_cg_spmv<0><<<c.grid, c.block, 0, st>>>(c);
+        k_cg_update<0><<<c.grid, c.block, 0, st>>>(c, cond, use_graph);
+    } else if (dot == 1) {
+        k_cg_spmv<1><<<c.grid, c.block, 0, st>>>(c);
+        k_cg_update<1><<<c.grid, c.block, 0, st>>>(c, cond, use_graph);
+    } else {
+        k_cg_spmv<2><<<c.grid, c.block, 0, st>>>(c);
+        k_cg_update<2><<<c.grid, c.block, 0, st>>>(c, cond, use_graph);
+    }
+    k_cg_direction<<<c.grid, c.block, 0, st>>>(c);
+    count_launches(3);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cg_part(const ClothDev& c, int dot, int part, cudaStream_t st)
+{
+    cudaGraphConditionalHandle none = 0;
+    if (part == 0) {
+        if (dot == 0) k_cg_spmv<0><<<c.grid, c.block, 0, st>>>(c);
+        else if (dot == 1) k_cg_spmv<1><<<c.grid, c.block, 0, st>>>(c);
+        else k_cg_spmv<2><<<c.grid, c.block, 0, st>>>(c);
+    } else if (part == 1) {
+        if (dot == 0) k_cg_update<0><<<c.grid, c.block, 0, st>>>(c, none, 0);
+        else if (dot == 1) k_cg_update<1><<<c.grid, c.block, 0, st>>>(c, none, 0);
+        else k_cg_update<2><<<c.grid, c.block, 0, st>>>(c, none, 0);
+    } else {
+        k_cg_direction<<<c.grid, c.block, 0, st>>>(c);
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const ClothDev& c, cudaStream_t st)
+{
+    k_finalize<<<blocks_for(c.n, 256), 256, 0, st>>>(c);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_contact_position(const ClothDev& c, cudaStream_t st)
+{
+    if (!c.nsph) return cudaSuccess;
+    k_contact_position<<<blocks_for(c.n, 256), 256, 0, st>>>(c);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_post(const ClothDev& c, cudaStream_t st)
+{
+    k_post<<<blocks_for(c.n, 256), 256, 0, st>>>(c);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_particle_ops(const ClothDev& c, const ParticleOp* ops, uint32_t count, cudaStream_t st)
+{
+    k_particle_ops<<<1, 32, 0, st>>>(c, ops, count);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_types(const ClothDev& c, const uint8_t* types, cudaStream_t st)
+{
+    k_set_types<<<blocks_for(c.n, 256), 256, 0, st>>>(c, types);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_add_vectors(const ClothDev& c, float* dst, const float* src, int only_dynamic, cudaStream_t st)
+{
+    k_add_vectors<<<blocks_for(c.n, 256), 256, 0, st>>>(c, dst, src, only_dynamic);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_clear_contacts(const ClothDev& c, cudaStream_t st)
+{
+    if (!c.nsph) return cudaSuccess;
+    k_clear_contacts<<<blocks_for(c.n, 256), 256, 0, st>>>(c);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace b3g

@@ -1,0 +1,225 @@
+/*
+ * b3g -- B200-native implicit cloth step with Bounce's b3Cloth semantics.
+ *
+ * C ABI of libb3g.so.  Every call returns a b3g_status; nothing aborts.  A
+ * cloth handle owns its device buffers and one CUDA stream; host pointers are
+ * borrowed for the duration of a call.  Distinct handles may be used from
+ * distinct host threads; one handle is not re-entrant.  There is no CPU
+ * fallback: without a usable CUDA device, b3g_cloth_create returns
+ * B3G_ERR_NO_DEVICE.
+ *
+ * Reference interfaces each entry point replaces are cited as path:line
+ * within the Bounce source tree (Kazade/bounce).
+ */
+#ifndef B3G_H
+#define B3G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    B3G_OK = 0,
+    B3G_ERR_INVALID_ARGUMENT = 1, /* null pointer, index out of range, bad option */
+    B3G_ERR_DEGENERATE_MESH = 2,  /* zero-area triangle, zero-length edge, vertex index out of range */
+    B3G_ERR_NO_DEVICE = 3,        /* no CUDA device / driver */
+    B3G_ERR_OUT_OF_MEMORY = 4,    /* device or host allocation failed */
+    B3G_ERR_CUDA = 5,             /* any other CUDA runtime error */
+    B3G_ERR_NUMERICAL = 6,        /* NaN/Inf in the CG scalars (breakdown) */
+    B3G_ERR_TIMEOUT = 7,          /* a bounded device-side wait gave up */
+    B3G_ERR_CAPACITY = 8,         /* request above a fixed capacity (spheres, batch slots, budget) */
+    B3G_ERR_UNSUPPORTED = 9       /* mesh feature outside what the kernels handle (vertex degree) */
+} b3g_status;
+
+/* b3ParticleType (include/bounce/cloth/particle.h:27-32) */
+typedef enum { B3G_STATIC = 0, B3G_KINEMATIC = 1, B3G_DYNAMIC = 2 } b3g_particle_type;
+
+/* b3ClothMesh (include/bounce/cloth/cloth_mesh.h:43-53): vertices as xyz
+ * triples, triangles as vertex triples, sewing lines as (s1, s2, v1, v2). */
+typedef struct {
+    uint32_t vertex_count;
+    const float* vertices;
+    uint32_t triangle_count;
+    const uint32_t* triangles;
+    uint32_t sewing_line_count;
+    const uint32_t* sewing_lines;
+} b3g_mesh_desc;
+
+/* b3ClothDef (include/bounce/cloth/cloth.h:56-95) */
+typedef struct {
+    float density;
+    float streching;
+    float shearing;
+    float bending;
+    float sewing;
+    float damping;
+    float thickness;
+    float friction;
+} b3g_cloth_def;
+
+/* CG stop rule.  REFERENCE is b3SolveMPCG's own rule
+ * (src/bounce/cloth/cloth_force_solver.cpp:105-113): at most max_iterations
+ * (the reference fixes 20) and delta <= FLT_EPSILON^2 * b_delta.  RELATIVE
+ * stops at sqrt(delta / b_delta) <= tolerance. */
+typedef enum { B3G_STOP_REFERENCE = 0, B3G_STOP_RELATIVE = 1 } b3g_stop_rule;
+
+/* Accumulation of the CG inner products (alpha, beta, residual). */
+typedef enum { B3G_DOT_F32 = 0, B3G_DOT_COMPENSATED = 1, B3G_DOT_F64 = 2 } b3g_dot_mode;
+
+typedef struct {
+    b3g_stop_rule stop_rule;
+    float tolerance;          /* RELATIVE only */
+    uint32_t max_iterations;  /* >= 1 */
+    b3g_dot_mode dot;
+} b3g_solver_opts;
+
+typedef struct {
+    uint32_t iterations;      /* CG iterations of the last step */
+    double delta0;            /* r^T P^-1 r at CG start */
+    double delta;             /* r^T P^-1 r at CG exit */
+    double b_delta;           /* filtered b^T P^-1 b */
+    uint32_t active_contacts; /* body contacts handed to the contact solver */
+    uint32_t contacts;        /* body contacts alive after the step */
+    float step_ms;            /* device time of the step (CUDA events) */
+} b3g_step_stats;
+
+typedef struct b3g_cloth b3g_cloth;
+
+/* ---- cloth lifetime ---------------------------------------------------- */
+
+/* b3Cloth::b3Cloth (src/bounce/cloth/cloth.cpp:96-266): lumped masses,
+ * rest-state triangle frames, one stretch and one shear element per triangle,
+ * a bending spring per edge-adjacent triangle pair, a spring per sewing line.
+ * The mesh is copied; it need not outlive the call. */
+b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, int device,
+                            b3g_cloth** out);
+/* b3Cloth::~b3Cloth (cloth.cpp:268-288) */
+b3g_status b3g_cloth_destroy(b3g_cloth* cloth);
+
+/* ---- configuration ----------------------------------------------------- */
+
+/* b3Cloth::SetGravity / GetGravity (include/bounce/cloth/cloth.h:106-110) */
+b3g_status b3g_cloth_set_gravity(b3g_cloth* cloth, const float gravity[3]);
+b3g_status b3g_cloth_get_gravity(const b3g_cloth* cloth, float gravity[3]);
+b3g_status b3g_cloth_set_solver(b3g_cloth* cloth, const b3g_solver_opts* opts);
+/* A static sphere collider: b3Cloth::SetWorld (cloth.cpp:290) with a static
+ * b3Body carrying a b3SphereShape (src/bounce/dynamics/shapes/sphere_shape.cpp).
+ * At most B3G_MAX_SPHERES per cloth. */
+#define B3G_MAX_SPHERES 4
+b3g_status b3g_cloth_add_static_sphere(b3g_cloth* cloth, const float center[3], float radius,
+                                       float friction, uint32_t* shape_id);
+/* b3Cloth::SetWorld(nullptr): drop every collider and its contacts. */
+b3g_status b3g_cloth_clear_colliders(b3g_cloth* cloth);
+
+/* ---- particles (include/bounce/cloth/particle.h:63-111) ------------------ */
+
+b3g_status b3g_particle_set_type(b3g_cloth* cloth, uint32_t vertex, b3g_particle_type type);
+b3g_status b3g_particle_get_type(const b3g_cloth* cloth, uint32_t vertex, b3g_particle_type* type);
+b3g_status b3g_particle_set_position(b3g_cloth* cloth, uint32_t vertex, const float position[3]);
+b3g_status b3g_particle_get_position(const b3g_cloth* cloth, uint32_t vertex, float position[3]);
+b3g_status b3g_particle_set_velocity(b3g_cloth* cloth, uint32_t vertex, const float velocity[3]);
+b3g_status b3g_particle_get_velocity(const b3g_cloth* cloth, uint32_t vertex, float velocity[3]);
+b3g_status b3g_particle_get_mass(const b3g_cloth* cloth, uint32_t vertex, float* mass);
+b3g_status b3g_particle_apply_force(b3g_cloth* cloth, uint32_t vertex, const float force[3]);
+b3g_status b3g_particle_apply_translation(b3g_cloth* cloth, uint32_t vertex, const float translation[3]);
+
+/* Whole-cloth forms of the particle calls: arrays of 3 * vertex_count floats
+ * (xyz per vertex) or vertex_count types, host memory. */
+b3g_status b3g_cloth_set_types(b3g_cloth* cloth, const uint8_t* types);
+b3g_status b3g_cloth_apply_forces(b3g_cloth* cloth, const float* forces);
+b3g_status b3g_cloth_apply_translations(b3g_cloth* cloth, const float* translations);
+
+/* ---- step ----------------------------------------------------------------- */
+
+/* b3Cloth::Step (cloth.cpp:551-601): body-contact update, force/Jacobian
+ * assembly, S-filtered Jacobi-preconditioned CG, contact velocity and position
+ * iterations, AABB sync, new body contacts.  Cloth self-collision is not part
+ * of this path.  stats may be NULL.  The step is enqueued and waited for. */
+b3g_status b3g_cloth_step(b3g_cloth* cloth, float dt, uint32_t velocity_iterations,
+                          uint32_t position_iterations, b3g_step_stats* stats);
+
+/* Device time per kernel of one step, for roofline accounting: the same step
+ * as b3g_cloth_step, launched kernel by kernel (no graph) with CUDA events
+ * around each launch on the cloth's stream.  Sums over the step's launches. */
+typedef struct {
+    float contacts_update_ms;
+    float assemble_ms;
+    float cg_init_ms;
+    float cg_spmv_ms;       /* all iterations */
+    float cg_update_ms;     /* all iterations */
+    float cg_direction_ms;  /* all iterations */
+    float finalize_ms;
+    float contact_position_ms;
+    float post_ms;
+    uint32_t cg_iterations;
+    uint32_t contact_position_launches;
+} b3g_phase_times;
+
+b3g_status b3g_cloth_step_profiled(b3g_cloth* cloth, float dt, uint32_t velocity_iterations,
+                                   uint32_t position_iterations, b3g_phase_times* times,
+                                   b3g_step_stats* stats);
+
+/* Bytes of the device-resident system: padded SELL-32 entries, unpadded
+ * blocks, vertices, triangles, springs. */
+typedef struct {
+    uint32_t vertices, triangles, springs, blocks, sell_entries, max_degree;
+} b3g_cloth_info;
+b3g_status b3g_cloth_get_info(const b3g_cloth* cloth, b3g_cloth_info* info);
+
+/* ---- state ---------------------------------------------------------------- */
+
+uint32_t b3g_cloth_vertex_count(const b3g_cloth* cloth);
+/* positions / velocities / last CG solution (b3Particle::m_x), 3 floats per
+ * vertex; any pointer may be NULL. */
+b3g_status b3g_cloth_read_state(const b3g_cloth* cloth, float* positions, float* velocities,
+                                float* cg_solution);
+b3g_status b3g_cloth_write_state(b3g_cloth* cloth, const float* positions, const float* velocities,
+                                 const float* cg_solution);
+b3g_status b3g_cloth_read_masses(const b3g_cloth* cloth, float* masses);
+/* b3Cloth::GetEnergy (cloth.cpp:366-374) */
+b3g_status b3g_cloth_get_energy(const b3g_cloth* cloth, float* energy);
+/* Body contacts per vertex and collider: exists, active (vertex_count *
+ * sphere_count bytes each), impulses (normal, tangent1, tangent2). */
+b3g_status b3g_cloth_read_contacts(const b3g_cloth* cloth, uint8_t* exists, uint8_t* active,
+                                   float* impulses);
+b3g_status b3g_cloth_last_stats(const b3g_cloth* cloth, b3g_step_stats* stats);
+
+/* ---- inspection of the assembled system ----------------------------------- */
+
+/* The block-sparse system of the last step (or b3g_cloth_assemble), A = M - h dfdv - h^2 dfdx and
+ * b = h (f + h dfdx v + dfdx y) (cloth_force_solver.cpp:193-204), as
+ * block CSR by vertex: rowptr (n + 1), cols (nnz), vals (9 floats per block,
+ * column-major like b3Mat33), b (3 n), filter S (n, 1 or 0), warm start x0 (3 n).
+ * Call with vals == NULL to get nnz only. */
+b3g_status b3g_cloth_read_system(const b3g_cloth* cloth, uint32_t* nnz, uint32_t* rowptr,
+                                 uint32_t* cols, float* vals, float* b, float* S, float* x0);
+
+/* Assemble A, b and P^-1 from the current state for a step of dt without
+ * changing the state (the first half of b3ClothForceSolver::Solve,
+ * cloth_force_solver.cpp:142-204); read them with b3g_cloth_read_system. */
+b3g_status b3g_cloth_assemble(b3g_cloth* cloth, float dt);
+
+/* ---- standalone MPCG -------------------------------------------------------- */
+
+/* b3SolveMPCG (cloth_force_solver.cpp:61-136) on a caller-supplied system in
+ * DEVICE memory: block CSR (rowptr n + 1, cols nnz, vals 9 per block,
+ * column-major), b (3 n), S (n floats, 1 or 0), x0 (3 n) -> x (3 n).  Device
+ * scratch is allocated per call.  iterations and stats may be NULL. */
+b3g_status b3g_mpcg_solve(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const float* vals,
+                          const float* b, const float* S, const float* x0, const b3g_solver_opts* opts,
+                          float* x, uint32_t* iterations, b3g_step_stats* stats, void* stream);
+
+/* ---- misc ----------------------------------------------------------------- */
+
+const char* b3g_status_string(b3g_status status);
+/* Number of kernels this library has launched in this process. */
+uint64_t b3g_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -61,6 +61,7 @@ def port_lib():
         L.oc_destroy.argtypes = [C.c_void_p]
         L.oc_set_gravity.argtypes = [C.c_void_p, _f32p]
         L.oc_set_type.argtypes = [C.c_void_p, C.c_uint32, C.c_int]
+        L.oc_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         for name in ("oc_apply_force", "oc_apply_translation", "oc_set_position", "oc_set_velocity"):
             getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, _f32p]
         L.oc_add_sphere.argtypes = [C.c_void_p, _f32p, C.c_float, C.c_float]
@@ -209,6 +210,10 @@ class PortCloth(_Base):
 
     def set_type(self, vertex, ty):
         self.L.oc_set_type(self.h, vertex, ty)
+
+    def set_state(self, x=None, v=None, dv=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1) for a in (x, v, dv)]
+        self.L.oc_set_state(self.h, *[None if a is None else a.ctypes.data for a in arrs])
 
     def apply_force(self, vertex, f):
         self.L.oc_apply_force(self.h, vertex, np.asarray(f, np.float32))

@@ -468,6 +468,17 @@ static void destroy_particle_contacts(oc_cloth* c, uint32_t i)
     c->ncontact = w;
 }
 
+/* Overwrite positions, velocities and the CG warm start of every particle
+ * (no proxy update): used to start both solvers from identical inputs. */
+void oc_set_state(oc_cloth* c, const float* x, const float* v, const float* dv)
+{
+    for (uint32_t i = 0; i < c->n; ++i) {
+        if (x) c->x[i] = V(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+        if (v) c->v[i] = V(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+        if (dv) c->mx[i] = V(dv[3 * i], dv[3 * i + 1], dv[3 * i + 2]);
+    }
+}
+
 void oc_set_gravity(oc_cloth* c, const float* g) { c->gravity = V(g[0], g[1], g[2]); }
 
 /* b3Particle::SetType (particle.cpp:121-143) */

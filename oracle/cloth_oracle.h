@@ -59,6 +59,7 @@ oc_cloth* oc_create(const float* vertices, uint32_t vertex_count, const uint32_t
 void oc_destroy(oc_cloth* c);
 
 void oc_set_gravity(oc_cloth* c, const float* g);
+void oc_set_state(oc_cloth* c, const float* x, const float* v, const float* dv);
 void oc_set_type(oc_cloth* c, uint32_t vertex, int type);
 void oc_apply_force(oc_cloth* c, uint32_t vertex, const float* f);
 void oc_apply_translation(oc_cloth* c, uint32_t vertex, const float* t);

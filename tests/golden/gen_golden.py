@@ -1,0 +1,74 @@
+"""Generate the golden fixtures from the reference library itself.
+
+Runs the reference (oracle/_ref/libbounce_ref.so, compiled from the Bounce
+sources by oracle/Makefile; needs the reference tree on disk) on seeded
+synthetic cloths and stores its outputs as compressed .npz files next to this
+script.  The parity tests check the C restatement (oracle/) and the CUDA path
+against these files, so they need neither the reference tree nor this script.
+
+    python tests/golden/gen_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from bounce_b200.meshes import plain_scene, sphere_scene  # noqa: E402
+
+
+def trajectory(scene, steps, keep):
+    ref = oracle.RefCloth(scene.mesh, scene.cdef, restated=False).setup(scene)
+    out = {"vertices": scene.mesh.vertices, "triangles": scene.mesh.triangles, "def": scene.cdef.as_array(),
+           "pinned": np.asarray(scene.pinned, np.uint32), "dt": np.float32(scene.dt)}
+    if scene.spheres:
+        c, r, mu = scene.spheres[0]
+        out["sphere"] = np.array([c[0], c[1], c[2], r, mu], np.float32)
+    iters = []
+    for k in range(1, steps + 1):
+        iters.append(ref.step(scene.dt, scene.velocity_iterations, scene.position_iterations)["iterations"])
+        if k in keep:
+            s = ref.state()
+            out[f"x_{k}"] = s["x"]
+            out[f"v_{k}"] = s["v"]
+            out[f"dv_{k}"] = s["dv"]
+            if scene.spheres:
+                cts = ref.contacts()
+                out[f"contact_exists_{k}"] = cts["exists"]
+                out[f"contact_active_{k}"] = cts["active"]
+                out[f"contact_impulses_{k}"] = cts["impulses"]
+    out["iterations"] = np.asarray(iters, np.uint32)
+    out["mass"] = ref.state()["mass"]
+    return out
+
+
+def system(scene):
+    ref = oracle.RefCloth(scene.mesh, scene.cdef, restated=False).setup(scene)
+    ref.step(scene.dt, scene.velocity_iterations, scene.position_iterations)
+    sys_ = ref.system(scene.dt)
+    out = {"vertices": scene.mesh.vertices, "triangles": scene.mesh.triangles, "def": scene.cdef.as_array(),
+           "pinned": np.asarray(scene.pinned, np.uint32), "dt": np.float32(scene.dt)}
+    st = ref.state()
+    out.update({"x_1": st["x"], "v_1": st["v"], "dv_1": st["dv"]})
+    out.update({f"sys_{k}": v for k, v in sys_.items()})
+    return out
+
+
+def main():
+    oracle.build(port=True, ref=True)
+    files = {
+        "plain32_ref.npz": trajectory(plain_scene(32, seed=1), 30, {1, 10, 30}),
+        "sphere32_ref.npz": trajectory(sphere_scene(32, seed=2), 40, {1, 20, 30, 40}),
+        "system16_bend_ref.npz": system(sphere_scene(16, seed=4)),
+    }
+    for name, data in files.items():
+        np.savez_compressed(os.path.join(HERE, name), **data)
+        print(name, os.path.getsize(os.path.join(HERE, name)), "bytes")
+
+
+if __name__ == "__main__":
+    main()

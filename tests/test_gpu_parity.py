@@ -1,0 +1,145 @@
+"""CUDA path against the CPU oracle (the reference's algorithm restated in C).
+
+Tolerances:
+* assembled A and b from identical state: bit-exact (both evaluate the
+  element arithmetic in the reference's operation order without FMA);
+* one step from identical inputs: relative error <= 1e-4 on x and v, CG
+  iteration count within +-1 (the grid reductions sum in a different order
+  than the reference's sequential FP32 dots);
+* 100-step trajectories: bounded drift, reported and held below 1e-2 m.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_err, system_blocks
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(b3g, port, scene, opts=None):
+    gpu = b3g.Cloth(scene.mesh, scene.cdef).setup(scene, opts)
+    ora = port.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    if opts is not None:
+        ora.set_solver(opts.stop_rule, opts.tolerance, opts.max_iterations, opts.dot)
+    return gpu, ora
+
+
+@pytest.mark.parametrize("maker", ["plain", "sphere"])
+def test_assembly_bit_exact(b3g, port, maker):
+    scene = b3g.plain_scene(24) if maker == "plain" else b3g.sphere_scene(24)
+    gpu, ora = _pair(b3g, port, scene)
+    # move away from the rest state so every element is active
+    rng = np.random.default_rng(5)
+    x = scene.mesh.vertices + rng.normal(0, 2e-3, scene.mesh.vertices.shape).astype(np.float32)
+    v = rng.normal(0, 0.1, scene.mesh.vertices.shape).astype(np.float32)
+    gpu.write_state(x=x, v=v)
+    ora.set_state(x=x, v=v)
+    gpu.assemble(scene.dt)
+    gs = gpu.system()
+    os_ = ora.system(scene.dt)
+    gb, gbv = system_blocks(gs)
+    ob, obv = system_blocks(os_, os_["vertex_of_row"])
+    # every block the reference creates exists in the GPU pattern with the same value
+    for key, val in ob.items():
+        assert key in gb, key
+        assert np.array_equal(gb[key], val), (key, gb[key], val)
+    # blocks only in the static GPU pattern are zero
+    for key, val in gb.items():
+        if key not in ob:
+            assert not np.any(val), key
+    assert np.array_equal(gbv, obv)
+
+
+def test_step_identical_inputs_reference_mode(b3g, port):
+    scene = b3g.plain_scene(32)
+    gpu, ora = _pair(b3g, port, scene)
+    worst = 0.0
+    for step in range(30):
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        gi = gpu.step(scene.dt)["iterations"]
+        oi = ora.step(scene.dt)["iterations"]
+        g, o = gpu.state(), ora.state()
+        ex, ev = rel_err(g["x"], o["x"]), rel_err(g["v"] - st["v"], o["v"] - st["v"])
+        worst = max(worst, ex)
+        assert abs(gi - oi) <= 1, (step, gi, oi)
+        assert ex <= 1e-4, (step, ex)
+        assert ev <= 1e-3, (step, ev)
+    print("worst per-step relative x error", worst)
+
+
+def test_trajectory_drift_plain(b3g, port):
+    """100 free steps of a cloth hanging from two corners.  The motion turns
+    chaotic once the cloth folds (about step 55): the oracle against itself
+    with FP64 instead of FP32 CG dots -- the same algorithm, another rounding --
+    drifts apart by centimetres there.  The GPU trajectory must stay within
+    1e-4 m of the oracle before that, and its bulk motion (centroid, kinetic
+    energy) must agree after it."""
+    scene = b3g.plain_scene(32)
+    gpu, ora = _pair(b3g, port, scene)
+    floor = port.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    floor.set_solver(0, 0.0, 20, 2)
+    drift, noise = [], []
+    for step in range(100):
+        gpu.step(scene.dt)
+        ora.step(scene.dt)
+        floor.step(scene.dt)
+        xo = ora.state()["x"]
+        drift.append(float(np.abs(gpu.state()["x"] - xo).max()))
+        noise.append(float(np.abs(floor.state()["x"] - xo).max()))
+    print("drift GPU-oracle (m) at 1/10/50/100:", drift[0], drift[9], drift[49], drift[99],
+          "| oracle f32 vs f64 dots:", noise[0], noise[9], noise[49], noise[99])
+    assert drift[0] <= 1e-6
+    assert max(drift[:50]) <= 1e-4
+    g, o = gpu.state(), ora.state()
+    assert abs(g["x"][:, 1].mean() - o["x"][:, 1].mean()) <= 0.02 * abs(o["x"][:, 1].mean())
+    assert abs(gpu.energy() - ora.energy()) <= 0.1 * ora.energy()
+
+
+def test_sphere_contacts_per_step(b3g, port):
+    """Bending springs and sphere contacts (velocity GS with friction,
+    position GS with the early out): each step starts the oracle from the
+    GPU's positions, velocities and CG warm start; contact bookkeeping runs
+    on both sides independently."""
+    scene = b3g.sphere_scene(32)
+    gpu, ora = _pair(b3g, port, scene)
+    seen_active = 0
+    for step in range(45):
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        seen_active = max(seen_active, o["active_contacts"])
+        assert abs(g["iterations"] - o["iterations"]) <= 1, step
+        assert abs(int(g["active_contacts"]) - int(o["active_contacts"])) <= max(2, o["active_contacts"] // 100), step
+        assert abs(int(g["contacts"]) - int(o["contacts"])) <= max(2, o["contacts"] // 100), step
+        e = rel_err(gpu.state()["x"], ora.state()["x"])
+        assert e <= 1e-4, (step, e)
+    assert seen_active > 100  # the cloth did hit the sphere
+
+
+def test_sphere_trajectory_start(b3g, port):
+    scene = b3g.sphere_scene(32)
+    gpu, ora = _pair(b3g, port, scene)
+    d = []
+    for step in range(25):
+        gpu.step(scene.dt)
+        ora.step(scene.dt)
+        d.append(float(np.abs(gpu.state()["x"] - ora.state()["x"]).max()))
+    print("sphere trajectory drift (m) at 1/10/25:", d[0], d[9], d[24])
+    assert max(d) <= 1e-3
+
+
+@pytest.mark.parametrize("dot", [0, 1, 2])
+def test_relative_mode_matches_oracle(b3g, port, dot):
+    scene = b3g.plain_scene(32)
+    opts = b3g.SolverOptions.relative(1e-4, 50, dot)
+    gpu, ora = _pair(b3g, port, scene, opts)
+    for step in range(10):
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        assert abs(g["iterations"] - o["iterations"]) <= 1
+        assert g["delta"] <= 1e-8 * g["b_delta"] * 1.0001 or g["iterations"] == 50
+        assert rel_err(gpu.state()["x"], ora.state()["x"]) <= 1e-4
