@@ -21,3 +21,36 @@ def rel_err(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def device_system(sysd, device="cuda:0"):
+    """Copy an exported block-CSR system to device tensors (uint32 as int32 bits)."""
+    import torch
+
+    def t(a, dt):
+        return torch.from_numpy(np.ascontiguousarray(a).view(dt)).to(device)
+
+    return {"n": int(sysd["rowptr"].size - 1), "rowptr": t(sysd["rowptr"], np.int32), "cols": t(sysd["cols"], np.int32),
+            "vals": t(sysd["vals"], np.float32), "b": t(sysd["b"], np.float32), "S": t(sysd["S"], np.float32),
+            "x0": t(sysd["x0"], np.float32)}
+
+
+def call_mpcg(b3g, entry, dsys, opts, x=None):
+    """Call a standalone MPCG entry point of libb3g.so on device tensors;
+    returns (status, x as numpy (n, 3), iterations, stats)."""
+    import ctypes as C
+
+    import torch
+
+    n = dsys["n"]
+    if x is None:
+        x = torch.zeros(3 * n, dtype=torch.float32, device=dsys["b"].device)
+    it = C.c_uint32(0)
+    st = b3g.StepStatsC()
+    o = opts.as_c()
+    fn = getattr(b3g.lib(), entry)
+    torch.cuda.synchronize()
+    status = fn(n, dsys["rowptr"].data_ptr(), dsys["cols"].data_ptr(), dsys["vals"].data_ptr(), dsys["b"].data_ptr(),
+                dsys["S"].data_ptr(), dsys["x0"].data_ptr(), C.byref(o), x.data_ptr(), C.byref(it), C.byref(st), None)
+    torch.cuda.synchronize()
+    return status, x.cpu().numpy().reshape(-1, 3), it.value, st
