@@ -114,6 +114,8 @@ def lib() -> C.CDLL:
             "b3g_cloth_get_info": [vp, C.POINTER(ClothInfoC)],
             "b3g_mpcg_solve": [u32, vp, vp, vp, vp, vp, vp, C.POINTER(SolverOptsC), vp, C.POINTER(u32),
                                C.POINTER(StepStatsC), vp],
+            "b3g_mpcg_solve_noalloc": [u32, vp, vp, vp, vp, vp, vp, C.POINTER(SolverOptsC), vp, C.POINTER(u32),
+                                       C.POINTER(StepStatsC), vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

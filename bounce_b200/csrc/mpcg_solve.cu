@@ -4,6 +4,7 @@
 // stop at the iteration cap or at the stop rule.  Vectors are xyz per row
 // (b3DenseVec3 layout); S holds one 1/0 per row.
 #include <cstring>
+#include <mutex>
 
 #include "../../include/b3g.h"
 #include "cg_common.cuh"
@@ -266,6 +267,98 @@ extern "C" b3g_status b3g_mpcg_solve(uint32_t n, const uint32_t* rowptr, const u
     StepScalars h;
     b3g_status r = csr_run(s, opts, st, &h);
     cudaFree(scratch);
+    if (r != B3G_OK) return r;
+    csr_report(h, iterations, stats);
+    return h.status ? (b3g_status)h.status : B3G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant
+// ---------------------------------------------------------------------------
+//
+// Some callers cannot call cudaMalloc at solve time: a game or physics loop
+// that reserves all of its device memory when a level loads and forbids
+// allocation inside the frame (cudaMalloc can take milliseconds and
+// synchronizes the device), a process whose device memory is already claimed
+// up front by another framework's caching allocator, or code that runs the
+// solver from inside its own allocator's callbacks.  For them the scratch
+// (P^-1, r, p, s, the reduction partials and the CG scalars) lives in one
+// file-scope device array, sized for systems of up to
+// B3G_MPCG_NOALLOC_MAX_ROWS block rows, which every GPU that loads the library
+// holds until the process exits.  The array's name is only a host-side
+// stand-in in host code, so its device address is looked up once per device
+// with cudaGetSymbolAddress, by the first call on that device.
+
+namespace b3g {
+namespace {
+
+constexpr uint32_t kNoAllocRows = B3G_MPCG_NOALLOC_MAX_ROWS;
+constexpr uint32_t kNoAllocGrid = (kNoAllocRows + 255) / 256 < 148 * 4 ? (kNoAllocRows + 255) / 256 : 148 * 4;
+constexpr size_t kNoAllocBytes = ((4ull * 3 * kNoAllocRows * sizeof(float) + 255) & ~size_t(255)) +
+                                 ((kNoAllocGrid * 32ull + 255) & ~size_t(255)) +
+                                 ((sizeof(StepScalars) + 255) & ~size_t(255));
+constexpr int kNoAllocDevices = 64;
+
+__device__ __align__(256) char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mutex;
+char* g_noalloc_addr[kNoAllocDevices];
+
+// Device address of the scratch array on the current device (looked up on
+// first use of each device).
+b3g_status noalloc_scratch(char** out)
+{
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return B3G_ERR_NO_DEVICE;
+    }
+    if (dev < 0 || dev >= kNoAllocDevices) return B3G_ERR_CAPACITY;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? B3G_ERR_NO_DEVICE : B3G_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = static_cast<char*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return B3G_OK;
+}
+
+}  // namespace
+}  // namespace b3g
+
+extern "C" b3g_status b3g_mpcg_solve_noalloc(uint32_t n, const uint32_t* rowptr, const uint32_t* cols,
+                                             const float* vals, const float* b, const float* S, const float* x0,
+                                             const b3g_solver_opts* opts, float* x, uint32_t* iterations,
+                                             b3g_step_stats* stats, void* stream)
+{
+    b3g_status v = csr_validate(n, rowptr, cols, vals, b, S, x0, opts, x);
+    if (v != B3G_OK) return v;
+    if (n > kNoAllocRows) return B3G_ERR_CAPACITY;
+    CsrSystem s{};
+    s.n = n;
+    s.rowptr = rowptr;
+    s.cols = cols;
+    s.vals = vals;
+    s.b = b;
+    s.S = S;
+    s.x0 = x0;
+    s.x = x;
+    s.block = 256;
+    s.grid = csr_grid(n);
+    if (csr_scratch_bytes(n, s.grid) > kNoAllocBytes) return B3G_ERR_CAPACITY;
+    char* scratch = nullptr;
+    v = noalloc_scratch(&scratch);
+    if (v != B3G_OK) return v;
+    csr_bind_scratch(&s, scratch);
+    // csr_run clears the CG scalars and reduction tickets before the first
+    // kernel; every other scratch word is written before it is read.
+    StepScalars h;
+    b3g_status r = csr_run(s, opts, (cudaStream_t)stream, &h);
     if (r != B3G_OK) return r;
     csr_report(h, iterations, stats);
     return h.status ? (b3g_status)h.status : B3G_OK;

@@ -212,6 +212,28 @@ b3g_status b3g_mpcg_solve(uint32_t n, const uint32_t* rowptr, const uint32_t* co
                           const float* b, const float* S, const float* x0, const b3g_solver_opts* opts,
                           float* x, uint32_t* iterations, b3g_step_stats* stats, void* stream);
 
+/* b3g_mpcg_solve without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc when they
+ * solve -- a game or physics loop that reserves all device memory at level
+ * load and forbids allocation inside a frame (cudaMalloc is slow and
+ * synchronizes the device), a process whose device memory is already held by
+ * another framework's caching allocator, or code running inside its own
+ * allocator's callbacks.  Same arguments and results as b3g_mpcg_solve.
+ *  - The scratch is one static device array in libb3g.so, sized for at most
+ *    B3G_MPCG_NOALLOC_MAX_ROWS block rows (about 3.2 MB); every GPU that
+ *    loads the library holds it until the process exits.  Larger systems
+ *    return B3G_ERR_CAPACITY.
+ *  - The first call on each device looks the array's device address up
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - All calls share the one array: calls whose work overlaps on the GPU
+ *    (other streams, other host threads) race and corrupt each other.  Each
+ *    call clears the CG scalars it needs zeroed; other scratch contents are
+ *    left from the previous call and overwritten before use. */
+#define B3G_MPCG_NOALLOC_MAX_ROWS 65536
+b3g_status b3g_mpcg_solve_noalloc(uint32_t n, const uint32_t* rowptr, const uint32_t* cols, const float* vals,
+                                  const float* b, const float* S, const float* x0, const b3g_solver_opts* opts,
+                                  float* x, uint32_t* iterations, b3g_step_stats* stats, void* stream);
+
 /* ---- misc ----------------------------------------------------------------- */
 
 const char* b3g_status_string(b3g_status status);
