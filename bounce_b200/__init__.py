@@ -70,6 +70,15 @@ class ClothInfoC(C.Structure):
                                            "max_degree")]
 
 
+class BatchScheduleC(C.Structure):
+    _fields_ = [("cluster", C.c_uint32), ("split_class", C.c_uint8 * 32), ("tuned_cg_ms", C.c_float)]
+
+
+class BatchStatsC(C.Structure):
+    _fields_ = [("count", C.c_uint32), ("rows", C.c_uint32), ("tasks", C.c_uint32),
+                ("cg_iterations_total", C.c_uint32), ("cg_iterations_max", C.c_uint32), ("step_ms", C.c_float)]
+
+
 _lib = None
 
 
@@ -114,6 +123,12 @@ def lib() -> C.CDLL:
             "b3g_cloth_get_info": [vp, C.POINTER(ClothInfoC)],
             "b3g_mpcg_solve": [u32, vp, vp, vp, vp, vp, vp, C.POINTER(SolverOptsC), vp, C.POINTER(u32),
                                C.POINTER(StepStatsC), vp],
+            "b3g_batch_create": [i32, u32, C.POINTER(vp)],
+            "b3g_batch_destroy": [vp],
+            "b3g_batch_step": [vp, vp, u32, f32, u32, u32, vp, C.POINTER(BatchStatsC)],
+            "b3g_batch_set_schedule": [vp, C.POINTER(BatchScheduleC)],
+            "b3g_batch_get_schedule": [vp, C.POINTER(BatchScheduleC)],
+            "b3g_batch_autotune": [vp, vp, u32, f32, C.POINTER(BatchScheduleC)],
             "b3g_mpcg_solve_noalloc": [u32, vp, vp, vp, vp, vp, vp, C.POINTER(SolverOptsC), vp, C.POINTER(u32),
                                        C.POINTER(StepStatsC), vp],
         }
@@ -357,6 +372,61 @@ class Cloth:
         if opts is not None:
             self.set_solver(opts)
         return self
+
+
+class Batch:
+    """Many cloths stepped together (b3g_batch): fixed launches per step, the
+    CG in one persistent launch, one cloth per CTA or per cluster."""
+
+    def __init__(self, capacity: int = 1024, device: int = 0):
+        h = C.c_void_p()
+        check(lib().b3g_batch_create(device, capacity, C.byref(h)), "b3g_batch_create")
+        self.h = h
+        self.stats = BatchStatsC()
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().b3g_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    @staticmethod
+    def _handles(cloths):
+        arr = (C.c_void_p * len(cloths))(*[c.h.value for c in cloths])
+        return arr
+
+    def step(self, cloths, dt: float, velocity_iterations: int = 8, position_iterations: int = 2,
+             per_cloth: bool = False):
+        arr = self._handles(cloths)
+        stats = (StepStatsC * len(cloths))() if per_cloth else None
+        check(lib().b3g_batch_step(self.h, arr, len(cloths), dt, velocity_iterations, position_iterations,
+                                   stats, C.byref(self.stats)), "batch_step")
+        s = self.stats
+        out = {"count": s.count, "rows": s.rows, "tasks": s.tasks, "cg_iterations_total": s.cg_iterations_total,
+               "cg_iterations_max": s.cg_iterations_max, "step_ms": s.step_ms}
+        if per_cloth:
+            out["per_cloth"] = [{"iterations": x.iterations, "delta": x.delta, "b_delta": x.b_delta,
+                                 "active_contacts": x.active_contacts, "contacts": x.contacts} for x in stats]
+        return out
+
+    def schedule(self) -> dict:
+        sc = BatchScheduleC()
+        check(lib().b3g_batch_get_schedule(self.h, C.byref(sc)), "get_schedule")
+        return {"cluster": sc.cluster, "split_class": list(sc.split_class), "tuned_cg_ms": sc.tuned_cg_ms}
+
+    def set_schedule(self, cluster: int = 1, split_classes=()) -> None:
+        sc = BatchScheduleC()
+        sc.cluster = cluster
+        for k in split_classes:
+            sc.split_class[k] = 1
+        check(lib().b3g_batch_set_schedule(self.h, C.byref(sc)), "set_schedule")
+
+    def autotune(self, cloths, dt: float) -> dict:
+        arr = self._handles(cloths)
+        sc = BatchScheduleC()
+        check(lib().b3g_batch_autotune(self.h, arr, len(cloths), dt, C.byref(sc)), "autotune")
+        return {"cluster": sc.cluster, "split_class": list(sc.split_class), "tuned_cg_ms": sc.tuned_cg_ms}
 
 
 def kernel_launch_count() -> int:

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libb3g.so")
-SOURCES = ["cloth_kernels.cu", "cloth_api.cu", "mpcg_solve.cu", "topology.cpp"]
+SOURCES = ["cloth_kernels.cu", "cloth_api.cu", "mpcg_solve.cu", "batch_cg.cu", "batch_api.cu", "topology.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-warn-spills"]
 
@@ -47,7 +47,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for s, o in zip(srcs, objs):
         cmd = [nvcc] + NVCC_FLAGS + ["-x", "cu" if s.endswith(".cu") else "c++", "-c", s, "-o", o]
         if s.endswith(".cpp"):
-            cmd = [nvcc, "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off", "-c", s, "-o", o]
+            cmd = [nvcc, "-O3", "-std=c++17", "-Wno-deprecated-gpu-targets", "-Xcompiler", "-fPIC,-ffp-contract=off",
+                   "-c", s, "-o", o]
         procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
     for cmd, p in procs:
         out, _ = p.communicate()

@@ -1,0 +1,301 @@
+// Batched MPCG: many cloths of uneven sizes in one persistent launch.
+//
+// A team -- one CTA, or a thread-block cluster of TEAM CTAs for large cloths
+// -- takes a cloth from a work queue (largest first), runs the whole
+// S-filtered Jacobi-preconditioned CG of that cloth (b3SolveMPCG,
+// src/bounce/cloth/cloth_force_solver.cpp:61-136) with team-local
+// barriers and reductions, then takes the next cloth.  No grid-wide
+// synchronisation.  Within a team the reduction tree is fixed (thread ->
+// warp shuffle -> CTA -> cluster ranks in order), so a cloth's result does
+// not depend on which other cloths share the launch.
+#include <cooperative_groups.h>
+
+#include "batch.cuh"
+#include "cg_common.cuh"
+#include "cloth_dev.cuh"
+#include "vec.cuh"
+
+namespace cgx = cooperative_groups;
+
+namespace b3g {
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kWarps = kBlock / 32;
+
+__device__ __forceinline__ uint32_t rbase(const ClothDev& c, uint32_t row)
+{
+    return c.slice_off[row >> 5] + (row & 31u);
+}
+
+__device__ __forceinline__ f3 spmv(const ClothDev& c, uint32_t row, const float* q)
+{
+    const uint32_t base = rbase(c, row);
+    const uint32_t deg = c.row_deg[row];
+    const uint32_t E = c.E;
+    const float* v = c.vals;
+    f3 acc = zero3();
+    for (uint32_t k = 0; k < deg; ++k) {
+        const uint32_t idx = base + 32u * k;
+        const uint32_t col = c.cols[idx];
+        const m3 a{f3{v[idx], v[E + idx], v[2 * E + idx]}, f3{v[3 * E + idx], v[4 * E + idx], v[5 * E + idx]},
+                   f3{v[6 * E + idx], v[7 * E + idx], v[8 * E + idx]}};
+        acc = acc + a * ld3(q, c.n, col);
+    }
+    return acc;
+}
+
+__device__ __forceinline__ bool dyn(const ClothDev& c, uint32_t i) { return c.type[i] == 2; }
+
+// Team = TEAM CTAs of one cluster (TEAM == 1: the CTA alone).
+template <int TEAM>
+struct Team {
+    __device__ static uint32_t rank()
+    {
+        if (TEAM == 1) return 0;
+        return cgx::this_cluster().block_rank();
+    }
+    __device__ static void sync()
+    {
+        if (TEAM == 1) __syncthreads();
+        else cgx::this_cluster().sync();
+    }
+};
+
+// Sum of NV values over the team, identical in every thread.  `slot` is this
+// CTA's shared buffer of NV partials (TEAM ranks read each other's).
+template <int TEAM, int DOT, int NV>
+__device__ void team_sum(typename DotT<DOT>::T (&v)[NV], typename DotT<DOT>::T* wsum, typename DotT<DOT>::T* slot)
+{
+    typedef DotT<DOT> D;
+    typedef typename D::T T;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int off = 16; off > 0; off >>= 1) v[k] = D::combine(v[k], D::shfl(v[k], off));
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) wsum[k * kWarps + warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            T a = wsum[k * kWarps];
+            for (int w = 1; w < kWarps; ++w) a = D::combine(a, wsum[k * kWarps + w]);
+            slot[k] = a;
+        }
+    }
+    Team<TEAM>::sync();
+    if (TEAM == 1) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k] = slot[k];
+    } else {
+        cgx::cluster_group cl = cgx::this_cluster();
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            T a = *cl.map_shared_rank(slot + k, 0);
+            for (int r = 1; r < TEAM; ++r) a = D::combine(a, *cl.map_shared_rank(slot + k, r));
+            v[k] = a;
+        }
+    }
+    // nobody may overwrite slot / wsum before every rank has read them
+    Team<TEAM>::sync();
+}
+
+// The CG of one cloth by one team.  Rows are split into TEAM contiguous
+// chunks; thread t of a CTA takes rows chunk_begin + t, + kBlock, ...
+template <int TEAM, int DOT>
+__device__ void team_cg(const ClothDev& c, typename DotT<DOT>::T* wsum, typename DotT<DOT>::T* slot)
+{
+    typedef DotT<DOT> D;
+    typedef typename D::T T;
+    StepScalars* sc = c.sc;
+    const uint32_t n = c.n;
+    const uint32_t chunk = (n + TEAM - 1) / TEAM;
+    const uint32_t r0 = Team<TEAM>::rank() * chunk;
+    const uint32_t r1 = min(n, r0 + chunk);
+    const uint32_t max_iter = sc->max_iter;
+
+    // x0 = S m_x, r = S (b - A x0), p = S P^-1 r (cloth_force_solver.cpp:90-100)
+    T v2[2] = {D::zero(), D::zero()};
+    for (uint32_t row = r0 + threadIdx.x; row < r1; row += kBlock) {
+        const bool Si = dyn(c, row);
+        const uint32_t base = rbase(c, row);
+        const uint32_t deg = c.row_deg[row];
+        f3 ax = zero3();
+        for (uint32_t k = 0; k < deg; ++k) {
+            const uint32_t idx = base + 32u * k;
+            const uint32_t col = c.cols[idx];
+            const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
+            const float* v = c.vals;
+            const uint32_t E = c.E;
+            const m3 a{f3{v[idx], v[E + idx], v[2 * E + idx]}, f3{v[3 * E + idx], v[4 * E + idx], v[5 * E + idx]},
+                       f3{v[6 * E + idx], v[7 * E + idx], v[8 * E + idx]}};
+            ax = ax + a * xj;
+        }
+        const f3 bi = ld3(c.b, n, row);
+        const f3 pv = ld3(c.pinv, n, row);
+        const f3 r = Si ? bi - ax : zero3();
+        const f3 p = Si ? mk(r.x * pv.x, r.y * pv.y, r.z * pv.z) : zero3();
+        const f3 bh = Si ? bi : zero3();
+        st3(c.dv, n, row, Si ? ld3(c.mx, n, row) : zero3());
+        st3(c.r, n, row, r);
+        st3(c.p, n, row, p);
+        v2[0] = D::add_term(v2[0], bh, mk(bh.x * pv.x, bh.y * pv.y, bh.z * pv.z));
+        v2[1] = D::add_term(v2[1], r, p);
+    }
+    team_sum<TEAM, DOT, 2>(v2, wsum, slot);  // also orders the p writes before the first SpMV
+    double b_delta = D::value(v2[0]), delta = D::value(v2[1]);
+    if (DOT != 2) {
+        b_delta = (double)(float)b_delta;
+        delta = (double)(float)delta;
+    }
+    const double delta0 = delta;
+    uint32_t status = (!isfinite(delta) || !isfinite(b_delta)) ? kStatusNumerical : 0u;
+    uint32_t it = 0;
+    bool cont = status == 0 && max_iter > 0 && !cg_stop(sc, delta, b_delta);
+    while (cont) {
+        // s = S A p, alpha = delta / p.s
+        T v1[1] = {D::zero()};
+        for (uint32_t row = r0 + threadIdx.x; row < r1; row += kBlock) {
+            const f3 ap = spmv(c, row, c.p);
+            const f3 s = dyn(c, row) ? ap : zero3();
+            st3(c.s, n, row, s);
+            v1[0] = D::add_term(v1[0], ld3(c.p, n, row), s);
+        }
+        team_sum<TEAM, DOT, 1>(v1, wsum, slot);
+        const double pAp = D::value(v1[0]);
+        const float alpha = DOT == 2 ? (float)(delta / pAp) : (float)delta / (float)pAp;
+        // x += alpha p, r -= alpha s, delta' = r.P^-1 r
+        T u1[1] = {D::zero()};
+        for (uint32_t row = r0 + threadIdx.x; row < r1; row += kBlock) {
+            const f3 x = ld3(c.dv, n, row) + alpha * ld3(c.p, n, row);
+            const f3 r = ld3(c.r, n, row) - alpha * ld3(c.s, n, row);
+            const f3 pv = ld3(c.pinv, n, row);
+            st3(c.dv, n, row, x);
+            st3(c.r, n, row, r);
+            u1[0] = D::add_term(u1[0], r, mk(r.x * pv.x, r.y * pv.y, r.z * pv.z));
+        }
+        team_sum<TEAM, DOT, 1>(u1, wsum, slot);
+        double dn = D::value(u1[0]);
+        float beta;
+        if (DOT == 2) {
+            beta = (float)(dn / delta);
+        } else {
+            dn = (double)(float)dn;
+            beta = (float)dn / (float)delta;
+        }
+        delta = dn;
+        ++it;
+        if (!isfinite(dn) || !isfinite(alpha) || !isfinite(beta)) status = kStatusNumerical;
+        cont = status == 0 && it < max_iter && !cg_stop(sc, dn, b_delta);
+        if (!cont) break;
+        // p = S (P^-1 r + beta p)
+        for (uint32_t row = r0 + threadIdx.x; row < r1; row += kBlock) {
+            const f3 r = ld3(c.r, n, row);
+            const f3 pv = ld3(c.pinv, n, row);
+            const f3 hv = mk(r.x * pv.x, r.y * pv.y, r.z * pv.z);
+            st3(c.p, n, row, dyn(c, row) ? hv + beta * ld3(c.p, n, row) : zero3());
+        }
+        Team<TEAM>::sync();
+    }
+    if (Team<TEAM>::rank() == 0 && threadIdx.x == 0) {
+        sc->b_delta = b_delta;
+        sc->delta0 = delta0;
+        sc->delta = delta;
+        sc->iter = it;
+        sc->status = status;
+        sc->cont = 0;
+    }
+}
+
+// One persistent launch with clusters of T CTAs.  A task is either one
+// large cloth split over the cluster's T CTAs (team_cg<T>) or up to T small
+// cloths, one per CTA (team_cg<1>, block-per-instance).  The host orders the
+// tasks largest first; clusters take them from a queue.
+template <int T>
+__global__ void __launch_bounds__(kBlock) k_batch_cg(const __grid_constant__ BatchCgArgs a)
+{
+    __shared__ double wsum[2 * kWarps];
+    __shared__ double slot[2];
+    __shared__ uint32_t item;
+    for (;;) {
+        if (threadIdx.x == 0 && Team<T>::rank() == 0) item = atomicAdd(a.next, 1u);
+        Team<T>::sync();
+        uint32_t k;
+        if (T == 1) k = item;
+        else k = *cgx::this_cluster().map_shared_rank(&item, 0);
+        Team<T>::sync();
+        if (k >= a.ntasks) break;
+        const uint2 task = a.tasks[k];  // (first index into order, count); count 0 = split
+        if (task.y == 0) {
+            const ClothDev& c = a.descs[a.order[task.x]];
+            const int dot = c.sc->dot;
+            if (dot == 2) team_cg<T, 2>(c, wsum, slot);
+            else if (dot == 1) team_cg<T, 1>(c, reinterpret_cast<CompF*>(wsum), reinterpret_cast<CompF*>(slot));
+            else team_cg<T, 0>(c, reinterpret_cast<float*>(wsum), reinterpret_cast<float*>(slot));
+        } else {
+            const uint32_t r = Team<T>::rank();
+            if (r < task.y) {
+                const ClothDev& c = a.descs[a.order[task.x + r]];
+                const int dot = c.sc->dot;
+                if (dot == 2) team_cg<1, 2>(c, wsum, slot);
+                else if (dot == 1)
+                    team_cg<1, 1>(c, reinterpret_cast<CompF*>(wsum), reinterpret_cast<CompF*>(slot));
+                else team_cg<1, 0>(c, reinterpret_cast<float*>(wsum), reinterpret_cast<float*>(slot));
+            }
+        }
+        Team<T>::sync();
+    }
+}
+
+}  // namespace
+
+int batch_team_max_blocks(int team)
+{
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void* fn = team == 1 ? (const void*)k_batch_cg<1> : team == 2 ? (const void*)k_batch_cg<2>
+                   : team == 4 ? (const void*)k_batch_cg<4> : (const void*)k_batch_cg<8>;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    return sms * per_sm;
+}
+
+cudaError_t launch_batch_cg(const BatchCgArgs& a, int team, int grid_blocks, cudaStream_t st)
+{
+    if (!a.ntasks) return cudaSuccess;
+    int blocks = grid_blocks > 0 ? grid_blocks : batch_team_max_blocks(team);
+    blocks = (blocks / team) * team;
+    const int teams_needed = (int)a.ntasks;
+    if (blocks / team > teams_needed) blocks = teams_needed * team;
+    if (blocks < team) blocks = team;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = team;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e;
+    switch (team) {
+        case 1: e = cudaLaunchKernelEx(&cfg, k_batch_cg<1>, a); break;
+        case 2: e = cudaLaunchKernelEx(&cfg, k_batch_cg<2>, a); break;
+        case 4: e = cudaLaunchKernelEx(&cfg, k_batch_cg<4>, a); break;
+        case 8: e = cudaLaunchKernelEx(&cfg, k_batch_cg<8>, a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    return e;
+}
+
+}  // namespace b3g

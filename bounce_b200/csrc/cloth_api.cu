@@ -10,22 +10,11 @@
 #include "../../include/b3g.h"
 #include "cloth_dev.cuh"
 #include "topology.h"
+#include "cloth_internal.h"
 
 using namespace b3g;
 
 namespace {
-
-// One device arena per cloth, carved into 256-byte aligned buffers.
-struct Arena {
-    char* base = nullptr;
-    size_t size = 0, used = 0;
-    template <class T> T* take(size_t count)
-    {
-        size_t off = (used + 255) & ~size_t(255);
-        used = off + count * sizeof(T);
-        return reinterpret_cast<T*>(base + off);
-    }
-};
 
 b3g_status from_cuda(cudaError_t e)
 {
@@ -44,41 +33,9 @@ b3g_status from_cuda(cudaError_t e)
 
 }  // namespace
 
-struct b3g_cloth {
-    int device = 0;
-    cudaStream_t stream = nullptr, body_stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    Arena arena;
-    ClothDev dev{};
-    ClothTopology topo;
-    float gravity[3] = {0.0f, 0.0f, 0.0f};
-    b3g_solver_opts opts{B3G_STOP_REFERENCE, 0.0f, 20u, B3G_DOT_F32};
-    uint32_t step_index = 0;
-    int assemble_block = 128;
-
-    // pinned staging
-    StepScalars* h_sc = nullptr;
-    ParticleOp* h_ops = nullptr;
-    uint32_t ops_cap = 0;
-    std::vector<ParticleOp> pending;
-    ParticleOp* d_ops = nullptr;
-    uint32_t d_ops_cap = 0;
-    float* d_stage = nullptr;  // 3 n floats for array uploads
-    uint8_t* d_stage_u8 = nullptr;
-
-    // graph cache
-    cudaGraphExec_t exec = nullptr;
-    int graph_dot = -1;
-    uint32_t graph_pos_iters = UINT32_MAX;
-    uint32_t graph_nsph = UINT32_MAX;
-    bool graph_ok = true;
-
-    b3g_step_stats last{};
-};
-
-namespace {
-
-b3g_status flush_ops(b3g_cloth* c)
+// Applies the queued particle edits on stream `st` (the cloth's own stream
+// by default).
+b3g_status flush_ops_on(b3g_cloth* c, cudaStream_t st)
 {
     if (c->pending.empty()) return B3G_OK;
     uint32_t cnt = (uint32_t)c->pending.size();
@@ -94,12 +51,47 @@ b3g_status flush_ops(b3g_cloth* c)
     }
     // The pinned buffer may still be read by an earlier copy.
     B3G_TRY(cudaStreamSynchronize(c->stream));
+    if (st != c->stream) B3G_TRY(cudaStreamSynchronize(st));
     std::memcpy(c->h_ops, c->pending.data(), cnt * sizeof(ParticleOp));
-    B3G_TRY(cudaMemcpyAsync(c->d_ops, c->h_ops, cnt * sizeof(ParticleOp), cudaMemcpyHostToDevice, c->stream));
-    B3G_TRY(launch_particle_ops(c->dev, c->d_ops, cnt, c->stream));
+    B3G_TRY(cudaMemcpyAsync(c->d_ops, c->h_ops, cnt * sizeof(ParticleOp), cudaMemcpyHostToDevice, st));
+    B3G_TRY(launch_particle_ops(c->dev, c->d_ops, cnt, st));
     c->pending.clear();
     return B3G_OK;
 }
+
+// Step parameters of the next step of cloth c (b3Cloth::Step arguments,
+// gravity, solver options); advances the cloth's step counter.
+void fill_step_scalars(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, StepScalars* h)
+{
+    std::memset(h, 0, sizeof(StepScalars));
+    h->dt = dt;
+    h->vel_iters = vel_iters;
+    h->pos_iters = pos_iters;
+    h->step_index = ++c->step_index;
+    h->max_iter = c->opts.max_iterations;
+    h->stop_rule = (int)c->opts.stop_rule;
+    h->tol = c->opts.tolerance;
+    h->dot = (int)c->opts.dot;
+    h->gx = c->gravity[0];
+    h->gy = c->gravity[1];
+    h->gz = c->gravity[2];
+}
+
+void record_stats(b3g_cloth* c, const StepScalars& h, float ms, bool solved)
+{
+    b3g_step_stats& L = c->last;
+    L.iterations = solved ? h.iter : 0;
+    L.delta0 = h.delta0;
+    L.delta = h.delta;
+    L.b_delta = h.b_delta;
+    L.active_contacts = h.active_contacts;
+    L.contacts = h.contacts;
+    L.step_ms = ms;
+}
+
+namespace {
+
+b3g_status flush_ops(b3g_cloth* c) { return flush_ops_on(c, c->stream); }
 
 void destroy_graph(b3g_cloth* c)
 {
@@ -151,8 +143,8 @@ b3g_status build_graph(b3g_cloth* c, uint32_t pos_iters)
         if (e2 != cudaSuccess) { err = e2; break; }
         if (e3 != cudaSuccess) { err = e3; break; }
         if ((err = launch_finalize(c->dev, st)) != cudaSuccess) break;
-        for (uint32_t k = 1; k < pos_iters; ++k)
-            if ((err = launch_contact_position(c->dev, st)) != cudaSuccess) break;
+        for (uint32_t k = 1; k < pos_iters && k < (uint32_t)kMaxPosIters; ++k)
+            if ((err = launch_contact_position(c->dev, k, st)) != cudaSuccess) break;
         if (err != cudaSuccess) break;
         if ((err = launch_post(c->dev, st)) != cudaSuccess) break;
     } while (0);
@@ -184,7 +176,8 @@ b3g_status launch_step_plain(b3g_cloth* c, uint32_t pos_iters)
     B3G_TRY(launch_cg_init(c->dev, dot, none, 0, st));
     for (uint32_t k = 0; k < c->opts.max_iterations; ++k) B3G_TRY(launch_cg_iteration(c->dev, dot, none, 0, st));
     B3G_TRY(launch_finalize(c->dev, st));
-    for (uint32_t k = 1; k < pos_iters; ++k) B3G_TRY(launch_contact_position(c->dev, st));
+    for (uint32_t k = 1; k < pos_iters && k < (uint32_t)kMaxPosIters; ++k)
+        B3G_TRY(launch_contact_position(c->dev, k, st));
     B3G_TRY(launch_post(c->dev, st));
     return B3G_OK;
 }
@@ -627,7 +620,6 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
     h->gx = c->gravity[0];
     h->gy = c->gravity[1];
     h->gz = c->gravity[2];
-    h->pos_solved = 1;
     B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, st));
     B3G_TRY(cudaEventRecord(c->ev0, st));
     if (dt > 0.0f) {
@@ -710,7 +702,6 @@ b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, u
     h->gx = c->gravity[0];
     h->gy = c->gravity[1];
     h->gz = c->gravity[2];
-    h->pos_solved = 1;
     B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, st));
     std::memset(times, 0, sizeof(*times));
     const int dot = (int)c->opts.dot;
@@ -739,8 +730,9 @@ b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, u
         times->cg_iterations += 1;
     }
     if ((s = timed(&times->finalize_ms, [&] { return launch_finalize(c->dev, st); }))) return s;
-    for (uint32_t k = 1; c->dev.nsph && k < pos_iters; ++k) {
-        if ((s = timed(&times->contact_position_ms, [&] { return launch_contact_position(c->dev, st); }))) return s;
+    for (uint32_t k = 1; c->dev.nsph && k < pos_iters && k < (uint32_t)kMaxPosIters; ++k) {
+        if ((s = timed(&times->contact_position_ms, [&] { return launch_contact_position(c->dev, k, st); })))
+            return s;
         times->contact_position_launches += 1;
     }
     if ((s = timed(&times->post_ms, [&] { return launch_post(c->dev, st); }))) return s;

@@ -27,6 +27,7 @@ namespace b3g {
 
 constexpr int kMaxSpheres = 4;
 constexpr int kSlice = 32;
+constexpr int kMaxPosIters = 16;
 
 // Device scalars of one cloth's step (CG state, reductions, contact flags).
 struct StepScalars {
@@ -41,9 +42,9 @@ struct StepScalars {
     uint32_t status;    // 0 ok, else b3g_status
     // last-block counters of the grid reductions
     uint32_t ticket[4];
-    // contacts
-    float min_sep;
-    uint32_t pos_solved;
+    // contacts: smallest separation of each position iteration, as
+    // order-preserving ints (0 = nothing below zero)
+    int min_sep[kMaxPosIters];
     uint32_t active_contacts;
     uint32_t contacts;
     // step parameters (written by the host before each step)
@@ -105,6 +106,20 @@ struct ClothDev {
     uint32_t block;             // threads of the row kernels
 };
 
+// A launch over several cloths: global thread g works on row
+// g - prefix[k] of descs[k], where prefix[k] <= g < prefix[k + 1].
+struct RowSpan {
+    const ClothDev* descs;      // device array of count cloth descriptors
+    const uint32_t* prefix;     // device array of count + 1 row offsets
+    uint32_t count, total, max_deg;
+};
+
+cudaError_t launch_span_contacts_update(const RowSpan& sp, cudaStream_t st);
+cudaError_t launch_span_assemble(const RowSpan& sp, int block, cudaStream_t st);
+cudaError_t launch_span_finalize(const RowSpan& sp, cudaStream_t st);
+cudaError_t launch_span_contact_position(const RowSpan& sp, uint32_t it, cudaStream_t st);
+cudaError_t launch_span_post(const RowSpan& sp, cudaStream_t st);
+
 // Host launchers (cloth_kernels.cu).  The assembly kernel needs
 // assemble_smem_bytes() of dynamic shared memory.
 size_t assemble_smem_bytes(const ClothDev& c, int block);
@@ -120,7 +135,7 @@ cudaError_t launch_cg_iteration(const ClothDev& c, int dot, cudaGraphConditional
 // The three kernels of one CG iteration, one at a time (profiling).
 cudaError_t launch_cg_part(const ClothDev& c, int dot, int part, cudaStream_t st);
 cudaError_t launch_finalize(const ClothDev& c, cudaStream_t st);
-cudaError_t launch_contact_position(const ClothDev& c, cudaStream_t st);
+cudaError_t launch_contact_position(const ClothDev& c, uint32_t it, cudaStream_t st);
 cudaError_t launch_post(const ClothDev& c, cudaStream_t st);
 
 // Sequential particle edits (set type / position / velocity, apply force /

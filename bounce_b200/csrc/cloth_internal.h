@@ -1,0 +1,62 @@
+// The cloth handle behind the C ABI, shared by cloth_api.cu and batch_api.cu.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/b3g.h"
+#include "cloth_dev.cuh"
+#include "topology.h"
+
+namespace b3g {
+
+// One device arena per cloth, carved into 256-byte aligned buffers.
+struct Arena {
+    char* base = nullptr;
+    size_t size = 0, used = 0;
+    template <class T> T* take(size_t count)
+    {
+        size_t off = (used + 255) & ~size_t(255);
+        used = off + count * sizeof(T);
+        return reinterpret_cast<T*>(base + off);
+    }
+};
+
+}  // namespace b3g
+
+struct b3g_cloth {
+    int device = 0;
+    cudaStream_t stream = nullptr, body_stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    b3g::Arena arena;
+    b3g::ClothDev dev{};
+    b3g::ClothTopology topo;
+    float gravity[3] = {0.0f, 0.0f, 0.0f};
+    b3g_solver_opts opts{B3G_STOP_REFERENCE, 0.0f, 20u, B3G_DOT_F32};
+    uint32_t step_index = 0;
+    int assemble_block = 128;
+
+    // pinned staging
+    b3g::StepScalars* h_sc = nullptr;
+    b3g::ParticleOp* h_ops = nullptr;
+    uint32_t ops_cap = 0;
+    std::vector<b3g::ParticleOp> pending;
+    b3g::ParticleOp* d_ops = nullptr;
+    uint32_t d_ops_cap = 0;
+    float* d_stage = nullptr;  // 3 n floats for array uploads
+    uint8_t* d_stage_u8 = nullptr;
+
+    // graph cache
+    cudaGraphExec_t exec = nullptr;
+    int graph_dot = -1;
+    uint32_t graph_pos_iters = UINT32_MAX;
+    uint32_t graph_nsph = UINT32_MAX;
+    bool graph_ok = true;
+
+    b3g_step_stats last{};
+};
+
+
+b3g_status flush_ops_on(b3g_cloth* c, cudaStream_t st);
+void fill_step_scalars(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, b3g::StepScalars* h);
+void record_stats(b3g_cloth* c, const b3g::StepScalars& h, float ms, bool solved);

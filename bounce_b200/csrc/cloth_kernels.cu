@@ -83,6 +83,52 @@ __device__ __forceinline__ f3 spmv_row(const ClothDev& c, uint32_t row, const fl
 __device__ __forceinline__ bool is_dynamic(const ClothDev& c, uint32_t i) { return c.type[i] == 2; }
 
 // ---------------------------------------------------------------------------
+// one cloth or many: thread -> (cloth, row)
+// ---------------------------------------------------------------------------
+
+// Single-cloth launches read the cloth from the kernel parameter; launches
+// over many cloths find the cloth of global thread g in the span's prefix sums
+// of row counts (prefix[k] <= g < prefix[k + 1]).
+template <bool MULTI>
+__device__ __forceinline__ bool resolve(const ClothDev& one, const RowSpan& sp, uint32_t g, const ClothDev*& c,
+                                        uint32_t& row)
+{
+    if (!MULTI) {
+        c = &one;
+        row = g;
+        return g < one.n;
+    }
+    if (g >= sp.total) return false;
+    uint32_t lo = 0, hi = sp.count;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(sp.prefix + mid) <= g) lo = mid;
+        else hi = mid;
+    }
+    c = sp.descs + lo;
+    row = g - __ldg(sp.prefix + lo);
+    return true;
+}
+
+// Adds v to *addr once per group of lanes that share addr (warp-aggregated,
+// integer, so the total does not depend on the order).  Every lane of the
+// warp must call it; lanes with nothing to add pass addr == nullptr.
+__device__ __forceinline__ void warp_add(uint32_t* addr, uint32_t v)
+{
+    const unsigned grp = __match_any_sync(0xffffffffu, (unsigned long long)addr);
+    const uint32_t sum = __reduce_add_sync(grp, v);
+    if (addr && sum && (threadIdx.x & 31u) == (unsigned)(__ffs(grp) - 1)) atomicAdd(addr, sum);
+}
+
+// Order-preserving float <-> int for atomicMin on separations.
+__device__ __forceinline__ int ord_enc(float f)
+{
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float ord_dec(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+// ---------------------------------------------------------------------------
 // assembly
 // ---------------------------------------------------------------------------
 
@@ -253,12 +299,17 @@ __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn,
     }
 }
 
-__global__ void __launch_bounds__(128) k_assemble(ClothDev c)
+template <bool MULTI>
+__global__ void __launch_bounds__(128) k_assemble(const __grid_constant__ ClothDev one,
+                                                  const __grid_constant__ RowSpan span)
 {
     extern __shared__ float smem[];
     const int B = blockDim.x, tid = threadIdx.x;
-    const uint32_t row = blockIdx.x * B + tid;
-    if (row >= c.n) return;
+    const ClothDev* cp;
+    uint32_t row;
+    if (!resolve<MULTI>(one, span, blockIdx.x * B + tid, cp, row)) return;
+    const ClothDev& c = *cp;
+    const uint32_t max_deg = MULTI ? span.max_deg : one.max_deg;
     const StepScalars* sc = c.sc;
     const float h = sc->dt;
     const float hh = h * h;
@@ -266,7 +317,7 @@ __global__ void __launch_bounds__(128) k_assemble(ClothDev c)
 
     RowAcc acc;
     acc.base = smem;
-    acc.touch = reinterpret_cast<uint8_t*>(smem + (size_t)c.max_deg * 18 * B);
+    acc.touch = reinterpret_cast<uint8_t*>(smem + (size_t)max_deg * 18 * B);
     acc.B = B;
     acc.tid = tid;
     const int deg = c.row_deg[row];
@@ -486,10 +537,14 @@ __device__ __forceinline__ void load_fat(const ClothDev& c, uint32_t i, float* l
 // UpdateBodyContacts + b3ParticleBodyContact::Update with TestSphere
 // (cloth_contact_manager.cpp:277-315, cloth_particle_body_contact.cpp:24-47,
 // sphere_shape.cpp:71-95)
-__global__ void k_contacts_update(ClothDev c)
+template <bool MULTI>
+__global__ void k_contacts_update(const __grid_constant__ ClothDev one, const __grid_constant__ RowSpan span)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
+    const ClothDev* cp;
+    uint32_t i;
+    if (!resolve<MULTI>(one, span, blockIdx.x * blockDim.x + threadIdx.x, cp, i)) return;
+    const ClothDev& c = *cp;
+    if (!c.nsph) return;
     const uint32_t n = c.n, nn = c.nsph * n;
     float lo[3], hi[3];
     load_fat(c, i, lo, hi);
@@ -571,66 +626,30 @@ __device__ float position_iteration(const ClothDev& c, uint32_t i, f3& pos, cons
     return min_sep;
 }
 
-__device__ void min_reduce_flag(const ClothDev& c, float local_min, uint32_t active)
+// v += dv; x += y; m_x = dv; contact solve (cloth_solver.cpp:95-164).  The
+// smallest separation of the first position iteration goes to
+// StepScalars::min_sep[0] (atomicMin, order-independent).
+template <bool MULTI>
+__global__ void k_finalize(const __grid_constant__ ClothDev one, const __grid_constant__ RowSpan span)
 {
-    __shared__ float smin[32];
-    __shared__ uint32_t scnt[32];
-    __shared__ bool last;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int off = 16; off > 0; off >>= 1) {
-        local_min = fminf(local_min, __shfl_down_sync(0xffffffffu, local_min, off));
-        active += __shfl_down_sync(0xffffffffu, active, off);
-    }
-    if (lane == 0) {
-        smin[warp] = local_min;
-        scnt[warp] = active;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float m = 0.0f;
-        uint32_t a = 0;
-        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) {
-            m = fminf(m, smin[w]);
-            a += scnt[w];
-        }
-        float* part = reinterpret_cast<float*>(c.partials);
-        part[blockIdx.x] = m;
-        if (a) atomicAdd(&c.sc->active_contacts, a);
-        __threadfence();
-        unsigned t = atomicAdd(&c.sc->ticket[3], 1u);
-        last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        const volatile float* part = reinterpret_cast<const volatile float*>(c.partials);
-        float m = 0.0f;
-        for (uint32_t b = 0; b < gridDim.x; ++b) m = fminf(m, part[b]);
-        c.sc->min_sep = m;
-        // cloth_solver.cpp:151-164: stop once every contact is within 3 slops
-        c.sc->pos_solved = m >= -3.0f * kLinearSlop ? 1u : 0u;
-        c.sc->ticket[3] = 0u;
-    }
-}
-
-// v += dv; x += y; m_x = dv; contact solve (cloth_solver.cpp:95-164)
-__global__ void k_finalize(ClothDev c)
-{
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = c.n, nn = c.nsph * n;
-    const StepScalars* sc = c.sc;
-    const float h = sc->dt;
-    float local_min = 0.0f;
+    const ClothDev* cp;
+    uint32_t i;
+    uint32_t* count_addr = nullptr;
     uint32_t active = 0;
-    if (i < n) {
+    if (resolve<MULTI>(one, span, blockIdx.x * blockDim.x + threadIdx.x, cp, i)) {
+        const ClothDev& c = *cp;
+        const uint32_t n = c.n, nn = c.nsph * n;
+        StepScalars* sc = c.sc;
+        const float h = sc->dt;
         const f3 dv = ld3(c.dv, n, i);
         f3 vel = ld3(c.v, n, i) + dv;
         f3 pos = ld3(c.x, n, i) + ld3(c.y, n, i);
         st3(c.mx, n, i, dv);
         int order[kMaxSpheres];
         const int k = c.nsph ? contact_order(c, i, order) : 0;
-        active = (uint32_t)k;
         if (k > 0) {
+            active = (uint32_t)k;
+            count_addr = &sc->active_contacts;
             const float mA = 1.0f / c.mass[i];
             // InitializeBodyContactConstraints (cloth_contact_solver.cpp:54-177), static body
             float nmass[kMaxSpheres], tm_xx[kMaxSpheres], tm_xy[kMaxSpheres], tm_yx[kMaxSpheres],
@@ -712,31 +731,37 @@ __global__ void k_finalize(ClothDev c)
         }
         // integrate positions (cloth_solver.cpp:143-147)
         pos = pos + h * vel;
-        if (k > 0 && sc->pos_iters > 0) local_min = position_iteration(c, i, pos, order, k);
+        if (k > 0 && sc->pos_iters > 0) {
+            const float ms = position_iteration(c, i, pos, order, k);
+            if (ms < 0.0f) atomicMin(&sc->min_sep[0], ord_enc(ms));
+        }
         st3(c.x, n, i, pos);
         st3(c.v, n, i, vel);
     }
-    if (c.nsph) min_reduce_flag(c, local_min, active);
+    warp_add(count_addr, active);
 }
 
-// A later position iteration, run only while the previous ones left a
-// contact deeper than 3 slops (cloth_solver.cpp:151-164).
-__global__ void k_contact_position(ClothDev c)
+// Position iteration `it` (>= 1), run for a cloth only while iteration it - 1
+// left a contact deeper than 3 slops (cloth_solver.cpp:151-164).
+template <bool MULTI>
+__global__ void k_contact_position(const __grid_constant__ ClothDev one, const __grid_constant__ RowSpan span,
+                                   uint32_t it)
 {
-    if (c.sc->pos_solved) return;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = c.n;
-    float local_min = 0.0f;
-    if (i < n) {
-        int order[kMaxSpheres];
-        const int k = contact_order(c, i, order);
-        if (k > 0) {
-            f3 pos = ld3(c.x, n, i);
-            local_min = position_iteration(c, i, pos, order, k);
-            st3(c.x, n, i, pos);
-        }
+    const ClothDev* cp;
+    uint32_t i;
+    if (!resolve<MULTI>(one, span, blockIdx.x * blockDim.x + threadIdx.x, cp, i)) return;
+    const ClothDev& c = *cp;
+    StepScalars* sc = c.sc;
+    if (!c.nsph || it >= sc->pos_iters || it >= kMaxPosIters) return;
+    if (ord_dec(sc->min_sep[it - 1]) >= -3.0f * kLinearSlop) return;
+    int order[kMaxSpheres];
+    const int k = contact_order(c, i, order);
+    if (k > 0) {
+        f3 pos = ld3(c.x, c.n, i);
+        const float ms = position_iteration(c, i, pos, order, k);
+        st3(c.x, c.n, i, pos);
+        if (ms < 0.0f) atomicMin(&sc->min_sep[it], ord_enc(ms));
     }
-    min_reduce_flag(c, local_min, 0u);
 }
 
 __device__ void move_proxy_dev(const ClothDev& c, uint32_t i, f3 disp)
@@ -764,13 +789,17 @@ __device__ void move_proxy_dev(const ClothDev& c, uint32_t i, f3 disp)
 
 // Clear f and y, sync the particle AABB (b3BroadPhase::MoveProxy,
 // broad_phase.cpp:99-149), new body contacts (cloth_contact_manager.cpp:64-123).
-__global__ void k_post(ClothDev c)
+template <bool MULTI>
+__global__ void k_post(const __grid_constant__ ClothDev one, const __grid_constant__ RowSpan span)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = c.n, nn = c.nsph * n;
-    const StepScalars* sc = c.sc;
+    const ClothDev* cp;
+    uint32_t i;
     uint32_t alive = 0;
-    if (i < n) {
+    uint32_t* count_addr = nullptr;
+    if (resolve<MULTI>(one, span, blockIdx.x * blockDim.x + threadIdx.x, cp, i)) {
+        const ClothDev& c = *cp;
+        const uint32_t n = c.n, nn = c.nsph * n;
+        const StepScalars* sc = c.sc;
         st3(c.fext, n, i, zero3());
         st3(c.y, n, i, zero3());
         move_proxy_dev(c, i, sc->dt * ld3(c.v, n, i));
@@ -789,11 +818,9 @@ __global__ void k_post(ClothDev c)
             }
             alive += c.c_exists[q];
         }
+        if (alive) count_addr = &c.sc->contacts;
     }
-    if (c.nsph) {
-        for (int off = 16; off > 0; off >>= 1) alive += __shfl_down_sync(0xffffffffu, alive, off);
-        if ((threadIdx.x & 31) == 0 && alive) atomicAdd(&c.sc->contacts, alive);
-    }
+    warp_add(count_addr, alive);
 }
 
 // ---------------------------------------------------------------------------
@@ -888,10 +915,12 @@ size_t assemble_smem_bytes(const ClothDev& c, int block)
     return (size_t)c.max_deg * 18 * sizeof(float) * block + (size_t)c.max_deg * block;
 }
 
+static const RowSpan kNoSpan{};
+
 cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st)
 {
     if (!c.nsph) return cudaSuccess;
-    k_contacts_update<<<blocks_for(c.n, 256), 256, 0, st>>>(c);
+    k_contacts_update<false><<<blocks_for(c.n, 256), 256, 0, st>>>(c, kNoSpan);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -899,9 +928,9 @@ cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st)
 cudaError_t launch_assemble(const ClothDev& c, int block, cudaStream_t st)
 {
     const size_t smem = assemble_smem_bytes(c, block);
-    cudaError_t e = cudaFuncSetAttribute(k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_assemble<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_assemble<<<blocks_for(c.n, block), block, smem, st>>>(c);
+    k_assemble<false><<<blocks_for(c.n, block), block, smem, st>>>(c, kNoSpan);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -954,22 +983,68 @@ cudaError_t launch_cg_part(const ClothDev& c, int dot, int part, cudaStream_t st
 
 cudaError_t launch_finalize(const ClothDev& c, cudaStream_t st)
 {
-    k_finalize<<<blocks_for(c.n, 256), 256, 0, st>>>(c);
+    k_finalize<false><<<blocks_for(c.n, 256), 256, 0, st>>>(c, kNoSpan);
     count_launches(1);
     return cudaGetLastError();
 }
 
-cudaError_t launch_contact_position(const ClothDev& c, cudaStream_t st)
+cudaError_t launch_contact_position(const ClothDev& c, uint32_t it, cudaStream_t st)
 {
     if (!c.nsph) return cudaSuccess;
-    k_contact_position<<<blocks_for(c.n, 256), 256, 0, st>>>(c);
+    k_contact_position<false><<<blocks_for(c.n, 256), 256, 0, st>>>(c, kNoSpan, it);
     count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_post(const ClothDev& c, cudaStream_t st)
 {
-    k_post<<<blocks_for(c.n, 256), 256, 0, st>>>(c);
+    k_post<false><<<blocks_for(c.n, 256), 256, 0, st>>>(c, kNoSpan);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+// ---- launches over many cloths ----
+static ClothDev g_unused_one{};
+
+cudaError_t launch_span_contacts_update(const RowSpan& sp, cudaStream_t st)
+{
+    if (!sp.total) return cudaSuccess;
+    k_contacts_update<true><<<blocks_for(sp.total, 256), 256, 0, st>>>(g_unused_one, sp);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_span_assemble(const RowSpan& sp, int block, cudaStream_t st)
+{
+    if (!sp.total) return cudaSuccess;
+    const size_t smem = (size_t)sp.max_deg * 18 * sizeof(float) * block + (size_t)sp.max_deg * block;
+    cudaError_t e = cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_assemble<true><<<blocks_for(sp.total, block), block, smem, st>>>(g_unused_one, sp);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_span_finalize(const RowSpan& sp, cudaStream_t st)
+{
+    if (!sp.total) return cudaSuccess;
+    k_finalize<true><<<blocks_for(sp.total, 256), 256, 0, st>>>(g_unused_one, sp);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_span_contact_position(const RowSpan& sp, uint32_t it, cudaStream_t st)
+{
+    if (!sp.total) return cudaSuccess;
+    k_contact_position<true><<<blocks_for(sp.total, 256), 256, 0, st>>>(g_unused_one, sp, it);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_span_post(const RowSpan& sp, cudaStream_t st)
+{
+    if (!sp.total) return cudaSuccess;
+    k_post<true><<<blocks_for(sp.total, 256), 256, 0, st>>>(g_unused_one, sp);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -234,6 +234,51 @@ b3g_status b3g_mpcg_solve_noalloc(uint32_t n, const uint32_t* rowptr, const uint
                                   const float* b, const float* S, const float* x0, const b3g_solver_opts* opts,
                                   float* x, uint32_t* iterations, b3g_step_stats* stats, void* stream);
 
+/* ---- batches: many cloths per launch ---------------------------------------- */
+
+/* No single reference counterpart: the reference steps each b3Cloth on its
+ * own (b3Cloth::Step).  A batch advances many cloths -- of uneven sizes,
+ * each with its own parameters, solver options and colliders -- by one
+ * b3Cloth::Step each, in a fixed number of launches captured in a CUDA
+ * graph: the per-row kernels cover every row of every cloth, the CG is one
+ * persistent launch that runs one cloth per CTA (block-per-instance) or per
+ * thread-block cluster (split-instance).  Each cloth's results are the same
+ * as when it is stepped alone in the same batch object (fixed reduction
+ * trees per cloth). */
+typedef struct b3g_batch b3g_batch;
+
+typedef struct {
+    uint32_t cluster;          /* CTAs per cluster of the CG launch: 1, 2, 4 or 8 */
+    uint8_t split_class[32];   /* per size class floor(log2(vertices)): 1 = split over a cluster */
+    float tuned_cg_ms;         /* CG time the autotuner measured for this schedule */
+} b3g_batch_schedule;
+
+typedef struct {
+    uint32_t count;                /* cloths stepped */
+    uint32_t rows;                 /* their vertices */
+    uint32_t tasks;                /* CG work items */
+    uint32_t cg_iterations_total;
+    uint32_t cg_iterations_max;
+    float step_ms;                 /* device time of the whole batch step (CUDA events) */
+} b3g_batch_stats;
+
+/* capacity: most cloths one step call may pass */
+b3g_status b3g_batch_create(int device, uint32_t capacity, b3g_batch** out);
+b3g_status b3g_batch_destroy(b3g_batch* batch);
+/* One b3Cloth::Step (dt, velocity and position iterations) of each listed
+ * cloth; per_cloth (count entries) and stats may be NULL.  A cloth may be
+ * listed once per call; all must live on the batch's device. */
+b3g_status b3g_batch_step(b3g_batch* batch, b3g_cloth* const* cloths, uint32_t count, float dt,
+                          uint32_t velocity_iterations, uint32_t position_iterations,
+                          b3g_step_stats* per_cloth, b3g_batch_stats* stats);
+b3g_status b3g_batch_set_schedule(b3g_batch* batch, const b3g_batch_schedule* schedule);
+b3g_status b3g_batch_get_schedule(const b3g_batch* batch, b3g_batch_schedule* schedule);
+/* Project autotuner: times the batched CG on these cloths' current systems
+ * for cluster sizes 1/2/4/8 and, per size class, block-per-instance against
+ * split-instance; keeps the fastest schedule.  Cloth state is not changed. */
+b3g_status b3g_batch_autotune(b3g_batch* batch, b3g_cloth* const* cloths, uint32_t count, float dt,
+                              b3g_batch_schedule* out);
+
 /* ---- misc ----------------------------------------------------------------- */
 
 const char* b3g_status_string(b3g_status status);
