@@ -42,6 +42,11 @@ def parse():
     ap.add_argument("--side", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=3)
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--skip-batch", action="store_true")
+    ap.add_argument("--skip-serve", action="store_true")
     return ap.parse_args()
 
 
@@ -123,6 +128,10 @@ def algorithmic_bytes(info: dict, kernel: str) -> float:
         return (3 * 12 + 12 + 1) * n
     if kernel == "cg_init":
         return 40.0 * blocks + (12 * 3 + 1 + 3 * 12) * n
+    if kernel.startswith("grid_cg"):
+        # the whole persistent solve: init + per iteration SpMV, update, direction
+        iters = float(kernel.split(":")[1])
+        return 40.0 * blocks + 73.0 * n + iters * (40.0 * blocks + (26 + 84 + 49) * n)
     if kernel == "assemble":
         inc = 3 * t + 2 * s
         return 36.0 * blocks + (24 + 24 + 4 + 1 + 24) * n + 40.0 * t + 24.0 * s + 8.0 * inc
@@ -138,6 +147,7 @@ def run_ours(args, rank, world):
     scene = b3g.sphere_scene(args.side, seed=2 + rank)
     opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
     cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene, opts)
+    cloth.set_cg_strategy(True)  # whole solve in one persistent cooperative launch
     info = cloth.info()
     n = info["vertices"]
     # L2 flush buffer (> 126 MB L2), written between timed steps
@@ -192,7 +202,10 @@ def run_ours(args, rank, world):
         flush.zero_()
         torch.cuda.synchronize()
         prof.append(cloth.step_profiled(scene.dt, scene.velocity_iterations, scene.position_iterations))
+    if not prof:
+        prof.append(cloth.step_profiled(scene.dt, scene.velocity_iterations, scene.position_iterations))
     it_total = sum(p["cg_iterations"] for p in prof)
+    persistent = all(p["cg_update_ms"] == 0.0 for p in prof)
     kern = {
         "assemble": (sum(p["assemble_ms"] for p in prof), len(prof)),
         "cg_init": (sum(p["cg_init_ms"] for p in prof), len(prof)),
@@ -203,10 +216,16 @@ def run_ours(args, rank, world):
         "post": (sum(p["post_ms"] for p in prof), len(prof)),
         "contacts_update": (sum(p["contacts_update_ms"] for p in prof), len(prof)),
     }
+    if persistent:
+        # one persistent launch per step holds the whole CG
+        kern.pop("cg_update")
+        kern.pop("cg_direction")
+        kern["grid_cg"] = kern.pop("cg_spmv")
+        kern["grid_cg"] = (kern["grid_cg"][0], len(prof))
     total = sum(v[0] for v in kern.values())
     dom = max(kern, key=lambda k: kern[k][0])
     avg_ms = kern[dom][0] / kern[dom][1]
-    alg = algorithmic_bytes(info, dom)
+    alg = algorithmic_bytes(info, dom if dom != "grid_cg" else f"grid_cg:{it_total / len(prof)}")
     peak, peak_kind = peaks()
     achieved = alg / (avg_ms / 1000.0) / 1e9
     cloth.close()
@@ -220,6 +239,57 @@ def run_ours(args, rank, world):
                      "share": kern[dom][0] / total if total else None},
         "kernel_ms": {k: v[0] / v[1] for k, v in kern.items()},
     }
+
+
+def run_batched(args, dev: int):
+    """Many cloths of uneven sizes per launch: 512 cloths, side U{16..128},
+    stretch log-U[1e3, 1e5], shear log-U[1e2, 1e4], row 0 pinned; against the
+    plain one-cloth-at-a-time GPU path on the same cloths."""
+    import bounce_b200 as b3g
+
+    scenes = b3g.batch_scenes(args.batch_count, seed=3)
+    opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
+    cloths = [b3g.Cloth(sc.mesh, sc.cdef, device=dev).setup(sc, opts) for sc in scenes]
+    plain = [b3g.Cloth(sc.mesh, sc.cdef, device=dev).setup(sc, opts) for sc in scenes]
+    rows = sum(c.n for c in cloths)
+    dt = scenes[0].dt
+    batch = b3g.Batch(max(1024, len(cloths)), device=dev)
+    for _ in range(args.warmup):
+        batch.step(cloths, dt)
+    sched = batch.autotune(cloths, dt)
+    ms, iters = [], []
+    launches0 = b3g.kernel_launch_count()
+    for _ in range(args.batch_steps):
+        out = batch.step(cloths, dt)
+        ms.append(out["step_ms"])
+        iters.append(out["cg_iterations_total"] / out["count"])
+    launches = b3g.kernel_launch_count() - launches0
+    # the plain single-instance path, same cloths, same number of steps
+    for _ in range(args.warmup):
+        for c in plain:
+            c.step(dt)
+    pms = 0.0
+    for _ in range(args.batch_steps):
+        for c in plain:
+            pms += c.step(dt)["step_ms"]
+    batched = rows * len(ms) / (sum(ms) / 1000.0)
+    plain_v = rows * args.batch_steps / (pms / 1000.0)
+    for c in cloths + plain:
+        c.close()
+    batch.close()
+    return {"cloths": len(scenes), "vertices": rows, "vertex_steps_per_s": batched,
+            "ms_per_step": sum(ms) / len(ms), "plain_vertex_steps_per_s": plain_v,
+            "speedup_vs_plain": batched / plain_v, "cg_iterations_mean": float(np.mean(iters)),
+            "schedule": {"cluster": sched["cluster"],
+                         "split_size_classes": [k for k, v in enumerate(sched["split_class"]) if v]},
+            "gpu_launches": launches, "steps": len(ms),
+            "l2": "inputs larger than L2 (about 1 GB of resident cloth state)"}
+
+
+def run_serving(args, dev: int):
+    from bounce_b200 import serving
+
+    return serving.run_poisson(rate=2000.0, seconds=args.serve_seconds, budget_bytes=150 * 10**9, device=dev)
 
 
 def cpu_reference_sample(side: int, steps: int, warm: int):
@@ -287,6 +357,8 @@ def main():
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     r = run_ours(args, rank, world)
+    batched = None if args.skip_batch else run_batched(args, local)
+    served = None if args.skip_serve else run_serving(args, local)
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -309,6 +381,7 @@ def main():
         "config": {"workload": f"grid{args.side}x{args.side}_bending_sphere", "vertices": n,
                    "triangles": r["info"]["triangles"], "springs": r["info"]["springs"],
                    "blocks": r["info"]["blocks"], "cg": "relative residual 1e-4, max 200, fp64 dots",
+                   "cg_strategy": "persistent cooperative launch",
                    "contact_iterations": [8, 2], "parallelism": f"replicas{world}",
                    "l2": "flushed (256 MB write) before every timed step",
                    "cg_iterations_mean": r["iterations_mean"], "active_contacts_mean": r["active_contacts_mean"]},
@@ -318,6 +391,8 @@ def main():
         "roofline": r["roofline"],
         "kernel_ms": r["kernel_ms"],
         "cpu_baseline": base,
+        "batched": batched,
+        "serving": served,
     }
     print(json.dumps(line))
 

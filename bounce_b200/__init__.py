@@ -26,6 +26,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libb3g.so")
 
 STOP_REFERENCE, STOP_RELATIVE = 0, 1
+CG_LAUNCHES, CG_PERSISTENT = 0, 1
 DOT_F32, DOT_COMPENSATED, DOT_F64 = 0, 1, 2
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "degenerate mesh", 3: "no CUDA device", 4: "out of memory",
@@ -79,6 +80,31 @@ class BatchStatsC(C.Structure):
                 ("cg_iterations_total", C.c_uint32), ("cg_iterations_max", C.c_uint32), ("step_ms", C.c_float)]
 
 
+class ServerConfigC(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_active", C.c_uint32), ("dt", C.c_float),
+                ("velocity_iterations", C.c_uint32), ("position_iterations", C.c_uint32),
+                ("gravity", C.c_float * 3), ("solver", SolverOptsC), ("schedule", BatchScheduleC),
+                ("host_threads", C.c_uint32)]
+
+
+class ServerTickC(C.Structure):
+    _fields_ = [(k, C.c_uint32) for k in ("admitted", "stepped", "completed", "active", "queued", "rows")] + \
+               [("bytes_used", C.c_uint64), ("tick_ms", C.c_float)]
+
+
+class RequestInfoC(C.Structure):
+    _fields_ = [("state", C.c_uint32), ("status", C.c_int), ("steps_done", C.c_uint32), ("steps_total", C.c_uint32),
+                ("vertex_count", C.c_uint32), ("arrival", C.c_double), ("admitted", C.c_double),
+                ("finished", C.c_double), ("bytes", C.c_uint64)]
+
+
+class ServerStatsC(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("ticks", "steps", "vertex_steps", "admitted", "completed", "rejected")] + \
+               [("busy_ms", C.c_double), ("active", C.c_uint32), ("queued", C.c_uint32), ("peak_active", C.c_uint32),
+                ("peak_bytes", C.c_uint64), ("p50_step_ms", C.c_float), ("p99_step_ms", C.c_float),
+                ("max_step_ms", C.c_float)]
+
+
 _lib = None
 
 
@@ -121,6 +147,8 @@ def lib() -> C.CDLL:
             "b3g_cloth_read_system": [vp, C.POINTER(u32), vp, vp, vp, vp, vp, vp],
             "b3g_cloth_step_profiled": [vp, f32, u32, u32, C.POINTER(PhaseTimesC), C.POINTER(StepStatsC)],
             "b3g_cloth_get_info": [vp, C.POINTER(ClothInfoC)],
+            "b3g_cloth_set_cg_strategy": [vp, i32],
+            "b3g_debug_cg_barrier_timeout": [vp, u32, C.POINTER(i32)],
             "b3g_mpcg_solve": [u32, vp, vp, vp, vp, vp, vp, C.POINTER(SolverOptsC), vp, C.POINTER(u32),
                                C.POINTER(StepStatsC), vp],
             "b3g_batch_create": [i32, u32, C.POINTER(vp)],
@@ -129,6 +157,15 @@ def lib() -> C.CDLL:
             "b3g_batch_set_schedule": [vp, C.POINTER(BatchScheduleC)],
             "b3g_batch_get_schedule": [vp, C.POINTER(BatchScheduleC)],
             "b3g_batch_autotune": [vp, vp, u32, f32, C.POINTER(BatchScheduleC)],
+            "b3g_server_create": [i32, C.POINTER(ServerConfigC), C.POINTER(vp)],
+            "b3g_server_destroy": [vp],
+            "b3g_server_submit": [vp, C.POINTER(MeshDesc), C.POINTER(ClothDefC), vp, vp, u32, u32, C.c_double,
+                                  C.POINTER(C.c_uint64)],
+            "b3g_server_tick": [vp, C.c_double, C.POINTER(ServerTickC)],
+            "b3g_server_poll": [vp, C.c_uint64, C.POINTER(RequestInfoC)],
+            "b3g_server_result": [vp, C.c_uint64, vp],
+            "b3g_server_release": [vp, C.c_uint64],
+            "b3g_server_stats": [vp, C.POINTER(ServerStatsC)],
             "b3g_mpcg_solve_noalloc": [u32, vp, vp, vp, vp, vp, vp, C.POINTER(SolverOptsC), vp, C.POINTER(u32),
                                        C.POINTER(StepStatsC), vp],
         }
@@ -304,6 +341,10 @@ class Cloth:
         out["iterations"] = self.stats.iterations
         return out
 
+    def set_cg_strategy(self, persistent: bool) -> None:
+        """False: per-iteration launches in a graph loop; True: one persistent cooperative launch."""
+        check(lib().b3g_cloth_set_cg_strategy(self.h, 1 if persistent else 0), "set_cg_strategy")
+
     def info(self) -> dict:
         i = ClothInfoC()
         check(lib().b3g_cloth_get_info(self.h, C.byref(i)), "get_info")
@@ -427,6 +468,94 @@ class Batch:
         sc = BatchScheduleC()
         check(lib().b3g_batch_autotune(self.h, arr, len(cloths), dt, C.byref(sc)), "autotune")
         return {"cluster": sc.cluster, "split_class": list(sc.split_class), "tuned_cg_ms": sc.tuned_cg_ms}
+
+
+class Server:
+    """Continuous-batching cloth-step server (b3g_server)."""
+
+    def __init__(self, budget_bytes: int, max_active: int = 1024, dt: float = 1.0 / 60.0,
+                 velocity_iterations: int = 8, position_iterations: int = 2, gravity=(0.0, -9.8, 0.0),
+                 solver: SolverOptions | None = None, cluster: int = 1, split_classes=(), host_threads: int = 0,
+                 device: int = 0):
+        cfg = ServerConfigC()
+        cfg.hbm_budget_bytes = int(budget_bytes)
+        cfg.max_active = max_active
+        cfg.dt = dt
+        cfg.velocity_iterations = velocity_iterations
+        cfg.position_iterations = position_iterations
+        for k in range(3):
+            cfg.gravity[k] = gravity[k]
+        cfg.solver = (solver or SolverOptions.relative(1e-4, 200, DOT_F64)).as_c()
+        cfg.schedule.cluster = cluster
+        for k in split_classes:
+            cfg.schedule.split_class[k] = 1
+        cfg.host_threads = host_threads
+        h = C.c_void_p()
+        check(lib().b3g_server_create(device, C.byref(cfg), C.byref(h)), "b3g_server_create")
+        self.h = h
+        self._keep = []
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().b3g_server_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def submit(self, mesh: Mesh, cdef: ClothDef, types=None, spheres=(), steps: int = 1, arrival: float = 0.0) -> int:
+        v = np.ascontiguousarray(mesh.vertices, np.float32)
+        t = np.ascontiguousarray(mesh.triangles, np.uint32)
+        md = MeshDesc(mesh.vertex_count, _ptr(v), mesh.triangle_count, _ptr(t), 0, None)
+        d = ClothDefC(cdef.density, cdef.streching, cdef.shearing, cdef.bending, cdef.sewing, cdef.damping,
+                      cdef.thickness, cdef.friction)
+        ty = None if types is None else np.ascontiguousarray(types, np.uint8)
+        sp = np.ascontiguousarray(np.asarray([[c[0], c[1], c[2], r, mu] for (c, r, mu) in spheres], np.float32)
+                                  .reshape(-1))
+        rid = C.c_uint64(0)
+        check(lib().b3g_server_submit(self.h, C.byref(md), C.byref(d), None if ty is None else _ptr(ty),
+                                      _ptr(sp) if sp.size else None, len(spheres), steps, arrival, C.byref(rid)),
+              "server_submit")
+        return rid.value
+
+    def submit_scene(self, scene: Scene, steps: int, arrival: float = 0.0) -> int:
+        types = np.full(scene.mesh.vertex_count, DYNAMIC, np.uint8)
+        types[np.asarray(scene.pinned, np.int64)] = STATIC
+        return self.submit(scene.mesh, scene.cdef, types, scene.spheres, steps, arrival)
+
+    def tick(self, now: float = 0.0) -> dict:
+        t = ServerTickC()
+        check(lib().b3g_server_tick(self.h, now, C.byref(t)), "server_tick")
+        return {k: getattr(t, k) for k, _ in ServerTickC._fields_}
+
+    def poll(self, rid: int) -> dict:
+        i = RequestInfoC()
+        check(lib().b3g_server_poll(self.h, rid, C.byref(i)), "server_poll")
+        return {k: getattr(i, k) for k, _ in RequestInfoC._fields_}
+
+    def result(self, rid: int) -> np.ndarray:
+        n = self.poll(rid)["vertex_count"]
+        out = np.zeros((n, 3), np.float32)
+        check(lib().b3g_server_result(self.h, rid, _ptr(out)), "server_result")
+        return out
+
+    def release(self, rid: int) -> None:
+        check(lib().b3g_server_release(self.h, rid), "server_release")
+
+    def stats(self) -> dict:
+        s = ServerStatsC()
+        check(lib().b3g_server_stats(self.h, C.byref(s)), "server_stats")
+        return {k: getattr(s, k) for k, _ in ServerStatsC._fields_}
+
+    def drain(self, now: float = 0.0, max_ticks: int = 100000) -> int:
+        """Tick until no request is queued or active; returns the ticks run."""
+        n = 0
+        while n < max_ticks:
+            st = self.stats()
+            if st["active"] == 0 and st["queued"] == 0:
+                break
+            self.tick(now)
+            n += 1
+        return n
 
 
 def kernel_launch_count() -> int:

@@ -273,8 +273,10 @@ b3g_status b3g_batch_get_schedule(const b3g_batch* b, b3g_batch_schedule* s)
     return B3G_OK;
 }
 
-b3g_status b3g_batch_step(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, float dt, uint32_t vel_iters,
-                          uint32_t pos_iters, b3g_step_stats* per_cloth, b3g_batch_stats* stats)
+}  // extern "C"
+
+b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, float dt, uint32_t vel_iters,
+                           uint32_t pos_iters, b3g_step_stats* per_cloth, b3g_batch_stats* stats, bool use_graph)
 {
     b3g_status s = check_list(b, cloths, count);
     if (s != B3G_OK) return s;
@@ -286,8 +288,18 @@ b3g_status b3g_batch_step(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count
         B3G_TRY(cudaStreamSynchronize(cloths[k]->stream));
     }
     B3G_TRY(cudaStreamSynchronize(st));
-    const bool same = b->exec && b->graph_pi == pos_iters && b->graph_sched == b->sched_version &&
-                      b->graph_list.size() == count && std::equal(b->graph_list.begin(), b->graph_list.end(), cloths);
+    if (!use_graph) {
+        destroy_graph(b);
+        plan(b, cloths, count);
+        for (uint32_t k = 0; k < count; ++k) fill_step_scalars(cloths[k], dt, vel_iters, pos_iters, b->h_stage + k);
+        B3G_TRY(cudaEventRecord(b->ev0, st));
+        uint32_t kern = 0;
+        if ((s = enqueue(b, count, pos_iters, st, &kern)) != B3G_OK) return s;
+        B3G_TRY(cudaEventRecord(b->ev1, st));
+        B3G_TRY(cudaStreamSynchronize(st));
+    }
+    const bool same = !use_graph || (b->exec && b->graph_pi == pos_iters && b->graph_sched == b->sched_version &&
+                      b->graph_list.size() == count && std::equal(b->graph_list.begin(), b->graph_list.end(), cloths));
     if (!same) {
         destroy_graph(b);
         plan(b, cloths, count);
@@ -312,16 +324,18 @@ b3g_status b3g_batch_step(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count
         b->graph_pi = pos_iters;
         b->graph_sched = b->sched_version;
         b->graph_kernels = kern;
-    } else {
+    } else if (use_graph) {
         // descriptors may have changed (colliders added): refresh the pinned copy the graph uploads
         for (uint32_t k = 0; k < count; ++k) b->h_descs[k] = cloths[k]->dev;
     }
-    for (uint32_t k = 0; k < count; ++k) fill_step_scalars(cloths[k], dt, vel_iters, pos_iters, b->h_stage + k);
-    B3G_TRY(cudaEventRecord(b->ev0, st));
-    B3G_TRY(cudaGraphLaunch(b->exec, st));
-    B3G_TRY(cudaEventRecord(b->ev1, st));
-    B3G_TRY(cudaStreamSynchronize(st));
-    count_launches(b->graph_kernels);
+    if (use_graph) {
+        for (uint32_t k = 0; k < count; ++k) fill_step_scalars(cloths[k], dt, vel_iters, pos_iters, b->h_stage + k);
+        B3G_TRY(cudaEventRecord(b->ev0, st));
+        B3G_TRY(cudaGraphLaunch(b->exec, st));
+        B3G_TRY(cudaEventRecord(b->ev1, st));
+        B3G_TRY(cudaStreamSynchronize(st));
+        count_launches(b->graph_kernels);
+    }
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     uint32_t it_total = 0, it_max = 0, status = 0;
@@ -343,6 +357,14 @@ b3g_status b3g_batch_step(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count
         stats->tasks = b->ntasks;
     }
     return status ? (b3g_status)status : B3G_OK;
+}
+
+extern "C" {
+
+b3g_status b3g_batch_step(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, float dt, uint32_t vel_iters,
+                          uint32_t pos_iters, b3g_step_stats* per_cloth, b3g_batch_stats* stats)
+{
+    return batch_step_impl(b, cloths, count, dt, vel_iters, pos_iters, per_cloth, stats, true);
 }
 
 // Times the batched CG alone on the systems assembled from the cloths'

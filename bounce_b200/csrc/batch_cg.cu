@@ -29,6 +29,16 @@ __device__ __forceinline__ uint32_t rbase(const ClothDev& c, uint32_t row)
     return c.slice_off[row >> 5] + (row & 31u);
 }
 
+// With a cluster team, p rows are written by other CTAs (other SMs) within the
+// launch, so the gather reads around L1 (ld.global.cg).
+template <bool L2ONLY>
+__device__ __forceinline__ f3 ldq(const float* q, uint32_t n, uint32_t i)
+{
+    if (L2ONLY) return f3{__ldcg(q + i), __ldcg(q + n + i), __ldcg(q + 2 * n + i)};
+    return ld3(q, n, i);
+}
+
+template <bool L2ONLY>
 __device__ __forceinline__ f3 spmv(const ClothDev& c, uint32_t row, const float* q)
 {
     const uint32_t base = rbase(c, row);
@@ -41,7 +51,7 @@ __device__ __forceinline__ f3 spmv(const ClothDev& c, uint32_t row, const float*
         const uint32_t col = c.cols[idx];
         const m3 a{f3{v[idx], v[E + idx], v[2 * E + idx]}, f3{v[3 * E + idx], v[4 * E + idx], v[5 * E + idx]},
                    f3{v[6 * E + idx], v[7 * E + idx], v[8 * E + idx]}};
-        acc = acc + a * ld3(q, c.n, col);
+        acc = acc + a * ldq<L2ONLY>(q, c.n, col);
     }
     return acc;
 }
@@ -58,8 +68,12 @@ struct Team {
     }
     __device__ static void sync()
     {
-        if (TEAM == 1) __syncthreads();
-        else cgx::this_cluster().sync();
+        if (TEAM == 1) {
+            __syncthreads();
+        } else {
+            __threadfence();  // global writes of this phase visible to the other SMs of the cluster
+            cgx::this_cluster().sync();
+        }
     }
 };
 
@@ -159,7 +173,7 @@ __device__ void team_cg(const ClothDev& c, typename DotT<DOT>::T* wsum, typename
         // s = S A p, alpha = delta / p.s
         T v1[1] = {D::zero()};
         for (uint32_t row = r0 + threadIdx.x; row < r1; row += kBlock) {
-            const f3 ap = spmv(c, row, c.p);
+            const f3 ap = spmv<(TEAM > 1)>(c, row, c.p);
             const f3 s = dyn(c, row) ? ap : zero3();
             st3(c.s, n, row, s);
             v1[0] = D::add_term(v1[0], ld3(c.p, n, row), s);

@@ -11,6 +11,7 @@
 #include "cloth_dev.cuh"
 #include "topology.h"
 #include "cloth_internal.h"
+#include "grid_cg.cuh"
 
 using namespace b3g;
 
@@ -114,34 +115,39 @@ b3g_status build_graph(b3g_cloth* c, uint32_t pos_iters)
     do {
         if ((err = launch_contacts_update(c->dev, st)) != cudaSuccess) break;
         if ((err = launch_assemble(c->dev, c->assemble_block, st)) != cudaSuccess) break;
-        cudaStreamCaptureStatus cs;
-        cudaGraph_t cap;
-        const cudaGraphNode_t* deps = nullptr;
-        size_t ndeps = 0;
-        if ((err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cap, &deps, &ndeps)) != cudaSuccess) break;
-        cudaGraphConditionalHandle cond;
-        if ((err = cudaGraphConditionalHandleCreate(&cond, cap, 0, 0)) != cudaSuccess) break;
-        if ((err = launch_cg_init(c->dev, dot, cond, 1, st)) != cudaSuccess) break;
-        if ((err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cap, &deps, &ndeps)) != cudaSuccess) break;
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = cond;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t wnode;
-        if ((err = cudaGraphAddNode(&wnode, cap, deps, ndeps, &cp)) != cudaSuccess) break;
-        if ((err = cudaStreamUpdateCaptureDependencies(st, &wnode, 1, cudaStreamSetCaptureDependencies)) !=
-            cudaSuccess)
-            break;
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        if ((err = cudaStreamBeginCaptureToGraph(c->body_stream, body, nullptr, nullptr, 0,
-                                                 cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
-            break;
-        cudaError_t e2 = launch_cg_iteration(c->dev, dot, cond, 1, c->body_stream);
-        cudaGraph_t body_out = nullptr;
-        cudaError_t e3 = cudaStreamEndCapture(c->body_stream, &body_out);
-        if (e2 != cudaSuccess) { err = e2; break; }
-        if (e3 != cudaSuccess) { err = e3; break; }
+        if (c->cg_strategy == B3G_CG_PERSISTENT) {
+            if ((err = cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st)) != cudaSuccess) break;
+            if ((err = launch_grid_cg(c->dev, dot, c->dev.bar, grid_cg_blocks(c->device), st)) != cudaSuccess) break;
+        } else {
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t cap;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t ndeps = 0;
+            if ((err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cap, &deps, &ndeps)) != cudaSuccess) break;
+            cudaGraphConditionalHandle cond;
+            if ((err = cudaGraphConditionalHandleCreate(&cond, cap, 0, 0)) != cudaSuccess) break;
+            if ((err = launch_cg_init(c->dev, dot, cond, 1, st)) != cudaSuccess) break;
+            if ((err = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cap, &deps, &ndeps)) != cudaSuccess) break;
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = cond;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t wnode;
+            if ((err = cudaGraphAddNode(&wnode, cap, deps, ndeps, &cp)) != cudaSuccess) break;
+            if ((err = cudaStreamUpdateCaptureDependencies(st, &wnode, 1, cudaStreamSetCaptureDependencies)) !=
+                cudaSuccess)
+                break;
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            if ((err = cudaStreamBeginCaptureToGraph(c->body_stream, body, nullptr, nullptr, 0,
+                                                     cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+                break;
+            cudaError_t e2 = launch_cg_iteration(c->dev, dot, cond, 1, c->body_stream);
+            cudaGraph_t body_out = nullptr;
+            cudaError_t e3 = cudaStreamEndCapture(c->body_stream, &body_out);
+            if (e2 != cudaSuccess) { err = e2; break; }
+            if (e3 != cudaSuccess) { err = e3; break; }
+        }
         if ((err = launch_finalize(c->dev, st)) != cudaSuccess) break;
         for (uint32_t k = 1; k < pos_iters && k < (uint32_t)kMaxPosIters; ++k)
             if ((err = launch_contact_position(c->dev, k, st)) != cudaSuccess) break;
@@ -159,6 +165,7 @@ b3g_status build_graph(b3g_cloth* c, uint32_t pos_iters)
         return from_cuda(err);
     }
     c->graph_dot = dot;
+    c->graph_strategy = c->cg_strategy;
     c->graph_pos_iters = pos_iters;
     c->graph_nsph = c->dev.nsph;
     return B3G_OK;
@@ -173,8 +180,13 @@ b3g_status launch_step_plain(b3g_cloth* c, uint32_t pos_iters)
     cudaGraphConditionalHandle none = 0;
     B3G_TRY(launch_contacts_update(c->dev, st));
     B3G_TRY(launch_assemble(c->dev, c->assemble_block, st));
-    B3G_TRY(launch_cg_init(c->dev, dot, none, 0, st));
-    for (uint32_t k = 0; k < c->opts.max_iterations; ++k) B3G_TRY(launch_cg_iteration(c->dev, dot, none, 0, st));
+    if (c->cg_strategy == B3G_CG_PERSISTENT) {
+        B3G_TRY(cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st));
+        B3G_TRY(launch_grid_cg(c->dev, dot, c->dev.bar, grid_cg_blocks(c->device), st));
+    } else {
+        B3G_TRY(launch_cg_init(c->dev, dot, none, 0, st));
+        for (uint32_t k = 0; k < c->opts.max_iterations; ++k) B3G_TRY(launch_cg_iteration(c->dev, dot, none, 0, st));
+    }
     B3G_TRY(launch_finalize(c->dev, st));
     for (uint32_t k = 1; k < pos_iters && k < (uint32_t)kMaxPosIters; ++k)
         B3G_TRY(launch_contact_position(c->dev, k, st));
@@ -207,20 +219,17 @@ const char* b3g_status_string(b3g_status s)
 
 uint64_t b3g_kernel_launch_count(void) { return kernel_launches(); }
 
-b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, int device, b3g_cloth** out)
+}  // extern "C"
+
+// Host half of cloth creation: validates the mesh, builds the topology and the
+// device images, sizes the arena.  Touches no CUDA state; thread-safe.
+b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3g_cloth** out)
 {
     if (!mesh || !def || !out || !mesh->vertices || !mesh->triangles || mesh->vertex_count == 0 ||
         mesh->triangle_count == 0 || (mesh->sewing_line_count && !mesh->sewing_lines))
         return B3G_ERR_INVALID_ARGUMENT;
     if (!(def->density > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
     *out = nullptr;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-        cudaGetLastError();
-        return B3G_ERR_NO_DEVICE;
-    }
-    if (device < 0 || device >= ndev) return B3G_ERR_INVALID_ARGUMENT;
-
     const float d8[8] = {def->density, def->streching, def->shearing, def->bending,
                          def->sewing,  def->damping,   def->thickness, def->friction};
     b3g_cloth* c = new (std::nothrow) b3g_cloth();
@@ -230,12 +239,6 @@ b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def,
     if (rc != 0) {
         delete c;
         return (b3g_status)rc;
-    }
-    c->device = device;
-    cudaError_t e = cudaSetDevice(device);
-    if (e != cudaSuccess) {
-        delete c;
-        return from_cuda(e);
     }
     const ClothTopology& T = c->topo;
     const uint32_t n = T.n, t = T.t, ns = T.ns;
@@ -255,7 +258,6 @@ b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def,
     d.block = 256;
     d.grid = std::min<uint32_t>((n + 255) / 256, 148 * 8);
 
-    // sizes
     const size_t vec = 3 * (size_t)n * sizeof(float);
     size_t bytes = 0;
     auto add = [&](size_t b) { bytes += ((b + 255) & ~size_t(255)) + 256; };
@@ -268,16 +270,73 @@ b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def,
     const size_t nn = (size_t)kMaxSpheres * n;
     add(nn); add(nn); add(nn * 4); add(nn * 12); add(nn * 12); add(nn * 12); add(nn * 12);
     add(sizeof(StepScalars));
+    add(sizeof(GridBarrier));
     add((size_t)d.grid * 32);
     add(vec); add(n);                       // staging
-    e = cudaMalloc(&c->arena.base, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
+    c->arena.size = bytes + 256;
+
+    HostImages* im = new (std::nothrow) HostImages();
+    if (!im) {
         delete c;
         return B3G_ERR_OUT_OF_MEMORY;
     }
-    c->arena.size = bytes;
+    im->tri.resize(t);
+    im->rest.resize(t);
+    im->rest2.resize(t);
+    for (uint32_t k = 0; k < t; ++k) {
+        im->tri[k] = make_uint4(mesh->triangles[3 * k], mesh->triangles[3 * k + 1], mesh->triangles[3 * k + 2], 0u);
+        const float* r = &T.rest[6 * (size_t)k];
+        im->rest[k] = make_float4(r[0], r[1], r[2], r[3]);
+        im->rest2[k] = make_float2(r[4], r[5]);
+    }
+    im->spr.resize(ns + 1);
+    im->sp.resize(ns + 1);
+    for (uint32_t q = 0; q < ns; ++q) {
+        im->spr[q] = make_uint2(T.spring_pairs[2 * q], T.spring_pairs[2 * q + 1]);
+        im->sp[q] = make_float4(T.spring_par[3 * q], T.spring_par[3 * q + 1], T.spring_par[3 * q + 2], 0.0f);
+    }
+    im->x.resize(3 * (size_t)n);
+    im->lo.resize(3 * (size_t)n);
+    im->hi.resize(3 * (size_t)n);
+    const float r = def->thickness;
+    for (uint32_t i = 0; i < n; ++i)
+        for (int q = 0; q < 3; ++q) {
+            float x = mesh->vertices[3 * i + q];
+            im->x[(size_t)q * n + i] = x;
+            // proxy at creation: [x - r, x + r] fattened by B3_AABB_EXTENSION (cloth.cpp:312-317)
+            im->lo[(size_t)q * n + i] = (x - r) - 0.2f;
+            im->hi[(size_t)q * n + i] = (x + r) + 0.2f;
+        }
+    im->types.assign(n, (uint8_t)B3G_DYNAMIC);
+    c->images.reset(im);
+    size_t smem = assemble_smem_bytes(d, c->assemble_block);
+    while (smem > 200 * 1024 && c->assemble_block > 32) {
+        c->assemble_block /= 2;
+        smem = assemble_smem_bytes(d, c->assemble_block);
+    }
+    *out = c;
+    return B3G_OK;
+}
+
+// Device half: binds the arena `base` (c->arena.size bytes, caller-owned when
+// owns_arena is false) and enqueues the uploads on `st`.  With own_stream the
+// cloth gets its own stream and events and the call waits for the uploads;
+// otherwise it uses `st` and the host images stay alive until
+// finish_upload() after the caller has synchronised `st`.
+b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, cudaStream_t st, bool own_stream)
+{
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return from_cuda(e);
+    c->device = device;
+    c->owns_arena = owns_arena;
+    c->arena.base = base;
+    c->arena.used = 0;
+    const ClothTopology& T = c->topo;
+    const uint32_t n = T.n, t = T.t, ns = T.ns;
+    ClothDev& d = c->dev;
     Arena& A = c->arena;
+    const size_t nn = (size_t)kMaxSpheres * n;
+    const size_t vec = 3 * (size_t)n * sizeof(float);
     uint32_t* slice_off = A.take<uint32_t>(T.nslices + 1);
     uint8_t* row_deg = A.take<uint8_t>(n);
     uint32_t* cols = A.take<uint32_t>(T.E);
@@ -313,9 +372,11 @@ b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def,
     d.c_t2 = A.take<float>(3 * nn);
     d.c_imp = A.take<float>(3 * nn);
     d.sc = A.take<StepScalars>(1);
+    d.bar = A.take<GridBarrier>(1);
     d.partials = A.take<char>((size_t)d.grid * 32);
     c->d_stage = A.take<float>(3 * (size_t)n);
     c->d_stage_u8 = A.take<uint8_t>(n);
+    if (A.used > A.size) return B3G_ERR_CUDA;  // sizing bug guard
     d.slice_off = slice_off;
     d.row_deg = row_deg;
     d.cols = cols;
@@ -329,43 +390,20 @@ b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def,
     d.spr_par = spr_par;
     d.mass = mass;
 
-    // host-side images
-    std::vector<uint4> h_tri(t);
-    std::vector<float4> h_rest(t);
-    std::vector<float2> h_rest2(t);
-    for (uint32_t k = 0; k < t; ++k) {
-        h_tri[k] = make_uint4(mesh->triangles[3 * k], mesh->triangles[3 * k + 1], mesh->triangles[3 * k + 2], 0u);
-        const float* r = &T.rest[6 * (size_t)k];
-        h_rest[k] = make_float4(r[0], r[1], r[2], r[3]);
-        h_rest2[k] = make_float2(r[4], r[5]);
+    if (own_stream) {
+        if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess ||
+            (e = cudaMallocHost(&c->h_sc, sizeof(StepScalars))) != cudaSuccess)
+            return from_cuda(e);
+        std::memset(c->h_sc, 0, sizeof(StepScalars));
+        st = c->stream;
+        c->owns_stream = true;
+    } else {
+        c->stream = st;
+        c->owns_stream = false;
     }
-    std::vector<uint2> h_spr(ns + 1);
-    std::vector<float4> h_sp(ns + 1);
-    for (uint32_t s = 0; s < ns; ++s) {
-        h_spr[s] = make_uint2(T.spring_pairs[2 * s], T.spring_pairs[2 * s + 1]);
-        h_sp[s] = make_float4(T.spring_par[3 * s], T.spring_par[3 * s + 1], T.spring_par[3 * s + 2], 0.0f);
-    }
-    std::vector<float> planes(3 * (size_t)n), lo(3 * (size_t)n), hi(3 * (size_t)n);
-    const float r = def->thickness;
-    for (uint32_t i = 0; i < n; ++i)
-        for (int q = 0; q < 3; ++q) {
-            float x = mesh->vertices[3 * i + q];
-            planes[(size_t)q * n + i] = x;
-            // proxy at creation: [x - r, x + r] fattened by B3_AABB_EXTENSION (cloth.cpp:312-317)
-            lo[(size_t)q * n + i] = (x - r) - 0.2f;
-            hi[(size_t)q * n + i] = (x + r) + 0.2f;
-        }
-    std::vector<uint8_t> types(n, (uint8_t)B3G_DYNAMIC);
-
-    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess ||
-        (e = cudaMallocHost(&c->h_sc, sizeof(StepScalars))) != cudaSuccess) {
-        b3g_cloth_destroy(c);
-        return from_cuda(e);
-    }
-    cudaStream_t st = c->stream;
-    std::memset(c->h_sc, 0, sizeof(StepScalars));
+    const HostImages& im = *c->images;
     auto up = [&](void* dst, const void* src, size_t b) {
         if (e == cudaSuccess && b) e = cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, st);
     };
@@ -376,25 +414,55 @@ b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def,
     up(inc_ptr, T.inc_ptr.data(), (n + 1) * 4);
     up(inc_elem, T.inc_elem.data(), T.inc_elem.size() * 4);
     up(inc_meta, T.inc_meta.data(), T.inc_meta.size() * 4);
-    up(tri, h_tri.data(), (size_t)t * 16);
-    up(tri_rest, h_rest.data(), (size_t)t * 16);
-    up(tri_rest2, h_rest2.data(), (size_t)t * 8);
-    up(spr, h_spr.data(), (size_t)ns * 8);
-    up(spr_par, h_sp.data(), (size_t)ns * 16);
-    up(d.x, planes.data(), vec);
+    up(tri, im.tri.data(), (size_t)t * 16);
+    up(tri_rest, im.rest.data(), (size_t)t * 16);
+    up(tri_rest2, im.rest2.data(), (size_t)t * 8);
+    up(spr, im.spr.data(), (size_t)ns * 8);
+    up(spr_par, im.sp.data(), (size_t)ns * 16);
+    up(d.x, im.x.data(), vec);
     up(mass, T.mass.data(), (size_t)n * 4);
-    up(d.type, types.data(), n);
-    up(d.fat_lo, lo.data(), vec);
-    up(d.fat_hi, hi.data(), vec);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-        b3g_cloth_destroy(c);
-        return from_cuda(e);
+    up(d.type, im.types.data(), n);
+    up(d.fat_lo, im.lo.data(), vec);
+    up(d.fat_hi, im.hi.data(), vec);
+    if (e != cudaSuccess) return from_cuda(e);
+    if (own_stream) {
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return from_cuda(e);
+        c->images.reset();
     }
-    size_t smem = assemble_smem_bytes(d, c->assemble_block);
-    while (smem > 200 * 1024 && c->assemble_block > 32) {
-        c->assemble_block /= 2;
-        smem = assemble_smem_bytes(d, c->assemble_block);
+    return B3G_OK;
+}
+
+// Releases the host images once the uploads on the cloth's stream are done.
+void finish_upload(b3g_cloth* c) { c->images.reset(); }
+
+extern "C" {
+
+b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, int device, b3g_cloth** out)
+{
+    if (!out) return B3G_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        if (!mesh || !def) return B3G_ERR_INVALID_ARGUMENT;
+        return B3G_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return B3G_ERR_INVALID_ARGUMENT;
+    b3g_cloth* c = nullptr;
+    b3g_status s = prepare_cloth(mesh, def, &c);
+    if (s != B3G_OK) return s;
+    cudaError_t e = cudaSetDevice(device);
+    char* base = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&base, c->arena.size);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return e == cudaErrorMemoryAllocation ? B3G_ERR_OUT_OF_MEMORY : from_cuda(e);
+    }
+    s = realize_cloth(c, device, base, true, nullptr, true);
+    if (s != B3G_OK) {
+        b3g_cloth_destroy(c);
+        return s;
     }
     *out = c;
     return B3G_OK;
@@ -403,20 +471,30 @@ b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def,
 b3g_status b3g_cloth_destroy(b3g_cloth* c)
 {
     if (!c) return B3G_ERR_INVALID_ARGUMENT;
+    if (!c->owns_stream && c->stream) return B3G_ERR_INVALID_ARGUMENT;  // owned by a server
+    return destroy_cloth(c);
+}
+
+}  // extern "C"
+
+b3g_status destroy_cloth(b3g_cloth* c)
+{
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     destroy_graph(c);
-    if (c->arena.base) cudaFree(c->arena.base);
+    if (c->arena.base && c->owns_arena) cudaFree(c->arena.base);
     if (c->d_ops) cudaFree(c->d_ops);
     if (c->h_ops) cudaFreeHost(c->h_ops);
     if (c->h_sc) cudaFreeHost(c->h_sc);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream && c->owns_stream) cudaStreamDestroy(c->stream);
     if (c->body_stream) cudaStreamDestroy(c->body_stream);
     delete c;
     return B3G_OK;
 }
+
+extern "C" {
 
 b3g_status b3g_cloth_set_gravity(b3g_cloth* c, const float g[3])
 {
@@ -600,7 +678,7 @@ b3g_status b3g_cloth_apply_translations(b3g_cloth* c, const float* t)
 
 b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, b3g_step_stats* stats)
 {
-    if (!valid(c)) return B3G_ERR_INVALID_ARGUMENT;
+    if (!valid(c) || !c->owns_stream) return B3G_ERR_INVALID_ARGUMENT;
     if (!(dt >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     b3g_status s = flush_ops(c);
@@ -624,7 +702,7 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
     B3G_TRY(cudaEventRecord(c->ev0, st));
     if (dt > 0.0f) {
         if (c->graph_ok && (!c->exec || c->graph_dot != (int)c->opts.dot || c->graph_pos_iters != pos_iters ||
-                            c->graph_nsph != c->dev.nsph)) {
+                            c->graph_nsph != c->dev.nsph || c->graph_strategy != c->cg_strategy)) {
             if (build_graph(c, pos_iters) != B3G_OK) c->graph_ok = false;
         }
         if (c->graph_ok && c->exec) {
@@ -654,7 +732,8 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
         // kernel nodes the graph ran: [contacts_update] assemble cg_init,
         // 3 per CG iteration, finalize, [contact_position x (pos_iters - 1)], post
         const uint64_t ns = c->dev.nsph ? 1 : 0;
-        count_launches(ns + 2 + 3ull * L.iterations + 1 + (ns && pos_iters > 1 ? pos_iters - 1 : 0) + 1);
+        const uint64_t cg = c->cg_strategy == B3G_CG_PERSISTENT ? 1 : 1 + 3ull * L.iterations;
+        count_launches(ns + 1 + cg + 1 + (ns && pos_iters > 1 ? pos_iters - 1 : 0) + 1);
     }
     if (stats) *stats = L;
     if (dt > 0.0f && h->status != 0) return (b3g_status)h->status;
@@ -663,7 +742,7 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
 
 b3g_status b3g_cloth_assemble(b3g_cloth* c, float dt)
 {
-    if (!valid(c) || !(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    if (!valid(c) || !c->owns_stream || !(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     b3g_status s = flush_ops(c);
     if (s != B3G_OK) return s;
@@ -683,7 +762,7 @@ b3g_status b3g_cloth_assemble(b3g_cloth* c, float dt)
 b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters,
                                    b3g_phase_times* times, b3g_step_stats* stats)
 {
-    if (!valid(c) || !times || !(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    if (!valid(c) || !c->owns_stream || !times || !(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     b3g_status s = flush_ops(c);
     if (s != B3G_OK) return s;
@@ -719,9 +798,19 @@ b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, u
     if (c->dev.nsph && (s = timed(&times->contacts_update_ms, [&] { return launch_contacts_update(c->dev, st); })))
         return s;
     if ((s = timed(&times->assemble_ms, [&] { return launch_assemble(c->dev, c->assemble_block, st); }))) return s;
-    if ((s = timed(&times->cg_init_ms, [&] { return launch_cg_init(c->dev, dot, none, 0, st); }))) return s;
     StepScalars probe;
-    for (;;) {
+    if (c->cg_strategy == B3G_CG_PERSISTENT) {
+        B3G_TRY(cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st));
+        if ((s = timed(&times->cg_spmv_ms, [&] {
+                 return launch_grid_cg(c->dev, dot, c->dev.bar, grid_cg_blocks(c->device), st);
+             })))
+            return s;
+        B3G_TRY(cudaMemcpy(&probe, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost));
+        times->cg_iterations = probe.iter;
+    } else if ((s = timed(&times->cg_init_ms, [&] { return launch_cg_init(c->dev, dot, none, 0, st); }))) {
+        return s;
+    }
+    for (; c->cg_strategy != B3G_CG_PERSISTENT;) {
         B3G_TRY(cudaMemcpy(&probe, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost));
         if (!probe.cont) break;
         if ((s = timed(&times->cg_spmv_ms, [&] { return launch_cg_part(c->dev, dot, 0, st); }))) return s;
@@ -750,6 +839,35 @@ b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, u
                 times->post_ms;
     if (stats) *stats = L;
     if (h->status != 0) return (b3g_status)h->status;
+    return B3G_OK;
+}
+
+b3g_status b3g_debug_cg_barrier_timeout(b3g_cloth* c, uint32_t spin_limit, b3g_status* result)
+{
+    if (!valid(c) || !c->owns_stream || !result || spin_limit == 0) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    cudaStream_t st = c->stream;
+    // a barrier that cannot complete: the arrival counter starts past the
+    // value the last arriver looks for, so every CTA waits until its limit
+    GridBarrier bar = {0x40000000u, 0u, 0u, spin_limit};
+    StepScalars* h = c->h_sc;
+    B3G_TRY(cudaStreamSynchronize(st));
+    fill_step_scalars(c, 1.0f / 60.0f, 8, 2, h);
+    c->step_index -= 1;
+    B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, st));
+    B3G_TRY(cudaMemcpyAsync(c->dev.bar, &bar, sizeof(bar), cudaMemcpyHostToDevice, st));
+    B3G_TRY(launch_assemble(c->dev, c->assemble_block, st));
+    B3G_TRY(launch_grid_cg(c->dev, (int)c->opts.dot, c->dev.bar, grid_cg_blocks(c->device), st));
+    B3G_TRY(cudaMemcpyAsync(h, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, st));
+    B3G_TRY(cudaStreamSynchronize(st));
+    *result = (b3g_status)h->status;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_set_cg_strategy(b3g_cloth* c, b3g_cg_strategy s)
+{
+    if (!valid(c) || (s != B3G_CG_LAUNCHES && s != B3G_CG_PERSISTENT)) return B3G_ERR_INVALID_ARGUMENT;
+    c->cg_strategy = s;
     return B3G_OK;
 }
 

@@ -58,6 +58,8 @@ struct StepScalars {
     float gx, gy, gz;
 };
 
+struct GridBarrier;
+
 struct SphereDev {
     float cx, cy, cz, radius, friction;
     float lo[3], hi[3];   // fat AABB of the shape proxy
@@ -101,7 +103,8 @@ struct ClothDev {
     SphereDev sph[kMaxSpheres];
 
     StepScalars* sc;
-    void* partials;             // reduction partials, >= grid blocks * 16 bytes
+    GridBarrier* bar;           // persistent-CG grid barrier
+    void* partials;             // reduction partials, >= grid blocks * 32 bytes
     uint32_t grid;              // blocks of the row kernels
     uint32_t block;             // threads of the row kernels
 };

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "../../include/b3g.h"
@@ -20,6 +21,18 @@ struct Arena {
         used = off + count * sizeof(T);
         return reinterpret_cast<T*>(base + off);
     }
+};
+
+// Host-side device images of a cloth between prepare_cloth and the end of
+// its uploads.
+struct HostImages {
+    std::vector<uint4> tri;
+    std::vector<float4> rest;
+    std::vector<float2> rest2;
+    std::vector<uint2> spr;
+    std::vector<float4> sp;
+    std::vector<float> x, lo, hi;
+    std::vector<uint8_t> types;
 };
 
 }  // namespace b3g
@@ -52,11 +65,23 @@ struct b3g_cloth {
     uint32_t graph_pos_iters = UINT32_MAX;
     uint32_t graph_nsph = UINT32_MAX;
     bool graph_ok = true;
+    b3g_cg_strategy cg_strategy = B3G_CG_LAUNCHES;
+    b3g_cg_strategy graph_strategy = B3G_CG_LAUNCHES;
 
     b3g_step_stats last{};
+
+    bool owns_arena = true;
+    bool owns_stream = true;
+    std::unique_ptr<b3g::HostImages> images;
 };
 
 
 b3g_status flush_ops_on(b3g_cloth* c, cudaStream_t st);
 void fill_step_scalars(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, b3g::StepScalars* h);
 void record_stats(b3g_cloth* c, const b3g::StepScalars& h, float ms, bool solved);
+b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3g_cloth** out);
+b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, cudaStream_t st, bool own_stream);
+void finish_upload(b3g_cloth* c);
+b3g_status destroy_cloth(b3g_cloth* c);
+b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, float dt, uint32_t vel_iters,
+                           uint32_t pos_iters, b3g_step_stats* per_cloth, b3g_batch_stats* stats, bool use_graph);

@@ -141,6 +141,18 @@ b3g_status b3g_cloth_apply_translations(b3g_cloth* cloth, const float* translati
 b3g_status b3g_cloth_step(b3g_cloth* cloth, float dt, uint32_t velocity_iterations,
                           uint32_t position_iterations, b3g_step_stats* stats);
 
+/* How one cloth's CG runs on the GPU.  LAUNCHES (default): three kernels
+ * per iteration inside a CUDA-graph while loop.  PERSISTENT: one cooperative
+ * launch for the whole solve, iterations separated by grid barriers with
+ * bounded waits (B3G_ERR_TIMEOUT if one gives up); for large cloths. */
+typedef enum { B3G_CG_LAUNCHES = 0, B3G_CG_PERSISTENT = 1 } b3g_cg_strategy;
+b3g_status b3g_cloth_set_cg_strategy(b3g_cloth* cloth, b3g_cg_strategy strategy);
+/* Diagnostic of the bounded waits: runs the persistent CG once with a grid
+ * barrier that can never complete and a wait limit of spin_limit polls;
+ * *result receives the solve status (B3G_ERR_TIMEOUT when the limit works).
+ * The cloth's state is not changed. */
+b3g_status b3g_debug_cg_barrier_timeout(b3g_cloth* cloth, uint32_t spin_limit, b3g_status* result);
+
 /* Device time per kernel of one step, for roofline accounting: the same step
  * as b3g_cloth_step, launched kernel by kernel (no graph) with CUDA events
  * around each launch on the cloth's stream.  Sums over the step's launches. */
@@ -278,6 +290,69 @@ b3g_status b3g_batch_get_schedule(const b3g_batch* batch, b3g_batch_schedule* sc
  * split-instance; keeps the fastest schedule.  Cloth state is not changed. */
 b3g_status b3g_batch_autotune(b3g_batch* batch, b3g_cloth* const* cloths, uint32_t count, float dt,
                               b3g_batch_schedule* out);
+
+/* ---- serving: continuous batching of cloth-step requests --------------------- */
+
+/* No reference counterpart (the reference is a single-threaded library).
+ * A server takes requests -- a cloth and a number of b3Cloth::Step calls --
+ * builds their topology on host worker threads, admits them in arrival order
+ * while an HBM budget and a slot limit allow, keeps their state resident on
+ * the device, and on every tick advances all admitted cloths by one step in
+ * one batched launch sequence.  Requests that arrive while others are in
+ * flight join the next tick.  Finished cloths are copied back to the host
+ * and their device memory returns to the server's pool.  Each request's
+ * result is the same alone and in any mix (fixed batch schedule). */
+typedef struct b3g_server b3g_server;
+
+typedef struct {
+    uint64_t hbm_budget_bytes;       /* admission cap on resident cloth memory */
+    uint32_t max_active;             /* most cloths in flight */
+    float dt;
+    uint32_t velocity_iterations;
+    uint32_t position_iterations;
+    float gravity[3];
+    b3g_solver_opts solver;          /* max_iterations 0: relative 1e-4, at most 200, FP64 dots */
+    b3g_batch_schedule schedule;     /* cluster 0: block-per-instance */
+    uint32_t host_threads;           /* topology worker threads, 0: one per core */
+} b3g_server_config;
+
+typedef struct {
+    uint32_t admitted, stepped, completed, active, queued, rows;
+    uint64_t bytes_used;
+    float tick_ms;                   /* device time of this tick's batched step */
+} b3g_server_tick_info;
+
+/* state: 0 queued, 1 prepared, 2 active, 3 done, 4 failed */
+typedef struct {
+    uint32_t state;
+    b3g_status status;
+    uint32_t steps_done, steps_total, vertex_count;
+    double arrival, admitted, finished;   /* in the caller's clock (submit / tick `now`) */
+    uint64_t bytes;
+} b3g_request_info;
+
+typedef struct {
+    uint64_t ticks, steps, vertex_steps, admitted, completed, rejected;
+    double busy_ms;                  /* summed device time of all ticks */
+    uint32_t active, queued, peak_active;
+    uint64_t peak_bytes;
+    float p50_step_ms, p99_step_ms, max_step_ms;  /* per request-step latency */
+} b3g_server_statistics;
+
+b3g_status b3g_server_create(int device, const b3g_server_config* config, b3g_server** out);
+b3g_status b3g_server_destroy(b3g_server* server);
+/* types: vertex_count particle types or NULL (all dynamic); spheres: 5 floats
+ * each (center xyz, radius, friction).  Thread-safe. */
+b3g_status b3g_server_submit(b3g_server* server, const b3g_mesh_desc* mesh, const b3g_cloth_def* def,
+                             const uint8_t* types, const float* spheres, uint32_t sphere_count, uint32_t steps,
+                             double arrival, uint64_t* request_id);
+/* Admit what fits, step every active cloth once, retire finished requests. */
+b3g_status b3g_server_tick(b3g_server* server, double now, b3g_server_tick_info* info);
+b3g_status b3g_server_poll(b3g_server* server, uint64_t request_id, b3g_request_info* info);
+/* Final positions (3 floats per vertex) of a finished request. */
+b3g_status b3g_server_result(b3g_server* server, uint64_t request_id, float* positions);
+b3g_status b3g_server_release(b3g_server* server, uint64_t request_id);
+b3g_status b3g_server_stats(const b3g_server* server, b3g_server_statistics* stats);
 
 /* ---- misc ----------------------------------------------------------------- */
 

@@ -169,3 +169,35 @@ def test_standalone_mpcg_matches_oracle(b3g, port):
         xo, ito, sto = port.mpcg(sysd, opts.stop_rule, opts.tolerance, opts.max_iterations, opts.dot)
         assert abs(it - ito) <= 1
         assert rel_err(x, xo) <= 1e-4, rel_err(x, xo)
+
+
+@pytest.mark.parametrize("side,maker", [(64, "sphere"), (200, "plain")])
+def test_persistent_cg_matches_launches(b3g, port, side, maker):
+    """The persistent cooperative CG (grid barriers) gives the per-step answer
+    of the oracle like the per-iteration launches do."""
+    scene = b3g.sphere_scene(side) if maker == "sphere" else b3g.plain_scene(side)
+    opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
+    gpu, ora = _pair(b3g, port, scene, opts)
+    gpu.set_cg_strategy(True)
+    for step in range(8):
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        assert abs(g["iterations"] - o["iterations"]) <= 1, (step, g["iterations"], o["iterations"])
+        assert rel_err(gpu.state()["x"], ora.state()["x"]) <= 1e-4
+
+
+def test_persistent_cg_bounded_wait_times_out(b3g):
+    """A grid barrier that never completes ends in B3G_ERR_TIMEOUT, and the
+    context stays usable: the next step works."""
+    import ctypes as C
+
+    scene = b3g.plain_scene(128)
+    cloth = b3g.Cloth(scene.mesh, scene.cdef).setup(scene, b3g.SolverOptions.relative(1e-4, 50))
+    cloth.set_cg_strategy(True)
+    res = C.c_int(0)
+    b3g.check(b3g.lib().b3g_debug_cg_barrier_timeout(cloth.h, 2000, C.byref(res)), "timeout diag")
+    assert res.value == 7  # B3G_ERR_TIMEOUT
+    out = cloth.step(scene.dt)
+    assert out["iterations"] > 0
