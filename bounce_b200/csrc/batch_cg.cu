@@ -13,6 +13,7 @@
 #include "batch.cuh"
 #include "cg_common.cuh"
 #include "cloth_dev.cuh"
+#include "sell_spmv.cuh"
 #include "vec.cuh"
 
 namespace cgx = cooperative_groups;
@@ -29,32 +30,8 @@ __device__ __forceinline__ uint32_t rbase(const ClothDev& c, uint32_t row)
     return c.slice_off[row >> 5] + (row & 31u);
 }
 
-// With a cluster team, p rows are written by other CTAs (other SMs) within the
-// launch, so the gather reads around L1 (ld.global.cg).
-template <bool L2ONLY>
-__device__ __forceinline__ f3 ldq(const float* q, uint32_t n, uint32_t i)
-{
-    if (L2ONLY) return f3{__ldcg(q + i), __ldcg(q + n + i), __ldcg(q + 2 * n + i)};
-    return ld3(q, n, i);
-}
-
-template <bool L2ONLY>
-__device__ __forceinline__ f3 spmv(const ClothDev& c, uint32_t row, const float* q)
-{
-    const uint32_t base = rbase(c, row);
-    const uint32_t deg = c.row_deg[row];
-    const uint32_t E = c.E;
-    const float* v = c.vals;
-    f3 acc = zero3();
-    for (uint32_t k = 0; k < deg; ++k) {
-        const uint32_t idx = base + 32u * k;
-        const uint32_t col = c.cols[idx];
-        const m3 a{f3{v[idx], v[E + idx], v[2 * E + idx]}, f3{v[3 * E + idx], v[4 * E + idx], v[5 * E + idx]},
-                   f3{v[6 * E + idx], v[7 * E + idx], v[8 * E + idx]}};
-        acc = acc + a * ldq<L2ONLY>(q, c.n, col);
-    }
-    return acc;
-}
+// With a cluster team, p rows are written by other SMs within the launch; the
+// SpMV reads them around L1 (sell_row_times<true>).
 
 __device__ __forceinline__ bool dyn(const ClothDev& c, uint32_t i) { return c.type[i] == 2; }
 
@@ -173,7 +150,7 @@ __device__ void team_cg(const ClothDev& c, typename DotT<DOT>::T* wsum, typename
         // s = S A p, alpha = delta / p.s
         T v1[1] = {D::zero()};
         for (uint32_t row = r0 + threadIdx.x; row < r1; row += kBlock) {
-            const f3 ap = spmv<(TEAM > 1)>(c, row, c.p);
+            const f3 ap = sell_row_times<(TEAM > 1), 8>(c, row, c.p);
             const f3 s = dyn(c, row) ? ap : zero3();
             st3(c.s, n, row, s);
             v1[0] = D::add_term(v1[0], ld3(c.p, n, row), s);
@@ -229,7 +206,7 @@ __device__ void team_cg(const ClothDev& c, typename DotT<DOT>::T* wsum, typename
 // cloths, one per CTA (team_cg<1>, block-per-instance).  The host orders the
 // tasks largest first; clusters take them from a queue.
 template <int T>
-__global__ void __launch_bounds__(kBlock) k_batch_cg(const __grid_constant__ BatchCgArgs a)
+__global__ void __launch_bounds__(kBlock, 4) k_batch_cg(const __grid_constant__ BatchCgArgs a)
 {
     __shared__ double wsum[2 * kWarps];
     __shared__ double slot[2];

@@ -24,6 +24,7 @@
 
 #include "cg_common.cuh"
 #include "cloth_dev.cuh"
+#include "sell_spmv.cuh"
 #include "vec.cuh"
 
 namespace b3g {
@@ -69,15 +70,7 @@ __device__ __forceinline__ void store_block(const ClothDev& c, uint32_t idx, con
 // (A q)_row for a vector q given as 3 planes.
 __device__ __forceinline__ f3 spmv_row(const ClothDev& c, uint32_t row, const float* q)
 {
-    const uint32_t base = row_base(c, row);
-    const uint32_t deg = c.row_deg[row];
-    f3 acc = zero3();
-    for (uint32_t k = 0; k < deg; ++k) {
-        const uint32_t idx = base + 32u * k;
-        const uint32_t col = c.cols[idx];
-        acc = acc + load_block(c, idx) * ld3(q, c.n, col);
-    }
-    return acc;
+    return sell_row_times<false>(c, row, q);
 }
 
 __device__ __forceinline__ bool is_dynamic(const ClothDev& c, uint32_t i) { return c.type[i] == 2; }

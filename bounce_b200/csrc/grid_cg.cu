@@ -13,6 +13,7 @@
 #include "cg_common.cuh"
 #include "cloth_dev.cuh"
 #include "grid_cg.cuh"
+#include "sell_spmv.cuh"
 #include "vec.cuh"
 
 namespace b3g {
@@ -180,13 +181,7 @@ __global__ void __launch_bounds__(kBlock) k_grid_cg(const __grid_constant__ Clot
         while (cont) {
             T v1[1] = {D::zero()};
             for (uint32_t row = first; row < n; row += stride) {
-                const uint32_t base = rbase(c, row);
-                const uint32_t deg = c.row_deg[row];
-                f3 ap = zero3();
-                for (uint32_t k = 0; k < deg; ++k) {
-                    const uint32_t idx = base + 32u * k;
-                    ap = ap + block_at(c, idx) * ld3_l2(c.p, n, c.cols[idx]);
-                }
+                const f3 ap = sell_row_times<true>(c, row, c.p);
                 const f3 s = dyn(c, row) ? ap : zero3();
                 st3(c.s, n, row, s);
                 v1[0] = D::add_term(v1[0], ld3(c.p, n, row), s);
