@@ -129,9 +129,11 @@ def algorithmic_bytes(info: dict, kernel: str) -> float:
     if kernel == "cg_init":
         return 40.0 * blocks + (12 * 3 + 1 + 3 * 12) * n
     if kernel.startswith("grid_cg"):
-        # the whole persistent solve: init + per iteration SpMV, update, direction
+        # the whole persistent solve: init, then per iteration phase A (A once;
+        # own z, p_old read, p and s written, filter byte) and phase B (x, p, r,
+        # s, P^-1 read; x, r, z written; filter byte)
         iters = float(kernel.split(":")[1])
-        return 40.0 * blocks + 73.0 * n + iters * (40.0 * blocks + (26 + 84 + 49) * n)
+        return 40.0 * blocks + 73.0 * n + iters * (40.0 * blocks + (49 + 97) * n)
     if kernel == "assemble":
         inc = 3 * t + 2 * s
         return 36.0 * blocks + (24 + 24 + 4 + 1 + 24) * n + 40.0 * t + 24.0 * s + 8.0 * inc

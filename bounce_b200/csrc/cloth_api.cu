@@ -117,7 +117,7 @@ b3g_status build_graph(b3g_cloth* c, uint32_t pos_iters)
         if ((err = launch_assemble(c->dev, c->assemble_block, st)) != cudaSuccess) break;
         if (c->cg_strategy == B3G_CG_PERSISTENT) {
             if ((err = cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st)) != cudaSuccess) break;
-            if ((err = launch_grid_cg(c->dev, dot, c->dev.bar, grid_cg_blocks(c->device), st)) != cudaSuccess) break;
+            if ((err = launch_grid_cg(c->dev, dot, c->dev.bar, st)) != cudaSuccess) break;
         } else {
             cudaStreamCaptureStatus cs;
             cudaGraph_t cap;
@@ -182,7 +182,7 @@ b3g_status launch_step_plain(b3g_cloth* c, uint32_t pos_iters)
     B3G_TRY(launch_assemble(c->dev, c->assemble_block, st));
     if (c->cg_strategy == B3G_CG_PERSISTENT) {
         B3G_TRY(cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st));
-        B3G_TRY(launch_grid_cg(c->dev, dot, c->dev.bar, grid_cg_blocks(c->device), st));
+        B3G_TRY(launch_grid_cg(c->dev, dot, c->dev.bar, st));
     } else {
         B3G_TRY(launch_cg_init(c->dev, dot, none, 0, st));
         for (uint32_t k = 0; k < c->opts.max_iterations; ++k) B3G_TRY(launch_cg_iteration(c->dev, dot, none, 0, st));
@@ -264,14 +264,14 @@ b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3
     add((T.nslices + 1) * 4); add(n); add((size_t)T.E * 4); add((size_t)T.E * 36);
     add((n + 1) * 4); add(T.inc_elem.size() * 4 + 4); add(T.inc_meta.size() * 4 + 4);
     add((size_t)t * 16); add((size_t)t * 16); add((size_t)t * 8); add((size_t)ns * 8 + 8); add((size_t)ns * 16 + 16);
-    for (int k = 0; k < 11; ++k) add(vec);  // x v fext y mx b dv r p s pinv
+    for (int k = 0; k < 13; ++k) add(vec);  // x v fext y mx b dv r p s pinv z p2
     add((size_t)n * 4); add(n);             // mass, type
     add(vec); add(vec);                     // fat lo / hi
     const size_t nn = (size_t)kMaxSpheres * n;
     add(nn); add(nn); add(nn * 4); add(nn * 12); add(nn * 12); add(nn * 12); add(nn * 12);
     add(sizeof(StepScalars));
     add(sizeof(GridBarrier));
-    add((size_t)d.grid * 32);
+    add(std::max((size_t)d.grid * 32, kGridCgPartialBytes));
     add(vec); add(n);                       // staging
     c->arena.size = bytes + 256;
 
@@ -360,6 +360,8 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     d.p = A.take<float>(3 * (size_t)n);
     d.s = A.take<float>(3 * (size_t)n);
     d.pinv = A.take<float>(3 * (size_t)n);
+    d.z = A.take<float>(3 * (size_t)n);
+    d.p2 = A.take<float>(3 * (size_t)n);
     float* mass = A.take<float>(n);
     d.type = A.take<uint8_t>(n);
     d.fat_lo = A.take<float>(3 * (size_t)n);
@@ -373,7 +375,7 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     d.c_imp = A.take<float>(3 * nn);
     d.sc = A.take<StepScalars>(1);
     d.bar = A.take<GridBarrier>(1);
-    d.partials = A.take<char>((size_t)d.grid * 32);
+    d.partials = A.take<char>(std::max((size_t)d.grid * 32, kGridCgPartialBytes));
     c->d_stage = A.take<float>(3 * (size_t)n);
     c->d_stage_u8 = A.take<uint8_t>(n);
     if (A.used > A.size) return B3G_ERR_CUDA;  // sizing bug guard
@@ -802,7 +804,7 @@ b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, u
     if (c->cg_strategy == B3G_CG_PERSISTENT) {
         B3G_TRY(cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st));
         if ((s = timed(&times->cg_spmv_ms, [&] {
-                 return launch_grid_cg(c->dev, dot, c->dev.bar, grid_cg_blocks(c->device), st);
+                 return launch_grid_cg(c->dev, dot, c->dev.bar, st);
              })))
             return s;
         B3G_TRY(cudaMemcpy(&probe, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost));
@@ -847,9 +849,9 @@ b3g_status b3g_debug_cg_barrier_timeout(b3g_cloth* c, uint32_t spin_limit, b3g_s
     if (!valid(c) || !c->owns_stream || !result || spin_limit == 0) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     cudaStream_t st = c->stream;
-    // a barrier that cannot complete: the arrival counter starts past the
-    // value the last arriver looks for, so every CTA waits until its limit
-    GridBarrier bar = {0x40000000u, 0u, 0u, spin_limit};
+    // a barrier that cannot complete: the arrival counter starts half its
+    // range away from every target, so every CTA waits until its limit
+    GridBarrier bar = {0x80000000u, 0u, 0u, spin_limit};
     StepScalars* h = c->h_sc;
     B3G_TRY(cudaStreamSynchronize(st));
     fill_step_scalars(c, 1.0f / 60.0f, 8, 2, h);
@@ -857,7 +859,7 @@ b3g_status b3g_debug_cg_barrier_timeout(b3g_cloth* c, uint32_t spin_limit, b3g_s
     B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, st));
     B3G_TRY(cudaMemcpyAsync(c->dev.bar, &bar, sizeof(bar), cudaMemcpyHostToDevice, st));
     B3G_TRY(launch_assemble(c->dev, c->assemble_block, st));
-    B3G_TRY(launch_grid_cg(c->dev, (int)c->opts.dot, c->dev.bar, grid_cg_blocks(c->device), st));
+    B3G_TRY(launch_grid_cg(c->dev, (int)c->opts.dot, c->dev.bar, st));
     B3G_TRY(cudaMemcpyAsync(h, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, st));
     B3G_TRY(cudaStreamSynchronize(st));
     *result = (b3g_status)h->status;

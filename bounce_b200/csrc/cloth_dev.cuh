@@ -2,8 +2,8 @@
 //
 // Layout (all in HBM, owned by the cloth handle):
 //  * per-vertex state as SoA planes of length n: x, v, f_ext, y (translation),
-//    mx (last CG solution, the warm start), b, dv, r, p, s, pinv (3 planes
-//    each), mass (1 plane), type (u8);
+//    mx (last CG solution, the warm start), b, dv, r, p, s, pinv, z, p2 (3
+//    planes each), mass (1 plane), type (u8);
 //  * the block matrix A in sliced ELL (SELL-32): rows in slices of 32, one
 //    slice padded to its widest row; entry (row 32 q + lane, slot k) sits at
 //    slice_off[q] + 32 k + lane, so a warp reading slot k of its 32 rows reads
@@ -90,6 +90,7 @@ struct ClothDev {
     const float* mass;
     uint8_t* type;
     float *b, *dv, *r, *p, *s, *pinv;
+    float *z, *p2;              // S P^-1 r and the second direction buffer (persistent CG)
     float *fat_lo, *fat_hi;
 
     // contacts, [sphere][vertex]
@@ -104,7 +105,7 @@ struct ClothDev {
 
     StepScalars* sc;
     GridBarrier* bar;           // persistent-CG grid barrier
-    void* partials;             // reduction partials, >= grid blocks * 32 bytes
+    void* partials;             // reduction partials, >= max(grid, persistent CG blocks) * 32 bytes
     uint32_t grid;              // blocks of the row kernels
     uint32_t block;             // threads of the row kernels
 };

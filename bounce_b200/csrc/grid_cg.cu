@@ -1,13 +1,17 @@
 // Persistent MPCG of one large cloth on the whole GPU.
 //
 // b3SolveMPCG (src/bounce/cloth/cloth_force_solver.cpp:61-136) as a single
-// cooperative launch: every CTA stays resident, the phases of an iteration
-// (SpMV + p.s, update + r.P^-1 r, new direction) are separated by a software
-// grid barrier instead of kernel boundaries, and each reduction is summed by
-// every CTA from the per-CTA partials in index order, so all CTAs agree on
-// alpha and beta without another barrier and the result is deterministic.
+// cooperative launch: every CTA stays resident, the two phases of an
+// iteration (new direction + SpMV + p.s; update + r.P^-1 r) are separated by
+// a software grid barrier instead of kernel boundaries, and each reduction
+// is summed by every CTA from the per-CTA partials in index order, so all
+// CTAs agree on alpha and beta without another barrier and the result is
+// deterministic.  The launch is shaped so that rows spread evenly over the
+// SMs (one CTA per SM, one row per thread, while that fits).
 // Every wait on the barrier is bounded: after kSpinLimit polls the CTA sets
 // the cloth's status to B3G_ERR_TIMEOUT and leaves, and so do the others.
+#include <algorithm>
+
 #include <cuda/atomic>
 
 #include "cg_common.cuh"
@@ -20,8 +24,9 @@ namespace b3g {
 
 namespace {
 
-constexpr int kBlock = 256;
-constexpr int kWarps = kBlock / 32;
+constexpr int kMaxBlock = 512;
+constexpr int kMaxWarps = kMaxBlock / 32;
+constexpr int kPrefetch = 16;  // partials per lane loaded together (up to 512 CTAs)
 constexpr uint64_t kSpinLimit = 1ull << 26;
 constexpr uint32_t kStatusTimeout = 7;
 
@@ -32,7 +37,8 @@ __device__ __forceinline__ uint32_t rbase(const ClothDev& c, uint32_t row)
 
 __device__ __forceinline__ bool dyn(const ClothDev& c, uint32_t i) { return c.type[i] == 2; }
 
-// p is rewritten by other CTAs inside the launch: read it around L1.
+// z and the previous direction are written by other CTAs inside the launch:
+// read them around L1.
 __device__ __forceinline__ f3 ld3_l2(const float* p, uint32_t n, uint32_t i)
 {
     return f3{__ldcg(p + i), __ldcg(p + n + i), __ldcg(p + 2 * n + i)};
@@ -46,36 +52,75 @@ __device__ __forceinline__ m3 block_at(const ClothDev& c, uint32_t idx)
               f3{v[6 * E + idx], v[7 * E + idx], v[8 * E + idx]}};
 }
 
-// Sense-counting grid barrier with a bounded wait.  Returns false (in every
-// thread of the CTA) once any CTA has given up.
-__device__ bool grid_sync(GridBarrier* b, uint32_t nblocks)
+// Row `row` of s = A p, where the direction p = z + beta p_old is formed on
+// the fly from the neighbours' z = S P^-1 r and previous direction (first
+// iteration: p = z).  That is the same float expression the owner of each
+// row evaluates for its own p, so every row sees bit-identical p values and
+// the new direction needs no grid barrier of its own.  Blocks are summed in
+// slot order, acc = acc + A_k p_k (b3Mat33 * b3Vec3,
+// include/bounce/common/math/mat33.h:129-132).
+__device__ __forceinline__ f3 row_times_direction(const ClothDev& c, uint32_t row, const float* z,
+                                                  const float* pold, float beta, bool first)
+{
+    constexpr int W = 8;
+    const uint32_t base = rbase(c, row);
+    const uint32_t deg = c.row_deg[row];
+    const uint32_t n = c.n;
+    f3 acc = zero3();
+    for (uint32_t k0 = 0; k0 < deg; k0 += W) {
+        uint32_t cl[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) cl[k] = (k0 + k < deg) ? c.cols[base + 32u * (k0 + k)] : 0u;
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            if (k0 + k < deg) {
+                const m3 a = block_at(c, base + 32u * (k0 + k));
+                const uint32_t j = cl[k];
+                const f3 zj = ld3_l2(z, n, j);
+                const f3 pj = first ? zj : zj + beta * ld3_l2(pold, n, j);
+                acc = acc + a * pj;
+            }
+        }
+    }
+    return acc;
+}
+
+__device__ __forceinline__ void bar_arrive(uint32_t* p)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
+}
+
+__device__ __forceinline__ uint32_t bar_poll(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid barrier on a monotonic arrival counter (zeroed before the launch):
+// the e-th barrier of the launch is complete once the counter has reached
+// e * nblocks.  Arrival is one release reduction, so the last CTA to arrive
+// completes the barrier without a second round trip.  The wait is bounded:
+// after the spin limit the CTA raises the error word, which the others see
+// and leave too.  Returns false (in every thread of the CTA) on error.
+__device__ bool grid_sync(GridBarrier* b, uint32_t nblocks, uint32_t& epoch)
 {
     __shared__ int ok;
-    // every thread's writes of this phase become visible device-wide first
-    __threadfence();
-    __syncthreads();
+    ++epoch;
+    __syncthreads();  // the CTA's writes of this phase precede thread 0's release
     if (threadIdx.x == 0) {
-        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> gen(b->gen);
-        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> count(b->count);
         cuda::atomic_ref<uint32_t, cuda::thread_scope_device> err(b->error);
-        const uint32_t g = gen.load(cuda::memory_order_acquire);
+        const uint32_t target = epoch * nblocks;
         const uint64_t limit = b->spin_limit ? (uint64_t)b->spin_limit : kSpinLimit;
         int good = err.load(cuda::memory_order_relaxed) == 0;
-        if (count.fetch_add(1u, cuda::memory_order_acq_rel) == nblocks - 1) {
-            count.store(0u, cuda::memory_order_relaxed);
-            gen.store(g + 1u, cuda::memory_order_release);
-        } else {
-            uint64_t spins = 0;
-            while (gen.load(cuda::memory_order_acquire) == g) {
-                if (err.load(cuda::memory_order_relaxed) != 0) {
-                    good = 0;
-                    break;
-                }
-                if (++spins > limit) {
-                    err.store(1u, cuda::memory_order_relaxed);
-                    good = 0;
-                    break;
-                }
+        bar_arrive(&b->count);
+        uint64_t spins = 0;
+        while (good && (int32_t)(bar_poll(&b->count) - target) < 0) {
+            if ((++spins & 63u) == 0 && err.load(cuda::memory_order_relaxed) != 0) good = 0;
+            else if (spins > limit) {
+                err.store(1u, cuda::memory_order_relaxed);
+                good = 0;
+            } else {
                 __nanosleep(20);
             }
         }
@@ -85,17 +130,20 @@ __device__ bool grid_sync(GridBarrier* b, uint32_t nblocks)
     return ok != 0;
 }
 
-// CTA-level sum, then the grid total from all CTAs' partials (every CTA
-// computes the same value from the same partials in the same order).
+// CTA-level sum, then the grid total from all CTAs' partials: every CTA sums
+// the same partials in the same order (lane l takes CTAs l, l + 32, ... in
+// order, then a fixed shuffle tree), so all agree without another barrier.
+// A lane's partials are loaded together before they are summed.
 template <int DOT, int NV>
 __device__ bool grid_total(typename DotT<DOT>::T (&v)[NV], typename DotT<DOT>::T* part, GridBarrier* bar,
-                           uint32_t nblocks)
+                           uint32_t nblocks, uint32_t& epoch)
 {
     typedef DotT<DOT> D;
     typedef typename D::T T;
-    __shared__ T wsum[NV][kWarps];
+    __shared__ T wsum[NV][kMaxWarps];
     __shared__ T tot[NV];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
 #pragma unroll
     for (int k = 0; k < NV; ++k)
         for (int off = 16; off > 0; off >>= 1) v[k] = D::combine(v[k], D::shfl(v[k], off));
@@ -107,18 +155,25 @@ __device__ bool grid_total(typename DotT<DOT>::T (&v)[NV], typename DotT<DOT>::T
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
             T a = wsum[k][0];
-            for (int w = 1; w < kWarps; ++w) a = D::combine(a, wsum[k][w]);
+            for (int w = 1; w < nwarps; ++w) a = D::combine(a, wsum[k][w]);
             part[blockIdx.x * NV + k] = a;
         }
     }
-    if (!grid_sync(bar, nblocks)) return false;
-    // warp 0 sums the partials: lane l takes blocks l, l + 32, ... in order,
-    // then the 32 lane sums combine in a fixed tree
+    if (!grid_sync(bar, nblocks, epoch)) return false;
     if (warp == 0) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
+            T buf[kPrefetch];
+#pragma unroll
+            for (int m = 0; m < kPrefetch; ++m) {
+                const uint32_t b = lane + 32u * m;
+                buf[m] = b < nblocks ? D::load(part + b * NV + k) : D::zero();
+            }
             T a = D::zero();
-            for (uint32_t b = lane; b < nblocks; b += 32) a = D::combine(a, D::load(part + b * NV + k));
+#pragma unroll
+            for (int m = 0; m < kPrefetch; ++m)
+                if (lane + 32u * m < nblocks) a = D::combine(a, buf[m]);
+            for (uint32_t b = lane + 32u * kPrefetch; b < nblocks; b += 32) a = D::combine(a, D::load(part + b * NV + k));
             for (int off = 16; off > 0; off >>= 1) a = D::combine(a, D::shfl(a, off));
             if (lane == 0) tot[k] = a;
         }
@@ -129,23 +184,31 @@ __device__ bool grid_total(typename DotT<DOT>::T (&v)[NV], typename DotT<DOT>::T
     return true;
 }
 
+// One CG iteration is two phases, each ended by a grid reduction:
+//   A: p = z + beta p_old (own rows, stored), s = S A p (neighbours' p formed
+//      on the fly), p.s                                   -> alpha
+//   B: x += alpha p, r -= alpha s, z = S P^-1 r, r.z     -> delta', beta
+// p alternates between two buffers so that phase A of one iteration never
+// overwrites a direction another CTA is still reading.
 template <int DOT>
-__global__ void __launch_bounds__(kBlock) k_grid_cg(const __grid_constant__ ClothDev c, GridBarrier* bar)
+__global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ ClothDev c, GridBarrier* bar)
 {
     typedef DotT<DOT> D;
     typedef typename D::T T;
     StepScalars* sc = c.sc;
     const uint32_t n = c.n;
     const uint32_t nb = gridDim.x;
-    const uint32_t stride = gridDim.x * kBlock;
-    const uint32_t first = blockIdx.x * kBlock + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t first_row = blockIdx.x * blockDim.x + threadIdx.x;
     // two alternating partial buffers: one is read while the next is written
     T* part0 = reinterpret_cast<T*>(c.partials);
     T* part1 = part0 + 2 * nb;
     const uint32_t max_iter = sc->max_iter;
+    uint32_t epoch = 0;
 
+    // x0 = S m_x, r = S (b - A x0), z = S P^-1 r (cloth_force_solver.cpp:90-100)
     T v2[2] = {D::zero(), D::zero()};
-    for (uint32_t row = first; row < n; row += stride) {
+    for (uint32_t row = first_row; row < n; row += stride) {
         const bool Si = dyn(c, row);
         const uint32_t base = rbase(c, row);
         const uint32_t deg = c.row_deg[row];
@@ -159,15 +222,15 @@ __global__ void __launch_bounds__(kBlock) k_grid_cg(const __grid_constant__ Clot
         const f3 bi = ld3(c.b, n, row);
         const f3 pv = ld3(c.pinv, n, row);
         const f3 r = Si ? bi - ax : zero3();
-        const f3 p = Si ? mk(r.x * pv.x, r.y * pv.y, r.z * pv.z) : zero3();
+        const f3 z = Si ? mk(r.x * pv.x, r.y * pv.y, r.z * pv.z) : zero3();
         const f3 bh = Si ? bi : zero3();
         st3(c.dv, n, row, Si ? ld3(c.mx, n, row) : zero3());
         st3(c.r, n, row, r);
-        st3(c.p, n, row, p);
+        st3(c.z, n, row, z);
         v2[0] = D::add_term(v2[0], bh, mk(bh.x * pv.x, bh.y * pv.y, bh.z * pv.z));
-        v2[1] = D::add_term(v2[1], r, p);
+        v2[1] = D::add_term(v2[1], r, z);
     }
-    if (!grid_total<DOT, 2>(v2, part0, bar, nb)) goto timeout;
+    if (!grid_total<DOT, 2>(v2, part0, bar, nb, epoch)) goto timeout;
     {
         double b_delta = D::value(v2[0]), delta = D::value(v2[1]);
         if (DOT != 2) {
@@ -177,30 +240,41 @@ __global__ void __launch_bounds__(kBlock) k_grid_cg(const __grid_constant__ Clot
         const double delta0 = delta;
         uint32_t status = (!isfinite(delta) || !isfinite(b_delta)) ? kStatusNumerical : 0u;
         uint32_t it = 0;
+        float beta = 0.0f;
         bool cont = status == 0 && max_iter > 0 && !cg_stop(sc, delta, b_delta);
         while (cont) {
+            const bool first = it == 0;
+            float* pnew = (it & 1u) ? c.p2 : c.p;
+            const float* pold = (it & 1u) ? c.p : c.p2;
+            // A: p = S (P^-1 r + beta p) (cloth_force_solver.cpp:130-131, folded
+            // into the next SpMV), s = S A p, alpha = delta / p.s
             T v1[1] = {D::zero()};
-            for (uint32_t row = first; row < n; row += stride) {
-                const f3 ap = sell_row_times<true>(c, row, c.p);
+            for (uint32_t row = first_row; row < n; row += stride) {
+                const f3 zi = ld3(c.z, n, row);
+                const f3 p = first ? zi : zi + beta * ld3(pold, n, row);
+                const f3 ap = row_times_direction(c, row, c.z, pold, beta, first);
                 const f3 s = dyn(c, row) ? ap : zero3();
+                st3(pnew, n, row, p);
                 st3(c.s, n, row, s);
-                v1[0] = D::add_term(v1[0], ld3(c.p, n, row), s);
+                v1[0] = D::add_term(v1[0], p, s);
             }
-            if (!grid_total<DOT, 1>(v1, part1, bar, nb)) goto timeout;
+            if (!grid_total<DOT, 1>(v1, part1, bar, nb, epoch)) goto timeout;
             const double pAp = D::value(v1[0]);
             const float alpha = DOT == 2 ? (float)(delta / pAp) : (float)delta / (float)pAp;
+            // B: x += alpha p, r -= alpha s, z = S P^-1 r, delta' = r.P^-1 r
             T u1[1] = {D::zero()};
-            for (uint32_t row = first; row < n; row += stride) {
-                const f3 x = ld3(c.dv, n, row) + alpha * ld3(c.p, n, row);
+            for (uint32_t row = first_row; row < n; row += stride) {
+                const f3 x = ld3(c.dv, n, row) + alpha * ld3(pnew, n, row);
                 const f3 r = ld3(c.r, n, row) - alpha * ld3(c.s, n, row);
                 const f3 pv = ld3(c.pinv, n, row);
+                const f3 h = mk(r.x * pv.x, r.y * pv.y, r.z * pv.z);
                 st3(c.dv, n, row, x);
                 st3(c.r, n, row, r);
-                u1[0] = D::add_term(u1[0], r, mk(r.x * pv.x, r.y * pv.y, r.z * pv.z));
+                st3(c.z, n, row, dyn(c, row) ? h : zero3());
+                u1[0] = D::add_term(u1[0], r, h);
             }
-            if (!grid_total<DOT, 1>(u1, part0, bar, nb)) goto timeout;
+            if (!grid_total<DOT, 1>(u1, part0, bar, nb, epoch)) goto timeout;
             double dn = D::value(u1[0]);
-            float beta;
             if (DOT == 2) {
                 beta = (float)(dn / delta);
             } else {
@@ -211,14 +285,6 @@ __global__ void __launch_bounds__(kBlock) k_grid_cg(const __grid_constant__ Clot
             ++it;
             if (!isfinite(dn) || !isfinite(alpha) || !isfinite(beta)) status = kStatusNumerical;
             cont = status == 0 && it < max_iter && !cg_stop(sc, dn, b_delta);
-            if (!cont) break;
-            for (uint32_t row = first; row < n; row += stride) {
-                const f3 r = ld3(c.r, n, row);
-                const f3 pv = ld3(c.pinv, n, row);
-                const f3 hv = mk(r.x * pv.x, r.y * pv.y, r.z * pv.z);
-                st3(c.p, n, row, dyn(c, row) ? hv + beta * ld3(c.p, n, row) : zero3());
-            }
-            if (!grid_sync(bar, nb)) goto timeout;
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             sc->b_delta = b_delta;
@@ -239,26 +305,38 @@ timeout:
 
 }  // namespace
 
-int grid_cg_blocks(int device)
+GridCgShape grid_cg_shape(uint32_t n, int device)
 {
-    int sms = 148, per_sm = 1;
+    int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_cg<2>, kBlock, 0) != cudaSuccess || per_sm < 1) {
-        cudaGetLastError();
-        per_sm = 1;
+    GridCgShape g;
+    const uint32_t rows_per_sm = (n + sms - 1) / (uint32_t)sms;
+    if (rows_per_sm <= (uint32_t)kMaxBlock) {
+        // one row per thread, at most one CTA per SM, rows spread evenly
+        g.threads = (int)std::max<uint32_t>(32u, (rows_per_sm + 31u) & ~31u);
+        g.blocks = (int)((n + g.threads - 1) / g.threads);
+    } else {
+        int per_sm = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_cg<2>, kMaxBlock, 0) != cudaSuccess ||
+            per_sm < 1) {
+            cudaGetLastError();
+            per_sm = 1;
+        }
+        g.threads = kMaxBlock;
+        g.blocks = std::min(sms * per_sm, kMaxGridCgBlocks);
     }
-    return sms * per_sm;
+    if (g.blocks < 1) g.blocks = 1;
+    return g;
 }
 
-cudaError_t launch_grid_cg(const ClothDev& c, int dot, GridBarrier* bar, int blocks, cudaStream_t st)
+cudaError_t launch_grid_cg(const ClothDev& c, int dot, GridBarrier* bar, cudaStream_t st)
 {
-    // no more CTAs than row groups: idle CTAs would only add barrier arrivals
-    const int need = (int)((c.n + kBlock - 1) / kBlock);
-    if (blocks > need) blocks = need;
-    if (blocks < 1) blocks = 1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const GridCgShape g = grid_cg_shape(c.n, dev);
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
-    cfg.blockDim = dim3(kBlock);
+    cfg.gridDim = dim3(g.blocks);
+    cfg.blockDim = dim3(g.threads);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
