@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--skip-batch", action="store_true")
     ap.add_argument("--skip-serve", action="store_true")
+    # profiling aids: leave out the single-cloth headline, or the one-cloth-at-a-time
+    # comparison inside the batched section
+    ap.add_argument("--skip-single", action="store_true")
+    ap.add_argument("--skip-plain", action="store_true")
     return ap.parse_args()
 
 
@@ -114,6 +118,13 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+# DRAM bytes (read + write) of one k_grid_cg launch on the 256x256 headline cloth,
+# from the ncu capture summarised in profiles/k_grid_cg_grid256_sphere.md.  The
+# whole system stays in L2 after its first touch, so the figure holds for any
+# iteration count.  Other sizes have no capture: traffic is reported as null.
+GRID_CG_TRAFFIC = {256: 36.52e6 + 0.03e6}
 
 
 def algorithmic_bytes(info: dict, kernel: str) -> float:
@@ -236,7 +247,9 @@ def run_ours(args, rank, world):
         "iterations_mean": float(np.mean(iters)), "active_contacts_mean": float(np.mean(contacts)),
         "launches": launches, "clocks": clocks.summary(), "info": info,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": GRID_CG_TRAFFIC.get(args.side) if dom == "grid_cg" else None,
+                     "traffic_source": "ncu capture, profiles/k_grid_cg_grid256_sphere.md",
                      "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
                      "share": kern[dom][0] / total if total else None},
         "kernel_ms": {k: v[0] / v[1] for k, v in kern.items()},
@@ -267,21 +280,23 @@ def run_batched(args, dev: int):
         iters.append(out["cg_iterations_total"] / out["count"])
     launches = b3g.kernel_launch_count() - launches0
     # the plain single-instance path, same cloths, same number of steps
-    for _ in range(args.warmup):
-        for c in plain:
-            c.step(dt)
-    pms = 0.0
-    for _ in range(args.batch_steps):
-        for c in plain:
-            pms += c.step(dt)["step_ms"]
     batched = rows * len(ms) / (sum(ms) / 1000.0)
-    plain_v = rows * args.batch_steps / (pms / 1000.0)
+    plain_v = None
+    if not args.skip_plain:
+        for _ in range(args.warmup):
+            for c in plain:
+                c.step(dt)
+        pms = 0.0
+        for _ in range(args.batch_steps):
+            for c in plain:
+                pms += c.step(dt)["step_ms"]
+        plain_v = rows * args.batch_steps / (pms / 1000.0)
     for c in cloths + plain:
         c.close()
     batch.close()
     return {"cloths": len(scenes), "vertices": rows, "vertex_steps_per_s": batched,
             "ms_per_step": sum(ms) / len(ms), "plain_vertex_steps_per_s": plain_v,
-            "speedup_vs_plain": batched / plain_v, "cg_iterations_mean": float(np.mean(iters)),
+            "speedup_vs_plain": batched / plain_v if plain_v else None, "cg_iterations_mean": float(np.mean(iters)),
             "schedule": {"cluster": sched["cluster"],
                          "split_size_classes": [k for k, v in enumerate(sched["split_class"]) if v]},
             "gpu_launches": launches, "steps": len(ms),
@@ -358,6 +373,18 @@ def main():
 
         torch.cuda.set_device(local)
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    if args.skip_single:
+        batched = None if args.skip_batch else run_batched(args, local)
+        served = None if args.skip_serve else run_serving(args, local)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "note": "headline skipped (--skip-single)",
+                              "batched": batched, "serving": served}))
+        if world > 1:
+            import torch
+
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
     r = run_ours(args, rank, world)
     batched = None if args.skip_batch else run_batched(args, local)
     served = None if args.skip_serve else run_serving(args, local)
