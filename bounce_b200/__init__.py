@@ -77,7 +77,8 @@ class BatchScheduleC(C.Structure):
 
 class BatchStatsC(C.Structure):
     _fields_ = [("count", C.c_uint32), ("rows", C.c_uint32), ("tasks", C.c_uint32),
-                ("cg_iterations_total", C.c_uint32), ("cg_iterations_max", C.c_uint32), ("step_ms", C.c_float)]
+                ("cg_iterations_total", C.c_uint32), ("cg_iterations_max", C.c_uint32), ("step_ms", C.c_float),
+                ("cg_ms", C.c_float)]
 
 
 class ServerConfigC(C.Structure):
@@ -445,7 +446,7 @@ class Batch:
                                    stats, C.byref(self.stats)), "batch_step")
         s = self.stats
         out = {"count": s.count, "rows": s.rows, "tasks": s.tasks, "cg_iterations_total": s.cg_iterations_total,
-               "cg_iterations_max": s.cg_iterations_max, "step_ms": s.step_ms}
+               "cg_iterations_max": s.cg_iterations_max, "step_ms": s.step_ms, "cg_ms": s.cg_ms}
         if per_cloth:
             out["per_cloth"] = [{"iterations": x.iterations, "delta": x.delta, "b_delta": x.b_delta,
                                  "active_contacts": x.active_contacts, "contacts": x.contacts} for x in stats]

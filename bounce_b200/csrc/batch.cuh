@@ -18,7 +18,9 @@ struct BatchCgArgs {
 };
 
 // Clusters of `team` CTAs (1, 2, 4 or 8); grid_blocks <= 0 fills the GPU.
-cudaError_t launch_batch_cg(const BatchCgArgs& a, int team, int grid_blocks, cudaStream_t st);
-int batch_team_max_blocks(int team);
+// dot: the dot precision (0, 1, 2) every cloth of the launch uses, or -1 when
+// they differ (each cloth's own setting is then read on the device).
+cudaError_t launch_batch_cg(const BatchCgArgs& a, int team, int dot, int grid_blocks, cudaStream_t st);
+int batch_team_max_blocks(int team, int dot);
 
 }  // namespace b3g

@@ -8,6 +8,8 @@
 // (split-instance), chosen per size class by b3g_batch_autotune.
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -84,8 +86,8 @@ struct b3g_batch {
     uint32_t graph_pi = UINT32_MAX, graph_sched = 0;
     uint32_t graph_kernels = 0;
     uint32_t ntasks = 0, total_rows = 0, max_deg = 0;
-    int assemble_block = 128;
-    bool timing_cg = false;
+    int assemble_block = 0;
+    int dot = -1;  // dot precision shared by every planned cloth, -1 if mixed
 };
 
 namespace {
@@ -102,13 +104,16 @@ void destroy_graph(b3g_batch* b)
 void plan(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count)
 {
     uint32_t total = 0, max_deg = 1;
+    int dot = count ? (int)cloths[0]->opts.dot : -1;
     for (uint32_t k = 0; k < count; ++k) {
+        if ((int)cloths[k]->opts.dot != dot) dot = -1;
         b->h_descs[k] = cloths[k]->dev;
         b->h_prefix[k] = total;
         total += cloths[k]->dev.n;
         max_deg = std::max(max_deg, cloths[k]->dev.max_deg);
     }
     b->h_prefix[count] = total;
+    b->dot = dot;
     b->total_rows = total;
     b->max_deg = max_deg;
     std::vector<uint32_t> idx(count);
@@ -135,13 +140,7 @@ void plan(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count)
         for (uint32_t r = 0; r < cnt; ++r) b->h_order[w++] = small[q + r];
     }
     b->ntasks = nt;
-    size_t smem = 0;
-    b->assemble_block = 128;
-    do {
-        smem = (size_t)max_deg * 18 * sizeof(float) * b->assemble_block + (size_t)max_deg * b->assemble_block;
-        if (smem <= 200 * 1024) break;
-        b->assemble_block /= 2;
-    } while (b->assemble_block > 32);
+    b->assemble_block = 0;  // chosen at launch for occupancy
 }
 
 b3g_status enqueue(b3g_batch* b, uint32_t count, uint32_t pi, cudaStream_t st, uint32_t* kernels)
@@ -160,9 +159,11 @@ b3g_status enqueue(b3g_batch* b, uint32_t count, uint32_t pi, cudaStream_t st, u
     B3G_TRY(launch_span_contacts_update(sp, st));
     B3G_TRY(launch_span_assemble(sp, b->assemble_block, st));
     B3G_TRY(cudaMemsetAsync(b->d_next, 0, sizeof(uint32_t), st));
-    if (b->timing_cg) B3G_TRY(cudaEventRecord(b->ev_cg0, st));
-    B3G_TRY(launch_batch_cg(a, (int)b->sched.cluster, 0, st));
-    if (b->timing_cg) B3G_TRY(cudaEventRecord(b->ev_cg1, st));
+    // external records: inside a captured graph these become event nodes, so
+    // the CG launch is timed on every replay
+    B3G_TRY(cudaEventRecordWithFlags(b->ev_cg0, st, cudaEventRecordExternal));
+    B3G_TRY(launch_batch_cg(a, (int)b->sched.cluster, b->dot, 0, st));
+    B3G_TRY(cudaEventRecordWithFlags(b->ev_cg1, st, cudaEventRecordExternal));
     B3G_TRY(launch_span_finalize(sp, st));
     k += 4;
     for (uint32_t it = 1; it < pi && it < (uint32_t)kMaxPosIters; ++it) {
@@ -336,8 +337,12 @@ b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t coun
         B3G_TRY(cudaStreamSynchronize(st));
         count_launches(b->graph_kernels);
     }
-    float ms = 0.0f;
+    float ms = 0.0f, cg_ms = 0.0f;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    if (cudaEventElapsedTime(&cg_ms, b->ev_cg0, b->ev_cg1) != cudaSuccess) {
+        cudaGetLastError();
+        cg_ms = 0.0f;
+    }
     uint32_t it_total = 0, it_max = 0, status = 0;
     for (uint32_t k = 0; k < count; ++k) {
         const StepScalars& h = b->h_stage[k];
@@ -352,6 +357,7 @@ b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t coun
         stats->count = count;
         stats->rows = b->total_rows;
         stats->step_ms = ms;
+        stats->cg_ms = cg_ms;
         stats->cg_iterations_total = it_total;
         stats->cg_iterations_max = it_max;
         stats->tasks = b->ntasks;
@@ -394,6 +400,8 @@ b3g_status b3g_batch_autotune(b3g_batch* b, b3g_cloth* const* cloths, uint32_t c
     b3g_batch_schedule best = b->sched;
     float best_ms = 1e30f;
     const uint32_t clusters[4] = {1, 2, 4, 8};
+    const char* env = std::getenv("B3G_TRACE_AUTOTUNE");  // every timed candidate to stderr
+    const bool trace_on = env && env[0] && env[0] != '0';
     for (uint32_t ci = 0; ci < 4; ++ci) {
         b3g_batch_schedule cand{};
         cand.cluster = clusters[ci];
@@ -414,7 +422,7 @@ b3g_status b3g_batch_autotune(b3g_batch* b, b3g_cloth* const* cloths, uint32_t c
             for (int rep = 0; rep < 3; ++rep) {
                 B3G_TRY(cudaMemsetAsync(b->d_next, 0, 4, st));
                 B3G_TRY(cudaEventRecord(b->ev0, st));
-                B3G_TRY(launch_batch_cg(a, (int)sc.cluster, 0, st));
+                B3G_TRY(launch_batch_cg(a, (int)sc.cluster, b->dot, 0, st));
                 B3G_TRY(cudaEventRecord(b->ev1, st));
                 B3G_TRY(cudaEventSynchronize(b->ev1));
                 float ms = 0.0f;
@@ -424,8 +432,16 @@ b3g_status b3g_batch_autotune(b3g_batch* b, b3g_cloth* const* cloths, uint32_t c
             *ms_out = bestrun;
             return B3G_OK;
         };
+        auto trace = [&](const b3g_batch_schedule& sc, float ms) {
+            if (!trace_on) return;
+            std::fprintf(stderr, "b3g autotune: cluster %u split", sc.cluster);
+            for (int cls = 0; cls < 32; ++cls)
+                if (sc.split_class[cls]) std::fprintf(stderr, " %d", cls);
+            std::fprintf(stderr, ": CG %.3f ms\n", ms);
+        };
         float cur = 0.0f;
         if ((s = time_cg(cand, &cur)) != B3G_OK) return s;
+        trace(cand, cur);
         if (cand.cluster > 1) {
             // largest classes first: keep a class split when that is faster
             for (int cls = 31; cls >= 0; --cls) {
@@ -434,6 +450,7 @@ b3g_status b3g_batch_autotune(b3g_batch* b, b3g_cloth* const* cloths, uint32_t c
                 trial.split_class[cls] = 1;
                 float t = 0.0f;
                 if ((s = time_cg(trial, &t)) != B3G_OK) return s;
+                trace(trial, t);
                 if (t < cur) {
                     cur = t;
                     cand = trial;

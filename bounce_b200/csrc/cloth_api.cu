@@ -309,11 +309,6 @@ b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3
         }
     im->types.assign(n, (uint8_t)B3G_DYNAMIC);
     c->images.reset(im);
-    size_t smem = assemble_smem_bytes(d, c->assemble_block);
-    while (smem > 200 * 1024 && c->assemble_block > 32) {
-        c->assemble_block /= 2;
-        smem = assemble_smem_bytes(d, c->assemble_block);
-    }
     *out = c;
     return B3G_OK;
 }

@@ -125,8 +125,10 @@ cudaError_t launch_span_contact_position(const RowSpan& sp, uint32_t it, cudaStr
 cudaError_t launch_span_post(const RowSpan& sp, cudaStream_t st);
 
 // Host launchers (cloth_kernels.cu).  The assembly kernel needs
-// assemble_smem_bytes() of dynamic shared memory.
+// assemble_smem_bytes() of dynamic shared memory; a block size <= 0 asks for
+// assemble_block_for() of the rows' widest degree.
 size_t assemble_smem_bytes(const ClothDev& c, int block);
+int assemble_block_for(uint32_t max_deg, bool multi);
 cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st);
 cudaError_t launch_assemble(const ClothDev& c, int block, cudaStream_t st);
 // CG kernels: when use_graph is set, the reduction tail of init/update sets

@@ -165,6 +165,19 @@ struct RowAcc {
         const float* p = base + (slot * 18) * B + tid;
         return m3{f3{p[0], p[B], p[2 * B]}, f3{p[3 * B], p[4 * B], p[5 * B]}, f3{p[6 * B], p[7 * B], p[8 * B]}};
     }
+    // reuse of a slot's dfdv area after A is stored: v and y of its column
+    __device__ void setD6(int slot, const f3& a, const f3& b)
+    {
+        float* p = base + (slot * 18 + 9) * B + tid;
+        p[0] = a.x; p[B] = a.y; p[2 * B] = a.z;
+        p[3 * B] = b.x; p[4 * B] = b.y; p[5 * B] = b.z;
+    }
+    __device__ void getD6(int slot, f3& a, f3& b) const
+    {
+        const float* p = base + (slot * 18 + 9) * B + tid;
+        a = f3{p[0], p[B], p[2 * B]};
+        b = f3{p[3 * B], p[4 * B], p[5 * B]};
+    }
     __device__ m3 getD(int slot) const
     {
         const float* p = base + (slot * 18 + 9) * B + tid;
@@ -212,6 +225,13 @@ __device__ void spring_row(const ClothDev& c, RowAcc& acc, uint32_t sid, int end
     f_row = end == 0 ? f_row + mf : f_row - mf;
 }
 
+// Element `cn` of a 3-array held in registers (a select, not local memory).
+template <typename T>
+__device__ __forceinline__ T corner(int cn, const T& a0, const T& a1, const T& a2)
+{
+    return cn == 0 ? a0 : (cn == 1 ? a1 : a2);
+}
+
 // b3ShearForce::Apply then b3StrechForce::Apply (the force list holds the
 // shear element of a triangle before its stretch element) for corner `cn`.
 __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn, const int slot[3], f3& f_row)
@@ -235,20 +255,21 @@ __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn,
         f3 dC[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) dC[i] = alpha * (dwudx[i] * wv + dwvdx[i] * wu);
+        const f3 dCc = corner(cn, dC[0], dC[1], dC[2]);
         f3 fe = zero3();
         if (ks > 0.0f) {
             const float C = alpha * dot(wu, wv);
-            fe = fe + (-ks * C) * dC[cn];
+            fe = fe + (-ks * C) * dCc;
 #pragma unroll
-            for (int j = 0; j < 3; ++j) acc.addK(slot[j], -ks * outer(dC[cn], dC[j]));
+            for (int j = 0; j < 3; ++j) acc.addK(slot[j], -ks * outer(dCc, dC[j]));
         }
         if (kd > 0.0f) {
             float dCdt = 0.0f;
 #pragma unroll
             for (int i = 0; i < 3; ++i) dCdt += dot(dC[i], vs[i]);
-            fe = fe + (-kd * dCdt) * dC[cn];
+            fe = fe + (-kd * dCdt) * dCc;
 #pragma unroll
-            for (int j = 0; j < 3; ++j) acc.addD(slot[j], -kd * outer(dC[cn], dC[j]));
+            for (int j = 0; j < 3; ++j) acc.addD(slot[j], -kd * outer(dCc, dC[j]));
         }
         f_row = f_row + fe;
     }
@@ -262,30 +283,33 @@ __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn,
         for (int d = 0; d < 2; ++d) {
             const f3 w = d == 0 ? wu : wv;
             const float len = d == 0 ? len_wu : len_wv;
-            const float* dw = d == 0 ? dwudx : dwvdx;
+            const float dw[3] = {d == 0 ? dwudx[0] : dwvdx[0], d == 0 ? dwudx[1] : dwvdx[1],
+                                 d == 0 ? dwudx[2] : dwvdx[2]};
             if (!(len > 0.0f)) continue;
+            const float dwc = corner(cn, dw[0], dw[1], dw[2]);
             const float inv_len = 1.0f / len;
             const f3 nw = inv_len * w;
             f3 dC[3];
 #pragma unroll
             for (int i = 0; i < 3; ++i) dC[i] = (alpha * dw[i]) * nw;
+            const f3 dCc = corner(cn, dC[0], dC[1], dC[2]);
             if (ks > 0.0f && len > 1.0f) {
                 const float C = alpha * (len - 1.0f);
-                fe = fe + (-ks * C) * dC[cn];
+                fe = fe + (-ks * C) * dCc;
                 const m3 P = I - outer(nw, nw);
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
-                    const m3 d2 = (alpha * inv_len * dw[cn] * dw[j]) * P;
-                    acc.addK(slot[j], -ks * (outer(dC[cn], dC[j]) + C * d2));
+                    const m3 d2 = (alpha * inv_len * dwc * dw[j]) * P;
+                    acc.addK(slot[j], -ks * (outer(dCc, dC[j]) + C * d2));
                 }
             }
             if (kd > 0.0f) {
                 float dCdt = 0.0f;
 #pragma unroll
                 for (int i = 0; i < 3; ++i) dCdt += dot(dC[i], vs[i]);
-                fe = fe + (-kd * dCdt) * dC[cn];
+                fe = fe + (-kd * dCdt) * dCc;
 #pragma unroll
-                for (int j = 0; j < 3; ++j) acc.addD(slot[j], -kd * outer(dC[cn], dC[j]));
+                for (int j = 0; j < 3; ++j) acc.addD(slot[j], -kd * outer(dCc, dC[j]));
             }
         }
         f_row = f_row + fe;
@@ -293,7 +317,7 @@ __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn,
 }
 
 template <bool MULTI>
-__global__ void __launch_bounds__(128) k_assemble(const __grid_constant__ ClothDev one,
+__global__ void __launch_bounds__(256) k_assemble(const __grid_constant__ ClothDev one,
                                                   const __grid_constant__ RowSpan span)
 {
     extern __shared__ float smem[];
@@ -322,9 +346,17 @@ __global__ void __launch_bounds__(128) k_assemble(const __grid_constant__ ClothD
     const bool dyn = is_dynamic(c, row);
     if (dyn) f = f + m * mk(sc->gx, sc->gy, sc->gz);
 
-    for (uint32_t e = c.inc_ptr[row]; e < c.inc_ptr[row + 1]; ++e) {
-        const uint32_t el = c.inc_elem[e];
-        const uint32_t meta = c.inc_meta[e];
+    // the next incidence entry is loaded while the current element is computed
+    const uint32_t e_end = c.inc_ptr[row + 1];
+    uint32_t e = c.inc_ptr[row];
+    uint32_t el_next = e < e_end ? c.inc_elem[e] : 0u, meta_next = e < e_end ? c.inc_meta[e] : 0u;
+    for (; e < e_end; ++e) {
+        const uint32_t el = el_next;
+        const uint32_t meta = meta_next;
+        if (e + 1 < e_end) {
+            el_next = c.inc_elem[e + 1];
+            meta_next = c.inc_meta[e + 1];
+        }
         const int cn = meta & 3u;
         const int s0 = (meta >> 8) & 0xffu, s1 = (meta >> 16) & 0xffu, s2 = (meta >> 24) & 0xffu;
         if (el & 0x80000000u) {
@@ -349,19 +381,29 @@ __global__ void __launch_bounds__(128) k_assemble(const __grid_constant__ ClothD
     st3(c.pinv, n, row, mk(1.0f / diag.x.x, 1.0f / diag.y.y, 1.0f / diag.z.z));
 
     // b = h (f + h dfdx v + dfdx y), dfdx summed in its row-list order
-    // (reverse first touch, sparse_mat33.h:264-282)
+    // (reverse first touch, sparse_mat33.h:264-282).  The v and y of every
+    // slot's column are gathered first, with independent loads, into the
+    // slot's dfdv accumulator (no longer needed once A is stored).
+    for (int k0 = 0; k0 < deg; k0 += 8) {
+        uint32_t cl[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) cl[k] = k0 + k < deg ? c.cols[base + 32u * (k0 + k)] : row;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k0 + k < deg) {
+                const f3 vj = ld3(c.v, n, cl[k]), yj = ld3(c.y, n, cl[k]);
+                acc.setD6(k0 + k, vj, yj);
+            }
+        }
+    }
     f3 t1 = zero3(), t2 = zero3();
     for (int q = acc.ntouch - 1; q >= 0; --q) {
         const int k = acc.touch[q * B + tid];
-        const uint32_t col = c.cols[base + 32u * k];
         const m3 K = acc.getK(k);
-        t1 = t1 + K * ld3(c.v, n, col);
-    }
-    for (int q = acc.ntouch - 1; q >= 0; --q) {
-        const int k = acc.touch[q * B + tid];
-        const uint32_t col = c.cols[base + 32u * k];
-        const m3 K = acc.getK(k);
-        t2 = t2 + K * ld3(c.y, n, col);
+        f3 vj, yj;
+        acc.getD6(k, vj, yj);
+        t1 = t1 + K * vj;
+        t2 = t2 + K * yj;
     }
     st3(c.b, n, row, h * ((f + h * t1) + t2));
 }
@@ -908,6 +950,45 @@ size_t assemble_smem_bytes(const ClothDev& c, int block)
     return (size_t)c.max_deg * 18 * sizeof(float) * block + (size_t)c.max_deg * block;
 }
 
+// Every launch raises the kernel's dynamic shared memory limit to the same
+// maximum, so concurrent launches from several host threads never lower it
+// under one another.
+constexpr size_t kAssembleSmemLimit = 227 * 1024;
+
+// The assembly keeps a row's accumulators in shared memory (73 bytes per
+// slot), so shared memory bounds how many rows an SM holds.  Of the block
+// sizes 32..256 take the one with the most resident rows per SM (the
+// smaller on ties, for a finer tail), from the occupancy calculator.
+int assemble_block_for(uint32_t max_deg, bool multi)
+{
+    static std::atomic<int> cache[2][256];  // 0: not computed yet
+    if (max_deg > 255) max_deg = 255;
+    std::atomic<int>& slot = cache[multi ? 1 : 0][max_deg];
+    if (const int known = slot.load(std::memory_order_relaxed)) return known;
+    const void* fn = multi ? (const void*)k_assemble<true> : (const void*)k_assemble<false>;
+    int best = 32, best_rows = 0;
+    for (int b = 32; b <= 256; b += 32) {
+        const size_t smem = (size_t)max_deg * 73 * b;
+        if (smem > kAssembleSmemLimit) break;
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAssembleSmemLimit) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            break;
+        }
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, b, smem) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (per_sm * b > best_rows) {
+            best_rows = per_sm * b;
+            best = b;
+        }
+    }
+    slot.store(best, std::memory_order_relaxed);
+    return best;
+}
+
 static const RowSpan kNoSpan{};
 
 cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st)
@@ -920,8 +1001,11 @@ cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st)
 
 cudaError_t launch_assemble(const ClothDev& c, int block, cudaStream_t st)
 {
+    if (block <= 0) block = assemble_block_for(c.max_deg, false);
     const size_t smem = assemble_smem_bytes(c, block);
-    cudaError_t e = cudaFuncSetAttribute(k_assemble<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (smem > kAssembleSmemLimit) return cudaErrorInvalidValue;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_assemble<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAssembleSmemLimit);
     if (e != cudaSuccess) return e;
     k_assemble<false><<<blocks_for(c.n, block), block, smem, st>>>(c, kNoSpan);
     count_launches(1);
@@ -1010,8 +1094,11 @@ cudaError_t launch_span_contacts_update(const RowSpan& sp, cudaStream_t st)
 cudaError_t launch_span_assemble(const RowSpan& sp, int block, cudaStream_t st)
 {
     if (!sp.total) return cudaSuccess;
+    if (block <= 0) block = assemble_block_for(sp.max_deg, true);
     const size_t smem = (size_t)sp.max_deg * 18 * sizeof(float) * block + (size_t)sp.max_deg * block;
-    cudaError_t e = cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (smem > kAssembleSmemLimit) return cudaErrorInvalidValue;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAssembleSmemLimit);
     if (e != cudaSuccess) return e;
     k_assemble<true><<<blocks_for(sp.total, block), block, smem, st>>>(g_unused_one, sp);
     count_launches(1);

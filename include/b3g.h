@@ -272,6 +272,7 @@ typedef struct {
     uint32_t cg_iterations_total;
     uint32_t cg_iterations_max;
     float step_ms;                 /* device time of the whole batch step (CUDA events) */
+    float cg_ms;                   /* device time of its batched CG launch */
 } b3g_batch_stats;
 
 /* capacity: most cloths one step call may pass */

@@ -92,3 +92,29 @@ def test_autotune_picks_a_valid_schedule(b3g):
     for c, x in zip(cloths, before):  # autotuning leaves the cloths unchanged
         assert np.array_equal(c.state()["x"], x)
     batch.step(cloths, scenes[0].dt)
+
+
+@pytest.mark.parametrize("cluster,split", [(1, ()), (8, (11, 12))])
+def test_batch_mixed_dot_precisions_equal_alone(b3g, cluster, split):
+    """A batch whose cloths use different dot precisions (FP32, compensated,
+    FP64) runs the kernel that reads each cloth's precision on the device;
+    every cloth's trajectory is bit-identical to stepping it in a batch of
+    its own, which runs the kernel specialised for its precision."""
+    scenes = _mix(b3g)
+    dots = [b3g.DOT_F32, b3g.DOT_COMPENSATED, b3g.DOT_F64, b3g.DOT_F32, b3g.DOT_F64, b3g.DOT_COMPENSATED]
+    mixed = [b3g.Cloth(s.mesh, s.cdef).setup(s, b3g.SolverOptions.relative(1e-4, 200, d))
+             for s, d in zip(scenes, dots)]
+    alone = [b3g.Cloth(s.mesh, s.cdef).setup(s, b3g.SolverOptions.relative(1e-4, 200, d))
+             for s, d in zip(scenes, dots)]
+    bm, ba = b3g.Batch(16), b3g.Batch(16)
+    bm.set_schedule(cluster, split)
+    ba.set_schedule(cluster, split)
+    dt = scenes[0].dt
+    for step in range(8):
+        bm.step(mixed, dt)
+        for c in alone:
+            ba.step([c], dt)
+    for a, m in zip(alone, mixed):
+        sa, sm = a.state(), m.state()
+        for q in ("x", "v", "dv"):
+            assert np.array_equal(sa[q], sm[q]), q
