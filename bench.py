@@ -29,6 +29,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from bounce_b200 import replicas  # noqa: E402  (rank partition and max-over-ranks timing)
+
 METRIC = "cloth vertex-steps/s"
 UNIT = "vertex-steps/s"
 
@@ -185,13 +187,12 @@ def run_ours(args, rank, world):
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
     launches = b3g.kernel_launch_count() - launches0
+    # every rank steps its own replica; the job takes as long as the slowest rank
     dev_s = sum(step_ms) / 1000.0
+    value = replicas.aggregate_rate(n * args.steps, dev_s)
+    dev_s = replicas.max_over_ranks(dev_s)
     if world > 1:
-        t = torch.tensor([dev_s], dtype=torch.float64, device=f"cuda:{dev}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.barrier()
-        dev_s = float(t.item())
-    value = world * n * args.steps / dev_s
 
     # end to end through the public API with host buffers: per step the
     # external forces go host->device, the positions come back device->host
@@ -203,11 +204,7 @@ def run_ours(args, rank, world):
         cloth.step(scene.dt, scene.velocity_iterations, scene.position_iterations)
         cloth.positions(pos)
     e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{dev}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * n * args.steps / e2e_s
+    e2e = replicas.aggregate_rate(n * args.steps, e2e_s)
 
     # per-kernel device times for the roofline
     prof = []
@@ -262,7 +259,12 @@ def run_batched(args, dev: int):
     plain one-cloth-at-a-time GPU path on the same cloths."""
     import bounce_b200 as b3g
 
-    scenes = b3g.batch_scenes(args.batch_count, seed=3)
+    # weak scaling over ranks: the job holds batch_count cloths per rank, and
+    # each rank takes its share of whole cloths (no collective in the step)
+    env = replicas.rank_env()
+    every = b3g.batch_scenes(args.batch_count * env.world, seed=3)
+    shards = replicas.plan_shards([s.mesh.vertex_count for s in every], env.world)
+    scenes = [every[k] for k in shards[env.rank]]
     opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
     cloths = [b3g.Cloth(sc.mesh, sc.cdef, device=dev).setup(sc, opts) for sc in scenes]
     plain = [b3g.Cloth(sc.mesh, sc.cdef, device=dev).setup(sc, opts) for sc in scenes]
@@ -272,15 +274,21 @@ def run_batched(args, dev: int):
     for _ in range(args.warmup):
         batch.step(cloths, dt)
     sched = batch.autotune(cloths, dt)
-    ms, iters = [], []
+    blocks = np.array([c.info()["blocks"] for c in cloths], dtype=np.float64)
+    nrows = np.array([c.n for c in cloths], dtype=np.float64)
+    ms, cg_ms, iters, cg_bytes = [], [], [], []
     launches0 = b3g.kernel_launch_count()
     for _ in range(args.batch_steps):
-        out = batch.step(cloths, dt)
+        out = batch.step(cloths, dt, per_cloth=True)
         ms.append(out["step_ms"])
+        cg_ms.append(out["cg_ms"])
         iters.append(out["cg_iterations_total"] / out["count"])
+        it = np.array([pc["iterations"] for pc in out["per_cloth"]], dtype=np.float64)
+        # the same per-cloth count as the persistent single-cloth solve
+        cg_bytes.append(float(np.sum(40.0 * blocks + 73.0 * nrows + it * (40.0 * blocks + 146.0 * nrows))))
     launches = b3g.kernel_launch_count() - launches0
     # the plain single-instance path, same cloths, same number of steps
-    batched = rows * len(ms) / (sum(ms) / 1000.0)
+    batched = replicas.aggregate_rate(rows * len(ms), sum(ms) / 1000.0)
     plain_v = None
     if not args.skip_plain:
         for _ in range(args.warmup):
@@ -290,16 +298,22 @@ def run_batched(args, dev: int):
         for _ in range(args.batch_steps):
             for c in plain:
                 pms += c.step(dt)["step_ms"]
-        plain_v = rows * args.batch_steps / (pms / 1000.0)
+        plain_v = replicas.aggregate_rate(rows * args.batch_steps, pms / 1000.0)
     for c in cloths + plain:
         c.close()
     batch.close()
-    return {"cloths": len(scenes), "vertices": rows, "vertex_steps_per_s": batched,
+    return {"cloths": int(replicas.sum_over_ranks(len(scenes))), "vertices": int(replicas.sum_over_ranks(rows)),
+            "vertex_steps_per_s": batched,
             "ms_per_step": sum(ms) / len(ms), "plain_vertex_steps_per_s": plain_v,
             "speedup_vs_plain": batched / plain_v if plain_v else None, "cg_iterations_mean": float(np.mean(iters)),
             "schedule": {"cluster": sched["cluster"],
                          "split_size_classes": [k for k, v in enumerate(sched["split_class"]) if v]},
             "gpu_launches": launches, "steps": len(ms),
+            "roofline": {"bound": "hbm", "kernel": "batch_cg", "achieved": sum(cg_bytes) / (sum(cg_ms) / 1e3) / 1e9,
+                         "peak": peaks()[0], "peak_kind": peaks()[1], "unit": "GB/s",
+                         "frac": sum(cg_bytes) / (sum(cg_ms) / 1e3) / 1e9 / peaks()[0],
+                         "algorithmic_bytes_per_launch": sum(cg_bytes) / len(cg_bytes),
+                         "avg_launch_ms": sum(cg_ms) / len(cg_ms), "share": sum(cg_ms) / sum(ms)},
             "l2": "inputs larger than L2 (about 1 GB of resident cloth state)"}
 
 

@@ -159,11 +159,14 @@ b3g_status enqueue(b3g_batch* b, uint32_t count, uint32_t pi, cudaStream_t st, u
     B3G_TRY(launch_span_contacts_update(sp, st));
     B3G_TRY(launch_span_assemble(sp, b->assemble_block, st));
     B3G_TRY(cudaMemsetAsync(b->d_next, 0, sizeof(uint32_t), st));
-    // external records: inside a captured graph these become event nodes, so
-    // the CG launch is timed on every replay
-    B3G_TRY(cudaEventRecordWithFlags(b->ev_cg0, st, cudaEventRecordExternal));
+    // under stream capture the records must be external to become event
+    // nodes, so that the CG launch is timed on every replay of the graph
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    B3G_TRY(cudaStreamIsCapturing(st, &cap));
+    const unsigned rec_flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+    B3G_TRY(cudaEventRecordWithFlags(b->ev_cg0, st, rec_flags));
     B3G_TRY(launch_batch_cg(a, (int)b->sched.cluster, b->dot, 0, st));
-    B3G_TRY(cudaEventRecordWithFlags(b->ev_cg1, st, cudaEventRecordExternal));
+    B3G_TRY(cudaEventRecordWithFlags(b->ev_cg1, st, rec_flags));
     B3G_TRY(launch_span_finalize(sp, st));
     k += 4;
     for (uint32_t it = 1; it < pi && it < (uint32_t)kMaxPosIters; ++it) {
@@ -443,10 +446,12 @@ b3g_status b3g_batch_autotune(b3g_batch* b, b3g_cloth* const* cloths, uint32_t c
         if ((s = time_cg(cand, &cur)) != B3G_OK) return s;
         trace(cand, cur);
         if (cand.cluster > 1) {
-            // largest classes first: keep a class split when that is faster
+            // split every class at or above a threshold, for each threshold from
+            // the largest class down: larger cloths gain the most from a whole
+            // cluster, so the useful split sets are these prefixes
+            b3g_batch_schedule trial = cand;
             for (int cls = 31; cls >= 0; --cls) {
                 if (!present[cls]) continue;
-                b3g_batch_schedule trial = cand;
                 trial.split_class[cls] = 1;
                 float t = 0.0f;
                 if ((s = time_cg(trial, &t)) != B3G_OK) return s;

@@ -287,8 +287,11 @@ b3g_status b3g_batch_step(b3g_batch* batch, b3g_cloth* const* cloths, uint32_t c
 b3g_status b3g_batch_set_schedule(b3g_batch* batch, const b3g_batch_schedule* schedule);
 b3g_status b3g_batch_get_schedule(const b3g_batch* batch, b3g_batch_schedule* schedule);
 /* Project autotuner: times the batched CG on these cloths' current systems
- * for cluster sizes 1/2/4/8 and, per size class, block-per-instance against
- * split-instance; keeps the fastest schedule.  Cloth state is not changed. */
+ * for cluster sizes 1/2/4/8, each with no class split and with every size
+ * class at or above a threshold split over a cluster (block-per-instance
+ * below it), for each threshold; keeps the fastest schedule.  Setting the
+ * environment variable B3G_TRACE_AUTOTUNE=1 prints every timed candidate to
+ * stderr.  Cloth state is not changed. */
 b3g_status b3g_batch_autotune(b3g_batch* batch, b3g_cloth* const* cloths, uint32_t count, float dt,
                               b3g_batch_schedule* out);
 
