@@ -323,8 +323,10 @@ def run_serving(args, dev: int):
     return serving.run_poisson(rate=2000.0, seconds=args.serve_seconds, budget_bytes=150 * 10**9, device=dev)
 
 
-def cpu_reference_sample(side: int, steps: int, warm: int):
-    """The reference (compiled from its sources) stepping the same cloth on one host core."""
+def _reference_worker(job):
+    """One host process: the reference (compiled from its sources) building and
+    stepping one cloth on one core."""
+    side, steps, warm = job
     import oracle
 
     import bounce_b200 as b3g
@@ -340,16 +342,35 @@ def cpu_reference_sample(side: int, steps: int, warm: int):
     for _ in range(steps):
         ref.step(scene.dt, scene.velocity_iterations, scene.position_iterations)
     dt = time.perf_counter() - t0
-    prof = oracle.ref_profile()
-    solve = prof.get("Cloth Solve", (0.0, 0))[0]
-    n = scene.mesh.vertex_count
-    return {"value": n * steps / dt, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": (f"{steps} steps (after {warm} warm-up) of the same {side}x{side} cloth with the reference "
-                       f"b3Cloth::Step minus the inert self-collision pass, CG at the reference's own 20-iteration "
-                       f"rule; {dt / steps:.2f} s/step, of which 'Cloth Solve' {solve / steps:.2f} s/step "
-                       f"({n * steps / max(solve, 1e-9):.3g} vertex-steps/s for the solve alone); "
-                       f"constructor {build_s:.1f} s"),
-            "seconds": dt}
+    solve = oracle.ref_profile().get("Cloth Solve", (0.0, 0))[0]
+    return {"n": scene.mesh.vertex_count, "steps": steps, "seconds": dt, "solve_s": solve, "build_s": build_s}
+
+
+def cpu_reference_sample(side: int, steps: int, warm: int, procs: int = 0):
+    """The reference stepping the headline cloth on the host cores: one
+    independent replica per core (the reference is single-threaded), the
+    rate being the vertex-steps of all replicas over the slowest one's time.
+    The workers start by spawn."""
+    import multiprocessing as mp
+
+    procs = procs or int(os.environ.get("B3G_REFERENCE_PROCS", "0")) or (os.cpu_count() or 1)
+    if procs == 1:
+        outs = [_reference_worker((side, steps, warm))]
+    else:
+        with mp.get_context("spawn").Pool(procs) as pool:
+            outs = pool.map(_reference_worker, [(side, steps, warm)] * procs)
+    n = outs[0]["n"]
+    slowest = max(o["seconds"] for o in outs)
+    per = outs[0]
+    value = sum(o["n"] * o["steps"] for o in outs) / slowest
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": (f"{procs} independent replicas, one per host core, each {steps} steps (after {warm} "
+                       f"warm-up) of the same {side}x{side} cloth with the reference b3Cloth::Step minus the inert "
+                       f"self-collision pass, CG at the reference's own 20-iteration rule; per replica "
+                       f"{per['seconds'] / steps:.2f} s/step, of which 'Cloth Solve' {per['solve_s'] / steps:.2f} "
+                       f"s/step; slowest replica {slowest / steps:.2f} s/step; constructor {per['build_s']:.1f} s; "
+                       f"one core alone: {n * steps / per['seconds']:.3g} vertex-steps/s"),
+            "seconds": slowest}
 
 
 def host_cpu():
