@@ -23,7 +23,8 @@ from .meshes import (DYNAMIC, KINEMATIC, STATIC, ClothDef, Mesh, Scene, batch_sc
                      plain_scene, sphere_scene, stiff_scene)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libb3g.so")
+# B3G_LIBRARY: another build of libb3g.so to load instead of the in-tree one
+LIB_PATH = os.environ.get("B3G_LIBRARY") or os.path.join(HERE, "_lib", "libb3g.so")
 
 STOP_REFERENCE, STOP_RELATIVE = 0, 1
 CG_LAUNCHES, CG_PERSISTENT = 0, 1

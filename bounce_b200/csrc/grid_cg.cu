@@ -184,13 +184,52 @@ __device__ bool grid_total(typename DotT<DOT>::T (&v)[NV], typename DotT<DOT>::T
     return true;
 }
 
+// The row of a one-row thread, kept in registers for the whole solve: its
+// SELL base, degree and column indices (they never change during a solve).
+constexpr int kRegCols = 16;
+struct RegRow {
+    uint32_t base, deg;
+    uint32_t col[kRegCols];
+};
+
+__device__ __forceinline__ void load_reg_row(const ClothDev& c, uint32_t row, RegRow& rr)
+{
+    rr.base = rbase(c, row);
+    rr.deg = c.row_deg[row];
+#pragma unroll
+    for (int k = 0; k < kRegCols; ++k) rr.col[k] = (uint32_t)k < rr.deg ? c.cols[rr.base + 32u * k] : row;
+}
+
+// row_times_direction with the row's columns already in registers: every
+// load of the row (blocks, neighbours' z and p_old) is issued at once.
+__device__ __forceinline__ f3 reg_row_times_direction(const ClothDev& c, const RegRow& rr, const float* z,
+                                                      const float* pold, float beta, bool first)
+{
+    const uint32_t n = c.n;
+    f3 acc = zero3();
+#pragma unroll
+    for (int k = 0; k < kRegCols; ++k) {
+        if ((uint32_t)k < rr.deg) {
+            const m3 a = block_at(c, rr.base + 32u * k);
+            const uint32_t j = rr.col[k];
+            const f3 zj = ld3_l2(z, n, j);
+            const f3 pj = first ? zj : zj + beta * ld3_l2(pold, n, j);
+            acc = acc + a * pj;
+        }
+    }
+    return acc;
+}
+
 // One CG iteration is two phases, each ended by a grid reduction:
 //   A: p = z + beta p_old (own rows, stored), s = S A p (neighbours' p formed
 //      on the fly), p.s                                   -> alpha
 //   B: x += alpha p, r -= alpha s, z = S P^-1 r, r.z     -> delta', beta
 // p alternates between two buffers so that phase A of one iteration never
-// overwrites a direction another CTA is still reading.
-template <int DOT>
+// overwrites a direction another CTA is still reading.  ONE_ROW: every
+// thread owns at most one row of at most kRegCols blocks and keeps its
+// columns and its x, r, z, p and P^-1 in registers for the whole solve;
+// only what neighbours read (z, p) and the solution go to memory.
+template <int DOT, bool ONE_ROW>
 __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ ClothDev c, GridBarrier* bar)
 {
     typedef DotT<DOT> D;
@@ -206,29 +245,52 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ C
     const uint32_t max_iter = sc->max_iter;
     uint32_t epoch = 0;
 
+    const bool act = first_row < n;
+    bool Si = false;
+    RegRow rr;
+    f3 x = zero3(), r = zero3(), z = zero3(), pv = zero3(), p = zero3();
+    if (ONE_ROW && act) load_reg_row(c, first_row, rr);
+
     // x0 = S m_x, r = S (b - A x0), z = S P^-1 r (cloth_force_solver.cpp:90-100)
     T v2[2] = {D::zero(), D::zero()};
     for (uint32_t row = first_row; row < n; row += stride) {
-        const bool Si = dyn(c, row);
-        const uint32_t base = rbase(c, row);
-        const uint32_t deg = c.row_deg[row];
+        const bool Sr = dyn(c, row);
         f3 ax = zero3();
-        for (uint32_t k = 0; k < deg; ++k) {
-            const uint32_t idx = base + 32u * k;
-            const uint32_t col = c.cols[idx];
-            const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
-            ax = ax + block_at(c, idx) * xj;
+        if (ONE_ROW) {
+#pragma unroll
+            for (int k = 0; k < kRegCols; ++k) {
+                if ((uint32_t)k < rr.deg) {
+                    const uint32_t col = rr.col[k];
+                    const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
+                    ax = ax + block_at(c, rr.base + 32u * k) * xj;
+                }
+            }
+        } else {
+            const uint32_t base = rbase(c, row);
+            const uint32_t deg = c.row_deg[row];
+            for (uint32_t k = 0; k < deg; ++k) {
+                const uint32_t idx = base + 32u * k;
+                const uint32_t col = c.cols[idx];
+                const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
+                ax = ax + block_at(c, idx) * xj;
+            }
         }
         const f3 bi = ld3(c.b, n, row);
-        const f3 pv = ld3(c.pinv, n, row);
-        const f3 r = Si ? bi - ax : zero3();
-        const f3 z = Si ? mk(r.x * pv.x, r.y * pv.y, r.z * pv.z) : zero3();
-        const f3 bh = Si ? bi : zero3();
-        st3(c.dv, n, row, Si ? ld3(c.mx, n, row) : zero3());
-        st3(c.r, n, row, r);
-        st3(c.z, n, row, z);
-        v2[0] = D::add_term(v2[0], bh, mk(bh.x * pv.x, bh.y * pv.y, bh.z * pv.z));
-        v2[1] = D::add_term(v2[1], r, z);
+        const f3 pvr = ld3(c.pinv, n, row);
+        const f3 rv = Sr ? bi - ax : zero3();
+        const f3 zv = Sr ? mk(rv.x * pvr.x, rv.y * pvr.y, rv.z * pvr.z) : zero3();
+        const f3 bh = Sr ? bi : zero3();
+        const f3 x0 = Sr ? ld3(c.mx, n, row) : zero3();
+        st3(c.z, n, row, zv);
+        if (ONE_ROW) {
+            Si = Sr, x = x0, r = rv, z = zv, pv = pvr;
+        } else {
+            st3(c.dv, n, row, x0);
+            st3(c.r, n, row, rv);
+        }
+        v2[0] = D::add_term(v2[0], bh, mk(bh.x * pvr.x, bh.y * pvr.y, bh.z * pvr.z));
+        v2[1] = D::add_term(v2[1], rv, zv);
+        if (ONE_ROW) break;
     }
     if (!grid_total<DOT, 2>(v2, part0, bar, nb, epoch)) goto timeout;
     {
@@ -249,29 +311,51 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ C
             // A: p = S (P^-1 r + beta p) (cloth_force_solver.cpp:130-131, folded
             // into the next SpMV), s = S A p, alpha = delta / p.s
             T v1[1] = {D::zero()};
-            for (uint32_t row = first_row; row < n; row += stride) {
-                const f3 zi = ld3(c.z, n, row);
-                const f3 p = first ? zi : zi + beta * ld3(pold, n, row);
-                const f3 ap = row_times_direction(c, row, c.z, pold, beta, first);
-                const f3 s = dyn(c, row) ? ap : zero3();
-                st3(pnew, n, row, p);
-                st3(c.s, n, row, s);
-                v1[0] = D::add_term(v1[0], p, s);
+            f3 s = zero3();
+            if (ONE_ROW) {
+                if (act) {
+                    p = first ? z : z + beta * p;
+                    const f3 ap = reg_row_times_direction(c, rr, c.z, pold, beta, first);
+                    s = Si ? ap : zero3();
+                    st3(pnew, n, first_row, p);
+                    v1[0] = D::add_term(v1[0], p, s);
+                }
+            } else {
+                for (uint32_t row = first_row; row < n; row += stride) {
+                    const f3 zi = ld3(c.z, n, row);
+                    const f3 pr = first ? zi : zi + beta * ld3(pold, n, row);
+                    const f3 ap = row_times_direction(c, row, c.z, pold, beta, first);
+                    const f3 sr = dyn(c, row) ? ap : zero3();
+                    st3(pnew, n, row, pr);
+                    st3(c.s, n, row, sr);
+                    v1[0] = D::add_term(v1[0], pr, sr);
+                }
             }
             if (!grid_total<DOT, 1>(v1, part1, bar, nb, epoch)) goto timeout;
             const double pAp = D::value(v1[0]);
             const float alpha = DOT == 2 ? (float)(delta / pAp) : (float)delta / (float)pAp;
             // B: x += alpha p, r -= alpha s, z = S P^-1 r, delta' = r.P^-1 r
             T u1[1] = {D::zero()};
-            for (uint32_t row = first_row; row < n; row += stride) {
-                const f3 x = ld3(c.dv, n, row) + alpha * ld3(pnew, n, row);
-                const f3 r = ld3(c.r, n, row) - alpha * ld3(c.s, n, row);
-                const f3 pv = ld3(c.pinv, n, row);
-                const f3 h = mk(r.x * pv.x, r.y * pv.y, r.z * pv.z);
-                st3(c.dv, n, row, x);
-                st3(c.r, n, row, r);
-                st3(c.z, n, row, dyn(c, row) ? h : zero3());
-                u1[0] = D::add_term(u1[0], r, h);
+            if (ONE_ROW) {
+                if (act) {
+                    x = x + alpha * p;
+                    r = r - alpha * s;
+                    const f3 h = mk(r.x * pv.x, r.y * pv.y, r.z * pv.z);
+                    z = Si ? h : zero3();
+                    st3(c.z, n, first_row, z);
+                    u1[0] = D::add_term(u1[0], r, h);
+                }
+            } else {
+                for (uint32_t row = first_row; row < n; row += stride) {
+                    const f3 xr = ld3(c.dv, n, row) + alpha * ld3(pnew, n, row);
+                    const f3 rv = ld3(c.r, n, row) - alpha * ld3(c.s, n, row);
+                    const f3 pvr = ld3(c.pinv, n, row);
+                    const f3 h = mk(rv.x * pvr.x, rv.y * pvr.y, rv.z * pvr.z);
+                    st3(c.dv, n, row, xr);
+                    st3(c.r, n, row, rv);
+                    st3(c.z, n, row, dyn(c, row) ? h : zero3());
+                    u1[0] = D::add_term(u1[0], rv, h);
+                }
             }
             if (!grid_total<DOT, 1>(u1, part0, bar, nb, epoch)) goto timeout;
             double dn = D::value(u1[0]);
@@ -286,6 +370,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ C
             if (!isfinite(dn) || !isfinite(alpha) || !isfinite(beta)) status = kStatusNumerical;
             cont = status == 0 && it < max_iter && !cg_stop(sc, dn, b_delta);
         }
+        if (ONE_ROW && act) st3(c.dv, n, first_row, x);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             sc->b_delta = b_delta;
             sc->delta0 = delta0;
@@ -303,6 +388,12 @@ timeout:
     }
 }
 
+template <int DOT>
+const void* grid_kernel(bool one_row)
+{
+    return one_row ? (const void*)k_grid_cg<DOT, true> : (const void*)k_grid_cg<DOT, false>;
+}
+
 }  // namespace
 
 GridCgShape grid_cg_shape(uint32_t n, int device)
@@ -317,7 +408,7 @@ GridCgShape grid_cg_shape(uint32_t n, int device)
         g.blocks = (int)((n + g.threads - 1) / g.threads);
     } else {
         int per_sm = 1;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_cg<2>, kMaxBlock, 0) != cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_cg<2, false>, kMaxBlock, 0) != cudaSuccess ||
             per_sm < 1) {
             cudaGetLastError();
             per_sm = 1;
@@ -334,6 +425,7 @@ cudaError_t launch_grid_cg(const ClothDev& c, int dot, GridBarrier* bar, cudaStr
     int dev = 0;
     cudaGetDevice(&dev);
     const GridCgShape g = grid_cg_shape(c.n, dev);
+    const bool one_row = (uint64_t)g.blocks * (uint64_t)g.threads >= c.n && c.max_deg <= (uint32_t)kRegCols;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(g.blocks);
     cfg.blockDim = dim3(g.threads);
@@ -343,10 +435,9 @@ cudaError_t launch_grid_cg(const ClothDev& c, int dot, GridBarrier* bar, cudaStr
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaError_t e;
-    if (dot == 2) e = cudaLaunchKernelEx(&cfg, k_grid_cg<2>, c, bar);
-    else if (dot == 1) e = cudaLaunchKernelEx(&cfg, k_grid_cg<1>, c, bar);
-    else e = cudaLaunchKernelEx(&cfg, k_grid_cg<0>, c, bar);
+    const void* fn = dot == 2 ? grid_kernel<2>(one_row) : dot == 1 ? grid_kernel<1>(one_row) : grid_kernel<0>(one_row);
+    void* args[2] = {const_cast<ClothDev*>(&c), &bar};
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     count_launches(1);
     return e;
 }
