@@ -105,7 +105,7 @@ template <bool L2ONLY>
 __device__ __forceinline__ f3 row_times_direction(const ClothDev& c, uint32_t row, const float* pold, float beta,
                                                   bool first)
 {
-    constexpr int W = 4;  // blocks whose loads are issued together (64 registers)
+    constexpr int W = 8;  // blocks whose loads are issued together (85 registers: 3 CTAs per SM)
     const uint32_t base = rbase(c, row);
     const uint32_t deg = c.row_deg[row];
     const uint32_t n = c.n, E = c.E;
@@ -279,7 +279,7 @@ __device__ __forceinline__ void run_cg(const ClothDev& c, double* wsum, double* 
 // cloths, one per CTA (team_cg<1>, block-per-instance).  The host orders the
 // tasks largest first; clusters take them from a queue.
 template <int T, int DOTSEL>
-__global__ void __launch_bounds__(kBlock, 4) k_batch_cg(const __grid_constant__ BatchCgArgs a)
+__global__ void __launch_bounds__(kBlock, 3) k_batch_cg(const __grid_constant__ BatchCgArgs a)
 {
     __shared__ double wsum[2 * kWarps];
     __shared__ double slot[4];  // two alternating reduction buffers of 2 values
