@@ -165,6 +165,30 @@ struct RowAcc {
         const float* p = base + (slot * 18) * B + tid;
         return m3{f3{p[0], p[B], p[2 * B]}, f3{p[3 * B], p[4 * B], p[5 * B]}, f3{p[6 * B], p[7 * B], p[8 * B]}};
     }
+    // the slot's dfdx accumulator, marking its first touch
+    __device__ m3 touchK(int slot)
+    {
+        if (!(touched & (1ull << slot))) {
+            touched |= 1ull << slot;
+            touch[ntouch * B + tid] = (uint8_t)slot;
+            ++ntouch;
+        }
+        return getK(slot);
+    }
+    __device__ void setK(int slot, const m3& m)
+    {
+        float* p = base + (slot * 18) * B + tid;
+        p[0 * B] = m.x.x; p[1 * B] = m.x.y; p[2 * B] = m.x.z;
+        p[3 * B] = m.y.x; p[4 * B] = m.y.y; p[5 * B] = m.y.z;
+        p[6 * B] = m.z.x; p[7 * B] = m.z.y; p[8 * B] = m.z.z;
+    }
+    __device__ void setD(int slot, const m3& m)
+    {
+        float* p = base + (slot * 18 + 9) * B + tid;
+        p[0 * B] = m.x.x; p[1 * B] = m.x.y; p[2 * B] = m.x.z;
+        p[3 * B] = m.y.x; p[4 * B] = m.y.y; p[5 * B] = m.y.z;
+        p[6 * B] = m.z.x; p[7 * B] = m.z.y; p[8 * B] = m.z.z;
+    }
     // reuse of a slot's dfdv area after A is stored: v and y of its column
     __device__ void setD6(int slot, const f3& a, const f3& b)
     {
@@ -234,6 +258,13 @@ __device__ __forceinline__ T corner(int cn, const T& a0, const T& a1, const T& a
 
 // b3ShearForce::Apply then b3StrechForce::Apply (the force list holds the
 // shear element of a triangle before its stretch element) for corner `cn`.
+//
+// A slot of the row receives up to three dfdx terms from the triangle -- the
+// shear term, then the stretch terms along u and along v -- and likewise
+// three dfdv terms.  The reference adds them one by one in that order
+// (shear_force.cpp:142-207, strech_force.cpp:151-325); here every factor is
+// computed first, then each slot's accumulators are read once, the present
+// terms added in the same order, and written back once.
 __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn, const int slot[3], f3& f_row)
 {
     const uint4 tv = c.tri[t];
@@ -250,69 +281,88 @@ __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn,
     const float dwvdx[3] = {inv_det * (du2 - du1), -inv_det * du2, inv_det * du1};
     const float kd = c.k_damp;
 
-    if (c.k_shear > 0.0f) {  // shear_force.cpp:57-212
-        const float ks = c.k_shear;
-        f3 dC[3];
+    // shear (shear_force.cpp:57-212)
+    const bool sh = c.k_shear > 0.0f;
+    const float ks_sh = c.k_shear;
+    const bool shK = sh && ks_sh > 0.0f, shD = sh && kd > 0.0f;
+    f3 dCs[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) dC[i] = alpha * (dwudx[i] * wv + dwvdx[i] * wu);
-        const f3 dCc = corner(cn, dC[0], dC[1], dC[2]);
+    for (int i = 0; i < 3; ++i) dCs[i] = alpha * (dwudx[i] * wv + dwvdx[i] * wu);
+    const f3 dCsc = corner(cn, dCs[0], dCs[1], dCs[2]);
+    if (sh) {
         f3 fe = zero3();
-        if (ks > 0.0f) {
+        if (shK) {
             const float C = alpha * dot(wu, wv);
-            fe = fe + (-ks * C) * dCc;
-#pragma unroll
-            for (int j = 0; j < 3; ++j) acc.addK(slot[j], -ks * outer(dCc, dC[j]));
+            fe = fe + (-ks_sh * C) * dCsc;
         }
-        if (kd > 0.0f) {
+        if (shD) {
             float dCdt = 0.0f;
 #pragma unroll
-            for (int i = 0; i < 3; ++i) dCdt += dot(dC[i], vs[i]);
-            fe = fe + (-kd * dCdt) * dCc;
-#pragma unroll
-            for (int j = 0; j < 3; ++j) acc.addD(slot[j], -kd * outer(dCc, dC[j]));
+            for (int i = 0; i < 3; ++i) dCdt += dot(dCs[i], vs[i]);
+            fe = fe + (-kd * dCdt) * dCsc;
         }
         f_row = f_row + fe;
     }
-    if (c.k_stretch > 0.0f) {  // strech_force.cpp:59-329, bu = bv = 1 (cloth.cpp:198-199)
-        const float ks = c.k_stretch;
-        const float len_wu = length(wu);
-        const float len_wv = length(wv);
-        const m3 I = mident();
+
+    // stretch along u (d = 0) and v (d = 1) (strech_force.cpp:59-329, bu = bv = 1, cloth.cpp:198-199)
+    const bool st = c.k_stretch > 0.0f;
+    const float ks = c.k_stretch;
+    const m3 I = mident();
+    bool K_on[2], D_on[2];
+    f3 dCst[2][3], dCstc[2];
+    float Cst[2], kfac[2][3];  // (alpha * inv_len * dw[cn] * dw[j]) of the second-derivative term
+    m3 P[2];
+    {
         f3 fe = zero3();
 #pragma unroll
         for (int d = 0; d < 2; ++d) {
             const f3 w = d == 0 ? wu : wv;
-            const float len = d == 0 ? len_wu : len_wv;
+            const float len = d == 0 ? length(wu) : length(wv);
             const float dw[3] = {d == 0 ? dwudx[0] : dwvdx[0], d == 0 ? dwudx[1] : dwvdx[1],
                                  d == 0 ? dwudx[2] : dwvdx[2]};
-            if (!(len > 0.0f)) continue;
-            const float dwc = corner(cn, dw[0], dw[1], dw[2]);
+            const bool live = st && len > 0.0f;
             const float inv_len = 1.0f / len;
             const f3 nw = inv_len * w;
-            f3 dC[3];
 #pragma unroll
-            for (int i = 0; i < 3; ++i) dC[i] = (alpha * dw[i]) * nw;
-            const f3 dCc = corner(cn, dC[0], dC[1], dC[2]);
-            if (ks > 0.0f && len > 1.0f) {
-                const float C = alpha * (len - 1.0f);
-                fe = fe + (-ks * C) * dCc;
-                const m3 P = I - outer(nw, nw);
+            for (int i = 0; i < 3; ++i) dCst[d][i] = (alpha * dw[i]) * nw;
+            dCstc[d] = corner(cn, dCst[d][0], dCst[d][1], dCst[d][2]);
+            K_on[d] = live && ks > 0.0f && len > 1.0f;
+            D_on[d] = live && kd > 0.0f;
+            Cst[d] = alpha * (len - 1.0f);
+            const float dwc = corner(cn, dw[0], dw[1], dw[2]);
 #pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const m3 d2 = (alpha * inv_len * dwc * dw[j]) * P;
-                    acc.addK(slot[j], -ks * (outer(dCc, dC[j]) + C * d2));
-                }
-            }
-            if (kd > 0.0f) {
+            for (int j = 0; j < 3; ++j) kfac[d][j] = alpha * inv_len * dwc * dw[j];
+            P[d] = I - outer(nw, nw);
+            if (K_on[d]) fe = fe + (-ks * Cst[d]) * dCstc[d];
+            if (D_on[d]) {
                 float dCdt = 0.0f;
 #pragma unroll
-                for (int i = 0; i < 3; ++i) dCdt += dot(dC[i], vs[i]);
-                fe = fe + (-kd * dCdt) * dCc;
-#pragma unroll
-                for (int j = 0; j < 3; ++j) acc.addD(slot[j], -kd * outer(dCc, dC[j]));
+                for (int i = 0; i < 3; ++i) dCdt += dot(dCst[d][i], vs[i]);
+                fe = fe + (-kd * dCdt) * dCstc[d];
             }
         }
-        f_row = f_row + fe;
+        if (st) f_row = f_row + fe;
+    }
+
+    // per slot, in the reference's order: shear, stretch u, stretch v
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        if (shK || K_on[0] || K_on[1]) {
+            m3 k = acc.touchK(slot[j]);
+            if (shK) k = k + -ks_sh * outer(dCsc, dCs[j]);
+#pragma unroll
+            for (int d = 0; d < 2; ++d)
+                if (K_on[d]) k = k + -ks * (outer(dCstc[d], dCst[d][j]) + Cst[d] * (kfac[d][j] * P[d]));
+            acc.setK(slot[j], k);
+        }
+        if (shD || D_on[0] || D_on[1]) {
+            m3 dm = acc.getD(slot[j]);
+            if (shD) dm = dm + -kd * outer(dCsc, dCs[j]);
+#pragma unroll
+            for (int d = 0; d < 2; ++d)
+                if (D_on[d]) dm = dm + -kd * outer(dCstc[d], dCst[d][j]);
+            acc.setD(slot[j], dm);
+        }
     }
 }
 
