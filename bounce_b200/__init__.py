@@ -19,7 +19,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .meshes import (DYNAMIC, KINEMATIC, STATIC, ClothDef, Mesh, Scene, batch_scenes, grid_mesh,  # noqa: F401
+from .meshes import (DYNAMIC, KINEMATIC, STATIC, ClothDef, Mesh, Scene, batch_scenes, grid_mesh, sewn_scene,  # noqa: F401
                      plain_scene, sphere_scene, stiff_scene)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -65,6 +65,16 @@ class PhaseTimesC(C.Structure):
                                           "cg_update_ms", "cg_direction_ms", "finalize_ms",
                                           "contact_position_ms", "post_ms")] + \
                [("cg_iterations", C.c_uint32), ("contact_position_launches", C.c_uint32)]
+
+
+class ParticleDefC(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("velocity", C.c_float * 3), ("force", C.c_float * 3),
+                ("mass", C.c_float), ("radius", C.c_float), ("friction", C.c_float)]
+
+
+class MouseForceDefC(C.Structure):
+    _fields_ = [("particle", C.c_uint32), ("triangle", C.c_uint32), ("w2", C.c_float), ("w3", C.c_float),
+                ("w4", C.c_float), ("mouse", C.c_float), ("damping", C.c_float)]
 
 
 class ClothInfoC(C.Structure):
@@ -126,6 +136,10 @@ def lib() -> C.CDLL:
             "b3g_cloth_set_solver": [vp, C.POINTER(SolverOptsC)],
             "b3g_cloth_add_static_sphere": [vp, vp, f32, f32, C.POINTER(u32)],
             "b3g_cloth_clear_colliders": [vp],
+            "b3g_cloth_create_particle": [vp, C.POINTER(ParticleDefC), C.POINTER(u32)],
+            "b3g_cloth_destroy_particle": [vp, u32],
+            "b3g_cloth_create_mouse_force": [vp, C.POINTER(MouseForceDefC), C.POINTER(u32)],
+            "b3g_cloth_destroy_force": [vp, u32],
             "b3g_particle_set_type": [vp, u32, i32],
             "b3g_particle_get_type": [vp, u32, C.POINTER(i32)],
             "b3g_particle_set_position": [vp, u32, vp],
@@ -276,7 +290,8 @@ class Cloth:
         h = C.c_void_p()
         check(L.b3g_cloth_create(C.byref(md), C.byref(d), device, C.byref(h)), "b3g_cloth_create")
         self.h = h
-        self.n = mesh.vertex_count
+        self.n_mesh = mesh.vertex_count
+        self.n = mesh.vertex_count      # particles: the mesh's, then created ones
         self.nsph = 0
         self.stats = StepStatsC()
 
@@ -286,6 +301,32 @@ class Cloth:
             self.h = None
 
     __del__ = close
+
+    # created particles and mouse forces (b3Cloth::CreateParticle / CreateForce)
+    def create_particle(self, position, velocity=(0.0, 0.0, 0.0), force=(0.0, 0.0, 0.0), mass: float = 0.0,
+                        radius: float = 0.0, friction: float = 0.0) -> int:
+        """A particle outside the mesh (mass 0: static); returns its index."""
+        d = ParticleDefC((C.c_float * 3)(*_f3(position)), (C.c_float * 3)(*_f3(velocity)),
+                         (C.c_float * 3)(*_f3(force)), mass, radius, friction)
+        idx = C.c_uint32(0)
+        check(lib().b3g_cloth_create_particle(self.h, C.byref(d), C.byref(idx)), "create_particle")
+        self.n = int(lib().b3g_cloth_vertex_count(self.h))
+        return int(idx.value)
+
+    def destroy_particle(self, index: int) -> None:
+        check(lib().b3g_cloth_destroy_particle(self.h, index), "destroy_particle")
+        self.n = int(lib().b3g_cloth_vertex_count(self.h))
+
+    def create_mouse_force(self, particle: int, triangle: int, w2: float, w3: float, w4: float, mouse: float,
+                           damping: float) -> int:
+        """Ties `particle` to the point w2 x(v1) + w3 x(v2) + w4 x(v3) of `triangle`; returns the force id."""
+        d = MouseForceDefC(particle, triangle, w2, w3, w4, mouse, damping)
+        fid = C.c_uint32(0)
+        check(lib().b3g_cloth_create_mouse_force(self.h, C.byref(d), C.byref(fid)), "create_mouse_force")
+        return int(fid.value)
+
+    def destroy_force(self, force_id: int) -> None:
+        check(lib().b3g_cloth_destroy_force(self.h, force_id), "destroy_force")
 
     # b3Cloth API
     def set_gravity(self, g) -> None:

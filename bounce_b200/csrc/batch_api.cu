@@ -83,6 +83,7 @@ struct b3g_batch {
     // graph cache
     cudaGraphExec_t exec = nullptr;
     std::vector<b3g_cloth*> graph_list;
+    std::vector<uint32_t> graph_layouts;  // each listed cloth's layout version when the graph was built
     uint32_t graph_pi = UINT32_MAX, graph_sched = 0;
     uint32_t graph_kernels = 0;
     uint32_t ntasks = 0, total_rows = 0, max_deg = 0;
@@ -97,6 +98,7 @@ void destroy_graph(b3g_batch* b)
     if (b->exec) cudaGraphExecDestroy(b->exec);
     b->exec = nullptr;
     b->graph_list.clear();
+    b->graph_layouts.clear();
 }
 
 // Host-side launch plan of a cloth list: row prefix sums, the CG task list
@@ -302,8 +304,10 @@ b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t coun
         B3G_TRY(cudaEventRecord(b->ev1, st));
         B3G_TRY(cudaStreamSynchronize(st));
     }
-    const bool same = !use_graph || (b->exec && b->graph_pi == pos_iters && b->graph_sched == b->sched_version &&
-                      b->graph_list.size() == count && std::equal(b->graph_list.begin(), b->graph_list.end(), cloths));
+    bool same = !use_graph || (b->exec && b->graph_pi == pos_iters && b->graph_sched == b->sched_version &&
+                b->graph_list.size() == count && std::equal(b->graph_list.begin(), b->graph_list.end(), cloths));
+    // a cloth laid out again (particles or forces created) has new sizes and buffers
+    for (uint32_t k = 0; same && use_graph && k < count; ++k) same = b->graph_layouts[k] == cloths[k]->layout_version;
     if (!same) {
         destroy_graph(b);
         plan(b, cloths, count);
@@ -325,6 +329,8 @@ b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t coun
             return from_cuda(e);
         }
         b->graph_list.assign(cloths, cloths + count);
+        b->graph_layouts.resize(count);
+        for (uint32_t k = 0; k < count; ++k) b->graph_layouts[k] = cloths[k]->layout_version;
         b->graph_pi = pos_iters;
         b->graph_sched = b->sched_version;
         b->graph_kernels = kern;

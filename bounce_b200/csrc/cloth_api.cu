@@ -2,6 +2,7 @@
 // per-step CUDA graph, particle edits and state transfers.
 #include <algorithm>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -230,23 +231,45 @@ b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3
         return B3G_ERR_INVALID_ARGUMENT;
     if (!(def->density > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
     *out = nullptr;
-    const float d8[8] = {def->density, def->streching, def->shearing, def->bending,
-                         def->sewing,  def->damping,   def->thickness, def->friction};
     b3g_cloth* c = new (std::nothrow) b3g_cloth();
     if (!c) return B3G_ERR_OUT_OF_MEMORY;
-    int rc = build_topology(mesh->vertex_count, mesh->vertices, mesh->triangle_count, mesh->triangles,
-                            mesh->sewing_line_count, mesh->sewing_lines, d8, &c->topo);
-    if (rc != 0) {
+    c->in_vertices.assign(mesh->vertices, mesh->vertices + 3 * (size_t)mesh->vertex_count);
+    c->in_tris.assign(mesh->triangles, mesh->triangles + 3 * (size_t)mesh->triangle_count);
+    if (mesh->sewing_line_count)
+        c->in_sewing.assign(mesh->sewing_lines, mesh->sewing_lines + 4 * (size_t)mesh->sewing_line_count);
+    c->in_def = *def;
+    const b3g_status s = layout_cloth(c);
+    if (s != B3G_OK) {
         delete c;
-        return (b3g_status)rc;
+        return s;
     }
+    *out = c;
+    return B3G_OK;
+}
+
+// The topology, device scalars, arena size and host images of the cloth's
+// current particles and forces: the mesh's, the created particles (after the
+// mesh vertices) and the mouse forces.  Keeps the colliders.
+b3g_status layout_cloth(b3g_cloth* c)
+{
+    const b3g_cloth_def* def = &c->in_def;
+    const float d8[8] = {def->density, def->streching, def->shearing, def->bending,
+                         def->sewing,  def->damping,   def->thickness, def->friction};
+    const uint32_t n_mesh = (uint32_t)(c->in_vertices.size() / 3);
+    ClothTopology topo;
+    int rc = build_topology(n_mesh, c->in_vertices.data(), (uint32_t)(c->in_tris.size() / 3), c->in_tris.data(),
+                            (uint32_t)(c->in_sewing.size() / 4), c->in_sewing.empty() ? nullptr : c->in_sewing.data(),
+                            d8, &topo, c->n_extra, c->mice.data(), (uint32_t)c->mice.size());
+    if (rc != 0) return (b3g_status)rc;
+    c->topo = std::move(topo);
     const ClothTopology& T = c->topo;
     const uint32_t n = T.n, t = T.t, ns = T.ns;
+    const uint32_t nmouse = (uint32_t)c->mice.size();
     ClothDev& d = c->dev;
     d.n = n;
     d.t = t;
     d.ns = ns;
-    d.nsph = 0;
+    d.nmouse = nmouse;
     d.nslices = T.nslices;
     d.max_deg = T.max_deg;
     d.E = T.E;
@@ -264,6 +287,7 @@ b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3
     add((T.nslices + 1) * 4); add(n); add((size_t)T.E * 4); add((size_t)T.E * 36);
     add((n + 1) * 4); add(T.inc_elem.size() * 4 + 4); add(T.inc_meta.size() * 4 + 4);
     add((size_t)t * 16); add((size_t)t * 16); add((size_t)t * 8); add((size_t)ns * 8 + 8); add((size_t)ns * 16 + 16);
+    add((size_t)nmouse * 16 + 16); add((size_t)nmouse * 32 + 32);  // mouse forces
     for (int k = 0; k < 13; ++k) add(vec);  // x v fext y mx b dv r p s pinv z p2
     add((size_t)n * 4); add(n);             // mass, type
     add(vec); add(vec);                     // fat lo / hi
@@ -276,15 +300,13 @@ b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3
     c->arena.size = bytes + 256;
 
     HostImages* im = new (std::nothrow) HostImages();
-    if (!im) {
-        delete c;
-        return B3G_ERR_OUT_OF_MEMORY;
-    }
+    if (!im) return B3G_ERR_OUT_OF_MEMORY;
+    const uint32_t* tris = c->in_tris.data();
     im->tri.resize(t);
     im->rest.resize(t);
     im->rest2.resize(t);
     for (uint32_t k = 0; k < t; ++k) {
-        im->tri[k] = make_uint4(mesh->triangles[3 * k], mesh->triangles[3 * k + 1], mesh->triangles[3 * k + 2], 0u);
+        im->tri[k] = make_uint4(tris[3 * k], tris[3 * k + 1], tris[3 * k + 2], 0u);
         const float* r = &T.rest[6 * (size_t)k];
         im->rest[k] = make_float4(r[0], r[1], r[2], r[3]);
         im->rest2[k] = make_float2(r[4], r[5]);
@@ -295,13 +317,24 @@ b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3
         im->spr[q] = make_uint2(T.spring_pairs[2 * q], T.spring_pairs[2 * q + 1]);
         im->sp[q] = make_float4(T.spring_par[3 * q], T.spring_par[3 * q + 1], T.spring_par[3 * q + 2], 0.0f);
     }
-    im->x.resize(3 * (size_t)n);
-    im->lo.resize(3 * (size_t)n);
-    im->hi.resize(3 * (size_t)n);
+    im->mouse_v.resize(nmouse + 1);
+    im->mouse_par.resize(2 * (size_t)nmouse + 2);
+    for (uint32_t m = 0; m < nmouse; ++m) {
+        const MouseForceDesc& f = c->mice[m];
+        const uint32_t* tv = tris + 3 * (size_t)f.triangle;
+        im->mouse_v[m] = make_uint4(f.particle, tv[0], tv[1], tv[2]);
+        im->mouse_par[2 * m] = make_float4(f.w2, f.w3, f.w4, f.mouse);
+        im->mouse_par[2 * m + 1] = make_float4(f.damping, 0.0f, 0.0f, 0.0f);
+    }
+    // mesh vertices at their creation positions; created particles are
+    // written by the caller that created them
+    im->x.assign(3 * (size_t)n, 0.0f);
+    im->lo.assign(3 * (size_t)n, 0.0f);
+    im->hi.assign(3 * (size_t)n, 0.0f);
     const float r = def->thickness;
-    for (uint32_t i = 0; i < n; ++i)
+    for (uint32_t i = 0; i < n_mesh; ++i)
         for (int q = 0; q < 3; ++q) {
-            float x = mesh->vertices[3 * i + q];
+            float x = c->in_vertices[3 * (size_t)i + q];
             im->x[(size_t)q * n + i] = x;
             // proxy at creation: [x - r, x + r] fattened by B3_AABB_EXTENSION (cloth.cpp:312-317)
             im->lo[(size_t)q * n + i] = (x - r) - 0.2f;
@@ -309,7 +342,6 @@ b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3
         }
     im->types.assign(n, (uint8_t)B3G_DYNAMIC);
     c->images.reset(im);
-    *out = c;
     return B3G_OK;
 }
 
@@ -344,6 +376,8 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     float2* tri_rest2 = A.take<float2>(t);
     uint2* spr = A.take<uint2>(ns + 1);
     float4* spr_par = A.take<float4>(ns + 1);
+    uint4* mouse_v = A.take<uint4>(d.nmouse + 1);
+    float4* mouse_par = A.take<float4>(2 * (size_t)d.nmouse + 2);
     d.x = A.take<float>(3 * (size_t)n);
     d.v = A.take<float>(3 * (size_t)n);
     d.fext = A.take<float>(3 * (size_t)n);
@@ -385,6 +419,8 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     d.tri_rest2 = tri_rest2;
     d.spr = spr;
     d.spr_par = spr_par;
+    d.mouse_v = mouse_v;
+    d.mouse_par = mouse_par;
     d.mass = mass;
 
     if (own_stream) {
@@ -416,6 +452,8 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     up(tri_rest2, im.rest2.data(), (size_t)t * 8);
     up(spr, im.spr.data(), (size_t)ns * 8);
     up(spr_par, im.sp.data(), (size_t)ns * 16);
+    up(mouse_v, im.mouse_v.data(), (size_t)d.nmouse * 16);
+    up(mouse_par, im.mouse_par.data(), (size_t)d.nmouse * 32);
     up(d.x, im.x.data(), vec);
     up(mass, T.mass.data(), (size_t)n * 4);
     up(d.type, im.types.data(), n);
@@ -549,6 +587,299 @@ b3g_status b3g_cloth_clear_colliders(b3g_cloth* c)
     destroy_graph(c);
     return B3G_OK;
 }
+
+// ---------------------------------------------------------------------------
+// created particles and forces (cloth.cpp:307-364): the layout is rebuilt
+// around the cloth's current state
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// Every per-particle device array of a cloth, on the host (SoA planes).
+struct ParticleState {
+    uint32_t n = 0, nsph = 0;
+    std::vector<float> x, v, fext, y, mx, lo, hi, mass;
+    std::vector<uint8_t> type, c_exists, c_active;
+    std::vector<uint32_t> c_key;
+    std::vector<float> c_normal, c_t1, c_t2, c_imp;
+};
+
+b3g_status download_state(b3g_cloth* c, ParticleState& s)
+{
+    const ClothDev& d = c->dev;
+    cudaStream_t st = c->stream;
+    s.n = d.n;
+    s.nsph = d.nsph;
+    const size_t n = s.n, nn = (size_t)s.nsph * n;
+    auto get = [&](auto& dst, const void* src, size_t count) {
+        dst.resize(count);
+        return count ? cudaMemcpyAsync(dst.data(), src, count * sizeof(dst[0]), cudaMemcpyDeviceToHost, st)
+                     : cudaSuccess;
+    };
+    B3G_TRY(get(s.x, d.x, 3 * n));
+    B3G_TRY(get(s.v, d.v, 3 * n));
+    B3G_TRY(get(s.fext, d.fext, 3 * n));
+    B3G_TRY(get(s.y, d.y, 3 * n));
+    B3G_TRY(get(s.mx, d.mx, 3 * n));
+    B3G_TRY(get(s.lo, d.fat_lo, 3 * n));
+    B3G_TRY(get(s.hi, d.fat_hi, 3 * n));
+    B3G_TRY(get(s.mass, d.mass, n));
+    B3G_TRY(get(s.type, d.type, n));
+    B3G_TRY(get(s.c_exists, d.c_exists, nn));
+    B3G_TRY(get(s.c_active, d.c_active, nn));
+    B3G_TRY(get(s.c_key, d.c_key, nn));
+    B3G_TRY(get(s.c_normal, d.c_normal, 3 * nn));
+    B3G_TRY(get(s.c_t1, d.c_t1, 3 * nn));
+    B3G_TRY(get(s.c_t2, d.c_t2, 3 * nn));
+    B3G_TRY(get(s.c_imp, d.c_imp, 3 * nn));
+    B3G_TRY(cudaStreamSynchronize(st));
+    return B3G_OK;
+}
+
+b3g_status upload_state(b3g_cloth* c, const ParticleState& s)
+{
+    const ClothDev& d = c->dev;
+    cudaStream_t st = c->stream;
+    const size_t n = s.n, nn = (size_t)s.nsph * n;
+    auto put = [&](void* dst, const auto& src, size_t count) {
+        return count ? cudaMemcpyAsync(dst, src.data(), count * sizeof(src[0]), cudaMemcpyHostToDevice, st)
+                     : cudaSuccess;
+    };
+    B3G_TRY(put(d.x, s.x, 3 * n));
+    B3G_TRY(put(d.v, s.v, 3 * n));
+    B3G_TRY(put(d.fext, s.fext, 3 * n));
+    B3G_TRY(put(d.y, s.y, 3 * n));
+    B3G_TRY(put(d.mx, s.mx, 3 * n));
+    B3G_TRY(put(d.fat_lo, s.lo, 3 * n));
+    B3G_TRY(put(d.fat_hi, s.hi, 3 * n));
+    B3G_TRY(put(const_cast<float*>(d.mass), s.mass, n));
+    B3G_TRY(put(d.type, s.type, n));
+    B3G_TRY(put(d.c_exists, s.c_exists, nn));
+    B3G_TRY(put(d.c_active, s.c_active, nn));
+    B3G_TRY(put(d.c_key, s.c_key, nn));
+    B3G_TRY(put(d.c_normal, s.c_normal, 3 * nn));
+    B3G_TRY(put(d.c_t1, s.c_t1, 3 * nn));
+    B3G_TRY(put(d.c_t2, s.c_t2, 3 * nn));
+    B3G_TRY(put(d.c_imp, s.c_imp, 3 * nn));
+    return B3G_OK;
+}
+
+// The state of a new particle set: particle k of the result is old particle
+// keep[k], or a zeroed new one when keep[k] is kNone.
+constexpr uint32_t kNone = 0xffffffffu;
+
+ParticleState remap(const ParticleState& s, const std::vector<uint32_t>& keep)
+{
+    ParticleState r;
+    r.n = (uint32_t)keep.size();
+    r.nsph = s.nsph;
+    const size_t n0 = s.n, n1 = r.n, nn0 = (size_t)s.nsph * n0, nn1 = (size_t)s.nsph * n1;
+    auto planes = [&](const std::vector<float>& a, std::vector<float>& b, size_t stride0, size_t stride1,
+                      uint32_t groups) {
+        b.assign(stride1 * 3, 0.0f);
+        for (int q = 0; q < 3; ++q)
+            for (uint32_t g = 0; g < groups; ++g)
+                for (size_t k = 0; k < n1; ++k)
+                    if (keep[k] != kNone) b[q * stride1 + g * n1 + k] = a[q * stride0 + g * n0 + keep[k]];
+    };
+    auto column = [&](const auto& a, auto& b, uint32_t groups) {
+        b.assign((size_t)groups * n1, {});
+        for (uint32_t g = 0; g < groups; ++g)
+            for (size_t k = 0; k < n1; ++k)
+                if (keep[k] != kNone) b[g * n1 + k] = a[g * n0 + keep[k]];
+    };
+    planes(s.x, r.x, n0, n1, 1);
+    planes(s.v, r.v, n0, n1, 1);
+    planes(s.fext, r.fext, n0, n1, 1);
+    planes(s.y, r.y, n0, n1, 1);
+    planes(s.mx, r.mx, n0, n1, 1);
+    planes(s.lo, r.lo, n0, n1, 1);
+    planes(s.hi, r.hi, n0, n1, 1);
+    column(s.mass, r.mass, 1);
+    column(s.type, r.type, 1);
+    column(s.c_exists, r.c_exists, s.nsph);
+    column(s.c_active, r.c_active, s.nsph);
+    column(s.c_key, r.c_key, s.nsph);
+    planes(s.c_normal, r.c_normal, nn0, nn1, s.nsph);
+    planes(s.c_t1, r.c_t1, nn0, nn1, s.nsph);
+    planes(s.c_t2, r.c_t2, nn0, nn1, s.nsph);
+    planes(s.c_imp, r.c_imp, nn0, nn1, s.nsph);
+    return r;
+}
+
+// Lays the cloth out again for its current particles and mouse forces
+// (n_extra and mice already updated) into a new arena, installs `s` there,
+// and frees the old arena.  On failure the previous layout is restored.
+b3g_status relayout(b3g_cloth* c, const ParticleState& s, uint32_t old_extra, std::vector<MouseForceDesc> old_mice,
+                    std::vector<uint32_t> old_ids)
+{
+    char* old_base = c->arena.base;
+    const size_t old_size = c->arena.size;
+    const ClothDev old_dev = c->dev;
+    ClothTopology old_topo = c->topo;
+    auto restore = [&]() {
+        c->n_extra = old_extra;
+        c->mice = std::move(old_mice);
+        c->mouse_ids = std::move(old_ids);
+        c->topo = std::move(old_topo);
+        c->dev = old_dev;
+        c->arena.base = old_base;
+        c->arena.size = old_size;
+        c->images.reset();
+    };
+    b3g_status st = layout_cloth(c);
+    if (st != B3G_OK) {
+        restore();
+        return st;
+    }
+    c->dev.nsph = old_dev.nsph;
+    std::memcpy(c->dev.sph, old_dev.sph, sizeof(old_dev.sph));
+    char* base = nullptr;
+    if (cudaMalloc(&base, c->arena.size) != cudaSuccess) {
+        cudaGetLastError();
+        restore();
+        return B3G_ERR_OUT_OF_MEMORY;
+    }
+    const bool owns_stream = c->owns_stream;
+    st = realize_cloth(c, c->device, base, true, c->stream, false);
+    c->owns_stream = owns_stream;
+    if (st == B3G_OK) st = upload_state(c, s);
+    if (st == B3G_OK && cudaStreamSynchronize(c->stream) != cudaSuccess) st = B3G_ERR_CUDA;
+    if (st != B3G_OK) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(base);
+        cudaGetLastError();
+        restore();
+        return st;
+    }
+    finish_upload(c);
+    destroy_graph(c);
+    cudaFree(old_base);
+    c->layout_version += 1;
+    return B3G_OK;
+}
+
+bool editable(const b3g_cloth* c) { return valid(c) && c->owns_arena && c->owns_stream; }
+
+}  // namespace
+
+extern "C" {
+
+b3g_status b3g_cloth_create_particle(b3g_cloth* c, const b3g_particle_def* def, uint32_t* index)
+{
+    if (!editable(c) || !def || !index) return B3G_ERR_INVALID_ARGUMENT;
+    for (int q = 0; q < 3; ++q)
+        if (!std::isfinite(def->position[q]) || !std::isfinite(def->velocity[q]) || !std::isfinite(def->force[q]))
+            return B3G_ERR_INVALID_ARGUMENT;
+    if (!(def->mass >= 0.0f) || !std::isfinite(def->mass) || !(def->radius >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    const bool dynamic = def->mass != 0.0f;
+    // a created dynamic particle meets colliders with the cloth's thickness and friction
+    if (dynamic && (def->radius != c->in_def.thickness || def->friction != c->in_def.friction))
+        return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status st = flush_ops(c);
+    if (st != B3G_OK) return st;
+    ParticleState s;
+    if ((st = download_state(c, s)) != B3G_OK) return st;
+    std::vector<uint32_t> keep(s.n + 1);
+    for (uint32_t k = 0; k < s.n; ++k) keep[k] = k;
+    keep[s.n] = kNone;
+    ParticleState r = remap(s, keep);
+    // b3Particle::b3Particle (particle.cpp:24-51); proxy: its AABB fattened
+    // by B3_AABB_EXTENSION (cloth.cpp:311-317)
+    const uint32_t i = s.n, n1 = r.n;
+    for (int q = 0; q < 3; ++q) {
+        const float p = def->position[q];
+        r.x[q * (size_t)n1 + i] = p;
+        r.v[q * (size_t)n1 + i] = def->velocity[q];
+        r.fext[q * (size_t)n1 + i] = def->force[q];
+        r.lo[q * (size_t)n1 + i] = (p - def->radius) - 0.2f;
+        r.hi[q * (size_t)n1 + i] = (p + def->radius) + 0.2f;
+    }
+    r.mass[i] = dynamic ? def->mass : 1.0f;
+    r.type[i] = (uint8_t)(dynamic ? B3G_DYNAMIC : B3G_STATIC);
+    const uint32_t old_extra = c->n_extra;
+    c->n_extra += 1;
+    if ((st = relayout(c, r, old_extra, c->mice, c->mouse_ids)) != B3G_OK) return st;
+    *index = i;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_destroy_particle(b3g_cloth* c, uint32_t index)
+{
+    if (!editable(c)) return B3G_ERR_INVALID_ARGUMENT;
+    const uint32_t n_mesh = c->topo.n_mesh;
+    if (index < n_mesh || index >= c->dev.n) return B3G_ERR_INVALID_ARGUMENT;  // only created particles
+    cudaSetDevice(c->device);
+    b3g_status st = flush_ops(c);
+    if (st != B3G_OK) return st;
+    ParticleState s;
+    if ((st = download_state(c, s)) != B3G_OK) return st;
+    std::vector<uint32_t> keep;
+    for (uint32_t k = 0; k < s.n; ++k)
+        if (k != index) keep.push_back(k);
+    ParticleState r = remap(s, keep);
+    const uint32_t old_extra = c->n_extra;
+    std::vector<MouseForceDesc> old_mice = c->mice;
+    std::vector<uint32_t> old_ids = c->mouse_ids;
+    // its forces go with it (cloth.cpp:329-340); later particles move down one
+    std::vector<MouseForceDesc> mice;
+    std::vector<uint32_t> ids;
+    for (size_t m = 0; m < c->mice.size(); ++m) {
+        MouseForceDesc f = c->mice[m];
+        if (f.particle == index) continue;
+        if (f.particle > index) f.particle -= 1;
+        mice.push_back(f);
+        ids.push_back(c->mouse_ids[m]);
+    }
+    c->mice = mice;
+    c->mouse_ids = ids;
+    c->n_extra -= 1;
+    return relayout(c, r, old_extra, old_mice, old_ids);
+}
+
+b3g_status b3g_cloth_create_mouse_force(b3g_cloth* c, const b3g_mouse_force_def* def, uint32_t* force_id)
+{
+    if (!editable(c) || !def || !force_id) return B3G_ERR_INVALID_ARGUMENT;
+    if (def->particle >= c->dev.n || def->triangle >= c->dev.t) return B3G_ERR_INVALID_ARGUMENT;
+    if (!std::isfinite(def->w2) || !std::isfinite(def->w3) || !std::isfinite(def->w4) ||
+        !std::isfinite(def->mouse) || !std::isfinite(def->damping))
+        return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status st = flush_ops(c);
+    if (st != B3G_OK) return st;
+    ParticleState s;
+    if ((st = download_state(c, s)) != B3G_OK) return st;
+    std::vector<MouseForceDesc> old_mice = c->mice;
+    std::vector<uint32_t> old_ids = c->mouse_ids;
+    c->mice.push_back(MouseForceDesc{def->particle, def->triangle, def->w2, def->w3, def->w4, def->mouse,
+                                     def->damping});
+    const uint32_t id = ++c->next_force_id;
+    c->mouse_ids.push_back(id);
+    if ((st = relayout(c, s, c->n_extra, old_mice, old_ids)) != B3G_OK) return st;
+    *force_id = id;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_destroy_force(b3g_cloth* c, uint32_t force_id)
+{
+    if (!editable(c)) return B3G_ERR_INVALID_ARGUMENT;
+    size_t m = 0;
+    while (m < c->mouse_ids.size() && c->mouse_ids[m] != force_id) ++m;
+    if (m == c->mouse_ids.size()) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status st = flush_ops(c);
+    if (st != B3G_OK) return st;
+    ParticleState s;
+    if ((st = download_state(c, s)) != B3G_OK) return st;
+    std::vector<MouseForceDesc> old_mice = c->mice;
+    std::vector<uint32_t> old_ids = c->mouse_ids;
+    c->mice.erase(c->mice.begin() + m);
+    c->mouse_ids.erase(c->mouse_ids.begin() + m);
+    return relayout(c, s, c->n_extra, old_mice, old_ids);
+}
+
+}  // extern "C"
 
 static b3g_status push_op(b3g_cloth* c, uint32_t vertex, uint32_t kind, const float* a)
 {

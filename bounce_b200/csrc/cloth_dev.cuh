@@ -74,7 +74,7 @@ struct ClothDev {
     float* vals;                // 9 E
 
     const uint32_t* inc_ptr;    // n + 1
-    const uint32_t* inc_elem;   // bit 31 set: spring id, else triangle id
+    const uint32_t* inc_elem;   // triangle id; bit 31: spring id; bits 31 and 30: mouse force id
     const uint32_t* inc_meta;   // corner/end (bits 0-1), slots of element vertices (8 bits each from bit 8)
 
     const uint4* tri;           // v1, v2, v3, 0
@@ -82,6 +82,9 @@ struct ClothDev {
     const float2* tri_rest2;    // inv_det, alpha
     const uint2* spr;           // p1, p2 (vertex ids)
     const float4* spr_par;      // L0, ks, kd, 0
+    const uint4* mouse_v;       // mouse forces: particle, triangle's v1, v2, v3
+    const float4* mouse_par;    // 2 per mouse force: (w2, w3, w4, mouse), (damping, 0, 0, 0)
+    uint32_t nmouse;
 
     float k_stretch, k_shear, k_damp;
     float thickness, friction;  // particle radius and friction (b3ClothDef)

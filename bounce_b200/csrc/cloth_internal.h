@@ -33,6 +33,8 @@ struct HostImages {
     std::vector<float4> sp;
     std::vector<float> x, lo, hi;
     std::vector<uint8_t> types;
+    std::vector<uint4> mouse_v;
+    std::vector<float4> mouse_par;
 };
 
 }  // namespace b3g
@@ -73,6 +75,17 @@ struct b3g_cloth {
     bool owns_arena = true;
     bool owns_stream = true;
     std::unique_ptr<b3g::HostImages> images;
+
+    // creation inputs, kept to lay the cloth out again when particles or
+    // forces are created or destroyed (cloth.cpp:307-364)
+    std::vector<float> in_vertices;
+    std::vector<uint32_t> in_tris, in_sewing;
+    b3g_cloth_def in_def{};
+    uint32_t n_extra = 0;                     // created particles, after the mesh vertices
+    std::vector<b3g::MouseForceDesc> mice;    // mouse forces in creation order
+    std::vector<uint32_t> mouse_ids;          // the id of each
+    uint32_t next_force_id = 0;
+    uint32_t layout_version = 0;              // bumped on every new layout (batches rebuild their graphs)
 };
 
 
@@ -80,6 +93,7 @@ b3g_status flush_ops_on(b3g_cloth* c, cudaStream_t st);
 void fill_step_scalars(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, b3g::StepScalars* h);
 void record_stats(b3g_cloth* c, const b3g::StepScalars& h, float ms, bool solved);
 b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3g_cloth** out);
+b3g_status layout_cloth(b3g_cloth* c);
 b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, cudaStream_t st, bool own_stream);
 void finish_upload(b3g_cloth* c);
 b3g_status destroy_cloth(b3g_cloth* c);

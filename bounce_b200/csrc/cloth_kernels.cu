@@ -249,6 +249,45 @@ __device__ void spring_row(const ClothDev& c, RowAcc& acc, uint32_t sid, int end
     f_row = end == 0 ? f_row + mf : f_row - mf;
 }
 
+// b3MouseForce::Apply (mouse_force.cpp:63-227) restricted to the row of the
+// force's vertex `role` (0: the particle, 1-3: the triangle's vertices):
+// C = |x1 - (w2 x2 + w3 x3 + w4 x4)|, dC/dx = (n, -w2 n, -w3 n, -w4 n), and
+// no second-derivative term.  The row's blocks are added for the force's
+// vertices in order.
+__device__ void mouse_row(const ClothDev& c, RowAcc& acc, uint32_t m, int role, const int slot[4], f3& f_row)
+{
+    const uint4 mv = c.mouse_v[m];
+    const float4 pa = c.mouse_par[2 * m], pb = c.mouse_par[2 * m + 1];
+    const float w2 = pa.x, w3 = pa.y, w4 = pa.z, km = pa.w, kd = pb.x;
+    const uint32_t n = c.n;
+    const f3 x1 = ld3(c.x, n, mv.x), x2 = ld3(c.x, n, mv.y), x3 = ld3(c.x, n, mv.z), x4 = ld3(c.x, n, mv.w);
+    const f3 c2 = (w2 * x2 + w3 * x3) + w4 * x4;
+    const f3 d = x1 - c2;
+    const float len = length(d);
+    f3 mf = zero3();
+    if (len > 0.0f) {
+        const f3 nrm = d / len;
+        const f3 dC[4] = {nrm, (-w2) * nrm, (-w3) * nrm, (-w4) * nrm};
+        const f3 dCr = role == 0 ? dC[0] : role == 1 ? dC[1] : role == 2 ? dC[2] : dC[3];
+        if (km > 0.0f) {
+            const float C = len;
+            mf = mf + (-km * C) * dCr;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc.addK(slot[j], -km * outer(dCr, dC[j]));
+        }
+        if (kd > 0.0f) {
+            const f3 vs[4] = {ld3(c.v, n, mv.x), ld3(c.v, n, mv.y), ld3(c.v, n, mv.z), ld3(c.v, n, mv.w)};
+            float dCdt = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) dCdt += dot(dC[i], vs[i]);
+            mf = mf + (-kd * dCdt) * dCr;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc.addD(slot[j], -kd * outer(dCr, dC[j]));
+        }
+    }
+    f_row = f_row + mf;
+}
+
 // Element `cn` of a 3-array held in registers (a select, not local memory).
 template <typename T>
 __device__ __forceinline__ T corner(int cn, const T& a0, const T& a1, const T& a2)
@@ -409,7 +448,12 @@ __global__ void __launch_bounds__(256) k_assemble(const __grid_constant__ ClothD
         }
         const int cn = meta & 3u;
         const int s0 = (meta >> 8) & 0xffu, s1 = (meta >> 16) & 0xffu, s2 = (meta >> 24) & 0xffu;
-        if (el & 0x80000000u) {
+        if ((el & 0xc0000000u) == 0xc0000000u) {
+            // mouse force: role in bits 0-1, the four slots 7 bits each from bit 4
+            const int ms[4] = {(int)((meta >> 4) & 0x7fu), (int)((meta >> 11) & 0x7fu), (int)((meta >> 18) & 0x7fu),
+                               (int)((meta >> 25) & 0x7fu)};
+            mouse_row(c, acc, el & 0x3fffffffu, cn, ms, f);
+        } else if (el & 0x80000000u) {
             // springs: slot of p1 in s0, of p2 in s1; cn = end
             spring_row(c, acc, el & 0x7fffffffu, cn, cn == 0 ? s0 : s1, cn == 0 ? s1 : s0, f);
         } else {

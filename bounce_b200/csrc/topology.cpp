@@ -57,10 +57,11 @@ void bending_pairs(uint32_t t, const uint32_t* tris, std::vector<uint32_t>* pair
 }
 
 int build_topology(uint32_t n, const float* X, uint32_t t, const uint32_t* tris, uint32_t nsew,
-                   const uint32_t* sewing, const float* def, ClothTopology* out)
+                   const uint32_t* sewing, const float* def, ClothTopology* out, uint32_t n_extra,
+                   const MouseForceDesc* mice, uint32_t nmice)
 {
     ClothTopology& c = *out;
-    c.n = n;
+    c.n_mesh = n;
     c.t = t;
     for (uint64_t k = 0; k < 3ull * t; ++k)
         if (tris[k] >= n) return kDegenerate;
@@ -79,6 +80,14 @@ int build_topology(uint32_t n, const float* X, uint32_t t, const uint32_t* tris,
     }
     for (uint32_t i = 0; i < n; ++i)
         if (!(c.mass[i] > 0.0f)) return kDegenerate;  // a vertex outside every triangle
+    const uint32_t n_mesh = n;
+    n += n_extra;
+    c.n = n;
+    c.mass.resize(n, 1.0f);
+    for (uint32_t m = 0; m < nmice; ++m) {
+        const MouseForceDesc& f = mice[m];
+        if (f.particle >= n || f.triangle >= t) return kDegenerate;
+    }
 
     // rest-state frames (cloth.cpp:152-191)
     c.rest.resize(6 * (size_t)t);
@@ -123,6 +132,7 @@ int build_topology(uint32_t n, const float* X, uint32_t t, const uint32_t* tris,
     }
     c.ns = (uint32_t)(c.spring_pairs.size() / 2);
 
+    (void)n_mesh;
     // row pattern
     std::vector<std::vector<uint32_t>> nb(n);
     for (uint32_t i = 0; i < n; ++i) nb[i].push_back(i);
@@ -136,6 +146,17 @@ int build_topology(uint32_t n, const float* X, uint32_t t, const uint32_t* tris,
             nb[p].push_back(q);
             nb[q].push_back(p);
         }
+    }
+    auto mouse_vertices = [&](uint32_t m, uint32_t (&ids)[4]) {
+        ids[0] = mice[m].particle;
+        for (int q = 0; q < 3; ++q) ids[q + 1] = tris[3 * (size_t)mice[m].triangle + q];
+    };
+    for (uint32_t m = 0; m < nmice; ++m) {
+        uint32_t ids[4];
+        mouse_vertices(m, ids);
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b)
+                if (ids[a] != ids[b]) nb[ids[a]].push_back(ids[b]);
     }
     c.row_ptr.assign(n + 1, 0);
     c.row_cols.clear();
@@ -181,15 +202,27 @@ int build_topology(uint32_t n, const float* X, uint32_t t, const uint32_t* tris,
         }
     }
 
-    // incidence in force-list order: springs newest first, then triangles
-    // newest first (each triangle's shear element precedes its stretch element)
+    // incidence in force-list order: mouse forces newest first (created after
+    // the constructor's forces, cloth.cpp:353-358), springs newest first, then
+    // triangles newest first (each triangle's shear element precedes its
+    // stretch element)
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> inc(n);
+    for (uint32_t m = nmice; m-- > 0;) {
+        uint32_t ids[4];
+        mouse_vertices(m, ids);
+        for (uint32_t role = 0; role < 4; ++role) {
+            const uint32_t i = ids[role];
+            uint32_t meta = role;
+            for (int q = 0; q < 4; ++q) meta |= slot_of(i, ids[q]) << (4 + 7 * q);
+            inc[i].push_back({kIncSpring | kIncMouse | m, meta});
+        }
+    }
     for (uint32_t s = c.ns; s-- > 0;) {
         uint32_t p = c.spring_pairs[2 * s], q = c.spring_pairs[2 * s + 1];
         for (uint32_t end = 0; end < 2; ++end) {
             uint32_t i = end == 0 ? p : q;
             uint32_t meta = end | (slot_of(i, p) << 8) | (slot_of(i, q) << 16);
-            inc[i].push_back({0x80000000u | s, meta});
+            inc[i].push_back({kIncSpring | s, meta});
         }
     }
     const bool tri_forces = def[1] > 0.0f || def[2] > 0.0f;

@@ -9,8 +9,24 @@
 
 namespace b3g {
 
+// A mouse force (include/bounce/cloth/forces/mouse_force.h:26-40): particle
+// `particle` tied to the point w2 x(v1) + w3 x(v2) + w4 x(v3) of `triangle`.
+struct MouseForceDesc {
+    uint32_t particle, triangle;
+    float w2, w3, w4, mouse, damping;
+};
+
+// Incidence element codes: a triangle id, or a spring id with kIncSpring set,
+// or a mouse force id with kIncSpring | kIncMouse set.  A mouse entry's meta
+// holds the row's role (0: the particle, 1-3: the triangle's vertices) in
+// bits 0-1 and the slots of the force's four vertices, 7 bits each, from
+// bit 4.
+constexpr uint32_t kIncSpring = 0x80000000u;
+constexpr uint32_t kIncMouse = 0x40000000u;
+
 struct ClothTopology {
     uint32_t n = 0, t = 0, ns = 0;
+    uint32_t n_mesh = 0;                     // particles of mesh vertices; created ones follow
     // reference constructor data
     std::vector<float> mass;                 // n
     std::vector<float> rest;                 // 6 per triangle: du1, dv1, du2, dv2, inv_det, alpha
@@ -30,8 +46,11 @@ struct ClothTopology {
 };
 
 // Returns 0 on success, else a b3g_status (degenerate mesh, unsupported degree).
+// n_extra created particles follow the n mesh vertices (masses left to the
+// caller, 1 each here); `mice` holds the mouse forces in creation order.
 int build_topology(uint32_t n, const float* vertices, uint32_t t, const uint32_t* tris, uint32_t nsew,
-                   const uint32_t* sewing, const float* def8, ClothTopology* out);
+                   const uint32_t* sewing, const float* def8, ClothTopology* out, uint32_t n_extra = 0,
+                   const MouseForceDesc* mice = nullptr, uint32_t nmice = 0);
 
 // Bending pairs of b3FindSharedEdges (cloth.cpp:40-94): for every triangle i,
 // each edge (a -> b), every later triangle holding (b -> a); the pair is the

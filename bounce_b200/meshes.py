@@ -123,6 +123,27 @@ def stiff_scene(side: int = 1024, steps: int = 50) -> Scene:
     return Scene(f"grid{side}_stiff", mesh, cdef, pins, steps=steps)
 
 
+def sewn_scene(side: int = 16, seed: int = 4, gap: float = 0.05, sewing: float = 1e3, steps: int = 60) -> Scene:
+    """Two grid panels, one `gap` below the other, sewn along both side edges
+    (column 0 and column side-1 of every row) like a sleeve: sewing springs
+    of rest length 0 (b3ClothDef::sewing, cloth.cpp:248-262).  Stretch 1e4,
+    shear 1e3, damping 0.05, jitter N(0, 1e-3 m), the two top corners of
+    both panels pinned."""
+    a = grid_mesh(side, 1.0, 1e-3, seed)
+    b = grid_mesh(side, 1.0, 1e-3, seed + 1)
+    nb = a.vertex_count
+    verts = np.concatenate([a.vertices, b.vertices + np.array([0.0, -gap, 0.0], np.float32)]).astype(np.float32)
+    tris = np.concatenate([a.triangles, b.triangles + np.uint32(nb)]).astype(np.uint32)
+    rows = np.arange(side, dtype=np.uint32)
+    left, right = rows * side, rows * side + (side - 1)
+    edge = np.concatenate([left, right])
+    sew = np.stack([np.zeros_like(edge), np.ones_like(edge), edge, edge + np.uint32(nb)], axis=1).astype(np.uint32)
+    mesh = Mesh(verts, tris, sew)
+    cdef = ClothDef(density=1.0, streching=1e4, shearing=1e3, sewing=sewing, damping=0.05, friction=0.3)
+    pins = np.array([0, side - 1, nb, nb + side - 1], dtype=np.uint32)
+    return Scene(f"sewn{side}", mesh, cdef, pins, steps=steps)
+
+
 def batch_scenes(count: int = 512, seed: int = 3, side_lo: int = 16, side_hi: int = 128,
                  steps: int = 100) -> list:
     """Many independent cloths: side ~ U{side_lo..side_hi}, stretch log-U[1e3, 1e5],

@@ -114,6 +114,46 @@ b3g_status b3g_cloth_add_static_sphere(b3g_cloth* cloth, const float center[3], 
 /* b3Cloth::SetWorld(nullptr): drop every collider and its contacts. */
 b3g_status b3g_cloth_clear_colliders(b3g_cloth* cloth);
 
+/* ---- created particles and mouse forces ------------------------------------ */
+
+/* b3ParticleDef (include/bounce/cloth/particle.h:38-60).  mass 0 makes a
+ * static particle (of mass 1, particle.cpp:34-39).  A created dynamic
+ * particle must use the cloth's thickness and friction as its radius and
+ * friction (colliders see every particle with those). */
+typedef struct {
+    float position[3];
+    float velocity[3];
+    float force[3];
+    float mass;
+    float radius;
+    float friction;
+} b3g_particle_def;
+
+/* b3Cloth::CreateParticle (src/bounce/cloth/cloth.cpp:307-322): the new
+ * particle's index follows every existing particle; use it with the
+ * b3g_particle_* calls.  The cloth's layout is rebuilt around its state. */
+b3g_status b3g_cloth_create_particle(b3g_cloth* cloth, const b3g_particle_def* def, uint32_t* index);
+/* b3Cloth::DestroyParticle (cloth.cpp:324-351), created particles only: its
+ * mouse forces and contacts go with it; particles created after it move
+ * down one index. */
+b3g_status b3g_cloth_destroy_particle(b3g_cloth* cloth, uint32_t index);
+
+/* b3MouseForceDef (include/bounce/cloth/forces/mouse_force.h:26-40): particle
+ * `particle` tied by a spring of stiffness `mouse` and damping `damping` to
+ * the point w2 x(v1) + w3 x(v2) + w4 x(v3) of `triangle`. */
+typedef struct {
+    uint32_t particle, triangle;
+    float w2, w3, w4;
+    float mouse, damping;
+} b3g_mouse_force_def;
+
+/* b3Cloth::CreateForce (cloth.cpp:353-358) of a mouse force, applied before
+ * every earlier force (mouse_force.cpp:63-227); returns an id for
+ * b3g_cloth_destroy_force.  b3Cloth::DestroyForce (cloth.cpp:360-364).
+ * Cloths that a server owns cannot take created particles or forces. */
+b3g_status b3g_cloth_create_mouse_force(b3g_cloth* cloth, const b3g_mouse_force_def* def, uint32_t* force_id);
+b3g_status b3g_cloth_destroy_force(b3g_cloth* cloth, uint32_t force_id);
+
 /* ---- particles (include/bounce/cloth/particle.h:63-111) ------------------ */
 
 b3g_status b3g_particle_set_type(b3g_cloth* cloth, uint32_t vertex, b3g_particle_type type);

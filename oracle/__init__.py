@@ -85,6 +85,16 @@ def port_lib():
         L.oc_mpcg.restype = C.c_uint32
         L.oc_mpcg.argtypes = [C.c_uint32, _u32p, _u32p, _f32p, _f32p, _f32p, _f32p, C.c_int, C.c_float,
                               C.c_uint32, C.c_int, _f32p, _f64p]
+        L.oc_create_particle.restype = C.c_uint32
+        L.oc_create_particle.argtypes = [C.c_void_p, _f32p, C.c_void_p, C.c_float, C.c_float, C.c_float]
+        L.oc_destroy_particle.restype = C.c_int
+        L.oc_destroy_particle.argtypes = [C.c_void_p, C.c_uint32]
+        L.oc_create_mouse_force.restype = C.c_uint32
+        L.oc_create_mouse_force.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32] + [C.c_float] * 5
+        L.oc_destroy_force.restype = C.c_int
+        L.oc_destroy_force.argtypes = [C.c_void_p, C.c_uint32]
+        L.oc_particle_count.restype = C.c_uint32
+        L.oc_particle_count.argtypes = [C.c_void_p]
         L.oc_solve_f64.restype = C.c_uint32
         L.oc_solve_f64.argtypes = [C.c_uint32, _u32p, _u32p, _f32p, _f32p, _f32p, _f32p, C.c_double,
                                    C.c_uint32, _f64p]
@@ -123,6 +133,16 @@ def ref_lib():
         L.ref_cloth_build_system.restype = C.c_uint32
         L.ref_cloth_build_system.argtypes = [C.c_void_p, C.c_float]
         L.ref_cloth_get_system.argtypes = [C.c_void_p, _u32p, _u32p, _f32p, _f32p, _f32p, _f32p, _u32p]
+        L.ref_cloth_create_particle.restype = C.c_uint32
+        L.ref_cloth_create_particle.argtypes = [C.c_void_p, _f32p, C.c_void_p, C.c_float, C.c_float, C.c_float]
+        L.ref_cloth_destroy_particle.restype = C.c_int
+        L.ref_cloth_destroy_particle.argtypes = [C.c_void_p, C.c_uint32]
+        L.ref_cloth_create_mouse_force.restype = C.c_uint32
+        L.ref_cloth_create_mouse_force.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32] + [C.c_float] * 5
+        L.ref_cloth_destroy_force.restype = C.c_int
+        L.ref_cloth_destroy_force.argtypes = [C.c_void_p, C.c_uint32]
+        L.ref_cloth_particle_count.restype = C.c_uint32
+        L.ref_cloth_particle_count.argtypes = [C.c_void_p]
         L.ref_profile_read.restype = C.c_uint32
         L.ref_profile_read.argtypes = [C.c_char_p, C.c_uint32, _f64p, np.ctypeslib.ndpointer(np.uint64)]
         L.ref_profile_reset.argtypes = []
@@ -134,7 +154,7 @@ class _Base:
     """Shared state accessors; subclasses bind the library calls."""
 
     def __init__(self, mesh, cdef):
-        self.n = mesh.vertex_count
+        self.n_mesh = mesh.vertex_count
         self.t = mesh.triangle_count
         self._verts = np.ascontiguousarray(mesh.vertices, np.float32).reshape(-1)
         self._tris = np.ascontiguousarray(mesh.triangles, np.uint32).reshape(-1)
@@ -142,6 +162,30 @@ class _Base:
         self._sew = sew if sew.size else np.zeros(4, np.uint32)
         self._nsew = int(mesh.sewing.shape[0])
         self._def = cdef.as_array()
+
+    @property
+    def n(self) -> int:
+        """Particles: the mesh's, then created ones."""
+        return int(self._particle_count()) if getattr(self, "h", None) else self.n_mesh
+
+    def create_particle(self, position, velocity=None, mass=0.0, radius=0.0, friction=0.0) -> int:
+        """b3Cloth::CreateParticle: returns the particle's index (after every existing one)."""
+        vel = None if velocity is None else np.asarray(velocity, np.float32)
+        return int(self._create_particle(np.asarray(position, np.float32), None if vel is None else vel.ctypes.data,
+                                         mass, radius, friction))
+
+    def destroy_particle(self, index: int) -> None:
+        if self._destroy_particle(index) != 0:
+            raise ValueError(f"particle {index} is not a created particle")
+
+    def create_mouse_force(self, particle: int, triangle: int, w2: float, w3: float, w4: float, mouse: float,
+                           damping: float) -> int:
+        """b3Cloth::CreateForce of a b3MouseForceDef: returns its id."""
+        return int(self._create_mouse_force(particle, triangle, w2, w3, w4, mouse, damping))
+
+    def destroy_force(self, force_id: int) -> None:
+        if self._destroy_force(force_id) != 0:
+            raise ValueError(f"no force {force_id}")
 
     def state(self):
         x = np.zeros(3 * self.n, np.float32)
@@ -197,7 +241,7 @@ class PortCloth(_Base):
     def __init__(self, mesh, cdef):
         super().__init__(mesh, cdef)
         self.L = port_lib()
-        self.h = self.L.oc_create(self._verts, self.n, self._tris, self.t, self._sew, self._nsew, self._def)
+        self.h = self.L.oc_create(self._verts, self.n_mesh, self._tris, self.t, self._sew, self._nsew, self._def)
         self.last = _OcStepInfo()
 
     def __del__(self):
@@ -253,6 +297,21 @@ class PortCloth(_Base):
     def _get_state(self, *a):
         self.L.oc_get_state(self.h, *a)
 
+    def _particle_count(self):
+        return self.L.oc_particle_count(self.h)
+
+    def _create_particle(self, *a):
+        return self.L.oc_create_particle(self.h, *a)
+
+    def _destroy_particle(self, i):
+        return self.L.oc_destroy_particle(self.h, i)
+
+    def _create_mouse_force(self, *a):
+        return self.L.oc_create_mouse_force(self.h, *a)
+
+    def _destroy_force(self, i):
+        return self.L.oc_destroy_force(self.h, i)
+
     def _describe(self, a, b, c):
         return self.L.oc_describe(self.h, a, b, c)
 
@@ -272,7 +331,7 @@ class RefCloth(_Base):
     def __init__(self, mesh, cdef, restated: bool = True):
         super().__init__(mesh, cdef)
         self.L = ref_lib()
-        self.h = self.L.ref_cloth_create(self._verts, self.n, self._tris, self.t, self._sew, self._nsew,
+        self.h = self.L.ref_cloth_create(self._verts, self.n_mesh, self._tris, self.t, self._sew, self._nsew,
                                          self._def, 1 if restated else 0)
 
     def __del__(self):
@@ -310,6 +369,21 @@ class RefCloth(_Base):
 
     def _get_state(self, *a):
         self.L.ref_cloth_get_state(self.h, *a)
+
+    def _particle_count(self):
+        return self.L.ref_cloth_particle_count(self.h)
+
+    def _create_particle(self, *a):
+        return self.L.ref_cloth_create_particle(self.h, *a)
+
+    def _destroy_particle(self, i):
+        return self.L.ref_cloth_destroy_particle(self.h, i)
+
+    def _create_mouse_force(self, *a):
+        return self.L.ref_cloth_create_mouse_force(self.h, *a)
+
+    def _destroy_force(self, i):
+        return self.L.ref_cloth_destroy_force(self.h, i)
 
     def _describe(self, a, b, c):
         return self.L.ref_cloth_describe(self.h, a, b, c)

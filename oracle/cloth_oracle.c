@@ -144,12 +144,15 @@ static void lrows_free(lrow* rows, uint32_t n)
 /* cloth state                                                               */
 /* ------------------------------------------------------------------------ */
 
-enum { F_STRETCH = 0, F_SHEAR = 1, F_SPRING = 2 };
+enum { F_STRETCH = 0, F_SHEAR = 1, F_SPRING = 2, F_MOUSE = 3 };
 
 typedef struct {
     int type;
-    uint32_t a, b, c;    /* triangle index (a) for stretch/shear; vertices (a, b) for springs */
-    float ks, kd, p0, p1; /* stretch: bu, bv; spring: L0 */
+    uint32_t a, b, c;    /* triangle index (a) for stretch/shear; vertices (a, b) for springs;
+                            mouse: particle (a), triangle (b) */
+    float ks, kd, p0, p1; /* stretch: bu, bv; spring: L0; mouse: km, kd, w2, w3 */
+    float p2;             /* mouse: w4 */
+    uint32_t id;          /* mouse: the handle oc_create_mouse_force returned */
 } force_t;
 
 typedef struct {
@@ -168,6 +171,8 @@ typedef struct {
 
 struct oc_cloth {
     uint32_t n, t;
+    uint32_t n_mesh;      /* particles made from mesh vertices; created particles follow */
+    uint32_t next_force_id;
     float def[8];
     uint32_t* tris;
 
@@ -239,6 +244,7 @@ oc_cloth* oc_create(const float* vertices, uint32_t n, const uint32_t* triangles
 {
     oc_cloth* c = (oc_cloth*)calloc(1, sizeof(oc_cloth));
     c->n = n;
+    c->n_mesh = n;
     c->t = t;
     memcpy(c->def, def, sizeof(c->def));
     c->tris = (uint32_t*)malloc(3 * (size_t)t * sizeof(uint32_t));
@@ -320,11 +326,11 @@ oc_cloth* oc_create(const float* vertices, uint32_t n, const uint32_t* triangles
         c->inv_det[k] = 1.0f / det;
         c->alpha[k] = 0.5f * A2;
         if (def[1] > 0.0f) {
-            force_t f = {F_STRETCH, k, 0, 0, def[1], def[5], 1.0f, 1.0f};
+            force_t f = {F_STRETCH, k, 0, 0, def[1], def[5], 1.0f, 1.0f, 0.0f, 0u};
             created[ncreated++] = f;
         }
         if (def[2] > 0.0f) {
-            force_t f = {F_SHEAR, k, 0, 0, def[2], def[5], 0.0f, 0.0f};
+            force_t f = {F_SHEAR, k, 0, 0, def[2], def[5], 0.0f, 0.0f, 0.0f, 0u};
             created[ncreated++] = f;
         }
     }
@@ -364,7 +370,7 @@ oc_cloth* oc_create(const float* vertices, uint32_t n, const uint32_t* triangles
                 /* b3SpringForceDef::Initialize (spring_force.cpp:25-35) */
                 float L0 = vlength(vsub(c->x[p3], c->x[p4]));
                 if (def[3] > 0.0f) {
-                    force_t f = {F_SPRING, p3, p4, 0, def[3], def[5], L0, 0.0f};
+                    force_t f = {F_SPRING, p3, p4, 0, def[3], def[5], L0, 0.0f, 0.0f, 0u};
                     if (ncreated == fcap) {
                         fcap *= 2;
                         created = (force_t*)realloc(created, fcap * sizeof(force_t));
@@ -382,7 +388,7 @@ oc_cloth* oc_create(const float* vertices, uint32_t n, const uint32_t* triangles
         uint32_t p1 = sewing[4 * s + 2], p2 = sewing[4 * s + 3];
         float L0 = vlength(vsub(c->x[p1], c->x[p2]));
         if (def[4] > 0.0f) {
-            force_t f = {F_SPRING, p1, p2, 0, def[4], def[5], L0, 0.0f};
+            force_t f = {F_SPRING, p1, p2, 0, def[4], def[5], L0, 0.0f, 0.0f, 0u};
             if (ncreated == fcap) {
                 fcap *= 2;
                 created = (force_t*)realloc(created, fcap * sizeof(force_t));
@@ -686,6 +692,188 @@ static void apply_spring(oc_cloth* c, const force_t* fo)
     c->sf[i2] = vsub(c->sf[i2], f);
 }
 
+/* b3MouseForce::Apply (mouse_force.cpp:63-227): particle 1 tied to the point
+ * w2 x2 + w3 x3 + w4 x4 of a triangle, C = |x1 - c2|, no second-derivative
+ * term; rows receive their blocks in the reference's (i, j) order. */
+static void apply_mouse(oc_cloth* c, const force_t* fo)
+{
+    const uint32_t* tv = c->tris + 3 * (size_t)fo->b;
+    const uint32_t ids[4] = {c->solver_of_vertex[fo->a], c->solver_of_vertex[tv[0]], c->solver_of_vertex[tv[1]],
+                             c->solver_of_vertex[tv[2]]};
+    const float km = fo->ks, kd = fo->kd, w2 = fo->p0, w3 = fo->p1, w4 = fo->p2;
+    v3 xs[4], vs[4], mf[4];
+    for (int i = 0; i < 4; ++i) {
+        xs[i] = c->sx[ids[i]];
+        vs[i] = c->sv[ids[i]];
+        mf[i] = vzero();
+    }
+    v3 c2 = vadd(vadd(vscale(w2, xs[1]), vscale(w3, xs[2])), vscale(w4, xs[3]));
+    v3 d = vsub(xs[0], c2);
+    float len = vlength(d);
+    if (len > 0.0f) {
+        v3 nrm = vdiv(d, len);
+        v3 dCdx[4] = {nrm, vscale(-w2, nrm), vscale(-w3, nrm), vscale(-w4, nrm)};
+        if (km > 0.0f) {
+            float C = len;
+            for (int i = 0; i < 4; ++i) mf[i] = vadd(mf[i], vscale(-km * C, dCdx[i]));
+            for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 4; ++j)
+                    madd_to(lrow_at(c->dfdx + ids[i], ids[j]), mscale(-km, mouter(dCdx[i], dCdx[j])));
+        }
+        if (kd > 0.0f) {
+            float dCdt = 0.0f;
+            for (int i = 0; i < 4; ++i) dCdt += vdot(dCdx[i], vs[i]);
+            for (int i = 0; i < 4; ++i) mf[i] = vadd(mf[i], vscale(-kd * dCdt, dCdx[i]));
+            for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 4; ++j)
+                    madd_to(lrow_at(c->dfdv + ids[i], ids[j]), mscale(-kd, mouter(dCdx[i], dCdx[j])));
+        }
+    }
+    for (int i = 0; i < 4; ++i) c->sf[ids[i]] = vadd(c->sf[ids[i]], mf[i]);
+}
+
+/* ------------------------------------------------------------------------ */
+/* created particles and forces (cloth.cpp:307-364)                          */
+/* ------------------------------------------------------------------------ */
+
+/* Every per-particle array (state, proxies, list order, solver scratch) to
+ * n_new entries; new entries zeroed. */
+static void resize_particles(oc_cloth* c, uint32_t n_new)
+{
+    uint32_t n_old = c->n;
+#define GROW(ptr, T)                                                                   \
+    do {                                                                               \
+        ptr = (T*)realloc(ptr, (size_t)(n_new ? n_new : 1) * sizeof(T));               \
+        if (n_new > n_old) memset(ptr + n_old, 0, (size_t)(n_new - n_old) * sizeof(T)); \
+    } while (0)
+    GROW(c->x, v3); GROW(c->v, v3); GROW(c->f, v3); GROW(c->y, v3); GROW(c->mx, v3);
+    GROW(c->mass, float); GROW(c->inv_mass, float); GROW(c->radius, float); GROW(c->friction, float);
+    GROW(c->type, uint8_t); GROW(c->fat_lo, v3); GROW(c->fat_hi, v3);
+    GROW(c->order, uint32_t); GROW(c->solver_of_vertex, uint32_t);
+    GROW(c->sx, v3); GROW(c->sv, v3); GROW(c->sf, v3); GROW(c->sy, v3); GROW(c->sx0, v3);
+    GROW(c->b, v3); GROW(c->dvsol, v3); GROW(c->Sflag, float);
+#undef GROW
+    c->a_rowptr = (uint32_t*)realloc(c->a_rowptr, (size_t)(n_new + 1) * sizeof(uint32_t));
+    for (uint32_t i = n_new; i < n_old; ++i) {  /* the rows that go: their buffers only */
+        free(c->dfdx[i].cols); free(c->dfdx[i].vals);
+        free(c->dfdv[i].cols); free(c->dfdv[i].vals);
+    }
+    c->dfdx = (lrow*)realloc(c->dfdx, (size_t)(n_new ? n_new : 1) * sizeof(lrow));
+    c->dfdv = (lrow*)realloc(c->dfdv, (size_t)(n_new ? n_new : 1) * sizeof(lrow));
+    if (n_new > n_old) {
+        memset(c->dfdx + n_old, 0, (size_t)(n_new - n_old) * sizeof(lrow));
+        memset(c->dfdv + n_old, 0, (size_t)(n_new - n_old) * sizeof(lrow));
+    }
+}
+
+/* b3Cloth::CreateParticle (cloth.cpp:307-322) with b3Particle::b3Particle
+ * (particle.cpp:24-51): mass 0 makes a static particle of mass 1; the proxy
+ * is the particle's AABB fattened by B3_AABB_EXTENSION; the particle heads
+ * the particle list.  Returns its index, after every existing particle. */
+uint32_t oc_create_particle(oc_cloth* c, const float* position, const float* velocity, float mass, float radius,
+                            float friction)
+{
+    uint32_t i = c->n;
+    resize_particles(c, i + 1);
+    c->n = i + 1;
+    c->x[i] = V(position[0], position[1], position[2]);
+    c->v[i] = velocity ? V(velocity[0], velocity[1], velocity[2]) : vzero();
+    if (mass == 0.0f) {
+        c->type[i] = OC_STATIC;
+        c->mass[i] = 1.0f;
+        c->inv_mass[i] = 1.0f;
+    } else {
+        c->type[i] = OC_DYNAMIC;
+        c->mass[i] = mass;
+        c->inv_mass[i] = 1.0f / mass;
+    }
+    c->radius[i] = radius;
+    c->friction[i] = friction;
+    v3 r = V(radius, radius, radius);
+    v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
+    c->fat_lo[i] = vsub(vsub(c->x[i], r), ext);
+    c->fat_hi[i] = vadd(vadd(c->x[i], r), ext);
+    memmove(c->order + 1, c->order, (size_t)i * sizeof(uint32_t));
+    c->order[0] = i;
+    return i;
+}
+
+/* b3Cloth::DestroyParticle (cloth.cpp:324-351) of a created particle: its
+ * forces, its contacts and its list entry go; particles created after it
+ * move down one index. */
+int oc_destroy_particle(oc_cloth* c, uint32_t i)
+{
+    if (i < c->n_mesh || i >= c->n) return -1;
+    uint32_t w = 0;
+    for (uint32_t q = 0; q < c->nforce; ++q) {
+        const force_t* fo = c->forces + q;
+        int has = 0;
+        if (fo->type == F_MOUSE) {
+            const uint32_t* tv = c->tris + 3 * (size_t)fo->b;
+            has = fo->a == i || tv[0] == i || tv[1] == i || tv[2] == i;
+        } else if (fo->type == F_SPRING) {
+            has = fo->a == i || fo->b == i;
+        }
+        if (!has) c->forces[w++] = *fo;
+    }
+    c->nforce = w;
+    destroy_particle_contacts(c, i);
+    uint32_t k = 0;
+    for (uint32_t q = 0; q < c->n; ++q)
+        if (c->order[q] != i) c->order[k++] = c->order[q] > i ? c->order[q] - 1 : c->order[q];
+    for (uint32_t q = 0; q < c->nforce; ++q)
+        if (c->forces[q].type == F_MOUSE && c->forces[q].a > i) c->forces[q].a -= 1;
+    for (uint32_t q = 0; q < c->ncontact; ++q)
+        if (c->contacts[q].particle > i) c->contacts[q].particle -= 1;
+    uint32_t tail = c->n - i - 1;
+#define SHIFT(ptr) memmove(ptr + i, ptr + i + 1, (size_t)tail * sizeof(*ptr))
+    SHIFT(c->x); SHIFT(c->v); SHIFT(c->f); SHIFT(c->y); SHIFT(c->mx);
+    SHIFT(c->mass); SHIFT(c->inv_mass); SHIFT(c->radius); SHIFT(c->friction); SHIFT(c->type);
+    SHIFT(c->fat_lo); SHIFT(c->fat_hi);
+#undef SHIFT
+    resize_particles(c, c->n - 1);
+    c->n -= 1;
+    return 0;
+}
+
+/* b3Cloth::CreateForce (cloth.cpp:353-358) of a b3MouseForceDef
+ * (mouse_force.h:26-40): the new force heads the force list. */
+uint32_t oc_create_mouse_force(oc_cloth* c, uint32_t particle, uint32_t triangle, float w2, float w3, float w4,
+                               float mouse, float damping)
+{
+    c->forces = (force_t*)realloc(c->forces, (size_t)(c->nforce + 1) * sizeof(force_t));
+    memmove(c->forces + 1, c->forces, (size_t)c->nforce * sizeof(force_t));
+    force_t f;
+    memset(&f, 0, sizeof(f));
+    f.type = F_MOUSE;
+    f.a = particle;
+    f.b = triangle;
+    f.ks = mouse;
+    f.kd = damping;
+    f.p0 = w2;
+    f.p1 = w3;
+    f.p2 = w4;
+    f.id = ++c->next_force_id;
+    c->forces[0] = f;
+    c->nforce += 1;
+    return f.id;
+}
+
+/* b3Cloth::DestroyForce (cloth.cpp:360-364) */
+int oc_destroy_force(oc_cloth* c, uint32_t id)
+{
+    for (uint32_t q = 0; q < c->nforce; ++q) {
+        if (c->forces[q].type == F_MOUSE && c->forces[q].id == id) {
+            memmove(c->forces + q, c->forces + q + 1, (size_t)(c->nforce - q - 1) * sizeof(force_t));
+            c->nforce -= 1;
+            return 0;
+        }
+    }
+    return -1;
+}
+
+uint32_t oc_particle_count(const oc_cloth* c) { return c->n; }
+
 /* ------------------------------------------------------------------------ */
 /* system formation                                                          */
 /* ------------------------------------------------------------------------ */
@@ -731,6 +919,7 @@ static void form_system(oc_cloth* c, float h)
         const force_t* fo = c->forces + q;
         if (fo->type == F_STRETCH) apply_stretch(c, fo);
         else if (fo->type == F_SHEAR) apply_shear(c, fo);
+        else if (fo->type == F_MOUSE) apply_mouse(c, fo);
         else apply_spring(c, fo);
     }
 
@@ -1375,6 +1564,9 @@ uint32_t oc_describe(const oc_cloth* c, float* tri_rest, float* fat_aabb, float*
             if (f->type == F_SPRING) {
                 o[1] = (float)f->a; o[2] = (float)f->b; o[3] = -1.0f;
                 o[4] = f->ks; o[5] = f->kd; o[6] = f->p0;
+            } else if (f->type == F_MOUSE) {
+                o[1] = (float)f->a; o[2] = (float)f->b; o[3] = -1.0f;
+                o[4] = f->ks; o[5] = f->kd; o[6] = f->p0; o[7] = f->p1;
             } else {
                 o[1] = (float)c->tris[3 * f->a]; o[2] = (float)c->tris[3 * f->a + 1];
                 o[3] = (float)c->tris[3 * f->a + 2];

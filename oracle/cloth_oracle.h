@@ -80,6 +80,22 @@ uint32_t oc_spring_count(const oc_cloth* c);
 /* Springs in creation order: vertex pairs (2 per spring) and rest lengths. */
 void oc_get_springs(const oc_cloth* c, uint32_t* pairs, float* rest_length, float* stiffness);
 
+/* Created particles and forces (cloth.cpp:307-364).  A created particle
+ * (b3ParticleDef: position, velocity, mass, radius, friction; mass 0 makes
+ * it static) takes the index after every existing particle and heads the
+ * particle list.  Destroying one (only created particles can be) removes its
+ * forces and contacts; particles created after it move down one index.  A
+ * mouse force (mouse_force.h:26-40) ties `particle` to the point
+ * w2 x(v1) + w3 x(v2) + w4 x(v3) of `triangle` and heads the force list;
+ * the returned id names it to oc_destroy_force.  Return 0 / -1 on error. */
+uint32_t oc_create_particle(oc_cloth* c, const float* position, const float* velocity, float mass, float radius,
+                            float friction);
+int oc_destroy_particle(oc_cloth* c, uint32_t particle);
+uint32_t oc_create_mouse_force(oc_cloth* c, uint32_t particle, uint32_t triangle, float w2, float w3, float w4,
+                               float mouse, float damping);
+int oc_destroy_force(oc_cloth* c, uint32_t id);
+uint32_t oc_particle_count(const oc_cloth* c);
+
 /* The system one force solve would build (cloth_force_solver.cpp:142-204),
  * rows in solver order, blocks in the reference's row-list order. */
 uint32_t oc_build_system(oc_cloth* c, float dt);

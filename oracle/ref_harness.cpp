@@ -56,6 +56,7 @@
 #include <bounce/cloth/forces/strech_force.h>
 #include <bounce/cloth/forces/shear_force.h>
 #include <bounce/cloth/forces/spring_force.h>
+#include <bounce/cloth/forces/mouse_force.h>
 #include <bounce/cloth/contacts/cloth_particle_body_contact.h>
 #include <bounce/sparse/dense_vec3.h>
 #include <bounce/sparse/diag_mat33.h>
@@ -118,11 +119,22 @@ struct RefCloth {
     b3Cloth* cloth = nullptr;
     b3World* world = nullptr;
     std::vector<b3SphereShape*> sphere_protos;
+    // Particles made with b3Cloth::CreateParticle, addressed after the mesh
+    // vertices (index vertexCount + k), and mouse forces by id - 1 (null once
+    // destroyed).
+    std::vector<b3Particle*> extra;
+    std::vector<b3MouseForce*> mice;
 
     // Last exported system (solver-row order).
     std::vector<uint32_t> sys_rowptr, sys_cols, sys_vertex_of_row;
     std::vector<float> sys_vals, sys_b, sys_S, sys_x0;
 };
+
+b3Particle* particle_at(RefCloth* h, uint32_t i)
+{
+    u32 n = h->mesh.vertexCount;
+    return i < n ? h->cloth->m_particles[i] : h->extra[i - n];
+}
 
 // Same pairs, same order as b3FindSharedEdges (cloth.cpp:40-94): for each
 // triangle i, each of its edges (a -> b) in vertex order, every later
@@ -373,27 +385,27 @@ void ref_cloth_set_gravity(void* hp, const float* g)
 
 void ref_cloth_set_type(void* hp, uint32_t vertex, int type)
 {
-    ((RefCloth*)hp)->cloth->GetParticle(vertex)->SetType((b3ParticleType)type);
+    particle_at((RefCloth*)hp, vertex)->SetType((b3ParticleType)type);
 }
 
 void ref_cloth_apply_force(void* hp, uint32_t vertex, const float* f)
 {
-    ((RefCloth*)hp)->cloth->GetParticle(vertex)->ApplyForce(b3Vec3(f[0], f[1], f[2]));
+    particle_at((RefCloth*)hp, vertex)->ApplyForce(b3Vec3(f[0], f[1], f[2]));
 }
 
 void ref_cloth_apply_translation(void* hp, uint32_t vertex, const float* t)
 {
-    ((RefCloth*)hp)->cloth->GetParticle(vertex)->ApplyTranslation(b3Vec3(t[0], t[1], t[2]));
+    particle_at((RefCloth*)hp, vertex)->ApplyTranslation(b3Vec3(t[0], t[1], t[2]));
 }
 
 void ref_cloth_set_position(void* hp, uint32_t vertex, const float* x)
 {
-    ((RefCloth*)hp)->cloth->GetParticle(vertex)->SetPosition(b3Vec3(x[0], x[1], x[2]));
+    particle_at((RefCloth*)hp, vertex)->SetPosition(b3Vec3(x[0], x[1], x[2]));
 }
 
 void ref_cloth_set_velocity(void* hp, uint32_t vertex, const float* v)
 {
-    ((RefCloth*)hp)->cloth->GetParticle(vertex)->SetVelocity(b3Vec3(v[0], v[1], v[2]));
+    particle_at((RefCloth*)hp, vertex)->SetVelocity(b3Vec3(v[0], v[1], v[2]));
 }
 
 // A static body at `center` carrying one sphere shape of `radius`, in a world
@@ -436,9 +448,9 @@ uint32_t ref_last_iterations() { return b3_clothSolverIterations; }
 void ref_cloth_get_state(void* hp, float* x, float* v, float* dv, float* mass, uint8_t* type)
 {
     RefCloth* h = (RefCloth*)hp;
-    u32 n = h->mesh.vertexCount;
+    u32 n = h->mesh.vertexCount + (u32)h->extra.size();
     for (u32 i = 0; i < n; ++i) {
-        b3Particle* p = h->cloth->m_particles[i];
+        b3Particle* p = particle_at(h, i);
         if (x) put3(x + 3 * i, p->m_position);
         if (v) put3(v + 3 * i, p->m_velocity);
         if (dv) put3(dv + 3 * i, p->m_x);
@@ -448,6 +460,69 @@ void ref_cloth_get_state(void* hp, float* x, float* v, float* dv, float* mass, u
 }
 
 float ref_cloth_energy(void* hp) { return ((RefCloth*)hp)->cloth->GetEnergy(); }
+
+// b3Cloth::CreateParticle (cloth.cpp:307-322); returns the particle's index.
+uint32_t ref_cloth_create_particle(void* hp, const float* position, const float* velocity, float mass, float radius,
+                                   float friction)
+{
+    RefCloth* h = (RefCloth*)hp;
+    b3ParticleDef pd;
+    pd.mass = mass;
+    pd.position.Set(position[0], position[1], position[2]);
+    if (velocity) pd.velocity.Set(velocity[0], velocity[1], velocity[2]);
+    pd.radius = radius;
+    pd.friction = friction;
+    h->extra.push_back(h->cloth->CreateParticle(pd));
+    return h->mesh.vertexCount + (uint32_t)h->extra.size() - 1;
+}
+
+// b3Cloth::DestroyParticle (cloth.cpp:324-351) of a created particle; the
+// mouse forces it takes with it are forgotten here too.
+int ref_cloth_destroy_particle(void* hp, uint32_t i)
+{
+    RefCloth* h = (RefCloth*)hp;
+    u32 n = h->mesh.vertexCount;
+    if (i < n || i >= n + h->extra.size()) return -1;
+    b3Particle* p = h->extra[i - n];
+    for (b3MouseForce*& m : h->mice)
+        if (m && m->HasParticle(p)) m = nullptr;
+    h->cloth->DestroyParticle(p);
+    h->extra.erase(h->extra.begin() + (i - n));
+    return 0;
+}
+
+// b3Cloth::CreateForce (cloth.cpp:353-358) of a b3MouseForceDef; returns its id.
+uint32_t ref_cloth_create_mouse_force(void* hp, uint32_t particle, uint32_t triangle, float w2, float w3, float w4,
+                                      float mouse, float damping)
+{
+    RefCloth* h = (RefCloth*)hp;
+    b3MouseForceDef def;
+    def.particle = particle_at(h, particle);
+    def.triangle = h->cloth->GetTriangle(triangle);
+    def.w2 = w2;
+    def.w3 = w3;
+    def.w4 = w4;
+    def.mouse = mouse;
+    def.damping = damping;
+    h->mice.push_back((b3MouseForce*)h->cloth->CreateForce(def));
+    return (uint32_t)h->mice.size();
+}
+
+// b3Cloth::DestroyForce (cloth.cpp:360-364)
+int ref_cloth_destroy_force(void* hp, uint32_t id)
+{
+    RefCloth* h = (RefCloth*)hp;
+    if (id == 0 || id > h->mice.size() || !h->mice[id - 1]) return -1;
+    h->cloth->DestroyForce(h->mice[id - 1]);
+    h->mice[id - 1] = nullptr;
+    return 0;
+}
+
+uint32_t ref_cloth_particle_count(void* hp)
+{
+    RefCloth* h = (RefCloth*)hp;
+    return h->mesh.vertexCount + (uint32_t)h->extra.size();
+}
 
 // Rest state per triangle (du1, dv1, du2, dv2, inv_det, alpha), particle fat
 // AABBs (lower xyz, upper xyz) and the force list in application order.
@@ -617,7 +692,14 @@ uint32_t ref_cloth_build_system(void* hp, float dt)
         put3(&h->sys_b[3 * i], b[i]);
         put3(&h->sys_x0[3 * i], sx0[i]);
         h->sys_S[i] = S[i].x.x;
-        h->sys_vertex_of_row[i] = particles[i]->m_vertex;
+    {
+        // created particles have no mesh vertex: report their index
+        uint32_t v = particles[i]->m_vertex;
+        if (v == ~0u)
+            for (size_t k = 0; k < h->extra.size(); ++k)
+                if (h->extra[k] == particles[i]) v = h->mesh.vertexCount + (uint32_t)k;
+        h->sys_vertex_of_row[i] = v;
+    }
     }
     return (uint32_t)h->sys_cols.size();
 }

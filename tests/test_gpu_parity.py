@@ -26,9 +26,10 @@ def _pair(b3g, port, scene, opts=None):
     return gpu, ora
 
 
-@pytest.mark.parametrize("maker", ["plain", "sphere"])
+@pytest.mark.parametrize("maker", ["plain", "sphere", "sewn"])
 def test_assembly_bit_exact(b3g, port, maker):
-    scene = b3g.plain_scene(24) if maker == "plain" else b3g.sphere_scene(24)
+    scene = {"plain": lambda: b3g.plain_scene(24), "sphere": lambda: b3g.sphere_scene(24),
+             "sewn": lambda: b3g.sewn_scene(16)}[maker]()
     gpu, ora = _pair(b3g, port, scene)
     # move away from the rest state so every element is active
     rng = np.random.default_rng(5)
@@ -201,3 +202,88 @@ def test_persistent_cg_bounded_wait_times_out(b3g):
     assert res.value == 7  # B3G_ERR_TIMEOUT
     out = cloth.step(scene.dt)
     assert out["iterations"] > 0
+
+
+def test_sewn_cloth_per_step(b3g, port):
+    """Two panels sewn along their side edges: from identical inputs every
+    step matches the oracle (CG iterations +-1, positions within 1e-4)."""
+    scene = b3g.sewn_scene(16)
+    opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
+    gpu, ora = _pair(b3g, port, scene, opts)
+    for step in range(40):
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        assert abs(g["iterations"] - o["iterations"]) <= 1, (step, g["iterations"], o["iterations"])
+        assert rel_err(gpu.state()["x"], ora.state()["x"]) <= 1e-4, step
+
+
+def test_assembly_bit_exact_with_mouse_force(b3g, port):
+    """A created static particle tied to a triangle point by a mouse force:
+    the assembled rows of the particle and the triangle's vertices match the
+    oracle bit for bit (the force heads the force list)."""
+    scene = b3g.sphere_scene(24)
+    gpu, ora = _pair(b3g, port, scene)
+    tri = 300
+    p0 = (scene.mesh.vertices[scene.mesh.triangles[tri]].mean(axis=0) + [0.0, 0.05, 0.0]).astype(np.float32)
+    ig = gpu.create_particle(p0)
+    io = ora.create_particle(p0)
+    assert ig == io == scene.mesh.vertex_count
+    gpu.create_mouse_force(ig, tri, 0.2, 0.3, 0.5, 800.0, 4.0)
+    ora.create_mouse_force(io, tri, 0.2, 0.3, 0.5, 800.0, 4.0)
+    rng = np.random.default_rng(7)
+    x = np.concatenate([scene.mesh.vertices, p0[None]]) + rng.normal(0, 2e-3, (gpu.n, 3)).astype(np.float32)
+    v = rng.normal(0, 0.1, (gpu.n, 3)).astype(np.float32)
+    gpu.write_state(x=x, v=v)
+    ora.set_state(x=x, v=v)
+    gpu.assemble(scene.dt)
+    gb, gbv = system_blocks(gpu.system())
+    os_ = ora.system(scene.dt)
+    ob, obv = system_blocks(os_, os_["vertex_of_row"])
+    for key, val in ob.items():
+        assert key in gb, key
+        assert np.array_equal(gb[key], val), key
+    for key, val in gb.items():
+        if key not in ob:
+            assert not np.any(val), key
+    assert np.array_equal(gbv, obv)
+
+
+def test_mouse_drag_per_step(b3g, port):
+    """A drag through the C ABI (create particle, mouse force, move the
+    particle every step, destroy both): from identical inputs every step
+    matches the oracle, before and after the release."""
+    scene = b3g.sphere_scene(32)
+    opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
+    gpu, ora = _pair(b3g, port, scene, opts)
+    for _ in range(5):
+        gpu.step(scene.dt)
+    tri = 500
+    p0 = gpu.state()["x"][scene.mesh.triangles[tri]].mean(axis=0).astype(np.float32)
+    ig = gpu.create_particle(p0)
+    io = ora.create_particle(p0)
+    fg = gpu.create_mouse_force(ig, tri, 1 / 3, 1 / 3, 1 / 3, 1000.0, 5.0)
+    fo = ora.create_mouse_force(io, tri, 1 / 3, 1 / 3, 1 / 3, 1000.0, 5.0)
+
+    def check(step):
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        assert abs(g["iterations"] - o["iterations"]) <= 1, (step, g["iterations"], o["iterations"])
+        assert rel_err(gpu.state()["x"], ora.state()["x"]) <= 1e-4, step
+
+    for k in range(25):
+        p = p0 + np.array([0.0, 0.02 * k, 0.0], np.float32)
+        gpu.particle(ig).set_position(p)
+        ora.set_position(io, p)
+        check(k)
+    assert gpu.state()["x"].shape[0] == scene.mesh.vertex_count + 1
+    gpu.destroy_force(fg)
+    ora.destroy_force(fo)
+    gpu.destroy_particle(ig)
+    ora.destroy_particle(io)
+    assert gpu.n == scene.mesh.vertex_count
+    for k in range(10):
+        check(100 + k)

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import oracle
-from bounce_b200.meshes import plain_scene, sphere_scene
+from bounce_b200.meshes import plain_scene, sewn_scene, sphere_scene
 
 pytestmark = pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built")
 
@@ -25,6 +25,18 @@ def test_restated_constructor_matches_reference(side):
     assert np.array_equal(real.state()["mass"], port.state()["mass"])
 
 
+def test_sewing_springs_match_reference_constructor():
+    """Two panels sewn along their side edges: the same force list (triangles
+    and the sewing springs of cloth.cpp:248-262) in the same order."""
+    scene = sewn_scene(12)
+    real = oracle.RefCloth(scene.mesh, scene.cdef, restated=False)
+    port = oracle.PortCloth(scene.mesh, scene.cdef)
+    a, c = real.describe(), port.describe()
+    assert a["forces"].shape[0] == 2 * scene.mesh.triangle_count + scene.mesh.sewing.shape[0]
+    for k in a:
+        assert np.array_equal(a[k], c[k]), k
+
+
 def test_skipping_self_collision_is_exact():
     """At thickness 0 the reference's own b3Cloth::Step (with its cloth
     self-collision pass) and the harness step without it agree bit for bit."""
@@ -39,7 +51,8 @@ def test_skipping_self_collision_is_exact():
             assert np.array_equal(sa[q], sb[q])
 
 
-@pytest.mark.parametrize("maker,steps", [(lambda: plain_scene(20), 25), (lambda: sphere_scene(24), 45)])
+@pytest.mark.parametrize("maker,steps", [(lambda: plain_scene(20), 25), (lambda: sphere_scene(24), 45),
+                                         (lambda: sewn_scene(12), 40)])
 def test_port_tracks_reference_bit_exact(maker, steps):
     scene = maker()
     ref = oracle.RefCloth(scene.mesh, scene.cdef).setup(scene)
@@ -68,3 +81,45 @@ def test_port_mpcg_reproduces_reference_solution():
     # rows are in solver order; m_x is reported by vertex
     dv = ref.state()["dv"]
     assert np.array_equal(x, dv[sysd["vertex_of_row"]])
+
+
+@pytest.mark.parametrize("maker", [lambda: plain_scene(12), lambda: sphere_scene(12)])
+def test_mouse_drag_matches_reference(maker):
+    """Created particle + mouse force (cloth.cpp:307-364, mouse_force.cpp:63-227),
+    as the testbed's cloth dragger uses them: a static particle at a point of
+    a triangle, a mouse force to it, the particle moved every step, then both
+    destroyed.  The restatement follows the reference bit for bit through the
+    drag, the release and the steps after it."""
+    scene = maker()
+    ref = oracle.RefCloth(scene.mesh, scene.cdef).setup(scene)
+    port = oracle.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    for _ in range(5):
+        ref.step(scene.dt)
+        port.step(scene.dt)
+    tri = 60
+    xs = ref.state()["x"][scene.mesh.triangles[tri]]
+    p0 = (0.2 * xs[0] + 0.3 * xs[1] + 0.5 * xs[2]).astype(np.float32)
+    ids = []
+    for cl in (ref, port):
+        i = cl.create_particle(p0)
+        ids.append((i, cl.create_mouse_force(i, tri, 0.2, 0.3, 0.5, 1000.0, 5.0)))
+    assert ids[0][0] == ids[1][0] == scene.mesh.vertex_count
+
+    def same():
+        sr, sp = ref.state(), port.state()
+        for q in ("x", "v", "dv"):
+            assert np.array_equal(sr[q], sp[q]), q
+
+    for k in range(25):
+        p = p0 + np.array([0.0, 0.01 * k, 0.005 * k], np.float32)
+        for cl, (i, _) in zip((ref, port), ids):
+            cl.set_position(i, p)
+        assert ref.step(scene.dt)["iterations"] == port.step(scene.dt)["iterations"]
+        same()
+    for cl, (i, f) in zip((ref, port), ids):
+        cl.destroy_force(f)
+        cl.destroy_particle(i)
+    assert ref.n == port.n == scene.mesh.vertex_count
+    for _ in range(8):
+        assert ref.step(scene.dt)["iterations"] == port.step(scene.dt)["iterations"]
+        same()
