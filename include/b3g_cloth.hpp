@@ -80,6 +80,26 @@ public:
     void ClearColliders() { b3gCheck(b3g_cloth_clear_colliders(m_cloth), "ClearColliders"); }
     void SetSolver(const b3g_solver_opts& o) { b3gCheck(b3g_cloth_set_solver(m_cloth, &o), "SetSolver"); }
     b3gParticle GetParticle(uint32_t i) { return b3gParticle(m_cloth, i); }
+    // b3Cloth::CreateParticle / DestroyParticle (cloth.cpp:307-351): a particle
+    // outside the mesh, addressed after the mesh vertices.
+    b3gParticle CreateParticle(const b3g_particle_def& def)
+    {
+        uint32_t i;
+        b3gCheck(b3g_cloth_create_particle(m_cloth, &def, &i), "CreateParticle");
+        return b3gParticle(m_cloth, i);
+    }
+    void DestroyParticle(const b3gParticle& p)
+    {
+        b3gCheck(b3g_cloth_destroy_particle(m_cloth, p.GetVertex()), "DestroyParticle");
+    }
+    // b3Cloth::CreateForce of a b3MouseForceDef, and DestroyForce (cloth.cpp:353-364)
+    uint32_t CreateMouseForce(const b3g_mouse_force_def& def)
+    {
+        uint32_t id;
+        b3gCheck(b3g_cloth_create_mouse_force(m_cloth, &def, &id), "CreateForce");
+        return id;
+    }
+    void DestroyForce(uint32_t id) { b3gCheck(b3g_cloth_destroy_force(m_cloth, id), "DestroyForce"); }
     float GetEnergy() const
     {
         float e;

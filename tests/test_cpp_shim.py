@@ -21,6 +21,16 @@ int main() {
         c.SetGravity(g);
         c.GetParticle(0).SetType(B3G_STATIC);
         b3g_step_stats s = c.Step(1.0f / 60.0f, 8, 2);
+        // a mouse drag as the testbed's cloth dragger does it
+        b3g_particle_def pd = {};
+        pd.position[0] = 0.3f; pd.position[1] = 0.1f; pd.position[2] = 0.3f;
+        b3gParticle mp = c.CreateParticle(pd);
+        b3g_mouse_force_def md = {mp.GetVertex(), 0u, 0.3f, 0.3f, 0.4f, 1000.0f, 5.0f};
+        uint32_t f = c.CreateMouseForce(md);
+        s = c.Step(1.0f / 60.0f, 8, 2);
+        c.DestroyForce(f);
+        c.DestroyParticle(mp);
+        s = c.Step(1.0f / 60.0f, 8, 2);
         std::printf("stepped %u\n", s.iterations);
         return 0;
     } catch (const b3gError& e) {
