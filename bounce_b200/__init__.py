@@ -19,8 +19,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .meshes import (DYNAMIC, KINEMATIC, STATIC, ClothDef, Mesh, Scene, batch_scenes, grid_mesh, sewn_scene,  # noqa: F401
-                     plain_scene, sphere_scene, stiff_scene)
+from .meshes import (DYNAMIC, KINEMATIC, STATIC, ClothDef, Mesh, Scene, batch_scenes, capsule_scene, grid_mesh,  # noqa: F401
+                     plain_scene, sewn_scene, sphere_scene, stiff_scene)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 # B3G_LIBRARY: another build of libb3g.so to load instead of the in-tree one
@@ -136,6 +136,7 @@ def lib() -> C.CDLL:
             "b3g_cloth_set_solver": [vp, C.POINTER(SolverOptsC)],
             "b3g_cloth_add_static_sphere": [vp, vp, f32, f32, C.POINTER(u32)],
             "b3g_cloth_clear_colliders": [vp],
+            "b3g_cloth_add_static_capsule": [vp, vp, vp, f32, f32, C.POINTER(u32)],
             "b3g_cloth_create_particle": [vp, C.POINTER(ParticleDefC), C.POINTER(u32)],
             "b3g_cloth_destroy_particle": [vp, u32],
             "b3g_cloth_create_mouse_force": [vp, C.POINTER(MouseForceDefC), C.POINTER(u32)],
@@ -205,6 +206,9 @@ def check(status: int, what: str) -> None:
 
 
 def _ptr(a: np.ndarray) -> int:
+    """The address of `a`'s data.  The caller keeps `a` alive across the call
+    that uses the address: a temporary array may be freed (and its memory
+    reused) before the call runs."""
     return a.ctypes.data
 
 
@@ -248,7 +252,8 @@ class Particle:
         return out.value
 
     def set_position(self, x) -> None:
-        check(lib().b3g_particle_set_position(self.cloth.h, self.vertex, _ptr(_f3(x))), "set_position")
+        x3 = _f3(x)
+        check(lib().b3g_particle_set_position(self.cloth.h, self.vertex, _ptr(x3)), "set_position")
 
     def get_position(self) -> np.ndarray:
         out = np.zeros(3, np.float32)
@@ -256,7 +261,8 @@ class Particle:
         return out
 
     def set_velocity(self, v) -> None:
-        check(lib().b3g_particle_set_velocity(self.cloth.h, self.vertex, _ptr(_f3(v))), "set_velocity")
+        v3 = _f3(v)
+        check(lib().b3g_particle_set_velocity(self.cloth.h, self.vertex, _ptr(v3)), "set_velocity")
 
     def get_velocity(self) -> np.ndarray:
         out = np.zeros(3, np.float32)
@@ -269,10 +275,12 @@ class Particle:
         return out.value
 
     def apply_force(self, f) -> None:
-        check(lib().b3g_particle_apply_force(self.cloth.h, self.vertex, _ptr(_f3(f))), "apply_force")
+        f3 = _f3(f)
+        check(lib().b3g_particle_apply_force(self.cloth.h, self.vertex, _ptr(f3)), "apply_force")
 
     def apply_translation(self, t) -> None:
-        check(lib().b3g_particle_apply_translation(self.cloth.h, self.vertex, _ptr(_f3(t))), "apply_translation")
+        t3 = _f3(t)
+        check(lib().b3g_particle_apply_translation(self.cloth.h, self.vertex, _ptr(t3)), "apply_translation")
 
 
 class Cloth:
@@ -330,7 +338,8 @@ class Cloth:
 
     # b3Cloth API
     def set_gravity(self, g) -> None:
-        check(lib().b3g_cloth_set_gravity(self.h, _ptr(_f3(g))), "set_gravity")
+        g3 = _f3(g)
+        check(lib().b3g_cloth_set_gravity(self.h, _ptr(g3)), "set_gravity")
 
     def get_gravity(self) -> np.ndarray:
         out = np.zeros(3, np.float32)
@@ -343,8 +352,18 @@ class Cloth:
 
     def add_sphere(self, center, radius: float, friction: float) -> int:
         sid = C.c_uint32(0)
-        check(lib().b3g_cloth_add_static_sphere(self.h, _ptr(_f3(center)), radius, friction, C.byref(sid)),
+        c3 = _f3(center)
+        check(lib().b3g_cloth_add_static_sphere(self.h, _ptr(c3), radius, friction, C.byref(sid)),
               "add_static_sphere")
+        self.nsph += 1
+        return sid.value
+
+    def add_capsule(self, a, b, radius: float, friction: float) -> int:
+        """A static capsule collider: segment a-b (world frame), `radius`."""
+        sid = C.c_uint32(0)
+        a3, b3 = _f3(a), _f3(b)
+        check(lib().b3g_cloth_add_static_capsule(self.h, _ptr(a3), _ptr(b3), radius, friction,
+                                                 C.byref(sid)), "add_static_capsule")
         self.nsph += 1
         return sid.value
 
@@ -453,6 +472,8 @@ class Cloth:
         self.set_types(types)
         for (c, r, mu) in scene.spheres:
             self.add_sphere(c, r, mu)
+        for (a, b, r, mu) in scene.capsules:
+            self.add_capsule(a, b, r, mu)
         if opts is not None:
             self.set_solver(opts)
         return self

@@ -292,7 +292,7 @@ b3g_status layout_cloth(b3g_cloth* c)
     add((size_t)n * 4); add(n);             // mass, type
     add(vec); add(vec);                     // fat lo / hi
     const size_t nn = (size_t)kMaxSpheres * n;
-    add(nn); add(nn); add(nn * 4); add(nn * 12); add(nn * 12); add(nn * 12); add(nn * 12);
+    add(nn); add(nn); add(nn * 4); add(nn * 12); add(nn * 12); add(nn * 12); add(nn * 12); add(nn * 12);
     add(sizeof(StepScalars));
     add(sizeof(GridBarrier));
     add(std::max((size_t)d.grid * 32, kGridCgPartialBytes));
@@ -402,6 +402,7 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     d.c_t1 = A.take<float>(3 * nn);
     d.c_t2 = A.take<float>(3 * nn);
     d.c_imp = A.take<float>(3 * nn);
+    d.c_point = A.take<float>(3 * nn);
     d.sc = A.take<StepScalars>(1);
     d.bar = A.take<GridBarrier>(1);
     d.partials = A.take<char>(std::max((size_t)d.grid * 32, kGridCgPartialBytes));
@@ -562,6 +563,8 @@ b3g_status b3g_cloth_add_static_sphere(b3g_cloth* c, const float center[3], floa
     if (!valid(c) || !center || !(radius > 0.0f) || !(friction >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
     if (c->dev.nsph >= (uint32_t)kMaxSpheres) return B3G_ERR_CAPACITY;
     SphereDev& s = c->dev.sph[c->dev.nsph];
+    s = SphereDev{};
+    s.kind = 0;
     s.cx = center[0];
     s.cy = center[1];
     s.cz = center[2];
@@ -571,6 +574,31 @@ b3g_status b3g_cloth_add_static_sphere(b3g_cloth* c, const float center[3], floa
     for (int q = 0; q < 3; ++q) {
         s.lo[q] = (center[q] - radius) - 0.2f;
         s.hi[q] = (center[q] + radius) + 0.2f;
+    }
+    if (shape_id) *shape_id = c->dev.nsph;
+    c->dev.nsph += 1;
+    destroy_graph(c);
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_add_static_capsule(b3g_cloth* c, const float a[3], const float b[3], float radius,
+                                        float friction, uint32_t* shape_id)
+{
+    if (!valid(c) || !a || !b || !(radius > 0.0f) || !(friction >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    for (int q = 0; q < 3; ++q)
+        if (!std::isfinite(a[q]) || !std::isfinite(b[q])) return B3G_ERR_INVALID_ARGUMENT;
+    if (c->dev.nsph >= (uint32_t)kMaxSpheres) return B3G_ERR_CAPACITY;
+    SphereDev& s = c->dev.sph[c->dev.nsph];
+    s = SphereDev{};
+    s.kind = 1;
+    s.ax = a[0], s.ay = a[1], s.az = a[2];
+    s.bx = b[0], s.by = b[1], s.bz = b[2];
+    s.radius = radius;
+    s.friction = friction;
+    // b3CapsuleShape::ComputeAABB (capsule_shape.cpp:130-137) fattened by B3_AABB_EXTENSION
+    for (int q = 0; q < 3; ++q) {
+        s.lo[q] = (std::min(a[q], b[q]) - radius) - 0.2f;
+        s.hi[q] = (std::max(a[q], b[q]) + radius) + 0.2f;
     }
     if (shape_id) *shape_id = c->dev.nsph;
     c->dev.nsph += 1;
@@ -601,7 +629,7 @@ struct ParticleState {
     std::vector<float> x, v, fext, y, mx, lo, hi, mass;
     std::vector<uint8_t> type, c_exists, c_active;
     std::vector<uint32_t> c_key;
-    std::vector<float> c_normal, c_t1, c_t2, c_imp;
+    std::vector<float> c_normal, c_t1, c_t2, c_imp, c_point;
 };
 
 b3g_status download_state(b3g_cloth* c, ParticleState& s)
@@ -632,6 +660,7 @@ b3g_status download_state(b3g_cloth* c, ParticleState& s)
     B3G_TRY(get(s.c_t1, d.c_t1, 3 * nn));
     B3G_TRY(get(s.c_t2, d.c_t2, 3 * nn));
     B3G_TRY(get(s.c_imp, d.c_imp, 3 * nn));
+    B3G_TRY(get(s.c_point, d.c_point, 3 * nn));
     B3G_TRY(cudaStreamSynchronize(st));
     return B3G_OK;
 }
@@ -661,6 +690,7 @@ b3g_status upload_state(b3g_cloth* c, const ParticleState& s)
     B3G_TRY(put(d.c_t1, s.c_t1, 3 * nn));
     B3G_TRY(put(d.c_t2, s.c_t2, 3 * nn));
     B3G_TRY(put(d.c_imp, s.c_imp, 3 * nn));
+    B3G_TRY(put(d.c_point, s.c_point, 3 * nn));
     return B3G_OK;
 }
 
@@ -704,6 +734,7 @@ ParticleState remap(const ParticleState& s, const std::vector<uint32_t>& keep)
     planes(s.c_t1, r.c_t1, nn0, nn1, s.nsph);
     planes(s.c_t2, r.c_t2, nn0, nn1, s.nsph);
     planes(s.c_imp, r.c_imp, nn0, nn1, s.nsph);
+    planes(s.c_point, r.c_point, nn0, nn1, s.nsph);
     return r;
 }
 

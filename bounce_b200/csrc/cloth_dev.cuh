@@ -60,9 +60,13 @@ struct StepScalars {
 
 struct GridBarrier;
 
+// A static collider: a sphere (kind 0) or a capsule (kind 1, segment a-b in
+// the world frame, its body at the origin).
 struct SphereDev {
     float cx, cy, cz, radius, friction;
     float lo[3], hi[3];   // fat AABB of the shape proxy
+    uint32_t kind;
+    float ax, ay, az, bx, by, bz;
 };
 
 struct ClothDev {
@@ -104,6 +108,7 @@ struct ClothDev {
     float* c_t1;
     float* c_t2;
     float* c_imp;               // normal, tangent x, tangent y
+    float* c_point;             // capsules: the shape point of the contact (3 planes of nsph * n)
     SphereDev sph[kMaxSpheres];
 
     StepScalars* sc;

@@ -688,16 +688,60 @@ __global__ void k_contacts_update(const __grid_constant__ ClothDev one, const __
             continue;
         }
         const float radius = sp.radius + c.thickness;
-        const float rr = radius * radius;
-        const f3 d = xi - mk(sp.cx, sp.cy, sp.cz);
-        const float dd = dot(d, d);
-        if (!(dd <= rr)) {
-            c.c_active[q] = 0;
-            continue;
+        f3 normal;
+        if (sp.kind == 0) {
+            // b3SphereShape::TestSphere (sphere_shape.cpp:71-95)
+            const float rr = radius * radius;
+            const f3 d = xi - mk(sp.cx, sp.cy, sp.cz);
+            const float dd = dot(d, d);
+            if (!(dd <= rr)) {
+                c.c_active[q] = 0;
+                continue;
+            }
+            const float d_len = sqrtf(dd);
+            normal = mk(0.0f, 1.0f, 0.0f);
+            if (d_len > kEps) normal = d / d_len;
+        } else {
+            // b3CapsuleShape::TestSphere (capsule_shape.cpp:186-284)
+            const f3 A = mk(sp.ax, sp.ay, sp.az), B = mk(sp.bx, sp.by, sp.bz);
+            const f3 AB = B - A;
+            const float u = dot(B - xi, AB);
+            const float v = dot(xi - A, AB);
+            f3 P;
+            if (v <= 0.0f || u <= 0.0f) {
+                P = v <= 0.0f ? A : B;
+                const f3 d = xi - P;
+                const float dd = dot(d, d);
+                if (dd > radius * radius) {
+                    c.c_active[q] = 0;
+                    continue;
+                }
+                normal = mk(0.0f, 1.0f, 0.0f);
+                const float len = sqrtf(dd);
+                if (len > kEps) normal = d / len;
+            } else {
+                const float ss = dot(AB, AB);
+                P = ss < kLinearSlop * kLinearSlop ? A : (u * A + v * B) / ss;
+                const f3 d = xi - P;
+                const float dd = dot(d, d);
+                if (dd > radius * radius) {
+                    c.c_active[q] = 0;
+                    continue;
+                }
+                const f3 QA = A - xi;
+                const f3 e = cross(AB, QA);
+                f3 nn3 = cross(AB, e);
+                if (dot(nn3, QA) < 0.0f) nn3 = mk(-nn3.x, -nn3.y, -nn3.z);
+                // b3Vec3::Normalize (vec3.h:93-104)
+                const float len = sqrtf(nn3.x * nn3.x + nn3.y * nn3.y + nn3.z * nn3.z);
+                if (len > kEps) {
+                    const float s1 = 1.0f / len;
+                    nn3 = mk(nn3.x * s1, nn3.y * s1, nn3.z * s1);
+                }
+                normal = mk(-nn3.x, -nn3.y, -nn3.z);
+            }
+            st3(c.c_point, nn, q, P);
         }
-        const float d_len = sqrtf(dd);
-        f3 normal = mk(0.0f, 1.0f, 0.0f);
-        if (d_len > kEps) normal = d / d_len;
         const f3 n1 = mk(-normal.x, -normal.y, -normal.z);
         const f3 t1 = perp(n1);
         const f3 t2 = cross(t1, n1);
@@ -741,7 +785,7 @@ __device__ float position_iteration(const ClothDev& c, uint32_t i, f3& pos, cons
         const int s = order[a];
         const SphereDev& sp = c.sph[s];
         const f3 nA = ld3(c.c_normal, nn, s * n + i);
-        const f3 cB = mk(sp.cx, sp.cy, sp.cz);
+        const f3 cB = sp.kind == 0 ? mk(sp.cx, sp.cy, sp.cz) : ld3(c.c_point, nn, s * n + i);
         const float separation = dot(cB - pos, nA) - c.thickness - sp.radius;
         min_sep = min_sep < separation ? min_sep : separation;
         const float Cv = kBaumgarte * (separation + kLinearSlop);

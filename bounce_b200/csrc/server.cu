@@ -149,6 +149,7 @@ b3g_status activate(b3g_server* s, Request* r)
     }
     for (size_t k = 0; k + 5 <= r->spheres.size() && c->dev.nsph < (uint32_t)kMaxSpheres; k += 5) {
         SphereDev& sp = c->dev.sph[c->dev.nsph++];
+        sp = SphereDev{};
         sp.cx = r->spheres[k];
         sp.cy = r->spheres[k + 1];
         sp.cz = r->spheres[k + 2];

@@ -86,6 +86,7 @@ class Scene:
     pinned: np.ndarray                      # vertex ids made static
     gravity: tuple = (0.0, -9.8, 0.0)
     spheres: list = field(default_factory=list)   # (center (3,), radius, friction)
+    capsules: list = field(default_factory=list)  # (a (3,), b (3,), radius, friction): static, world frame
     dt: float = 1.0 / 60.0
     steps: int = 100
     velocity_iterations: int = 8
@@ -113,6 +114,16 @@ def sphere_scene(side: int = 256, seed: int = 2, steps: int = 200) -> Scene:
     pins = np.array([0, side - 1], dtype=np.uint32)
     sph = [((0.0, -0.5, 0.0), 0.3, 0.3)]
     return Scene(f"grid{side}_bend_sphere", mesh, cdef, pins, spheres=sph, steps=steps)
+
+
+def capsule_scene(side: int = 32, seed: int = 5, steps: int = 120) -> Scene:
+    """A cloth falling over a static capsule (a rod along z, radius 0.1 m,
+    0.4 m below the cloth), stretch 1e4, shear 1e3, bending 1e2, damping
+    0.05, friction 0.3, jitter N(0, 1e-3 m), nothing pinned."""
+    mesh = grid_mesh(side, 1.0, 1e-3, seed)
+    cdef = ClothDef(density=1.0, streching=1e4, shearing=1e3, bending=1e2, damping=0.05, friction=0.3)
+    caps = [((0.1, -0.4, -0.6), (-0.1, -0.4, 0.6), 0.1, 0.3)]
+    return Scene(f"grid{side}_capsule", mesh, cdef, np.zeros(0, np.uint32), capsules=caps, steps=steps)
 
 
 def stiff_scene(side: int = 1024, steps: int = 50) -> Scene:

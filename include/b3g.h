@@ -112,6 +112,13 @@ b3g_status b3g_cloth_set_solver(b3g_cloth* cloth, const b3g_solver_opts* opts);
 b3g_status b3g_cloth_add_static_sphere(b3g_cloth* cloth, const float center[3], float radius,
                                        float friction, uint32_t* shape_id);
 /* b3Cloth::SetWorld(nullptr): drop every collider and its contacts. */
+/* A static capsule collider (b3CapsuleShape, include/bounce/dynamics/shapes/
+ * capsule_shape.h) on a static body at the origin: segment a-b in world
+ * coordinates, `radius`; contacts as b3CapsuleShape::TestSphere
+ * (src/bounce/dynamics/shapes/capsule_shape.cpp:186-284).  Shares the
+ * collider capacity with spheres. */
+b3g_status b3g_cloth_add_static_capsule(b3g_cloth* cloth, const float a[3], const float b[3], float radius,
+                                        float friction, uint32_t* shape_id);
 b3g_status b3g_cloth_clear_colliders(b3g_cloth* cloth);
 
 /* ---- created particles and mouse forces ------------------------------------ */

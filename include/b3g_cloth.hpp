@@ -77,6 +77,13 @@ public:
         b3gCheck(b3g_cloth_add_static_sphere(m_cloth, c, radius, friction, &id), "AddStaticSphere");
         return id;
     }
+    // a static capsule body: segment a-b (world frame), radius
+    uint32_t AddStaticCapsule(const float a[3], const float b[3], float radius, float friction)
+    {
+        uint32_t id;
+        b3gCheck(b3g_cloth_add_static_capsule(m_cloth, a, b, radius, friction, &id), "AddStaticCapsule");
+        return id;
+    }
     void ClearColliders() { b3gCheck(b3g_cloth_clear_colliders(m_cloth), "ClearColliders"); }
     void SetSolver(const b3g_solver_opts& o) { b3gCheck(b3g_cloth_set_solver(m_cloth, &o), "SetSolver"); }
     b3gParticle GetParticle(uint32_t i) { return b3gParticle(m_cloth, i); }

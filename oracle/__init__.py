@@ -65,6 +65,7 @@ def port_lib():
         for name in ("oc_apply_force", "oc_apply_translation", "oc_set_position", "oc_set_velocity"):
             getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, _f32p]
         L.oc_add_sphere.argtypes = [C.c_void_p, _f32p, C.c_float, C.c_float]
+        L.oc_add_capsule.argtypes = [C.c_void_p, _f32p, _f32p, C.c_float, C.c_float]
         L.oc_set_solver.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_uint32, C.c_int]
         L.oc_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(_OcStepInfo)]
         L.oc_get_state.argtypes = [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _u8p]
@@ -121,6 +122,7 @@ def ref_lib():
                      "ref_cloth_set_velocity"):
             getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, _f32p]
         L.ref_cloth_add_sphere.argtypes = [C.c_void_p, _f32p, C.c_float, C.c_float]
+        L.ref_cloth_add_capsule.argtypes = [C.c_void_p, _f32p, _f32p, C.c_float, C.c_float]
         L.ref_cloth_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_uint32, C.c_int]
         L.ref_last_iterations.restype = C.c_uint32
         L.ref_cloth_get_state.argtypes = [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _u8p]
@@ -232,6 +234,8 @@ class _Base:
             self.set_type(int(p), 0)
         for (c, r, mu) in scene.spheres:
             self.add_sphere(c, r, mu)
+        for (a, b, r, mu) in getattr(scene, "capsules", ()):
+            self.add_capsule(a, b, r, mu)
         return self
 
 
@@ -273,6 +277,9 @@ class PortCloth(_Base):
 
     def add_sphere(self, center, radius, friction):
         return self.L.oc_add_sphere(self.h, np.asarray(center, np.float32), radius, friction)
+
+    def add_capsule(self, a, b, radius, friction):
+        return self.L.oc_add_capsule(self.h, np.asarray(a, np.float32), np.asarray(b, np.float32), radius, friction)
 
     def set_solver(self, stop_rule=STOP_REFERENCE, tol=0.0, max_iterations=20, dot=DOT_F32):
         self.L.oc_set_solver(self.h, stop_rule, tol, max_iterations, dot)
@@ -359,6 +366,9 @@ class RefCloth(_Base):
 
     def add_sphere(self, center, radius, friction):
         self.L.ref_cloth_add_sphere(self.h, np.asarray(center, np.float32), radius, friction)
+
+    def add_capsule(self, a, b, radius, friction):
+        self.L.ref_cloth_add_capsule(self.h, np.asarray(a, np.float32), np.asarray(b, np.float32), radius, friction)
 
     def step(self, dt, vel_iters=8, pos_iters=2, full=False):
         self.L.ref_cloth_step(self.h, dt, vel_iters, pos_iters, 1 if full else 0)

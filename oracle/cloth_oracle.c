@@ -155,8 +155,12 @@ typedef struct {
     uint32_t id;          /* mouse: the handle oc_create_mouse_force returned */
 } force_t;
 
+enum { SHAPE_SPHERE = 0, SHAPE_CAPSULE = 1 };
+
 typedef struct {
-    v3 center;
+    int kind;
+    v3 center;         /* sphere */
+    v3 a, b;           /* capsule segment, world frame (the body at the origin) */
     float radius, friction;
     v3 fat_lo, fat_hi; /* the shape's proxy in the world broadphase */
 } sphere_t;
@@ -534,6 +538,8 @@ int oc_add_sphere(oc_cloth* c, const float* center, float radius, float friction
 {
     c->spheres = (sphere_t*)realloc(c->spheres, (c->nsphere + 1) * sizeof(sphere_t));
     sphere_t* s = c->spheres + c->nsphere;
+    memset(s, 0, sizeof(*s));
+    s->kind = SHAPE_SPHERE;
     s->center = V(center[0], center[1], center[2]);
     s->radius = radius;
     s->friction = friction;
@@ -541,6 +547,26 @@ int oc_add_sphere(oc_cloth* c, const float* center, float radius, float friction
     v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
     s->fat_lo = vsub(vsub(s->center, r), ext);
     s->fat_hi = vadd(vadd(s->center, r), ext);
+    return (int)c->nsphere++;
+}
+
+/* A static body at the origin with one capsule shape (capsule_shape.h):
+ * segment a-b in the world frame; the proxy is ComputeAABB
+ * (capsule_shape.cpp:130-137) fattened by B3_AABB_EXTENSION. */
+int oc_add_capsule(oc_cloth* c, const float* a, const float* b, float radius, float friction)
+{
+    c->spheres = (sphere_t*)realloc(c->spheres, (c->nsphere + 1) * sizeof(sphere_t));
+    sphere_t* s = c->spheres + c->nsphere;
+    memset(s, 0, sizeof(*s));
+    s->kind = SHAPE_CAPSULE;
+    s->a = V(a[0], a[1], a[2]);
+    s->b = V(b[0], b[1], b[2]);
+    s->radius = radius;
+    s->friction = friction;
+    v3 r = V(radius, radius, radius);
+    v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
+    s->fat_lo = vsub(vsub(vmin(s->a, s->b), r), ext);
+    s->fat_hi = vadd(vadd(vmax(s->a, s->b), r), ext);
     return (int)c->nsphere++;
 }
 
@@ -1240,19 +1266,68 @@ static void contact_update(oc_cloth* c, contact_t* k)
     const sphere_t* sp = c->spheres + k->shape;
     uint32_t i = k->particle;
     float radius = sp->radius + c->radius[i];
-    float rr = radius * radius;
-    v3 d = vsub(c->x[i], sp->center);
-    float dd = vdot(d, d);
-    if (!(dd <= rr)) {
-        k->active = 0;
-        return;
+    v3 Q = c->x[i];
+    v3 normal, point;
+    if (sp->kind == SHAPE_SPHERE) {
+        /* b3SphereShape::TestSphere (sphere_shape.cpp:71-95) */
+        float rr = radius * radius;
+        v3 d = vsub(Q, sp->center);
+        float dd = vdot(d, d);
+        if (!(dd <= rr)) {
+            k->active = 0;
+            return;
+        }
+        float d_len = sqrtf(dd);
+        normal = V(0.0f, 1.0f, 0.0f);
+        if (d_len > kEps) normal = vdiv(d, d_len);
+        point = sp->center;
+    } else {
+        /* b3CapsuleShape::TestSphere (capsule_shape.cpp:186-284) */
+        v3 A = sp->a, B = sp->b;
+        v3 AB = vsub(B, A);
+        float u = vdot(vsub(B, Q), AB);
+        float v = vdot(vsub(Q, A), AB);
+        if (v <= 0.0f || u <= 0.0f) {
+            v3 P = v <= 0.0f ? A : B;
+            v3 d = vsub(Q, P);
+            float dd = vdot(d, d);
+            if (dd > radius * radius) {
+                k->active = 0;
+                return;
+            }
+            normal = V(0.0f, 1.0f, 0.0f);
+            float len = sqrtf(dd);
+            if (len > kEps) normal = vdiv(d, len);
+            point = P;
+        } else {
+            float ss = vdot(AB, AB);
+            v3 P;
+            if (ss < kLinearSlop * kLinearSlop) P = A;
+            else P = vdiv(vadd(vscale(u, A), vscale(v, B)), ss);
+            v3 d = vsub(Q, P);
+            float dd = vdot(d, d);
+            if (dd > radius * radius) {
+                k->active = 0;
+                return;
+            }
+            v3 QA = vsub(A, Q);
+            v3 e = vcross(AB, QA);
+            v3 nn = vcross(AB, e);
+            if (vdot(nn, QA) < 0.0f) nn = vneg(nn);
+            float len = sqrtf(nn.x * nn.x + nn.y * nn.y + nn.z * nn.z); /* b3Vec3::Normalize (vec3.h:93-104) */
+            if (len > kEps) {
+                float s1 = 1.0f / len;
+                nn = V(nn.x * s1, nn.y * s1, nn.z * s1);
+            }
+            normal = vneg(nn);
+            point = P;
+        }
     }
-    float d_len = sqrtf(dd);
-    v3 normal = V(0.0f, 1.0f, 0.0f);
-    if (d_len > kEps) normal = vdiv(d, d_len);
     k->active = 1;
     k->normal1 = vneg(normal);
-    k->local_point2 = vzero();
+    /* body->GetLocalPoint(point) for a static body: the sphere's body sits at
+     * its centre, the capsule's at the origin */
+    k->local_point2 = sp->kind == SHAPE_SPHERE ? vzero() : point;
     k->tangent1 = vperp(k->normal1);
     k->tangent2 = vcross(k->tangent1, k->normal1);
 }
@@ -1347,7 +1422,7 @@ static void solve_contacts(oc_cloth* c, float h, uint32_t vel_iters, uint32_t po
         x->inv_mass = c->type[i] == OC_STATIC ? 0.0f : c->inv_mass[i];
         x->friction = sqrtf(c->friction[i] * sp->friction); /* b3MixFriction */
         x->normal_a = k->normal1;
-        x->center_b = sp->center;
+        x->center_b = sp->kind == SHAPE_SPHERE ? sp->center : k->local_point2;
         x->radius_a = c->radius[i];
         x->radius_b = sp->radius;
         /* InitializeBodyContactConstraints (:54-177) */

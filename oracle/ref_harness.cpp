@@ -119,6 +119,7 @@ struct RefCloth {
     b3Cloth* cloth = nullptr;
     b3World* world = nullptr;
     std::vector<b3SphereShape*> sphere_protos;
+    std::vector<b3CapsuleShape*> capsule_protos;
     // Particles made with b3Cloth::CreateParticle, addressed after the mesh
     // vertices (index vertexCount + k), and mouse forces by id - 1 (null once
     // destroyed).
@@ -375,6 +376,7 @@ void ref_cloth_destroy(void* hp)
     }
     delete h->world;
     for (b3SphereShape* s : h->sphere_protos) delete s;
+    for (b3CapsuleShape* s : h->capsule_protos) delete s;
     delete h;
 }
 
@@ -427,6 +429,28 @@ void ref_cloth_add_sphere(void* hp, const float* center, float radius, float fri
     h->sphere_protos.push_back(sphere);
     b3ShapeDef sd;
     sd.shape = sphere;
+    sd.friction = friction;
+    body->CreateShape(sd);
+}
+
+// A static body at the origin carrying one capsule shape, segment a-b.
+void ref_cloth_add_capsule(void* hp, const float* a, const float* b, float radius, float friction)
+{
+    RefCloth* h = (RefCloth*)hp;
+    if (!h->world) {
+        h->world = new b3World();
+        h->cloth->SetWorld(h->world);
+    }
+    b3BodyDef bd;
+    bd.type = e_staticBody;
+    b3Body* body = h->world->CreateBody(bd);
+    b3CapsuleShape* cap = new b3CapsuleShape();
+    cap->m_centers[0].Set(a[0], a[1], a[2]);
+    cap->m_centers[1].Set(b[0], b[1], b[2]);
+    cap->m_radius = radius;
+    h->capsule_protos.push_back(cap);
+    b3ShapeDef sd;
+    sd.shape = cap;
     sd.friction = friction;
     body->CreateShape(sd);
 }

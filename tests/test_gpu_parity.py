@@ -287,3 +287,24 @@ def test_mouse_drag_per_step(b3g, port):
     assert gpu.n == scene.mesh.vertex_count
     for k in range(10):
         check(100 + k)
+
+
+def test_capsule_contacts_per_step(b3g, port):
+    """A cloth draping over and sliding off a static capsule (the capsule's
+    b3CapsuleShape::TestSphere: end caps and the segment): each step starts
+    the oracle from the GPU's state; contact bookkeeping runs on both sides."""
+    scene = b3g.capsule_scene(32)
+    gpu, ora = _pair(b3g, port, scene)
+    seen_active = 0
+    for step in range(90):
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        seen_active = max(seen_active, o["active_contacts"])
+        assert abs(g["iterations"] - o["iterations"]) <= 1, step
+        assert abs(int(g["active_contacts"]) - int(o["active_contacts"])) <= max(2, o["active_contacts"] // 100), step
+        assert abs(int(g["contacts"]) - int(o["contacts"])) <= max(2, o["contacts"] // 100), step
+        e = rel_err(gpu.state()["x"], ora.state()["x"])
+        assert e <= 1e-4, (step, e)
+    assert seen_active > 20  # the cloth did lie on the capsule

@@ -123,3 +123,25 @@ def test_mouse_drag_matches_reference(maker):
     for _ in range(8):
         assert ref.step(scene.dt)["iterations"] == port.step(scene.dt)["iterations"]
         same()
+
+
+def test_capsule_collider_matches_reference():
+    """A static capsule collider (b3CapsuleShape::TestSphere, ComputeAABB):
+    contacts, positions and velocities bit for bit over the drape and slide."""
+    from bounce_b200.meshes import capsule_scene
+
+    scene = capsule_scene(16)
+    ref = oracle.RefCloth(scene.mesh, scene.cdef).setup(scene)
+    port = oracle.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    active = 0
+    for _ in range(120):
+        assert ref.step(scene.dt)["iterations"] == port.step(scene.dt)["iterations"]
+        sr, sp = ref.state(), port.state()
+        for q in ("x", "v", "dv"):
+            assert np.array_equal(sr[q], sp[q]), q
+        cr, cp = ref.contacts(), port.contacts()
+        assert cr["count"] == cp["count"]
+        assert np.array_equal(cr["active"], cp["active"])
+        assert np.array_equal(cr["impulses"], cp["impulses"])
+        active = max(active, int(cr["active"].sum()))
+    assert active > 10
