@@ -145,3 +145,24 @@ def test_capsule_collider_matches_reference():
         assert np.array_equal(cr["impulses"], cp["impulses"])
         active = max(active, int(cr["active"].sum()))
     assert active > 10
+
+
+def test_particle_edits_match_reference():
+    """Forces, translations, velocities, positions and type changes between
+    steps (particle.cpp, particle.h:205-271), on the sphere scene so that type
+    changes also drop contacts: the restatement follows the reference bit for
+    bit."""
+    import edit_script
+
+    scene = sphere_scene(16)
+    ref = oracle.RefCloth(scene.mesh, scene.cdef).setup(scene)
+    port = oracle.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    for step in range(40):
+        x = ref.state()["x"]
+        edit_script.apply(ref, step, x, gpu=False)
+        edit_script.apply(port, step, x, gpu=False)
+        assert ref.step(scene.dt)["iterations"] == port.step(scene.dt)["iterations"]
+        sr, sp = ref.state(), port.state()
+        for q in ("x", "v", "dv", "type"):
+            assert np.array_equal(sr[q], sp[q]), (step, q)
+        assert ref.contacts()["count"] == port.contacts()["count"]
