@@ -765,6 +765,8 @@ b3g_status relayout(b3g_cloth* c, const ParticleState& s, uint32_t old_extra, st
     }
     c->dev.nsph = old_dev.nsph;
     std::memcpy(c->dev.sph, old_dev.sph, sizeof(old_dev.sph));
+    // the host copy of the masses follows the state (created particles carry their own)
+    for (uint32_t i = 0; i < s.n && i < c->topo.mass.size(); ++i) c->topo.mass[i] = s.mass[i];
     char* base = nullptr;
     if (cudaMalloc(&base, c->arena.size) != cudaSuccess) {
         cudaGetLastError();
@@ -1244,14 +1246,14 @@ b3g_status b3g_cloth_get_info(const b3g_cloth* c, b3g_cloth_info* info)
 
 uint32_t b3g_cloth_vertex_count(const b3g_cloth* c) { return valid(c) ? c->dev.n : 0u; }
 
+// Planes to the caller's xyz buffer: transposed on the device into the
+// staging buffer, then one copy.
 static b3g_status read_planes(b3g_cloth* c, const float* planes, float* out)
 {
     const uint32_t n = c->dev.n;
-    std::vector<float> tmp(3 * (size_t)n);
-    B3G_TRY(cudaMemcpyAsync(tmp.data(), planes, 3 * (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+    B3G_TRY(launch_planes_to_xyz(planes, c->d_stage, n, c->stream));
+    B3G_TRY(cudaMemcpyAsync(out, c->d_stage, 3 * (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
     B3G_TRY(cudaStreamSynchronize(c->stream));
-    for (uint32_t i = 0; i < n; ++i)
-        for (int q = 0; q < 3; ++q) out[3 * i + q] = tmp[(size_t)q * n + i];
     return B3G_OK;
 }
 
@@ -1275,23 +1277,24 @@ b3g_status b3g_cloth_write_state(b3g_cloth* c, const float* x, const float* v, c
     b3g_status s = flush_ops(c);
     if (s != B3G_OK) return s;
     const uint32_t n = c->dev.n;
-    std::vector<float> tmp(3 * (size_t)n);
     const float* srcs[3] = {x, v, mx};
     float* dsts[3] = {c->dev.x, c->dev.v, c->dev.mx};
     for (int k = 0; k < 3; ++k) {
         if (!srcs[k]) continue;
-        for (uint32_t i = 0; i < n; ++i)
-            for (int q = 0; q < 3; ++q) tmp[(size_t)q * n + i] = srcs[k][3 * i + q];
-        B3G_TRY(cudaMemcpyAsync(dsts[k], tmp.data(), 3 * (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
-        B3G_TRY(cudaStreamSynchronize(c->stream));
+        B3G_TRY(cudaMemcpyAsync(c->d_stage, srcs[k], 3 * (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
+        B3G_TRY(launch_xyz_to_planes(c->d_stage, dsts[k], n, c->stream));
     }
+    B3G_TRY(cudaStreamSynchronize(c->stream));
     return B3G_OK;
 }
 
 b3g_status b3g_cloth_read_masses(const b3g_cloth* c, float* m)
 {
     if (!valid(c) || !m) return B3G_ERR_INVALID_ARGUMENT;
-    std::memcpy(m, c->topo.mass.data(), c->topo.mass.size() * 4);
+    cudaSetDevice(c->device);
+    // the device copy: created particles carry their own masses
+    B3G_TRY(cudaMemcpyAsync(m, c->dev.mass, (size_t)c->dev.n * 4, cudaMemcpyDeviceToHost, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
     return B3G_OK;
 }
 

@@ -149,6 +149,9 @@ cudaError_t launch_cg_iteration(const ClothDev& c, int dot, cudaGraphConditional
 // The three kernels of one CG iteration, one at a time (profiling).
 cudaError_t launch_cg_part(const ClothDev& c, int dot, int part, cudaStream_t st);
 cudaError_t launch_finalize(const ClothDev& c, cudaStream_t st);
+// xyz per particle <-> three planes (host transfers go through the staging buffer)
+cudaError_t launch_planes_to_xyz(const float* planes, float* xyz, uint32_t n, cudaStream_t st);
+cudaError_t launch_xyz_to_planes(const float* xyz, float* planes, uint32_t n, cudaStream_t st);
 cudaError_t launch_contact_position(const ClothDev& c, uint32_t it, cudaStream_t st);
 cudaError_t launch_post(const ClothDev& c, cudaStream_t st);
 

@@ -1069,6 +1069,26 @@ __global__ void k_add_vectors(ClothDev c, float* dst, const float* src, int only
     st3(dst, c.n, i, ld3(dst, c.n, i) + a);
 }
 
+// Three planes of n floats to n xyz triples, and back (host buffers hold
+// xyz per particle; the device keeps planes).
+__global__ void k_planes_to_xyz(const float* planes, float* xyz, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    xyz[3 * i] = planes[i];
+    xyz[3 * i + 1] = planes[n + i];
+    xyz[3 * i + 2] = planes[2 * n + i];
+}
+
+__global__ void k_xyz_to_planes(const float* xyz, float* planes, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    planes[i] = xyz[3 * i];
+    planes[n + i] = xyz[3 * i + 1];
+    planes[2 * n + i] = xyz[3 * i + 2];
+}
+
 __global__ void k_clear_contacts(ClothDev c)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1284,6 +1304,22 @@ cudaError_t launch_set_types(const ClothDev& c, const uint8_t* types, cudaStream
 cudaError_t launch_add_vectors(const ClothDev& c, float* dst, const float* src, int only_dynamic, cudaStream_t st)
 {
     k_add_vectors<<<blocks_for(c.n, 256), 256, 0, st>>>(c, dst, src, only_dynamic);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_planes_to_xyz(const float* planes, float* xyz, uint32_t n, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    k_planes_to_xyz<<<blocks_for(n, 256), 256, 0, st>>>(planes, xyz, n);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_xyz_to_planes(const float* xyz, float* planes, uint32_t n, cudaStream_t st)
+{
+    if (!n) return cudaSuccess;
+    k_xyz_to_planes<<<blocks_for(n, 256), 256, 0, st>>>(xyz, planes, n);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -333,3 +333,23 @@ def test_particle_edits_per_step(b3g, port):
             assert gpu.particle(vtx).get_type() == os_["type"][vtx], (step, vtx)
         assert rel_err(gs["x"], os_["x"]) <= 1e-4, step
         assert rel_err(gs["v"], os_["v"]) <= 1e-4, step
+
+
+def test_created_dynamic_particle_mass_and_fall(b3g):
+    """A created dynamic particle (mass given) reports its own mass, falls
+    under gravity like b3Particle integration, and state transfers through
+    the xyz host buffers round-trip exactly."""
+    scene = b3g.plain_scene(16)
+    gpu = b3g.Cloth(scene.mesh, scene.cdef).setup(scene)
+    i = gpu.create_particle((0.0, 1.0, 0.0), mass=0.25, radius=scene.cdef.thickness, friction=scene.cdef.friction)
+    assert gpu.particle(i).get_mass() == np.float32(0.25)
+    assert gpu.masses()[i] == np.float32(0.25)
+    y0 = gpu.particle(i).get_position()[1]
+    for _ in range(5):
+        gpu.step(scene.dt)
+    assert gpu.particle(i).get_position()[1] < y0
+    st = gpu.state()
+    gpu.write_state(x=st["x"], v=st["v"], dv=st["dv"])
+    st2 = gpu.state()
+    for q in ("x", "v", "dv"):
+        assert np.array_equal(st[q], st2[q]), q
