@@ -289,9 +289,17 @@ b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t coun
     if (!(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(b->device);
     cudaStream_t st = b->stream;
+    // queued particle edits go first, on the batch's stream; earlier work on
+    // the cloths' own streams is waited for once per distinct stream (a
+    // server's cloths share one)
+    std::vector<cudaStream_t> waited;
     for (uint32_t k = 0; k < count; ++k) {
-        if ((s = flush_ops_on(cloths[k], st)) != B3G_OK) return s;
-        B3G_TRY(cudaStreamSynchronize(cloths[k]->stream));
+        if (!cloths[k]->pending.empty() && (s = flush_ops_on(cloths[k], st)) != B3G_OK) return s;
+        cudaStream_t cs = cloths[k]->stream;
+        if (cs && cs != st && std::find(waited.begin(), waited.end(), cs) == waited.end()) {
+            B3G_TRY(cudaStreamSynchronize(cs));
+            waited.push_back(cs);
+        }
     }
     B3G_TRY(cudaStreamSynchronize(st));
     if (!use_graph) {

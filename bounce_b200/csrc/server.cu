@@ -164,24 +164,31 @@ b3g_status activate(b3g_server* s, Request* r)
     return B3G_OK;
 }
 
-void retire(b3g_server* s, Request* r, double now)
+// Finished requests: every cloth's positions are transposed on the device
+// and copied out on the server's stream, one wait for all of them, then the
+// arenas go back to the pool.
+void retire(b3g_server* s, const std::vector<Request*>& done, double now)
 {
-    b3g_cloth* c = r->cloth;
-    const uint32_t n = c->dev.n;
-    std::vector<float> planes(3 * (size_t)n);
-    cudaMemcpyAsync(planes.data(), c->dev.x, 3 * (size_t)n * 4, cudaMemcpyDeviceToHost, s->stream);
+    if (done.empty()) return;
+    for (Request* r : done) {
+        b3g_cloth* c = r->cloth;
+        const uint32_t n = c->dev.n;
+        r->result.resize(3 * (size_t)n);
+        launch_planes_to_xyz(c->dev.x, c->d_stage, n, s->stream);
+        cudaMemcpyAsync(r->result.data(), c->d_stage, 3 * (size_t)n * 4, cudaMemcpyDeviceToHost, s->stream);
+    }
     cudaStreamSynchronize(s->stream);
-    r->result.resize(3 * (size_t)n);
-    for (uint32_t i = 0; i < n; ++i)
-        for (int q = 0; q < 3; ++q) r->result[3 * i + q] = planes[(size_t)q * n + i];
-    cudaFreeAsync(r->arena, s->stream);
-    r->arena = nullptr;
-    destroy_cloth(c);
-    r->cloth = nullptr;
-    s->used -= r->bytes;
-    r->finished = now;
-    r->state = R_DONE;
-    s->completed += 1;
+    for (Request* r : done) {
+        cudaFreeAsync(r->arena, s->stream);
+        r->arena = nullptr;
+        r->cloth->stream = nullptr;  // the server's stream, waited for above
+        destroy_cloth(r->cloth);
+        r->cloth = nullptr;
+        s->used -= r->bytes;
+        r->finished = now;
+        r->state = R_DONE;
+        s->completed += 1;
+    }
 }
 
 }  // namespace
@@ -351,16 +358,17 @@ b3g_status b3g_server_tick(b3g_server* s, double now, b3g_server_tick_info* info
         s->steps += cl.size();
         s->busy_ms += bs.step_ms;
         s->ticks += 1;
-        std::vector<Request*> still;
+        std::vector<Request*> still, done;
         for (Request* r : s->active) {
             r->steps_done += 1;
             if (r->steps_done >= r->steps_total) {
-                retire(s, r, now);
+                done.push_back(r);
                 ti.completed += 1;
             } else {
                 still.push_back(r);
             }
         }
+        retire(s, done, now);
         s->active.swap(still);
     }
     ti.active = (uint32_t)s->active.size();
