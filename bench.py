@@ -195,9 +195,10 @@ def run_ours(args, rank, world):
         torch.distributed.barrier()
 
     # end to end through the public API with host buffers: per step the
-    # external forces go host->device, the positions come back device->host
-    forces = np.zeros((n, 3), np.float32)
-    pos = np.zeros((n, 3), np.float32)
+    # external forces go host->device, the positions come back device->host,
+    # both through page-locked host buffers
+    forces = torch.zeros((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    pos = torch.zeros((n, 3), dtype=torch.float32, pin_memory=True).numpy()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         cloth.apply_forces(forces)

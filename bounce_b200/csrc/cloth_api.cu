@@ -1012,6 +1012,8 @@ b3g_status b3g_cloth_set_types(b3g_cloth* c, const uint8_t* types)
     b3g_status s = flush_ops(c);
     if (s != B3G_OK) return s;
     B3G_TRY(cudaMemcpyAsync(c->d_stage_u8, types, c->dev.n, cudaMemcpyHostToDevice, c->stream));
+    // the caller's buffer is free on return, page-locked or not
+    B3G_TRY(cudaStreamSynchronize(c->stream));
     B3G_TRY(launch_set_types(c->dev, c->d_stage_u8, c->stream));
     return B3G_OK;
 }
@@ -1023,6 +1025,9 @@ static b3g_status add_array(b3g_cloth* c, float* dst, const float* src, int only
     b3g_status s = flush_ops(c);
     if (s != B3G_OK) return s;
     B3G_TRY(cudaMemcpyAsync(c->d_stage, src, 3 * (size_t)c->dev.n * 4, cudaMemcpyHostToDevice, c->stream));
+    // the caller's buffer is free on return: a copy from page-locked memory
+    // runs asynchronously, one from pageable memory is only staged
+    B3G_TRY(cudaStreamSynchronize(c->stream));
     B3G_TRY(launch_add_vectors(c->dev, dst, c->d_stage, only_dynamic, c->stream));
     return B3G_OK;
 }
