@@ -170,3 +170,79 @@ def batch_scenes(count: int = 512, seed: int = 3, side_lo: int = 16, side_hi: in
         pins = np.arange(side, dtype=np.uint32)
         out.append(Scene(f"batch{k}_{side}", mesh, cdef, pins, steps=steps))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Soft bodies
+
+@dataclass
+class SoftBodyDef:
+    """b3SoftBodyDef (include/bounce/softbody/softbody.h:64-99); its
+    defaults are the reference's."""
+
+    density: float = 0.1
+    E: float = 100.0
+    nu: float = 0.3
+    c_yield: float = float(np.finfo(np.float32).max)
+    c_creep: float = 0.0
+    c_max: float = 0.0
+
+
+@dataclass
+class SoftBodyScene:
+    vertices: np.ndarray            # (n, 3) float32
+    tets: np.ndarray                # (t, 4) uint32
+    sdef: SoftBodyDef
+    mass_damping: np.ndarray        # (n,) float32, b3SoftBodyNode::SetMassDamping
+    static_nodes: np.ndarray        # node ids set to e_staticSoftBodyNode
+    gravity: tuple = (0.0, -9.8, 0.0)
+    dt: float = 1.0 / 60.0
+    velocity_iterations: int = 8
+    position_iterations: int = 2
+    steps: int = 100
+
+
+def block_softbody_mesh(w: int, h: int, d: int, spacing: float = 1.0) -> tuple:
+    """The tetrahedral block of b3BlockSoftBodyMesh<W, H, D>
+    (include/bounce/softbody/block_softbody_mesh.h:24-120): (W+1)(H+1)(D+1)
+    vertices on a grid of the given spacing centred at the origin, vertex
+    (x, y, z) at index (x (H+1) + y)(D+1) + z, and 5 tetrahedra per cell in
+    the two mirrored splits the template alternates by the cell parity."""
+    xs, ys, zs = np.meshgrid(np.arange(w + 1), np.arange(h + 1), np.arange(d + 1), indexing="ij")
+    verts = np.stack([xs, ys, zs], axis=-1).reshape(-1, 3).astype(np.float32)
+    verts = (verts + np.array([-0.5 * w, -0.5 * h, -0.5 * d], np.float32)) * np.float32(spacing)
+
+    def vid(x, y, z):
+        return (x * (h + 1) + y) * (d + 1) + z
+
+    tets = []
+    for x in range(w):
+        for y in range(h):
+            for z in range(d):
+                c0 = vid(x, y, z)
+                c1 = c0 + 1
+                c3 = vid(x + 1, y, z)
+                c2 = c3 + 1
+                c7 = vid(x + 1, y + 1, z)
+                c6 = c7 + 1
+                c4 = vid(x, y + 1, z)
+                c5 = c4 + 1
+                if (x + y + z) % 2 == 1:
+                    tets += [(c2, c1, c6, c3), (c6, c3, c4, c7), (c4, c1, c6, c5), (c3, c1, c4, c0), (c6, c1, c4, c3)]
+                else:
+                    tets += [(c0, c2, c5, c1), (c7, c2, c0, c3), (c5, c2, c7, c6), (c7, c0, c5, c4), (c0, c2, c7, c5)]
+    return verts, np.asarray(tets, np.uint32)
+
+
+def pinned_block_scene(w: int = 4, h: int = 4, d: int = 4, spacing: float = 1.0, steps: int = 100) -> SoftBodyScene:
+    """A block hanging from one node, with the material of the reference's
+    pinned soft body (examples/testbed/tests/pinned_softbody.h:27-59):
+    density 0.2, E 1000, nu 0.33, yield 0.1, creep 0.5, max plastic strain 1,
+    mass damping 0.2 on every node, the first node of largest height static,
+    gravity (0, -9.8, 0).  The block stands in for that scene's quickhull
+    sphere mesh."""
+    verts, tets = block_softbody_mesh(w, h, d, spacing)
+    sdef = SoftBodyDef(density=0.2, E=1000.0, nu=0.33, c_yield=0.1, c_creep=0.5, c_max=1.0)
+    pin = int(np.argmax(verts[:, 1]))  # the first index of the largest y
+    return SoftBodyScene(verts, tets, sdef, np.full(len(verts), 0.2, np.float32), np.array([pin], np.uint32),
+                         steps=steps)

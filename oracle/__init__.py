@@ -443,3 +443,242 @@ def solve_f64(system, tol=1e-12, max_iterations=100000):
     it = L.oc_solve_f64(n, system["rowptr"], system["cols"], system["vals"], system["b"], system["S"],
                         system["x0"], tol, max_iterations, x)
     return x.reshape(-1, 3), int(it)
+
+
+# ---------------------------------------------------------------------------
+# Soft body: softbody_oracle.c (PortSoftBody) and the reference's b3SoftBody
+# through ref_softbody.cpp (RefSoftBody), with one interface.
+
+class _OsStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("delta0", C.c_double), ("delta", C.c_double),
+                ("b_delta", C.c_double)]
+
+
+_sb_port_ready = False
+_sb_ref_ready = False
+
+
+def _sb_port():
+    global _sb_port_ready
+    L = port_lib()
+    if not _sb_port_ready:
+        L.os_create.restype = C.c_void_p
+        L.os_create.argtypes = [C.c_uint32, _f32p, C.c_uint32, _u32p] + [C.c_float] * 6
+        L.os_destroy.argtypes = [C.c_void_p]
+        L.os_node_count.restype = C.c_uint32
+        L.os_node_count.argtypes = [C.c_void_p]
+        L.os_set_type.argtypes = [C.c_void_p, C.c_uint32, C.c_int]
+        L.os_set_mass_damping.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.os_set_gravity.argtypes = [C.c_void_p, _f32p]
+        L.os_apply_force.argtypes = [C.c_void_p, C.c_uint32, _f32p]
+        L.os_set_velocity.argtypes = [C.c_void_p, C.c_uint32, _f32p]
+        L.os_set_solver.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_uint32, C.c_int]
+        L.os_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(_OsStats)]
+        L.os_get_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.os_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.os_get_masses.argtypes = [C.c_void_p, _f32p]
+        L.os_get_elements.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.os_set_elements.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.os_get_element_data.argtypes = [C.c_void_p, C.c_uint32, _f32p, _f32p, _f32p, _f32p]
+        L.os_energy.restype = C.c_float
+        L.os_energy.argtypes = [C.c_void_p]
+        L.os_system.restype = C.c_uint32
+        L.os_system.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_void_p]
+        _sb_port_ready = True
+    return L
+
+
+def _sb_ref():
+    global _sb_ref_ready
+    L = ref_lib()
+    if not _sb_ref_ready:
+        L.ref_softbody_create.restype = C.c_void_p
+        L.ref_softbody_create.argtypes = [_f32p, C.c_uint32, _u32p, C.c_uint32, _f32p]
+        L.ref_softbody_destroy.argtypes = [C.c_void_p]
+        L.ref_softbody_set_type.argtypes = [C.c_void_p, C.c_uint32, C.c_int]
+        L.ref_softbody_set_mass_damping.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.ref_softbody_set_gravity.argtypes = [C.c_void_p, _f32p]
+        L.ref_softbody_apply_force.argtypes = [C.c_void_p, C.c_uint32, _f32p]
+        L.ref_softbody_set_velocity.argtypes = [C.c_void_p, C.c_uint32, _f32p]
+        L.ref_softbody_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_uint32]
+        L.ref_softbody_last_iterations.restype = C.c_uint32
+        L.ref_softbody_get_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_softbody_get_masses.argtypes = [C.c_void_p, _f32p]
+        L.ref_softbody_get_elements.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_softbody_get_element_data.argtypes = [C.c_void_p, C.c_uint32, _f32p, _f32p, _f32p, _f32p]
+        L.ref_softbody_energy.restype = C.c_float
+        L.ref_softbody_energy.argtypes = [C.c_void_p]
+        _sb_ref_ready = True
+    return L
+
+
+def _addr(a):
+    return None if a is None else a.ctypes.data
+
+
+class _SoftBase:
+    """Common soft-body front-end; `scene` is a bounce_b200.SoftBodyScene-like
+    object (vertices (n,3) float32, tets (t,4) uint32, def fields, node types,
+    mass damping, gravity)."""
+
+    def setup(self, scene):
+        self.set_gravity(scene.gravity)
+        for i, d in enumerate(scene.mass_damping):
+            if d != 0.0:
+                self.set_mass_damping(i, float(d))
+        for i in scene.static_nodes:
+            self.set_type(int(i), 0)
+        return self
+
+    def state(self):
+        x = np.zeros((self.n, 3), np.float32)
+        v = np.zeros((self.n, 3), np.float32)
+        self._get_state(x, v)
+        return {"x": x, "v": v}
+
+    def elements(self):
+        q = np.zeros((self.t, 4), np.float32)
+        e = np.zeros((self.t, 6), np.float32)
+        self._get_elements(q, e)
+        return {"q": q, "eps": e}
+
+    def element_data(self, e):
+        K = np.zeros(144, np.float32)
+        invE = np.zeros(9, np.float32)
+        B = np.zeros(72, np.float32)
+        P = np.zeros(72, np.float32)
+        self._get_element_data(e, K, invE, B, P)
+        return {"K": K.reshape(16, 3, 3), "invE": invE.reshape(3, 3), "B": B, "P": P}
+
+
+class PortSoftBody(_SoftBase):
+    def __init__(self, vertices, tets, density, E, nu, c_yield, c_creep, c_max):
+        self.L = _sb_port()
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1)
+        t = np.ascontiguousarray(tets, np.uint32).reshape(-1)
+        self.n, self.t = v.size // 3, t.size // 4
+        self.h = self.L.os_create(self.n, v, self.t, t, density, E, nu, c_yield, c_creep, c_max)
+        self.last = _OsStats()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.os_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_type(self, i, type_):
+        self.L.os_set_type(self.h, i, type_)
+
+    def set_mass_damping(self, i, d):
+        self.L.os_set_mass_damping(self.h, i, d)
+
+    def set_gravity(self, g):
+        self.L.os_set_gravity(self.h, np.asarray(g, np.float32))
+
+    def apply_force(self, i, f):
+        self.L.os_apply_force(self.h, i, np.asarray(f, np.float32))
+
+    def set_velocity(self, i, v):
+        self.L.os_set_velocity(self.h, i, np.asarray(v, np.float32))
+
+    def set_solver(self, stop_rule=STOP_REFERENCE, tol=0.0, max_iterations=20, dot=DOT_F32):
+        self.L.os_set_solver(self.h, stop_rule, tol, max_iterations, dot)
+
+    def step(self, dt, vel_iters=8, pos_iters=2):
+        self.L.os_step(self.h, dt, vel_iters, pos_iters, C.byref(self.last))
+        s = self.last
+        return {"iterations": s.iterations, "delta0": s.delta0, "delta": s.delta, "b_delta": s.b_delta}
+
+    def _get_state(self, x, v):
+        self.L.os_get_state(self.h, _addr(x), _addr(v))
+
+    def set_state(self, x=None, v=None):
+        xs = None if x is None else np.ascontiguousarray(x, np.float32)
+        vs = None if v is None else np.ascontiguousarray(v, np.float32)
+        self.L.os_set_state(self.h, _addr(xs), _addr(vs))
+
+    def _get_elements(self, q, e):
+        self.L.os_get_elements(self.h, _addr(q), _addr(e))
+
+    def set_elements(self, q=None, eps=None):
+        qs = None if q is None else np.ascontiguousarray(q, np.float32)
+        es = None if eps is None else np.ascontiguousarray(eps, np.float32)
+        self.L.os_set_elements(self.h, _addr(qs), _addr(es))
+
+    def _get_element_data(self, e, K, invE, B, P):
+        self.L.os_get_element_data(self.h, e, K, invE, B, P)
+
+    def masses(self):
+        m = np.zeros(self.n, np.float32)
+        self.L.os_get_masses(self.h, m)
+        return m
+
+    def energy(self):
+        return float(self.L.os_energy(self.h))
+
+    def system(self, dt):
+        """A (rows in the reference's list order), b and S of one force solve
+        from the current state; the state is left unchanged."""
+        need = self.L.os_system(self.h, dt, 0, None, None, None, None, None)
+        rowptr = np.zeros(self.n + 1, np.uint32)
+        cols = np.zeros(need, np.uint32)
+        vals = np.zeros(9 * need, np.float32)
+        b = np.zeros(3 * self.n, np.float32)
+        S = np.zeros(self.n, np.float32)
+        self.L.os_system(self.h, dt, need, _addr(rowptr), _addr(cols), _addr(vals), _addr(b), _addr(S))
+        return {"rowptr": rowptr, "cols": cols, "vals": vals, "b": b, "S": S}
+
+
+class RefSoftBody(_SoftBase):
+    def __init__(self, vertices, tets, density, E, nu, c_yield, c_creep, c_max):
+        self.L = _sb_ref()
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1)
+        t = np.ascontiguousarray(tets, np.uint32).reshape(-1)
+        self.n, self.t = v.size // 3, t.size // 4
+        d = np.array([density, E, nu, c_yield, c_creep, c_max], np.float32)
+        self.h = self.L.ref_softbody_create(v, self.n, t, self.t, d)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ref_softbody_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_type(self, i, type_):
+        self.L.ref_softbody_set_type(self.h, i, type_)
+
+    def set_mass_damping(self, i, d):
+        self.L.ref_softbody_set_mass_damping(self.h, i, d)
+
+    def set_gravity(self, g):
+        self.L.ref_softbody_set_gravity(self.h, np.asarray(g, np.float32))
+
+    def apply_force(self, i, f):
+        self.L.ref_softbody_apply_force(self.h, i, np.asarray(f, np.float32))
+
+    def set_velocity(self, i, v):
+        self.L.ref_softbody_set_velocity(self.h, i, np.asarray(v, np.float32))
+
+    def step(self, dt, vel_iters=8, pos_iters=2):
+        self.L.ref_softbody_step(self.h, dt, vel_iters, pos_iters)
+        return {"iterations": int(self.L.ref_softbody_last_iterations())}
+
+    def _get_state(self, x, v):
+        self.L.ref_softbody_get_state(self.h, _addr(x), _addr(v))
+
+    def _get_elements(self, q, e):
+        self.L.ref_softbody_get_elements(self.h, _addr(q), _addr(e))
+
+    def _get_element_data(self, e, K, invE, B, P):
+        self.L.ref_softbody_get_element_data(self.h, e, K, invE, B, P)
+
+    def masses(self):
+        m = np.zeros(self.n, np.float32)
+        self.L.ref_softbody_get_masses(self.h, m)
+        return m
+
+    def energy(self):
+        return float(self.L.ref_softbody_energy(self.h))

@@ -18,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
-from bounce_b200.meshes import plain_scene, sphere_scene  # noqa: E402
+from bounce_b200.meshes import pinned_block_scene, plain_scene, sphere_scene  # noqa: E402
 
 
 def trajectory(scene, steps, keep):
@@ -58,14 +58,52 @@ def system(scene):
     return out
 
 
+def softbody(w, h, d, spacing, steps, keep):
+    """The pinned block with node 3 kinematic (moving at 0.1 m/s along x) and
+    a force pulse on node 10 every 7 steps: states, element rotations and
+    plastic strains at the kept steps, and the element data."""
+    scene = pinned_block_scene(w, h, d, spacing)
+    sd = scene.sdef
+    args = (scene.vertices, scene.tets, sd.density, sd.E, sd.nu, sd.c_yield, sd.c_creep, sd.c_max)
+    ref = oracle.RefSoftBody(*args).setup(scene)
+    kin, kin_v, fnode, fvec, fper = 3, np.array([0.1, 0.0, 0.0], np.float32), 10, np.array([0.0, 50.0, 3.0], np.float32), 7
+    ref.set_type(kin, 1)
+    ref.set_velocity(kin, kin_v)
+    out = {"vertices": scene.vertices, "tets": scene.tets,
+           "def": np.array([sd.density, sd.E, sd.nu, sd.c_yield, sd.c_creep, sd.c_max], np.float32),
+           "mass_damping": scene.mass_damping, "static": scene.static_nodes, "dt": np.float32(scene.dt),
+           "gravity": np.asarray(scene.gravity, np.float32), "kinematic": np.uint32(kin), "kinematic_v": kin_v,
+           "force_node": np.uint32(fnode), "force": fvec, "force_period": np.uint32(fper),
+           "mass": ref.masses()}
+    for e in range(0, ref.t, max(1, ref.t // 8)):
+        ed = ref.element_data(e)
+        for k, v in ed.items():
+            out[f"el{e}_{k}"] = v
+    iters = []
+    for k in range(1, steps + 1):
+        if (k - 1) % fper == 0:
+            ref.apply_force(fnode, fvec)
+        iters.append(ref.step(scene.dt)["iterations"])
+        if k in keep:
+            st, el = ref.state(), ref.elements()
+            out[f"x_{k}"], out[f"v_{k}"] = st["x"], st["v"]
+            out[f"q_{k}"], out[f"eps_{k}"] = el["q"], el["eps"]
+    out["iterations"] = np.asarray(iters, np.uint32)
+    return out
+
+
 def main():
     oracle.build(port=True, ref=True)
     files = {
+        "softbody_block_ref.npz": softbody(5, 3, 4, 0.5, 120, {1, 40, 80, 120}),
         "plain32_ref.npz": trajectory(plain_scene(32, seed=1), 30, {1, 10, 30}),
         "sphere32_ref.npz": trajectory(sphere_scene(32, seed=2), 40, {1, 20, 30, 40}),
         "system16_bend_ref.npz": system(sphere_scene(16, seed=4)),
     }
+    only = set(sys.argv[1:])
     for name, data in files.items():
+        if only and name not in only:
+            continue
         np.savez_compressed(os.path.join(HERE, name), **data)
         print(name, os.path.getsize(os.path.join(HERE, name)), "bytes")
 

@@ -1,0 +1,82 @@
+"""The soft body restatement (oracle/softbody_oracle.c) against the reference.
+
+Against the golden fixture the reference produced (tests/golden/gen_golden.py,
+needs no reference tree) and, where the reference library is built here,
+against the live b3SoftBody: masses, element matrices, states, element
+rotations and plastic strains bit for bit, CG iterations equal.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from bounce_b200.meshes import SoftBodyDef, SoftBodyScene, pinned_block_scene
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "softbody_block_ref.npz")
+
+
+def _golden_scene(d):
+    a = [float(x) for x in d["def"]]
+    sdef = SoftBodyDef(*a)
+    return SoftBodyScene(d["vertices"], d["tets"], sdef, d["mass_damping"], d["static"],
+                         gravity=tuple(float(g) for g in d["gravity"]), dt=float(d["dt"]))
+
+
+def _make(cls, scene):
+    s = scene.sdef
+    return cls(scene.vertices, scene.tets, s.density, s.E, s.nu, s.c_yield, s.c_creep, s.c_max).setup(scene)
+
+
+def test_softbody_oracle_matches_golden(port):
+    d = np.load(GOLDEN)
+    scene = _golden_scene(d)
+    b = _make(port.PortSoftBody, scene)
+    assert np.array_equal(b.masses(), d["mass"])
+    for key in d.files:
+        if key.startswith("el") and key.endswith("_K"):
+            e = int(key[2:-2])
+            ed = b.element_data(e)
+            for k in ("K", "invE", "B", "P"):
+                assert np.array_equal(ed[k], d[f"el{e}_{k}"]), (e, k)
+    b.set_type(int(d["kinematic"]), 1)
+    b.set_velocity(int(d["kinematic"]), d["kinematic_v"])
+    per = int(d["force_period"])
+    for k in range(1, len(d["iterations"]) + 1):
+        if (k - 1) % per == 0:
+            b.apply_force(int(d["force_node"]), d["force"])
+        it = b.step(scene.dt)["iterations"]
+        assert it == d["iterations"][k - 1], (k, it)
+        if f"x_{k}" in d:
+            st, el = b.state(), b.elements()
+            assert np.array_equal(st["x"], d[f"x_{k}"]), k
+            assert np.array_equal(st["v"], d[f"v_{k}"]), k
+            assert np.array_equal(el["q"], d[f"q_{k}"]), k
+            assert np.array_equal(el["eps"], d[f"eps_{k}"]), k
+    # the plastic flow and the rotations were exercised
+    assert np.abs(d["eps_120"]).max() > 1e-2
+    assert d["q_120"][:, 3].min() < 0.999
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("dims", [(2, 2, 2), (3, 4, 2)])
+def test_softbody_oracle_matches_live_reference(dims):
+    scene = pinned_block_scene(*dims, spacing=0.75)
+    port = _make(oracle.PortSoftBody, scene)
+    ref = _make(oracle.RefSoftBody, scene)
+    for e in range(port.t):
+        a, b = port.element_data(e), ref.element_data(e)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (e, k)
+    for k in range(40):
+        if k % 5 == 0:
+            for o in (port, ref):
+                o.apply_force(1, [2.0, 30.0, -1.0])
+        a = port.step(scene.dt)
+        b = ref.step(scene.dt)
+        assert a["iterations"] == b["iterations"]
+        sa, sb = port.state(), ref.state()
+        assert np.array_equal(sa["x"], sb["x"]) and np.array_equal(sa["v"], sb["v"]), k
+        ea, eb = port.elements(), ref.elements()
+        assert np.array_equal(ea["q"], eb["q"]) and np.array_equal(ea["eps"], eb["eps"]), k
+    assert port.energy() == ref.energy()
