@@ -20,7 +20,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from .meshes import (DYNAMIC, KINEMATIC, STATIC, ClothDef, Mesh, Scene, batch_scenes, capsule_scene, grid_mesh,  # noqa: F401
-                     plain_scene, sewn_scene, sphere_scene, stiff_scene)
+                     plain_scene, sewn_scene, sphere_scene, stiff_scene, SoftBodyDef, SoftBodyScene,
+                     block_softbody_mesh, pinned_block_scene)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 # B3G_LIBRARY: another build of libb3g.so to load instead of the in-tree one
@@ -53,6 +54,11 @@ class ClothDefC(C.Structure):
 
 class SolverOptsC(C.Structure):
     _fields_ = [("stop_rule", C.c_int), ("tolerance", C.c_float), ("max_iterations", C.c_uint32), ("dot", C.c_int)]
+
+
+class SoftBodyDefC(C.Structure):
+    _fields_ = [("density", C.c_float), ("E", C.c_float), ("nu", C.c_float), ("c_yield", C.c_float),
+                ("c_creep", C.c_float), ("c_max", C.c_float)]
 
 
 class StepStatsC(C.Structure):
@@ -185,6 +191,23 @@ def lib() -> C.CDLL:
             "b3g_server_stats": [vp, C.POINTER(ServerStatsC)],
             "b3g_mpcg_solve_noalloc": [u32, vp, vp, vp, vp, vp, vp, C.POINTER(SolverOptsC), vp, C.POINTER(u32),
                                        C.POINTER(StepStatsC), vp],
+            "b3g_softbody_create": [u32, vp, u32, vp, C.POINTER(SoftBodyDefC), i32, C.POINTER(vp)],
+            "b3g_softbody_destroy": [vp],
+            "b3g_softbody_set_gravity": [vp, vp],
+            "b3g_softbody_set_node_type": [vp, u32, i32],
+            "b3g_softbody_set_mass_damping": [vp, u32, f32],
+            "b3g_softbody_apply_force": [vp, u32, vp],
+            "b3g_softbody_set_velocity": [vp, u32, vp],
+            "b3g_softbody_set_position": [vp, u32, vp],
+            "b3g_softbody_set_solver": [vp, C.POINTER(SolverOptsC)],
+            "b3g_softbody_step": [vp, f32, u32, u32, C.POINTER(StepStatsC)],
+            "b3g_softbody_read_state": [vp, vp, vp],
+            "b3g_softbody_write_state": [vp, vp, vp],
+            "b3g_softbody_read_elements": [vp, vp, vp],
+            "b3g_softbody_write_elements": [vp, vp, vp],
+            "b3g_softbody_read_masses": [vp, vp],
+            "b3g_softbody_energy": [vp, C.POINTER(f32)],
+            "b3g_softbody_export_system": [vp, f32, u32, vp, vp, vp, vp, vp, C.POINTER(u32)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -192,6 +215,9 @@ def lib() -> C.CDLL:
             fn.restype = C.c_int
         L.b3g_cloth_vertex_count.argtypes = [vp]
         L.b3g_cloth_vertex_count.restype = u32
+        for name in ("b3g_softbody_node_count", "b3g_softbody_element_count"):
+            getattr(L, name).argtypes = [vp]
+            getattr(L, name).restype = u32
         L.b3g_status_string.argtypes = [C.c_int]
         L.b3g_status_string.restype = C.c_char_p
         L.b3g_kernel_launch_count.argtypes = []
@@ -403,9 +429,11 @@ class Cloth:
         out["iterations"] = self.stats.iterations
         return out
 
-    def set_cg_strategy(self, persistent: bool) -> None:
-        """False: per-iteration launches in a graph loop; True: one persistent cooperative launch."""
-        check(lib().b3g_cloth_set_cg_strategy(self.h, 1 if persistent else 0), "set_cg_strategy")
+    def set_cg_strategy(self, persistent, fused: bool = False) -> None:
+        """False: per-iteration launches in a graph loop; True: one persistent
+        cooperative launch (fused: one grid reduction per iteration)."""
+        code = 0 if not persistent else 2 if fused else 1
+        check(lib().b3g_cloth_set_cg_strategy(self.h, code), "set_cg_strategy")
 
     def info(self) -> dict:
         i = ClothInfoC()
@@ -624,3 +652,129 @@ class Server:
 
 def kernel_launch_count() -> int:
     return int(lib().b3g_kernel_launch_count())
+
+
+class SoftBody:
+    """A b3SoftBody on the GPU (b3g_softbody_*): tetrahedral corotated FEM
+    with plasticity and the reference's MPCG, stepped without a world."""
+
+    def __init__(self, vertices, tets, sdef, device: int = 0):
+        L = lib()
+        self._v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        self._t = np.ascontiguousarray(tets, np.uint32).reshape(-1, 4)
+        d = SoftBodyDefC(sdef.density, sdef.E, sdef.nu, sdef.c_yield, sdef.c_creep, sdef.c_max)
+        h = C.c_void_p()
+        check(L.b3g_softbody_create(len(self._v), _ptr(self._v), len(self._t), _ptr(self._t), C.byref(d), device,
+                                    C.byref(h)), "b3g_softbody_create")
+        self.h = h.value
+        self.n, self.t = len(self._v), len(self._t)
+        self.stats = StepStatsC()
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            L = lib() if _lib is not None else None
+            if L is not None:
+                L.b3g_softbody_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def setup(self, scene, opts: SolverOptions | None = None) -> "SoftBody":
+        """Gravity, mass damping and static nodes of a SoftBodyScene."""
+        self.set_gravity(scene.gravity)
+        for i, dmp in enumerate(scene.mass_damping):
+            if dmp != 0.0:
+                self.set_mass_damping(i, float(dmp))
+        for i in scene.static_nodes:
+            self.set_node_type(int(i), 0)
+        if opts is not None:
+            self.set_solver(opts)
+        return self
+
+    def set_gravity(self, g) -> None:
+        a = _f3(g)
+        check(lib().b3g_softbody_set_gravity(self.h, _ptr(a)), "softbody_set_gravity")
+
+    def set_node_type(self, i: int, type_: int) -> None:
+        check(lib().b3g_softbody_set_node_type(self.h, i, type_), "softbody_set_node_type")
+
+    def set_mass_damping(self, i: int, d: float) -> None:
+        check(lib().b3g_softbody_set_mass_damping(self.h, i, d), "softbody_set_mass_damping")
+
+    def apply_force(self, i: int, f) -> None:
+        a = _f3(f)
+        check(lib().b3g_softbody_apply_force(self.h, i, _ptr(a)), "softbody_apply_force")
+
+    def set_velocity(self, i: int, v) -> None:
+        a = _f3(v)
+        check(lib().b3g_softbody_set_velocity(self.h, i, _ptr(a)), "softbody_set_velocity")
+
+    def set_position(self, i: int, x) -> None:
+        a = _f3(x)
+        check(lib().b3g_softbody_set_position(self.h, i, _ptr(a)), "softbody_set_position")
+
+    def set_solver(self, o: SolverOptions) -> None:
+        c = SolverOptsC(o.stop_rule, o.tolerance, o.max_iterations, o.dot)
+        check(lib().b3g_softbody_set_solver(self.h, C.byref(c)), "softbody_set_solver")
+
+    def step(self, dt: float, velocity_iterations: int = 8, position_iterations: int = 2) -> dict:
+        check(lib().b3g_softbody_step(self.h, dt, velocity_iterations, position_iterations, C.byref(self.stats)),
+              "softbody_step")
+        s = self.stats
+        return {"iterations": s.iterations, "delta0": s.delta0, "delta": s.delta, "b_delta": s.b_delta,
+                "step_ms": s.step_ms}
+
+    def state(self) -> dict:
+        x = np.zeros((self.n, 3), np.float32)
+        v = np.zeros((self.n, 3), np.float32)
+        check(lib().b3g_softbody_read_state(self.h, _ptr(x), _ptr(v)), "softbody_read_state")
+        return {"x": x, "v": v}
+
+    def write_state(self, x=None, v=None) -> None:
+        xs = None if x is None else np.ascontiguousarray(x, np.float32)
+        vs = None if v is None else np.ascontiguousarray(v, np.float32)
+        check(lib().b3g_softbody_write_state(self.h, None if xs is None else _ptr(xs),
+                                             None if vs is None else _ptr(vs)), "softbody_write_state")
+
+    def elements(self) -> dict:
+        q = np.zeros((self.t, 4), np.float32)
+        e = np.zeros((self.t, 6), np.float32)
+        check(lib().b3g_softbody_read_elements(self.h, _ptr(q), _ptr(e)), "softbody_read_elements")
+        return {"q": q, "eps": e}
+
+    def write_elements(self, q=None, eps=None) -> None:
+        qs = None if q is None else np.ascontiguousarray(q, np.float32)
+        es = None if eps is None else np.ascontiguousarray(eps, np.float32)
+        check(lib().b3g_softbody_write_elements(self.h, None if qs is None else _ptr(qs),
+                                                None if es is None else _ptr(es)), "softbody_write_elements")
+
+    def masses(self) -> np.ndarray:
+        m = np.zeros(self.n, np.float32)
+        check(lib().b3g_softbody_read_masses(self.h, _ptr(m)), "softbody_read_masses")
+        return m
+
+    def energy(self) -> float:
+        e = C.c_float(0.0)
+        check(lib().b3g_softbody_energy(self.h, C.byref(e)), "softbody_energy")
+        return float(e.value)
+
+    def system(self, dt: float) -> dict:
+        """A (rows in the reference's list order), b and S of one force solve
+        from the current state; the state is not changed."""
+        cnt = C.c_uint32(0)
+        L = lib()
+        check(L.b3g_softbody_export_system(self.h, dt, 0, None, None, None, None, None, C.byref(cnt)),
+              "softbody_export_system")
+        m = cnt.value
+        rowptr = np.zeros(self.n + 1, np.uint32)
+        cols = np.zeros(m, np.uint32)
+        vals = np.zeros(9 * m, np.float32)
+        b = np.zeros(3 * self.n, np.float32)
+        S = np.zeros(self.n, np.float32)
+        check(L.b3g_softbody_export_system(self.h, dt, m, _ptr(rowptr), _ptr(cols), _ptr(vals), _ptr(b), _ptr(S),
+                                           C.byref(cnt)), "softbody_export_system")
+        return {"rowptr": rowptr, "cols": cols, "vals": vals, "b": b, "S": S}

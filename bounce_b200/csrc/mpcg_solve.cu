@@ -45,7 +45,7 @@ __global__ void k_csr_init(CsrSystem s)
             const uint32_t j = s.cols[k];
             const m3 a = ldm(s.vals, k);
             if (j == i) diag = a;
-            const f3 xj = Sf(s, j) ? ldv(s.x0, j) : zero3();
+            const f3 xj = (s.softbody_mode || Sf(s, j)) ? ldv(s.x0, j) : zero3();
             ax = ax + a * xj;
         }
         const f3 pv = mk(1.0f / diag.x.x, 1.0f / diag.y.y, 1.0f / diag.z.z);
@@ -54,10 +54,11 @@ __global__ void k_csr_init(CsrSystem s)
         const f3 p = Si ? mk(r.x * pv.x, r.y * pv.y, r.z * pv.z) : zero3();
         const f3 bh = Si ? bi : zero3();
         stv(s.pinv, i, pv);
-        stv(s.x, i, Si ? ldv(s.x0, i) : zero3());
+        stv(s.x, i, (s.softbody_mode || Si) ? ldv(s.x0, i) : zero3());
         stv(s.r, i, r);
         stv(s.p, i, p);
-        v[0] = D::add_term(v[0], bh, mk(bh.x * pv.x, bh.y * pv.y, bh.z * pv.z));
+        const f3 w = s.softbody_mode ? mk(diag.x.x, diag.y.y, diag.z.z) : pv;
+        v[0] = D::add_term(v[0], bh, mk(bh.x * w.x, bh.y * w.y, bh.z * w.z));
         v[1] = D::add_term(v[1], r, p);
     }
     if (grid_reduce<DOT, 2>(v, s.partials, &s.sc->ticket[0]) && threadIdx.x == 0) {

@@ -26,6 +26,10 @@ struct CsrSystem {
     void* partials;
     StepScalars* sc;
     uint32_t grid, block;
+    // 0: b3SolveMPCG of the cloth (cloth_force_solver.cpp:61-136): x = S x0,
+    // b_delta = Sb . P^-1 Sb.  1: the soft body's (softbody_force_solver.cpp:
+    // 93-164): x = x0 on every row, delta_0 = Sb . P Sb with P = diag(A).
+    int softbody_mode;
 };
 
 inline size_t csr_align(size_t b) { return (b + 255) & ~size_t(255); }

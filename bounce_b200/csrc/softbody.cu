@@ -1,0 +1,705 @@
+// Soft body step on the GPU: b3SoftBody::Step (src/bounce/softbody/
+// softbody.cpp:700-735) without a world.
+//
+//   k_sb_elements   one thread per tetrahedron: the element rotation by
+//                   b3ExtractRotation from the element's previous rotation
+//                   (softbody_force_solver.cpp:53-91), the element's f0 terms
+//                   R Ke x0 and its plastic strain update and plastic forces
+//                   (:256-357)
+//   k_sb_assemble   one thread per node: the node's row of K summed over its
+//                   elements in element order (the reference's K(vi, vj) +=
+//                   R Ke RT), then b = M v - h (K p + f0 - (f_plastic + f_ext))
+//                   and A = M + h C + h^2 K (:359-377) in the reference's
+//                   float order; K p runs in the row list's order
+//   MPCG            the block-CSR MPCG in its soft body mode (x0 = v,
+//                   delta_0 = Sb . diag(A) Sb; softbody_force_solver.cpp:93-164)
+//   k_sb_integrate  v = solution, x += h v, forces cleared
+//                   (softbody_solver.cpp:105-110, softbody.cpp:716-720)
+//
+// Node vectors are xyz per node (b3DenseVec3 layout).  With -fmad=false the
+// element and assembly arithmetic is the reference's; the one difference is
+// the C library's double sin and cos in b3Quat::Set against CUDA's, which can
+// differ in the last bit of the rounded float in rare cases.
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/b3g.h"
+#include "cloth_dev.cuh"
+#include "mpcg_solve.cuh"
+#include "softbody_prep.h"
+#include "vec.cuh"
+
+namespace b3g {
+
+struct SoftDev {
+    uint32_t n, t, nnz;
+    const float* rest;
+    float *x, *v, *f;
+    const float* mass;
+    float* damping;
+    uint8_t* type;
+    const uint4* tets;
+    const float *Ke, *invE, *B, *P;
+    float4* q;
+    float* eps;
+    float *R, *f0s, *fps;
+    float c_yield, c_creep, c_max;
+    const uint32_t *rowptr, *cols, *diag;
+    float* vals;
+    const uint32_t *inc_ptr, *inc_elem, *inc_meta;
+    float *b, *S, *xsol;
+    float gx, gy, gz;
+};
+
+namespace {
+
+__device__ __forceinline__ f3 ldv(const float* p, uint32_t i) { return f3{p[3 * i], p[3 * i + 1], p[3 * i + 2]}; }
+__device__ __forceinline__ void stv(float* p, uint32_t i, f3 v)
+{
+    p[3 * i] = v.x;
+    p[3 * i + 1] = v.y;
+    p[3 * i + 2] = v.z;
+}
+__device__ __forceinline__ m3 ldm(const float* p)
+{
+    return m3{f3{p[0], p[1], p[2]}, f3{p[3], p[4], p[5]}, f3{p[6], p[7], p[8]}};
+}
+__device__ __forceinline__ void stm(float* p, const m3& a)
+{
+    p[0] = a.x.x, p[1] = a.x.y, p[2] = a.x.z;
+    p[3] = a.y.x, p[4] = a.y.y, p[5] = a.y.z;
+    p[6] = a.z.x, p[7] = a.z.y, p[8] = a.z.z;
+}
+__device__ __forceinline__ m3 mmul(const m3& a, const m3& b) { return m3{a * b.x, a * b.y, a * b.z}; }
+__device__ __forceinline__ m3 transpose(const m3& a)
+{
+    return m3{f3{a.x.x, a.y.x, a.z.x}, f3{a.x.y, a.y.y, a.z.y}, f3{a.x.z, a.y.z, a.z.z}};
+}
+__device__ __forceinline__ m3 diag3(float s) { return m3{f3{s, 0.0f, 0.0f}, f3{0.0f, s, 0.0f}, f3{0.0f, 0.0f, s}}; }
+
+// include/bounce/common/math/quat.h: b3QuatMat33 (:306-318), b3Mul (:170-178),
+// Normalize (:83-97), Set(axis, angle) (:99-107)
+__device__ __forceinline__ m3 quat_mat(float4 q)
+{
+    const float x = q.x, y = q.y, z = q.z, w = q.w;
+    const float x2 = x + x, y2 = y + y, z2 = z + z;
+    const float xx = x * x2, xy = x * y2, xz = x * z2;
+    const float yy = y * y2, yz = y * z2, zz = z * z2;
+    const float wx = w * x2, wy = w * y2, wz = w * z2;
+    return m3{f3{1.0f - (yy + zz), xy + wz, xz - wy}, f3{xy - wz, 1.0f - (xx + zz), yz + wx},
+              f3{xz + wy, yz - wx, 1.0f - (xx + yy)}};
+}
+__device__ __forceinline__ float4 quat_mul(float4 a, float4 b)
+{
+    return make_float4(a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y, a.w * b.y + a.y * b.w + a.z * b.x - a.x * b.z,
+                       a.w * b.z + a.z * b.w + a.x * b.y - a.y * b.x, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z);
+}
+
+// b3ExtractRotation (softbody_force_solver.cpp:53-91): at most 20 steps of
+// the rotation update from the previous rotation q
+__device__ m3 extract_rotation(float4& q, const m3& A)
+{
+    for (int iteration = 0; iteration < 20; ++iteration) {
+        const m3 R = quat_mat(q);
+        const float s = fabsf(dot(R.x, A.x) + dot(R.y, A.y) + dot(R.z, A.z));
+        if (s == 0.0f) break;
+        const float inv_s = 1.0f / s + 1.0e-9f;
+        const f3 v = (cross(R.x, A.x) + cross(R.y, A.y)) + cross(R.z, A.z);
+        const f3 omega = inv_s * v;
+        const float w = length(omega);
+        if (w < 1.0e-9f) break;
+        const f3 axis = omega / w;
+        const float theta = 0.5f * w;
+        const float sine = (float)sin((double)theta);
+        const float4 oq = make_float4(sine * axis.x, sine * axis.y, sine * axis.z, (float)cos((double)theta));
+        q = quat_mul(oq, q);
+        const float len = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+        if (len > 1.1920929e-07f) {
+            const float sc = 1.0f / len;
+            q.x *= sc;
+            q.y *= sc;
+            q.z *= sc;
+            q.w *= sc;
+        }
+    }
+    return quat_mat(q);
+}
+
+__device__ __forceinline__ float len6(const float* v)
+{
+    float r = 0.0f;
+    for (int i = 0; i < 6; ++i) r += v[i] * v[i];
+    return sqrtf(r);
+}
+
+__global__ void k_sb_elements(SoftDev d, float h, float inv_h)
+{
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= d.t) return;
+    const uint4 tv = d.tets[e];
+    const uint32_t vs[4] = {tv.x, tv.y, tv.z, tv.w};
+    f3 ps[4], xs[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        ps[k] = ldv(d.x, vs[k]);
+        xs[k] = ldv(d.rest, vs[k]);
+    }
+    const m3 E = m3{ps[1] - ps[0], ps[2] - ps[0], ps[3] - ps[0]};
+    const m3 A = mmul(E, ldm(d.invE + 9 * (size_t)e));
+    float4 q = d.q[e];
+    const m3 R = extract_rotation(q, A);
+    d.q[e] = q;
+    const m3 RT = transpose(R);
+    stm(d.R + 9 * (size_t)e, R);
+    const float* Ke = d.Ke + 144 * (size_t)e;
+    // f0 terms: sum_j (R Ke_ij) x0_j
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        f3 acc = zero3();
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc = acc + mmul(R, ldm(Ke + 9 * (i + 4 * j))) * xs[j];
+        stv(d.f0s + 12 * (size_t)e, i, acc);
+    }
+    // plasticity: total strain B (R^T p - x0), elastic = total - plastic
+    float rx[12];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const f3 dd = RT * ps[i] - xs[i];
+        rx[3 * i] = dd.x, rx[3 * i + 1] = dd.y, rx[3 * i + 2] = dd.z;
+    }
+    const float* B = d.B + 72 * (size_t)e;
+    float* ep = d.eps + 6 * (size_t)e;
+    float plastic[6], elastic[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) acc += B[i + 6 * k] * rx[k];
+        plastic[i] = ep[i];
+        elastic[i] = acc - plastic[i];
+    }
+    if (len6(elastic) > d.c_yield) {
+        const float amount = h * (d.c_creep < inv_h ? d.c_creep : inv_h);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) plastic[i] += amount * elastic[i];
+    }
+    const float lp = len6(plastic);
+    if (lp > d.c_max) {
+        const float scale = d.c_max / lp;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) plastic[i] *= scale;
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) ep[i] = plastic[i];
+    const float* P = d.P + 72 * (size_t)e;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float c[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) acc += P[3 * i + r + 12 * k] * plastic[k];
+            c[r] = acc;
+        }
+        stv(d.fps + 12 * (size_t)e, i, R * mk(c[0], c[1], c[2]));
+    }
+}
+
+__global__ void k_sb_assemble(SoftDev d, float h)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const uint32_t r0 = d.rowptr[i], deg = d.rowptr[i + 1] - r0;
+    float* vals = d.vals + 9 * (size_t)r0;
+    for (uint32_t k = 0; k < 9 * deg; ++k) vals[k] = 0.0f;
+    f3 f0 = zero3(), fp = zero3();
+    for (uint32_t q = d.inc_ptr[i]; q < d.inc_ptr[i + 1]; ++q) {
+        const uint32_t e = d.inc_elem[q], meta = d.inc_meta[q];
+        const uint32_t li = meta & 3u;
+        const m3 R = ldm(d.R + 9 * (size_t)e);
+        const m3 RT = transpose(R);
+        const float* Ke = d.Ke + 144 * (size_t)e;
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) {
+            const uint32_t slot = (meta >> (4 + 7 * j)) & 127u;
+            const m3 X = mmul(mmul(R, ldm(Ke + 9 * (li + 4 * j))), RT);
+            stm(vals + 9 * slot, ldm(vals + 9 * slot) + X);
+        }
+        f0 = f0 + ldv(d.f0s + 12 * (size_t)e, li);
+        fp = fp + ldv(d.fps + 12 * (size_t)e, li);
+    }
+    const f3 f0n = mk(-f0.x, -f0.y, -f0.z);
+    // K p in the row list's order (newest first touch first)
+    f3 kp = zero3();
+    for (uint32_t k = deg; k-- > 0;) kp = kp + ldm(vals + 9 * k) * ldv(d.x, d.cols[r0 + k]);
+    const bool dyn = d.type[i] == 2;
+    const float m = d.mass[i];
+    f3 fe = ldv(d.f, i);
+    if (dyn) fe = fe + m * mk(d.gx, d.gy, d.gz);
+    const m3 M = diag3(m);
+    const f3 mv = zero3() + M * ldv(d.v, i);
+    stv(d.b, i, mv - h * ((kp + f0n) - (fp + fe)));
+    d.S[i] = dyn ? 1.0f : 0.0f;
+    // A = (M + h C) + (h h) K on the diagonal, 0 + (h h) K elsewhere
+    const float hh = h * h;
+    const float cd = d.damping[i] * m;
+    const uint32_t dg = d.diag[i] - r0;
+    for (uint32_t k = 0; k < deg; ++k) {
+        const m3 K = ldm(vals + 9 * k);
+        m3 a;
+        if (k == dg) a = (M + h * diag3(cd)) + hh * K;
+        else a = mzero() + hh * K;
+        stm(vals + 9 * k, a);
+    }
+}
+
+__global__ void k_sb_integrate(SoftDev d, float h)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const f3 v = ldv(d.xsol, i);
+    stv(d.v, i, v);
+    stv(d.x, i, ldv(d.x, i) + h * v);
+    stv(d.f, i, zero3());
+}
+
+// Edits of one node, in stream order with the steps: 0 type, 1 mass damping,
+// 2 force +=, 3 velocity (ignored on static nodes), 4 position.
+__global__ void k_sb_node_op(SoftDev d, uint32_t i, int op, float a, float b, float c)
+{
+    if (op == 0) {
+        const uint8_t t = (uint8_t)a;
+        if (d.type[i] == t) return;
+        d.type[i] = t;
+        stv(d.f, i, zero3());
+        if (t == 0) stv(d.v, i, zero3());
+    } else if (op == 1) {
+        d.damping[i] = a;
+    } else if (op == 2) {
+        stv(d.f, i, ldv(d.f, i) + mk(a, b, c));
+    } else if (op == 3) {
+        if (d.type[i] != 0) stv(d.v, i, mk(a, b, c));
+    } else {
+        stv(d.x, i, mk(a, b, c));
+    }
+}
+
+constexpr uint32_t kBlock = 256;
+inline uint32_t blocks_for(uint32_t n) { return (n + kBlock - 1) / kBlock; }
+
+}  // namespace
+
+}  // namespace b3g
+
+using namespace b3g;
+
+struct b3g_softbody {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    char* arena = nullptr;
+    SoftDev dev{};
+    CsrSystem cs{};
+    b3g_solver_opts opts{B3G_STOP_REFERENCE, 0.0f, 20, B3G_DOT_F32};
+    uint32_t tets_count = 0;
+    std::vector<uint32_t> rowptr, cols, diag;  // host copies for the export
+    std::vector<float> mass;
+    b3g_step_stats last{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+b3g_status cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return B3G_OK;
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? B3G_ERR_OUT_OF_MEMORY : B3G_ERR_CUDA;
+}
+#define SB_TRY(expr)                                      \
+    do {                                                  \
+        b3g_status s_ = cuda_status(expr);                \
+        if (s_ != B3G_OK) return s_;                      \
+    } while (0)
+
+bool ok(const b3g_softbody* b) { return b && b->dev.n > 0; }
+
+b3g_status node_op(b3g_softbody* b, uint32_t i, int op, float x, float y, float z)
+{
+    if (!ok(b) || i >= b->dev.n) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    k_sb_node_op<<<1, 1, 0, b->stream>>>(b->dev, i, op, x, y, z);
+    count_launches(1);
+    SB_TRY(cudaGetLastError());
+    return B3G_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+b3g_status b3g_softbody_create(uint32_t vertex_count, const float* vertices, uint32_t tet_count,
+                               const uint32_t* tets, const b3g_softbody_def* def, int device, b3g_softbody** out)
+{
+    if (!out || !vertices || !tets || !def || vertex_count == 0 || tet_count == 0) return B3G_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!(def->density > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return B3G_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return B3G_ERR_INVALID_ARGUMENT;
+    SoftBodyPrep P;
+    const int st = prepare_softbody(vertex_count, vertices, tet_count, tets, def->density, def->E, def->nu, &P);
+    if (st != 0) return (b3g_status)st;
+    b3g_softbody* b = new (std::nothrow) b3g_softbody();
+    if (!b) return B3G_ERR_OUT_OF_MEMORY;
+    b->device = device;
+    cudaSetDevice(device);
+    const uint32_t n = vertex_count, t = tet_count, nnz = (uint32_t)P.cols.size();
+    const size_t vec = 3 * (size_t)n * sizeof(float);
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const uint32_t grid = csr_grid(n);
+    size_t bytes = 0;
+    const size_t sizes[] = {vec,       vec,       vec,       vec,          (size_t)n * 4, (size_t)n * 4, (size_t)n,
+                            (size_t)t * 16, (size_t)t * 576, (size_t)t * 36, (size_t)t * 288, (size_t)t * 288,
+                            (size_t)t * 16, (size_t)t * 24, (size_t)t * 36, (size_t)t * 48, (size_t)t * 48,
+                            (size_t)(n + 1) * 4, (size_t)nnz * 4, (size_t)n * 4, (size_t)nnz * 36,
+                            (size_t)(n + 1) * 4, (size_t)t * 16, (size_t)t * 16, vec, (size_t)n * 4, vec,
+                            csr_scratch_bytes(n, grid)};
+    for (size_t s : sizes) bytes += al(s);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&b->arena, bytes);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b3g_softbody_destroy(b);
+        return e == cudaErrorMemoryAllocation ? B3G_ERR_OUT_OF_MEMORY : B3G_ERR_CUDA;
+    }
+    char* p = b->arena;
+    auto take = [&](size_t s) {
+        char* r = p;
+        p += al(s);
+        return r;
+    };
+    SoftDev& d = b->dev;
+    d.n = n;
+    d.t = t;
+    d.nnz = nnz;
+    float* rest = (float*)take(vec);
+    d.rest = rest;
+    d.x = (float*)take(vec);
+    d.v = (float*)take(vec);
+    d.f = (float*)take(vec);
+    float* mass = (float*)take((size_t)n * 4);
+    d.mass = mass;
+    d.damping = (float*)take((size_t)n * 4);
+    d.type = (uint8_t*)take(n);
+    uint4* tv = (uint4*)take((size_t)t * 16);
+    d.tets = tv;
+    float* Ke = (float*)take((size_t)t * 576);
+    d.Ke = Ke;
+    float* invE = (float*)take((size_t)t * 36);
+    d.invE = invE;
+    float* Bm = (float*)take((size_t)t * 288);
+    d.B = Bm;
+    float* Pm = (float*)take((size_t)t * 288);
+    d.P = Pm;
+    d.q = (float4*)take((size_t)t * 16);
+    d.eps = (float*)take((size_t)t * 24);
+    d.R = (float*)take((size_t)t * 36);
+    d.f0s = (float*)take((size_t)t * 48);
+    d.fps = (float*)take((size_t)t * 48);
+    uint32_t* rowptr = (uint32_t*)take((size_t)(n + 1) * 4);
+    d.rowptr = rowptr;
+    uint32_t* cols = (uint32_t*)take((size_t)nnz * 4);
+    d.cols = cols;
+    uint32_t* dg = (uint32_t*)take((size_t)n * 4);
+    d.diag = dg;
+    d.vals = (float*)take((size_t)nnz * 36);
+    uint32_t* inc_ptr = (uint32_t*)take((size_t)(n + 1) * 4);
+    d.inc_ptr = inc_ptr;
+    uint32_t* inc_elem = (uint32_t*)take((size_t)t * 16);
+    d.inc_elem = inc_elem;
+    uint32_t* inc_meta = (uint32_t*)take((size_t)t * 16);
+    d.inc_meta = inc_meta;
+    d.b = (float*)take(vec);
+    d.S = (float*)take((size_t)n * 4);
+    d.xsol = (float*)take(vec);
+    char* scratch = take(csr_scratch_bytes(n, grid));
+    d.c_yield = def->c_yield;
+    d.c_creep = def->c_creep;
+    d.c_max = def->c_max;
+    // uploads
+    std::vector<uint4> tets4(t);
+    for (uint32_t k = 0; k < t; ++k) tets4[k] = make_uint4(tets[4 * k], tets[4 * k + 1], tets[4 * k + 2], tets[4 * k + 3]);
+    std::vector<float4> q0(t, make_float4(0.0f, 0.0f, 0.0f, 1.0f));  // the rest state's rotation
+    std::vector<uint8_t> types(n, 2);
+    cudaStream_t s = b->stream;
+    struct Up {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    } ups[] = {{rest, vertices, vec}, {d.x, vertices, vec}, {mass, P.mass.data(), (size_t)n * 4},
+               {tv, tets4.data(), (size_t)t * 16}, {Ke, P.Ke.data(), (size_t)t * 576},
+               {invE, P.invE.data(), (size_t)t * 36}, {Bm, P.B.data(), (size_t)t * 288},
+               {Pm, P.P.data(), (size_t)t * 288}, {d.q, q0.data(), (size_t)t * 16},
+               {rowptr, P.rowptr.data(), (size_t)(n + 1) * 4}, {cols, P.cols.data(), (size_t)nnz * 4},
+               {dg, P.diag.data(), (size_t)n * 4}, {inc_ptr, P.inc_ptr.data(), (size_t)(n + 1) * 4},
+               {inc_elem, P.inc_elem.data(), (size_t)t * 16}, {inc_meta, P.inc_meta.data(), (size_t)t * 16},
+               {d.type, types.data(), (size_t)n}};
+    for (const Up& u : ups)
+        if (e == cudaSuccess) e = cudaMemcpyAsync(u.dst, u.src, u.bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d.v, 0, vec, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d.f, 0, vec, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d.damping, 0, (size_t)n * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d.eps, 0, (size_t)t * 24, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the host vectors above go out of scope
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b3g_softbody_destroy(b);
+        return B3G_ERR_CUDA;
+    }
+    CsrSystem& c = b->cs;
+    c.n = n;
+    c.rowptr = rowptr;
+    c.cols = cols;
+    c.vals = d.vals;
+    c.b = d.b;
+    c.S = d.S;
+    c.x0 = d.v;
+    c.x = d.xsol;
+    c.block = 256;
+    c.grid = grid;
+    c.softbody_mode = 1;
+    csr_bind_scratch(&c, scratch);
+    b->tets_count = t;
+    b->rowptr = P.rowptr;
+    b->cols = P.cols;
+    b->diag = P.diag;
+    b->mass = P.mass;
+    *out = b;
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_destroy(b3g_softbody* b)
+{
+    if (!b) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->arena) cudaFree(b->arena);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return B3G_OK;
+}
+
+uint32_t b3g_softbody_node_count(const b3g_softbody* b) { return ok(b) ? b->dev.n : 0u; }
+uint32_t b3g_softbody_element_count(const b3g_softbody* b) { return ok(b) ? b->dev.t : 0u; }
+
+b3g_status b3g_softbody_set_gravity(b3g_softbody* b, const float* g)
+{
+    if (!ok(b) || !g) return B3G_ERR_INVALID_ARGUMENT;
+    b->dev.gx = g[0];
+    b->dev.gy = g[1];
+    b->dev.gz = g[2];
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_set_node_type(b3g_softbody* b, uint32_t i, int type)
+{
+    if (type < 0 || type > 2) return B3G_ERR_INVALID_ARGUMENT;
+    return node_op(b, i, 0, (float)type, 0.0f, 0.0f);
+}
+
+b3g_status b3g_softbody_set_mass_damping(b3g_softbody* b, uint32_t i, float damping)
+{
+    return node_op(b, i, 1, damping, 0.0f, 0.0f);
+}
+
+b3g_status b3g_softbody_apply_force(b3g_softbody* b, uint32_t i, const float* f)
+{
+    if (!f) return B3G_ERR_INVALID_ARGUMENT;
+    return node_op(b, i, 2, f[0], f[1], f[2]);
+}
+
+b3g_status b3g_softbody_set_velocity(b3g_softbody* b, uint32_t i, const float* v)
+{
+    if (!v) return B3G_ERR_INVALID_ARGUMENT;
+    return node_op(b, i, 3, v[0], v[1], v[2]);
+}
+
+b3g_status b3g_softbody_set_position(b3g_softbody* b, uint32_t i, const float* x)
+{
+    if (!x) return B3G_ERR_INVALID_ARGUMENT;
+    return node_op(b, i, 4, x[0], x[1], x[2]);
+}
+
+b3g_status b3g_softbody_set_solver(b3g_softbody* b, const b3g_solver_opts* o)
+{
+    if (!ok(b) || !o || o->max_iterations < 1 ||
+        (o->stop_rule != B3G_STOP_REFERENCE && o->stop_rule != B3G_STOP_RELATIVE) ||
+        (o->dot != B3G_DOT_F32 && o->dot != B3G_DOT_COMPENSATED && o->dot != B3G_DOT_F64))
+        return B3G_ERR_INVALID_ARGUMENT;
+    b->opts = *o;
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_step(b3g_softbody* b, float dt, uint32_t velocity_iterations, uint32_t position_iterations,
+                             b3g_step_stats* stats)
+{
+    (void)velocity_iterations;
+    (void)position_iterations;  // no contacts without a world
+    if (!ok(b) || !(dt >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    cudaStream_t s = b->stream;
+    SoftDev& d = b->dev;
+    std::memset(&b->last, 0, sizeof(b->last));
+    SB_TRY(cudaEventRecord(b->ev0, s));
+    StepScalars h;
+    std::memset(&h, 0, sizeof(h));
+    if (dt > 0.0f) {
+        k_sb_elements<<<blocks_for(d.t), kBlock, 0, s>>>(d, dt, 1.0f / dt);
+        k_sb_assemble<<<blocks_for(d.n), kBlock, 0, s>>>(d, dt);
+        count_launches(2);
+        SB_TRY(cudaGetLastError());
+        const b3g_status r = csr_run(b->cs, &b->opts, s, &h);
+        if (r != B3G_OK) return r;
+        k_sb_integrate<<<blocks_for(d.n), kBlock, 0, s>>>(d, dt);
+        count_launches(1);
+    } else {
+        SB_TRY(cudaMemsetAsync(d.f, 0, 3 * (size_t)d.n * sizeof(float), s));
+    }
+    SB_TRY(cudaGetLastError());
+    SB_TRY(cudaEventRecord(b->ev1, s));
+    SB_TRY(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    csr_report(h, nullptr, &b->last);
+    b->last.step_ms = ms;
+    if (stats) *stats = b->last;
+    return h.status ? (b3g_status)h.status : B3G_OK;
+}
+
+static b3g_status copy_nodes(b3g_softbody* b, float* dst, const float* src, size_t bytes, cudaMemcpyKind kind)
+{
+    SB_TRY(cudaMemcpyAsync(dst, src, bytes, kind, b->stream));
+    SB_TRY(cudaStreamSynchronize(b->stream));
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_read_state(const b3g_softbody* cb, float* x, float* v)
+{
+    b3g_softbody* b = const_cast<b3g_softbody*>(cb);
+    if (!ok(b)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    const size_t vec = 3 * (size_t)b->dev.n * sizeof(float);
+    b3g_status r = B3G_OK;
+    if (x && (r = copy_nodes(b, x, b->dev.x, vec, cudaMemcpyDeviceToHost)) != B3G_OK) return r;
+    if (v && (r = copy_nodes(b, v, b->dev.v, vec, cudaMemcpyDeviceToHost)) != B3G_OK) return r;
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_write_state(b3g_softbody* b, const float* x, const float* v)
+{
+    if (!ok(b)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    const size_t vec = 3 * (size_t)b->dev.n * sizeof(float);
+    b3g_status r = B3G_OK;
+    if (x && (r = copy_nodes(b, b->dev.x, x, vec, cudaMemcpyHostToDevice)) != B3G_OK) return r;
+    if (v && (r = copy_nodes(b, b->dev.v, v, vec, cudaMemcpyHostToDevice)) != B3G_OK) return r;
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_read_elements(const b3g_softbody* cb, float* q, float* eps)
+{
+    b3g_softbody* b = const_cast<b3g_softbody*>(cb);
+    if (!ok(b)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    b3g_status r = B3G_OK;
+    if (q && (r = copy_nodes(b, q, (const float*)b->dev.q, (size_t)b->dev.t * 16, cudaMemcpyDeviceToHost)) != B3G_OK)
+        return r;
+    if (eps && (r = copy_nodes(b, eps, b->dev.eps, (size_t)b->dev.t * 24, cudaMemcpyDeviceToHost)) != B3G_OK) return r;
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_write_elements(b3g_softbody* b, const float* q, const float* eps)
+{
+    if (!ok(b)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    b3g_status r = B3G_OK;
+    if (q && (r = copy_nodes(b, (float*)b->dev.q, q, (size_t)b->dev.t * 16, cudaMemcpyHostToDevice)) != B3G_OK) return r;
+    if (eps && (r = copy_nodes(b, b->dev.eps, eps, (size_t)b->dev.t * 24, cudaMemcpyHostToDevice)) != B3G_OK) return r;
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_read_masses(const b3g_softbody* b, float* m)
+{
+    if (!ok(b) || !m) return B3G_ERR_INVALID_ARGUMENT;
+    std::memcpy(m, b->mass.data(), b->mass.size() * sizeof(float));
+    return B3G_OK;
+}
+
+// b3SoftBody::GetEnergy (softbody.cpp:627-637): 0.5 sum m v.v in node order
+b3g_status b3g_softbody_energy(const b3g_softbody* b, float* energy)
+{
+    if (!ok(b) || !energy) return B3G_ERR_INVALID_ARGUMENT;
+    std::vector<float> v(3 * (size_t)b->dev.n);
+    b3g_status r = b3g_softbody_read_state(b, nullptr, v.data());
+    if (r != B3G_OK) return r;
+    float E = 0.0f;
+    for (uint32_t i = 0; i < b->dev.n; ++i) E += b->mass[i] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+    *energy = 0.5f * E;
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_export_system(b3g_softbody* b, float dt, uint32_t capacity, uint32_t* rowptr, uint32_t* cols,
+                                      float* vals, float* rhs, float* S, uint32_t* count)
+{
+    if (!ok(b) || !count || !(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    const SoftDev& d = b->dev;
+    *count = d.nnz;
+    if (capacity < d.nnz) return B3G_OK;
+    if (!rowptr || !cols || !vals || !rhs || !S) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    cudaStream_t s = b->stream;
+    // the element pass updates rotations and plastic strains: keep them
+    std::vector<float> q(4 * (size_t)d.t), eps(6 * (size_t)d.t);
+    b3g_status r = b3g_softbody_read_elements(b, q.data(), eps.data());
+    if (r != B3G_OK) return r;
+    k_sb_elements<<<blocks_for(d.t), kBlock, 0, s>>>(d, dt, 1.0f / dt);
+    k_sb_assemble<<<blocks_for(d.n), kBlock, 0, s>>>(d, dt);
+    count_launches(2);
+    SB_TRY(cudaGetLastError());
+    std::vector<float> v(9 * (size_t)d.nnz);
+    SB_TRY(cudaMemcpyAsync(v.data(), d.vals, v.size() * 4, cudaMemcpyDeviceToHost, s));
+    SB_TRY(cudaMemcpyAsync(rhs, d.b, 3 * (size_t)d.n * 4, cudaMemcpyDeviceToHost, s));
+    SB_TRY(cudaMemcpyAsync(S, d.S, (size_t)d.n * 4, cudaMemcpyDeviceToHost, s));
+    SB_TRY(cudaStreamSynchronize(s));
+    r = b3g_softbody_write_elements(b, q.data(), eps.data());
+    if (r != B3G_OK) return r;
+    // rows in the reference's list order: the off-diagonal blocks newest
+    // first touch first, then the diagonal block
+    uint32_t k = 0;
+    for (uint32_t i = 0; i < d.n; ++i) {
+        rowptr[i] = k;
+        const uint32_t r0 = b->rowptr[i], r1 = b->rowptr[i + 1];
+        for (uint32_t j = r1; j-- > r0;) {
+            if (j == b->diag[i]) continue;
+            cols[k] = b->cols[j];
+            std::memcpy(vals + 9 * (size_t)k, &v[9 * (size_t)j], 36);
+            ++k;
+        }
+        cols[k] = i;
+        std::memcpy(vals + 9 * (size_t)k, &v[9 * (size_t)b->diag[i]], 36);
+        ++k;
+    }
+    rowptr[d.n] = k;
+    return B3G_OK;
+}
+
+}  // extern "C"

@@ -191,8 +191,14 @@ b3g_status b3g_cloth_step(b3g_cloth* cloth, float dt, uint32_t velocity_iteratio
 /* How one cloth's CG runs on the GPU.  LAUNCHES (default): three kernels
  * per iteration inside a CUDA-graph while loop.  PERSISTENT: one cooperative
  * launch for the whole solve, iterations separated by grid barriers with
- * bounded waits (B3G_ERR_TIMEOUT if one gives up); for large cloths. */
-typedef enum { B3G_CG_LAUNCHES = 0, B3G_CG_PERSISTENT = 1 } b3g_cg_strategy;
+ * bounded waits (B3G_ERR_TIMEOUT if one gives up); for large cloths.
+ * PERSISTENT_FUSED: as PERSISTENT with one grid reduction per iteration
+ * instead of two; the next r.P^-1 r comes from the same sums as alpha
+ * (r.z - 2 alpha s.z + alpha^2 s.P^-1 s), so x, r, z and p follow the
+ * reference's expressions and only beta's numerator rounds differently.
+ * Cloths of up to one row per thread of the GPU (about 75k vertices on a
+ * B200) take the fused form; larger ones run PERSISTENT. */
+typedef enum { B3G_CG_LAUNCHES = 0, B3G_CG_PERSISTENT = 1, B3G_CG_PERSISTENT_FUSED = 2 } b3g_cg_strategy;
 b3g_status b3g_cloth_set_cg_strategy(b3g_cloth* cloth, b3g_cg_strategy strategy);
 /* Diagnostic of the bounded waits: runs the persistent CG once with a grid
  * barrier that can never complete and a wait limit of spin_limit polls;
@@ -404,6 +410,61 @@ b3g_status b3g_server_poll(b3g_server* server, uint64_t request_id, b3g_request_
 b3g_status b3g_server_result(b3g_server* server, uint64_t request_id, float* positions);
 b3g_status b3g_server_release(b3g_server* server, uint64_t request_id);
 b3g_status b3g_server_stats(const b3g_server* server, b3g_server_statistics* stats);
+
+/* ---- soft bodies ---------------------------------------------------------- */
+
+/* b3SoftBody (include/bounce/softbody/softbody.h, src/bounce/softbody/): a
+ * tetrahedral mesh simulated by corotated linear FEM with plasticity and the
+ * MPCG of softbody_force_solver.cpp.  The body has no world here, so it has
+ * no contacts.  Vectors are 3 floats per node in mesh order. */
+typedef struct b3g_softbody b3g_softbody;
+
+/* b3SoftBodyDef (softbody.h:64-99): density, Young's modulus E, Poisson's
+ * ratio nu, plastic yield, creep and maximum plastic strain. */
+typedef struct {
+    float density, E, nu, c_yield, c_creep, c_max;
+} b3g_softbody_def;
+
+/* b3SoftBody::b3SoftBody (softbody.cpp:436-553).  tets: 4 vertex ids each
+ * (b3SoftBodyMeshTetrahedron).  Every node starts dynamic with zero
+ * velocity and zero mass damping; each element's rotation starts at the
+ * identity.  B3G_ERR_DEGENERATE_MESH for a zero-volume or repeated-vertex
+ * tetrahedron, an id out of range or a vertex no tetrahedron uses. */
+b3g_status b3g_softbody_create(uint32_t vertex_count, const float* vertices, uint32_t tet_count,
+                               const uint32_t* tets, const b3g_softbody_def* def, int device, b3g_softbody** out);
+b3g_status b3g_softbody_destroy(b3g_softbody* body);
+uint32_t b3g_softbody_node_count(const b3g_softbody* body);
+uint32_t b3g_softbody_element_count(const b3g_softbody* body);
+/* b3SoftBody::SetGravity (softbody.h:192-195) */
+b3g_status b3g_softbody_set_gravity(b3g_softbody* body, const float* gravity);
+/* b3SoftBodyNode::SetType / SetMassDamping / ApplyForce / SetVelocity /
+ * SetPosition (softbody_node.h:146-211); type 0 static, 1 kinematic,
+ * 2 dynamic.  Applied in order with the steps. */
+b3g_status b3g_softbody_set_node_type(b3g_softbody* body, uint32_t node, int type);
+b3g_status b3g_softbody_set_mass_damping(b3g_softbody* body, uint32_t node, float damping);
+b3g_status b3g_softbody_apply_force(b3g_softbody* body, uint32_t node, const float* force);
+b3g_status b3g_softbody_set_velocity(b3g_softbody* body, uint32_t node, const float* velocity);
+b3g_status b3g_softbody_set_position(b3g_softbody* body, uint32_t node, const float* position);
+/* Default: the reference's MPCG (20 iterations, FLT_EPSILON^2, FP32 dots). */
+b3g_status b3g_softbody_set_solver(b3g_softbody* body, const b3g_solver_opts* opts);
+/* b3SoftBody::Step (softbody.cpp:700-735) without a world.  stats->delta0 is
+ * r.P^-1 r at the CG start, b_delta the soft body's delta_0 (Sb . diag(A) Sb). */
+b3g_status b3g_softbody_step(b3g_softbody* body, float dt, uint32_t velocity_iterations,
+                             uint32_t position_iterations, b3g_step_stats* stats);
+b3g_status b3g_softbody_read_state(const b3g_softbody* body, float* positions, float* velocities);
+b3g_status b3g_softbody_write_state(b3g_softbody* body, const float* positions, const float* velocities);
+/* Element state: the rotation q (x, y, z, w per element) that the next
+ * rotation extraction starts from, and the plastic strain (6 per element). */
+b3g_status b3g_softbody_read_elements(const b3g_softbody* body, float* q, float* plastic_strain);
+b3g_status b3g_softbody_write_elements(b3g_softbody* body, const float* q, const float* plastic_strain);
+b3g_status b3g_softbody_read_masses(const b3g_softbody* body, float* masses);
+/* b3SoftBody::GetEnergy (softbody.cpp:627-637) */
+b3g_status b3g_softbody_energy(const b3g_softbody* body, float* energy);
+/* The system A, b, S of one force solve from the current state, rows in the
+ * reference's b3SparseMat33 list order; the state is not changed.  *count
+ * receives the block count; nothing is written while capacity < *count. */
+b3g_status b3g_softbody_export_system(b3g_softbody* body, float dt, uint32_t capacity, uint32_t* rowptr,
+                                      uint32_t* cols, float* vals, float* b, float* S, uint32_t* count);
 
 /* ---- misc ----------------------------------------------------------------- */
 

@@ -1,0 +1,130 @@
+"""Soft body on the GPU (b3g_softbody_*) against the CPU oracle.
+
+Tolerances:
+* masses and, from identical state, the assembled system A, b and S:
+  bit-exact (the element and assembly arithmetic is the reference's; the
+  rotation extraction's sin and cos are CUDA's double functions rounded to
+  float, equal to the C library's there);
+* one step from identical state: CG iterations within +-1 (the GPU sums the
+  dot products in another order), positions and velocities within 1e-4
+  relative;
+* free trajectories: bounded drift, and the bulk motion agrees.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "softbody_block_ref.npz")
+
+
+def _pair(b3g, port, scene, opts=None):
+    s = scene.sdef
+    gpu = b3g.SoftBody(scene.vertices, scene.tets, s).setup(scene, opts)
+    ora = port.PortSoftBody(scene.vertices, scene.tets, s.density, s.E, s.nu, s.c_yield, s.c_creep,
+                            s.c_max).setup(scene)
+    if opts is not None:
+        ora.set_solver(opts.stop_rule, opts.tolerance, opts.max_iterations, opts.dot)
+    return gpu, ora
+
+
+def _sync(gpu, ora):
+    st, el = gpu.state(), gpu.elements()
+    ora.set_state(x=st["x"], v=st["v"])
+    ora.set_elements(q=el["q"], eps=el["eps"])
+
+
+def test_softbody_system_bit_exact(b3g, port):
+    scene = b3g.pinned_block_scene(4, 3, 3, spacing=0.5)
+    gpu, ora = _pair(b3g, port, scene)
+    assert np.array_equal(gpu.masses(), ora.masses())
+    for step in range(25):
+        if step % 6 == 0:
+            gpu.apply_force(7, [3.0, 40.0, -2.0])
+            ora.apply_force(7, [3.0, 40.0, -2.0])
+        if step in (0, 5, 24):
+            _sync(gpu, ora)
+            gs, os_ = gpu.system(scene.dt), ora.system(scene.dt)
+            for k in ("rowptr", "cols", "vals", "b", "S"):
+                assert np.array_equal(gs[k], os_[k]), (step, k)
+        gpu.step(scene.dt)
+        ora.step(scene.dt)
+
+
+@pytest.mark.parametrize("dot", [0, 2])
+def test_softbody_step_matches_oracle(b3g, port, dot):
+    """Each step starts the oracle from the GPU's state (positions,
+    velocities, element rotations and plastic strains)."""
+    scene = b3g.pinned_block_scene(5, 4, 3, spacing=0.5)
+    opts = b3g.SolverOptions.reference() if dot == 0 else b3g.SolverOptions.relative(1e-5, 200, dot)
+    gpu, ora = _pair(b3g, port, scene, opts)
+    gpu.set_node_type(3, 1)
+    ora.set_type(3, 1)
+    gpu.set_velocity(3, [0.2, 0.0, 0.0])
+    ora.set_velocity(3, [0.2, 0.0, 0.0])
+    for step in range(40):
+        _sync(gpu, ora)
+        if step % 9 == 0:
+            gpu.apply_force(11, [0.0, 60.0, 5.0])
+            ora.apply_force(11, [0.0, 60.0, 5.0])
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        assert abs(g["iterations"] - o["iterations"]) <= 1, (step, g["iterations"], o["iterations"])
+        gs, os_ = gpu.state(), ora.state()
+        assert rel_err(gs["x"], os_["x"]) <= 1e-4, step
+        assert rel_err(gs["v"], os_["v"]) <= 1e-4, step
+        ge, oe = gpu.elements(), ora.elements()
+        assert np.abs(ge["q"] - oe["q"]).max() <= 1e-5, step
+        assert np.abs(ge["eps"] - oe["eps"]).max() <= 1e-5, step
+    assert np.abs(gpu.elements()["eps"]).max() > 1e-3  # plastic flow happened
+
+
+def test_softbody_against_reference_golden(b3g, port):
+    """The reference's own trajectory (golden file, 120 steps with a
+    kinematic node and force pulses): the GPU trajectory stays within a
+    bounded drift of it, and the oracle reproduces it exactly."""
+    d = np.load(GOLDEN)
+    sdef = b3g.SoftBodyDef(*[float(x) for x in d["def"]])
+    scene = b3g.SoftBodyScene(d["vertices"], d["tets"], sdef, d["mass_damping"], d["static"],
+                              gravity=tuple(float(g) for g in d["gravity"]), dt=float(d["dt"]))
+    gpu = b3g.SoftBody(scene.vertices, scene.tets, sdef).setup(scene)
+    assert np.array_equal(gpu.masses(), d["mass"])
+    gpu.set_node_type(int(d["kinematic"]), 1)
+    gpu.set_velocity(int(d["kinematic"]), d["kinematic_v"])
+    per = int(d["force_period"])
+    drift = []
+    for k in range(1, len(d["iterations"]) + 1):
+        if (k - 1) % per == 0:
+            gpu.apply_force(int(d["force_node"]), d["force"])
+        g = gpu.step(scene.dt)
+        assert abs(g["iterations"] - int(d["iterations"][k - 1])) <= 1
+        if f"x_{k}" in d:
+            drift.append(float(np.abs(gpu.state()["x"] - d[f"x_{k}"]).max()))
+    print("soft body drift against the reference (m) at the kept steps:", drift)
+    assert drift[0] <= 1e-5
+    assert max(drift) <= 1e-2
+
+
+def test_softbody_free_fall_matches_oracle_bulk(b3g, port):
+    scene = b3g.pinned_block_scene(4, 4, 4)
+    gpu, ora = _pair(b3g, port, scene)
+    d = []
+    for step in range(100):
+        gpu.step(scene.dt)
+        ora.step(scene.dt)
+        d.append(float(np.abs(gpu.state()["x"] - ora.state()["x"]).max()))
+    print("soft body drift GPU-oracle (m) at 1/10/50/100:", d[0], d[9], d[49], d[99])
+    assert d[0] <= 1e-5
+    assert max(d) <= 1e-2
+    assert abs(gpu.energy() - ora.energy()) <= 1e-2 * max(ora.energy(), 1e-6)
+
+
+def test_softbody_rejects_degenerate_mesh(b3g):
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0]], np.float32)  # flat: zero volume
+    t = np.array([[0, 1, 2, 3]], np.uint32)
+    with pytest.raises(b3g.B3gError):
+        b3g.SoftBody(v, t, b3g.SoftBodyDef())
