@@ -53,6 +53,9 @@ def parse():
     # comparison inside the batched section
     ap.add_argument("--skip-single", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--skip-softbody", action="store_true")
+    ap.add_argument("--softbody-side", type=int, default=40)
+    ap.add_argument("--softbody-steps", type=int, default=10)
     return ap.parse_args()
 
 
@@ -318,6 +321,48 @@ def run_batched(args, dev: int):
             "l2": "inputs larger than L2 (about 1 GB of resident cloth state)"}
 
 
+def run_softbody(args, dev: int, cpu_sample: bool):
+    """The soft body step (b3SoftBody::Step) on a side^3 tetrahedral block of
+    1 m edge, hanging from one node, with the reference's pinned soft body
+    material and its own MPCG rule (20 iterations).  At side 40: 68,921 nodes
+    and 320,000 tetrahedra, whose per-element stiffness matrices alone
+    (12 x 12 floats each) are 184 MB, above L2.  The CPU figure is the oracle
+    (the C restatement, one core) on the same block for two steps."""
+    import bounce_b200 as b3g
+
+    side = args.softbody_side
+    scene = b3g.pinned_block_scene(side, side, side, spacing=1.0 / side)
+    body = b3g.SoftBody(scene.vertices, scene.tets, scene.sdef, device=dev).setup(scene)
+    for _ in range(args.warmup):
+        body.step(scene.dt)
+    launches0 = b3g.kernel_launch_count()
+    ms, iters = [], []
+    for _ in range(args.softbody_steps):
+        s = body.step(scene.dt)
+        ms.append(s["step_ms"])
+        iters.append(s["iterations"])
+    launches = b3g.kernel_launch_count() - launches0
+    body.close()
+    n, t = len(scene.vertices), len(scene.tets)
+    out = {"workload": f"block{side}x{side}x{side}_pinned", "nodes": n, "tetrahedra": t,
+           "node_steps_per_s": n * len(ms) / (sum(ms) / 1e3), "ms_per_step": sum(ms) / len(ms),
+           "cg_iterations_mean": float(np.mean(iters)), "cg": "reference rule (20 iterations, f32 dots)",
+           "gpu_launches": launches, "steps": len(ms)}
+    if cpu_sample:
+        import oracle
+
+        ora = oracle.PortSoftBody(scene.vertices, scene.tets, scene.sdef.density, scene.sdef.E, scene.sdef.nu,
+                                  scene.sdef.c_yield, scene.sdef.c_creep, scene.sdef.c_max).setup(scene)
+        t0 = time.perf_counter()
+        for _ in range(2):
+            ora.step(scene.dt)
+        sec = time.perf_counter() - t0
+        ora.close()
+        out["cpu_baseline"] = {"value": n * 2 / sec, "unit": "node-steps/s", "cores": 1, "kind": "port",
+                               "sample": f"the oracle's soft body step, 2 steps of the same block, {sec / 2:.2f} s/step"}
+    return out
+
+
 def run_serving(args, dev: int):
     from bounce_b200 import serving
 
@@ -424,6 +469,8 @@ def main():
     r = run_ours(args, rank, world)
     batched = None if args.skip_batch else run_batched(args, local)
     served = None if args.skip_serve else run_serving(args, local)
+    soft = None if args.skip_softbody else run_softbody(args, local, rank == 0 and world == 1
+                                                         and not args.no_cpu_baseline)
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -458,6 +505,7 @@ def main():
         "cpu_baseline": base,
         "batched": batched,
         "serving": served,
+        "softbody": soft,
     }
     print(json.dumps(line))
 
