@@ -20,7 +20,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from .meshes import (DYNAMIC, KINEMATIC, STATIC, ClothDef, Mesh, Scene, batch_scenes, capsule_scene, grid_mesh,  # noqa: F401
-                     plain_scene, sewn_scene, sphere_scene, stiff_scene, SoftBodyDef, SoftBodyScene,
+                     plain_scene, self_collision_scene, sewn_scene, sphere_scene, stiff_scene, SoftBodyDef,
+                     SoftBodyScene,
                      block_softbody_mesh, pinned_block_scene)
 
 HERE = os.path.dirname(os.path.abspath(__file__))

@@ -126,6 +126,19 @@ def capsule_scene(side: int = 32, seed: int = 5, steps: int = 120) -> Scene:
     return Scene(f"grid{side}_capsule", mesh, cdef, np.zeros(0, np.uint32), capsules=caps, steps=steps)
 
 
+def self_collision_scene(side: int = 11, seed: int = 6, steps: int = 150) -> Scene:
+    """The reference's self-collision scene (examples/testbed/tests/
+    cloth_self_collision.h:24-60): a side x side vertex grid of 1 m spacing,
+    5 m up, density 1, stretch 1e5, no shear or damping, thickness 0.2,
+    friction 0.3, falling onto a static capsule from (0, 0, -5) to (0, 0, 5),
+    radius 1, friction 1.  Jitter N(0, 1e-3 m); nothing pinned."""
+    mesh = grid_mesh(side, float(side - 1), 1e-3, seed)
+    mesh.vertices[:, 1] += np.float32(5.0)
+    cdef = ClothDef(density=1.0, streching=1e5, thickness=0.2, friction=0.3)
+    caps = [((0.0, 0.0, -5.0), (0.0, 0.0, 5.0), 1.0, 1.0)]
+    return Scene(f"grid{side}_self_collision", mesh, cdef, np.zeros(0, np.uint32), capsules=caps, steps=steps)
+
+
 def stiff_scene(side: int = 1024, steps: int = 50) -> Scene:
     """Ill-conditioned large cloth: stretch 1e5, damping 0.1, shear 1e3, no jitter."""
     mesh = grid_mesh(side, 1.0, 0.0, 0)

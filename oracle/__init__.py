@@ -43,7 +43,8 @@ def build(port: bool = True, ref: bool = True) -> None:
 
 class _OcStepInfo(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("delta0", C.c_double), ("delta", C.c_double),
-                ("b_delta", C.c_double), ("active_contacts", C.c_uint32), ("contacts", C.c_uint32)]
+                ("b_delta", C.c_double), ("active_contacts", C.c_uint32), ("contacts", C.c_uint32),
+                ("active_tri_contacts", C.c_uint32), ("tri_contacts", C.c_uint32)]
 
 
 _port = None
@@ -75,6 +76,8 @@ def port_lib():
         L.oc_describe.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_get_contacts.restype = C.c_uint32
         L.oc_get_contacts.argtypes = [C.c_void_p, _u8p, _u8p, _f32p]
+        L.oc_get_tri_contacts.restype = C.c_uint32
+        L.oc_get_tri_contacts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_force_count.restype = C.c_uint32
         L.oc_force_count.argtypes = [C.c_void_p]
         L.oc_spring_count.restype = C.c_uint32
@@ -132,6 +135,8 @@ def ref_lib():
         L.ref_cloth_describe.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_cloth_get_contacts.restype = C.c_uint32
         L.ref_cloth_get_contacts.argtypes = [C.c_void_p, _u8p, _u8p, _f32p]
+        L.ref_cloth_get_tri_contacts.restype = C.c_uint32
+        L.ref_cloth_get_tri_contacts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_cloth_build_system.restype = C.c_uint32
         L.ref_cloth_build_system.argtypes = [C.c_void_p, C.c_float]
         L.ref_cloth_get_system.argtypes = [C.c_void_p, _u32p, _u32p, _f32p, _f32p, _f32p, _f32p, _u32p]
@@ -214,6 +219,17 @@ class _Base:
         cnt = self._get_contacts(ex, ac, imp)
         return {"count": int(cnt), "exists": ex, "active": ac, "impulses": imp.reshape(-1, 3)}
 
+    def tri_contacts(self):
+        """Particle-triangle contacts in list order (head first)."""
+        m = int(self._get_tri_contacts(None, None, None, None))
+        pt = np.zeros(2 * max(m, 1), np.uint32)
+        ac = np.zeros(max(m, 1), np.uint8)
+        w = np.zeros(3 * max(m, 1), np.float32)
+        imp = np.zeros(3 * max(m, 1), np.float32)
+        self._get_tri_contacts(pt.ctypes.data, ac.ctypes.data, w.ctypes.data, imp.ctypes.data)
+        return {"count": m, "pt": pt.reshape(-1, 2)[:m], "active": ac[:m], "w": w.reshape(-1, 3)[:m],
+                "impulses": imp.reshape(-1, 3)[:m]}
+
     def system(self, dt: float):
         nnz = self._build_system(dt)
         rowptr = np.zeros(self.n + 1, np.uint32)
@@ -288,7 +304,8 @@ class PortCloth(_Base):
         self.L.oc_step(self.h, dt, vel_iters, pos_iters, C.byref(self.last))
         return {"iterations": self.last.iterations, "delta0": self.last.delta0, "delta": self.last.delta,
                 "b_delta": self.last.b_delta, "active_contacts": self.last.active_contacts,
-                "contacts": self.last.contacts}
+                "contacts": self.last.contacts, "active_tri_contacts": self.last.active_tri_contacts,
+                "tri_contacts": self.last.tri_contacts}
 
     def energy(self):
         return float(self.L.oc_energy(self.h))
@@ -324,6 +341,9 @@ class PortCloth(_Base):
 
     def _get_contacts(self, *a):
         return self.L.oc_get_contacts(self.h, *a)
+
+    def _get_tri_contacts(self, *a):
+        return self.L.oc_get_tri_contacts(self.h, *a)
 
     def _build_system(self, dt):
         return self.L.oc_build_system(self.h, dt)
@@ -400,6 +420,9 @@ class RefCloth(_Base):
 
     def _get_contacts(self, *a):
         return self.L.ref_cloth_get_contacts(self.h, *a)
+
+    def _get_tri_contacts(self, *a):
+        return self.L.ref_cloth_get_tri_contacts(self.h, *a)
 
     def _build_system(self, dt):
         return self.L.ref_cloth_build_system(self.h, dt)

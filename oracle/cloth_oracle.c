@@ -165,6 +165,16 @@ typedef struct {
     v3 fat_lo, fat_hi; /* the shape's proxy in the world broadphase */
 } sphere_t;
 
+/* b3ParticleTriangleContact (cloth_particle_triangle_contact.h): particle p
+ * against triangle t, whose vertices are b, cc, d (the contact's m_p2, m_p3,
+ * m_p4). */
+typedef struct {
+    uint32_t p, t, b, cc, d;
+    int active;
+    float w2, w3, w4;
+    float normal_impulse, tangent_impulse1, tangent_impulse2;
+} tcontact_t;
+
 typedef struct {
     uint32_t particle, shape;
     int active;
@@ -203,6 +213,14 @@ struct oc_cloth {
     /* body-contact list stored tail first: element [ncontact-1] is the list head */
     contact_t* contacts;
     uint32_t ncontact, contact_cap;
+
+    /* self-collision (thickness > 0): triangle proxies, the broadphase move
+     * buffer as one flag per proxy, and the particle-triangle contact list,
+     * stored tail first like the body contacts */
+    v3 *tri_lo, *tri_hi;
+    uint8_t *p_moved, *t_moved;
+    tcontact_t* tcs;
+    uint32_t ntc, tc_cap;
 
     int stop_rule, dot;
     float tol;
@@ -297,6 +315,23 @@ oc_cloth* oc_create(const float* vertices, uint32_t n, const uint32_t* triangles
         c->mass[triangles[3 * k + 2]] += inv3 * m;
     }
     for (uint32_t i = 0; i < n; ++i) c->inv_mass[i] = 1.0f / c->mass[i];
+
+    /* triangle proxies (cloth.cpp:140-150): the triangle's AABB extended by
+     * the thickness, fattened by B3_AABB_EXTENSION in CreateProxy
+     * (broad_phase.cpp:78-90); every new proxy is in the move buffer */
+    c->tri_lo = (v3*)malloc((t ? t : 1) * sizeof(v3));
+    c->tri_hi = (v3*)malloc((t ? t : 1) * sizeof(v3));
+    c->t_moved = (uint8_t*)malloc(t ? t : 1);
+    c->p_moved = (uint8_t*)malloc(n ? n : 1);
+    memset(c->t_moved, 1, t ? t : 1);
+    memset(c->p_moved, 1, n ? n : 1);
+    for (uint32_t k = 0; k < t; ++k) {
+        v3 A = c->x[triangles[3 * k]], B = c->x[triangles[3 * k + 1]], C = c->x[triangles[3 * k + 2]];
+        v3 r = V(thickness, thickness, thickness);
+        v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
+        c->tri_lo[k] = vsub(vsub(vmin(A, vmin(B, C)), r), ext);
+        c->tri_hi[k] = vadd(vadd(vmax(A, vmax(B, C)), r), ext);
+    }
 
     /* triangles (cloth.cpp:129-215) */
     c->du1 = (float*)malloc(t * sizeof(float));
@@ -431,6 +466,7 @@ void oc_destroy(oc_cloth* c)
 {
     if (!c) return;
     free(c->tris);
+    free(c->tri_lo); free(c->tri_hi); free(c->t_moved); free(c->p_moved); free(c->tcs);
     free(c->x); free(c->v); free(c->f); free(c->y); free(c->mx);
     free(c->mass); free(c->inv_mass); free(c->radius); free(c->friction); free(c->type);
     free(c->fat_lo); free(c->fat_hi); free(c->order); free(c->solver_of_vertex);
@@ -467,6 +503,53 @@ static void move_proxy(oc_cloth* c, uint32_t i, v3 displacement)
     if (d.z < 0.0f) lo.z += d.z; else hi.z += d.z;
     c->fat_lo[i] = lo;
     c->fat_hi[i] = hi;
+    c->p_moved[i] = 1; /* BufferMove */
+}
+
+static inline int self_collision(const oc_cloth* c) { return c->def[6] > 0.0f; }
+
+/* b3ClothTriangle::Synchronize (cloth_triangle.cpp:24-40) with
+ * b3BroadPhase::MoveProxy (broad_phase.cpp:99-149). */
+static void move_triangle_proxy(oc_cloth* c, uint32_t k, v3 displacement)
+{
+    const float rad = c->def[6];
+    v3 A = c->x[c->tris[3 * k]], B = c->x[c->tris[3 * k + 1]], C = c->x[c->tris[3 * k + 2]];
+    v3 r = V(rad, rad, rad);
+    v3 lo = vsub(vmin(A, vmin(B, C)), r), hi = vadd(vmax(A, vmax(B, C)), r);
+    v3 flo = c->tri_lo[k], fhi = c->tri_hi[k];
+    int contains = flo.x <= lo.x && lo.x <= fhi.x && flo.y <= lo.y && lo.y <= fhi.y &&
+                   flo.z <= lo.z && lo.z <= fhi.z && flo.x <= hi.x && hi.x <= fhi.x &&
+                   flo.y <= hi.y && hi.y <= fhi.y && flo.z <= hi.z && hi.z <= fhi.z;
+    if (contains) return;
+    v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
+    lo = vsub(lo, ext);
+    hi = vadd(hi, ext);
+    v3 d = vscale(kAabbMultiplier, displacement);
+    if (d.x < 0.0f) lo.x += d.x; else hi.x += d.x;
+    if (d.y < 0.0f) lo.y += d.y; else hi.y += d.y;
+    if (d.z < 0.0f) lo.z += d.z; else hi.z += d.z;
+    c->tri_lo[k] = lo;
+    c->tri_hi[k] = hi;
+    c->t_moved[k] = 1;
+}
+
+/* b3Particle::SynchronizeTriangles (particle.cpp:66-82): every triangle of a
+ * mesh vertex, with no displacement. */
+static void sync_vertex_triangles(oc_cloth* c, uint32_t i)
+{
+    if (i >= c->n_mesh) return;
+    for (uint32_t k = 0; k < c->t; ++k)
+        if (c->tris[3 * k] == i || c->tris[3 * k + 1] == i || c->tris[3 * k + 2] == i)
+            move_triangle_proxy(c, k, vzero());
+}
+
+/* The particle-triangle contacts whose particle is i (particle.cpp:103-118). */
+static void destroy_particle_triangle_contacts(oc_cloth* c, uint32_t i)
+{
+    uint32_t w = 0;
+    for (uint32_t k = 0; k < c->ntc; ++k)
+        if (c->tcs[k].p != i) c->tcs[w++] = c->tcs[k];
+    c->ntc = w;
 }
 
 /* Remove every body contact of particle i (particle.cpp:66-83). */
@@ -501,8 +584,11 @@ void oc_set_type(oc_cloth* c, uint32_t i, int type)
         c->v[i] = vzero();
         c->y[i] = vzero();
         move_proxy(c, i, vzero());
+        sync_vertex_triangles(c, i);
     }
     destroy_particle_contacts(c, i);
+    destroy_particle_triangle_contacts(c, i);
+    c->p_moved[i] = 1; /* TouchProxy */
 }
 
 /* b3Particle::ApplyForce / ApplyTranslation / SetPosition / SetVelocity (particle.h:205-271) */
@@ -524,6 +610,7 @@ void oc_set_position(oc_cloth* c, uint32_t i, const float* x)
     c->x[i] = p;
     c->y[i] = vzero();
     move_proxy(c, i, d);
+    sync_vertex_triangles(c, i);
 }
 
 void oc_set_velocity(oc_cloth* c, uint32_t i, const float* v)
@@ -774,7 +861,7 @@ static void resize_particles(oc_cloth* c, uint32_t n_new)
     } while (0)
     GROW(c->x, v3); GROW(c->v, v3); GROW(c->f, v3); GROW(c->y, v3); GROW(c->mx, v3);
     GROW(c->mass, float); GROW(c->inv_mass, float); GROW(c->radius, float); GROW(c->friction, float);
-    GROW(c->type, uint8_t); GROW(c->fat_lo, v3); GROW(c->fat_hi, v3);
+    GROW(c->type, uint8_t); GROW(c->fat_lo, v3); GROW(c->fat_hi, v3); GROW(c->p_moved, uint8_t);
     GROW(c->order, uint32_t); GROW(c->solver_of_vertex, uint32_t);
     GROW(c->sx, v3); GROW(c->sv, v3); GROW(c->sf, v3); GROW(c->sy, v3); GROW(c->sx0, v3);
     GROW(c->b, v3); GROW(c->dvsol, v3); GROW(c->Sflag, float);
@@ -819,6 +906,7 @@ uint32_t oc_create_particle(oc_cloth* c, const float* position, const float* vel
     v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
     c->fat_lo[i] = vsub(vsub(c->x[i], r), ext);
     c->fat_hi[i] = vadd(vadd(c->x[i], r), ext);
+    c->p_moved[i] = 1;
     memmove(c->order + 1, c->order, (size_t)i * sizeof(uint32_t));
     c->order[0] = i;
     return i;
@@ -851,11 +939,14 @@ int oc_destroy_particle(oc_cloth* c, uint32_t i)
         if (c->forces[q].type == F_MOUSE && c->forces[q].a > i) c->forces[q].a -= 1;
     for (uint32_t q = 0; q < c->ncontact; ++q)
         if (c->contacts[q].particle > i) c->contacts[q].particle -= 1;
+    destroy_particle_triangle_contacts(c, i);
+    for (uint32_t q = 0; q < c->ntc; ++q)
+        if (c->tcs[q].p > i) c->tcs[q].p -= 1;
     uint32_t tail = c->n - i - 1;
 #define SHIFT(ptr) memmove(ptr + i, ptr + i + 1, (size_t)tail * sizeof(*ptr))
     SHIFT(c->x); SHIFT(c->v); SHIFT(c->f); SHIFT(c->y); SHIFT(c->mx);
     SHIFT(c->mass); SHIFT(c->inv_mass); SHIFT(c->radius); SHIFT(c->friction); SHIFT(c->type);
-    SHIFT(c->fat_lo); SHIFT(c->fat_hi);
+    SHIFT(c->fat_lo); SHIFT(c->fat_hi); SHIFT(c->p_moved);
 #undef SHIFT
     resize_particles(c, c->n - 1);
     c->n -= 1;
@@ -1386,6 +1477,295 @@ static void find_new_body_contacts(oc_cloth* c)
     free(has);
 }
 
+/* ------------------------------------------------------------------------ */
+/* self-collision: particle-triangle contacts                                */
+/* ------------------------------------------------------------------------ */
+
+/* b3BarycentricCoordinates for a segment and a triangle (geometry.h:105-145). */
+static void bary2(float out[3], v3 A, v3 B, v3 Q)
+{
+    v3 AB = vsub(B, A), QA = vsub(A, Q), QB = vsub(B, Q);
+    float divisor = vdot(AB, AB);
+    out[0] = vdot(QB, AB);
+    out[1] = -vdot(QA, AB);
+    out[2] = divisor;
+}
+
+static void bary3(float out[4], v3 A, v3 B, v3 C, v3 Q)
+{
+    v3 AB = vsub(B, A), AC = vsub(C, A);
+    v3 QA = vsub(A, Q), QB = vsub(B, Q), QC = vsub(C, Q);
+    v3 QB_x_QC = vcross(QB, QC), QC_x_QA = vcross(QC, QA), QA_x_QB = vcross(QA, QB);
+    v3 AB_x_AC = vcross(AB, AC);
+    out[0] = vdot(QB_x_QC, AB_x_AC);
+    out[1] = vdot(QC_x_QA, AB_x_AC);
+    out[2] = vdot(QA_x_QB, AB_x_AC);
+    out[3] = out[0] + out[1] + out[2];
+}
+
+/* b3Solve3 (cloth_particle_triangle_contact.cpp:26-122): the barycentric
+ * coordinates of the point of ABC closest to Q. */
+static void solve3(float out[3], v3 A, v3 B, v3 C, v3 Q)
+{
+    float wAB[3], wBC[3], wCA[3];
+    bary2(wAB, A, B, Q);
+    bary2(wBC, B, C, Q);
+    bary2(wCA, C, A, Q);
+    if (wAB[1] <= 0.0f && wCA[0] <= 0.0f) { out[0] = 1.0f; out[1] = 0.0f; out[2] = 0.0f; return; }
+    if (wAB[0] <= 0.0f && wBC[1] <= 0.0f) { out[0] = 0.0f; out[1] = 1.0f; out[2] = 0.0f; return; }
+    if (wBC[0] <= 0.0f && wCA[1] <= 0.0f) { out[0] = 0.0f; out[1] = 0.0f; out[2] = 1.0f; return; }
+    float wABC[4];
+    bary3(wABC, A, B, C, Q);
+    if (wAB[0] > 0.0f && wAB[1] > 0.0f && wABC[3] * wABC[2] <= 0.0f) {
+        float s = 1.0f / wAB[2];
+        out[0] = s * wAB[0]; out[1] = s * wAB[1]; out[2] = 0.0f;
+        return;
+    }
+    if (wBC[0] > 0.0f && wBC[1] > 0.0f && wABC[3] * wABC[0] <= 0.0f) {
+        float s = 1.0f / wBC[2];
+        out[0] = 0.0f; out[1] = s * wBC[0]; out[2] = s * wBC[1];
+        return;
+    }
+    if (wCA[0] > 0.0f && wCA[1] > 0.0f && wABC[3] * wABC[1] <= 0.0f) {
+        float s = 1.0f / wCA[2];
+        out[0] = s * wCA[1]; out[1] = 0.0f; out[2] = s * wCA[0];
+        return;
+    }
+    float divisor = wABC[3];
+    if (divisor == 0.0f) {
+        float s = 1.0f / 3.0f;
+        out[0] = s; out[1] = s; out[2] = s;
+        return;
+    }
+    float s = 1.0f / divisor;
+    out[0] = s * wABC[0]; out[1] = s * wABC[1]; out[2] = s * wABC[2];
+}
+
+/* b3ParticleTriangleContact::Update (cloth_particle_triangle_contact.cpp:124-179). */
+static void tcontact_update(oc_cloth* c, tcontact_t* k)
+{
+    v3 A = c->x[k->b], B = c->x[k->cc], C = c->x[k->d];
+    v3 N = vcross(vsub(B, A), vsub(C, A));
+    float len = sqrtf(N.x * N.x + N.y * N.y + N.z * N.z); /* b3Vec3::Normalize */
+    if (len > kEps) {
+        float s1 = 1.0f / len;
+        N = V(N.x * s1, N.y * s1, N.z * s1);
+    }
+    if (len == 0.0f) {
+        k->active = 0;
+        return;
+    }
+    float totalRadius = c->radius[k->p] + c->def[6];
+    v3 P1 = c->x[k->p];
+    float distance = vdot(N, vsub(P1, A));
+    if (distance < -totalRadius || distance > totalRadius) {
+        k->active = 0;
+        return;
+    }
+    float w[3];
+    solve3(w, A, B, C, P1);
+    v3 P2 = vadd(vadd(vscale(w[0], A), vscale(w[1], B)), vscale(w[2], C));
+    v3 dd = vsub(P1, P2);
+    if (vdot(dd, dd) > totalRadius * totalRadius) {
+        k->active = 0;
+        return;
+    }
+    k->active = 1;
+    k->w2 = w[0];
+    k->w3 = w[1];
+    k->w4 = w[2];
+}
+
+static inline int tri_dynamic(const oc_cloth* c, const tcontact_t* k)
+{
+    return c->type[k->b] == OC_DYNAMIC || c->type[k->cc] == OC_DYNAMIC || c->type[k->d] == OC_DYNAMIC;
+}
+
+/* UpdateClothContacts (cloth_contact_manager.cpp:229-275). */
+static void update_cloth_contacts(oc_cloth* c)
+{
+    uint32_t w = 0;
+    for (uint32_t q = 0; q < c->ntc; ++q) {
+        tcontact_t* k = c->tcs + q;
+        if (c->type[k->p] != OC_DYNAMIC && !tri_dynamic(c, k)) continue;
+        if (!aabb_overlap(c->fat_lo[k->p], c->fat_hi[k->p], c->tri_lo[k->t], c->tri_hi[k->t])) continue;
+        tcontact_update(c, k);
+        c->tcs[w++] = *k;
+    }
+    c->ntc = w;
+}
+
+/* FindNewClothContacts (cloth_contact_manager.cpp:43-48) through
+ * b3BroadPhase::FindPairs (broad_phase.h:160-208) and AddPair (:125-199).
+ * FindPairs reports each overlapping pair with at least one proxy in the
+ * move buffer once, in ascending (proxy1, proxy2) order.  Proxy ids follow
+ * creation order, particles (cloth.cpp:109-123) before triangles (:129-150),
+ * so a particle-triangle pair is ordered by (particle, triangle).  AddPair
+ * pushes each new contact to the list front. */
+static void find_new_cloth_contacts(oc_cloth* c)
+{
+    const uint32_t n = c->n, t = c->t;
+    uint8_t* has = (uint8_t*)calloc((size_t)n * t + 1, 1);
+    for (uint32_t q = 0; q < c->ntc; ++q) has[(size_t)c->tcs[q].p * t + c->tcs[q].t] = 1;
+    for (uint32_t i = 0; i < n; ++i) {
+        for (uint32_t k = 0; k < t; ++k) {
+            if (!c->p_moved[i] && !c->t_moved[k]) continue;
+            if (!aabb_overlap(c->fat_lo[i], c->fat_hi[i], c->tri_lo[k], c->tri_hi[k])) continue;
+            if (has[(size_t)i * t + k]) continue;
+            tcontact_t nk;
+            memset(&nk, 0, sizeof(nk));
+            nk.p = i;
+            nk.t = k;
+            nk.b = c->tris[3 * k];
+            nk.cc = c->tris[3 * k + 1];
+            nk.d = c->tris[3 * k + 2];
+            if (c->type[i] != OC_DYNAMIC && !tri_dynamic(c, &nk)) continue;
+            if (i == nk.b || i == nk.cc || i == nk.d) continue;
+            if (c->ntc == c->tc_cap) {
+                c->tc_cap = c->tc_cap ? 2 * c->tc_cap : 1024;
+                c->tcs = (tcontact_t*)realloc(c->tcs, c->tc_cap * sizeof(tcontact_t));
+            }
+            c->tcs[c->ntc++] = nk;
+        }
+    }
+    free(has);
+    memset(c->p_moved, 0, n ? n : 1);
+    memset(c->t_moved, 0, t ? t : 1);
+}
+
+/* The solver's view of one active particle-triangle contact
+ * (b3ClothSolverTriangleContactVelocityConstraint / PositionConstraint). */
+typedef struct {
+    uint32_t ia, ib, ic, id; /* solver rows */
+    float mA, mB, mC, mD;
+    float radiusA, triangleRadius;
+    float wB, wC, wD;
+    v3 normal, tangent1, tangent2;
+    float normalMass, tangentMass1, tangentMass2, friction;
+    float normalImpulse, tangentImpulse1, tangentImpulse2;
+    tcontact_t* src;
+} tc_t;
+
+static inline float tc_mass(const oc_cloth* c, uint32_t v)
+{
+    return c->type[v] == OC_STATIC ? 0.0f : c->inv_mass[v];
+}
+
+/* InitializeTriangleContactConstraints (cloth_contact_solver.cpp:179-262). */
+static void tc_init(oc_cloth* c, tc_t* x, tcontact_t* k, const v3* pos)
+{
+    x->src = k;
+    x->ia = c->solver_of_vertex[k->p];
+    x->ib = c->solver_of_vertex[k->b];
+    x->ic = c->solver_of_vertex[k->cc];
+    x->id = c->solver_of_vertex[k->d];
+    x->mA = tc_mass(c, k->p);
+    x->mB = tc_mass(c, k->b);
+    x->mC = tc_mass(c, k->cc);
+    x->mD = tc_mass(c, k->d);
+    x->radiusA = c->radius[k->p];
+    x->triangleRadius = c->def[6];
+    x->wB = k->w2;
+    x->wC = k->w3;
+    x->wD = k->w4;
+    v3 xA = pos[x->ia], xB = pos[x->ib], xC = pos[x->ic], xD = pos[x->id];
+    v3 cB = vadd(vadd(vscale(x->wB, xB), vscale(x->wC, xC)), vscale(x->wD, xD));
+    v3 n = vsub(cB, xA);
+    float len = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
+    if (len > kEps) {
+        float s1 = 1.0f / len;
+        n = V(n.x * s1, n.y * s1, n.z * s1);
+    }
+    x->normal = n;
+    float K = x->mA + x->mB * x->wB * x->wB + x->mC * x->wC * x->wC + x->mD * x->wD * x->wD;
+    x->normalMass = K > 0.0f ? 1.0f / K : 0.0f;
+    x->normalImpulse = k->normal_impulse;
+    x->friction = sqrtf(c->friction[k->p] * c->def[7]);
+    x->tangent1 = vperp(n);
+    x->tangent2 = vcross(x->tangent1, n);
+    x->tangentMass1 = x->normalMass;
+    x->tangentMass2 = x->normalMass;
+    x->tangentImpulse1 = k->tangent_impulse1;
+    x->tangentImpulse2 = k->tangent_impulse2;
+}
+
+/* The impulse `lambda` along direction `u` on the four particles. */
+static inline void tc_apply(const tc_t* x, float lambda, v3 u, v3* vA, v3* vB, v3* vC, v3* vD)
+{
+    v3 JA = vneg(u), JB = vscale(x->wB, u), JC = vscale(x->wC, u), JD = vscale(x->wD, u);
+    v3 PA = vscale(lambda, JA), PB = vscale(lambda, JB), PC = vscale(lambda, JC), PD = vscale(lambda, JD);
+    *vA = vadd(*vA, vscale(x->mA, PA));
+    *vB = vadd(*vB, vscale(x->mB, PB));
+    *vC = vadd(*vC, vscale(x->mC, PC));
+    *vD = vadd(*vD, vscale(x->mD, PD));
+}
+
+/* WarmStartTriangleContactConstraints (cloth_contact_solver.cpp:309-386). */
+static void tc_warm_start(const tc_t* x, v3* vel)
+{
+    v3 vA = vel[x->ia], vB = vel[x->ib], vC = vel[x->ic], vD = vel[x->id];
+    tc_apply(x, x->normalImpulse, x->normal, &vA, &vB, &vC, &vD);
+    tc_apply(x, x->tangentImpulse1, x->tangent1, &vA, &vB, &vC, &vD);
+    tc_apply(x, x->tangentImpulse2, x->tangent2, &vA, &vB, &vC, &vD);
+    vel[x->ia] = vA; vel[x->ib] = vB; vel[x->ic] = vC; vel[x->id] = vD;
+}
+
+/* SolveTriangleContactVelocityConstraints (cloth_contact_solver.cpp:474-596). */
+static void tc_solve_velocity(tc_t* x, v3* vel)
+{
+    v3 vA = vel[x->ia], vB = vel[x->ib], vC = vel[x->ic], vD = vel[x->id];
+    {
+        v3 vCB = vadd(vadd(vscale(x->wB, vB), vscale(x->wC, vC)), vscale(x->wD, vD));
+        float Cdot = vdot(vsub(vCB, vA), x->normal);
+        float impulse = -x->normalMass * Cdot;
+        float old = x->normalImpulse;
+        float sum = x->normalImpulse + impulse;
+        x->normalImpulse = sum > 0.0f ? sum : 0.0f;
+        impulse = x->normalImpulse - old;
+        tc_apply(x, impulse, x->normal, &vA, &vB, &vC, &vD);
+    }
+    for (int dir = 0; dir < 2; ++dir) {
+        float hi = x->friction * x->normalImpulse;
+        float lo = -hi;
+        v3 u = dir == 0 ? x->tangent1 : x->tangent2;
+        float* acc = dir == 0 ? &x->tangentImpulse1 : &x->tangentImpulse2;
+        float tm = dir == 0 ? x->tangentMass1 : x->tangentMass2;
+        v3 vCB = vadd(vadd(vscale(x->wB, vB), vscale(x->wC, vC)), vscale(x->wD, vD));
+        float Cdot = vdot(vsub(vCB, vA), u);
+        float impulse = -tm * Cdot;
+        float old = *acc;
+        float a = *acc + impulse;
+        float m = a < hi ? a : hi;   /* b3Clamp = b3Max(lo, b3Min(a, hi)) */
+        *acc = lo > m ? lo : m;
+        impulse = *acc - old;
+        tc_apply(x, impulse, u, &vA, &vB, &vC, &vD);
+    }
+    vel[x->ia] = vA; vel[x->ib] = vB; vel[x->ic] = vC; vel[x->id] = vD;
+}
+
+/* SolveTriangleContactPositionConstraints (cloth_contact_solver.cpp:720-794);
+ * returns the contact's separation. */
+static float tc_solve_position(const tc_t* x, v3* pos)
+{
+    v3 xA = pos[x->ia], xB = pos[x->ib], xC = pos[x->ic], xD = pos[x->id];
+    v3 cB = vadd(vadd(vscale(x->wB, xB), vscale(x->wC, xC)), vscale(x->wD, xD));
+    v3 n = vsub(cB, xA);
+    float distance = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z); /* b3Vec3::Normalize */
+    if (distance > kEps) {
+        float s1 = 1.0f / distance;
+        n = V(n.x * s1, n.y * s1, n.z * s1);
+    }
+    float separation = distance - x->radiusA - x->triangleRadius;
+    float Cv = kBaumgarte * (separation + kLinearSlop);
+    float m = Cv < 0.0f ? Cv : 0.0f;
+    float C = -kMaxLinearCorrection > m ? -kMaxLinearCorrection : m;
+    float K = x->mA + x->mB * x->wB * x->wB + x->mC * x->wC * x->wC + x->mD * x->wD * x->wD;
+    float impulse = K > 0.0f ? -C / K : 0.0f;
+    tc_apply(x, impulse, n, &xA, &xB, &xC, &xD);
+    pos[x->ia] = xA; pos[x->ib] = xB; pos[x->ic] = xC; pos[x->id] = xD;
+    return separation;
+}
+
 typedef struct {
     uint32_t index;     /* solver row */
     float inv_mass, friction, normal_mass;
@@ -1403,8 +1783,18 @@ typedef struct {
  * body-contact functions of cloth_contact_solver.cpp, for static bodies
  * (inverse mass and inertia 0, zero velocity). */
 static void solve_contacts(oc_cloth* c, float h, uint32_t vel_iters, uint32_t pos_iters, v3* pos, v3* vel,
-                           uint32_t* nactive)
+                           uint32_t* nactive, uint32_t* ntactive)
 {
+    /* active particle-triangle contacts in list order (cloth.cpp:532-538) */
+    uint32_t nt = 0;
+    for (uint32_t q = c->ntc; q-- > 0;) nt += c->tcs[q].active != 0;
+    *ntactive = nt;
+    tc_t* tc = (tc_t*)calloc(nt + 1, sizeof(tc_t));
+    {
+        uint32_t w = 0;
+        for (uint32_t q = c->ntc; q-- > 0;)
+            if (c->tcs[q].active) tc_init(c, tc + w++, c->tcs + q, pos);
+    }
     uint32_t na = 0;
     for (uint32_t q = c->ncontact; q-- > 0;) na += c->contacts[q].active != 0;
     *nactive = na;
@@ -1455,7 +1845,8 @@ static void solve_contacts(oc_cloth* c, float h, uint32_t vel_iters, uint32_t po
         vA = vsub(vA, vscale(mA, vadd(P1, P2)));
         vel[x->index] = vA;
     }
-    /* SolveBodyContactVelocityConstraints (:388-472) */
+    for (uint32_t q = 0; q < nt; ++q) tc_warm_start(tc + q, vel);
+    /* SolveBodyContactVelocityConstraints (:388-472), then the triangle contacts */
     for (uint32_t it = 0; it < vel_iters; ++it) {
         for (uint32_t q = 0; q < na; ++q) {
             bc_t* x = bc + q;
@@ -1502,11 +1893,17 @@ static void solve_contacts(oc_cloth* c, float h, uint32_t vel_iters, uint32_t po
             }
             vel[x->index] = vA;
         }
+        for (uint32_t q = 0; q < nt; ++q) tc_solve_velocity(tc + q, vel);
     }
-    /* StoreImpulses (:598-607) */
+    /* StoreImpulses (:598-616) */
     for (uint32_t q = 0; q < na; ++q) {
         bc[q].src->normal_impulse = bc[q].normal_impulse;
         bc[q].src->tangent_impulse = bc[q].tangent_impulse;
+    }
+    for (uint32_t q = 0; q < nt; ++q) {
+        tc[q].src->normal_impulse = tc[q].normalImpulse;
+        tc[q].src->tangent_impulse1 = tc[q].tangentImpulse1;
+        tc[q].src->tangent_impulse2 = tc[q].tangentImpulse2;
     }
     /* integrate positions (cloth_solver.cpp:143-147) */
     for (uint32_t k = 0; k < c->n; ++k) pos[k] = vadd(pos[k], vscale(h, vel[k]));
@@ -1530,16 +1927,24 @@ static void solve_contacts(oc_cloth* c, float h, uint32_t vel_iters, uint32_t po
             cA = vsub(cA, vscale(mA, P));
             pos[x->index] = cA;
         }
-        if (minSeparation >= -3.0f * kLinearSlop) break;
+        float minTri = 0.0f;
+        for (uint32_t q = 0; q < nt; ++q) {
+            float sep = tc_solve_position(tc + q, pos);
+            minTri = minTri < sep ? minTri : sep;
+        }
+        if (minSeparation >= -3.0f * kLinearSlop && minTri >= -3.0f * kLinearSlop) break;
     }
     free(bc);
+    free(tc);
 }
 
 /* ------------------------------------------------------------------------ */
 /* step                                                                      */
 /* ------------------------------------------------------------------------ */
 
-/* b3Cloth::Step (cloth.cpp:551-601) without the self-collision pass, with
+/* b3Cloth::Step (cloth.cpp:551-601), its self-collision pass run only when
+ * the thickness is above zero (below that no particle-triangle contact can
+ * become active), with
  * b3Cloth::Solve (:507-549), b3ClothSolver::Solve (cloth_solver.cpp:78-193)
  * and b3ClothForceSolver::Solve (cloth_force_solver.cpp:138-222). */
 void oc_step(oc_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, oc_step_info* info)
@@ -1548,6 +1953,7 @@ void oc_step(oc_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, oc_s
     oc_step_info local;
     memset(&local, 0, sizeof(local));
 
+    if (self_collision(c)) update_cloth_contacts(c);
     update_body_contacts(c);
 
     if (dt > 0.0f) {
@@ -1568,7 +1974,7 @@ void oc_step(oc_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, oc_s
             pos[k] = vadd(c->sx[k], c->sy[k]);
             c->mx[i] = c->dvsol[k];
         }
-        solve_contacts(c, h, vel_iters, pos_iters, pos, vel, &local.active_contacts);
+        solve_contacts(c, h, vel_iters, pos_iters, pos, vel, &local.active_contacts, &local.active_tri_contacts);
         for (uint32_t k = 0; k < n; ++k) {
             uint32_t i = c->order[k];
             c->x[i] = pos[k];
@@ -1585,8 +1991,18 @@ void oc_step(oc_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, oc_s
         uint32_t i = c->order[k];
         move_proxy(c, i, vscale(dt, c->v[i]));
     }
+    if (self_collision(c)) {
+        /* triangle proxies (cloth.cpp:580-597), then FindNewClothContacts */
+        for (uint32_t k = 0; k < c->t; ++k) {
+            v3 v1 = c->v[c->tris[3 * k]], v2 = c->v[c->tris[3 * k + 1]], v3_ = c->v[c->tris[3 * k + 2]];
+            v3 velocity = vdiv(vadd(vadd(v1, v2), v3_), 3.0f);
+            move_triangle_proxy(c, k, vscale(dt, velocity));
+        }
+        find_new_cloth_contacts(c);
+    }
     find_new_body_contacts(c);
     local.contacts = c->ncontact;
+    local.tri_contacts = c->ntc;
     if (info) *info = local;
 }
 
@@ -1686,6 +2102,26 @@ uint32_t oc_get_contacts(const oc_cloth* c, uint8_t* exists, uint8_t* active, fl
         }
     }
     return c->ncontact;
+}
+
+/* Particle-triangle contacts in list order (head first): particle and
+ * triangle (2 per contact), active flag, barycentric weights w2, w3, w4 and
+ * the normal and two tangent impulses (3 each).  Any pointer may be null. */
+uint32_t oc_get_tri_contacts(const oc_cloth* c, uint32_t* pt, uint8_t* active, float* w, float* impulses)
+{
+    uint32_t k = 0;
+    for (uint32_t q = c->ntc; q-- > 0; ++k) {
+        const tcontact_t* x = c->tcs + q;
+        if (pt) { pt[2 * k] = x->p; pt[2 * k + 1] = x->t; }
+        if (active) active[k] = (uint8_t)(x->active != 0);
+        if (w) { w[3 * k] = x->w2; w[3 * k + 1] = x->w3; w[3 * k + 2] = x->w4; }
+        if (impulses) {
+            impulses[3 * k] = x->normal_impulse;
+            impulses[3 * k + 1] = x->tangent_impulse1;
+            impulses[3 * k + 2] = x->tangent_impulse2;
+        }
+    }
+    return k;
 }
 
 uint32_t oc_build_system(oc_cloth* c, float dt)

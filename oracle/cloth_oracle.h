@@ -50,6 +50,8 @@ typedef struct {
     double b_delta;          /* b^T P^-1 b, filtered */
     uint32_t active_contacts;/* body contacts handed to the solver */
     uint32_t contacts;       /* body contacts alive after the step */
+    uint32_t active_tri_contacts; /* particle-triangle contacts handed to the solver */
+    uint32_t tri_contacts;        /* particle-triangle contacts alive after the step */
 } oc_step_info;
 
 /* def: density, streching, shearing, bending, sewing, damping, thickness, friction */
@@ -77,6 +79,7 @@ void oc_get_state(const oc_cloth* c, float* x, float* v, float* dv, float* mass,
 float oc_energy(const oc_cloth* c);
 uint32_t oc_describe(const oc_cloth* c, float* tri_rest, float* fat_aabb, float* force_desc);
 uint32_t oc_get_contacts(const oc_cloth* c, uint8_t* exists, uint8_t* active, float* impulses);
+uint32_t oc_get_tri_contacts(const oc_cloth* c, uint32_t* pt, uint8_t* active, float* w, float* impulses);
 uint32_t oc_force_count(const oc_cloth* c);
 uint32_t oc_spring_count(const oc_cloth* c);
 /* Springs in creation order: vertex pairs (2 per spring) and rest lengths. */

@@ -58,6 +58,7 @@
 #include <bounce/cloth/forces/spring_force.h>
 #include <bounce/cloth/forces/mouse_force.h>
 #include <bounce/cloth/contacts/cloth_particle_body_contact.h>
+#include <bounce/cloth/contacts/cloth_particle_triangle_contact.h>
 #include <bounce/sparse/dense_vec3.h>
 #include <bounce/sparse/diag_mat33.h>
 #include <bounce/sparse/sparse_mat33.h>
@@ -634,6 +635,35 @@ uint32_t ref_cloth_get_contacts(void* hp, uint8_t* exists, uint8_t* active, floa
         }
     }
     return count;
+}
+
+// Particle-triangle contacts in list order (head first): particle vertex and
+// triangle index (2 per contact), active flag, barycentric weights
+// m_w2, m_w3, m_w4 and the normal and two tangent impulses.  Any pointer may
+// be null.  Returns the number of contacts.
+uint32_t ref_cloth_get_tri_contacts(void* hp, uint32_t* pt, uint8_t* active, float* w, float* impulses)
+{
+    RefCloth* h = (RefCloth*)hp;
+    uint32_t k = 0;
+    for (b3ParticleTriangleContact* c = h->cloth->m_contactManager.m_particleTriangleContactList.m_head; c;
+         c = c->m_next, ++k) {
+        if (pt) {
+            pt[2 * k] = c->m_p1->m_vertex;
+            pt[2 * k + 1] = c->m_t2->m_triangle;
+        }
+        if (active) active[k] = c->m_active ? 1 : 0;
+        if (w) {
+            w[3 * k] = c->m_w2;
+            w[3 * k + 1] = c->m_w3;
+            w[3 * k + 2] = c->m_w4;
+        }
+        if (impulses) {
+            impulses[3 * k] = c->m_normalImpulse;
+            impulses[3 * k + 1] = c->m_tangentImpulse1;
+            impulses[3 * k + 2] = c->m_tangentImpulse2;
+        }
+    }
+    return k;
 }
 
 // Assemble A and b exactly as one force solve would (the gather of
