@@ -18,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
-from bounce_b200.meshes import pinned_block_scene, plain_scene, sphere_scene  # noqa: E402
+from bounce_b200.meshes import pinned_block_scene, plain_scene, self_collision_scene, sphere_scene  # noqa: E402
 
 
 def trajectory(scene, steps, keep):
@@ -43,6 +43,29 @@ def trajectory(scene, steps, keep):
                 out[f"contact_impulses_{k}"] = cts["impulses"]
     out["iterations"] = np.asarray(iters, np.uint32)
     out["mass"] = ref.state()["mass"]
+    return out
+
+
+def self_collision(scene, steps, keep):
+    """The reference's full b3Cloth::Step (self-collision included) on the
+    self-collision scene: states and the particle-triangle contact list (list
+    order; weights only where active) at the kept steps."""
+    ref = oracle.RefCloth(scene.mesh, scene.cdef, restated=False).setup(scene)
+    a, b, r, mu = scene.capsules[0]
+    out = {"vertices": scene.mesh.vertices, "triangles": scene.mesh.triangles, "def": scene.cdef.as_array(),
+           "capsule": np.array([*a, *b, r, mu], np.float32), "dt": np.float32(scene.dt)}
+    iters = []
+    for k in range(1, steps + 1):
+        iters.append(ref.step(scene.dt, scene.velocity_iterations, scene.position_iterations, full=True)["iterations"])
+        if k in keep:
+            s = ref.state()
+            out[f"x_{k}"], out[f"v_{k}"], out[f"dv_{k}"] = s["x"], s["v"], s["dv"]
+            c = ref.tri_contacts()
+            w = c["w"].copy()
+            w[c["active"] == 0] = 0.0
+            out[f"tc_pt_{k}"], out[f"tc_active_{k}"] = c["pt"], c["active"]
+            out[f"tc_w_{k}"], out[f"tc_impulses_{k}"] = w, c["impulses"]
+    out["iterations"] = np.asarray(iters, np.uint32)
     return out
 
 
@@ -99,6 +122,7 @@ def main():
         "plain32_ref.npz": trajectory(plain_scene(32, seed=1), 30, {1, 10, 30}),
         "sphere32_ref.npz": trajectory(sphere_scene(32, seed=2), 40, {1, 20, 30, 40}),
         "system16_bend_ref.npz": system(sphere_scene(16, seed=4)),
+        "self_collision11_ref.npz": self_collision(self_collision_scene(11), 130, {1, 60, 90, 100, 115, 130}),
     }
     only = set(sys.argv[1:])
     for name, data in files.items():

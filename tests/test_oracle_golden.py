@@ -82,3 +82,36 @@ def test_oracle_relative_mode_converges(port, dot):
     for _ in range(5):
         info = c.step(scene.dt)
         assert info["iterations"] == 50 or info["delta"] <= 1e-8 * info["b_delta"] * (1 + 1e-6)
+
+
+def self_collision_golden_scene(d):
+    """The scene of self_collision11_ref.npz (a cloth folding over a capsule
+    with thickness 0.2)."""
+    mesh = Mesh(d["vertices"], d["triangles"])
+    cdef = ClothDef(*[float(x) for x in d["def"]])
+    c = [float(x) for x in d["capsule"]]
+    return Scene("golden_self", mesh, cdef, np.zeros(0, np.uint32), capsules=[(c[0:3], c[3:6], c[6], c[7])],
+                 dt=float(d["dt"]))
+
+
+def test_oracle_self_collision_bit_exact(port):
+    """Particle-triangle contacts: the restatement reproduces the reference's
+    trajectory and its contact list (order, active flags, weights of active
+    contacts, impulses) at the kept steps."""
+    d = np.load(os.path.join(GOLDEN, "self_collision11_ref.npz"))
+    scene = self_collision_golden_scene(d)
+    c = port.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    for k in range(1, len(d["iterations"]) + 1):
+        assert c.step(scene.dt)["iterations"] == d["iterations"][k - 1], k
+        if f"x_{k}" in d:
+            s = c.state()
+            for q in ("x", "v", "dv"):
+                assert np.array_equal(s[q], d[f"{q}_{k}"]), (k, q)
+            t = c.tri_contacts()
+            w = t["w"].copy()
+            w[t["active"] == 0] = 0.0
+            assert np.array_equal(t["pt"], d[f"tc_pt_{k}"]), k
+            assert np.array_equal(t["active"], d[f"tc_active_{k}"]), k
+            assert np.array_equal(w, d[f"tc_w_{k}"]), k
+            assert np.array_equal(t["impulses"], d[f"tc_impulses_{k}"]), k
+    assert int(d["tc_active_100"].sum()) > 10

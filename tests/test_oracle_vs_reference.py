@@ -166,3 +166,46 @@ def test_particle_edits_match_reference():
         for q in ("x", "v", "dv", "type"):
             assert np.array_equal(sr[q], sp[q]), (step, q)
         assert ref.contacts()["count"] == port.contacts()["count"]
+
+
+def _same_tri_contacts(a, b):
+    ca, cb = a.tri_contacts(), b.tri_contacts()
+    assert ca["count"] == cb["count"]
+    for k in ("pt", "active", "impulses"):
+        assert np.array_equal(ca[k], cb[k]), k
+    # an inactive contact's weights are stale (never set for a new contact)
+    on = ca["active"] != 0
+    assert np.array_equal(ca["w"][on], cb["w"][on])
+    return ca
+
+
+@pytest.mark.parametrize("edit_from", [None, 84])
+def test_self_collision_matches_reference(edit_from):
+    """Thickness 0.2: the reference's full b3Cloth::Step with its
+    particle-triangle contacts (cloth_contact_manager.cpp, broad_phase.h
+    FindPairs, cloth_particle_triangle_contact.cpp, cloth_contact_solver.cpp)
+    against the restatement, bit for bit: positions, velocities, and the
+    contact list in list order with active flags, barycentric weights and
+    impulses.  With edit_from set, the particle edit script runs while the
+    cloth is folding (type changes drop a particle's contacts and touch its
+    proxy; position edits move its triangles' proxies)."""
+    import edit_script
+    from bounce_b200.meshes import self_collision_scene
+
+    scene = self_collision_scene(11)
+    ref = oracle.RefCloth(scene.mesh, scene.cdef, restated=False).setup(scene)
+    port = oracle.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    most_active, most = 0, 0
+    for step in range(130):
+        if edit_from is not None:
+            x = ref.state()["x"]
+            edit_script.apply(ref, step - edit_from, x, gpu=False)
+            edit_script.apply(port, step - edit_from, x, gpu=False)
+        assert ref.step(scene.dt, full=True)["iterations"] == port.step(scene.dt)["iterations"]
+        sr, sp = ref.state(), port.state()
+        for q in ("x", "v", "dv", "type"):
+            assert np.array_equal(sr[q], sp[q]), (step, q)
+        c = _same_tri_contacts(ref, port)
+        most = max(most, c["count"])
+        most_active = max(most_active, int(c["active"].sum()))
+    assert most > 500 and most_active > 50
