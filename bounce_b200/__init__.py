@@ -167,6 +167,8 @@ def lib() -> C.CDLL:
             "b3g_cloth_read_masses": [vp, vp],
             "b3g_cloth_get_energy": [vp, C.POINTER(f32)],
             "b3g_cloth_read_contacts": [vp, vp, vp, vp],
+            "b3g_cloth_read_tri_contacts": [vp, C.POINTER(u32), vp, vp, vp, vp],
+            "b3g_cloth_get_self_stats": [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)],
             "b3g_cloth_last_stats": [vp, C.POINTER(StepStatsC)],
             "b3g_cloth_read_system": [vp, C.POINTER(u32), vp, vp, vp, vp, vp, vp],
             "b3g_cloth_step_profiled": [vp, f32, u32, u32, C.POINTER(PhaseTimesC), C.POINTER(StepStatsC)],
@@ -478,6 +480,27 @@ class Cloth:
         check(lib().b3g_cloth_read_contacts(self.h, _ptr(ex), _ptr(ac), _ptr(imp)), "read_contacts")
         return {"exists": ex[: self.nsph * self.n], "active": ac[: self.nsph * self.n],
                 "impulses": imp[: self.nsph * self.n]}
+
+    def tri_contacts(self) -> dict:
+        """Particle-triangle contacts (thickness > 0) in list order, head
+        first: (particle, triangle) pairs, active flags, weights w2, w3, w4
+        (zero while inactive), impulses (normal, tangent 1, tangent 2)."""
+        cnt = C.c_uint32(0)
+        L = lib()
+        check(L.b3g_cloth_read_tri_contacts(self.h, C.byref(cnt), None, None, None, None), "read_tri_contacts")
+        m = cnt.value
+        pt = np.zeros((max(m, 1), 2), np.uint32)
+        ac = np.zeros(max(m, 1), np.uint8)
+        w = np.zeros((max(m, 1), 3), np.float32)
+        imp = np.zeros((max(m, 1), 3), np.float32)
+        check(L.b3g_cloth_read_tri_contacts(self.h, C.byref(cnt), _ptr(pt), _ptr(ac), _ptr(w), _ptr(imp)),
+              "read_tri_contacts")
+        return {"count": m, "pt": pt[:m], "active": ac[:m], "w": w[:m], "impulses": imp[:m]}
+
+    def self_stats(self) -> dict:
+        a, b, c = C.c_uint32(0), C.c_uint32(0), C.c_uint32(0)
+        check(lib().b3g_cloth_get_self_stats(self.h, C.byref(a), C.byref(b), C.byref(c)), "get_self_stats")
+        return {"contacts": a.value, "active": b.value, "levels": c.value}
 
     def system(self) -> dict:
         nnz = C.c_uint32(0)

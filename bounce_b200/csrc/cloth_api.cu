@@ -195,6 +195,34 @@ b3g_status launch_step_plain(b3g_cloth* c, uint32_t pos_iters)
     return B3G_OK;
 }
 
+// A step of a cloth with self-collision, launched without a graph: the
+// particle-triangle contact list is updated before the solve, the contact
+// phase solves both contact kinds in list order, and the new pairs are found
+// after the proxies moved (b3Cloth::Step, cloth.cpp:551-601).
+b3g_status launch_step_self(b3g_cloth* c, float dt)
+{
+    const int dot = (int)c->opts.dot;
+    cudaStream_t st = c->stream;
+    cudaGraphConditionalHandle none = 0;
+    b3g_status s = self_update(c, st);
+    if (s != B3G_OK) return s;
+    B3G_TRY(launch_contacts_update(c->dev, st));
+    if (dt > 0.0f) {
+        B3G_TRY(launch_assemble(c->dev, c->assemble_block, st));
+        if (c->cg_strategy == B3G_CG_PERSISTENT) {
+            B3G_TRY(cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st));
+            B3G_TRY(launch_grid_cg(c->dev, dot, c->dev.bar, st));
+        } else {
+            B3G_TRY(launch_cg_init(c->dev, dot, none, 0, st));
+            for (uint32_t k = 0; k < c->opts.max_iterations; ++k)
+                B3G_TRY(launch_cg_iteration(c->dev, dot, none, 0, st));
+        }
+        if ((s = self_solve(c, st)) != B3G_OK) return s;
+    }
+    B3G_TRY(launch_post(c->dev, st));
+    return self_find(c, st);
+}
+
 bool valid(const b3g_cloth* c) { return c != nullptr && c->dev.n > 0; }
 
 }  // namespace
@@ -496,6 +524,7 @@ b3g_status b3g_cloth_create(const b3g_mesh_desc* mesh, const b3g_cloth_def* def,
         return e == cudaErrorMemoryAllocation ? B3G_ERR_OUT_OF_MEMORY : from_cuda(e);
     }
     s = realize_cloth(c, device, base, true, nullptr, true);
+    if (s == B3G_OK && def->thickness > 0.0f) s = self_attach(c);
     if (s != B3G_OK) {
         b3g_cloth_destroy(c);
         return s;
@@ -517,6 +546,7 @@ b3g_status destroy_cloth(b3g_cloth* c)
 {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    self_free(c);
     destroy_graph(c);
     if (c->arena.base && c->owns_arena) cudaFree(c->arena.base);
     if (c->d_ops) cudaFree(c->d_ops);
@@ -800,6 +830,7 @@ extern "C" {
 
 b3g_status b3g_cloth_create_particle(b3g_cloth* c, const b3g_particle_def* def, uint32_t* index)
 {
+    if (c && c->self) return B3G_ERR_UNSUPPORTED;  // not with self-collision
     if (!editable(c) || !def || !index) return B3G_ERR_INVALID_ARGUMENT;
     for (int q = 0; q < 3; ++q)
         if (!std::isfinite(def->position[q]) || !std::isfinite(def->velocity[q]) || !std::isfinite(def->force[q]))
@@ -840,6 +871,7 @@ b3g_status b3g_cloth_create_particle(b3g_cloth* c, const b3g_particle_def* def, 
 
 b3g_status b3g_cloth_destroy_particle(b3g_cloth* c, uint32_t index)
 {
+    if (c && c->self) return B3G_ERR_UNSUPPORTED;  // not with self-collision
     if (!editable(c)) return B3G_ERR_INVALID_ARGUMENT;
     const uint32_t n_mesh = c->topo.n_mesh;
     if (index < n_mesh || index >= c->dev.n) return B3G_ERR_INVALID_ARGUMENT;  // only created particles
@@ -873,6 +905,7 @@ b3g_status b3g_cloth_destroy_particle(b3g_cloth* c, uint32_t index)
 
 b3g_status b3g_cloth_create_mouse_force(b3g_cloth* c, const b3g_mouse_force_def* def, uint32_t* force_id)
 {
+    if (c && c->self) return B3G_ERR_UNSUPPORTED;  // not with self-collision
     if (!editable(c) || !def || !force_id) return B3G_ERR_INVALID_ARGUMENT;
     if (def->particle >= c->dev.n || def->triangle >= c->dev.t) return B3G_ERR_INVALID_ARGUMENT;
     if (!std::isfinite(def->w2) || !std::isfinite(def->w3) || !std::isfinite(def->w4) ||
@@ -896,6 +929,7 @@ b3g_status b3g_cloth_create_mouse_force(b3g_cloth* c, const b3g_mouse_force_def*
 
 b3g_status b3g_cloth_destroy_force(b3g_cloth* c, uint32_t force_id)
 {
+    if (c && c->self) return B3G_ERR_UNSUPPORTED;  // not with self-collision
     if (!editable(c)) return B3G_ERR_INVALID_ARGUMENT;
     size_t m = 0;
     while (m < c->mouse_ids.size() && c->mouse_ids[m] != force_id) ++m;
@@ -1066,7 +1100,9 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
     h->gz = c->gravity[2];
     B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, st));
     B3G_TRY(cudaEventRecord(c->ev0, st));
-    if (dt > 0.0f) {
+    if (c->self) {
+        if ((s = launch_step_self(c, dt)) != B3G_OK) return s;
+    } else if (dt > 0.0f) {
         if (c->graph_ok && (!c->exec || c->graph_dot != (int)c->opts.dot || c->graph_pos_iters != pos_iters ||
                             c->graph_nsph != c->dev.nsph || c->graph_strategy != c->cg_strategy)) {
             if (build_graph(c, pos_iters) != B3G_OK) c->graph_ok = false;
@@ -1094,7 +1130,7 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
     L.active_contacts = h->active_contacts;
     L.contacts = h->contacts;
     L.step_ms = ms;
-    if (dt > 0.0f && c->graph_ok && c->exec) {
+    if (dt > 0.0f && !c->self && c->graph_ok && c->exec) {
         // kernel nodes the graph ran: [contacts_update] assemble cg_init,
         // 3 per CG iteration, finalize, [contact_position x (pos_iters - 1)], post
         const uint64_t ns = c->dev.nsph ? 1 : 0;
@@ -1128,6 +1164,7 @@ b3g_status b3g_cloth_assemble(b3g_cloth* c, float dt)
 b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters,
                                    b3g_phase_times* times, b3g_step_stats* stats)
 {
+    if (c && c->self) return B3G_ERR_UNSUPPORTED;
     if (!valid(c) || !c->owns_stream || !times || !(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     b3g_status s = flush_ops(c);
@@ -1342,6 +1379,21 @@ b3g_status b3g_cloth_read_contacts(const b3g_cloth* cc, uint8_t* exists, uint8_t
             for (int k = 0; k < 3; ++k) impulses[3 * q + k] = tmp[k * nn + q];
     }
     B3G_TRY(cudaStreamSynchronize(c->stream));
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_read_tri_contacts(const b3g_cloth* c, uint32_t* count, uint32_t* pairs, uint8_t* active,
+                                       float* weights, float* impulses)
+{
+    if (!valid(c) || !count) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    return self_read(c, count, pairs, active, weights, impulses);
+}
+
+b3g_status b3g_cloth_get_self_stats(const b3g_cloth* c, uint32_t* contacts, uint32_t* active, uint32_t* levels)
+{
+    if (!valid(c) || !contacts || !active || !levels) return B3G_ERR_INVALID_ARGUMENT;
+    self_stats(c, contacts, active, levels);
     return B3G_OK;
 }
 

@@ -116,6 +116,13 @@ struct ClothDev {
     void* partials;             // reduction partials, >= max(grid, persistent CG blocks) * 32 bytes
     uint32_t grid;              // blocks of the row kernels
     uint32_t block;             // threads of the row kernels
+
+    // self-collision (thickness > 0, single cloths only; null otherwise):
+    // triangle fat AABBs (3 planes of t each) and the broadphase move buffer
+    // as flags, and the particles whose particle-triangle contacts a type
+    // change dropped (removed at the next contact update)
+    float *tri_lo, *tri_hi;
+    uint8_t *t_moved, *p_moved, *p_purge;
 };
 
 // A launch over several cloths: global thread g works on row

@@ -11,6 +11,8 @@
 
 namespace b3g {
 
+struct SelfState;
+
 // One device arena per cloth, carved into 256-byte aligned buffers.
 struct Arena {
     char* base = nullptr;
@@ -86,6 +88,8 @@ struct b3g_cloth {
     std::vector<uint32_t> mouse_ids;          // the id of each
     uint32_t next_force_id = 0;
     uint32_t layout_version = 0;              // bumped on every new layout (batches rebuild their graphs)
+
+    b3g::SelfState* self = nullptr;           // particle-triangle contacts (thickness > 0)
 };
 
 
@@ -97,5 +101,18 @@ b3g_status layout_cloth(b3g_cloth* c);
 b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, cudaStream_t st, bool own_stream);
 void finish_upload(b3g_cloth* c);
 b3g_status destroy_cloth(b3g_cloth* c);
+
+// Self-collision (self_collision.cu): set up for a cloth whose thickness is
+// above zero, free, and the three phases of a step.
+namespace b3g {
+b3g_status self_attach(b3g_cloth* c);
+void self_free(b3g_cloth* c);
+b3g_status self_update(b3g_cloth* c, cudaStream_t st);
+b3g_status self_solve(b3g_cloth* c, cudaStream_t st);
+b3g_status self_find(b3g_cloth* c, cudaStream_t st);
+b3g_status self_read(const b3g_cloth* c, uint32_t* count, uint32_t* pairs, uint8_t* active, float* weights,
+                     float* impulses);
+void self_stats(const b3g_cloth* c, uint32_t* contacts, uint32_t* active, uint32_t* levels);
+}  // namespace b3g
 b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, float dt, uint32_t vel_iters,
                            uint32_t pos_iters, b3g_step_stats* per_cloth, b3g_batch_stats* stats, bool use_graph);

@@ -24,6 +24,7 @@
 
 #include "cg_common.cuh"
 #include "cloth_dev.cuh"
+#include "self_collision.cuh"
 #include "sell_spmv.cuh"
 #include "vec.cuh"
 
@@ -958,6 +959,7 @@ __device__ void move_proxy_dev(const ClothDev& c, uint32_t i, f3 disp)
     }
     c.fat_lo[i] = lo[0]; c.fat_lo[n + i] = lo[1]; c.fat_lo[2 * n + i] = lo[2];
     c.fat_hi[i] = hi[0]; c.fat_hi[n + i] = hi[1]; c.fat_hi[2 * n + i] = hi[2];
+    if (c.p_moved) c.p_moved[i] = 1;  // BufferMove
 }
 
 // Clear f and y, sync the particle AABB (b3BroadPhase::MoveProxy,
@@ -1019,8 +1021,13 @@ __device__ void set_type_dev(const ClothDev& c, uint32_t i, uint8_t type)
         st3(c.v, n, i, zero3());
         st3(c.y, n, i, zero3());
         move_proxy_dev(c, i, zero3());
+        if (c.p_moved) sync_vertex_triangles_dev(c, i);
     }
     destroy_contacts_dev(c, i);
+    if (c.p_moved) {
+        c.p_purge[i] = 1;   // DestroyContacts (particle.cpp:103-118)
+        c.p_moved[i] = 1;   // TouchProxy
+    }
 }
 
 __global__ void k_particle_ops(ClothDev c, const ParticleOp* ops, uint32_t count)
@@ -1039,6 +1046,7 @@ __global__ void k_particle_ops(ClothDev c, const ParticleOp* ops, uint32_t count
                 st3(c.x, n, i, a);
                 st3(c.y, n, i, zero3());
                 move_proxy_dev(c, i, d);
+                if (c.p_moved) sync_vertex_triangles_dev(c, i);
                 break;
             }
             case OP_SET_VELOCITY:  // particle.h:221-228

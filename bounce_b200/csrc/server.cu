@@ -275,6 +275,7 @@ b3g_status b3g_server_submit(b3g_server* s, const b3g_mesh_desc* mesh, const b3g
     if (!s || !mesh || !def || !mesh->vertices || !mesh->triangles || mesh->vertex_count == 0 ||
         mesh->triangle_count == 0 || steps == 0 || (sphere_count && !spheres) || sphere_count > kMaxSpheres)
         return B3G_ERR_INVALID_ARGUMENT;
+    if (def->thickness > 0.0f) return B3G_ERR_UNSUPPORTED;  // self-collision runs on single cloths only
     Request* r = new (std::nothrow) Request();
     if (!r) return B3G_ERR_OUT_OF_MEMORY;
     r->verts.assign(mesh->vertices, mesh->vertices + 3 * (size_t)mesh->vertex_count);

@@ -250,6 +250,22 @@ b3g_status b3g_cloth_get_energy(const b3g_cloth* cloth, float* energy);
  * sphere_count bytes each), impulses (normal, tangent1, tangent2). */
 b3g_status b3g_cloth_read_contacts(const b3g_cloth* cloth, uint8_t* exists, uint8_t* active,
                                    float* impulses);
+/* Self-collision: the particle-triangle contacts of a cloth whose thickness
+ * is above zero (b3ClothContactManager::m_particleTriangleContactList,
+ * include/bounce/cloth/cloth_contact_manager.h; b3ParticleTriangleContact,
+ * include/bounce/cloth/contacts/cloth_particle_triangle_contact.h), in list
+ * order (head first).  *count gets the list length; each non-null array gets
+ * per contact: the particle and triangle (2 u32), the active flag, the
+ * barycentric weights m_w2, m_w3, m_w4 (zero while inactive) and the normal
+ * and two tangent impulses.  A cloth of thickness 0 has no such contacts.
+ * Cloths with self-collision take neither created particles nor mouse forces
+ * (B3G_ERR_UNSUPPORTED), and cannot join a batch or a server. */
+b3g_status b3g_cloth_read_tri_contacts(const b3g_cloth* cloth, uint32_t* count, uint32_t* pairs, uint8_t* active,
+                                       float* weights, float* impulses);
+/* Of the last step: particle-triangle contacts alive after it, active ones
+ * handed to its contact solve, and the dependency levels that solve ran. */
+b3g_status b3g_cloth_get_self_stats(const b3g_cloth* cloth, uint32_t* contacts, uint32_t* active,
+                                    uint32_t* levels);
 b3g_status b3g_cloth_last_stats(const b3g_cloth* cloth, b3g_step_stats* stats);
 
 /* ---- inspection of the assembled system ----------------------------------- */

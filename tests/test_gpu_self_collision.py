@@ -1,0 +1,117 @@
+"""Self-collision on the GPU (thickness > 0: particle-triangle contacts)
+against the oracle, which matches the reference's full b3Cloth::Step bit for
+bit (tests/test_oracle_vs_reference.py, tests/test_oracle_golden.py).
+
+Tolerances: each step starts the oracle from the GPU's positions,
+velocities and CG warm start.  The CG dot products are summed in another
+order on the GPU, so x and v agree within 1e-4 relative (as every other
+per-step test), and the contact list -- which pairs, in which order, which
+are active -- agrees except where a proxy sits within rounding of an AABB
+boundary: at least 98% of the list entries are the same pair at the same
+position, the lengths within 1%.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(b3g, port, scene, opts=None):
+    gpu = b3g.Cloth(scene.mesh, scene.cdef).setup(scene, opts)
+    ora = port.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    if opts is not None:
+        ora.set_solver(opts.stop_rule, opts.tolerance, opts.max_iterations, opts.dot)
+    return gpu, ora
+
+
+def _compare_lists(g, o, step):
+    assert abs(g["count"] - o["count"]) <= max(2, o["count"] // 100), (step, g["count"], o["count"])
+    m = min(g["count"], o["count"])
+    if m == 0:
+        return 1.0
+    same = np.all(g["pt"][:m] == o["pt"][:m], axis=1)
+    frac = float(same.mean())
+    assert frac >= 0.98, (step, frac)
+    ga, oa = int(g["active"].sum()), int(o["active"].sum())
+    assert abs(ga - oa) <= max(2, oa // 50), (step, ga, oa)
+    # where both hold the same active pair, the weights match closely
+    both = same & (g["active"][:m] != 0) & (o["active"][:m] != 0)
+    if both.any():
+        assert np.abs(g["w"][:m][both] - o["w"][:m][both]).max() <= 1e-3, step
+    return frac
+
+
+@pytest.mark.parametrize("edit_from", [None, 84])
+def test_self_collision_per_step(b3g, port, edit_from):
+    """The reference's self-collision scene (a 11 x 11 cloth of 1 m spacing,
+    thickness 0.2, folding over a capsule), 130 steps; with edit_from set the
+    particle edit script (type changes, position and velocity edits) runs
+    while the cloth folds."""
+    import edit_script
+
+    scene = b3g.self_collision_scene(11)
+    gpu, ora = _pair(b3g, port, scene)
+    most_active = 0
+    fracs = []
+    for step in range(130):
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        if edit_from is not None:
+            edit_script.apply(gpu, step - edit_from, st["x"], gpu=True)
+            edit_script.apply(ora, step - edit_from, st["x"], gpu=False)
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        assert abs(g["iterations"] - o["iterations"]) <= 1, (step, g["iterations"], o["iterations"])
+        gs, os_ = gpu.state(), ora.state()
+        assert rel_err(gs["x"], os_["x"]) <= 1e-4, step
+        assert rel_err(gs["v"], os_["v"]) <= 1e-4, step
+        tg, to = gpu.tri_contacts(), ora.tri_contacts()
+        fracs.append(_compare_lists(tg, to, step))
+        most_active = max(most_active, int(to["active"].sum()))
+        s = gpu.self_stats()
+        assert s["contacts"] == tg["count"]
+    print("self-collision: most active contacts", most_active, "worst list agreement", min(fracs))
+    assert most_active > 40  # the cloth did fold onto itself
+
+
+def test_self_collision_against_reference_golden(b3g, port):
+    """The reference's own trajectory (golden file): the GPU runs free from
+    the same start; before the fold (no active self contact yet) positions
+    stay within 1e-4 m, and the contact list matches exactly there."""
+    import os
+
+    from test_oracle_golden import GOLDEN, self_collision_golden_scene
+
+    d = np.load(os.path.join(GOLDEN, "self_collision11_ref.npz"))
+    scene = self_collision_golden_scene(d)
+    gpu = b3g.Cloth(scene.mesh, scene.cdef).setup(scene)
+    for k in range(1, 61):
+        gpu.step(scene.dt)
+        if f"x_{k}" in d:
+            assert np.abs(gpu.state()["x"] - d[f"x_{k}"]).max() <= 1e-4, k
+            t = gpu.tri_contacts()
+            assert np.array_equal(t["pt"], d[f"tc_pt_{k}"]), k
+            assert np.array_equal(t["active"], d[f"tc_active_{k}"]), k
+
+
+def test_self_collision_levels_and_limits(b3g):
+    """The solve reports its dependency levels; cloths with self-collision
+    take no created particles and join no batch."""
+    scene = b3g.self_collision_scene(11)
+    gpu = b3g.Cloth(scene.mesh, scene.cdef).setup(scene)
+    levels = 0
+    for _ in range(100):
+        gpu.step(scene.dt)
+        s = gpu.self_stats()
+        if s["active"]:
+            assert 1 <= s["levels"] <= s["active"]
+            levels = max(levels, s["levels"])
+    assert levels >= 2
+    with pytest.raises(b3g.B3gError):
+        gpu.create_particle((0.0, 6.0, 0.0), mass=0.0)
+    batch = b3g.Batch(4)
+    with pytest.raises(b3g.B3gError):
+        batch.step([gpu], scene.dt)
+    batch.close()
