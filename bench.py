@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--skip-single", action="store_true")
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-softbody", action="store_true")
+    ap.add_argument("--skip-self", action="store_true")
+    ap.add_argument("--self-side", type=int, default=24)
     ap.add_argument("--softbody-side", type=int, default=40)
     ap.add_argument("--softbody-steps", type=int, default=10)
     return ap.parse_args()
@@ -363,6 +365,54 @@ def run_softbody(args, dev: int, cpu_sample: bool):
     return out
 
 
+def run_self_collision(args, dev: int, cpu_sample: bool):
+    """Self-collision (thickness 0.2): the reference's self-collision scene
+    scaled to a side x side grid of 1 m spacing over a capsule as long as the
+    cloth.  Steps 0-59 fall (contacts exist, none active); steps 60-119, the
+    fold, are timed on the GPU with CUDA events.  The CPU figure is the
+    reference's own full b3Cloth::Step on the same cloth over the same 60
+    steps, one core."""
+    import bounce_b200 as b3g
+
+    scene = b3g.self_collision_scene(args.self_side)
+    cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene)
+    lo, hi = 60, 120
+    for _ in range(lo):
+        cloth.step(scene.dt)
+    launches0 = b3g.kernel_launch_count()
+    ms, contacts, active, levels = [], [], [], []
+    for _ in range(lo, hi):
+        ms.append(cloth.step(scene.dt)["step_ms"])
+        st = cloth.self_stats()
+        contacts.append(st["contacts"])
+        active.append(st["active"])
+        levels.append(st["levels"])
+    launches = b3g.kernel_launch_count() - launches0
+    cloth.close()
+    n = scene.mesh.vertex_count
+    out = {"workload": f"grid{args.self_side}_self_collision_capsule", "vertices": n,
+           "triangles": scene.mesh.triangle_count, "steps": f"{lo}-{hi - 1}",
+           "ms_per_step": sum(ms) / len(ms), "vertex_steps_per_s": n * len(ms) / (sum(ms) / 1e3),
+           "tri_contacts_mean": float(np.mean(contacts)), "active_mean": float(np.mean(active)),
+           "active_max": int(max(active)), "levels_mean": float(np.mean(levels)), "gpu_launches": launches}
+    if cpu_sample:
+        import oracle
+
+        if oracle.ref_available():
+            ref = oracle.RefCloth(scene.mesh, scene.cdef, restated=True).setup(scene)
+            for _ in range(lo):
+                ref.step(scene.dt, full=True)
+            t0 = time.perf_counter()
+            for _ in range(lo, hi):
+                ref.step(scene.dt, full=True)
+            sec = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": n * (hi - lo) / sec, "unit": "vertex-steps/s", "cores": 1,
+                                   "kind": "reference",
+                                   "sample": f"the reference's full b3Cloth::Step, steps {lo}-{hi - 1} of the same "
+                                             f"cloth, {1e3 * sec / (hi - lo):.1f} ms/step"}
+    return out
+
+
 def run_serving(args, dev: int):
     from bounce_b200 import serving
 
@@ -457,9 +507,11 @@ def main():
     if args.skip_single:
         batched = None if args.skip_batch else run_batched(args, local)
         served = None if args.skip_serve else run_serving(args, local)
+        soft = None if args.skip_softbody else run_softbody(args, local, False)
+        selfc = None if args.skip_self else run_self_collision(args, local, False)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "note": "headline skipped (--skip-single)",
-                              "batched": batched, "serving": served}))
+                              "batched": batched, "serving": served, "softbody": soft, "self_collision": selfc}))
         if world > 1:
             import torch
 
@@ -471,6 +523,8 @@ def main():
     served = None if args.skip_serve else run_serving(args, local)
     soft = None if args.skip_softbody else run_softbody(args, local, rank == 0 and world == 1
                                                          and not args.no_cpu_baseline)
+    selfc = None if args.skip_self else run_self_collision(args, local, rank == 0 and world == 1
+                                                            and not args.no_cpu_baseline)
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -506,6 +560,7 @@ def main():
         "batched": batched,
         "serving": served,
         "softbody": soft,
+        "self_collision": selfc,
     }
     print(json.dumps(line))
 

@@ -130,12 +130,14 @@ def self_collision_scene(side: int = 11, seed: int = 6, steps: int = 150) -> Sce
     """The reference's self-collision scene (examples/testbed/tests/
     cloth_self_collision.h:24-60): a side x side vertex grid of 1 m spacing,
     5 m up, density 1, stretch 1e5, no shear or damping, thickness 0.2,
-    friction 0.3, falling onto a static capsule from (0, 0, -5) to (0, 0, 5),
-    radius 1, friction 1.  Jitter N(0, 1e-3 m); nothing pinned."""
+    friction 0.3, falling onto a static capsule from (0, 0, -5) to (0, 0, 5)
+    (larger cloths: as long as the cloth), radius 1, friction 1.  Jitter
+    N(0, 1e-3 m); nothing pinned."""
     mesh = grid_mesh(side, float(side - 1), 1e-3, seed)
     mesh.vertices[:, 1] += np.float32(5.0)
     cdef = ClothDef(density=1.0, streching=1e5, thickness=0.2, friction=0.3)
-    caps = [((0.0, 0.0, -5.0), (0.0, 0.0, 5.0), 1.0, 1.0)]
+    half = max(5.0, 0.5 * (side - 1))  # larger cloths: the capsule spans the cloth
+    caps = [((0.0, 0.0, -half), (0.0, 0.0, half), 1.0, 1.0)]
     return Scene(f"grid{side}_self_collision", mesh, cdef, np.zeros(0, np.uint32), capsules=caps, steps=steps)
 
 
