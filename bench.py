@@ -368,14 +368,16 @@ def run_softbody(args, dev: int, cpu_sample: bool):
 def run_self_collision(args, dev: int, cpu_sample: bool):
     """Self-collision (thickness 0.2): the reference's self-collision scene
     scaled to a side x side grid of 1 m spacing over a capsule as long as the
-    cloth.  Steps 0-59 fall (contacts exist, none active); steps 60-119, the
-    fold, are timed on the GPU with CUDA events.  The CPU figure is the
+    cloth, CG at the reference's 20-iteration rule.  Steps 0-59 fall (contacts
+    exist, none active); steps 60-119, the fold, are timed on the GPU with
+    CUDA events.  The CPU figure is the
     reference's own full b3Cloth::Step on the same cloth over the same 60
     steps, one core."""
     import bounce_b200 as b3g
 
     scene = b3g.self_collision_scene(args.self_side)
     cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene)
+    cloth.set_cg_strategy(True)  # the whole CG in one persistent launch
     lo, hi = 60, 120
     for _ in range(lo):
         cloth.step(scene.dt)
