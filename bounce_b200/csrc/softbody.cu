@@ -6,7 +6,7 @@
 //                   (softbody_force_solver.cpp:53-91), the element's f0 terms
 //                   R Ke x0 and its plastic strain update and plastic forces
 //                   (:256-357)
-//   k_sb_assemble   one thread per node: the node's row of K summed over its
+//   k_sb_assemble   one warp per node: the node's row of K summed over its
 //                   elements in element order (the reference's K(vi, vj) +=
 //                   R Ke RT), then b = M v - h (K p + f0 - (f_plastic + f_ext))
 //                   and A = M + h C + h^2 K (:359-377) in the reference's
@@ -207,51 +207,108 @@ __global__ void k_sb_elements(SoftDev d, float h, float inv_h)
     }
 }
 
-__global__ void k_sb_assemble(SoftDev d, float h)
+// One warp per node.  The node's incidences are taken 32 at a time: each
+// lane forms its element's four R Ke_ij R^T blocks (and f0, f_plastic terms)
+// into shared memory; then each lane owns up to four of the row's slots and
+// adds, in incidence (= element) order, every block that lands on them --
+// the reference's K(vi, vj) += R Ke R^T order, so the row is the same float
+// for float.  K p, b and A follow as in the reference (:359-377), the serial
+// sums on lane 0.
+constexpr int kAsmWarps = 4;
+constexpr uint32_t kMaxRowSlots = 128;  // slot ids are 7 bits wide
+
+__global__ void __launch_bounds__(32 * kAsmWarps) k_sb_assemble(SoftDev d, float h)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.n) return;
+    __shared__ float sX[kAsmWarps][32 * 4 * 9];   // element blocks of one chunk; later the row's K blocks
+    __shared__ uint8_t sSlot[kAsmWarps][32 * 4];
+    __shared__ float sF[kAsmWarps][32 * 6];       // f0 and f_plastic terms of one chunk
+    __shared__ float sXc[kAsmWarps][kMaxRowSlots * 3];
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const uint32_t i = blockIdx.x * kAsmWarps + w;
+    if (i >= d.n) return;  // whole warps leave together
+    float* X = sX[w];
+    uint8_t* SL = sSlot[w];
+    float* F = sF[w];
+    float* XC = sXc[w];
     const uint32_t r0 = d.rowptr[i], deg = d.rowptr[i + 1] - r0;
-    float* vals = d.vals + 9 * (size_t)r0;
-    for (uint32_t k = 0; k < 9 * deg; ++k) vals[k] = 0.0f;
-    f3 f0 = zero3(), fp = zero3();
-    for (uint32_t q = d.inc_ptr[i]; q < d.inc_ptr[i + 1]; ++q) {
-        const uint32_t e = d.inc_elem[q], meta = d.inc_meta[q];
-        const uint32_t li = meta & 3u;
-        const m3 R = ldm(d.R + 9 * (size_t)e);
-        const m3 RT = transpose(R);
-        const float* Ke = d.Ke + 144 * (size_t)e;
+    m3 acc[4];
 #pragma unroll
-        for (uint32_t j = 0; j < 4; ++j) {
-            const uint32_t slot = (meta >> (4 + 7 * j)) & 127u;
-            const m3 X = mmul(mmul(R, ldm(Ke + 9 * (li + 4 * j))), RT);
-            stm(vals + 9 * slot, ldm(vals + 9 * slot) + X);
+    for (int k = 0; k < 4; ++k) acc[k] = mzero();
+    f3 f0 = zero3(), fp = zero3();
+    const uint32_t q0 = d.inc_ptr[i], q1 = d.inc_ptr[i + 1];
+    for (uint32_t qb = q0; qb < q1; qb += 32u) {
+        const uint32_t cnt = min(32u, q1 - qb);
+        if (lane < cnt) {
+            const uint32_t e = d.inc_elem[qb + lane], meta = d.inc_meta[qb + lane];
+            const uint32_t li = meta & 3u;
+            const m3 R = ldm(d.R + 9 * (size_t)e);
+            const m3 RT = transpose(R);
+            const float* Ke = d.Ke + 144 * (size_t)e;
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j) {
+                SL[4 * lane + j] = (uint8_t)((meta >> (4 + 7 * j)) & 127u);
+                stm(X + 9 * (4 * lane + j), mmul(mmul(R, ldm(Ke + 9 * (li + 4 * j))), RT));
+            }
+            const f3 a = ldv(d.f0s + 12 * (size_t)e, li), b = ldv(d.fps + 12 * (size_t)e, li);
+            F[6 * lane] = a.x; F[6 * lane + 1] = a.y; F[6 * lane + 2] = a.z;
+            F[6 * lane + 3] = b.x; F[6 * lane + 4] = b.y; F[6 * lane + 5] = b.z;
         }
-        f0 = f0 + ldv(d.f0s + 12 * (size_t)e, li);
-        fp = fp + ldv(d.fps + 12 * (size_t)e, li);
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t slot = lane + 32u * k;
+            if (slot >= deg) break;
+            for (uint32_t q = 0; q < cnt; ++q)
+#pragma unroll
+                for (uint32_t j = 0; j < 4; ++j)
+                    if (SL[4 * q + j] == slot) acc[k] = acc[k] + ldm(X + 9 * (4 * q + j));
+        }
+        if (lane == 0)
+            for (uint32_t q = 0; q < cnt; ++q) {
+                f0 = f0 + mk(F[6 * q], F[6 * q + 1], F[6 * q + 2]);
+                fp = fp + mk(F[6 * q + 3], F[6 * q + 4], F[6 * q + 5]);
+            }
+        __syncwarp();
     }
-    const f3 f0n = mk(-f0.x, -f0.y, -f0.z);
-    // K p in the row list's order (newest first touch first)
-    f3 kp = zero3();
-    for (uint32_t k = deg; k-- > 0;) kp = kp + ldm(vals + 9 * k) * ldv(d.x, d.cols[r0 + k]);
+    // the row's K blocks and the x of their columns, for the serial K p
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t slot = lane + 32u * k;
+        if (slot < deg) {
+            stm(X + 9 * slot, acc[k]);
+            const f3 xc = ldv(d.x, d.cols[r0 + slot]);
+            XC[3 * slot] = xc.x; XC[3 * slot + 1] = xc.y; XC[3 * slot + 2] = xc.z;
+        }
+    }
+    __syncwarp();
     const bool dyn = d.type[i] == 2;
     const float m = d.mass[i];
-    f3 fe = ldv(d.f, i);
-    if (dyn) fe = fe + m * mk(d.gx, d.gy, d.gz);
     const m3 M = diag3(m);
-    const f3 mv = zero3() + M * ldv(d.v, i);
-    stv(d.b, i, mv - h * ((kp + f0n) - (fp + fe)));
-    d.S[i] = dyn ? 1.0f : 0.0f;
+    if (lane == 0) {
+        const f3 f0n = mk(-f0.x, -f0.y, -f0.z);
+        // K p in the row list's order (newest first touch first)
+        f3 kp = zero3();
+        for (uint32_t k = deg; k-- > 0;) kp = kp + ldm(X + 9 * k) * mk(XC[3 * k], XC[3 * k + 1], XC[3 * k + 2]);
+        f3 fe = ldv(d.f, i);
+        if (dyn) fe = fe + m * mk(d.gx, d.gy, d.gz);
+        const f3 mv = zero3() + M * ldv(d.v, i);
+        stv(d.b, i, mv - h * ((kp + f0n) - (fp + fe)));
+        d.S[i] = dyn ? 1.0f : 0.0f;
+    }
     // A = (M + h C) + (h h) K on the diagonal, 0 + (h h) K elsewhere
     const float hh = h * h;
     const float cd = d.damping[i] * m;
     const uint32_t dg = d.diag[i] - r0;
-    for (uint32_t k = 0; k < deg; ++k) {
-        const m3 K = ldm(vals + 9 * k);
-        m3 a;
-        if (k == dg) a = (M + h * diag3(cd)) + hh * K;
-        else a = mzero() + hh * K;
-        stm(vals + 9 * k, a);
+    float* vals = d.vals + 9 * (size_t)r0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t slot = lane + 32u * k;
+        if (slot < deg) {
+            m3 a;
+            if (slot == dg) a = (M + h * diag3(cd)) + hh * acc[k];
+            else a = mzero() + hh * acc[k];
+            stm(vals + 9 * slot, a);
+        }
     }
 }
 
@@ -564,7 +621,7 @@ b3g_status b3g_softbody_step(b3g_softbody* b, float dt, uint32_t velocity_iterat
     std::memset(&h, 0, sizeof(h));
     if (dt > 0.0f) {
         k_sb_elements<<<blocks_for(d.t), kBlock, 0, s>>>(d, dt, 1.0f / dt);
-        k_sb_assemble<<<blocks_for(d.n), kBlock, 0, s>>>(d, dt);
+        k_sb_assemble<<<(d.n + kAsmWarps - 1) / kAsmWarps, 32 * kAsmWarps, 0, s>>>(d, dt);
         count_launches(2);
         SB_TRY(cudaGetLastError());
         const b3g_status r = csr_run(b->cs, &b->opts, s, &h);
@@ -672,7 +729,7 @@ b3g_status b3g_softbody_export_system(b3g_softbody* b, float dt, uint32_t capaci
     b3g_status r = b3g_softbody_read_elements(b, q.data(), eps.data());
     if (r != B3G_OK) return r;
     k_sb_elements<<<blocks_for(d.t), kBlock, 0, s>>>(d, dt, 1.0f / dt);
-    k_sb_assemble<<<blocks_for(d.n), kBlock, 0, s>>>(d, dt);
+    k_sb_assemble<<<(d.n + kAsmWarps - 1) / kAsmWarps, 32 * kAsmWarps, 0, s>>>(d, dt);
     count_launches(2);
     SB_TRY(cudaGetLastError());
     std::vector<float> v(9 * (size_t)d.nnz);
