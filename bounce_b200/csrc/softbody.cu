@@ -152,15 +152,25 @@ __global__ void k_sb_elements(SoftDev d, float h, float inv_h)
     d.q[e] = q;
     const m3 RT = transpose(R);
     stm(d.R + 9 * (size_t)e, R);
-    const float* Ke = d.Ke + 144 * (size_t)e;
-    // f0 terms: sum_j (R Ke_ij) x0_j
+    // f0 terms: sum_j (R Ke_ij) x0_j.  Ke is read in memory order, 16 bytes
+    // per load: block (i, j) sits at 9 (i + 4 j), so the four blocks of one j
+    // are 36 consecutive floats; each of the four sums still runs over j in
+    // order.
+    const float4* Ke4 = reinterpret_cast<const float4*>(d.Ke + 144 * (size_t)e);
+    f3 f0acc[4] = {zero3(), zero3(), zero3(), zero3()};
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        f3 acc = zero3();
+    for (int j = 0; j < 4; ++j) {
+        float kb[36];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc = acc + mmul(R, ldm(Ke + 9 * (i + 4 * j))) * xs[j];
-        stv(d.f0s + 12 * (size_t)e, i, acc);
+        for (int q = 0; q < 9; ++q) {
+            const float4 t4 = Ke4[9 * j + q];
+            kb[4 * q] = t4.x, kb[4 * q + 1] = t4.y, kb[4 * q + 2] = t4.z, kb[4 * q + 3] = t4.w;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) f0acc[i] = f0acc[i] + mmul(R, ldm(kb + 9 * i)) * xs[j];
     }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) stv(d.f0s + 12 * (size_t)e, i, f0acc[i]);
     // plasticity: total strain B (R^T p - x0), elastic = total - plastic
     float rx[12];
 #pragma unroll
@@ -168,16 +178,27 @@ __global__ void k_sb_elements(SoftDev d, float h, float inv_h)
         const f3 dd = RT * ps[i] - xs[i];
         rx[3 * i] = dd.x, rx[3 * i + 1] = dd.y, rx[3 * i + 2] = dd.z;
     }
-    const float* B = d.B + 72 * (size_t)e;
+    // B (6 x 12, entry (i, k) at i + 6 k) in memory order, 16 bytes per load
+    const float4* B4 = reinterpret_cast<const float4*>(d.B + 72 * (size_t)e);
     float* ep = d.eps + 6 * (size_t)e;
-    float plastic[6], elastic[6];
+    float plastic[6], elastic[6], bacc[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int k2 = 0; k2 < 6; ++k2) {  // two columns k = 2 k2, 2 k2 + 1: 12 floats
+        float bb[12];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const float4 t4 = B4[3 * k2 + q];
+            bb[4 * q] = t4.x, bb[4 * q + 1] = t4.y, bb[4 * q + 2] = t4.z, bb[4 * q + 3] = t4.w;
+        }
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2)
+#pragma unroll
+            for (int i = 0; i < 6; ++i) bacc[i] += bb[6 * h2 + i] * rx[2 * k2 + h2];
+    }
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        float acc = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 12; ++k) acc += B[i + 6 * k] * rx[k];
         plastic[i] = ep[i];
-        elastic[i] = acc - plastic[i];
+        elastic[i] = bacc[i] - plastic[i];
     }
     if (len6(elastic) > d.c_yield) {
         const float amount = h * (d.c_creep < inv_h ? d.c_creep : inv_h);
@@ -192,19 +213,22 @@ __global__ void k_sb_elements(SoftDev d, float h, float inv_h)
     }
 #pragma unroll
     for (int i = 0; i < 6; ++i) ep[i] = plastic[i];
-    const float* P = d.P + 72 * (size_t)e;
+    // P (12 x 6, entry (3 i + r, k) at 3 i + r + 12 k) in memory order
+    const float4* P4 = reinterpret_cast<const float4*>(d.P + 72 * (size_t)e);
+    float pc[12] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        float c[3];
+    for (int k = 0; k < 6; ++k) {
+        float pp[12];
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            float acc = 0.0f;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) acc += P[3 * i + r + 12 * k] * plastic[k];
-            c[r] = acc;
+        for (int q = 0; q < 3; ++q) {
+            const float4 t4 = P4[3 * k + q];
+            pp[4 * q] = t4.x, pp[4 * q + 1] = t4.y, pp[4 * q + 2] = t4.z, pp[4 * q + 3] = t4.w;
         }
-        stv(d.fps + 12 * (size_t)e, i, R * mk(c[0], c[1], c[2]));
+#pragma unroll
+        for (int m = 0; m < 12; ++m) pc[m] += pp[m] * plastic[k];
     }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) stv(d.fps + 12 * (size_t)e, i, R * mk(pc[3 * i], pc[3 * i + 1], pc[3 * i + 2]));
 }
 
 // One warp per node.  The node's incidences are taken 32 at a time: each
