@@ -82,18 +82,33 @@ __global__ void k_csr_init(CsrSystem s)
     }
 }
 
+// s = S A p and p.s.  Four lanes share a row: lane g sums the row's blocks
+// g, g + 4, ... (neighbouring lanes read neighbouring blocks, so the block
+// loads coalesce), then the four partial sums combine as (0 + 1) + (2 + 3).
 template <int DOT>
 __global__ void k_csr_spmv(CsrSystem s)
 {
     typedef DotT<DOT> D;
     if (s.sc->cont == 0u) return;
     typename D::T v[1] = {D::zero()};
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += gridDim.x * blockDim.x) {
+    const uint32_t lane = threadIdx.x & 31u, g = lane & 3u;
+    const unsigned mask = 0xFu << (lane & ~3u);
+    const uint32_t stride = (gridDim.x * blockDim.x) >> 2;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; i < s.n; i += stride) {
         f3 ap = zero3();
-        for (uint32_t k = s.rowptr[i]; k < s.rowptr[i + 1]; ++k) ap = ap + ldm(s.vals, k) * ldv(s.p, s.cols[k]);
-        const f3 sv = Sf(s, i) ? ap : zero3();
-        stv(s.s, i, sv);
-        v[0] = D::add_term(v[0], ldv(s.p, i), sv);
+        const uint32_t k1 = s.rowptr[i + 1];
+        for (uint32_t k = s.rowptr[i] + g; k < k1; k += 4u) ap = ap + ldm(s.vals, k) * ldv(s.p, s.cols[k]);
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+            ap.x += __shfl_xor_sync(mask, ap.x, o);
+            ap.y += __shfl_xor_sync(mask, ap.y, o);
+            ap.z += __shfl_xor_sync(mask, ap.z, o);
+        }
+        if (g == 0) {
+            const f3 sv = Sf(s, i) ? ap : zero3();
+            stv(s.s, i, sv);
+            v[0] = D::add_term(v[0], ldv(s.p, i), sv);
+        }
     }
     if (grid_reduce<DOT, 1>(v, s.partials, &s.sc->ticket[1]) && threadIdx.x == 0) {
         StepScalars* sc = s.sc;

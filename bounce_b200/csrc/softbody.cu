@@ -243,10 +243,10 @@ constexpr uint32_t kMaxRowSlots = 128;  // slot ids are 7 bits wide
 
 __global__ void __launch_bounds__(32 * kAsmWarps) k_sb_assemble(SoftDev d, float h)
 {
-    __shared__ float sX[kAsmWarps][32 * 4 * 9];   // element blocks of one chunk; later the row's K blocks
+    __shared__ float sX[kAsmWarps][32 * 4 * 9];   // element blocks of one chunk
     __shared__ uint8_t sSlot[kAsmWarps][32 * 4];
     __shared__ float sF[kAsmWarps][32 * 6];       // f0 and f_plastic terms of one chunk
-    __shared__ float sXc[kAsmWarps][kMaxRowSlots * 3];
+    __shared__ float sXc[kAsmWarps][kMaxRowSlots * 3];  // K_k x_col per slot
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     const uint32_t i = blockIdx.x * kAsmWarps + w;
     if (i >= d.n) return;  // whole warps leave together
@@ -294,14 +294,13 @@ __global__ void __launch_bounds__(32 * kAsmWarps) k_sb_assemble(SoftDev d, float
             }
         __syncwarp();
     }
-    // the row's K blocks and the x of their columns, for the serial K p
+    // each slot's K_k x_col; lane 0 sums them in the row list's order below
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const uint32_t slot = lane + 32u * k;
         if (slot < deg) {
-            stm(X + 9 * slot, acc[k]);
-            const f3 xc = ldv(d.x, d.cols[r0 + slot]);
-            XC[3 * slot] = xc.x; XC[3 * slot + 1] = xc.y; XC[3 * slot + 2] = xc.z;
+            const f3 kx = acc[k] * ldv(d.x, d.cols[r0 + slot]);
+            XC[3 * slot] = kx.x; XC[3 * slot + 1] = kx.y; XC[3 * slot + 2] = kx.z;
         }
     }
     __syncwarp();
@@ -312,7 +311,7 @@ __global__ void __launch_bounds__(32 * kAsmWarps) k_sb_assemble(SoftDev d, float
         const f3 f0n = mk(-f0.x, -f0.y, -f0.z);
         // K p in the row list's order (newest first touch first)
         f3 kp = zero3();
-        for (uint32_t k = deg; k-- > 0;) kp = kp + ldm(X + 9 * k) * mk(XC[3 * k], XC[3 * k + 1], XC[3 * k + 2]);
+        for (uint32_t k = deg; k-- > 0;) kp = kp + mk(XC[3 * k], XC[3 * k + 1], XC[3 * k + 2]);
         f3 fe = ldv(d.f, i);
         if (dyn) fe = fe + m * mk(d.gx, d.gy, d.gz);
         const f3 mv = zero3() + M * ldv(d.v, i);
