@@ -344,12 +344,27 @@ def run_softbody(args, dev: int, cpu_sample: bool):
         ms.append(s["step_ms"])
         iters.append(s["iterations"])
     launches = b3g.kernel_launch_count() - launches0
+    nnz = body.block_count()
     body.close()
     n, t = len(scene.vertices), len(scene.tets)
-    out = {"workload": f"block{side}x{side}x{side}_pinned", "nodes": n, "tetrahedra": t,
+    # algorithmic bytes of one step (FP32): the element kernel reads an
+    # element's vertices, rest frame, Ke, B, P and state and writes R, q, eps,
+    # f0, f_plastic (1,512 B); the assembly reads R, Ke, f0, f_plastic and the
+    # incidences per element (708 B), per node its state (41 B) and per block
+    # the column, the gathered x and the value written (52 B); each CG
+    # iteration moves 40 B per block and 164 B per row, the CG start 40 B per
+    # block and 100 B per row; the integration 48 B per node.
+    it = float(np.mean(iters))
+    step_bytes = 1512.0 * t + 708.0 * t + 41.0 * n + 52.0 * nnz + (40.0 * nnz + 100.0 * n) + \
+        it * (40.0 * nnz + 164.0 * n) + 48.0 * n
+    achieved = step_bytes / (sum(ms) / len(ms) / 1e3) / 1e9
+    out = {"workload": f"block{side}x{side}x{side}_pinned", "nodes": n, "tetrahedra": t, "blocks": nnz,
            "node_steps_per_s": n * len(ms) / (sum(ms) / 1e3), "ms_per_step": sum(ms) / len(ms),
-           "cg_iterations_mean": float(np.mean(iters)), "cg": "reference rule (20 iterations, f32 dots)",
-           "gpu_launches": launches, "steps": len(ms)}
+           "cg_iterations_mean": it, "cg": "reference rule (20 iterations, f32 dots)",
+           "gpu_launches": launches, "steps": len(ms),
+           "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": achieved, "peak": peaks()[0],
+                        "peak_kind": peaks()[1], "unit": "GB/s", "frac": achieved / peaks()[0],
+                        "algorithmic_bytes_per_step": step_bytes}}
     if cpu_sample:
         import oracle
 

@@ -786,6 +786,13 @@ class SoftBody:
         check(lib().b3g_softbody_energy(self.h, C.byref(e)), "softbody_energy")
         return float(e.value)
 
+    def block_count(self) -> int:
+        """Blocks of the assembled matrix (its nonzero 3x3 blocks)."""
+        cnt = C.c_uint32(0)
+        check(lib().b3g_softbody_export_system(self.h, 1.0 / 60.0, 0, None, None, None, None, None, C.byref(cnt)),
+              "softbody_export_system")
+        return int(cnt.value)
+
     def system(self, dt: float) -> dict:
         """A (rows in the reference's list order), b and S of one force solve
         from the current state; the state is not changed."""

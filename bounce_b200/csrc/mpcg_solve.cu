@@ -82,11 +82,13 @@ __global__ void k_csr_init(CsrSystem s)
     }
 }
 
-// s = S A p and p.s.  Four lanes share a row: lane g sums the row's blocks
+// s = S A p and p.s, launched with four times the other kernels' threads
+// per block (same grid, so the same reduction partials).  Four lanes share a
+// row: lane g sums the row's blocks
 // g, g + 4, ... (neighbouring lanes read neighbouring blocks, so the block
 // loads coalesce), then the four partial sums combine as (0 + 1) + (2 + 3).
 template <int DOT>
-__global__ void k_csr_spmv(CsrSystem s)
+__global__ void __launch_bounds__(1024) k_csr_spmv(CsrSystem s)
 {
     typedef DotT<DOT> D;
     if (s.sc->cont == 0u) return;
@@ -173,7 +175,7 @@ cudaError_t launch_all(const CsrSystem& s, uint32_t max_iter, cudaStream_t st)
 {
     k_csr_init<DOT><<<s.grid, s.block, 0, st>>>(s);
     for (uint32_t k = 0; k < max_iter; ++k) {
-        k_csr_spmv<DOT><<<s.grid, s.block, 0, st>>>(s);
+        k_csr_spmv<DOT><<<s.grid, 4 * s.block, 0, st>>>(s);  // four lanes per row, one partial per block
         k_csr_update<DOT><<<s.grid, s.block, 0, st>>>(s);
         k_csr_direction<<<s.grid, s.block, 0, st>>>(s);
     }
