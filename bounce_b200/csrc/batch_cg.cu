@@ -48,7 +48,10 @@ struct Team {
         if (TEAM == 1) {
             __syncthreads();
         } else {
-            __threadfence();  // global writes of this phase visible to the other SMs of the cluster
+            // barrier.cluster.arrive releases and barrier.cluster.wait
+            // acquires at cluster scope: this phase's global writes are
+            // visible to the cluster's other CTAs after it, with no
+            // device-wide fence
             cgx::this_cluster().sync();
         }
     }
