@@ -259,7 +259,7 @@ def run_ours(args, rank, world):
     }
 
 
-def run_batched(args, dev: int):
+def run_batched(args, dev: int, cpu_sample: bool = False):
     """Many cloths of uneven sizes per launch: 512 cloths, side U{16..128},
     stretch log-U[1e3, 1e5], shear log-U[1e2, 1e4], row 0 pinned; against the
     plain one-cloth-at-a-time GPU path on the same cloths."""
@@ -320,7 +320,8 @@ def run_batched(args, dev: int):
                          "frac": sum(cg_bytes) / (sum(cg_ms) / 1e3) / 1e9 / peaks()[0],
                          "algorithmic_bytes_per_launch": sum(cg_bytes) / len(cg_bytes),
                          "avg_launch_ms": sum(cg_ms) / len(cg_ms), "share": sum(cg_ms) / sum(ms)},
-            "l2": "inputs larger than L2 (about 1 GB of resident cloth state)"}
+            "l2": "inputs larger than L2 (about 1 GB of resident cloth state)",
+            "cpu_baseline": cpu_batch_sample(args.batch_count) if cpu_sample else None}
 
 
 def run_softbody(args, dev: int, cpu_sample: bool):
@@ -486,6 +487,47 @@ def cpu_reference_sample(side: int, steps: int, warm: int, procs: int = 0):
             "seconds": slowest}
 
 
+def _reference_batch_worker(job):
+    """One host process: the reference stepping its share of the batched
+    cloths (same seeded scenes), `steps` steps each, one after another."""
+    count, indices, steps = job
+    import oracle
+
+    import bounce_b200 as b3g
+
+    scenes = b3g.batch_scenes(count, seed=3)
+    vs, sec = 0, 0.0
+    for k in indices:
+        sc = scenes[k]
+        ref = oracle.RefCloth(sc.mesh, sc.cdef, restated=True).setup(sc)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            ref.step(sc.dt, sc.velocity_iterations, sc.position_iterations)
+        sec += time.perf_counter() - t0
+        vs += sc.mesh.vertex_count * steps
+        del ref
+    return {"vertex_steps": vs, "seconds": sec}
+
+
+def cpu_batch_sample(count: int, every: int = 8, steps: int = 2, procs: int = 0):
+    """The reference on the batched workload: every `every`-th of the
+    `count` cloths, dealt round-robin to one process per host core; the rate is
+    all vertex-steps over the slowest process's stepping time."""
+    import multiprocessing as mp
+
+    procs = procs or int(os.environ.get("B3G_REFERENCE_PROCS", "0")) or (os.cpu_count() or 1)
+    picked = list(range(0, count, every))
+    jobs = [(count, picked[w::procs], steps) for w in range(procs) if picked[w::procs]]
+    with mp.get_context("spawn").Pool(len(jobs)) as pool:
+        outs = pool.map(_reference_batch_worker, jobs)
+    slowest = max(o["seconds"] for o in outs)
+    vs = sum(o["vertex_steps"] for o in outs)
+    return {"value": vs / slowest, "unit": UNIT, "cores": len(jobs), "kind": "reference",
+            "sample": f"{len(picked)} of the {count} batched cloths (every {every}th), {steps} steps each with the "
+                      f"reference b3Cloth::Step at its own 20-iteration CG rule, spread over {len(jobs)} processes "
+                      f"(one per host core); slowest process {slowest:.2f} s"}
+
+
 def host_cpu():
     try:
         with open("/proc/cpuinfo") as f:
@@ -536,7 +578,8 @@ def main():
             torch.distributed.destroy_process_group()
         return
     r = run_ours(args, rank, world)
-    batched = None if args.skip_batch else run_batched(args, local)
+    batched = None if args.skip_batch else run_batched(args, local, rank == 0 and world == 1
+                                                         and not args.no_cpu_baseline)
     served = None if args.skip_serve else run_serving(args, local)
     soft = None if args.skip_softbody else run_softbody(args, local, rank == 0 and world == 1
                                                          and not args.no_cpu_baseline)
