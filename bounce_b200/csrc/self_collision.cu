@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_sc_solve(ClothDev c, SelfDev 
 {
     extern __shared__ uint32_t last[];  // per particle: level of its latest contact
     __shared__ int s_min[2];
-    __shared__ uint32_t s_levels;
+    __shared__ uint32_t s_levels, s_width;
     const uint32_t n = c.n, tid = threadIdx.x, nt = blockDim.x;
     StepScalars* sc = c.sc;
     const float h = sc->dt;
@@ -517,6 +517,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_sc_solve(ClothDev c, SelfDev 
         uint32_t* lsw = s.level_start;
         for (uint32_t L = 0; L <= top + 1; ++L) lsw[L] = 0;
         for (uint32_t a = 0; a < A; ++a) lsw[__float_as_uint(s.con[a].pad)] += 1;
+        uint32_t width = 0;
+        for (uint32_t L = 1; L <= top; ++L) width = lsw[L] > width ? lsw[L] : width;
+        s_width = width;
         for (uint32_t L = 1; L <= top; ++L) lsw[L] += lsw[L - 1];
         lsw[top + 1] = A;
         for (uint32_t a = A; a-- > 0;) s.by_level[--lsw[__float_as_uint(s.con[a].pad)]] = a;
@@ -525,6 +528,27 @@ __global__ void __launch_bounds__(kSolveThreads) k_sc_solve(ClothDev c, SelfDev 
     }
     __syncthreads();
     const uint32_t top = s_levels;
+    // Levels of at most 32 contacts run in warp 0 alone, with warp
+    // barriers between levels; wider ones use the whole block.
+    const bool narrow = s_width <= 32u;
+    const uint32_t lane = tid & 31u;
+    auto sweep = [&](auto&& fn) {
+        if (narrow) {
+            if (tid < 32u) {
+                for (uint32_t L = 1; L <= top; ++L) {
+                    const uint32_t j = ls[L] + lane;
+                    if (j < ls[L + 1]) fn(j);
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+        } else {
+            for (uint32_t L = 1; L <= top; ++L) {
+                for (uint32_t j = ls[L] + tid; j < ls[L + 1]; j += nt) fn(j);
+                __syncthreads();
+            }
+        }
+    };
 
     // warm start: body contacts, then triangle contacts
     uint32_t body_active = 0;
@@ -536,10 +560,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_sc_solve(ClothDev c, SelfDev 
     }
     if (body_active) atomicAdd(&sc->active_contacts, body_active);
     __syncthreads();
-    for (uint32_t L = 1; L <= top; ++L) {
-        for (uint32_t j = ls[L] + tid; j < ls[L + 1]; j += nt) tri_warm_start(c, s.con[s.by_level[j]]);
-        __syncthreads();
-    }
+    sweep([&](uint32_t j) { tri_warm_start(c, s.con[s.by_level[j]]); });
     // velocity iterations
     for (uint32_t it = 0; it < sc->vel_iters; ++it) {
         for (uint32_t i = tid; i < n; i += nt) {
@@ -548,10 +569,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_sc_solve(ClothDev c, SelfDev 
             if (k) body_velocity(c, i, order, k);
         }
         __syncthreads();
-        for (uint32_t L = 1; L <= top; ++L) {
-            for (uint32_t j = ls[L] + tid; j < ls[L + 1]; j += nt) tri_velocity(c, s.con[s.by_level[j]]);
-            __syncthreads();
-        }
+        sweep([&](uint32_t j) { tri_velocity(c, s.con[s.by_level[j]]); });
     }
     // store impulses (body impulses live in c_imp already); integrate positions
     for (uint32_t a = tid; a < A; a += nt) {
@@ -576,13 +594,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_sc_solve(ClothDev c, SelfDev 
         if (mb < 0.0f) atomicMin(&s_min[0], enc_min(mb));
         __syncthreads();
         float mt = 0.0f;
-        for (uint32_t L = 1; L <= top; ++L) {
-            for (uint32_t j = ls[L] + tid; j < ls[L + 1]; j += nt) {
-                const float sep = tri_position(c, s.con[s.by_level[j]]);
-                mt = mt < sep ? mt : sep;
-            }
-            __syncthreads();
-        }
+        sweep([&](uint32_t j) {
+            const float sep = tri_position(c, s.con[s.by_level[j]]);
+            mt = mt < sep ? mt : sep;
+        });
         if (mt < 0.0f) atomicMin(&s_min[1], enc_min(mt));
         __syncthreads();
         const bool solved = dec_min(s_min[0]) >= -3.0f * kSlop && dec_min(s_min[1]) >= -3.0f * kSlop;
