@@ -144,6 +144,7 @@ def lib() -> C.CDLL:
             "b3g_cloth_add_static_sphere": [vp, vp, f32, f32, C.POINTER(u32)],
             "b3g_cloth_clear_colliders": [vp],
             "b3g_cloth_add_static_capsule": [vp, vp, vp, f32, f32, C.POINTER(u32)],
+            "b3g_cloth_add_static_hull": [vp, vp, u32, vp, u32, f32, C.POINTER(u32)],
             "b3g_cloth_create_particle": [vp, C.POINTER(ParticleDefC), C.POINTER(u32)],
             "b3g_cloth_destroy_particle": [vp, u32],
             "b3g_cloth_create_mouse_force": [vp, C.POINTER(MouseForceDefC), C.POINTER(u32)],
@@ -396,6 +397,17 @@ class Cloth:
         self.nsph += 1
         return sid.value
 
+    def add_hull(self, vertices, planes, friction: float) -> int:
+        """A static convex hull collider: vertices (n, 3) and face planes
+        (f, 4: normal, offset), world frame."""
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        p = np.ascontiguousarray(planes, np.float32).reshape(-1, 4)
+        sid = C.c_uint32(0)
+        check(lib().b3g_cloth_add_static_hull(self.h, _ptr(v), len(v), _ptr(p), len(p), friction, C.byref(sid)),
+              "add_static_hull")
+        self.nsph += 1
+        return sid.value
+
     def clear_colliders(self) -> None:
         check(lib().b3g_cloth_clear_colliders(self.h), "clear_colliders")
         self.nsph = 0
@@ -526,6 +538,8 @@ class Cloth:
             self.add_sphere(c, r, mu)
         for (a, b, r, mu) in scene.capsules:
             self.add_capsule(a, b, r, mu)
+        for (hv, hp, mu) in scene.hulls:
+            self.add_hull(hv, hp, mu)
         if opts is not None:
             self.set_solver(opts)
         return self

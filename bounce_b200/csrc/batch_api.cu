@@ -85,8 +85,10 @@ struct b3g_batch {
     std::vector<b3g_cloth*> graph_list;
     std::vector<uint32_t> graph_layouts;  // each listed cloth's layout version when the graph was built
     uint32_t graph_pi = UINT32_MAX, graph_sched = 0;
+    uint32_t graph_hulls = 0;  // whether the graph holds the hull contact kernel
     uint32_t graph_kernels = 0;
     uint32_t ntasks = 0, total_rows = 0, max_deg = 0;
+    uint32_t hulls = 0;  // some cloth of the batch has a hull collider
     int assemble_block = 0;
     int dot = -1;  // dot precision shared by every planned cloth, -1 if mixed
 };
@@ -105,7 +107,7 @@ void destroy_graph(b3g_batch* b)
 // (split cloths first, then groups of `cluster` small cloths, largest first).
 void plan(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count)
 {
-    uint32_t total = 0, max_deg = 1;
+    uint32_t total = 0, max_deg = 1, hulls = 0;
     int dot = count ? (int)cloths[0]->opts.dot : -1;
     for (uint32_t k = 0; k < count; ++k) {
         if ((int)cloths[k]->opts.dot != dot) dot = -1;
@@ -113,11 +115,13 @@ void plan(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count)
         b->h_prefix[k] = total;
         total += cloths[k]->dev.n;
         max_deg = std::max(max_deg, cloths[k]->dev.max_deg);
+        for (uint32_t q = 0; q < cloths[k]->dev.nsph; ++q) hulls |= cloths[k]->dev.sph[q].kind == 2 ? 1u : 0u;
     }
     b->h_prefix[count] = total;
     b->dot = dot;
     b->total_rows = total;
     b->max_deg = max_deg;
+    b->hulls = hulls;
     std::vector<uint32_t> idx(count);
     for (uint32_t k = 0; k < count; ++k) idx[k] = k;
     // work estimate: stored blocks
@@ -147,7 +151,7 @@ void plan(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count)
 
 b3g_status enqueue(b3g_batch* b, uint32_t count, uint32_t pi, cudaStream_t st, uint32_t* kernels)
 {
-    RowSpan sp{b->d_descs, b->d_prefix, count, b->total_rows, b->max_deg};
+    RowSpan sp{b->d_descs, b->d_prefix, count, b->total_rows, b->max_deg, b->hulls};
     BatchCgArgs a{b->d_descs, b->d_order, b->d_tasks, b->ntasks, b->d_next};
     uint32_t k = 0;
     B3G_TRY(cudaMemcpyAsync(b->d_descs, b->h_descs, count * sizeof(ClothDev), cudaMemcpyHostToDevice, st));
@@ -314,7 +318,11 @@ b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t coun
         B3G_TRY(cudaEventRecord(b->ev1, st));
         B3G_TRY(cudaStreamSynchronize(st));
     }
+    uint32_t hulls_now = 0;
+    for (uint32_t k = 0; k < count; ++k)
+        for (uint32_t q = 0; q < cloths[k]->dev.nsph; ++q) hulls_now |= cloths[k]->dev.sph[q].kind == 2 ? 1u : 0u;
     bool same = !use_graph || (b->exec && b->graph_pi == pos_iters && b->graph_sched == b->sched_version &&
+                b->graph_hulls == hulls_now &&
                 b->graph_list.size() == count && std::equal(b->graph_list.begin(), b->graph_list.end(), cloths));
     // a cloth laid out again (particles or forces created) has new sizes and buffers
     for (uint32_t k = 0; same && use_graph && k < count; ++k) same = b->graph_layouts[k] == cloths[k]->layout_version;
@@ -343,6 +351,7 @@ b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t coun
         for (uint32_t k = 0; k < count; ++k) b->graph_layouts[k] = cloths[k]->layout_version;
         b->graph_pi = pos_iters;
         b->graph_sched = b->sched_version;
+        b->graph_hulls = hulls_now;
         b->graph_kernels = kern;
     } else if (use_graph) {
         // descriptors may have changed (colliders added): refresh the pinned copy the graph uploads
@@ -427,7 +436,7 @@ b3g_status b3g_batch_autotune(b3g_batch* b, b3g_cloth* const* cloths, uint32_t c
         auto time_cg = [&](const b3g_batch_schedule& sc, float* ms_out) -> b3g_status {
             b->sched = sc;
             plan(b, cloths, count);
-            RowSpan sp{b->d_descs, b->d_prefix, count, b->total_rows, b->max_deg};
+            RowSpan sp{b->d_descs, b->d_prefix, count, b->total_rows, b->max_deg, b->hulls};
             BatchCgArgs a{b->d_descs, b->d_order, b->d_tasks, b->ntasks, b->d_next};
             B3G_TRY(cudaMemcpyAsync(b->d_descs, b->h_descs, count * sizeof(ClothDev), cudaMemcpyHostToDevice, st));
             B3G_TRY(cudaMemcpyAsync(b->d_stage, b->h_stage, count * sizeof(StepScalars), cudaMemcpyHostToDevice, st));

@@ -547,6 +547,8 @@ b3g_status destroy_cloth(b3g_cloth* c)
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     self_free(c);
+    for (void* p : c->hull_bufs) cudaFree(p);
+    c->hull_bufs.clear();
     destroy_graph(c);
     if (c->arena.base && c->owns_arena) cudaFree(c->arena.base);
     if (c->d_ops) cudaFree(c->d_ops);
@@ -636,12 +638,82 @@ b3g_status b3g_cloth_add_static_capsule(b3g_cloth* c, const float a[3], const fl
     return B3G_OK;
 }
 
+b3g_status b3g_cloth_add_static_hull(b3g_cloth* c, const float* vertices, uint32_t vertex_count,
+                                     const float* planes, uint32_t face_count, float friction, uint32_t* shape_id)
+{
+    if (!valid(c) || !vertices || !planes || vertex_count == 0 || face_count == 0 || vertex_count > 4096 ||
+        face_count > 4096 || !(friction >= 0.0f))
+        return B3G_ERR_INVALID_ARGUMENT;
+    for (uint32_t k = 0; k < 3 * vertex_count; ++k)
+        if (!std::isfinite(vertices[k])) return B3G_ERR_INVALID_ARGUMENT;
+    for (uint32_t k = 0; k < 4 * face_count; ++k)
+        if (!std::isfinite(planes[k])) return B3G_ERR_INVALID_ARGUMENT;
+    if (c->dev.nsph >= (uint32_t)kMaxSpheres) return B3G_ERR_CAPACITY;
+    cudaSetDevice(c->device);
+    const size_t nf = 3 * (size_t)vertex_count + 4 * (size_t)face_count;
+    std::vector<float> img(nf);
+    std::memcpy(img.data(), vertices, 3 * (size_t)vertex_count * sizeof(float));
+    std::memcpy(img.data() + 3 * (size_t)vertex_count, planes, 4 * (size_t)face_count * sizeof(float));
+    float* d = nullptr;
+    B3G_TRY(cudaMalloc(&d, nf * sizeof(float)));
+    cudaError_t e = cudaMemcpyAsync(d, img.data(), nf * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return from_cuda(e);
+    }
+    c->hull_bufs.push_back(d);
+    SphereDev& s = c->dev.sph[c->dev.nsph];
+    s = SphereDev{};
+    s.kind = 2;
+    s.radius = 0.0f;  // B3_HULL_RADIUS
+    s.friction = friction;
+    s.hull = d;
+    s.nhv = vertex_count;
+    s.nhf = face_count;
+    // b3HullShape::ComputeAABB (hull_shape.cpp:162-166): the body-frame
+    // vertices' bounds, extended by the hull radius, fattened by
+    // B3_AABB_EXTENSION
+    float lo[3], hi[3];
+    for (uint32_t k = 0; k < vertex_count; ++k) {
+        const float* v = vertices + 3 * k;
+        // b3Mul(xf, v) with the identity rotation at the origin
+        const float w[3] = {((v[0] * 1.0f + v[1] * 0.0f) + v[2] * 0.0f) + 0.0f,
+                            ((v[0] * 0.0f + v[1] * 1.0f) + v[2] * 0.0f) + 0.0f,
+                            ((v[0] * 0.0f + v[1] * 0.0f) + v[2] * 1.0f) + 0.0f};
+        for (int q = 0; q < 3; ++q) {
+            if (k == 0) {
+                lo[q] = hi[q] = w[q];
+            } else {
+                lo[q] = lo[q] < w[q] ? lo[q] : w[q];
+                hi[q] = hi[q] > w[q] ? hi[q] : w[q];
+            }
+        }
+    }
+    for (int q = 0; q < 3; ++q) {
+        s.lo[q] = (lo[q] - s.radius) - 0.2f;
+        s.hi[q] = (hi[q] + s.radius) + 0.2f;
+    }
+    if (shape_id) *shape_id = c->dev.nsph;
+    c->dev.nsph += 1;
+    destroy_graph(c);
+    return B3G_OK;
+}
+
+static void free_hulls(b3g_cloth* c)
+{
+    for (void* p : c->hull_bufs) cudaFree(p);
+    c->hull_bufs.clear();
+}
+
 b3g_status b3g_cloth_clear_colliders(b3g_cloth* c)
 {
     if (!valid(c)) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     B3G_TRY(launch_clear_contacts(c->dev, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
     c->dev.nsph = 0;
+    free_hulls(c);
     destroy_graph(c);
     return B3G_OK;
 }

@@ -60,13 +60,16 @@ struct StepScalars {
 
 struct GridBarrier;
 
-// A static collider: a sphere (kind 0) or a capsule (kind 1, segment a-b in
-// the world frame, its body at the origin).
+// A static collider: a sphere (kind 0), a capsule (kind 1, segment a-b in
+// the world frame, its body at the origin) or a convex hull (kind 2, world
+// frame, its body at the origin).
 struct SphereDev {
     float cx, cy, cz, radius, friction;
     float lo[3], hi[3];   // fat AABB of the shape proxy
-    uint32_t kind;
+    uint32_t kind;        // 0 sphere, 1 capsule, 2 hull
     float ax, ay, az, bx, by, bz;
+    const float* hull;    // hull: nhv vertices (3 floats), then nhf planes (normal, offset)
+    uint32_t nhv, nhf;
 };
 
 struct ClothDev {
@@ -131,6 +134,7 @@ struct RowSpan {
     const ClothDev* descs;      // device array of count cloth descriptors
     const uint32_t* prefix;     // device array of count + 1 row offsets
     uint32_t count, total, max_deg;
+    uint32_t hulls;             // nonzero when some cloth has a hull collider
 };
 
 cudaError_t launch_span_contacts_update(const RowSpan& sp, cudaStream_t st);

@@ -90,6 +90,7 @@ struct b3g_cloth {
     uint32_t layout_version = 0;              // bumped on every new layout (batches rebuild their graphs)
 
     b3g::SelfState* self = nullptr;           // particle-triangle contacts (thickness > 0)
+    std::vector<void*> hull_bufs;             // device copies of the hull colliders' data
 };
 
 

@@ -24,6 +24,7 @@
 
 #include "cg_common.cuh"
 #include "cloth_dev.cuh"
+#include "hull_gjk.cuh"
 #include "self_collision.cuh"
 #include "sell_spmv.cuh"
 #include "vec.cuh"
@@ -681,7 +682,7 @@ __global__ void k_contacts_update(const __grid_constant__ ClothDev one, const __
     const f3 xi = ld3(c.x, n, i);
     for (uint32_t s = 0; s < c.nsph; ++s) {
         const uint32_t q = s * n + i;
-        if (!c.c_exists[q]) continue;
+        if (!c.c_exists[q] || c.sph[s].kind == 2) continue;  // hulls: k_hull_contacts_update
         const SphereDev& sp = c.sph[s];
         if (!is_dynamic(c, i) || !overlap(lo, hi, sp)) {
             c.c_exists[q] = 0;
@@ -743,6 +744,46 @@ __global__ void k_contacts_update(const __grid_constant__ ClothDev one, const __
             }
             st3(c.c_point, nn, q, P);
         }
+        const f3 n1 = mk(-normal.x, -normal.y, -normal.z);
+        const f3 t1 = perp(n1);
+        const f3 t2 = cross(t1, n1);
+        c.c_active[q] = 1;
+        st3(c.c_normal, nn, q, n1);
+        st3(c.c_t1, nn, q, t1);
+        st3(c.c_t2, nn, q, t2);
+    }
+}
+
+// The same update for the hull colliders (b3HullShape::TestSphere,
+// hull_shape.cpp:187-254), in a kernel of its own so that the GJK's
+// registers stay out of the sphere and capsule update.
+template <bool MULTI>
+__global__ void k_hull_contacts_update(const __grid_constant__ ClothDev one, const __grid_constant__ RowSpan span)
+{
+    const ClothDev* cp;
+    uint32_t i;
+    if (!resolve<MULTI>(one, span, blockIdx.x * blockDim.x + threadIdx.x, cp, i)) return;
+    const ClothDev& c = *cp;
+    const uint32_t n = c.n, nn = c.nsph * n;
+    float lo[3], hi[3];
+    load_fat(c, i, lo, hi);
+    const f3 xi = ld3(c.x, n, i);
+    for (uint32_t s = 0; s < c.nsph; ++s) {
+        const uint32_t q = s * n + i;
+        const SphereDev& sp = c.sph[s];
+        if (sp.kind != 2 || !c.c_exists[q]) continue;
+        if (!is_dynamic(c, i) || !overlap(lo, hi, sp)) {
+            c.c_exists[q] = 0;
+            c.c_active[q] = 0;
+            continue;
+        }
+        const float radius = sp.radius + c.thickness;
+        f3 normal, P;
+        if (!hull::test_sphere(sp.hull, sp.nhv, sp.hull + 3 * sp.nhv, sp.nhf, radius, xi, normal, P)) {
+            c.c_active[q] = 0;
+            continue;
+        }
+        st3(c.c_point, nn, q, hull::xf_mult(P));  // body->GetLocalPoint
         const f3 n1 = mk(-normal.x, -normal.y, -normal.z);
         const f3 t1 = perp(n1);
         const f3 t2 = cross(t1, n1);
@@ -1162,6 +1203,12 @@ cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st)
     if (!c.nsph) return cudaSuccess;
     k_contacts_update<false><<<blocks_for(c.n, 256), 256, 0, st>>>(c, kNoSpan);
     count_launches(1);
+    bool hulls = false;
+    for (uint32_t s = 0; s < c.nsph; ++s) hulls = hulls || c.sph[s].kind == 2;
+    if (hulls) {
+        k_hull_contacts_update<false><<<blocks_for(c.n, 128), 128, 0, st>>>(c, kNoSpan);
+        count_launches(1);
+    }
     return cudaGetLastError();
 }
 
@@ -1254,6 +1301,10 @@ cudaError_t launch_span_contacts_update(const RowSpan& sp, cudaStream_t st)
     if (!sp.total) return cudaSuccess;
     k_contacts_update<true><<<blocks_for(sp.total, 256), 256, 0, st>>>(g_unused_one, sp);
     count_launches(1);
+    if (sp.hulls) {
+        k_hull_contacts_update<true><<<blocks_for(sp.total, 128), 128, 0, st>>>(g_unused_one, sp);
+        count_launches(1);
+    }
     return cudaGetLastError();
 }
 

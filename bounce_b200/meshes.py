@@ -87,6 +87,7 @@ class Scene:
     gravity: tuple = (0.0, -9.8, 0.0)
     spheres: list = field(default_factory=list)   # (center (3,), radius, friction)
     capsules: list = field(default_factory=list)  # (a (3,), b (3,), radius, friction): static, world frame
+    hulls: list = field(default_factory=list)     # (vertices (n, 3), planes (f, 4), friction): static, world frame
     dt: float = 1.0 / 60.0
     steps: int = 100
     velocity_iterations: int = 8

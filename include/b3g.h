@@ -119,6 +119,15 @@ b3g_status b3g_cloth_add_static_sphere(b3g_cloth* cloth, const float center[3], 
  * collider capacity with spheres. */
 b3g_status b3g_cloth_add_static_capsule(b3g_cloth* cloth, const float a[3], const float b[3], float radius,
                                         float friction, uint32_t* shape_id);
+/* A static convex hull collider (b3HullShape, include/bounce/dynamics/shapes/
+ * hull_shape.h) on a static body at the origin: `vertices` (3 floats each)
+ * and face planes (`planes`: normal xyz and offset, 4 floats each) in world
+ * coordinates, hull radius 0 (B3_HULL_RADIUS); contacts as
+ * b3HullShape::TestSphere (src/bounce/dynamics/shapes/hull_shape.cpp:187-254,
+ * GJK from src/bounce/collision/gjk/gjk.cpp:579-740).  At most 4096 vertices
+ * and faces.  Shares the collider capacity with spheres and capsules. */
+b3g_status b3g_cloth_add_static_hull(b3g_cloth* cloth, const float* vertices, uint32_t vertex_count,
+                                     const float* planes, uint32_t face_count, float friction, uint32_t* shape_id);
 b3g_status b3g_cloth_clear_colliders(b3g_cloth* cloth);
 
 /* ---- created particles and mouse forces ------------------------------------ */

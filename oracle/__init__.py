@@ -67,6 +67,7 @@ def port_lib():
             getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, _f32p]
         L.oc_add_sphere.argtypes = [C.c_void_p, _f32p, C.c_float, C.c_float]
         L.oc_add_capsule.argtypes = [C.c_void_p, _f32p, _f32p, C.c_float, C.c_float]
+        L.oc_add_hull.argtypes = [C.c_void_p, _f32p, C.c_uint32, _f32p, C.c_uint32, C.c_float]
         L.oc_set_solver.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_uint32, C.c_int]
         L.oc_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(_OcStepInfo)]
         L.oc_get_state.argtypes = [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _u8p]
@@ -126,6 +127,9 @@ def ref_lib():
             getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, _f32p]
         L.ref_cloth_add_sphere.argtypes = [C.c_void_p, _f32p, C.c_float, C.c_float]
         L.ref_cloth_add_capsule.argtypes = [C.c_void_p, _f32p, _f32p, C.c_float, C.c_float]
+        L.ref_cloth_add_hull.restype = C.c_uint32
+        L.ref_cloth_add_hull.argtypes = [C.c_void_p, _f32p, C.c_uint32, C.c_float, _f32p, _f32p,
+                                         C.POINTER(C.c_uint32)]
         L.ref_cloth_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_uint32, C.c_int]
         L.ref_last_iterations.restype = C.c_uint32
         L.ref_cloth_get_state.argtypes = [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _u8p]
@@ -252,6 +256,8 @@ class _Base:
             self.add_sphere(c, r, mu)
         for (a, b, r, mu) in getattr(scene, "capsules", ()):
             self.add_capsule(a, b, r, mu)
+        for (hv, hp, mu) in getattr(scene, "hulls", ()):
+            self.add_hull(hv, hp, mu)
         return self
 
 
@@ -296,6 +302,11 @@ class PortCloth(_Base):
 
     def add_capsule(self, a, b, radius, friction):
         return self.L.oc_add_capsule(self.h, np.asarray(a, np.float32), np.asarray(b, np.float32), radius, friction)
+
+    def add_hull(self, vertices, planes, friction):
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1)
+        p = np.ascontiguousarray(planes, np.float32).reshape(-1)
+        return self.L.oc_add_hull(self.h, v, v.size // 3, p, p.size // 4, friction)
 
     def set_solver(self, stop_rule=STOP_REFERENCE, tol=0.0, max_iterations=20, dot=DOT_F32):
         self.L.oc_set_solver(self.h, stop_rule, tol, max_iterations, dot)
@@ -389,6 +400,16 @@ class RefCloth(_Base):
 
     def add_capsule(self, a, b, radius, friction):
         self.L.ref_cloth_add_capsule(self.h, np.asarray(a, np.float32), np.asarray(b, np.float32), radius, friction)
+
+    def add_hull_from_points(self, points, friction):
+        """A static hull that the reference's quickhull builds from `points`;
+        returns its vertices (n, 3) and face planes (f, 4)."""
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1)
+        verts = np.zeros(3 * 256, np.float32)
+        planes = np.zeros(4 * 256, np.float32)
+        nf = C.c_uint32(0)
+        nv = self.L.ref_cloth_add_hull(self.h, pts, pts.size // 3, friction, verts, planes, C.byref(nf))
+        return verts[:3 * nv].reshape(-1, 3).copy(), planes[:4 * nf.value].reshape(-1, 4).copy()
 
     def step(self, dt, vel_iters=8, pos_iters=2, full=False):
         self.L.ref_cloth_step(self.h, dt, vel_iters, pos_iters, 1 if full else 0)

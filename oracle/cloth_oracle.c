@@ -155,12 +155,16 @@ typedef struct {
     uint32_t id;          /* mouse: the handle oc_create_mouse_force returned */
 } force_t;
 
-enum { SHAPE_SPHERE = 0, SHAPE_CAPSULE = 1 };
+enum { SHAPE_SPHERE = 0, SHAPE_CAPSULE = 1, SHAPE_HULL = 2 };
 
 typedef struct {
     int kind;
     v3 center;         /* sphere */
     v3 a, b;           /* capsule segment, world frame (the body at the origin) */
+    v3* hv;            /* hull: vertices and face planes (normal, offset), world frame (body at the origin) */
+    v3* hn;
+    float* ho;
+    uint32_t nhv, nhf;
     float radius, friction;
     v3 fat_lo, fat_hi; /* the shape's proxy in the world broadphase */
 } sphere_t;
@@ -471,6 +475,9 @@ void oc_destroy(oc_cloth* c)
     free(c->mass); free(c->inv_mass); free(c->radius); free(c->friction); free(c->type);
     free(c->fat_lo); free(c->fat_hi); free(c->order); free(c->solver_of_vertex);
     free(c->du1); free(c->dv1); free(c->du2); free(c->dv2); free(c->inv_det); free(c->alpha);
+    for (uint32_t k = 0; k < c->nsphere; ++k) {
+        free(c->spheres[k].hv); free(c->spheres[k].hn); free(c->spheres[k].ho);
+    }
     free(c->forces); free(c->spheres); free(c->contacts);
     lrows_free(c->dfdx, c->n);
     lrows_free(c->dfdv, c->n);
@@ -655,6 +662,372 @@ int oc_add_capsule(oc_cloth* c, const float* a, const float* b, float radius, fl
     s->fat_lo = vsub(vsub(vmin(s->a, s->b), r), ext);
     s->fat_hi = vadd(vadd(vmax(s->a, s->b), r), ext);
     return (int)c->nsphere++;
+}
+
+/* b3Mul(b3Transform, b3Vec3) and b3MulT for a static body at the origin
+ * with the identity rotation (transform.h:74-110, mat33.h:129-160), written
+ * out so that the float operations are the reference's. */
+static const v3 kIdX = {1.0f, 0.0f, 0.0f}, kIdY = {0.0f, 1.0f, 0.0f}, kIdZ = {0.0f, 0.0f, 1.0f};
+static inline v3 xf_mul(v3 v)
+{
+    v3 r = vadd(vadd(vscale(v.x, kIdX), vscale(v.y, kIdY)), vscale(v.z, kIdZ));
+    return vadd(r, vzero());
+}
+static inline v3 xf_mult(v3 v)
+{
+    v3 d = vsub(v, vzero());
+    return V(vdot(kIdX, d), vdot(kIdY, d), vdot(kIdZ, d));
+}
+
+/* A static b3HullShape (hull radius B3_HULL_RADIUS = 0) on a body at the
+ * origin: its proxy is b3HullShape::ComputeAABB (hull_shape.cpp:162-166)
+ * fattened by B3_AABB_EXTENSION. */
+int oc_add_hull(oc_cloth* c, const float* vertices, uint32_t nv, const float* planes, uint32_t nf, float friction)
+{
+    c->spheres = (sphere_t*)realloc(c->spheres, (c->nsphere + 1) * sizeof(sphere_t));
+    sphere_t* s = c->spheres + c->nsphere;
+    memset(s, 0, sizeof(*s));
+    s->kind = SHAPE_HULL;
+    s->radius = 0.0f;
+    s->friction = friction;
+    s->nhv = nv;
+    s->nhf = nf;
+    s->hv = (v3*)malloc((nv ? nv : 1) * sizeof(v3));
+    s->hn = (v3*)malloc((nf ? nf : 1) * sizeof(v3));
+    s->ho = (float*)malloc((nf ? nf : 1) * sizeof(float));
+    for (uint32_t i = 0; i < nv; ++i) s->hv[i] = V(vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]);
+    for (uint32_t i = 0; i < nf; ++i) {
+        s->hn[i] = V(planes[4 * i], planes[4 * i + 1], planes[4 * i + 2]);
+        s->ho[i] = planes[4 * i + 3];
+    }
+    v3 lo = xf_mul(s->hv[0]), hi = lo;
+    for (uint32_t i = 1; i < nv; ++i) {
+        v3 w = xf_mul(s->hv[i]);
+        lo = vmin(lo, w);
+        hi = vmax(hi, w);
+    }
+    v3 r = V(s->radius, s->radius, s->radius);
+    v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
+    s->fat_lo = vsub(vsub(lo, r), ext);
+    s->fat_hi = vadd(vadd(hi, r), ext);
+    return (int)c->nsphere++;
+}
+
+/* ---- b3GJK between a hull and a point (gjk.cpp) ------------------------ */
+
+typedef struct {
+    v3 point1, point2, point;
+    float weight;
+    uint32_t index1, index2;
+} gjk_vertex;
+
+typedef struct {
+    gjk_vertex v[4];
+    uint32_t count;
+} gjk_simplex;
+
+/* b3Barycentric for a segment, a triangle, a tetrahedron (gjk.cpp:32-99) */
+static void gbary2(float out[3], v3 A, v3 B, v3 Q)
+{
+    v3 AB = vsub(B, A), QA = vsub(A, Q), QB = vsub(B, Q);
+    out[0] = vdot(QB, AB);
+    out[1] = -vdot(QA, AB);
+    out[2] = out[0] + out[1];
+}
+
+static void gbary3(float out[4], v3 A, v3 B, v3 C, v3 Q)
+{
+    v3 AB = vsub(B, A), AC = vsub(C, A), QA = vsub(A, Q), QB = vsub(B, Q), QC = vsub(C, Q);
+    v3 QB_x_QC = vcross(QB, QC), QC_x_QA = vcross(QC, QA), QA_x_QB = vcross(QA, QB);
+    v3 AB_x_AC = vcross(AB, AC);
+    out[0] = vdot(QB_x_QC, AB_x_AC);
+    out[1] = vdot(QC_x_QA, AB_x_AC);
+    out[2] = vdot(QA_x_QB, AB_x_AC);
+    out[3] = out[0] + out[1] + out[2];
+}
+
+static inline float gdet(v3 a, v3 b, v3 c) { return vdot(a, vcross(b, c)); }
+static inline float gsign(float x) { return (float)(0.0f < x) - (float)(x < 0.0f); }
+
+static void gbary4(float out[5], v3 A, v3 B, v3 C, v3 D, v3 Q)
+{
+    v3 AB = vsub(B, A), AC = vsub(C, A), AD = vsub(D, A);
+    v3 QA = vsub(A, Q), QB = vsub(B, Q), QC = vsub(C, Q), QD = vsub(D, Q);
+    float divisor = gdet(AB, AC, AD);
+    float sign = gsign(divisor);
+    out[0] = sign * gdet(QB, QC, QD);
+    out[1] = sign * gdet(QA, QD, QC);
+    out[2] = sign * gdet(QA, QB, QD);
+    out[3] = sign * gdet(QA, QC, QB);
+    out[4] = sign * divisor;
+}
+
+static void gset1(gjk_simplex* s, gjk_vertex a)
+{
+    s->count = 1;
+    s->v[0] = a;
+    s->v[0].weight = 1.0f;
+}
+
+static void gset2(gjk_simplex* s, gjk_vertex a, float wa, gjk_vertex b, float wb)
+{
+    s->count = 2;
+    s->v[0] = a;
+    s->v[0].weight = wa;
+    s->v[1] = b;
+    s->v[1].weight = wb;
+}
+
+static void gset3(gjk_simplex* s, gjk_vertex a, float wa, gjk_vertex b, float wb, gjk_vertex c, float wc)
+{
+    s->count = 3;
+    s->v[0] = a;
+    s->v[0].weight = wa;
+    s->v[1] = b;
+    s->v[1].weight = wb;
+    s->v[2] = c;
+    s->v[2].weight = wc;
+}
+
+/* b3Simplex::Solve2 (gjk.cpp:201-236) */
+static void gsolve2(gjk_simplex* s, v3 Q)
+{
+    gjk_vertex A = s->v[0], B = s->v[1];
+    float wAB[3];
+    gbary2(wAB, A.point, B.point, Q);
+    if (wAB[1] <= 0.0f) { gset1(s, A); return; }
+    if (wAB[0] <= 0.0f) { gset1(s, B); return; }
+    float sc = 1.0f / wAB[2];
+    gset2(s, A, sc * wAB[0], B, sc * wAB[1]);
+}
+
+/* b3Simplex::Solve3 (gjk.cpp:240-346) */
+static void gsolve3(gjk_simplex* s, v3 Q)
+{
+    gjk_vertex A = s->v[0], B = s->v[1], C = s->v[2];
+    float wAB[3], wBC[3], wCA[3];
+    gbary2(wAB, A.point, B.point, Q);
+    gbary2(wBC, B.point, C.point, Q);
+    gbary2(wCA, C.point, A.point, Q);
+    if (wAB[1] <= 0.0f && wCA[0] <= 0.0f) { gset1(s, A); return; }
+    if (wAB[0] <= 0.0f && wBC[1] <= 0.0f) { gset1(s, B); return; }
+    if (wBC[0] <= 0.0f && wCA[1] <= 0.0f) { gset1(s, C); return; }
+    float wABC[4];
+    gbary3(wABC, A.point, B.point, C.point, Q);
+    float area = wABC[3];
+    if (wAB[0] > 0.0f && wAB[1] > 0.0f && area * wABC[2] <= 0.0f) {
+        float sc = 1.0f / wAB[2];
+        gset2(s, A, sc * wAB[0], B, sc * wAB[1]);
+        return;
+    }
+    if (wBC[0] > 0.0f && wBC[1] > 0.0f && area * wABC[0] <= 0.0f) {
+        float sc = 1.0f / wBC[2];
+        gset2(s, B, sc * wBC[0], C, sc * wBC[1]);
+        return;
+    }
+    if (wCA[0] > 0.0f && wCA[1] > 0.0f && area * wABC[1] <= 0.0f) {
+        float sc = 1.0f / wCA[2];
+        gset2(s, C, sc * wCA[0], A, sc * wCA[1]);
+        return;
+    }
+    float divisor = wABC[3];
+    if (divisor <= 0.0f) return; /* give up: the simplex and its weights stay */
+    float sc = 1.0f / divisor;
+    gset3(s, A, sc * wABC[0], B, sc * wABC[1], C, sc * wABC[2]);
+}
+
+/* b3Simplex::Solve4 (gjk.cpp:349-575) */
+static void gsolve4(gjk_simplex* s, v3 Q)
+{
+    gjk_vertex A = s->v[0], B = s->v[1], C = s->v[2], D = s->v[3];
+    float wAB[3], wAC[3], wAD[3], wBC[3], wCD[3], wDB[3];
+    gbary2(wAB, A.point, B.point, Q);
+    gbary2(wBC, B.point, C.point, Q);
+    gbary2(wAC, A.point, C.point, Q);
+    gbary2(wAD, A.point, D.point, Q);
+    gbary2(wCD, C.point, D.point, Q);
+    gbary2(wDB, D.point, B.point, Q);
+    if (wAB[1] <= 0.0f && wAC[1] <= 0.0f && wAD[1] <= 0.0f) { gset1(s, A); return; }
+    if (wAB[0] <= 0.0f && wDB[0] <= 0.0f && wBC[1] <= 0.0f) { gset1(s, B); return; }
+    if (wAC[0] <= 0.0f && wBC[0] <= 0.0f && wCD[1] <= 0.0f) { gset1(s, C); return; }
+    if (wAD[0] <= 0.0f && wCD[0] <= 0.0f && wDB[1] <= 0.0f) { gset1(s, D); return; }
+    float wACB[4], wABD[4], wADC[4], wBCD[4];
+    gbary3(wACB, A.point, C.point, B.point, Q);
+    gbary3(wABD, A.point, B.point, D.point, Q);
+    gbary3(wADC, A.point, D.point, C.point, Q);
+    gbary3(wBCD, B.point, C.point, D.point, Q);
+    if (wABD[2] <= 0.0f && wACB[1] <= 0.0f && wAB[0] > 0.0f && wAB[1] > 0.0f) {
+        float sc = 1.0f / wAB[2];
+        gset2(s, A, sc * wAB[0], B, sc * wAB[1]);
+        return;
+    }
+    if (wACB[2] <= 0.0f && wADC[1] <= 0.0f && wAC[0] > 0.0f && wAC[1] > 0.0f) {
+        float sc = 1.0f / wAC[2];
+        gset2(s, A, sc * wAC[0], C, sc * wAC[1]);
+        return;
+    }
+    if (wADC[2] <= 0.0f && wABD[1] <= 0.0f && wAD[0] > 0.0f && wAD[1] > 0.0f) {
+        float sc = 1.0f / wAD[2];
+        gset2(s, A, sc * wAD[0], D, sc * wAD[1]);
+        return;
+    }
+    if (wACB[0] <= 0.0f && wBCD[2] <= 0.0f && wBC[0] > 0.0f && wBC[1] > 0.0f) {
+        float sc = 1.0f / wBC[2];
+        gset2(s, B, sc * wBC[0], C, sc * wBC[1]);
+        return;
+    }
+    if (wADC[0] <= 0.0f && wBCD[0] <= 0.0f && wCD[0] > 0.0f && wCD[1] > 0.0f) {
+        float sc = 1.0f / wCD[2];
+        gset2(s, C, sc * wCD[0], D, sc * wCD[1]);
+        return;
+    }
+    if (wABD[0] <= 0.0f && wBCD[1] <= 0.0f && wDB[0] > 0.0f && wDB[1] > 0.0f) {
+        float sc = 1.0f / wDB[2];
+        gset2(s, D, sc * wDB[0], B, sc * wDB[1]);
+        return;
+    }
+    float wABCD[5];
+    gbary4(wABCD, A.point, B.point, C.point, D.point, Q);
+    if (wABCD[3] <= 0.0f && wACB[0] > 0.0f && wACB[1] > 0.0f && wACB[2] > 0.0f) {
+        float sc = 1.0f / (wACB[0] + wACB[1] + wACB[2]);
+        gset3(s, A, sc * wACB[0], C, sc * wACB[1], B, sc * wACB[2]);
+        return;
+    }
+    if (wABCD[2] <= 0.0f && wABD[0] > 0.0f && wABD[1] > 0.0f && wABD[2] > 0.0f) {
+        float sc = 1.0f / (wABD[0] + wABD[1] + wABD[2]);
+        gset3(s, A, sc * wABD[0], B, sc * wABD[1], D, sc * wABD[2]);
+        return;
+    }
+    if (wABCD[1] <= 0.0f && wADC[0] > 0.0f && wADC[1] > 0.0f && wADC[2] > 0.0f) {
+        float sc = 1.0f / (wADC[0] + wADC[1] + wADC[2]);
+        gset3(s, A, sc * wADC[0], D, sc * wADC[1], C, sc * wADC[2]);
+        return;
+    }
+    if (wABCD[0] <= 0.0f && wBCD[0] > 0.0f && wBCD[1] > 0.0f && wBCD[2] > 0.0f) {
+        float sc = 1.0f / (wBCD[0] + wBCD[1] + wBCD[2]);
+        gset3(s, B, sc * wBCD[0], C, sc * wBCD[1], D, sc * wBCD[2]);
+        return;
+    }
+    float divisor = wABCD[0] + wABCD[1] + wABCD[2] + wABCD[3];
+    if (divisor <= 0.0f) return;
+    float sc = 1.0f / divisor;
+    s->count = 4;
+    s->v[0].weight = sc * wABCD[0];
+    s->v[1].weight = sc * wABCD[1];
+    s->v[2].weight = sc * wABCD[2];
+    s->v[3].weight = sc * wABCD[3];
+}
+
+/* b3Simplex::GetSearchDirection and GetClosestPoint(s) (gjk.cpp:101-199) */
+static v3 gsearch(const gjk_simplex* s, v3 Q)
+{
+    if (s->count == 1) return vsub(Q, s->v[0].point);
+    if (s->count == 2) {
+        v3 A = s->v[0].point, B = s->v[1].point;
+        v3 AB = vsub(B, A), AQ = vsub(Q, A);
+        return vcross(vcross(AB, AQ), AB);
+    }
+    v3 A = s->v[0].point, B = s->v[1].point, C = s->v[2].point;
+    v3 AB = vsub(B, A), AC = vsub(C, A), AQ = vsub(Q, A);
+    v3 AB_x_AC = vcross(AB, AC);
+    return vdot(AB_x_AC, AQ) > 0.0f ? AB_x_AC : vneg(AB_x_AC);
+}
+
+static v3 gclosest(const gjk_simplex* s)
+{
+    const gjk_vertex* v = s->v;
+    if (s->count == 1) return v[0].point;
+    if (s->count == 2) return vadd(vscale(v[0].weight, v[0].point), vscale(v[1].weight, v[1].point));
+    if (s->count == 3)
+        return vadd(vadd(vscale(v[0].weight, v[0].point), vscale(v[1].weight, v[1].point)),
+                    vscale(v[2].weight, v[2].point));
+    return vzero();
+}
+
+static void gwitness(const gjk_simplex* s, v3* p1, v3* p2)
+{
+    const gjk_vertex* v = s->v;
+    switch (s->count) {
+        case 1:
+            *p1 = v[0].point1;
+            *p2 = v[0].point2;
+            break;
+        case 2:
+            *p1 = vadd(vscale(v[0].weight, v[0].point1), vscale(v[1].weight, v[1].point1));
+            *p2 = vadd(vscale(v[0].weight, v[0].point2), vscale(v[1].weight, v[1].point2));
+            break;
+        case 3:
+            *p1 = vadd(vadd(vscale(v[0].weight, v[0].point1), vscale(v[1].weight, v[1].point1)),
+                       vscale(v[2].weight, v[2].point1));
+            *p2 = vadd(vadd(vscale(v[0].weight, v[0].point2), vscale(v[1].weight, v[1].point2)),
+                       vscale(v[2].weight, v[2].point2));
+            break;
+        default:
+            *p1 = vadd(vadd(vadd(vscale(v[0].weight, v[0].point1), vscale(v[1].weight, v[1].point1)),
+                            vscale(v[2].weight, v[2].point1)),
+                       vscale(v[3].weight, v[3].point1));
+            *p2 = *p1;
+            break;
+    }
+}
+
+/* b3GJK (gjk.cpp:579-740, no cache, no radius) between the hull (proxy 1,
+ * body at the origin) and the point Q (proxy 2, identity frame). */
+static float gjk_hull_point(const sphere_t* h, v3 Q, v3* p1, v3* p2)
+{
+    gjk_simplex s;
+    memset(&s, 0, sizeof(s));
+    /* ReadCache with an empty cache (gjk.cpp:743-795): vertex 0 of both */
+    s.v[0].point1 = xf_mul(h->hv[0]);
+    s.v[0].point2 = xf_mul(Q);
+    s.v[0].point = vsub(s.v[0].point2, s.v[0].point1);
+    s.v[0].weight = 1.0f;
+    s.count = 1;
+    uint32_t save1[4], save2[4], saveCount = 0;
+    const v3 origin = vzero();
+    uint32_t iter = 0;
+    while (iter < 20) {
+        saveCount = s.count;
+        for (uint32_t i = 0; i < saveCount; ++i) {
+            save1[i] = s.v[i].index1;
+            save2[i] = s.v[i].index2;
+        }
+        if (s.count == 2) gsolve2(&s, origin);
+        else if (s.count == 3) gsolve3(&s, origin);
+        else if (s.count == 4) gsolve4(&s, origin);
+        if (s.count == 4) break;
+        (void)gclosest(&s);
+        v3 d = gsearch(&s, origin);
+        if (vdot(d, d) < kEps * kEps) break;
+        gjk_vertex* vx = s.v + s.count;
+        /* proxy 1: the hull's support in -d (b3GJKProxy::GetSupportIndex) */
+        v3 dl = xf_mult(vneg(d));
+        uint32_t best = 0;
+        float bestp = vdot(dl, h->hv[0]);
+        for (uint32_t i = 1; i < h->nhv; ++i) {
+            float pr = vdot(dl, h->hv[i]);
+            if (pr > bestp) {
+                best = i;
+                bestp = pr;
+            }
+        }
+        vx->index1 = best;
+        vx->point1 = xf_mul(h->hv[best]);
+        vx->index2 = 0;
+        vx->point2 = xf_mul(Q);
+        vx->point = vsub(vx->point2, vx->point1);
+        ++iter;
+        int duplicate = 0;
+        for (uint32_t i = 0; i < saveCount; ++i)
+            if (vx->index1 == save1[i] && vx->index2 == save2[i]) {
+                duplicate = 1;
+                break;
+            }
+        if (duplicate) break;
+        ++s.count;
+    }
+    gwitness(&s, p1, p2);
+    return vlength(vsub(*p1, *p2));
 }
 
 void oc_set_solver(oc_cloth* c, int stop_rule, float tol, uint32_t max_iterations, int dot)
@@ -1372,6 +1745,43 @@ static void contact_update(oc_cloth* c, contact_t* k)
         normal = V(0.0f, 1.0f, 0.0f);
         if (d_len > kEps) normal = vdiv(d, d_len);
         point = sp->center;
+    } else if (sp->kind == SHAPE_HULL) {
+        /* b3HullShape::TestSphere (hull_shape.cpp:187-254): GJK between the
+         * hull and the particle's point; inside the hull, the face of
+         * largest separation */
+        v3 c1, c2;
+        float distance = gjk_hull_point(sp, Q, &c1, &c2);
+        float total = sp->radius + c->radius[i];
+        if (distance > total) {
+            k->active = 0;
+            return;
+        }
+        if (distance > 0.0f) {
+            normal = vdiv(vsub(c2, c1), distance);
+            point = c1;
+        } else {
+            v3 support = xf_mult(Q);
+            uint32_t maxIndex = ~0u;
+            float maxSeparation = -FLT_MAX;
+            for (uint32_t f = 0; f < sp->nhf; ++f) {
+                float separation = vdot(sp->hn[f], support) - sp->ho[f];
+                if (separation > total) {
+                    k->active = 0;
+                    return;
+                }
+                if (separation > maxSeparation) {
+                    maxIndex = f;
+                    maxSeparation = separation;
+                }
+            }
+            /* b3Mul(xf, plane) (geometry.h:77-81), b3ClosestPointOnPlane (:96-100) */
+            v3 pn = vadd(vadd(vscale(sp->hn[maxIndex].x, kIdX), vscale(sp->hn[maxIndex].y, kIdY)),
+                         vscale(sp->hn[maxIndex].z, kIdZ));
+            float po = sp->ho[maxIndex] + vdot(pn, vzero());
+            float fraction = vdot(pn, Q) - po;
+            point = vsub(Q, vscale(fraction, pn));
+            normal = pn;
+        }
     } else {
         /* b3CapsuleShape::TestSphere (capsule_shape.cpp:186-284) */
         v3 A = sp->a, B = sp->b;
@@ -1418,7 +1828,7 @@ static void contact_update(oc_cloth* c, contact_t* k)
     k->normal1 = vneg(normal);
     /* body->GetLocalPoint(point) for a static body: the sphere's body sits at
      * its centre, the capsule's at the origin */
-    k->local_point2 = sp->kind == SHAPE_SPHERE ? vzero() : point;
+    k->local_point2 = sp->kind == SHAPE_SPHERE ? vzero() : sp->kind == SHAPE_HULL ? xf_mult(point) : point;
     k->tangent1 = vperp(k->normal1);
     k->tangent2 = vcross(k->tangent1, k->normal1);
 }

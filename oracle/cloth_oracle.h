@@ -70,6 +70,10 @@ void oc_set_velocity(oc_cloth* c, uint32_t vertex, const float* v);
 int oc_add_sphere(oc_cloth* c, const float* center, float radius, float friction);
 /* a static capsule collider, segment a-b in the world frame */
 int oc_add_capsule(oc_cloth* c, const float* a, const float* b, float radius, float friction);
+/* A static hull on a body at the origin: vertices (3 floats each) and face
+ * planes (normal, offset: 4 floats each) in the world frame. */
+int oc_add_hull(oc_cloth* c, const float* vertices, uint32_t vertex_count, const float* planes, uint32_t face_count,
+                float friction);
 void oc_set_solver(oc_cloth* c, int stop_rule, float tol, uint32_t max_iterations, int dot);
 
 void oc_step(oc_cloth* c, float dt, uint32_t velocity_iterations, uint32_t position_iterations,

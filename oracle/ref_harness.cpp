@@ -66,6 +66,8 @@
 #include <bounce/dynamics/world.h>
 #include <bounce/dynamics/body.h>
 #include <bounce/dynamics/shapes/sphere_shape.h>
+#include <bounce/dynamics/shapes/hull_shape.h>
+#include <bounce/collision/shapes/qhull.h>
 #undef private
 #undef protected
 
@@ -121,6 +123,8 @@ struct RefCloth {
     b3World* world = nullptr;
     std::vector<b3SphereShape*> sphere_protos;
     std::vector<b3CapsuleShape*> capsule_protos;
+    std::vector<b3HullShape*> hull_protos;
+    std::vector<b3QHull*> hulls;  // the hulls the shapes point to
     // Particles made with b3Cloth::CreateParticle, addressed after the mesh
     // vertices (index vertexCount + k), and mouse forces by id - 1 (null once
     // destroyed).
@@ -378,6 +382,8 @@ void ref_cloth_destroy(void* hp)
     delete h->world;
     for (b3SphereShape* s : h->sphere_protos) delete s;
     for (b3CapsuleShape* s : h->capsule_protos) delete s;
+    for (b3HullShape* s : h->hull_protos) delete s;
+    for (b3QHull* q : h->hulls) delete q;
     delete h;
 }
 
@@ -454,6 +460,42 @@ void ref_cloth_add_capsule(void* hp, const float* a, const float* b, float radiu
     sd.shape = cap;
     sd.friction = friction;
     body->CreateShape(sd);
+}
+
+// A static body at the origin with a b3HullShape: the hull b3QHull::Set
+// builds from `points` (quickhull), friction as given.  Its vertices (3 floats
+// each, at most 256) and face planes (normal and offset, 4 floats each, at most
+// 256) are written out; returns the vertex count, *face_count the face count.
+uint32_t ref_cloth_add_hull(void* hp, const float* points, uint32_t count, float friction, float* vertices,
+                            float* planes, uint32_t* face_count)
+{
+    RefCloth* h = (RefCloth*)hp;
+    if (!h->world) {
+        h->world = new b3World();
+        h->cloth->SetWorld(h->world);
+    }
+    std::vector<b3Vec3> pts(count);
+    for (uint32_t i = 0; i < count; ++i) pts[i].Set(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
+    b3QHull* hull = new b3QHull();
+    hull->Set(sizeof(b3Vec3), pts.data(), count);
+    h->hulls.push_back(hull);
+    b3BodyDef bd;
+    bd.type = e_staticBody;
+    b3Body* body = h->world->CreateBody(bd);
+    b3HullShape* shape = new b3HullShape();
+    shape->m_hull = hull;
+    h->hull_protos.push_back(shape);
+    b3ShapeDef sd;
+    sd.shape = shape;
+    sd.friction = friction;
+    body->CreateShape(sd);
+    for (uint32_t i = 0; i < hull->vertexCount; ++i) put3(vertices + 3 * i, hull->vertices[i]);
+    for (uint32_t i = 0; i < hull->faceCount; ++i) {
+        put3(planes + 4 * i, hull->planes[i].normal);
+        planes[4 * i + 3] = hull->planes[i].offset;
+    }
+    *face_count = hull->faceCount;
+    return hull->vertexCount;
 }
 
 // full = 1: the reference's own b3Cloth::Step; full = 0: harness_step.

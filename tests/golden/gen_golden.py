@@ -18,7 +18,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
-from bounce_b200.meshes import pinned_block_scene, plain_scene, self_collision_scene, sphere_scene  # noqa: E402
+from bounce_b200.meshes import (capsule_scene, pinned_block_scene, plain_scene, self_collision_scene,  # noqa: E402
+                                sphere_scene)
 
 
 def trajectory(scene, steps, keep):
@@ -65,6 +66,37 @@ def self_collision(scene, steps, keep):
             w[c["active"] == 0] = 0.0
             out[f"tc_pt_{k}"], out[f"tc_active_{k}"] = c["pt"], c["active"]
             out[f"tc_w_{k}"], out[f"tc_impulses_{k}"] = w, c["impulses"]
+    out["iterations"] = np.asarray(iters, np.uint32)
+    return out
+
+
+def hull_points():
+    """A slab-like hull's point cloud: two 12-gons of radius 0.35 m at heights
+    -0.35 and -0.45 m (the reference's quickhull merges it into a box)."""
+    ang = np.linspace(0.0, 2.0 * np.pi, 13)[:-1]
+    pts = [(0.35 * np.cos(a), y, 0.35 * np.sin(a)) for y in (-0.35, -0.45) for a in ang]
+    return np.asarray(pts, np.float32)
+
+
+def hull_trajectory(side, steps, keep):
+    """A cloth falling onto a static hull that the reference's quickhull
+    builds: the hull's vertices and planes, states and body contacts at the
+    kept steps."""
+    scene = capsule_scene(side)
+    scene.capsules = []
+    ref = oracle.RefCloth(scene.mesh, scene.cdef, restated=False).setup(scene)
+    hv, hp = ref.add_hull_from_points(hull_points(), 0.3)
+    out = {"vertices": scene.mesh.vertices, "triangles": scene.mesh.triangles, "def": scene.cdef.as_array(),
+           "hull_vertices": hv, "hull_planes": hp, "hull_friction": np.float32(0.3), "dt": np.float32(scene.dt)}
+    iters = []
+    for k in range(1, steps + 1):
+        iters.append(ref.step(scene.dt, scene.velocity_iterations, scene.position_iterations)["iterations"])
+        if k in keep:
+            s = ref.state()
+            out[f"x_{k}"], out[f"v_{k}"], out[f"dv_{k}"] = s["x"], s["v"], s["dv"]
+            c = ref.contacts()
+            out[f"contact_exists_{k}"], out[f"contact_active_{k}"] = c["exists"], c["active"]
+            out[f"contact_impulses_{k}"] = c["impulses"]
     out["iterations"] = np.asarray(iters, np.uint32)
     return out
 
@@ -123,6 +155,7 @@ def main():
         "sphere32_ref.npz": trajectory(sphere_scene(32, seed=2), 40, {1, 20, 30, 40}),
         "system16_bend_ref.npz": system(sphere_scene(16, seed=4)),
         "self_collision11_ref.npz": self_collision(self_collision_scene(11), 130, {1, 60, 90, 100, 115, 130}),
+        "hull16_ref.npz": hull_trajectory(16, 120, {1, 30, 60, 120}),
     }
     only = set(sys.argv[1:])
     for name, data in files.items():

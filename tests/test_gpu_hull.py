@@ -1,0 +1,88 @@
+"""Static hull colliders on the GPU (b3HullShape::TestSphere with b3GJK)
+against the oracle, which reproduces the reference bit for bit
+(tests/test_oracle_golden.py, tests/test_oracle_vs_reference.py).
+
+The hull is the reference's own quickhull output, stored in
+tests/golden/hull16_ref.npz.  Tolerances as for the other colliders: each
+step starts the oracle from the GPU's state; CG iterations within +-1, body
+contact counts within 1% (2 at least), x within 1e-4 relative.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _golden():
+    from test_oracle_golden import GOLDEN, hull_golden_scene
+
+    d = np.load(os.path.join(GOLDEN, "hull16_ref.npz"))
+    return d, hull_golden_scene(d)
+
+
+def test_hull_contacts_per_step(b3g, port):
+    d, scene = _golden()
+    gpu = b3g.Cloth(scene.mesh, scene.cdef).setup(scene)
+    ora = port.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    seen = 0
+    for step in range(100):
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        seen = max(seen, o["active_contacts"])
+        assert abs(g["iterations"] - o["iterations"]) <= 1, step
+        assert abs(int(g["active_contacts"]) - int(o["active_contacts"])) <= max(2, o["active_contacts"] // 100), step
+        assert abs(int(g["contacts"]) - int(o["contacts"])) <= max(2, o["contacts"] // 100), step
+        assert rel_err(gpu.state()["x"], ora.state()["x"]) <= 1e-4, step
+    assert seen > 100  # the cloth lay on the hull
+
+
+def test_hull_against_reference_golden(b3g):
+    """Free run from the reference's start: after one step x within 1e-4 m
+    and the same body contacts; once the cloth lies on the hull (step 30)
+    the same active set within 2% and x within 1e-2 m (the CGs, stopped at
+    the reference's 20 iterations, part)."""
+    d, scene = _golden()
+    gpu = b3g.Cloth(scene.mesh, scene.cdef).setup(scene)
+    for k in range(1, 31):
+        gpu.step(scene.dt)
+        if f"x_{k}" in d:
+            dx = float(np.abs(gpu.state()["x"] - d[f"x_{k}"]).max())
+            cts = gpu.contacts()
+            ga, ra = int(cts["active"].sum()), int(d[f"contact_active_{k}"].sum())
+            print("hull golden: step", k, "max |dx|", dx, "active", ga, ra)
+            if k == 1:
+                assert dx <= 1e-4
+                assert np.array_equal(cts["exists"], d["contact_exists_1"])
+                assert np.array_equal(cts["active"], d["contact_active_1"])
+            else:
+                assert dx <= 1e-2
+                assert abs(ga - ra) <= max(2, ra // 50)
+
+
+def test_hull_cloth_in_a_batch(b3g, port):
+    """A hull cloth stepped in a batch beside a plain cloth matches the
+    oracle per step like the single-cloth path."""
+    d, scene = _golden()
+    plain = b3g.plain_scene(12)
+    opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
+    hull_cloth = b3g.Cloth(scene.mesh, scene.cdef).setup(scene, opts)
+    other = b3g.Cloth(plain.mesh, plain.cdef).setup(plain, opts)
+    ora = port.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    ora.set_solver(opts.stop_rule, opts.tolerance, opts.max_iterations, opts.dot)
+    batch = b3g.Batch(4)
+    seen = 0
+    for step in range(60):
+        st = hull_cloth.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        batch.step([hull_cloth, other], scene.dt)
+        o = ora.step(scene.dt)
+        seen = max(seen, o["active_contacts"])
+        assert rel_err(hull_cloth.state()["x"], ora.state()["x"]) <= 1e-4, step
+    assert seen > 100
+    batch.close()

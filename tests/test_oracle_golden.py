@@ -115,3 +115,31 @@ def test_oracle_self_collision_bit_exact(port):
             assert np.array_equal(w, d[f"tc_w_{k}"]), k
             assert np.array_equal(t["impulses"], d[f"tc_impulses_{k}"]), k
     assert int(d["tc_active_100"].sum()) > 10
+
+
+def hull_golden_scene(d):
+    """The scene of hull16_ref.npz: a 16 x 16 cloth falling onto a static
+    hull (the reference's quickhull output, stored in the file)."""
+    mesh = Mesh(d["vertices"], d["triangles"])
+    cdef = ClothDef(*[float(x) for x in d["def"]])
+    return Scene("golden_hull", mesh, cdef, np.zeros(0, np.uint32),
+                 hulls=[(d["hull_vertices"], d["hull_planes"], float(d["hull_friction"]))], dt=float(d["dt"]))
+
+
+def test_oracle_hull_bit_exact(port):
+    """Hull colliders (b3HullShape::TestSphere with b3GJK): the restatement
+    reproduces the reference's trajectory and body contacts exactly."""
+    d = np.load(os.path.join(GOLDEN, "hull16_ref.npz"))
+    scene = hull_golden_scene(d)
+    c = port.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    for k in range(1, len(d["iterations"]) + 1):
+        assert c.step(scene.dt)["iterations"] == d["iterations"][k - 1], k
+        if f"x_{k}" in d:
+            s = c.state()
+            for q in ("x", "v", "dv"):
+                assert np.array_equal(s[q], d[f"{q}_{k}"]), (k, q)
+            cts = c.contacts()
+            assert np.array_equal(cts["exists"], d[f"contact_exists_{k}"]), k
+            assert np.array_equal(cts["active"], d[f"contact_active_{k}"]), k
+            assert np.array_equal(cts["impulses"], d[f"contact_impulses_{k}"]), k
+    assert int(d["contact_active_60"].sum()) > 100

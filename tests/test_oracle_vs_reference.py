@@ -209,3 +209,32 @@ def test_self_collision_matches_reference(edit_from):
         most = max(most, c["count"])
         most_active = max(most_active, int(c["active"].sum()))
     assert most > 500 and most_active > 50
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_hull_collider_matches_reference(seed):
+    """Static hulls from the reference's quickhull over random point clouds:
+    b3HullShape::TestSphere runs b3GJK (every simplex case) and, inside the
+    hull, its face search; contacts, positions and velocities bit for bit."""
+    from bounce_b200.meshes import capsule_scene
+
+    rng = np.random.default_rng(seed)
+    pts = (rng.normal(0.0, 0.2, (30, 3)) + np.array([0.0, -0.45, 0.0])).astype(np.float32)
+    scene = capsule_scene(16)
+    scene.capsules = []
+    ref = oracle.RefCloth(scene.mesh, scene.cdef).setup(scene)
+    hv, hp = ref.add_hull_from_points(pts, 0.3)
+    port = oracle.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    port.add_hull(hv, hp, 0.3)
+    active = 0
+    for _ in range(150):
+        assert ref.step(scene.dt)["iterations"] == port.step(scene.dt)["iterations"]
+        sr, sp = ref.state(), port.state()
+        for q in ("x", "v", "dv"):
+            assert np.array_equal(sr[q], sp[q]), q
+        cr, cp = ref.contacts(), port.contacts()
+        assert cr["count"] == cp["count"]
+        assert np.array_equal(cr["active"], cp["active"])
+        assert np.array_equal(cr["impulses"], cp["impulses"])
+        active = max(active, int(cr["active"].sum()))
+    assert active > 100
