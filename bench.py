@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-softbody", action="store_true")
     ap.add_argument("--skip-self", action="store_true")
+    ap.add_argument("--skip-colliders", action="store_true")
+    ap.add_argument("--collider-side", type=int, default=128)
     ap.add_argument("--self-side", type=int, default=24)
     ap.add_argument("--softbody-side", type=int, default=40)
     ap.add_argument("--softbody-steps", type=int, default=10)
@@ -431,6 +433,66 @@ def run_self_collision(args, dev: int, cpu_sample: bool):
     return out
 
 
+def box_hull(hx: float, hy: float, hz: float, cy: float):
+    """A box as a hull (vertices and face planes, world frame) centred at
+    (0, cy, 0)."""
+    v = np.array([(sx * hx, cy + sy * hy, sz * hz) for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)], np.float32)
+    planes = np.array([(1, 0, 0, hx), (-1, 0, 0, hx), (0, 1, 0, cy + hy), (0, -1, 0, -(cy - hy)), (0, 0, 1, hz),
+                       (0, 0, -1, hz)], np.float32)
+    return v, planes
+
+
+def run_colliders(args, dev: int, cpu_sample: bool):
+    """Static capsule and hull colliders: a side x side cloth (bending on)
+    falling onto a capsule (a rod along z) and onto a box hull (a 0.7 m
+    table top), 10 steps timed with CUDA events after it lands.  The CPU
+    figure is the reference's b3Cloth::Step on the same cloth and shape (its
+    quickhull builds the box from the same eight corners), two steps."""
+    import bounce_b200 as b3g
+
+    side = args.collider_side
+    out = {}
+    for kind in ("capsule", "hull"):
+        scene = b3g.capsule_scene(side)
+        if kind == "hull":
+            hv, hp = box_hull(0.35, 0.05, 0.35, -0.4)
+            scene.capsules = []
+            scene.hulls = [(hv, hp, 0.3)]
+        cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene)
+        cloth.set_cg_strategy(True)
+        for _ in range(40):  # fall onto the shape
+            cloth.step(scene.dt)
+        ms, active = [], []
+        for _ in range(10):
+            st = cloth.step(scene.dt)
+            ms.append(st["step_ms"])
+            active.append(st["active_contacts"])
+        cloth.close()
+        n = scene.mesh.vertex_count
+        r = {"workload": f"grid{side}_{kind}", "vertices": n, "steps": "40-49", "ms_per_step": sum(ms) / len(ms),
+             "vertex_steps_per_s": n * len(ms) / (sum(ms) / 1e3), "active_contacts_mean": float(np.mean(active))}
+        if cpu_sample:
+            import oracle
+
+            if oracle.ref_available():
+                ref = oracle.RefCloth(scene.mesh, scene.cdef, restated=True)
+                ref.set_gravity(scene.gravity)
+                if kind == "capsule":
+                    for (a, b, rad, mu) in scene.capsules:
+                        ref.add_capsule(a, b, rad, mu)
+                else:
+                    ref.add_hull_from_points(hv, 0.3)
+                t0 = time.perf_counter()
+                for _ in range(2):
+                    ref.step(scene.dt)
+                sec = time.perf_counter() - t0
+                r["cpu_baseline"] = {"value": n * 2 / sec, "unit": "vertex-steps/s", "cores": 1, "kind": "reference",
+                                     "sample": f"the reference's b3Cloth::Step, the first 2 steps of the same cloth "
+                                               f"and shape, {sec / 2:.2f} s/step"}
+        out[kind] = r
+    return out
+
+
 def run_serving(args, dev: int):
     from bounce_b200 import serving
 
@@ -568,9 +630,11 @@ def main():
         served = None if args.skip_serve else run_serving(args, local)
         soft = None if args.skip_softbody else run_softbody(args, local, False)
         selfc = None if args.skip_self else run_self_collision(args, local, False)
+        colliders = None if args.skip_colliders else run_colliders(args, local, False)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "note": "headline skipped (--skip-single)",
-                              "batched": batched, "serving": served, "softbody": soft, "self_collision": selfc}))
+                              "batched": batched, "serving": served, "softbody": soft, "self_collision": selfc,
+                              "colliders": colliders}))
         if world > 1:
             import torch
 
@@ -585,6 +649,8 @@ def main():
                                                          and not args.no_cpu_baseline)
     selfc = None if args.skip_self else run_self_collision(args, local, rank == 0 and world == 1
                                                             and not args.no_cpu_baseline)
+    colliders = None if args.skip_colliders else run_colliders(args, local, rank == 0 and world == 1
+                                                                and not args.no_cpu_baseline)
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -621,6 +687,7 @@ def main():
         "serving": served,
         "softbody": soft,
         "self_collision": selfc,
+        "colliders": colliders,
     }
     print(json.dumps(line))
 
