@@ -169,6 +169,8 @@ def lib() -> C.CDLL:
             "b3g_cloth_get_energy": [vp, C.POINTER(f32)],
             "b3g_cloth_read_contacts": [vp, vp, vp, vp],
             "b3g_cloth_read_tri_contacts": [vp, C.POINTER(u32), vp, vp, vp, vp],
+            "b3g_cloth_ray_cast_single": [vp, vp, vp, C.POINTER(u32), C.POINTER(f32), vp, C.POINTER(i32)],
+            "b3g_cloth_ray_cast": [vp, vp, vp, f32, u32, C.POINTER(f32), vp, C.POINTER(i32)],
             "b3g_cloth_get_self_stats": [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)],
             "b3g_cloth_last_stats": [vp, C.POINTER(StepStatsC)],
             "b3g_cloth_read_system": [vp, C.POINTER(u32), vp, vp, vp, vp, vp, vp],
@@ -492,6 +494,25 @@ class Cloth:
         check(lib().b3g_cloth_read_contacts(self.h, _ptr(ex), _ptr(ac), _ptr(imp)), "read_contacts")
         return {"exists": ex[: self.nsph * self.n], "active": ac[: self.nsph * self.n],
                 "impulses": imp[: self.nsph * self.n]}
+
+    def ray_cast_single(self, p1, p2):
+        """b3Cloth::RayCastSingle: (triangle, fraction, normal) of the first
+        triangle the segment p1 -> p2 hits, or None."""
+        a, b = _f3(p1), _f3(p2)
+        t, f, hit = C.c_uint32(0), C.c_float(0.0), C.c_int(0)
+        n = np.zeros(3, np.float32)
+        check(lib().b3g_cloth_ray_cast_single(self.h, _ptr(a), _ptr(b), C.byref(t), C.byref(f), _ptr(n),
+                                              C.byref(hit)), "ray_cast_single")
+        return (int(t.value), float(f.value), n) if hit.value else None
+
+    def ray_cast(self, p1, p2, triangle: int, max_fraction: float = 1.0):
+        """b3Cloth::RayCast against one triangle: (fraction, normal) or None."""
+        a, b = _f3(p1), _f3(p2)
+        f, hit = C.c_float(0.0), C.c_int(0)
+        n = np.zeros(3, np.float32)
+        check(lib().b3g_cloth_ray_cast(self.h, _ptr(a), _ptr(b), max_fraction, triangle, C.byref(f), _ptr(n),
+                                       C.byref(hit)), "ray_cast")
+        return (float(f.value), n) if hit.value else None
 
     def tri_contacts(self) -> dict:
         """Particle-triangle contacts (thickness > 0) in list order, head

@@ -549,6 +549,7 @@ b3g_status destroy_cloth(b3g_cloth* c)
     self_free(c);
     for (void* p : c->hull_bufs) cudaFree(p);
     c->hull_bufs.clear();
+    if (c->ray_buf) cudaFree(c->ray_buf);
     destroy_graph(c);
     if (c->arena.base && c->owns_arena) cudaFree(c->arena.base);
     if (c->d_ops) cudaFree(c->d_ops);
@@ -1452,6 +1453,57 @@ b3g_status b3g_cloth_read_contacts(const b3g_cloth* cc, uint8_t* exists, uint8_t
     }
     B3G_TRY(cudaStreamSynchronize(c->stream));
     return B3G_OK;
+}
+
+// One ray query: `triangle` < 0 casts against every triangle
+// (RayCastSingle), otherwise against that triangle alone (RayCast).
+static b3g_status ray_query(b3g_cloth* c, const float p1[3], const float p2[3], float max_fraction, int64_t triangle,
+                            uint32_t* tri_out, float* fraction, float normal[3], int* hit)
+{
+    if (!valid(c) || !p1 || !p2 || !hit || !(max_fraction >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    if (triangle >= (int64_t)c->dev.t) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    if (!c->ray_buf) B3G_TRY(cudaMalloc(&c->ray_buf, 64));
+    RayQuery q{};
+    for (int k = 0; k < 3; ++k) {
+        q.p1[k] = p1[k];
+        q.p2[k] = p2[k];
+    }
+    q.max_fraction = max_fraction;
+    q.best = static_cast<unsigned long long*>(c->ray_buf);
+    q.out = reinterpret_cast<RayHit*>(static_cast<char*>(c->ray_buf) + 16);
+    if (triangle < 0) {
+        B3G_TRY(launch_ray_cast(c->dev, q, c->stream));
+    } else {
+        const unsigned long long key = (unsigned long long)triangle;
+        B3G_TRY(cudaMemcpyAsync(q.best, &key, sizeof(key), cudaMemcpyHostToDevice, c->stream));
+        B3G_TRY(launch_ray_result(c->dev, q, c->stream));
+    }
+    RayHit h{};
+    B3G_TRY(cudaMemcpyAsync(&h, q.out, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    *hit = (int)h.hit;
+    if (h.hit) {
+        if (tri_out) *tri_out = h.triangle;
+        if (fraction) *fraction = h.fraction;
+        if (normal)
+            for (int k = 0; k < 3; ++k) normal[k] = h.normal[k];
+    }
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_ray_cast_single(b3g_cloth* c, const float p1[3], const float p2[3], uint32_t* triangle,
+                                     float* fraction, float normal[3], int* hit)
+{
+    return ray_query(c, p1, p2, 1.0f, -1, triangle, fraction, normal, hit);
+}
+
+b3g_status b3g_cloth_ray_cast(b3g_cloth* c, const float p1[3], const float p2[3], float max_fraction,
+                              uint32_t triangle, float* fraction, float normal[3], int* hit)
+{
+    return ray_query(c, p1, p2, max_fraction, (int64_t)triangle, nullptr, fraction, normal, hit);
 }
 
 b3g_status b3g_cloth_read_tri_contacts(const b3g_cloth* c, uint32_t* count, uint32_t* pairs, uint8_t* active,

@@ -143,6 +143,23 @@ cudaError_t launch_span_finalize(const RowSpan& sp, cudaStream_t st);
 cudaError_t launch_span_contact_position(const RowSpan& sp, uint32_t it, cudaStream_t st);
 cudaError_t launch_span_post(const RowSpan& sp, cudaStream_t st);
 
+// A ray p1 -> p2 against the cloth's triangles (b3Cloth::RayCast /
+// RayCastSingle): `best` is device scratch for the winning (fraction,
+// triangle) key, `out` receives the result.
+struct RayHit {
+    uint32_t hit, triangle;
+    float fraction;
+    float normal[3];
+};
+struct RayQuery {
+    float p1[3], p2[3], max_fraction;
+    unsigned long long* best;
+    RayHit* out;
+};
+cudaError_t launch_ray_cast(const ClothDev& c, const RayQuery& q, cudaStream_t st);
+// The result kernel alone, for a key already in q.best (one triangle).
+cudaError_t launch_ray_result(const ClothDev& c, const RayQuery& q, cudaStream_t st);
+
 // Host launchers (cloth_kernels.cu).  The assembly kernel needs
 // assemble_smem_bytes() of dynamic shared memory; a block size <= 0 asks for
 // assemble_block_for() of the rows' widest degree.

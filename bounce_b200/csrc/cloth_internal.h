@@ -91,6 +91,7 @@ struct b3g_cloth {
 
     b3g::SelfState* self = nullptr;           // particle-triangle contacts (thickness > 0)
     std::vector<void*> hull_bufs;             // device copies of the hull colliders' data
+    void* ray_buf = nullptr;                  // ray cast scratch (key and result)
 };
 
 

@@ -1040,6 +1040,76 @@ __global__ void k_post(const __grid_constant__ ClothDev one, const __grid_consta
 }
 
 // ---------------------------------------------------------------------------
+// ray casts (b3Cloth::RayCast / RayCastSingle)
+// ---------------------------------------------------------------------------
+
+// b3RayCast against triangle k (src/bounce/collision/collision.cpp:31-118)
+__device__ bool ray_triangle(const ClothDev& c, uint32_t k, f3 p1, f3 p2, float max_fraction, float& fraction,
+                             f3& normal)
+{
+    const uint32_t n = c.n;
+    const uint4 tv = c.tri[k];
+    const f3 v1 = ld3(c.x, n, tv.x), v2 = ld3(c.x, n, tv.y), v3 = ld3(c.x, n, tv.z);
+    const f3 d = p2 - p1;
+    if (d.x * d.x + d.y * d.y + d.z * d.z < kEps * kEps) return false;
+    f3 nn = cross(v2 - v1, v3 - v1);
+    const float len = sqrtf(nn.x * nn.x + nn.y * nn.y + nn.z * nn.z);
+    if (len == 0.0f) return false;
+    const float s1 = 1.0f / len;  // b3Vec3::operator/=
+    nn = mk(nn.x * s1, nn.y * s1, nn.z * s1);
+    const float num = dot(nn, v1 - p1);
+    const float den = dot(nn, d);
+    if (den == 0.0f) return false;
+    const float f = num / den;
+    if (f < 0.0f || max_fraction < f) return false;
+    const f3 Q = p1 + f * d;
+    const f3 AB = v2 - v1, AC = v3 - v1, QA = v1 - Q, QB = v2 - Q, QC = v3 - Q;
+    const f3 AB_x_AC = cross(AB, AC);
+    const float u = dot(cross(QB, QC), AB_x_AC);
+    const float v = dot(cross(QC, QA), AB_x_AC);
+    const float w = dot(cross(QA, QB), AB_x_AC);
+    if (!(u >= 0.0f && v >= 0.0f && w >= 0.0f)) return false;
+    fraction = f;
+    normal = num > 0.0f ? mk(-nn.x, -nn.y, -nn.z) : nn;
+    return true;
+}
+
+// Every triangle against the ray; the smallest (fraction, triangle) wins.
+__global__ void k_ray_min(ClothDev c, RayQuery q)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= c.t) return;
+    float f;
+    f3 nrm;
+    if (!ray_triangle(c, k, mk(q.p1[0], q.p1[1], q.p1[2]), mk(q.p2[0], q.p2[1], q.p2[2]), q.max_fraction, f, nrm))
+        return;
+    const unsigned long long key = ((unsigned long long)__float_as_uint(f + 0.0f) << 32) | k;
+    atomicMin(q.best, key);
+}
+
+// The winner's fraction and normal, or no hit.
+__global__ void k_ray_result(ClothDev c, RayQuery q)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    RayHit h{};
+    const unsigned long long key = *q.best;
+    if (key != ~0ull) {
+        const uint32_t k = (uint32_t)(key & 0xffffffffull);
+        float f;
+        f3 nrm;
+        if (ray_triangle(c, k, mk(q.p1[0], q.p1[1], q.p1[2]), mk(q.p2[0], q.p2[1], q.p2[2]), q.max_fraction, f, nrm)) {
+            h.hit = 1;
+            h.triangle = k;
+            h.fraction = f;
+            h.normal[0] = nrm.x;
+            h.normal[1] = nrm.y;
+            h.normal[2] = nrm.z;
+        }
+    }
+    *q.out = h;
+}
+
+// ---------------------------------------------------------------------------
 // particle edits
 // ---------------------------------------------------------------------------
 
@@ -1197,6 +1267,23 @@ int assemble_block_for(uint32_t max_deg, bool multi)
 }
 
 static const RowSpan kNoSpan{};
+
+cudaError_t launch_ray_cast(const ClothDev& c, const RayQuery& q, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(q.best, 0xff, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    if (c.t) k_ray_min<<<blocks_for(c.t, 256), 256, 0, st>>>(c, q);
+    k_ray_result<<<1, 32, 0, st>>>(c, q);
+    count_launches(c.t ? 2 : 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ray_result(const ClothDev& c, const RayQuery& q, cudaStream_t st)
+{
+    k_ray_result<<<1, 32, 0, st>>>(c, q);
+    count_launches(1);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st)
 {

@@ -269,6 +269,17 @@ b3g_status b3g_cloth_read_contacts(const b3g_cloth* cloth, uint8_t* exists, uint
  * and two tangent impulses.  A cloth of thickness 0 has no such contacts.
  * Cloths with self-collision take neither created particles nor mouse forces
  * (B3G_ERR_UNSUPPORTED), and cannot join a batch or a server. */
+/* b3Cloth::RayCastSingle (cloth.cpp:466-491): the first triangle the
+ * segment p1 -> p2 hits (b3RayCast, src/bounce/collision/collision.cpp:31-118),
+ * its fraction along the segment and the normal facing p1.  *hit is 0 when
+ * nothing is hit.  Equal fractions go to the lowest triangle index (the
+ * reference takes the first its tree visits). */
+b3g_status b3g_cloth_ray_cast_single(b3g_cloth* cloth, const float p1[3], const float p2[3], uint32_t* triangle,
+                                     float* fraction, float normal[3], int* hit);
+/* b3Cloth::RayCast (cloth.cpp:493-503): the segment against one triangle,
+ * up to max_fraction. */
+b3g_status b3g_cloth_ray_cast(b3g_cloth* cloth, const float p1[3], const float p2[3], float max_fraction,
+                              uint32_t triangle, float* fraction, float normal[3], int* hit);
 b3g_status b3g_cloth_read_tri_contacts(const b3g_cloth* cloth, uint32_t* count, uint32_t* pairs, uint8_t* active,
                                        float* weights, float* impulses);
 /* Of the last step: particle-triangle contacts alive after it, active ones

@@ -77,6 +77,8 @@ def port_lib():
         L.oc_describe.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_get_contacts.restype = C.c_uint32
         L.oc_get_contacts.argtypes = [C.c_void_p, _u8p, _u8p, _f32p]
+        L.oc_ray_cast_single.restype = C.c_int
+        L.oc_ray_cast_single.argtypes = [C.c_void_p, _f32p, _f32p, C.POINTER(C.c_uint32), C.POINTER(C.c_float), _f32p]
         L.oc_get_tri_contacts.restype = C.c_uint32
         L.oc_get_tri_contacts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_force_count.restype = C.c_uint32
@@ -139,6 +141,9 @@ def ref_lib():
         L.ref_cloth_describe.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_cloth_get_contacts.restype = C.c_uint32
         L.ref_cloth_get_contacts.argtypes = [C.c_void_p, _u8p, _u8p, _f32p]
+        L.ref_cloth_ray_cast_single.restype = C.c_int
+        L.ref_cloth_ray_cast_single.argtypes = [C.c_void_p, _f32p, _f32p, C.POINTER(C.c_uint32), C.POINTER(C.c_float),
+                                                _f32p]
         L.ref_cloth_get_tri_contacts.restype = C.c_uint32
         L.ref_cloth_get_tri_contacts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_cloth_build_system.restype = C.c_uint32
@@ -222,6 +227,13 @@ class _Base:
         imp = np.zeros(3 * self.n, np.float32)
         cnt = self._get_contacts(ex, ac, imp)
         return {"count": int(cnt), "exists": ex, "active": ac, "impulses": imp.reshape(-1, 3)}
+
+    def ray_cast_single(self, p1, p2):
+        """b3Cloth::RayCastSingle: (triangle, fraction, normal) or None."""
+        t, f = C.c_uint32(0), C.c_float(0.0)
+        n = np.zeros(3, np.float32)
+        hit = self._ray_cast_single(np.asarray(p1, np.float32), np.asarray(p2, np.float32), C.byref(t), C.byref(f), n)
+        return (int(t.value), float(f.value), n) if hit else None
 
     def tri_contacts(self):
         """Particle-triangle contacts in list order (head first)."""
@@ -356,6 +368,9 @@ class PortCloth(_Base):
     def _get_tri_contacts(self, *a):
         return self.L.oc_get_tri_contacts(self.h, *a)
 
+    def _ray_cast_single(self, *a):
+        return self.L.oc_ray_cast_single(self.h, *a)
+
     def _build_system(self, dt):
         return self.L.oc_build_system(self.h, dt)
 
@@ -444,6 +459,9 @@ class RefCloth(_Base):
 
     def _get_tri_contacts(self, *a):
         return self.L.ref_cloth_get_tri_contacts(self.h, *a)
+
+    def _ray_cast_single(self, *a):
+        return self.L.ref_cloth_ray_cast_single(self.h, *a)
 
     def _build_system(self, dt):
         return self.L.ref_cloth_build_system(self.h, dt)

@@ -2514,6 +2514,64 @@ uint32_t oc_get_contacts(const oc_cloth* c, uint8_t* exists, uint8_t* active, fl
     return c->ncontact;
 }
 
+/* b3RayCast against one triangle (collision.cpp:31-118): the hit fraction
+ * along p1 -> p2 and the normal facing the ray's start. */
+static int ray_triangle(v3 p1, v3 p2, float maxFraction, v3 v1, v3 v2, v3 v3_, float* fraction_out, v3* normal)
+{
+    v3 d = vsub(p2, p1);
+    if (d.x * d.x + d.y * d.y + d.z * d.z < kEps * kEps) return 0;
+    v3 n = vcross(vsub(v2, v1), vsub(v3_, v1));
+    float len = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
+    if (len == 0.0f) return 0;
+    float s1 = 1.0f / len; /* b3Vec3::operator/= */
+    n = V(n.x * s1, n.y * s1, n.z * s1);
+    float num = vdot(n, vsub(v1, p1));
+    float den = vdot(n, d);
+    if (den == 0.0f) return 0;
+    float fraction = num / den;
+    if (fraction < 0.0f || maxFraction < fraction) return 0;
+    v3 Q = vadd(p1, vscale(fraction, d));
+    v3 AB = vsub(v2, v1), AC = vsub(v3_, v1);
+    v3 QA = vsub(v1, Q), QB = vsub(v2, Q), QC = vsub(v3_, Q);
+    v3 AB_x_AC = vcross(AB, AC);
+    float u = vdot(vcross(QB, QC), AB_x_AC);
+    float v = vdot(vcross(QC, QA), AB_x_AC);
+    float w = vdot(vcross(QA, QB), AB_x_AC);
+    if (!(u >= 0.0f && v >= 0.0f && w >= 0.0f)) return 0;
+    *fraction_out = fraction;
+    *normal = num > 0.0f ? vneg(n) : n;
+    return 1;
+}
+
+/* b3Cloth::RayCastSingle (cloth.cpp:466-491): the triangle hit first along
+ * p1 -> p2.  Candidates are visited in triangle order (the reference visits
+ * them in its tree's order; only exact ties of the fraction can tell the
+ * two apart).  Returns 1 on a hit. */
+int oc_ray_cast_single(const oc_cloth* c, const float* p1, const float* p2, uint32_t* triangle, float* fraction,
+                       float* normal)
+{
+    v3 a = V(p1[0], p1[1], p1[2]), b = V(p2[0], p2[1], p2[2]);
+    uint32_t best = ~0u;
+    float best_f = FLT_MAX;
+    v3 best_n = vzero();
+    for (uint32_t k = 0; k < c->t; ++k) {
+        float f;
+        v3 n;
+        if (ray_triangle(a, b, 1.0f, c->x[c->tris[3 * k]], c->x[c->tris[3 * k + 1]], c->x[c->tris[3 * k + 2]], &f,
+                         &n) &&
+            f < best_f) {
+            best = k;
+            best_f = f;
+            best_n = n;
+        }
+    }
+    if (best == ~0u) return 0;
+    *triangle = best;
+    *fraction = best_f;
+    normal[0] = best_n.x; normal[1] = best_n.y; normal[2] = best_n.z;
+    return 1;
+}
+
 /* Particle-triangle contacts in list order (head first): particle and
  * triangle (2 per contact), active flag, barycentric weights w2, w3, w4 and
  * the normal and two tangent impulses (3 each).  Any pointer may be null. */

@@ -679,6 +679,19 @@ uint32_t ref_cloth_get_contacts(void* hp, uint8_t* exists, uint8_t* active, floa
     return count;
 }
 
+// b3Cloth::RayCastSingle: 1 on a hit, with the triangle, fraction and normal.
+int ref_cloth_ray_cast_single(void* hp, const float* p1, const float* p2, uint32_t* triangle, float* fraction,
+                              float* normal)
+{
+    RefCloth* h = (RefCloth*)hp;
+    b3ClothRayCastSingleOutput out;
+    if (!h->cloth->RayCastSingle(&out, b3Vec3(p1[0], p1[1], p1[2]), b3Vec3(p2[0], p2[1], p2[2]))) return 0;
+    *triangle = out.triangle;
+    *fraction = out.fraction;
+    put3(normal, out.normal);
+    return 1;
+}
+
 // Particle-triangle contacts in list order (head first): particle vertex and
 // triangle index (2 per contact), active flag, barycentric weights
 // m_w2, m_w3, m_w4 and the normal and two tangent impulses.  Any pointer may

@@ -353,3 +353,30 @@ def test_created_dynamic_particle_mass_and_fall(b3g):
     st2 = gpu.state()
     for q in ("x", "v", "dv"):
         assert np.array_equal(st[q], st2[q]), q
+
+
+def test_ray_cast_matches_oracle(b3g, port):
+    """b3Cloth::RayCastSingle and RayCast on the GPU against the oracle on the
+    same positions: same triangle, fraction and normal, bit for bit."""
+    scene = b3g.sphere_scene(24)
+    gpu, ora = _pair(b3g, port, scene)
+    rng = np.random.default_rng(9)
+    hits = 0
+    for step in range(20):
+        gpu.step(scene.dt)
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        for _ in range(10):
+            p1 = rng.uniform(-0.6, 0.6, 3).astype(np.float32)
+            p1[1] = 1.0
+            p2 = p1.copy()
+            p2[1] = -1.5
+            a, b = gpu.ray_cast_single(p1, p2), ora.ray_cast_single(p1, p2)
+            assert (a is None) == (b is None), step
+            if a is not None:
+                assert a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2]), step
+                single = gpu.ray_cast(p1, p2, a[0])
+                assert single is not None and single[0] == a[1] and np.array_equal(single[1], a[2])
+                assert gpu.ray_cast(p1, p2, a[0], max_fraction=0.5 * a[1]) is None
+                hits += 1
+    assert hits > 50

@@ -238,3 +238,31 @@ def test_hull_collider_matches_reference(seed):
         assert np.array_equal(cr["impulses"], cp["impulses"])
         active = max(active, int(cr["active"].sum()))
     assert active > 100
+
+
+def test_ray_cast_single_matches_reference():
+    """b3Cloth::RayCastSingle (the dragger's pick): the restatement finds
+    the same triangle, fraction and normal as the reference for vertical
+    segments through a falling cloth (the reference's full Step keeps its
+    triangle proxies up to date)."""
+    scene = sphere_scene(16)
+    ref = oracle.RefCloth(scene.mesh, scene.cdef, restated=False).setup(scene)
+    port = oracle.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    rng = np.random.default_rng(3)
+    hits = 0
+    for _ in range(30):
+        ref.step(scene.dt, full=True)
+        port.step(scene.dt)
+        for _ in range(10):
+            p1 = rng.uniform(-0.6, 0.6, 3).astype(np.float32)
+            p1[1] = 1.0
+            p2 = p1.copy()
+            p2[1] = -1.5
+            p2[0] += rng.normal(0.0, 0.2)
+            p2[2] += rng.normal(0.0, 0.2)
+            a, b = ref.ray_cast_single(p1, p2), port.ray_cast_single(p1, p2)
+            assert (a is None) == (b is None)
+            if a is not None:
+                assert a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2])
+                hits += 1
+    assert hits > 100
