@@ -547,6 +547,12 @@ def _sb_port():
         L.os_system.restype = C.c_uint32
         L.os_system.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_void_p]
+        L.os_set_node_radius.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.os_set_node_friction.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.os_add_hull.restype = C.c_int
+        L.os_add_hull.argtypes = [C.c_void_p, _f32p, C.c_uint32, _f32p, C.c_uint32, C.c_float]
+        L.os_get_contacts.restype = C.c_uint32
+        L.os_get_contacts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _sb_port_ready = True
     return L
 
@@ -571,6 +577,13 @@ def _sb_ref():
         L.ref_softbody_get_element_data.argtypes = [C.c_void_p, C.c_uint32, _f32p, _f32p, _f32p, _f32p]
         L.ref_softbody_energy.restype = C.c_float
         L.ref_softbody_energy.argtypes = [C.c_void_p]
+        L.ref_softbody_add_hull.restype = C.c_uint32
+        L.ref_softbody_add_hull.argtypes = [C.c_void_p, _f32p, C.c_uint32, C.c_float, _f32p, _f32p,
+                                            C.POINTER(C.c_uint32)]
+        L.ref_softbody_set_node_radius.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.ref_softbody_set_node_friction.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.ref_softbody_get_contacts.restype = C.c_uint32
+        L.ref_softbody_get_contacts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _sb_ref_ready = True
     return L
 
@@ -605,6 +618,15 @@ class _SoftBase:
         self._get_elements(q, e)
         return {"q": q, "eps": e}
 
+    def contacts(self):
+        """Node contacts with the (single) hull: per node exists, active,
+        impulses (normal, tangent x, tangent y)."""
+        ex = np.zeros(self.n, np.uint8)
+        ac = np.zeros(self.n, np.uint8)
+        imp = np.zeros(3 * self.n, np.float32)
+        cnt = self._get_contacts(ex.ctypes.data, ac.ctypes.data, imp.ctypes.data)
+        return {"count": int(cnt), "exists": ex, "active": ac, "impulses": imp.reshape(-1, 3)}
+
     def element_data(self, e):
         K = np.zeros(144, np.float32)
         invE = np.zeros(9, np.float32)
@@ -615,6 +637,20 @@ class _SoftBase:
 
 
 class PortSoftBody(_SoftBase):
+    def add_hull(self, vertices, planes, friction):
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1)
+        p = np.ascontiguousarray(planes, np.float32).reshape(-1)
+        return self.L.os_add_hull(self.h, v, v.size // 3, p, p.size // 4, friction)
+
+    def set_node_radius(self, i, r):
+        self.L.os_set_node_radius(self.h, i, r)
+
+    def set_node_friction(self, i, f):
+        self.L.os_set_node_friction(self.h, i, f)
+
+    def _get_contacts(self, *a):
+        return self.L.os_get_contacts(self.h, *a)
+
     def __init__(self, vertices, tets, density, E, nu, c_yield, c_creep, c_max):
         self.L = _sb_port()
         v = np.ascontiguousarray(vertices, np.float32).reshape(-1)
@@ -694,6 +730,23 @@ class PortSoftBody(_SoftBase):
 
 
 class RefSoftBody(_SoftBase):
+    def add_hull_from_points(self, points, friction):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1)
+        verts = np.zeros(3 * 256, np.float32)
+        planes = np.zeros(4 * 256, np.float32)
+        nf = C.c_uint32(0)
+        nv = self.L.ref_softbody_add_hull(self.h, pts, pts.size // 3, friction, verts, planes, C.byref(nf))
+        return verts[:3 * nv].reshape(-1, 3).copy(), planes[:4 * nf.value].reshape(-1, 4).copy()
+
+    def set_node_radius(self, i, r):
+        self.L.ref_softbody_set_node_radius(self.h, i, r)
+
+    def set_node_friction(self, i, f):
+        self.L.ref_softbody_set_node_friction(self.h, i, f)
+
+    def _get_contacts(self, *a):
+        return self.L.ref_softbody_get_contacts(self.h, *a)
+
     def __init__(self, vertices, tets, density, E, nu, c_yield, c_creep, c_max):
         self.L = _sb_ref()
         v = np.ascontiguousarray(vertices, np.float32).reshape(-1)

@@ -1030,6 +1030,64 @@ static float gjk_hull_point(const sphere_t* h, v3 Q, v3* p1, v3* p2)
     return vlength(vsub(*p1, *p2));
 }
 
+/* b3HullShape::TestSphere (hull_shape.cpp:187-254) for a hull on a static
+ * body at the origin, shared with the soft body oracle: vertices (3 floats
+ * each), planes (normal and offset), the sphere's centre q and radius
+ * (particle radius plus hull radius).  On contact: the normal (hull to
+ * sphere) and the contact point on the hull; returns 1. */
+int oc_hull_test_sphere(const float* vertices, uint32_t nv, const float* planes, uint32_t nf, float radius,
+                        const float* q, float* normal_out, float* point_out)
+{
+    sphere_t h;
+    memset(&h, 0, sizeof(h));
+    h.nhv = nv;
+    h.nhf = nf;
+    h.hv = (v3*)malloc((nv ? nv : 1) * sizeof(v3));
+    h.hn = (v3*)malloc((nf ? nf : 1) * sizeof(v3));
+    h.ho = (float*)malloc((nf ? nf : 1) * sizeof(float));
+    for (uint32_t i = 0; i < nv; ++i) h.hv[i] = V(vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]);
+    for (uint32_t i = 0; i < nf; ++i) {
+        h.hn[i] = V(planes[4 * i], planes[4 * i + 1], planes[4 * i + 2]);
+        h.ho[i] = planes[4 * i + 3];
+    }
+    v3 Q = V(q[0], q[1], q[2]), c1, c2, normal, point;
+    int hit = 1;
+    float distance = gjk_hull_point(&h, Q, &c1, &c2);
+    if (distance > radius) {
+        hit = 0;
+    } else if (distance > 0.0f) {
+        normal = vdiv(vsub(c2, c1), distance);
+        point = c1;
+    } else {
+        v3 support = xf_mult(Q);
+        uint32_t maxIndex = ~0u;
+        float maxSeparation = -FLT_MAX;
+        for (uint32_t f = 0; f < nf && hit; ++f) {
+            float separation = vdot(h.hn[f], support) - h.ho[f];
+            if (separation > radius) hit = 0;
+            else if (separation > maxSeparation) {
+                maxIndex = f;
+                maxSeparation = separation;
+            }
+        }
+        if (hit) {
+            v3 pn = vadd(vadd(vscale(h.hn[maxIndex].x, kIdX), vscale(h.hn[maxIndex].y, kIdY)),
+                         vscale(h.hn[maxIndex].z, kIdZ));
+            float po = h.ho[maxIndex] + vdot(pn, vzero());
+            float fraction = vdot(pn, Q) - po;
+            point = vsub(Q, vscale(fraction, pn));
+            normal = pn;
+        }
+    }
+    if (hit) {
+        normal_out[0] = normal.x; normal_out[1] = normal.y; normal_out[2] = normal.z;
+        v3 lp = xf_mult(point); /* body->GetLocalPoint */
+        point_out[0] = lp.x; point_out[1] = lp.y; point_out[2] = lp.z;
+    }
+    free(h.hv); free(h.hn); free(h.ho);
+    return hit;
+}
+
 void oc_set_solver(oc_cloth* c, int stop_rule, float tol, uint32_t max_iterations, int dot)
 {
     c->stop_rule = stop_rule;

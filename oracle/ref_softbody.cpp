@@ -20,6 +20,11 @@
 #include <bounce/softbody/softbody.h>
 #include <bounce/softbody/softbody_mesh.h>
 #include <bounce/softbody/softbody_node.h>
+#include <bounce/softbody/contacts/softbody_node_body_contact.h>
+#include <bounce/dynamics/world.h>
+#include <bounce/dynamics/body.h>
+#include <bounce/dynamics/shapes/hull_shape.h>
+#include <bounce/collision/shapes/qhull.h>
 #undef private
 #undef protected
 
@@ -32,6 +37,9 @@ struct RefSoftBody {
     std::vector<b3SoftBodyMeshTetrahedron> tets;
     b3SoftBodyMesh mesh;
     b3SoftBody* body = nullptr;
+    b3World* world = nullptr;
+    std::vector<b3QHull*> hulls;
+    std::vector<b3HullShape*> protos;
 };
 
 }  // namespace
@@ -74,7 +82,82 @@ void ref_softbody_destroy(void* p)
 {
     RefSoftBody* h = static_cast<RefSoftBody*>(p);
     delete h->body;
+    delete h->world;
+    for (b3HullShape* s : h->protos) delete s;
+    for (b3QHull* q : h->hulls) delete q;
     delete h;
+}
+
+// A world with a static body at the origin carrying a b3HullShape built by
+// the reference's quickhull from `points` (b3SoftBody::SetWorld); writes the
+// hull's vertices and planes (at most 256 each), returns the vertex count.
+uint32_t ref_softbody_add_hull(void* p, const float* points, uint32_t count, float friction, float* vertices,
+                               float* planes, uint32_t* face_count)
+{
+    RefSoftBody* h = static_cast<RefSoftBody*>(p);
+    if (!h->world) {
+        h->world = new b3World();
+        h->body->SetWorld(h->world);
+    }
+    std::vector<b3Vec3> pts(count);
+    for (uint32_t i = 0; i < count; ++i) pts[i].Set(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
+    b3QHull* hull = new b3QHull();
+    hull->Set(sizeof(b3Vec3), pts.data(), count);
+    h->hulls.push_back(hull);
+    b3BodyDef bd;
+    bd.type = e_staticBody;
+    b3Body* body = h->world->CreateBody(bd);
+    b3HullShape* shape = new b3HullShape();
+    shape->m_hull = hull;
+    h->protos.push_back(shape);
+    b3ShapeDef sd;
+    sd.shape = shape;
+    sd.friction = friction;
+    body->CreateShape(sd);
+    for (uint32_t i = 0; i < hull->vertexCount; ++i) {
+        vertices[3 * i] = hull->vertices[i].x;
+        vertices[3 * i + 1] = hull->vertices[i].y;
+        vertices[3 * i + 2] = hull->vertices[i].z;
+    }
+    for (uint32_t i = 0; i < hull->faceCount; ++i) {
+        planes[4 * i] = hull->planes[i].normal.x;
+        planes[4 * i + 1] = hull->planes[i].normal.y;
+        planes[4 * i + 2] = hull->planes[i].normal.z;
+        planes[4 * i + 3] = hull->planes[i].offset;
+    }
+    *face_count = hull->faceCount;
+    return hull->vertexCount;
+}
+
+// b3SoftBodyNode::SetRadius / SetFriction
+void ref_softbody_set_node_radius(void* p, uint32_t i, float r)
+{
+    static_cast<RefSoftBody*>(p)->body->m_nodes[i].SetRadius(r);
+}
+void ref_softbody_set_node_friction(void* p, uint32_t i, float f)
+{
+    static_cast<RefSoftBody*>(p)->body->m_nodes[i].SetFriction(f);
+}
+
+// Node-body contacts (one shape): per node exists, active, normal and
+// tangent impulses; returns the contact count.
+uint32_t ref_softbody_get_contacts(void* p, uint8_t* exists, uint8_t* active, float* impulses)
+{
+    RefSoftBody* h = static_cast<RefSoftBody*>(p);
+    const uint32_t n = h->mesh.vertexCount;
+    std::memset(exists, 0, n);
+    std::memset(active, 0, n);
+    std::memset(impulses, 0, 3 * (size_t)n * sizeof(float));
+    uint32_t count = 0;
+    for (b3NodeBodyContact* c = h->body->m_contactManager.m_nodeBodyContactList.m_head; c; c = c->m_next, ++count) {
+        const uint32_t v = c->m_n1->m_vertex;
+        exists[v] = 1;
+        active[v] = c->m_active ? 1 : 0;
+        impulses[3 * v] = c->m_normalImpulse;
+        impulses[3 * v + 1] = c->m_tangentImpulse.x;
+        impulses[3 * v + 2] = c->m_tangentImpulse.y;
+    }
+    return count;
 }
 
 void ref_softbody_set_type(void* p, uint32_t i, int type)

@@ -176,6 +176,32 @@ static m33* lrow_at(lrow* r, uint32_t col) /* b3SparseMat33::operator(), sparse_
     return &r->val[r->n++];
 }
 
+/* A static hull on a body at the origin (world frame), with its fattened
+ * proxy in the world broadphase. */
+typedef struct {
+    float* verts;
+    float* planes;
+    uint32_t nv, nf;
+    float friction;
+    v3 lo, hi;
+} os_hull;
+
+/* b3NodeBodyContact (softbody_node_body_contact.h) */
+typedef struct {
+    uint32_t node, shape;
+    int active;
+    v3 normal1, local_point2, tangent1, tangent2;
+    float normal_impulse, ti_x, ti_y;
+} os_contact;
+
+int oc_hull_test_sphere(const float* vertices, uint32_t nv, const float* planes, uint32_t nf, float radius,
+                        const float* q, float* normal_out, float* point_out);
+
+static const float kAabbExt = 0.2f;      /* B3_AABB_EXTENSION */
+static const float kLinSlop = 0.005f;    /* B3_LINEAR_SLOP */
+static const float kMaxCorr = 0.2f;      /* B3_MAX_LINEAR_CORRECTION */
+static const float kBaum = 0.1f;         /* B3_BAUMGARTE */
+
 struct os_body {
     uint32_t n, t;
     v3* rest; /* mesh vertices */
@@ -189,6 +215,14 @@ struct os_body {
     float tol;
     uint32_t max_iter;
     lrow* K; /* scratch rows */
+    /* contacts with a world of static hulls (softbody_contact_manager.cpp) */
+    float *radius, *friction;
+    v3 *fat_lo, *fat_hi;
+    os_hull hulls[4];
+    uint32_t nhull;
+    os_contact* contacts; /* tail first: element [ncontact - 1] is the list head */
+    uint32_t ncontact, contact_cap;
+    uint32_t active_contacts;
 };
 
 /* softbody.cpp:43-74 */
@@ -261,6 +295,17 @@ os_body* os_create(uint32_t nv, const float* vertices, uint32_t nt, const uint32
         b->x[i] = b->rest[i];
         b->type[i] = 2;
     }
+    /* node proxies (softbody.cpp:477-480): the point AABB fattened by
+     * B3_AABB_EXTENSION in CreateProxy */
+    b->radius = (float*)calloc(nv ? nv : 1, sizeof(float));
+    b->friction = (float*)calloc(nv ? nv : 1, sizeof(float));
+    b->fat_lo = (v3*)malloc((nv ? nv : 1) * sizeof(v3));
+    b->fat_hi = (v3*)malloc((nv ? nv : 1) * sizeof(v3));
+    for (uint32_t i = 0; i < nv; ++i) {
+        v3 r = V(0.0f, 0.0f, 0.0f), e = V(kAabbExt, kAabbExt, kAabbExt);
+        b->fat_lo[i] = vsub(vsub(b->x[i], r), e);
+        b->fat_hi[i] = vadd(vadd(b->x[i], r), e);
+    }
     b->stop_rule = 0;
     b->tol = 0.0f;
     b->max_iter = 20;
@@ -317,10 +362,46 @@ void os_destroy(os_body* b)
     free(b->type);
     free(b->tets);
     free(b->el);
+    free(b->radius); free(b->friction); free(b->fat_lo); free(b->fat_hi); free(b->contacts);
+    for (uint32_t k = 0; k < b->nhull; ++k) {
+        free(b->hulls[k].verts);
+        free(b->hulls[k].planes);
+    }
     free(b);
 }
 
 uint32_t os_node_count(const os_body* b) { return b->n; }
+
+/* b3BroadPhase::MoveProxy (broad_phase.cpp:99-149) for node i's proxy
+ * (b3SoftBodyNode::Synchronize, softbody_node.cpp:22-28). */
+static void node_move_proxy(os_body* b, uint32_t i, v3 displacement)
+{
+    v3 r = V(b->radius[i], b->radius[i], b->radius[i]);
+    v3 lo = vsub(b->x[i], r), hi = vadd(b->x[i], r);
+    v3 flo = b->fat_lo[i], fhi = b->fat_hi[i];
+    int contains = flo.x <= lo.x && lo.x <= fhi.x && flo.y <= lo.y && lo.y <= fhi.y && flo.z <= lo.z &&
+                   lo.z <= fhi.z && flo.x <= hi.x && hi.x <= fhi.x && flo.y <= hi.y && hi.y <= fhi.y &&
+                   flo.z <= hi.z && hi.z <= fhi.z;
+    if (contains) return;
+    v3 e = V(kAabbExt, kAabbExt, kAabbExt);
+    lo = vsub(lo, e);
+    hi = vadd(hi, e);
+    v3 d = vscale(2.0f, displacement); /* B3_AABB_MULTIPLIER */
+    if (d.x < 0.0f) lo.x += d.x; else hi.x += d.x;
+    if (d.y < 0.0f) lo.y += d.y; else hi.y += d.y;
+    if (d.z < 0.0f) lo.z += d.z; else hi.z += d.z;
+    b->fat_lo[i] = lo;
+    b->fat_hi[i] = hi;
+}
+
+/* b3SoftBodyNode::DestroyContacts (softbody_node.cpp:30-48) */
+static void node_destroy_contacts(os_body* b, uint32_t i)
+{
+    uint32_t w = 0;
+    for (uint32_t k = 0; k < b->ncontact; ++k)
+        if (b->contacts[k].node != i) b->contacts[w++] = b->contacts[k];
+    b->ncontact = w;
+}
 
 /* b3SoftBodyNode::SetType (softbody_node.h:146-163) */
 void os_set_type(os_body* b, uint32_t i, int type)
@@ -328,13 +409,231 @@ void os_set_type(os_body* b, uint32_t i, int type)
     if (b->type[i] == type) return;
     b->type[i] = type;
     b->f[i] = vzero();
-    if (type == 0) b->v[i] = vzero();
+    if (type == 0) {
+        b->v[i] = vzero();
+        node_move_proxy(b, i, vzero());
+    }
+    node_destroy_contacts(b, i);
+}
+
+/* b3SoftBodyNode::SetRadius / SetFriction (softbody_node.h:218-235) */
+void os_set_node_radius(os_body* b, uint32_t i, float radius)
+{
+    b->radius[i] = radius;
+    node_move_proxy(b, i, vzero());
+}
+void os_set_node_friction(os_body* b, uint32_t i, float friction) { b->friction[i] = friction; }
+
+/* A static b3HullShape on a body at the origin, in the soft body's world
+ * (b3SoftBody::SetWorld): proxy as b3HullShape::ComputeAABB fattened. */
+int os_add_hull(os_body* b, const float* vertices, uint32_t nv, const float* planes, uint32_t nf, float friction)
+{
+    if (b->nhull >= 4 || nv == 0) return -1;
+    os_hull* h = b->hulls + b->nhull;
+    h->verts = (float*)malloc(3 * (size_t)nv * sizeof(float));
+    h->planes = (float*)malloc(4 * (size_t)(nf ? nf : 1) * sizeof(float));
+    memcpy(h->verts, vertices, 3 * (size_t)nv * sizeof(float));
+    memcpy(h->planes, planes, 4 * (size_t)nf * sizeof(float));
+    h->nv = nv;
+    h->nf = nf;
+    h->friction = friction;
+    /* b3Mul(xf, v) with the identity at the origin, then min / max */
+    for (uint32_t k = 0; k < nv; ++k) {
+        const float* v = vertices + 3 * k;
+        v3 w = vadd(vadd(vadd(vscale(v[0], V(1.0f, 0.0f, 0.0f)), vscale(v[1], V(0.0f, 1.0f, 0.0f))),
+                         vscale(v[2], V(0.0f, 0.0f, 1.0f))),
+                    vzero());
+        if (k == 0) {
+            h->lo = w;
+            h->hi = w;
+        } else {
+            h->lo = V(h->lo.x < w.x ? h->lo.x : w.x, h->lo.y < w.y ? h->lo.y : w.y, h->lo.z < w.z ? h->lo.z : w.z);
+            h->hi = V(h->hi.x > w.x ? h->hi.x : w.x, h->hi.y > w.y ? h->hi.y : w.y, h->hi.z > w.z ? h->hi.z : w.z);
+        }
+    }
+    v3 e = V(kAabbExt, kAabbExt, kAabbExt), r = vzero();
+    h->lo = vsub(vsub(h->lo, r), e);
+    h->hi = vadd(vadd(h->hi, r), e);
+    return (int)b->nhull++;
+}
+
+static inline int sb_overlap(v3 alo, v3 ahi, v3 blo, v3 bhi)
+{
+    return alo.x <= bhi.x && alo.y <= bhi.y && alo.z <= bhi.z && ahi.x >= blo.x && ahi.y >= blo.y && ahi.z >= blo.z;
+}
+
+static inline v3 sb_perp(v3 v)
+{
+    if (fabsf(v.x) >= 0.57735027f) return V(v.y, -v.x, 0.0f);
+    return V(0.0f, v.z, -v.y);
+}
+
+/* UpdateBodyContacts (softbody_contact_manager.cpp:109-150) with
+ * b3NodeBodyContact::Update (softbody_node_body_contact.cpp:24-47). */
+static void sb_update_contacts(os_body* b)
+{
+    uint32_t w = 0;
+    for (uint32_t q = 0; q < b->ncontact; ++q) {
+        os_contact k = b->contacts[q];
+        if (b->type[k.node] != 2) continue;  /* the shape's body is static */
+        const os_hull* h = b->hulls + k.shape;
+        if (!sb_overlap(b->fat_lo[k.node], b->fat_hi[k.node], h->lo, h->hi)) continue;
+        float q3[3] = {b->x[k.node].x, b->x[k.node].y, b->x[k.node].z}, nrm[3], pt[3];
+        if (!oc_hull_test_sphere(h->verts, h->nv, h->planes, h->nf, 0.0f + b->radius[k.node], q3, nrm, pt)) {
+            k.active = 0;
+        } else {
+            k.active = 1;
+            k.normal1 = vneg(V(nrm[0], nrm[1], nrm[2]));
+            k.local_point2 = V(pt[0], pt[1], pt[2]);
+            k.tangent1 = sb_perp(k.normal1);
+            k.tangent2 = vcross(k.tangent1, k.normal1);
+        }
+        b->contacts[w++] = k;
+    }
+    b->ncontact = w;
+}
+
+/* FindNewBodyContacts + AddNSPair (softbody_contact_manager.cpp:44-107):
+ * dynamic nodes in index order, each against every overlapping shape. */
+static void sb_find_new_contacts(os_body* b)
+{
+    for (uint32_t i = 0; i < b->n; ++i) {
+        if (b->type[i] != 2) continue;
+        for (uint32_t sh = 0; sh < b->nhull; ++sh) {
+            if (!sb_overlap(b->fat_lo[i], b->fat_hi[i], b->hulls[sh].lo, b->hulls[sh].hi)) continue;
+            int exists = 0;
+            for (uint32_t q = 0; q < b->ncontact && !exists; ++q)
+                exists = b->contacts[q].node == i && b->contacts[q].shape == sh;
+            if (exists) continue;
+            if (b->ncontact == b->contact_cap) {
+                b->contact_cap = b->contact_cap ? 2 * b->contact_cap : 256;
+                b->contacts = (os_contact*)realloc(b->contacts, b->contact_cap * sizeof(os_contact));
+            }
+            os_contact* c = b->contacts + b->ncontact++;
+            memset(c, 0, sizeof(*c));
+            c->node = i;
+            c->shape = sh;
+        }
+    }
+}
+
+/* The contact part of b3SoftBodySolver::Solve (softbody_solver.cpp:62-126)
+ * with b3SoftBodyContactSolver (softbody_contact_solver.cpp) for static
+ * bodies (inverse mass and inertia 0, zero velocity). */
+static void sb_solve_contacts(os_body* b, float h, uint32_t vel_iters, uint32_t pos_iters)
+{
+    uint32_t na = 0;
+    for (uint32_t q = 0; q < b->ncontact; ++q) na += b->contacts[q].active != 0;
+    b->active_contacts = na;
+    os_contact** ac = (os_contact**)malloc((na + 1) * sizeof(os_contact*));
+    float* nmass = (float*)malloc((na + 1) * sizeof(float));
+    float* tm = (float*)malloc(4 * (na + 1) * sizeof(float));
+    uint32_t w = 0;
+    for (uint32_t q = b->ncontact; q-- > 0;) /* list order, head first */
+        if (b->contacts[q].active) ac[w++] = b->contacts + q;
+    for (uint32_t k = 0; k < na; ++k) {
+        const uint32_t i = ac[k]->node;
+        const float mA = b->type[i] == 0 ? 0.0f : 1.0f / b->mass[i];
+        float K = mA + 0.0f + 0.0f + 0.0f;
+        nmass[k] = K > 0.0f ? 1.0f / K : 0.0f;
+        float k11 = mA + 0.0f + 0.0f + 0.0f, k12 = 0.0f + 0.0f, k22 = mA + 0.0f + 0.0f + 0.0f;
+        float det = k11 * k22 - k12 * k12;
+        if (det != 0.0f) det = 1.0f / det;
+        tm[4 * k] = det * k22;
+        tm[4 * k + 1] = -det * k12;
+        tm[4 * k + 2] = -det * k12;
+        tm[4 * k + 3] = det * k11;
+    }
+    /* WarmStart */
+    for (uint32_t k = 0; k < na; ++k) {
+        os_contact* c = ac[k];
+        const uint32_t i = c->node;
+        const float mA = b->type[i] == 0 ? 0.0f : 1.0f / b->mass[i];
+        v3 vA = b->v[i];
+        v3 P = vscale(c->normal_impulse, c->normal1);
+        vA = vsub(vA, vscale(mA, P));
+        v3 P1 = vscale(c->ti_x, c->tangent1), P2 = vscale(c->ti_y, c->tangent2);
+        vA = vsub(vA, vscale(mA, vadd(P1, P2)));
+        b->v[i] = vA;
+    }
+    for (uint32_t it = 0; it < vel_iters; ++it)
+        for (uint32_t k = 0; k < na; ++k) {
+            os_contact* c = ac[k];
+            const uint32_t i = c->node;
+            const float mA = b->type[i] == 0 ? 0.0f : 1.0f / b->mass[i];
+            const float fr = sqrtf(b->friction[i] * b->hulls[c->shape].friction);
+            v3 vA = b->v[i];
+            {
+                v3 dv = vsub(vzero(), vA);
+                float Cdot = vdot(c->normal1, dv);
+                float impulse = nmass[k] * (-Cdot + 0.0f);
+                float old = c->normal_impulse;
+                float sum = old + impulse;
+                c->normal_impulse = sum > 0.0f ? sum : 0.0f;
+                impulse = c->normal_impulse - old;
+                vA = vsub(vA, vscale(mA, vscale(impulse, c->normal1)));
+            }
+            {
+                v3 dv = vsub(vzero(), vA);
+                float cx = vdot(dv, c->tangent1), cy = vdot(dv, c->tangent2);
+                float ncx = -cx, ncy = -cy;
+                float ix = ncx * tm[4 * k] + ncy * tm[4 * k + 1];
+                float iy = ncx * tm[4 * k + 2] + ncy * tm[4 * k + 3];
+                float ox = c->ti_x, oy = c->ti_y;
+                c->ti_x += ix;
+                c->ti_y += iy;
+                float maxImpulse = fr * c->normal_impulse;
+                if (c->ti_x * c->ti_x + c->ti_y * c->ti_y > maxImpulse * maxImpulse) {
+                    float sl = sqrtf(c->ti_x * c->ti_x + c->ti_y * c->ti_y);
+                    if (sl > kEps) {
+                        c->ti_x /= sl;
+                        c->ti_y /= sl;
+                    }
+                    c->ti_x *= maxImpulse;
+                    c->ti_y *= maxImpulse;
+                }
+                float jx = c->ti_x - ox, jy = c->ti_y - oy;
+                v3 P = vadd(vscale(jx, c->tangent1), vscale(jy, c->tangent2));
+                vA = vsub(vA, vscale(mA, P));
+            }
+            b->v[i] = vA;
+        }
+    /* integrate positions */
+    for (uint32_t i = 0; i < b->n; ++i) b->x[i] = vadd(b->x[i], vscale(h, b->v[i]));
+    for (uint32_t it = 0; it < pos_iters; ++it) {
+        float minSeparation = 0.0f;
+        for (uint32_t k = 0; k < na; ++k) {
+            os_contact* c = ac[k];
+            const uint32_t i = c->node;
+            const float mA = b->type[i] == 0 ? 0.0f : 1.0f / b->mass[i];
+            v3 cA = b->x[i];
+            float separation = vdot(vsub(c->local_point2, cA), c->normal1) - b->radius[i] - 0.0f;
+            minSeparation = minSeparation < separation ? minSeparation : separation;
+            float Cv = kBaum * (separation + kLinSlop);
+            float C = Cv < 0.0f ? Cv : 0.0f;
+            C = -kMaxCorr > C ? -kMaxCorr : C;
+            float K = mA + 0.0f + 0.0f + 0.0f;
+            float impulse = K > 0.0f ? -C / K : 0.0f;
+            cA = vsub(cA, vscale(mA, vscale(impulse, c->normal1)));
+            b->x[i] = cA;
+        }
+        if (minSeparation >= -3.0f * kLinSlop) break;
+    }
+    free(ac);
+    free(nmass);
+    free(tm);
 }
 void os_set_mass_damping(os_body* b, uint32_t i, float d) { b->damping[i] = d; }
 void os_set_gravity(os_body* b, const float* g) { b->gravity = V(g[0], g[1], g[2]); }
 /* b3SoftBodyNode::ApplyForce: m_force += force */
 void os_apply_force(os_body* b, uint32_t i, const float* f) { b->f[i] = vadd(b->f[i], V(f[0], f[1], f[2])); }
-void os_set_position(os_body* b, uint32_t i, const float* x) { b->x[i] = V(x[0], x[1], x[2]); }
+void os_set_position(os_body* b, uint32_t i, const float* x)
+{
+    v3 p = V(x[0], x[1], x[2]);
+    v3 d = vsub(p, b->x[i]);
+    b->x[i] = p;
+    node_move_proxy(b, i, d);
+}
 void os_set_velocity(os_body* b, uint32_t i, const float* v)
 {
     if (b->type[i] == 0) return;
@@ -538,6 +837,8 @@ void os_step(os_body* b, float dt, uint32_t velocity_iterations, uint32_t positi
 {
     os_stats st;
     memset(&st, 0, sizeof(st));
+    b->active_contacts = 0;
+    if (b->nhull) sb_update_contacts(b);
     if (dt > 0.0f) {
         const uint32_t n = b->n;
         lrow* arows = (lrow*)calloc(n, sizeof(lrow));
@@ -546,13 +847,39 @@ void os_step(os_body* b, float dt, uint32_t velocity_iterations, uint32_t positi
         form_system(b, dt, arows, rhs);
         mpcg(b, arows, rhs, sx, &st);
         for (uint32_t i = 0; i < n; ++i) b->v[i] = sx[i];
-        for (uint32_t i = 0; i < n; ++i) b->x[i] = vadd(b->x[i], vscale(dt, b->v[i]));
+        if (b->nhull) sb_solve_contacts(b, dt, velocity_iterations, position_iterations);
+        else
+            for (uint32_t i = 0; i < n; ++i) b->x[i] = vadd(b->x[i], vscale(dt, b->v[i]));
         free_rows(arows, n);
         free(rhs);
         free(sx);
     }
     for (uint32_t i = 0; i < b->n; ++i) b->f[i] = vzero();
+    if (b->nhull) {
+        /* node proxies (softbody.cpp:764-775), then FindNewBodyContacts */
+        for (uint32_t i = 0; i < b->n; ++i)
+            if (b->type[i] != 0) node_move_proxy(b, i, vscale(dt, b->v[i]));
+        sb_find_new_contacts(b);
+    }
     if (out) *out = st;
+}
+
+/* Node contacts (one shape): per node exists, active, impulses (normal,
+ * tangent x, tangent y); returns the contact count. */
+uint32_t os_get_contacts(const os_body* b, uint8_t* exists, uint8_t* active, float* impulses)
+{
+    memset(exists, 0, b->n);
+    memset(active, 0, b->n);
+    memset(impulses, 0, 3 * (size_t)b->n * sizeof(float));
+    for (uint32_t q = 0; q < b->ncontact; ++q) {
+        const os_contact* c = b->contacts + q;
+        exists[c->node] = 1;
+        active[c->node] = (uint8_t)(c->active != 0);
+        impulses[3 * c->node] = c->normal_impulse;
+        impulses[3 * c->node + 1] = c->ti_x;
+        impulses[3 * c->node + 2] = c->ti_y;
+    }
+    return b->ncontact;
 }
 
 void os_get_state(const os_body* b, float* x, float* v)

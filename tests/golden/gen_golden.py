@@ -101,6 +101,42 @@ def hull_trajectory(side, steps, keep):
     return out
 
 
+def softbody_ground_points():
+    """A ground slab's corners: 6 m x 0.5 m x 6 m, top at y = -1.5 m."""
+    return np.array([(x, y, z) for x in (-3.0, 3.0) for y in (-2.0, -1.5) for z in (-3.0, 3.0)], np.float32)
+
+
+def softbody_hull(steps, keep):
+    """A 4 x 3 x 3 block (0.5 m cells, nothing pinned) falling onto a static
+    ground hull built by the reference's quickhull; every node with radius
+    0.05 and friction 0.2 (as examples/testbed/tests/smash_softbody.h sets
+    them).  States and node contacts at the kept steps."""
+    scene = pinned_block_scene(4, 3, 3, 0.5)
+    sd = scene.sdef
+    args = (scene.vertices, scene.tets, sd.density, sd.E, sd.nu, sd.c_yield, sd.c_creep, sd.c_max)
+    scene.static_nodes = np.zeros(0, np.uint32)
+    ref = oracle.RefSoftBody(*args).setup(scene)
+    hv, hp = ref.add_hull_from_points(softbody_ground_points(), 0.6)
+    for i in range(len(scene.vertices)):
+        ref.set_node_radius(i, 0.05)
+        ref.set_node_friction(i, 0.2)
+    out = {"vertices": scene.vertices, "tets": scene.tets,
+           "def": np.array([sd.density, sd.E, sd.nu, sd.c_yield, sd.c_creep, sd.c_max], np.float32),
+           "mass_damping": scene.mass_damping, "dt": np.float32(scene.dt),
+           "gravity": np.asarray(scene.gravity, np.float32), "hull_vertices": hv, "hull_planes": hp,
+           "hull_friction": np.float32(0.6), "node_radius": np.float32(0.05), "node_friction": np.float32(0.2)}
+    iters = []
+    for k in range(1, steps + 1):
+        iters.append(ref.step(scene.dt)["iterations"])
+        if k in keep:
+            st, c = ref.state(), ref.contacts()
+            out[f"x_{k}"], out[f"v_{k}"] = st["x"], st["v"]
+            out[f"contact_exists_{k}"], out[f"contact_active_{k}"] = c["exists"], c["active"]
+            out[f"contact_impulses_{k}"] = c["impulses"]
+    out["iterations"] = np.asarray(iters, np.uint32)
+    return out
+
+
 def system(scene):
     ref = oracle.RefCloth(scene.mesh, scene.cdef, restated=False).setup(scene)
     ref.step(scene.dt, scene.velocity_iterations, scene.position_iterations)
@@ -156,6 +192,7 @@ def main():
         "system16_bend_ref.npz": system(sphere_scene(16, seed=4)),
         "self_collision11_ref.npz": self_collision(self_collision_scene(11), 130, {1, 60, 90, 100, 115, 130}),
         "hull16_ref.npz": hull_trajectory(16, 120, {1, 30, 60, 120}),
+        "softbody_hull_ref.npz": softbody_hull(150, {1, 25, 75, 150}),
     }
     only = set(sys.argv[1:])
     for name, data in files.items():

@@ -80,3 +80,39 @@ def test_softbody_oracle_matches_live_reference(dims):
         ea, eb = port.elements(), ref.elements()
         assert np.array_equal(ea["q"], eb["q"]) and np.array_equal(ea["eps"], eb["eps"]), k
     assert port.energy() == ref.energy()
+
+
+def softbody_hull_golden():
+    """The scene of softbody_hull_ref.npz: a block falling onto a ground
+    hull (the reference's quickhull output, stored in the file)."""
+    import os
+
+    from bounce_b200.meshes import SoftBodyDef, SoftBodyScene
+
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "softbody_hull_ref.npz"))
+    sdef = SoftBodyDef(*[float(x) for x in d["def"]])
+    scene = SoftBodyScene(d["vertices"], d["tets"], sdef, d["mass_damping"], np.zeros(0, np.uint32),
+                          gravity=tuple(float(g) for g in d["gravity"]), dt=float(d["dt"]))
+    return d, scene
+
+
+def test_softbody_hull_contacts_match_golden(port):
+    """Node contacts with a static hull (b3SoftBody with a world,
+    softbody_contact_manager.cpp, softbody_contact_solver.cpp): the
+    restatement reproduces the reference's trajectory and contacts."""
+    d, scene = softbody_hull_golden()
+    s = scene.sdef
+    b = port.PortSoftBody(scene.vertices, scene.tets, s.density, s.E, s.nu, s.c_yield, s.c_creep,
+                          s.c_max).setup(scene)
+    b.add_hull(d["hull_vertices"], d["hull_planes"], float(d["hull_friction"]))
+    for i in range(len(scene.vertices)):
+        b.set_node_radius(i, float(d["node_radius"]))
+        b.set_node_friction(i, float(d["node_friction"]))
+    for k in range(1, len(d["iterations"]) + 1):
+        assert b.step(scene.dt)["iterations"] == d["iterations"][k - 1], k
+        if f"x_{k}" in d:
+            st, c = b.state(), b.contacts()
+            assert np.array_equal(st["x"], d[f"x_{k}"]) and np.array_equal(st["v"], d[f"v_{k}"]), k
+            for q in ("exists", "active", "impulses"):
+                assert np.array_equal(c[q], d[f"contact_{q}_{k}"]), (k, q)
+    assert int(d["contact_active_150"].sum()) > 10
