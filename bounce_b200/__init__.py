@@ -214,6 +214,10 @@ def lib() -> C.CDLL:
             "b3g_softbody_read_masses": [vp, vp],
             "b3g_softbody_energy": [vp, C.POINTER(f32)],
             "b3g_softbody_export_system": [vp, f32, u32, vp, vp, vp, vp, vp, C.POINTER(u32)],
+            "b3g_softbody_add_static_hull": [vp, vp, u32, vp, u32, f32, C.POINTER(u32)],
+            "b3g_softbody_set_node_radius": [vp, u32, f32],
+            "b3g_softbody_set_node_friction": [vp, u32, f32],
+            "b3g_softbody_read_contacts": [vp, vp, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -727,6 +731,7 @@ class SoftBody:
                                     C.byref(h)), "b3g_softbody_create")
         self.h = h.value
         self.n, self.t = len(self._v), len(self._t)
+        self.nhull = 0
         self.stats = StepStatsC()
 
     def close(self) -> None:
@@ -779,6 +784,33 @@ class SoftBody:
     def set_solver(self, o: SolverOptions) -> None:
         c = SolverOptsC(o.stop_rule, o.tolerance, o.max_iterations, o.dot)
         check(lib().b3g_softbody_set_solver(self.h, C.byref(c)), "softbody_set_solver")
+
+    def add_hull(self, vertices, planes, friction: float) -> int:
+        """A static convex hull the nodes collide with: vertices (n, 3) and
+        face planes (f, 4: normal, offset), world frame."""
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        p = np.ascontiguousarray(planes, np.float32).reshape(-1, 4)
+        sid = C.c_uint32(0)
+        check(lib().b3g_softbody_add_static_hull(self.h, _ptr(v), len(v), _ptr(p), len(p), friction, C.byref(sid)),
+              "softbody_add_static_hull")
+        self.nhull += 1
+        return sid.value
+
+    def set_node_radius(self, i: int, r: float) -> None:
+        check(lib().b3g_softbody_set_node_radius(self.h, i, r), "softbody_set_node_radius")
+
+    def set_node_friction(self, i: int, f: float) -> None:
+        check(lib().b3g_softbody_set_node_friction(self.h, i, f), "softbody_set_node_friction")
+
+    def contacts(self) -> dict:
+        """Node contacts per (hull, node), hull-major: exists, active and the
+        (normal, tangent, tangent) impulses."""
+        m = self.nhull * self.n
+        ex = np.zeros(m, np.uint8)
+        ac = np.zeros(m, np.uint8)
+        imp = np.zeros(3 * m, np.float32)
+        check(lib().b3g_softbody_read_contacts(self.h, _ptr(ex), _ptr(ac), _ptr(imp)), "softbody_read_contacts")
+        return {"exists": ex, "active": ac, "impulses": imp.reshape(-1, 3)}
 
     def step(self, dt: float, velocity_iterations: int = 8, position_iterations: int = 2) -> dict:
         check(lib().b3g_softbody_step(self.h, dt, velocity_iterations, position_iterations, C.byref(self.stats)),

@@ -14,6 +14,7 @@
 
 namespace b3g {
 namespace hull {
+namespace {  // internal linkage: every file that includes this gets its own copy
 
 struct Vtx {
     f3 p1, p2, p;
@@ -348,5 +349,6 @@ __device__ __forceinline__ bool test_sphere(const float* hv, uint32_t nv, const 
     return true;
 }
 
+}  // namespace
 }  // namespace hull
 }  // namespace b3g

@@ -20,6 +20,7 @@
 // element and assembly arithmetic is the reference's; the one difference is
 // the C library's double sin and cos in b3Quat::Set against CUDA's, which can
 // differ in the last bit of the rounded float in rare cases.
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -27,6 +28,7 @@
 #include "../../include/b3g.h"
 #include "cloth_dev.cuh"
 #include "mpcg_solve.cuh"
+#include "hull_gjk.cuh"
 #include "softbody_prep.h"
 #include "vec.cuh"
 
@@ -50,6 +52,19 @@ struct SoftDev {
     const uint32_t *inc_ptr, *inc_elem, *inc_meta;
     float *b, *S, *xsol;
     float gx, gy, gz;
+
+    // contacts with static hulls (b3SoftBody::SetWorld): node radius and
+    // friction, node proxies (fat AABBs, 3 floats per node for lo and hi),
+    // and per (hull, node) contact slots; the proxies are kept from creation
+    float *radius, *friction, *fat_lo, *fat_hi;
+    uint32_t nhull, step_index;
+    SphereDev hull[kMaxSpheres];
+    uint8_t *c_exists, *c_active;
+    uint32_t* c_key;                // creation key: step index * kMaxSpheres + hull
+    float *c_normal, *c_t1, *c_t2, *c_point, *c_imp;  // 3 planes of nhull * n each
+    int* min_sep;                   // per position iteration, order-preserving ints
+    uint32_t* active_count;
+    uint32_t vel_iters, pos_iters;
 };
 
 namespace {
@@ -335,6 +350,44 @@ __global__ void __launch_bounds__(32 * kAsmWarps) k_sb_assemble(SoftDev d, float
     }
 }
 
+// b3BroadPhase::MoveProxy for node i's proxy (b3SoftBodyNode::Synchronize,
+// softbody_node.cpp:22-28; broad_phase.cpp:99-149)
+__device__ void node_move_proxy(const SoftDev& d, uint32_t i, f3 disp)
+{
+    const f3 x = ldv(d.x, i);
+    const float r = d.radius[i];
+    float lo[3] = {d.fat_lo[3 * i], d.fat_lo[3 * i + 1], d.fat_lo[3 * i + 2]};
+    float hi[3] = {d.fat_hi[3 * i], d.fat_hi[3 * i + 1], d.fat_hi[3 * i + 2]};
+    const float tlo[3] = {x.x - r, x.y - r, x.z - r}, thi[3] = {x.x + r, x.y + r, x.z + r};
+    bool contains = true;
+    for (int k = 0; k < 3; ++k) contains = contains && lo[k] <= tlo[k] && tlo[k] <= hi[k] && lo[k] <= thi[k] && thi[k] <= hi[k];
+    if (contains) return;
+    const float dd[3] = {2.0f * disp.x, 2.0f * disp.y, 2.0f * disp.z};
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = tlo[k] - 0.2f;
+        hi[k] = thi[k] + 0.2f;
+        if (dd[k] < 0.0f) lo[k] += dd[k];
+        else hi[k] += dd[k];
+        d.fat_lo[3 * i + k] = lo[k];
+        d.fat_hi[3 * i + k] = hi[k];
+    }
+}
+
+__device__ __forceinline__ bool node_overlap(const SoftDev& d, uint32_t i, const SphereDev& s)
+{
+    return d.fat_lo[3 * i] <= s.hi[0] && d.fat_lo[3 * i + 1] <= s.hi[1] && d.fat_lo[3 * i + 2] <= s.hi[2] &&
+           d.fat_hi[3 * i] >= s.lo[0] && d.fat_hi[3 * i + 1] >= s.lo[1] && d.fat_hi[3 * i + 2] >= s.lo[2];
+}
+
+__device__ __forceinline__ int sb_enc(float f)
+{
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float sb_dec(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+// Without hulls: v = solution, x += h v, forces cleared, node proxies moved
+// (softbody_solver.cpp:105-110, softbody.cpp:716-775)
 __global__ void k_sb_integrate(SoftDev d, float h)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -343,6 +396,216 @@ __global__ void k_sb_integrate(SoftDev d, float h)
     stv(d.v, i, v);
     stv(d.x, i, ldv(d.x, i) + h * v);
     stv(d.f, i, zero3());
+    if (d.type[i] != 0) node_move_proxy(d, i, h * v);
+}
+
+// UpdateBodyContacts (softbody_contact_manager.cpp:109-150) with
+// b3NodeBodyContact::Update and b3HullShape::TestSphere
+__global__ void k_sb_contacts_update(SoftDev d)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const uint32_t n = d.n, nn = (uint32_t)kMaxSpheres * n;  // slot planes laid out for the hull capacity
+    const f3 xi = ldv(d.x, i);
+    for (uint32_t s = 0; s < d.nhull; ++s) {
+        const uint32_t q = s * n + i;
+        if (!d.c_exists[q]) continue;
+        const SphereDev& sp = d.hull[s];
+        if (d.type[i] != 2 || !node_overlap(d, i, sp)) {
+            d.c_exists[q] = 0;
+            d.c_active[q] = 0;
+            continue;
+        }
+        f3 normal, P;
+        if (!hull::test_sphere(sp.hull, sp.nhv, sp.hull + 3 * sp.nhv, sp.nhf, sp.radius + d.radius[i], xi, normal, P)) {
+            d.c_active[q] = 0;
+            continue;
+        }
+        const f3 n1 = mk(-normal.x, -normal.y, -normal.z);
+        const f3 t1 = perp(n1);
+        const f3 t2 = cross(t1, n1);
+        d.c_active[q] = 1;
+        st3(d.c_normal, nn, q, n1);
+        st3(d.c_t1, nn, q, t1);
+        st3(d.c_t2, nn, q, t2);
+        st3(d.c_point, nn, q, hull::xf_mult(P));
+    }
+}
+
+// Node i's active contacts in list order (newest first).
+__device__ int sb_contact_order(const SoftDev& d, uint32_t i, int* order)
+{
+    int k = 0;
+    const uint32_t n = d.n;
+    for (uint32_t s = 0; s < d.nhull; ++s)
+        if (d.c_exists[s * n + i] && d.c_active[s * n + i]) order[k++] = (int)s;
+    for (int a = 1; a < k; ++a) {
+        const int v = order[a];
+        int b = a - 1;
+        while (b >= 0 && d.c_key[order[b] * n + i] < d.c_key[v * n + i]) {
+            order[b + 1] = order[b];
+            --b;
+        }
+        order[b + 1] = v;
+    }
+    return k;
+}
+
+// One position iteration for node i (softbody_contact_solver.cpp:330-410);
+// returns its smallest separation.
+__device__ float sb_position_iteration(const SoftDev& d, uint32_t i, f3& pos, const int* order, int k, float mA)
+{
+    const uint32_t n = d.n, nn = (uint32_t)kMaxSpheres * n;  // slot planes laid out for the hull capacity
+    float min_sep = 0.0f;
+    for (int a = 0; a < k; ++a) {
+        const uint32_t q = order[a] * n + i;
+        const f3 nA = ld3(d.c_normal, nn, q);
+        const f3 cB = ld3(d.c_point, nn, q);
+        const float separation = dot(cB - pos, nA) - d.radius[i] - d.hull[order[a]].radius;
+        min_sep = min_sep < separation ? min_sep : separation;
+        const float Cv = 0.1f * (separation + 0.005f);
+        float C = Cv < 0.0f ? Cv : 0.0f;
+        C = -0.2f > C ? -0.2f : C;
+        const float K = mA + 0.0f + 0.0f + 0.0f;
+        const float impulse = K > 0.0f ? -C / K : 0.0f;
+        pos = pos - mA * (impulse * nA);
+    }
+    return min_sep;
+}
+
+// With hulls: v = solution, then the contact solve of b3SoftBodySolver::Solve
+// (softbody_solver.cpp:62-126) for node i -- warm start, velocity
+// iterations, impulses stored, x += h v, first position iteration.  Contacts
+// of different nodes are independent (static shapes), so each node runs its
+// own sweep in list order.
+__global__ void k_sb_contact_solve(SoftDev d, float h)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const uint32_t n = d.n, nn = (uint32_t)kMaxSpheres * n;  // slot planes laid out for the hull capacity
+    f3 vel = ldv(d.xsol, i);
+    int order[kMaxSpheres];
+    const int k = sb_contact_order(d, i, order);
+    const float mA = d.type[i] == 0 ? 0.0f : 1.0f / d.mass[i];
+    if (k > 0) {
+        atomicAdd(d.active_count, (uint32_t)k);
+        for (int a = 0; a < k; ++a) {  // WarmStart
+            const uint32_t q = order[a] * n + i;
+            const f3 P = d.c_imp[q] * ld3(d.c_normal, nn, q);
+            vel = vel - mA * P;
+            const f3 P1 = d.c_imp[nn + q] * ld3(d.c_t1, nn, q), P2 = d.c_imp[2 * nn + q] * ld3(d.c_t2, nn, q);
+            vel = vel - mA * (P1 + P2);
+        }
+        for (uint32_t it = 0; it < d.vel_iters; ++it)
+            for (int a = 0; a < k; ++a) {
+                const uint32_t q = order[a] * n + i;
+                const float K = mA + 0.0f + 0.0f + 0.0f;
+                const float nmass = K > 0.0f ? 1.0f / K : 0.0f;
+                const float k11 = mA + 0.0f + 0.0f + 0.0f, k12 = 0.0f + 0.0f, k22 = mA + 0.0f + 0.0f + 0.0f;
+                float det = k11 * k22 - k12 * k12;
+                if (det != 0.0f) det = 1.0f / det;
+                const float tm_xx = det * k22, tm_yx = -det * k12, tm_xy = -det * k12, tm_yy = det * k11;
+                const float fr = sqrtf(d.friction[i] * d.hull[order[a]].friction);
+                const f3 nrm = ld3(d.c_normal, nn, q), t1 = ld3(d.c_t1, nn, q), t2 = ld3(d.c_t2, nn, q);
+                float ni = d.c_imp[q], tix = d.c_imp[nn + q], tiy = d.c_imp[2 * nn + q];
+                {
+                    const f3 dvv = zero3() - vel;
+                    const float Cdot = dot(nrm, dvv);
+                    float impulse = nmass * (-Cdot + 0.0f);
+                    const float old = ni;
+                    const float sum = old + impulse;
+                    ni = sum > 0.0f ? sum : 0.0f;
+                    impulse = ni - old;
+                    vel = vel - mA * (impulse * nrm);
+                }
+                {
+                    const f3 dvv = zero3() - vel;
+                    const float cx = dot(dvv, t1), cy = dot(dvv, t2);
+                    const float ncx = -cx, ncy = -cy;
+                    const float ix = ncx * tm_xx + ncy * tm_yx;
+                    const float iy = ncx * tm_xy + ncy * tm_yy;
+                    const float ox = tix, oy = tiy;
+                    tix += ix;
+                    tiy += iy;
+                    const float maxImpulse = fr * ni;
+                    if (tix * tix + tiy * tiy > maxImpulse * maxImpulse) {
+                        const float sl = sqrtf(tix * tix + tiy * tiy);
+                        if (sl > 1.1920929e-7f) {
+                            tix /= sl;
+                            tiy /= sl;
+                        }
+                        tix *= maxImpulse;
+                        tiy *= maxImpulse;
+                    }
+                    const float jx = tix - ox, jy = tiy - oy;
+                    vel = vel - mA * (jx * t1 + jy * t2);
+                }
+                d.c_imp[q] = ni;
+                d.c_imp[nn + q] = tix;
+                d.c_imp[2 * nn + q] = tiy;
+            }
+    }
+    f3 pos = ldv(d.x, i) + h * vel;
+    if (k > 0 && d.pos_iters > 0) {
+        const float ms = sb_position_iteration(d, i, pos, order, k, mA);
+        if (ms < 0.0f) atomicMin(&d.min_sep[0], sb_enc(ms));
+    }
+    stv(d.v, i, vel);
+    stv(d.x, i, pos);
+}
+
+// Position iteration `it` >= 1, run while the previous one left a
+// separation below -3 slops (softbody_solver.cpp:114-126).
+__global__ void k_sb_contact_position(SoftDev d, uint32_t it)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n || sb_dec(d.min_sep[it - 1]) >= -3.0f * 0.005f) return;
+    int order[kMaxSpheres];
+    const int k = sb_contact_order(d, i, order);
+    if (k == 0) return;
+    const float mA = d.type[i] == 0 ? 0.0f : 1.0f / d.mass[i];
+    f3 pos = ldv(d.x, i);
+    const float ms = sb_position_iteration(d, i, pos, order, k, mA);
+    stv(d.x, i, pos);
+    if (ms < 0.0f) atomicMin(&d.min_sep[it], sb_enc(ms));
+}
+
+// Forces cleared, node proxies moved, new contacts (softbody.cpp:757-778,
+// FindNewBodyContacts and AddNSPair, softbody_contact_manager.cpp:44-107)
+__global__ void k_sb_post(SoftDev d, float h)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const uint32_t n = d.n, nn = (uint32_t)kMaxSpheres * n;  // slot planes laid out for the hull capacity
+    stv(d.f, i, zero3());
+    if (d.type[i] != 0) node_move_proxy(d, i, h * ldv(d.v, i));
+    if (d.type[i] != 2) return;
+    for (uint32_t s = 0; s < d.nhull; ++s) {
+        const uint32_t q = s * n + i;
+        if (d.c_exists[q] || !node_overlap(d, i, d.hull[s])) continue;
+        d.c_exists[q] = 1;
+        d.c_active[q] = 0;
+        d.c_key[q] = d.step_index * kMaxSpheres + s;
+        d.c_imp[q] = 0.0f;
+        d.c_imp[nn + q] = 0.0f;
+        d.c_imp[2 * nn + q] = 0.0f;
+    }
+}
+
+__global__ void k_sb_init_proxies(SoftDev d)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const f3 x = ldv(d.x, i);
+    // aabb.Set(position, 0) fattened by B3_AABB_EXTENSION (softbody.cpp:477-480)
+    d.fat_lo[3 * i] = (x.x - 0.0f) - 0.2f;
+    d.fat_lo[3 * i + 1] = (x.y - 0.0f) - 0.2f;
+    d.fat_lo[3 * i + 2] = (x.z - 0.0f) - 0.2f;
+    d.fat_hi[3 * i] = (x.x + 0.0f) + 0.2f;
+    d.fat_hi[3 * i + 1] = (x.y + 0.0f) + 0.2f;
+    d.fat_hi[3 * i + 2] = (x.z + 0.0f) + 0.2f;
+    d.radius[i] = 0.0f;
+    d.friction[i] = 0.0f;
 }
 
 // Edits of one node, in stream order with the steps: 0 type, 1 mass damping,
@@ -354,7 +617,19 @@ __global__ void k_sb_node_op(SoftDev d, uint32_t i, int op, float a, float b, fl
         if (d.type[i] == t) return;
         d.type[i] = t;
         stv(d.f, i, zero3());
-        if (t == 0) stv(d.v, i, zero3());
+        if (t == 0) {
+            stv(d.v, i, zero3());
+            node_move_proxy(d, i, zero3());
+        }
+        for (uint32_t s = 0; s < d.nhull; ++s) {  // DestroyContacts
+            d.c_exists[s * d.n + i] = 0;
+            d.c_active[s * d.n + i] = 0;
+        }
+    } else if (op == 5) {  // SetRadius
+        d.radius[i] = a;
+        node_move_proxy(d, i, zero3());
+    } else if (op == 6) {  // SetFriction
+        d.friction[i] = a;
     } else if (op == 1) {
         d.damping[i] = a;
     } else if (op == 2) {
@@ -362,7 +637,10 @@ __global__ void k_sb_node_op(SoftDev d, uint32_t i, int op, float a, float b, fl
     } else if (op == 3) {
         if (d.type[i] != 0) stv(d.v, i, mk(a, b, c));
     } else {
-        stv(d.x, i, mk(a, b, c));
+        const f3 p = mk(a, b, c);
+        const f3 disp = p - ldv(d.x, i);
+        stv(d.x, i, p);
+        node_move_proxy(d, i, disp);
     }
 }
 
@@ -387,6 +665,9 @@ struct b3g_softbody {
     std::vector<float> mass;
     b3g_step_stats last{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void* cbuf = nullptr;                 // node radius, friction, proxies, position-iteration words
+    void* slots = nullptr;                // contact slots for kMaxSpheres hulls
+    std::vector<void*> hull_bufs;         // device copies of the hulls' vertices and planes
 };
 
 namespace {
@@ -561,6 +842,30 @@ b3g_status b3g_softbody_create(uint32_t vertex_count, const float* vertices, uin
     b->cols = P.cols;
     b->diag = P.diag;
     b->mass = P.mass;
+    // node proxies from creation on, with radius and friction 0
+    // (softbody.cpp:462-481)
+    {
+        const size_t words = 8 * (size_t)n + kMaxPosIters + 4;
+        cudaError_t ce = cudaMalloc(&b->cbuf, words * sizeof(float));
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            b3g_softbody_destroy(b);
+            return ce == cudaErrorMemoryAllocation ? B3G_ERR_OUT_OF_MEMORY : B3G_ERR_CUDA;
+        }
+        float* f = static_cast<float*>(b->cbuf);
+        d.radius = f;
+        d.friction = f + n;
+        d.fat_lo = f + 2 * (size_t)n;
+        d.fat_hi = f + 5 * (size_t)n;
+        d.min_sep = reinterpret_cast<int*>(f + 8 * (size_t)n);
+        d.active_count = reinterpret_cast<uint32_t*>(f + 8 * (size_t)n + kMaxPosIters);
+        k_sb_init_proxies<<<blocks_for(n), kBlock, 0, b->stream>>>(d);
+        count_launches(1);
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(b->stream) != cudaSuccess) {
+            b3g_softbody_destroy(b);
+            return B3G_ERR_CUDA;
+        }
+    }
     *out = b;
     return B3G_OK;
 }
@@ -573,6 +878,9 @@ b3g_status b3g_softbody_destroy(b3g_softbody* b)
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->arena) cudaFree(b->arena);
+    if (b->cbuf) cudaFree(b->cbuf);
+    if (b->slots) cudaFree(b->slots);
+    for (void* p : b->hull_bufs) cudaFree(p);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return B3G_OK;
@@ -632,12 +940,19 @@ b3g_status b3g_softbody_set_solver(b3g_softbody* b, const b3g_solver_opts* o)
 b3g_status b3g_softbody_step(b3g_softbody* b, float dt, uint32_t velocity_iterations, uint32_t position_iterations,
                              b3g_step_stats* stats)
 {
-    (void)velocity_iterations;
-    (void)position_iterations;  // no contacts without a world
     if (!ok(b) || !(dt >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(b->device);
     cudaStream_t s = b->stream;
     SoftDev& d = b->dev;
+    d.vel_iters = velocity_iterations;
+    d.pos_iters = position_iterations;
+    d.step_index += 1;
+    if (d.nhull) {
+        // UpdateBodyContacts (softbody.cpp:752)
+        SB_TRY(cudaMemsetAsync(d.min_sep, 0, (kMaxPosIters + 4) * sizeof(int), s));
+        k_sb_contacts_update<<<blocks_for(d.n), kBlock, 0, s>>>(d);
+        count_launches(1);
+    }
     std::memset(&b->last, 0, sizeof(b->last));
     SB_TRY(cudaEventRecord(b->ev0, s));
     StepScalars h;
@@ -649,10 +964,21 @@ b3g_status b3g_softbody_step(b3g_softbody* b, float dt, uint32_t velocity_iterat
         SB_TRY(cudaGetLastError());
         const b3g_status r = csr_run(b->cs, &b->opts, s, &h);
         if (r != B3G_OK) return r;
-        k_sb_integrate<<<blocks_for(d.n), kBlock, 0, s>>>(d, dt);
-        count_launches(1);
+        if (d.nhull) {
+            k_sb_contact_solve<<<blocks_for(d.n), kBlock, 0, s>>>(d, dt);
+            for (uint32_t it = 1; it < position_iterations && it < (uint32_t)kMaxPosIters; ++it)
+                k_sb_contact_position<<<blocks_for(d.n), kBlock, 0, s>>>(d, it);
+            k_sb_post<<<blocks_for(d.n), kBlock, 0, s>>>(d, dt);
+            const uint32_t extra = position_iterations > 1 ? std::min<uint32_t>(position_iterations, kMaxPosIters) - 1 : 0;
+            count_launches(2 + extra);
+        } else {
+            k_sb_integrate<<<blocks_for(d.n), kBlock, 0, s>>>(d, dt);
+            count_launches(1);
+        }
     } else {
-        SB_TRY(cudaMemsetAsync(d.f, 0, 3 * (size_t)d.n * sizeof(float), s));
+        // no solve: forces cleared, proxies moved by no displacement, new contacts
+        k_sb_post<<<blocks_for(d.n), kBlock, 0, s>>>(d, 0.0f);
+        count_launches(1);
     }
     SB_TRY(cudaGetLastError());
     SB_TRY(cudaEventRecord(b->ev1, s));
@@ -661,6 +987,11 @@ b3g_status b3g_softbody_step(b3g_softbody* b, float dt, uint32_t velocity_iterat
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     csr_report(h, nullptr, &b->last);
     b->last.step_ms = ms;
+    if (d.nhull) {
+        uint32_t active = 0;
+        SB_TRY(cudaMemcpy(&active, d.active_count, sizeof(active), cudaMemcpyDeviceToHost));
+        b->last.active_contacts = active;
+    }
     if (stats) *stats = b->last;
     return h.status ? (b3g_status)h.status : B3G_OK;
 }
@@ -669,6 +1000,109 @@ static b3g_status copy_nodes(b3g_softbody* b, float* dst, const float* src, size
 {
     SB_TRY(cudaMemcpyAsync(dst, src, bytes, kind, b->stream));
     SB_TRY(cudaStreamSynchronize(b->stream));
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_set_node_radius(b3g_softbody* b, uint32_t node, float radius)
+{
+    if (!(radius >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    return node_op(b, node, 5, radius, 0.0f, 0.0f);
+}
+
+b3g_status b3g_softbody_set_node_friction(b3g_softbody* b, uint32_t node, float friction)
+{
+    if (!(friction >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    return node_op(b, node, 6, friction, 0.0f, 0.0f);
+}
+
+b3g_status b3g_softbody_add_static_hull(b3g_softbody* b, const float* vertices, uint32_t vertex_count,
+                                        const float* planes, uint32_t face_count, float friction, uint32_t* shape_id)
+{
+    if (!ok(b) || !vertices || !planes || vertex_count == 0 || face_count == 0 || vertex_count > 4096 ||
+        face_count > 4096 || !(friction >= 0.0f))
+        return B3G_ERR_INVALID_ARGUMENT;
+    SoftDev& d = b->dev;
+    if (d.nhull >= (uint32_t)kMaxSpheres) return B3G_ERR_CAPACITY;
+    cudaSetDevice(b->device);
+    const uint32_t n = d.n;
+    if (!b->slots) {
+        // contact slots for every hull the body can take, zeroed
+        const size_t nn = (size_t)kMaxSpheres * n;
+        const size_t bytes = 2 * nn + 4 * nn + 15 * nn * sizeof(float);
+        SB_TRY(cudaMalloc(&b->slots, bytes));
+        SB_TRY(cudaMemsetAsync(b->slots, 0, bytes, b->stream));
+    }
+    const size_t nf = 3 * (size_t)vertex_count + 4 * (size_t)face_count;
+    std::vector<float> img(nf);
+    std::memcpy(img.data(), vertices, 3 * (size_t)vertex_count * sizeof(float));
+    std::memcpy(img.data() + 3 * (size_t)vertex_count, planes, 4 * (size_t)face_count * sizeof(float));
+    float* hd = nullptr;
+    SB_TRY(cudaMalloc(&hd, nf * sizeof(float)));
+    b->hull_bufs.push_back(hd);
+    SB_TRY(cudaMemcpyAsync(hd, img.data(), nf * sizeof(float), cudaMemcpyHostToDevice, b->stream));
+    SB_TRY(cudaStreamSynchronize(b->stream));
+    SphereDev& h = d.hull[d.nhull];
+    h = SphereDev{};
+    h.kind = 2;
+    h.radius = 0.0f;  // B3_HULL_RADIUS
+    h.friction = friction;
+    h.hull = hd;
+    h.nhv = vertex_count;
+    h.nhf = face_count;
+    // b3HullShape::ComputeAABB with the identity at the origin, fattened
+    float lo[3], hi[3];
+    for (uint32_t k = 0; k < vertex_count; ++k) {
+        const float* v = vertices + 3 * k;
+        const float w[3] = {((v[0] * 1.0f + v[1] * 0.0f) + v[2] * 0.0f) + 0.0f,
+                            ((v[0] * 0.0f + v[1] * 1.0f) + v[2] * 0.0f) + 0.0f,
+                            ((v[0] * 0.0f + v[1] * 0.0f) + v[2] * 1.0f) + 0.0f};
+        for (int q = 0; q < 3; ++q) {
+            lo[q] = k == 0 ? w[q] : (lo[q] < w[q] ? lo[q] : w[q]);
+            hi[q] = k == 0 ? w[q] : (hi[q] > w[q] ? hi[q] : w[q]);
+        }
+    }
+    for (int q = 0; q < 3; ++q) {
+        h.lo[q] = (lo[q] - h.radius) - 0.2f;
+        h.hi[q] = (hi[q] + h.radius) + 0.2f;
+    }
+    // slot planes for the new hull count: every array is laid out per
+    // (hull, node) with the body's hull capacity, so the layout is fixed
+    const size_t nn = (size_t)kMaxSpheres * n;
+    char* base = static_cast<char*>(b->slots);
+    d.c_exists = reinterpret_cast<uint8_t*>(base);
+    d.c_active = reinterpret_cast<uint8_t*>(base + nn);
+    d.c_key = reinterpret_cast<uint32_t*>(base + 2 * nn);
+    float* f = reinterpret_cast<float*>(base + 6 * nn);
+    d.c_normal = f;
+    d.c_t1 = f + 3 * nn;
+    d.c_t2 = f + 6 * nn;
+    d.c_point = f + 9 * nn;
+    d.c_imp = f + 12 * nn;
+    if (shape_id) *shape_id = d.nhull;
+    d.nhull += 1;
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_read_contacts(const b3g_softbody* cb, uint8_t* exists, uint8_t* active, float* impulses)
+{
+    b3g_softbody* b = const_cast<b3g_softbody*>(cb);
+    if (!ok(b)) return B3G_ERR_INVALID_ARGUMENT;
+    const SoftDev& d = b->dev;
+    const size_t m = (size_t)d.nhull * d.n;
+    if (!m) return B3G_OK;
+    cudaSetDevice(b->device);
+    SB_TRY(cudaStreamSynchronize(b->stream));
+    if (exists) SB_TRY(cudaMemcpy(exists, d.c_exists, m, cudaMemcpyDeviceToHost));
+    if (active) SB_TRY(cudaMemcpy(active, d.c_active, m, cudaMemcpyDeviceToHost));
+    if (impulses) {
+        // per slot: normal, tangent x, tangent y
+        std::vector<float> planes(3 * m);
+        const size_t nn = (size_t)kMaxSpheres * d.n;
+        for (int k = 0; k < 3; ++k)
+            SB_TRY(cudaMemcpy(planes.data() + k * m, d.c_imp + k * nn, m * sizeof(float), cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < m; ++q)
+            for (int k = 0; k < 3; ++k) impulses[3 * q + k] = planes[k * m + q];
+    }
     return B3G_OK;
 }
 

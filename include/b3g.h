@@ -487,6 +487,21 @@ b3g_status b3g_softbody_set_solver(b3g_softbody* body, const b3g_solver_opts* op
  * r.P^-1 r at the CG start, b_delta the soft body's delta_0 (Sb . diag(A) Sb). */
 b3g_status b3g_softbody_step(b3g_softbody* body, float dt, uint32_t velocity_iterations,
                              uint32_t position_iterations, b3g_step_stats* stats);
+/* b3SoftBody::SetWorld with static hulls (b3HullShape on a static body at the
+ * origin; vertices and face planes in world coordinates, as for cloths):
+ * node contacts follow b3NodeBodyContact::Update and b3SoftBodyContactSolver
+ * (src/bounce/softbody/softbody_contact_manager.cpp,
+ * src/bounce/softbody/contacts/softbody_contact_solver.cpp).  At most
+ * B3G_MAX_SPHERES hulls per body. */
+b3g_status b3g_softbody_add_static_hull(b3g_softbody* body, const float* vertices, uint32_t vertex_count,
+                                        const float* planes, uint32_t face_count, float friction, uint32_t* shape_id);
+/* b3SoftBodyNode::SetRadius / SetFriction (softbody_node.h:218-235); both 0
+ * by default. */
+b3g_status b3g_softbody_set_node_radius(b3g_softbody* body, uint32_t node, float radius);
+b3g_status b3g_softbody_set_node_friction(b3g_softbody* body, uint32_t node, float friction);
+/* Node contacts per (hull, node): exists, active (hull_count * node_count
+ * bytes each), impulses (normal, tangent x, tangent y). */
+b3g_status b3g_softbody_read_contacts(const b3g_softbody* body, uint8_t* exists, uint8_t* active, float* impulses);
 b3g_status b3g_softbody_read_state(const b3g_softbody* body, float* positions, float* velocities);
 b3g_status b3g_softbody_write_state(b3g_softbody* body, const float* positions, const float* velocities);
 /* Element state: the rotation q (x, y, z, w per element) that the next

@@ -128,3 +128,68 @@ def test_softbody_rejects_degenerate_mesh(b3g):
     t = np.array([[0, 1, 2, 3]], np.uint32)
     with pytest.raises(b3g.B3gError):
         b3g.SoftBody(v, t, b3g.SoftBodyDef())
+
+
+def _hull_pair(b3g, port):
+    from test_softbody_oracle import softbody_hull_golden
+
+    d, scene = softbody_hull_golden()
+    s = scene.sdef
+    bodies = (b3g.SoftBody(scene.vertices, scene.tets, s).setup(scene),
+              port.PortSoftBody(scene.vertices, scene.tets, s.density, s.E, s.nu, s.c_yield, s.c_creep,
+                                s.c_max).setup(scene))
+    for b in bodies:
+        b.add_hull(d["hull_vertices"], d["hull_planes"], float(d["hull_friction"]))
+        for i in range(len(scene.vertices)):
+            b.set_node_radius(i, float(d["node_radius"]))
+            b.set_node_friction(i, float(d["node_friction"]))
+    return d, scene, bodies[0], bodies[1]
+
+
+def test_softbody_hull_contacts_per_step(b3g, port):
+    """Node contacts with a static hull (softbody_contact_manager.cpp,
+    softbody_contact_solver.cpp): each step starts the oracle from the GPU's
+    positions, velocities and element state; x within 1e-4 relative, the
+    contact sets within 2 nodes.  Once the block rests its velocities are
+    near zero, so v is held to 1e-4 of the larger of its own size and the
+    velocity one step of gravity adds."""
+    d, scene, gpu, ora = _hull_pair(b3g, port)
+    vscale = float(np.linalg.norm(scene.gravity)) * scene.dt
+    seen, worst = 0, 0.0
+    for step in range(150):
+        _sync(gpu, ora)
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        gc, oc = gpu.contacts(), ora.contacts()
+        seen = max(seen, int(oc["active"].sum()))
+        assert abs(g["iterations"] - o["iterations"]) <= 1, step
+        assert int(np.sum(gc["exists"] != oc["exists"])) <= 2, step
+        assert int(np.sum(gc["active"] != oc["active"])) <= 2, step
+        gs, os_ = gpu.state(), ora.state()
+        assert rel_err(gs["x"], os_["x"]) <= 1e-4, step
+        ev = float(np.abs(gs["v"] - os_["v"]).max()) / max(float(np.abs(os_["v"]).max()), vscale)
+        worst = max(worst, ev)
+        assert ev <= 1e-4, step
+    print("softbody hull per step: worst v error", worst, "of scale; most active", seen)
+    assert seen > 10  # the block came to rest on the hull
+
+
+def test_softbody_hull_against_reference_golden(b3g, port):
+    """Free run from the reference's start: after one step the same contacts
+    and x within 1e-4 m; at steps 25, 75 and 150 the block rests on the hull
+    with x within 5e-4 m and the active contacts within 2."""
+    d, scene, gpu, _ = _hull_pair(b3g, port)
+    for k in range(1, len(d["iterations"]) + 1):
+        gpu.step(scene.dt)
+        if f"x_{k}" in d:
+            x, c = gpu.state()["x"], gpu.contacts()
+            dx = float(np.abs(x - d[f"x_{k}"]).max())
+            ga, ra = int(c["active"].sum()), int(d[f"contact_active_{k}"].sum())
+            print("softbody hull golden: step", k, "max |dx|", dx, "active", ga, ra)
+            if k == 1:
+                assert dx <= 1e-4
+                assert np.array_equal(c["exists"], d["contact_exists_1"])
+                assert np.array_equal(c["active"], d["contact_active_1"])
+            else:
+                assert dx <= 5e-4, k
+                assert abs(ga - ra) <= 2, k
