@@ -256,97 +256,90 @@ __global__ void k_sb_elements(SoftDev d, float h, float inv_h)
 constexpr int kAsmWarps = 4;
 constexpr uint32_t kMaxRowSlots = 128;  // slot ids are 7 bits wide
 
-__global__ void __launch_bounds__(32 * kAsmWarps) k_sb_assemble(SoftDev d, float h)
+__global__ void __launch_bounds__(32 * kAsmWarps, 8) k_sb_assemble(SoftDev d, float h)
 {
     __shared__ float sX[kAsmWarps][32 * 4 * 9];   // element blocks of one chunk
     __shared__ uint8_t sSlot[kAsmWarps][32 * 4];
     __shared__ float sF[kAsmWarps][32 * 6];       // f0 and f_plastic terms of one chunk
-    __shared__ float sXc[kAsmWarps][kMaxRowSlots * 3];  // K_k x_col per slot
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     const uint32_t i = blockIdx.x * kAsmWarps + w;
     if (i >= d.n) return;  // whole warps leave together
     float* X = sX[w];
     uint8_t* SL = sSlot[w];
     float* F = sF[w];
-    float* XC = sXc[w];
     const uint32_t r0 = d.rowptr[i], deg = d.rowptr[i + 1] - r0;
-    m3 acc[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) acc[k] = mzero();
-    f3 f0 = zero3(), fp = zero3();
-    const uint32_t q0 = d.inc_ptr[i], q1 = d.inc_ptr[i + 1];
-    for (uint32_t qb = q0; qb < q1; qb += 32u) {
-        const uint32_t cnt = min(32u, q1 - qb);
-        if (lane < cnt) {
-            const uint32_t e = d.inc_elem[qb + lane], meta = d.inc_meta[qb + lane];
-            const uint32_t li = meta & 3u;
-            const m3 R = ldm(d.R + 9 * (size_t)e);
-            const m3 RT = transpose(R);
-            const float* Ke = d.Ke + 144 * (size_t)e;
-#pragma unroll
-            for (uint32_t j = 0; j < 4; ++j) {
-                SL[4 * lane + j] = (uint8_t)((meta >> (4 + 7 * j)) & 127u);
-                stm(X + 9 * (4 * lane + j), mmul(mmul(R, ldm(Ke + 9 * (li + 4 * j))), RT));
-            }
-            const f3 a = ldv(d.f0s + 12 * (size_t)e, li), b = ldv(d.fps + 12 * (size_t)e, li);
-            F[6 * lane] = a.x; F[6 * lane + 1] = a.y; F[6 * lane + 2] = a.z;
-            F[6 * lane + 3] = b.x; F[6 * lane + 4] = b.y; F[6 * lane + 5] = b.z;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const uint32_t slot = lane + 32u * k;
-            if (slot >= deg) break;
-            for (uint32_t q = 0; q < cnt; ++q)
-#pragma unroll
-                for (uint32_t j = 0; j < 4; ++j)
-                    if (SL[4 * q + j] == slot) acc[k] = acc[k] + ldm(X + 9 * (4 * q + j));
-        }
-        if (lane == 0)
-            for (uint32_t q = 0; q < cnt; ++q) {
-                f0 = f0 + mk(F[6 * q], F[6 * q + 1], F[6 * q + 2]);
-                fp = fp + mk(F[6 * q + 3], F[6 * q + 4], F[6 * q + 5]);
-            }
-        __syncwarp();
-    }
-    // each slot's K_k x_col; lane 0 sums them in the row list's order below
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t slot = lane + 32u * k;
-        if (slot < deg) {
-            const f3 kx = acc[k] * ldv(d.x, d.cols[r0 + slot]);
-            XC[3 * slot] = kx.x; XC[3 * slot + 1] = kx.y; XC[3 * slot + 2] = kx.z;
-        }
-    }
-    __syncwarp();
-    const bool dyn = d.type[i] == 2;
     const float m = d.mass[i];
     const m3 M = diag3(m);
-    if (lane == 0) {
-        const f3 f0n = mk(-f0.x, -f0.y, -f0.z);
-        // K p in the row list's order (newest first touch first)
-        f3 kp = zero3();
-        for (uint32_t k = deg; k-- > 0;) kp = kp + mk(XC[3 * k], XC[3 * k + 1], XC[3 * k + 2]);
-        f3 fe = ldv(d.f, i);
-        if (dyn) fe = fe + m * mk(d.gx, d.gy, d.gz);
-        const f3 mv = zero3() + M * ldv(d.v, i);
-        stv(d.b, i, mv - h * ((kp + f0n) - (fp + fe)));
-        d.S[i] = dyn ? 1.0f : 0.0f;
-    }
     // A = (M + h C) + (h h) K on the diagonal, 0 + (h h) K elsewhere
     const float hh = h * h;
     const float cd = d.damping[i] * m;
     const uint32_t dg = d.diag[i] - r0;
     float* vals = d.vals + 9 * (size_t)r0;
+    f3 f0 = zero3(), fp = zero3(), kp = zero3();
+    const uint32_t q0 = d.inc_ptr[i], q1 = d.inc_ptr[i + 1];
+    // Each lane owns one slot of a group of 32; a row wider than 32 slots
+    // (rare) takes the incidences again for each further group, so one
+    // accumulator suffices and the kernel keeps to 64 registers.  Groups run
+    // from the last down, so lane 0 can add K p in the row list's order
+    // (newest first touch first: slot deg-1 down to 0) as they finish.
+    for (uint32_t g = (deg + 31u) / 32u; g-- > 0;) {
+        const uint32_t slot = lane + 32u * g;
+        m3 acc = mzero();
+        for (uint32_t qb = q0; qb < q1; qb += 32u) {
+            const uint32_t cnt = min(32u, q1 - qb);
+            if (lane < cnt) {
+                const uint32_t e = d.inc_elem[qb + lane], meta = d.inc_meta[qb + lane];
+                const uint32_t li = meta & 3u;
+                const m3 R = ldm(d.R + 9 * (size_t)e);
+                const m3 RT = transpose(R);
+                const float* Ke = d.Ke + 144 * (size_t)e;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t slot = lane + 32u * k;
+                for (uint32_t j = 0; j < 4; ++j) {
+                    SL[4 * lane + j] = (uint8_t)((meta >> (4 + 7 * j)) & 127u);
+                    stm(X + 9 * (4 * lane + j), mmul(mmul(R, ldm(Ke + 9 * (li + 4 * j))), RT));
+                }
+                if (g == 0) {
+                    const f3 a = ldv(d.f0s + 12 * (size_t)e, li), b = ldv(d.fps + 12 * (size_t)e, li);
+                    F[6 * lane] = a.x; F[6 * lane + 1] = a.y; F[6 * lane + 2] = a.z;
+                    F[6 * lane + 3] = b.x; F[6 * lane + 4] = b.y; F[6 * lane + 5] = b.z;
+                }
+            }
+            __syncwarp();
+            // every block that lands on this slot, in incidence (= element) order
+            if (slot < deg)
+                for (uint32_t q = 0; q < cnt; ++q)
+#pragma unroll
+                    for (uint32_t j = 0; j < 4; ++j)
+                        if (SL[4 * q + j] == slot) acc = acc + ldm(X + 9 * (4 * q + j));
+            if (g == 0 && lane == 0)
+                for (uint32_t q = 0; q < cnt; ++q) {
+                    f0 = f0 + mk(F[6 * q], F[6 * q + 1], F[6 * q + 2]);
+                    fp = fp + mk(F[6 * q + 3], F[6 * q + 4], F[6 * q + 5]);
+                }
+            __syncwarp();
+        }
+        f3 kx = zero3();
+        if (slot < deg) kx = acc * ldv(d.x, d.cols[r0 + slot]);  // this slot's K_k x_col
+        for (uint32_t l = min(31u, deg - 1u - 32u * g) + 1u; l-- > 0;) {
+            const f3 t = mk(__shfl_sync(0xffffffffu, kx.x, l), __shfl_sync(0xffffffffu, kx.y, l),
+                            __shfl_sync(0xffffffffu, kx.z, l));
+            if (lane == 0) kp = kp + t;
+        }
         if (slot < deg) {
             m3 a;
-            if (slot == dg) a = (M + h * diag3(cd)) + hh * acc[k];
-            else a = mzero() + hh * acc[k];
+            if (slot == dg) a = (M + h * diag3(cd)) + hh * acc;
+            else a = mzero() + hh * acc;
             stm(vals + 9 * slot, a);
         }
+    }
+    if (lane == 0) {
+        const bool dyn = d.type[i] == 2;
+        const f3 f0n = mk(-f0.x, -f0.y, -f0.z);
+        f3 fe = ldv(d.f, i);
+        if (dyn) fe = fe + m * mk(d.gx, d.gy, d.gz);
+        const f3 mv = zero3() + M * ldv(d.v, i);
+        stv(d.b, i, mv - h * ((kp + f0n) - (fp + fe)));
+        d.S[i] = dyn ? 1.0f : 0.0f;
     }
 }
 
