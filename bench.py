@@ -380,6 +380,59 @@ def run_softbody(args, dev: int, cpu_sample: bool):
         ora.close()
         out["cpu_baseline"] = {"value": n * 2 / sec, "unit": "node-steps/s", "cores": 1, "kind": "port",
                                "sample": f"the oracle's soft body step, 2 steps of the same block, {sec / 2:.2f} s/step"}
+    out["hull"] = run_softbody_hull(args, dev, cpu_sample)
+    return out
+
+
+def run_softbody_hull(args, dev: int, cpu_sample: bool):
+    """The same block, free, resting on a static ground hull (a 6 x 0.5 x 6 m
+    box whose top is 0.06 m below the block; node radius 0.05, friction 0.2,
+    hull friction 0.6): node contacts (GJK TestSphere, velocity and position
+    iterations) inside the step.  12 steps to land, then 10 timed with CUDA
+    events.  The CPU figure is the oracle on the same scene, 2 steps after
+    the same 12."""
+    import dataclasses
+
+    import bounce_b200 as b3g
+
+    side = args.softbody_side
+    scene = dataclasses.replace(b3g.pinned_block_scene(side, side, side, spacing=1.0 / side),
+                                static_nodes=np.zeros(0, np.uint32))
+    hv, hp = box_hull(3.0, 0.25, 3.0, -0.81)
+    land, timed = 12, 10
+
+    def dress(b):
+        b.add_hull(hv, hp, 0.6)
+        for i in range(len(scene.vertices)):
+            b.set_node_radius(i, 0.05)
+            b.set_node_friction(i, 0.2)
+        return b
+
+    body = dress(b3g.SoftBody(scene.vertices, scene.tets, scene.sdef, device=dev).setup(scene))
+    for _ in range(land):
+        body.step(scene.dt)
+    ms = [body.step(scene.dt)["step_ms"] for _ in range(timed)]
+    active = int(body.contacts()["active"].sum())
+    body.close()
+    n = len(scene.vertices)
+    out = {"workload": f"block{side}x{side}x{side}_on_hull", "nodes": n, "steps": f"{land}-{land + timed - 1}",
+           "ms_per_step": sum(ms) / len(ms), "node_steps_per_s": n * len(ms) / (sum(ms) / 1e3),
+           "active_contacts": active}
+    if cpu_sample:
+        import oracle
+
+        s = scene.sdef
+        ora = dress(oracle.PortSoftBody(scene.vertices, scene.tets, s.density, s.E, s.nu, s.c_yield, s.c_creep,
+                                        s.c_max).setup(scene))
+        for _ in range(land):
+            ora.step(scene.dt)
+        t0 = time.perf_counter()
+        for _ in range(2):
+            ora.step(scene.dt)
+        sec = time.perf_counter() - t0
+        ora.close()
+        out["cpu_baseline"] = {"value": n * 2 / sec, "unit": "node-steps/s", "cores": 1, "kind": "port",
+                               "sample": f"the oracle on the same scene, steps {land}-{land + 1}, {sec / 2:.2f} s/step"}
     return out
 
 
