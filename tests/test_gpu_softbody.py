@@ -193,3 +193,73 @@ def test_softbody_hull_against_reference_golden(b3g, port):
             else:
                 assert dx <= 5e-4, k
                 assert abs(ga - ra) <= 2, k
+
+
+def _box(c, h):
+    """A box hull (vertices, face planes) with centre c and half extents h."""
+    c, h = np.asarray(c, np.float32), np.asarray(h, np.float32)
+    v = np.array([c + h * (2 * np.array(s, np.float32) - 1) for s in np.ndindex(2, 2, 2)], np.float32)
+    planes = []
+    for k in range(3):
+        n = np.zeros(3, np.float32)
+        n[k] = 1.0
+        planes.append((*n, c[k] + h[k]))
+        planes.append((*(-n), -(c[k] - h[k])))
+    return v, np.array(planes, np.float32)
+
+
+def test_softbody_two_hulls_per_step(b3g, port):
+    """A free block falling onto a ground hull beside a wall hull that its
+    side already touches: contacts with both hulls, per step from the GPU's
+    state as above; the oracle's contact count equals the GPU's."""
+    import dataclasses
+
+    scene = dataclasses.replace(b3g.pinned_block_scene(6, 6, 6, spacing=1.0 / 6),
+                                static_nodes=np.zeros(0, np.uint32))
+    s = scene.sdef
+    gpu = b3g.SoftBody(scene.vertices, scene.tets, s).setup(scene)
+    ora = port.PortSoftBody(scene.vertices, scene.tets, s.density, s.E, s.nu, s.c_yield, s.c_creep,
+                            s.c_max).setup(scene)
+    hulls = [_box((0.0, -0.81, 0.0), (3.0, 0.25, 3.0)), _box((0.78, 0.0, 0.0), (0.25, 2.0, 2.0))]
+    for b in (gpu, ora):
+        for hv, hp in hulls:
+            b.add_hull(hv, hp, 0.6)
+        for i in range(len(scene.vertices)):
+            b.set_node_radius(i, 0.05)
+            b.set_node_friction(i, 0.2)
+    vscale = float(np.linalg.norm(scene.gravity)) * scene.dt
+    per_hull = np.zeros(2, int)
+    for step in range(40):
+        _sync(gpu, ora)
+        gpu.step(scene.dt)
+        ora.step(scene.dt)
+        gc, oc = gpu.contacts(), ora.contacts()
+        assert abs(int(gc["exists"].sum()) - oc["count"]) <= 2, step
+        per_hull = np.maximum(per_hull, gc["active"].reshape(2, -1).sum(axis=1))
+        gs, os_ = gpu.state(), ora.state()
+        assert rel_err(gs["x"], os_["x"]) <= 1e-4, step
+        assert float(np.abs(gs["v"] - os_["v"]).max()) <= 1e-4 * max(float(np.abs(os_["v"]).max()), vscale), step
+    assert per_hull.min() > 0, per_hull  # both hulls pushed nodes
+
+
+def test_softbody_hull_arguments(b3g):
+    """Argument and capacity errors of the hull and node-property calls."""
+    scene = b3g.pinned_block_scene(3, 3, 3, spacing=0.5)
+    body = b3g.SoftBody(scene.vertices, scene.tets, scene.sdef).setup(scene)
+    assert body.contacts()["exists"].size == 0  # no hull, no contact slots
+    body.step(scene.dt)
+    n = len(scene.vertices)
+    for call in (lambda: body.set_node_radius(n, 0.1), lambda: body.set_node_radius(0, -1.0),
+                 lambda: body.set_node_friction(0, float("nan")),
+                 lambda: body.add_hull(np.zeros((0, 3)), np.zeros((0, 4)), 0.5)):
+        with pytest.raises(b3g.B3gError) as e:
+            call()
+        assert e.value.status == 1
+    hv, hp = _box((0.0, -3.0, 0.0), (1.0, 0.5, 1.0))
+    for _ in range(4):
+        body.add_hull(hv, hp, 0.5)
+    with pytest.raises(b3g.B3gError) as e:
+        body.add_hull(hv, hp, 0.5)
+    assert e.value.status == 8
+    body.step(scene.dt)
+    assert body.contacts()["exists"].size == 4 * n
