@@ -5,7 +5,7 @@ state; the curve is max |x_gpu - x_oracle| (metres) after every step.  Beside
 it, the floor: the oracle against itself with FP64 instead of FP32 CG dots
 (the same algorithm rounded differently).  Where the motion is chaotic (a
 cloth folding, a particle on the contact boundary) two correct solvers part
-ways, and the GPU curve is compared with that floor, not against zero.
+ways, and the GPU curve is compared with that floor, not with zero.
 Bulk quantities are reported too: the difference of the mean height and the
 relative difference of the energy (b3Cloth::GetEnergy, cloth.cpp:366-374).
 
