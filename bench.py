@@ -42,6 +42,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--side", type=int, default=256)
+    ap.add_argument("--cg", choices=["fused", "persistent"], default="fused",
+                    help="the headline cloth's CG: one persistent launch with one grid reduction per "
+                         "iteration (fused) or two")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--batch-count", type=int, default=512)
@@ -149,11 +152,14 @@ def algorithmic_bytes(info: dict, kernel: str) -> float:
     if kernel == "cg_init":
         return 40.0 * blocks + (12 * 3 + 1 + 3 * 12) * n
     if kernel.startswith("grid_cg"):
-        # the whole persistent solve: init, then per iteration phase A (A once;
-        # own z, p_old read, p and s written, filter byte) and phase B (x, p, r,
-        # s, P^-1 read; x, r, z written; filter byte)
+        # the whole persistent solve: the start (A x0: A once, m_x, b, P^-1
+        # read, r and z written, filter byte), then per iteration the MPCG's
+        # minimum, whatever the form: A values and columns once (40 B per
+        # block), the row pointer (4 B per row), the direction read and the
+        # product written (24 B per row), one fused vector pass reading p, s,
+        # x, r, P^-1 and the filter and writing x, r, p (100 B per row)
         iters = float(kernel.split(":")[1])
-        return 40.0 * blocks + 73.0 * n + iters * (40.0 * blocks + (49 + 97) * n)
+        return 40.0 * blocks + 73.0 * n + iters * (40.0 * blocks + 128.0 * n)
     if kernel == "assemble":
         inc = 3 * t + 2 * s
         return 36.0 * blocks + (24 + 24 + 4 + 1 + 24) * n + 40.0 * t + 24.0 * s + 8.0 * inc
@@ -169,7 +175,8 @@ def run_ours(args, rank, world):
     scene = b3g.sphere_scene(args.side, seed=2 + rank)
     opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
     cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene, opts)
-    cloth.set_cg_strategy(True)  # whole solve in one persistent cooperative launch
+    # the whole solve in one persistent cooperative launch
+    cloth.set_cg_strategy(True, fused=args.cg == "fused")
     info = cloth.info()
     n = info["vertices"]
     # L2 flush buffer (> 126 MB L2), written between timed steps
@@ -735,7 +742,9 @@ def main():
         "config": {"workload": f"grid{args.side}x{args.side}_bending_sphere", "vertices": n,
                    "triangles": r["info"]["triangles"], "springs": r["info"]["springs"],
                    "blocks": r["info"]["blocks"], "cg": "relative residual 1e-4, max 200, fp64 dots",
-                   "cg_strategy": "persistent cooperative launch",
+                   "cg_strategy": ("persistent cooperative launch, one grid reduction per iteration"
+                                   if args.cg == "fused" else "persistent cooperative launch, two grid "
+                                                              "reductions per iteration"),
                    "contact_iterations": [8, 2], "parallelism": f"replicas{world}",
                    "l2": "flushed (256 MB write) before every timed step",
                    "cg_iterations_mean": r["iterations_mean"], "active_contacts_mean": r["active_contacts_mean"]},

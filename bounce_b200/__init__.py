@@ -168,6 +168,7 @@ def lib() -> C.CDLL:
             "b3g_cloth_read_masses": [vp, vp],
             "b3g_cloth_get_energy": [vp, C.POINTER(f32)],
             "b3g_cloth_read_contacts": [vp, vp, vp, vp],
+            "b3g_cloth_read_proxies": [vp, vp, vp],
             "b3g_cloth_read_tri_contacts": [vp, C.POINTER(u32), vp, vp, vp, vp],
             "b3g_cloth_ray_cast_single": [vp, vp, vp, C.POINTER(u32), C.POINTER(f32), vp, C.POINTER(i32)],
             "b3g_cloth_ray_cast": [vp, vp, vp, f32, u32, C.POINTER(f32), vp, C.POINTER(i32)],
@@ -498,6 +499,13 @@ class Cloth:
         check(lib().b3g_cloth_read_contacts(self.h, _ptr(ex), _ptr(ac), _ptr(imp)), "read_contacts")
         return {"exists": ex[: self.nsph * self.n], "active": ac[: self.nsph * self.n],
                 "impulses": imp[: self.nsph * self.n]}
+
+    def proxies(self):
+        """The particles' fat AABBs: (lo, hi), n x 3 each."""
+        lo = np.zeros((self.n, 3), np.float32)
+        hi = np.zeros((self.n, 3), np.float32)
+        check(lib().b3g_cloth_read_proxies(self.h, _ptr(lo), _ptr(hi)), "read_proxies")
+        return lo, hi
 
     def ray_cast_single(self, p1, p2):
         """b3Cloth::RayCastSingle: (triangle, fraction, normal) of the first

@@ -292,7 +292,7 @@ b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t coun
 {
     b3g_status s = check_list(b, cloths, count);
     if (s != B3G_OK) return s;
-    if (!(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    if (!(dt > 0.0f) || pos_iters > (uint32_t)kMaxPosIters) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(b->device);
     cudaStream_t st = b->stream;
     // queued particle edits go first, on the batch's stream; earlier work on

@@ -101,6 +101,32 @@ void destroy_graph(b3g_cloth* c)
     c->exec = nullptr;
 }
 
+bool persistent_cg(const b3g_cloth* c) { return c->cg_strategy != B3G_CG_LAUNCHES; }
+
+// The fused CG's record buffer, sized for the cloth's current vertex count
+// (a new layout changes it; a captured graph holding the old one is dropped).
+b3g_status ensure_cg_rec(b3g_cloth* c)
+{
+    if (c->cg_strategy != B3G_CG_PERSISTENT_FUSED || (c->cg_rec && c->cg_rec_n == c->dev.n)) return B3G_OK;
+    destroy_graph(c);
+    if (c->cg_rec) cudaFree(c->cg_rec);
+    c->cg_rec = nullptr;
+    c->cg_rec_n = 0;
+    B3G_TRY(cudaMalloc(&c->cg_rec, grid_cg_fused_rec_bytes(c->dev.n)));
+    c->cg_rec_n = c->dev.n;
+    return B3G_OK;
+}
+
+// The persistent CG of the cloth's strategy: the barrier is cleared, then one
+// cooperative launch (two grid reductions per iteration, or the fused form).
+cudaError_t launch_persistent_cg(b3g_cloth* c, int dot, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st);
+    if (e != cudaSuccess) return e;
+    if (c->cg_strategy == B3G_CG_PERSISTENT_FUSED) return launch_grid_cg_fused(c->dev, dot, c->dev.bar, c->cg_rec, st);
+    return launch_grid_cg(c->dev, dot, c->dev.bar, st);
+}
+
 // Captures one step: [contacts_update] assemble cg_init while{cg iteration}
 // finalize [contact_position x (pos_iters - 1)] post.
 b3g_status build_graph(b3g_cloth* c, uint32_t pos_iters)
@@ -116,9 +142,8 @@ b3g_status build_graph(b3g_cloth* c, uint32_t pos_iters)
     do {
         if ((err = launch_contacts_update(c->dev, st)) != cudaSuccess) break;
         if ((err = launch_assemble(c->dev, c->assemble_block, st)) != cudaSuccess) break;
-        if (c->cg_strategy == B3G_CG_PERSISTENT) {
-            if ((err = cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st)) != cudaSuccess) break;
-            if ((err = launch_grid_cg(c->dev, dot, c->dev.bar, st)) != cudaSuccess) break;
+        if (persistent_cg(c)) {
+            if ((err = launch_persistent_cg(c, dot, st)) != cudaSuccess) break;
         } else {
             cudaStreamCaptureStatus cs;
             cudaGraph_t cap;
@@ -181,9 +206,8 @@ b3g_status launch_step_plain(b3g_cloth* c, uint32_t pos_iters)
     cudaGraphConditionalHandle none = 0;
     B3G_TRY(launch_contacts_update(c->dev, st));
     B3G_TRY(launch_assemble(c->dev, c->assemble_block, st));
-    if (c->cg_strategy == B3G_CG_PERSISTENT) {
-        B3G_TRY(cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st));
-        B3G_TRY(launch_grid_cg(c->dev, dot, c->dev.bar, st));
+    if (persistent_cg(c)) {
+        B3G_TRY(launch_persistent_cg(c, dot, st));
     } else {
         B3G_TRY(launch_cg_init(c->dev, dot, none, 0, st));
         for (uint32_t k = 0; k < c->opts.max_iterations; ++k) B3G_TRY(launch_cg_iteration(c->dev, dot, none, 0, st));
@@ -209,9 +233,8 @@ b3g_status launch_step_self(b3g_cloth* c, float dt)
     B3G_TRY(launch_contacts_update(c->dev, st));
     if (dt > 0.0f) {
         B3G_TRY(launch_assemble(c->dev, c->assemble_block, st));
-        if (c->cg_strategy == B3G_CG_PERSISTENT) {
-            B3G_TRY(cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st));
-            B3G_TRY(launch_grid_cg(c->dev, dot, c->dev.bar, st));
+        if (persistent_cg(c)) {
+            B3G_TRY(launch_persistent_cg(c, dot, st));
         } else {
             B3G_TRY(launch_cg_init(c->dev, dot, none, 0, st));
             for (uint32_t k = 0; k < c->opts.max_iterations; ++k)
@@ -550,6 +573,7 @@ b3g_status destroy_cloth(b3g_cloth* c)
     for (void* p : c->hull_bufs) cudaFree(p);
     c->hull_bufs.clear();
     if (c->ray_buf) cudaFree(c->ray_buf);
+    if (c->cg_rec) cudaFree(c->cg_rec);
     destroy_graph(c);
     if (c->arena.base && c->owns_arena) cudaFree(c->arena.base);
     if (c->d_ops) cudaFree(c->d_ops);
@@ -1152,7 +1176,7 @@ b3g_status b3g_cloth_apply_translations(b3g_cloth* c, const float* t)
 b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, b3g_step_stats* stats)
 {
     if (!valid(c) || !c->owns_stream) return B3G_ERR_INVALID_ARGUMENT;
-    if (!(dt >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    if (!(dt >= 0.0f) || pos_iters > (uint32_t)kMaxPosIters) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     b3g_status s = flush_ops(c);
     if (s != B3G_OK) return s;
@@ -1171,6 +1195,7 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
     h->gx = c->gravity[0];
     h->gy = c->gravity[1];
     h->gz = c->gravity[2];
+    if ((s = ensure_cg_rec(c)) != B3G_OK) return s;
     B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, st));
     B3G_TRY(cudaEventRecord(c->ev0, st));
     if (c->self) {
@@ -1207,7 +1232,7 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
         // kernel nodes the graph ran: [contacts_update] assemble cg_init,
         // 3 per CG iteration, finalize, [contact_position x (pos_iters - 1)], post
         const uint64_t ns = c->dev.nsph ? 1 : 0;
-        const uint64_t cg = c->cg_strategy == B3G_CG_PERSISTENT ? 1 : 1 + 3ull * L.iterations;
+        const uint64_t cg = persistent_cg(c) ? 1 : 1 + 3ull * L.iterations;
         count_launches(ns + 1 + cg + 1 + (ns && pos_iters > 1 ? pos_iters - 1 : 0) + 1);
     }
     if (stats) *stats = L;
@@ -1238,7 +1263,8 @@ b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, u
                                    b3g_phase_times* times, b3g_step_stats* stats)
 {
     if (c && c->self) return B3G_ERR_UNSUPPORTED;
-    if (!valid(c) || !c->owns_stream || !times || !(dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    if (!valid(c) || !c->owns_stream || !times || !(dt > 0.0f) || pos_iters > (uint32_t)kMaxPosIters)
+        return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(c->device);
     b3g_status s = flush_ops(c);
     if (s != B3G_OK) return s;
@@ -1257,6 +1283,7 @@ b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, u
     h->gx = c->gravity[0];
     h->gy = c->gravity[1];
     h->gz = c->gravity[2];
+    if ((s = ensure_cg_rec(c)) != B3G_OK) return s;
     B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, st));
     std::memset(times, 0, sizeof(*times));
     const int dot = (int)c->opts.dot;
@@ -1275,18 +1302,14 @@ b3g_status b3g_cloth_step_profiled(b3g_cloth* c, float dt, uint32_t vel_iters, u
         return s;
     if ((s = timed(&times->assemble_ms, [&] { return launch_assemble(c->dev, c->assemble_block, st); }))) return s;
     StepScalars probe;
-    if (c->cg_strategy == B3G_CG_PERSISTENT) {
-        B3G_TRY(cudaMemsetAsync(c->dev.bar, 0, sizeof(GridBarrier), st));
-        if ((s = timed(&times->cg_spmv_ms, [&] {
-                 return launch_grid_cg(c->dev, dot, c->dev.bar, st);
-             })))
-            return s;
+    if (persistent_cg(c)) {
+        if ((s = timed(&times->cg_spmv_ms, [&] { return launch_persistent_cg(c, dot, st); }))) return s;
         B3G_TRY(cudaMemcpy(&probe, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost));
         times->cg_iterations = probe.iter;
     } else if ((s = timed(&times->cg_init_ms, [&] { return launch_cg_init(c->dev, dot, none, 0, st); }))) {
         return s;
     }
-    for (; c->cg_strategy != B3G_CG_PERSISTENT;) {
+    for (; !persistent_cg(c);) {
         B3G_TRY(cudaMemcpy(&probe, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost));
         if (!probe.cont) break;
         if ((s = timed(&times->cg_spmv_ms, [&] { return launch_cg_part(c->dev, dot, 0, st); }))) return s;
@@ -1333,7 +1356,13 @@ b3g_status b3g_debug_cg_barrier_timeout(b3g_cloth* c, uint32_t spin_limit, b3g_s
     B3G_TRY(cudaMemcpyAsync(c->dev.sc, h, sizeof(StepScalars), cudaMemcpyHostToDevice, st));
     B3G_TRY(cudaMemcpyAsync(c->dev.bar, &bar, sizeof(bar), cudaMemcpyHostToDevice, st));
     B3G_TRY(launch_assemble(c->dev, c->assemble_block, st));
-    B3G_TRY(launch_grid_cg(c->dev, (int)c->opts.dot, c->dev.bar, st));
+    if (c->cg_strategy == B3G_CG_PERSISTENT_FUSED) {
+        b3g_status s = ensure_cg_rec(c);
+        if (s != B3G_OK) return s;
+        B3G_TRY(launch_grid_cg_fused(c->dev, (int)c->opts.dot, c->dev.bar, c->cg_rec, st));
+    } else {
+        B3G_TRY(launch_grid_cg(c->dev, (int)c->opts.dot, c->dev.bar, st));
+    }
     B3G_TRY(cudaMemcpyAsync(h, c->dev.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, st));
     B3G_TRY(cudaStreamSynchronize(st));
     *result = (b3g_status)h->status;
@@ -1342,9 +1371,12 @@ b3g_status b3g_debug_cg_barrier_timeout(b3g_cloth* c, uint32_t spin_limit, b3g_s
 
 b3g_status b3g_cloth_set_cg_strategy(b3g_cloth* c, b3g_cg_strategy s)
 {
-    if (!valid(c) || (s != B3G_CG_LAUNCHES && s != B3G_CG_PERSISTENT)) return B3G_ERR_INVALID_ARGUMENT;
+    if (!valid(c) || (s != B3G_CG_LAUNCHES && s != B3G_CG_PERSISTENT && s != B3G_CG_PERSISTENT_FUSED))
+        return B3G_ERR_INVALID_ARGUMENT;
     c->cg_strategy = s;
-    return B3G_OK;
+    if (!c->owns_stream) return B3G_OK;  // batch and server cloths run their own CG
+    cudaSetDevice(c->device);
+    return ensure_cg_rec(c);
 }
 
 b3g_status b3g_cloth_get_info(const b3g_cloth* c, b3g_cloth_info* info)
@@ -1428,6 +1460,18 @@ b3g_status b3g_cloth_get_energy(const b3g_cloth* cc, float* energy)
         E += c->topo.mass[i] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
     }
     *energy = 0.5f * E;
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_read_proxies(const b3g_cloth* cc, float* lo, float* hi)
+{
+    b3g_cloth* c = const_cast<b3g_cloth*>(cc);
+    if (!valid(c) || (!lo && !hi)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    if (lo && (s = read_planes(c, c->dev.fat_lo, lo)) != B3G_OK) return s;
+    if (hi && (s = read_planes(c, c->dev.fat_hi, hi)) != B3G_OK) return s;
     return B3G_OK;
 }
 

@@ -27,7 +27,7 @@ namespace b3g {
 
 constexpr int kMaxSpheres = 4;
 constexpr int kSlice = 32;
-constexpr int kMaxPosIters = 16;
+constexpr int kMaxPosIters = 16;  // B3G_MAX_POSITION_ITERATIONS
 
 // Device scalars of one cloth's step (CG state, reductions, contact flags).
 struct StepScalars {

@@ -71,6 +71,8 @@ struct b3g_cloth {
     bool graph_ok = true;
     b3g_cg_strategy cg_strategy = B3G_CG_LAUNCHES;
     b3g_cg_strategy graph_strategy = B3G_CG_LAUNCHES;
+    float4* cg_rec = nullptr;                 // fused persistent CG: per-vertex records of two iterations
+    uint32_t cg_rec_n = 0;                    // vertices cg_rec was sized for
 
     b3g_step_stats last{};
 

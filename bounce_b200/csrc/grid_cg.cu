@@ -394,9 +394,287 @@ const void* grid_kernel(bool one_row)
     return one_row ? (const void*)k_grid_cg<DOT, true> : (const void*)k_grid_cg<DOT, false>;
 }
 
+// ---------------------------------------------------------------------------
+// The fused form: one grid reduction per iteration
+// ---------------------------------------------------------------------------
+//
+// Every vertex publishes, once per iteration, a record of its r, s and p and
+// its S P^-1 (zero on rows that are not dynamic) as three float4:
+// (r.xyz, s.x) (s.yz, p.xy) (p.z, SP^-1.xyz).  Records alternate between two
+// buffers by iteration parity.
+//
+// A pass starts from everyone's record of the previous pass and that pass's
+// alpha and beta.  Each row applies the previous update to itself,
+//   x += alpha p,  r -= alpha s,  z = S P^-1 r,  p = z + beta p
+// (cloth_force_solver.cpp:115-131), forms the same p for each neighbour it
+// multiplies from the neighbour's record (the same float expressions, so
+// every row sees bit-identical p), and computes s = S A p.  One reduction then
+// gives four sums of the new iterate: p.s, s.z, s.P^-1 s and r.z.
+//  - r.z is the reference's delta_new of this iterate, recomputed, not carried;
+//    when it meets the stop rule the pass is discarded, as the reference would
+//    stop before it.
+//  - alpha = r.z / p.s, the reference's expression.
+//  - The next delta is r'.z' for r' = r - alpha s, expanded:
+//    r.z - 2 alpha s.z + alpha^2 s.P^-1 s.  It sets beta = delta' / r.z and
+//    the stop test; the next pass recomputes it exactly.  So x, r, z and p
+//    follow the reference's expressions, and only beta's numerator rounds
+//    differently (by one iteration's rounding, never accumulated).
+// The pass after the last accepted one applies nothing; the solution takes
+// the last update itself.
+
+struct Rec {
+    f3 r, s, p, sp;
+};
+
+__device__ __forceinline__ Rec ld_rec(const float4* rec, uint32_t j)
+{
+    const float4 a = __ldcg(rec + 3 * (size_t)j), b = __ldcg(rec + 3 * (size_t)j + 1),
+                 c = __ldcg(rec + 3 * (size_t)j + 2);
+    return Rec{f3{a.x, a.y, a.z}, f3{a.w, b.x, b.y}, f3{b.z, b.w, c.x}, f3{c.y, c.z, c.w}};
+}
+
+__device__ __forceinline__ void st_rec(float4* rec, uint32_t j, f3 r, f3 s, f3 p, f3 sp)
+{
+    rec[3 * (size_t)j] = make_float4(r.x, r.y, r.z, s.x);
+    rec[3 * (size_t)j + 1] = make_float4(s.y, s.z, p.x, p.y);
+    rec[3 * (size_t)j + 2] = make_float4(p.z, sp.x, sp.y, sp.z);
+}
+
+__device__ __forceinline__ f3 hadamard(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+
+// The direction of this pass at a vertex, from its record of the previous
+// pass: the owner evaluates exactly this for its own row.
+__device__ __forceinline__ f3 rec_direction(const Rec& q, float alpha, float beta, bool first)
+{
+    if (first) return hadamard(q.r, q.sp);
+    const f3 rn = q.r - alpha * q.s;
+    return hadamard(rn, q.sp) + beta * q.p;
+}
+
+// The scalars of one pass from its four sums.  Returns false when the true
+// delta of the iterate (r.z) already meets the stop rule: the pass is then
+// discarded.  DOT 0 and 1 round every scalar to float, as the reference's
+// float32 b3Dot does.
+template <int DOT>
+__device__ __forceinline__ bool fused_scalars(const StepScalars* sc, double ps, double sz, double sps, double rz,
+                                              double b_delta, float& alpha, float& beta, double& delta_next,
+                                              double& delta_true)
+{
+    if (DOT != 2) {
+        ps = (double)(float)ps;
+        rz = (double)(float)rz;
+    }
+    delta_true = rz;
+    if (cg_stop(sc, rz, b_delta)) return false;
+    alpha = DOT == 2 ? (float)(rz / ps) : (float)rz / (float)ps;
+    const double a = (double)alpha;
+    double dn = rz - 2.0 * a * sz + a * a * sps;
+    if (DOT != 2) dn = (double)(float)dn;
+    delta_next = dn;
+    beta = DOT == 2 ? (float)(dn / rz) : (float)dn / (float)rz;
+    return true;
+}
+
+template <int DOT, bool ONE_ROW>
+__global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_constant__ ClothDev c, GridBarrier* bar,
+                                                             float4* rec0, float4* rec1)
+{
+    typedef DotT<DOT> D;
+    typedef typename D::T T;
+    StepScalars* sc = c.sc;
+    const uint32_t n = c.n;
+    const uint32_t nb = gridDim.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t first_row = blockIdx.x * blockDim.x + threadIdx.x;
+    T* part0 = reinterpret_cast<T*>(c.partials);
+    T* part1 = part0 + 4 * nb;
+    const uint32_t max_iter = sc->max_iter;
+    uint32_t epoch = 0;
+
+    const bool act = first_row < n;
+    bool Si = false;
+    RegRow rr;
+    f3 x = zero3(), r = zero3(), s = zero3(), p = zero3(), sp = zero3();
+    if (ONE_ROW && act) load_reg_row(c, first_row, rr);
+
+    // x0 = S m_x, r = S (b - A x0), b_delta, delta = r.S P^-1 r
+    // (cloth_force_solver.cpp:90-100); record 0 holds r with s = p = 0.
+    T v2[2] = {D::zero(), D::zero()};
+    for (uint32_t row = first_row; row < n; row += stride) {
+        const bool Sr = dyn(c, row);
+        f3 ax = zero3();
+        if (ONE_ROW) {
+#pragma unroll
+            for (int k = 0; k < kRegCols; ++k) {
+                if ((uint32_t)k < rr.deg) {
+                    const uint32_t col = rr.col[k];
+                    const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
+                    ax = ax + block_at(c, rr.base + 32u * k) * xj;
+                }
+            }
+        } else {
+            const uint32_t base = rbase(c, row);
+            const uint32_t deg = c.row_deg[row];
+            for (uint32_t k = 0; k < deg; ++k) {
+                const uint32_t idx = base + 32u * k;
+                const uint32_t col = c.cols[idx];
+                const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
+                ax = ax + block_at(c, idx) * xj;
+            }
+        }
+        const f3 bi = ld3(c.b, n, row);
+        const f3 pvr = ld3(c.pinv, n, row);
+        const f3 rv = Sr ? bi - ax : zero3();
+        const f3 spr = Sr ? pvr : zero3();
+        const f3 zv = hadamard(rv, spr);
+        const f3 bh = Sr ? bi : zero3();
+        const f3 x0 = Sr ? ld3(c.mx, n, row) : zero3();
+        st_rec(rec0, row, rv, zero3(), zero3(), spr);
+        if (ONE_ROW) {
+            Si = Sr, x = x0, r = rv, sp = spr;
+        } else {
+            st3(c.dv, n, row, x0);
+        }
+        v2[0] = D::add_term(v2[0], bh, mk(bh.x * pvr.x, bh.y * pvr.y, bh.z * pvr.z));
+        v2[1] = D::add_term(v2[1], rv, zv);
+        if (ONE_ROW) break;
+    }
+    if (!grid_total<DOT, 2>(v2, part0, bar, nb, epoch)) goto timeout;
+    {
+        double b_delta = D::value(v2[0]), delta = D::value(v2[1]);
+        if (DOT != 2) {
+            b_delta = (double)(float)b_delta;
+            delta = (double)(float)delta;
+        }
+        const double delta0 = delta;
+        uint32_t status = (!isfinite(delta) || !isfinite(b_delta)) ? kStatusNumerical : 0u;
+        uint32_t it = 0;
+        float alpha = 0.0f, beta = 0.0f;
+        bool pending = false;  // the last accepted pass's update of x is not applied yet
+        bool cont = status == 0 && max_iter > 0 && !cg_stop(sc, delta, b_delta);
+        while (cont) {
+            const bool first = it == 0;
+            const float4* rin = (it & 1u) ? rec1 : rec0;
+            float4* rout = (it & 1u) ? rec0 : rec1;
+            T v4[4] = {D::zero(), D::zero(), D::zero(), D::zero()};
+            if (ONE_ROW) {
+                if (act) {
+                    f3 z;
+                    if (first) {
+                        z = hadamard(r, sp);
+                        p = z;
+                    } else {
+                        x = x + alpha * p;
+                        r = r - alpha * s;
+                        z = hadamard(r, sp);
+                        p = z + beta * p;
+                    }
+                    // s = S A p; slot 0 is the row's own diagonal block
+                    f3 acc = zero3() + block_at(c, rr.base) * p;
+#pragma unroll
+                    for (int k = 1; k < kRegCols; ++k) {
+                        if ((uint32_t)k < rr.deg) {
+                            const m3 a = block_at(c, rr.base + 32u * k);
+                            const Rec q = ld_rec(rin, rr.col[k]);
+                            acc = acc + a * rec_direction(q, alpha, beta, first);
+                        }
+                    }
+                    s = Si ? acc : zero3();
+                    st_rec(rout, first_row, r, s, p, sp);
+                    v4[0] = D::add_term(v4[0], p, s);
+                    v4[1] = D::add_term(v4[1], s, z);
+                    v4[2] = D::add_term(v4[2], s, hadamard(s, sp));
+                    v4[3] = D::add_term(v4[3], r, z);
+                }
+            } else {
+                for (uint32_t row = first_row; row < n; row += stride) {
+                    const Rec own = ld_rec(rin, row);
+                    f3 rv = own.r, pv;
+                    if (!first) {
+                        st3(c.dv, n, row, ld3(c.dv, n, row) + alpha * own.p);
+                        rv = own.r - alpha * own.s;
+                    }
+                    const f3 z = hadamard(rv, own.sp);
+                    pv = first ? z : z + beta * own.p;
+                    const uint32_t base = rbase(c, row);
+                    const uint32_t deg = c.row_deg[row];
+                    f3 acc = zero3() + block_at(c, base) * pv;
+                    constexpr int W = 4;
+                    for (uint32_t k0 = 1; k0 < deg; k0 += W) {
+                        uint32_t cl[W];
+#pragma unroll
+                        for (int k = 0; k < W; ++k) cl[k] = (k0 + k < deg) ? c.cols[base + 32u * (k0 + k)] : 0u;
+#pragma unroll
+                        for (int k = 0; k < W; ++k) {
+                            if (k0 + k < deg) {
+                                const m3 a = block_at(c, base + 32u * (k0 + k));
+                                const Rec q = ld_rec(rin, cl[k]);
+                                acc = acc + a * rec_direction(q, alpha, beta, first);
+                            }
+                        }
+                    }
+                    const f3 sv = dyn(c, row) ? acc : zero3();
+                    st_rec(rout, row, rv, sv, pv, own.sp);
+                    v4[0] = D::add_term(v4[0], pv, sv);
+                    v4[1] = D::add_term(v4[1], sv, z);
+                    v4[2] = D::add_term(v4[2], sv, hadamard(sv, own.sp));
+                    v4[3] = D::add_term(v4[3], rv, z);
+                }
+            }
+            if (!grid_total<DOT, 4>(v4, (it & 1u) ? part0 : part1, bar, nb, epoch)) goto timeout;
+            double dn = 0.0, dt = 0.0;
+            float a1 = 0.0f, b1 = 0.0f;
+            const bool accept = fused_scalars<DOT>(sc, D::value(v4[0]), D::value(v4[1]), D::value(v4[2]),
+                                                   D::value(v4[3]), b_delta, a1, b1, dn, dt);
+            if (!accept) {
+                // the iterate already meets the stop rule: the reference stops
+                // before this pass; its x is the current one
+                pending = false;
+                delta = dt;
+                break;
+            }
+            alpha = a1;
+            beta = b1;
+            pending = true;
+            delta = dn;
+            ++it;
+            if (!isfinite(dn) || !isfinite(alpha) || !isfinite(beta)) status = kStatusNumerical;
+            cont = status == 0 && it < max_iter && !cg_stop(sc, dn, b_delta);
+        }
+        // the last accepted update, x += alpha p
+        if (ONE_ROW) {
+            if (act) st3(c.dv, n, first_row, pending ? x + alpha * p : x);
+        } else if (pending) {
+            const float4* rl = (it & 1u) ? rec1 : rec0;
+            for (uint32_t row = first_row; row < n; row += stride)
+                st3(c.dv, n, row, ld3(c.dv, n, row) + alpha * ld_rec(rl, row).p);
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            sc->b_delta = b_delta;
+            sc->delta0 = delta0;
+            sc->delta = delta;
+            sc->iter = it;
+            sc->status = status;
+            sc->cont = 0;
+        }
+        return;
+    }
+timeout:
+    if (threadIdx.x == 0) {
+        sc->status = kStatusTimeout;
+        sc->cont = 0;
+    }
+}
+
+template <int DOT>
+const void* fused_kernel(bool one_row)
+{
+    return one_row ? (const void*)k_grid_cg_fused<DOT, true> : (const void*)k_grid_cg_fused<DOT, false>;
+}
+
 }  // namespace
 
-GridCgShape grid_cg_shape(uint32_t n, int device)
+GridCgShape grid_cg_shape(uint32_t n, int device, bool fused)
 {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -408,7 +686,8 @@ GridCgShape grid_cg_shape(uint32_t n, int device)
         g.blocks = (int)((n + g.threads - 1) / g.threads);
     } else {
         int per_sm = 1;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_cg<2, false>, kMaxBlock, 0) != cudaSuccess ||
+        const void* fn = fused ? (const void*)k_grid_cg_fused<2, false> : (const void*)k_grid_cg<2, false>;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMaxBlock, 0) != cudaSuccess ||
             per_sm < 1) {
             cudaGetLastError();
             per_sm = 1;
@@ -424,7 +703,7 @@ cudaError_t launch_grid_cg(const ClothDev& c, int dot, GridBarrier* bar, cudaStr
 {
     int dev = 0;
     cudaGetDevice(&dev);
-    const GridCgShape g = grid_cg_shape(c.n, dev);
+    const GridCgShape g = grid_cg_shape(c.n, dev, false);
     const bool one_row = (uint64_t)g.blocks * (uint64_t)g.threads >= c.n && c.max_deg <= (uint32_t)kRegCols;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(g.blocks);
@@ -437,6 +716,29 @@ cudaError_t launch_grid_cg(const ClothDev& c, int dot, GridBarrier* bar, cudaStr
     cfg.numAttrs = 1;
     const void* fn = dot == 2 ? grid_kernel<2>(one_row) : dot == 1 ? grid_kernel<1>(one_row) : grid_kernel<0>(one_row);
     void* args[2] = {const_cast<ClothDev*>(&c), &bar};
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
+    count_launches(1);
+    return e;
+}
+
+cudaError_t launch_grid_cg_fused(const ClothDev& c, int dot, GridBarrier* bar, float4* rec, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const GridCgShape g = grid_cg_shape(c.n, dev, true);
+    const bool one_row = (uint64_t)g.blocks * (uint64_t)g.threads >= c.n && c.max_deg <= (uint32_t)kRegCols;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(g.blocks);
+    cfg.blockDim = dim3(g.threads);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const void* fn = dot == 2 ? fused_kernel<2>(one_row) : dot == 1 ? fused_kernel<1>(one_row) : fused_kernel<0>(one_row);
+    float4* rec1 = rec + 3 * (size_t)c.n;
+    void* args[4] = {const_cast<ClothDev*>(&c), &bar, &rec, &rec1};
     const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     count_launches(1);
     return e;

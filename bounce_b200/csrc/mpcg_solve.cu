@@ -305,7 +305,9 @@ extern "C" b3g_status b3g_mpcg_solve(uint32_t n, const uint32_t* rowptr, const u
 // B3G_MPCG_NOALLOC_MAX_ROWS block rows, which every GPU that loads the library
 // holds until the process exits.  The array's name is only a host-side
 // stand-in in host code, so its device address is looked up once per device
-// with cudaGetSymbolAddress, by the first call on that device.
+// with cudaGetSymbolAddress, by the first call on that device, and kept for
+// the life of the process: a cudaDeviceReset after that call is not
+// supported, since the module and the array may then load at another address.
 
 namespace b3g {
 namespace {

@@ -197,7 +197,9 @@ extern "C" {
 
 b3g_status b3g_server_create(int device, const b3g_server_config* cfg, b3g_server** out)
 {
-    if (!cfg || !out || cfg->max_active == 0 || !(cfg->dt > 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    if (!cfg || !out || cfg->max_active == 0 || !(cfg->dt > 0.0f) ||
+        cfg->position_iterations > (uint32_t)kMaxPosIters)
+        return B3G_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {

@@ -933,7 +933,7 @@ b3g_status b3g_softbody_set_solver(b3g_softbody* b, const b3g_solver_opts* o)
 b3g_status b3g_softbody_step(b3g_softbody* b, float dt, uint32_t velocity_iterations, uint32_t position_iterations,
                              b3g_step_stats* stats)
 {
-    if (!ok(b) || !(dt >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
+    if (!ok(b) || !(dt >= 0.0f) || position_iterations > (uint32_t)kMaxPosIters) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(b->device);
     cudaStream_t s = b->stream;
     SoftDev& d = b->dev;

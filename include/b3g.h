@@ -192,21 +192,29 @@ b3g_status b3g_cloth_apply_translations(b3g_cloth* cloth, const float* translati
 
 /* b3Cloth::Step (cloth.cpp:551-601): body-contact update, force/Jacobian
  * assembly, S-filtered Jacobi-preconditioned CG, contact velocity and position
- * iterations, AABB sync, new body contacts.  Cloth self-collision is not part
- * of this path.  stats may be NULL.  The step is enqueued and waited for. */
+ * iterations, AABB sync, new body contacts; at thickness > 0 also the
+ * particle-triangle contacts (self-collision).  stats may be NULL.  The step
+ * is enqueued and waited for.  At most B3G_MAX_POSITION_ITERATIONS position
+ * iterations (the reference takes any number; more than that returns
+ * B3G_ERR_INVALID_ARGUMENT, here and in every other step call). */
+#define B3G_MAX_POSITION_ITERATIONS 16
 b3g_status b3g_cloth_step(b3g_cloth* cloth, float dt, uint32_t velocity_iterations,
                           uint32_t position_iterations, b3g_step_stats* stats);
 
 /* How one cloth's CG runs on the GPU.  LAUNCHES (default): three kernels
  * per iteration inside a CUDA-graph while loop.  PERSISTENT: one cooperative
- * launch for the whole solve, iterations separated by grid barriers with
- * bounded waits (B3G_ERR_TIMEOUT if one gives up); for large cloths.
- * PERSISTENT_FUSED: as PERSISTENT with one grid reduction per iteration
- * instead of two; the next r.P^-1 r comes from the same sums as alpha
- * (r.z - 2 alpha s.z + alpha^2 s.P^-1 s), so x, r, z and p follow the
- * reference's expressions and only beta's numerator rounds differently.
- * Cloths of up to one row per thread of the GPU (about 75k vertices on a
- * B200) take the fused form; larger ones run PERSISTENT. */
+ * launch for the whole solve, two grid reductions per iteration, separated by
+ * grid barriers with bounded waits (B3G_ERR_TIMEOUT if one gives up); for
+ * large cloths.  PERSISTENT_FUSED: as PERSISTENT with one grid reduction per
+ * iteration.  Each vertex publishes r, s and p once per iteration, and every
+ * row forms its neighbours' next direction from them.  The reduction returns
+ * p.s, s.z, s.P^-1 s and r.z (z = S P^-1 r) of the iterate: alpha = r.z / p.s
+ * as the reference's, and the next r.z expanded as
+ * r.z - 2 alpha s.z + alpha^2 s.P^-1 s gives beta and the stop test.  So x, r,
+ * z and p follow the reference's expressions and only beta's numerator
+ * rounds differently; the next iteration recomputes r.z exactly, and a pass
+ * whose exact r.z already meets the stop rule is discarded.  It needs a
+ * device buffer of 96 bytes per vertex, allocated when the strategy is set. */
 typedef enum { B3G_CG_LAUNCHES = 0, B3G_CG_PERSISTENT = 1, B3G_CG_PERSISTENT_FUSED = 2 } b3g_cg_strategy;
 b3g_status b3g_cloth_set_cg_strategy(b3g_cloth* cloth, b3g_cg_strategy strategy);
 /* Diagnostic of the bounded waits: runs the persistent CG once with a grid
@@ -259,6 +267,11 @@ b3g_status b3g_cloth_get_energy(const b3g_cloth* cloth, float* energy);
  * sphere_count bytes each), impulses (normal, tangent1, tangent2). */
 b3g_status b3g_cloth_read_contacts(const b3g_cloth* cloth, uint8_t* exists, uint8_t* active,
                                    float* impulses);
+/* The particles' broadphase proxies (b3Particle's fat AABB, cloth.cpp:
+ * 312-317, moved by b3Particle::Synchronize as in b3ClothSolver, and read by
+ * the body-contact lifetime test): lower and upper corners, 3 floats per
+ * vertex; either pointer may be NULL. */
+b3g_status b3g_cloth_read_proxies(const b3g_cloth* cloth, float* lo, float* hi);
 /* Self-collision: the particle-triangle contacts of a cloth whose thickness
  * is above zero (b3ClothContactManager::m_particleTriangleContactList,
  * include/bounce/cloth/cloth_contact_manager.h; b3ParticleTriangleContact,
@@ -325,7 +338,12 @@ b3g_status b3g_mpcg_solve(uint32_t n, const uint32_t* rowptr, const uint32_t* co
  *    loads the library holds it until the process exits.  Larger systems
  *    return B3G_ERR_CAPACITY.
  *  - The first call on each device looks the array's device address up
- *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *    (cudaGetSymbolAddress) and keeps it for the life of the process; make
+ *    that first call before any stream capture.  A cudaDeviceReset after it
+ *    is not supported (the library's module, and the array with it, may come
+ *    back at another address).
+ *  - Like b3g_mpcg_solve, it waits for its work to finish before it returns:
+ *    the iteration count and residual are read back to the host.
  *  - All calls share the one array: calls whose work overlaps on the GPU
  *    (other streams, other host threads) race and corrupt each other.  Each
  *    call clears the CG scalars it needs zeroed; other scratch contents are
@@ -484,7 +502,8 @@ b3g_status b3g_softbody_set_position(b3g_softbody* body, uint32_t node, const fl
 /* Default: the reference's MPCG (20 iterations, FLT_EPSILON^2, FP32 dots). */
 b3g_status b3g_softbody_set_solver(b3g_softbody* body, const b3g_solver_opts* opts);
 /* b3SoftBody::Step (softbody.cpp:700-735) without a world.  stats->delta0 is
- * r.P^-1 r at the CG start, b_delta the soft body's delta_0 (Sb . diag(A) Sb). */
+ * r.P^-1 r at the CG start, b_delta the soft body's delta_0 (Sb . diag(A) Sb).
+ * At most B3G_MAX_POSITION_ITERATIONS position iterations. */
 b3g_status b3g_softbody_step(b3g_softbody* body, float dt, uint32_t velocity_iterations,
                              uint32_t position_iterations, b3g_step_stats* stats);
 /* b3SoftBody::SetWorld with static hulls (b3HullShape on a static body at the

@@ -63,6 +63,8 @@ def port_lib():
         L.oc_set_gravity.argtypes = [C.c_void_p, _f32p]
         L.oc_set_type.argtypes = [C.c_void_p, C.c_uint32, C.c_int]
         L.oc_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oc_set_contacts.argtypes = [C.c_void_p, C.c_uint32, _u32p, _u32p, _f32p]
+        L.oc_set_proxies.argtypes = [C.c_void_p, _f32p, _f32p]
         for name in ("oc_apply_force", "oc_apply_translation", "oc_set_position", "oc_set_velocity"):
             getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, _f32p]
         L.oc_add_sphere.argtypes = [C.c_void_p, _f32p, C.c_float, C.c_float]
@@ -296,6 +298,21 @@ class PortCloth(_Base):
     def set_state(self, x=None, v=None, dv=None):
         arrs = [None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1) for a in (x, v, dv)]
         self.L.oc_set_state(self.h, *[None if a is None else a.ctypes.data for a in arrs])
+
+    def set_contacts(self, particles, shapes, impulses):
+        """Replace the body-contact list: contacts from the list's tail (the
+        oldest) to its head, each (particle, shape, 3 impulses)."""
+        p = np.ascontiguousarray(particles, np.uint32).reshape(-1)
+        s = np.ascontiguousarray(shapes, np.uint32).reshape(-1)
+        imp = np.ascontiguousarray(impulses, np.float32).reshape(-1)
+        assert p.size == s.size and imp.size == 3 * p.size
+        self.L.oc_set_contacts(self.h, p.size, p if p.size else np.zeros(1, np.uint32),
+                               s if s.size else np.zeros(1, np.uint32), imp if imp.size else np.zeros(3, np.float32))
+
+    def set_proxies(self, lo, hi):
+        """Overwrite the particles' fat AABBs (n x 3 each)."""
+        self.L.oc_set_proxies(self.h, np.ascontiguousarray(lo, np.float32).reshape(-1),
+                              np.ascontiguousarray(hi, np.float32).reshape(-1))
 
     def apply_force(self, vertex, f):
         self.L.oc_apply_force(self.h, vertex, np.asarray(f, np.float32))

@@ -579,6 +579,41 @@ void oc_set_state(oc_cloth* c, const float* x, const float* v, const float* dv)
     }
 }
 
+/* Replace the body-contact list (used to start the oracle from another
+ * solver's state): `count` contacts in list order from the tail (the oldest)
+ * to the head, each a (particle, shape) pair with its normal and two tangent
+ * impulses (3 floats).  The contact update at the next step start recomputes
+ * activity, normal, tangents and point from the positions, as
+ * b3ClothContactManager::UpdateBodyContacts does (cloth_contact_manager.cpp:
+ * 277-315); what persists between steps is the list and the impulses. */
+void oc_set_contacts(oc_cloth* c, uint32_t count, const uint32_t* particle, const uint32_t* shape,
+                     const float* impulses)
+{
+    if (count > c->contact_cap) {
+        c->contact_cap = count;
+        c->contacts = (contact_t*)realloc(c->contacts, c->contact_cap * sizeof(contact_t));
+    }
+    c->ncontact = count;
+    for (uint32_t q = 0; q < count; ++q) {
+        contact_t* k = c->contacts + q;
+        memset(k, 0, sizeof(*k));
+        k->particle = particle[q];
+        k->shape = shape[q];
+        k->normal_impulse = impulses[3 * q];
+        k->tangent_impulse.x = impulses[3 * q + 1];
+        k->tangent_impulse.y = impulses[3 * q + 2];
+    }
+}
+
+/* Overwrite the particles' broadphase proxies (fat AABBs, xyz triples). */
+void oc_set_proxies(oc_cloth* c, const float* lo, const float* hi)
+{
+    for (uint32_t i = 0; i < c->n; ++i) {
+        c->fat_lo[i] = V(lo[3 * i], lo[3 * i + 1], lo[3 * i + 2]);
+        c->fat_hi[i] = V(hi[3 * i], hi[3 * i + 1], hi[3 * i + 2]);
+    }
+}
+
 void oc_set_gravity(oc_cloth* c, const float* g) { c->gravity = V(g[0], g[1], g[2]); }
 
 /* b3Particle::SetType (particle.cpp:121-143) */

@@ -62,6 +62,11 @@ void oc_destroy(oc_cloth* c);
 
 void oc_set_gravity(oc_cloth* c, const float* g);
 void oc_set_state(oc_cloth* c, const float* x, const float* v, const float* dv);
+/* Replace the body-contact list (tail to head; per contact its particle,
+ * shape and 3 impulses) and the particles' fat AABBs (xyz triples). */
+void oc_set_contacts(oc_cloth* c, uint32_t count, const uint32_t* particle, const uint32_t* shape,
+                     const float* impulses);
+void oc_set_proxies(oc_cloth* c, const float* lo, const float* hi);
 void oc_set_type(oc_cloth* c, uint32_t vertex, int type);
 void oc_apply_force(oc_cloth* c, uint32_t vertex, const float* f);
 void oc_apply_translation(oc_cloth* c, uint32_t vertex, const float* t);

@@ -99,3 +99,51 @@ def test_batch512_sample_matches_oracle(b3g, port):
             oi = o.step(dt)
             assert abs(out["per_cloth"][k]["iterations"] - oi["iterations"]) <= 1, (step, k)
             assert rel_err(cloths[k].state()["x"], o.state()["x"]) <= 1e-4, (step, k)
+
+
+def test_headline_in_contact_one_step(b3g, port):
+    """The headline cloth draped on the sphere, at the benchmark's own setting
+    (CG to relative residual 1e-4, FP64 dots, the fused persistent CG).  After
+    30 steps of fall, some 25,000 particles touch the sphere.  The oracle is
+    given the GPU's whole state: positions, velocities, the CG warm start,
+    the body-contact list with its impulses and the particles' fat AABBs.
+    Then both take one step.
+     - The contact update at the step start is the same arithmetic on the
+       same positions, so the active contacts handed to the solver agree
+       exactly.
+     - CG iterations agree within +-1, positions within 1e-4 relative.
+     - Velocities agree within 1e-4 of the largest velocity.
+     - The contacts alive after the step agree within 0.1%: a particle whose
+       new fat AABB lies within rounding of the sphere's proxy may differ."""
+    scene = b3g.sphere_scene(256)
+    opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
+    gpu = b3g.Cloth(scene.mesh, scene.cdef).setup(scene, opts)
+    gpu.set_cg_strategy(True, fused=True)
+    for _ in range(30):
+        gpu.step(scene.dt)
+    st = gpu.state()
+    gc = gpu.contacts()
+    lo, hi = gpu.proxies()
+    ora = port.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    ora.set_solver(opts.stop_rule, opts.tolerance, opts.max_iterations, opts.dot)
+    ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+    live = np.nonzero(gc["exists"])[0]
+    ora.set_contacts(live, np.zeros(live.size, np.uint32), gc["impulses"][live])
+    ora.set_proxies(lo, hi)
+    assert ora.contacts()["count"] == live.size
+
+    g = gpu.step(scene.dt)
+    o = ora.step(scene.dt)
+    assert o["active_contacts"] > 20000, o["active_contacts"]
+    assert g["active_contacts"] == o["active_contacts"], (g["active_contacts"], o["active_contacts"])
+    assert abs(g["iterations"] - o["iterations"]) <= 1, (g["iterations"], o["iterations"])
+    gs, os_ = gpu.state(), ora.state()
+    ex = rel_err(gs["x"], os_["x"])
+    ev = rel_err(gs["v"], os_["v"])
+    print(f"in contact: {o['active_contacts']} active, iterations {g['iterations']}/{o['iterations']}, "
+          f"x rel {ex:.2e}, v rel {ev:.2e}")
+    assert ex <= 1e-4, ex
+    assert ev <= 1e-4, ev
+    ge = gpu.contacts()["exists"].astype(bool)
+    oe = ora.contacts()["exists"].astype(bool)
+    assert np.count_nonzero(ge != oe) <= max(2, oe.sum() // 1000), np.count_nonzero(ge != oe)

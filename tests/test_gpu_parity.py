@@ -172,14 +172,17 @@ def test_standalone_mpcg_matches_oracle(b3g, port):
         assert rel_err(x, xo) <= 1e-4, rel_err(x, xo)
 
 
-@pytest.mark.parametrize("side,maker", [(64, "sphere"), (200, "plain")])
-def test_persistent_cg_matches_launches(b3g, port, side, maker):
+@pytest.mark.parametrize("fused", [False, True])
+@pytest.mark.parametrize("side,maker", [(64, "sphere"), (200, "plain"), (320, "plain")])
+def test_persistent_cg_matches_launches(b3g, port, side, maker, fused):
     """The persistent cooperative CG (grid barriers) gives the per-step answer
-    of the oracle like the per-iteration launches do."""
+    of the oracle like the per-iteration launches do: in its two-reduction
+    form and in the fused form (one reduction per iteration).  200x200 keeps
+    one row per thread in registers; 320x320 has more rows than threads."""
     scene = b3g.sphere_scene(side) if maker == "sphere" else b3g.plain_scene(side)
     opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
     gpu, ora = _pair(b3g, port, scene, opts)
-    gpu.set_cg_strategy(True)
+    gpu.set_cg_strategy(True, fused=fused)
     for step in range(8):
         st = gpu.state()
         ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
@@ -187,16 +190,40 @@ def test_persistent_cg_matches_launches(b3g, port, side, maker):
         o = ora.step(scene.dt)
         assert abs(g["iterations"] - o["iterations"]) <= 1, (step, g["iterations"], o["iterations"])
         assert rel_err(gpu.state()["x"], ora.state()["x"]) <= 1e-4
+        assert g["delta"] <= 1e-8 * g["b_delta"] * 1.001 or g["iterations"] == 200
 
 
-def test_persistent_cg_bounded_wait_times_out(b3g):
+@pytest.mark.parametrize("dot", [0, 1, 2])
+@pytest.mark.parametrize("maker", ["plain", "sphere"])
+def test_fused_cg_reference_rule_per_step(b3g, port, maker, dot):
+    """The fused CG at the reference's own rule (20 iterations, delta <=
+    FLT_EPSILON^2 b_delta): from identical inputs every step matches the
+    oracle, including contacts, in every dot precision."""
+    scene = b3g.plain_scene(32) if maker == "plain" else b3g.sphere_scene(32)
+    opts = b3g.SolverOptions(b3g.STOP_REFERENCE, 0.0, 20, dot)
+    gpu, ora = _pair(b3g, port, scene, opts)
+    gpu.set_cg_strategy(True, fused=True)
+    for step in range(40):
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        assert abs(g["iterations"] - o["iterations"]) <= 1, (step, g["iterations"], o["iterations"])
+        assert rel_err(gpu.state()["x"], ora.state()["x"]) <= 1e-4, step
+        if maker == "sphere":
+            gc, oc = gpu.contacts(), ora.contacts()
+            assert abs(int(gc["active"].sum()) - int(oc["active"].sum())) <= max(2, oc["active"].sum() // 100)
+
+
+@pytest.mark.parametrize("fused", [False, True])
+def test_persistent_cg_bounded_wait_times_out(b3g, fused):
     """A grid barrier that never completes ends in B3G_ERR_TIMEOUT, and the
     context stays usable: the next step works."""
     import ctypes as C
 
     scene = b3g.plain_scene(128)
     cloth = b3g.Cloth(scene.mesh, scene.cdef).setup(scene, b3g.SolverOptions.relative(1e-4, 50))
-    cloth.set_cg_strategy(True)
+    cloth.set_cg_strategy(True, fused=fused)
     res = C.c_int(0)
     b3g.check(b3g.lib().b3g_debug_cg_barrier_timeout(cloth.h, 2000, C.byref(res)), "timeout diag")
     assert res.value == 7  # B3G_ERR_TIMEOUT
