@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=10)
-    ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--serve-seconds", type=float, default=30.0)
     ap.add_argument("--skip-batch", action="store_true")
     ap.add_argument("--skip-serve", action="store_true")
     # profiling aids: leave out the single-cloth headline, or the one-cloth-at-a-time
@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--self-side", type=int, default=24)
     ap.add_argument("--softbody-side", type=int, default=40)
     ap.add_argument("--softbody-steps", type=int, default=10)
+    ap.add_argument("--skip-stiff", action="store_true")
+    ap.add_argument("--stiff-side", type=int, default=1024)
+    ap.add_argument("--skip-fp64", action="store_true")
     return ap.parse_args()
 
 
@@ -132,10 +135,11 @@ def peaks():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (read + write) of one k_grid_cg launch on the 256x256 headline cloth,
-# from the ncu capture summarised in profiles/k_grid_cg_grid256_sphere.md.  The
-# whole system stays in L2 after its first touch, so the figure holds for any
-# iteration count.  Other sizes have no capture: traffic is reported as null.
+# DRAM bytes (read + write) of one persistent-CG launch on the 256x256 headline
+# cloth, from one ncu capture of that launch (dram__bytes_read.sum +
+# dram__bytes_write.sum).  The whole system stays in L2 after its first
+# touch, so the figure holds for any iteration count.  Other sizes have no
+# capture: traffic is reported as null.
 GRID_CG_TRAFFIC = {256: 36.53e6 + 0.04e6}
 
 
@@ -164,6 +168,45 @@ def algorithmic_bytes(info: dict, kernel: str) -> float:
         inc = 3 * t + 2 * s
         return 36.0 * blocks + (24 + 24 + 4 + 1 + 24) * n + 40.0 * t + 24.0 * s + 8.0 * inc
     return 0.0
+
+
+def fp64_error(system: dict, dv: np.ndarray, tol: float = 1e-11) -> dict:
+    """One step's CG solution against an FP64 solve of the same system on the
+    host (scipy, Jacobi-preconditioned CG to relative residual `tol`, started
+    from the GPU's solution).  The system is the step's A and b with the
+    filter S applied (static rows identity, right-hand side zero).  Returns the
+    relative 2-norm error of dv and the relative residual of the GPU's dv
+    recomputed in FP64 in the P^-1 norm, the norm of the CG stop rule."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+
+    t0 = time.perf_counter()
+    rowptr, cols = system["rowptr"].astype(np.int64), system["cols"].astype(np.int64)
+    n = rowptr.size - 1
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(rowptr))
+    blk = system["vals"].reshape(-1, 3, 3).astype(np.float64)  # [block][column][row]
+    three = np.arange(3, dtype=np.int64)
+    ri = np.broadcast_to(3 * rows[:, None, None] + three[None, None, :], blk.shape).ravel()
+    ci = np.broadcast_to(3 * cols[:, None, None] + three[None, :, None], blk.shape).ravel()
+    A = sp.csr_matrix((blk.ravel(), (ri, ci)), shape=(3 * n, 3 * n))
+    s3 = np.repeat(system["S"].astype(np.float64), 3)
+    Sd = sp.diags(s3)
+    Af = (Sd @ A @ Sd + sp.diags(1.0 - s3)).tocsr()
+    bf = s3 * system["b"].astype(np.float64)
+    pinv = 1.0 / Af.diagonal()
+    M = sp.diags(pinv)
+    x0 = s3 * dv.reshape(-1).astype(np.float64)
+    its = [0]
+
+    def count(_):
+        its[0] += 1
+
+    x64, info = spl.cg(Af, bf, x0=x0, rtol=tol, atol=0.0, maxiter=20000, M=M, callback=count)
+    r = bf - Af @ x0
+    res = float(np.sqrt((r @ (pinv * r)) / (bf @ (pinv * bf))))
+    err = float(np.linalg.norm(x0 - x64) / np.linalg.norm(x64))
+    return {"rel_dv_error": err, "true_residual_fp64": res, "fp64_cg_iterations": its[0],
+            "fp64_converged": info == 0, "seconds": time.perf_counter() - t0}
 
 
 def run_ours(args, rank, world):
@@ -221,6 +264,15 @@ def run_ours(args, rank, world):
     e2e_s = time.perf_counter() - t0
     e2e = replicas.aggregate_rate(n * args.steps, e2e_s)
 
+    # accuracy of one step: its system, then the GPU's CG solution, against
+    # an FP64 solve of that system on the host
+    fp64 = None
+    if not args.skip_fp64:
+        cloth.assemble(scene.dt)
+        system = cloth.system()
+        cloth.step(scene.dt, scene.velocity_iterations, scene.position_iterations)
+        fp64 = fp64_error(system, cloth.state()["dv"])
+
     # per-kernel device times for the roofline
     prof = []
     for _ in range(args.profile_steps):
@@ -255,17 +307,62 @@ def run_ours(args, rank, world):
     achieved = alg / (avg_ms / 1000.0) / 1e9
     cloth.close()
     return {
-        "value": value, "ms_per_step": 1000.0 * dev_s / args.steps, "wall_s": wall, "e2e": e2e,
+        "value": value, "ms_per_step": 1000.0 * dev_s / args.steps, "wall_s": wall, "e2e": e2e, "fp64": fp64,
         "iterations_mean": float(np.mean(iters)), "active_contacts_mean": float(np.mean(contacts)),
         "launches": launches, "clocks": clocks.summary(), "info": info,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                      "unit": "GB/s", "frac": achieved / peak,
                      "traffic": GRID_CG_TRAFFIC.get(args.side) if dom == "grid_cg" else None,
-                     "traffic_source": "ncu capture, profiles/k_grid_cg_grid256_sphere.md",
+                     "traffic_source": "ncu capture of one launch at this size",
                      "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
                      "share": kern[dom][0] / total if total else None},
         "kernel_ms": {k: v[0] / v[1] for k, v in kern.items()},
     }
+
+
+def run_stiff(args, dev: int):
+    """The 1024 x 1024 study cloth (1,048,576 vertices, 2,093,058 triangles,
+    no bending): stretch 1e5, damping 0.1, shear 1e3, the two corners of row
+    0 pinned, no jitter, CG to relative residual 1e-4 (at most 2000
+    iterations) with FP64 dots in the fused persistent form.  Of its 50 steps
+    from rest, steps 3-49 are timed with CUDA events (the first three build
+    the step graph and load the modules).  Its system, 7.3 M blocks or 293 MB
+    of values and columns, is larger than L2, so every CG iteration streams
+    it from HBM.  The roofline is of the CG launch, from three more steps
+    launched kernel by kernel."""
+    import bounce_b200 as b3g
+
+    side = args.stiff_side
+    scene = b3g.stiff_scene(side)
+    opts = b3g.SolverOptions.relative(1e-4, 2000, b3g.DOT_F64)
+    cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene, opts)
+    cloth.set_cg_strategy(True, fused=True)
+    info = cloth.info()
+    warm = 3
+    for _ in range(warm):
+        cloth.step(scene.dt)
+    ms, its = [], []
+    for _ in range(warm, scene.steps):
+        st = cloth.step(scene.dt)
+        ms.append(st["step_ms"])
+        its.append(st["iterations"])
+    prof = [cloth.step_profiled(scene.dt) for _ in range(3)]
+    cloth.close()
+    cg_ms = sum(p["cg_spmv_ms"] for p in prof) / len(prof)
+    cg_it = sum(p["cg_iterations"] for p in prof) / len(prof)
+    alg = algorithmic_bytes(info, f"grid_cg:{cg_it}")
+    peak, peak_kind = peaks()
+    achieved = alg / (cg_ms / 1e3) / 1e9
+    n = info["vertices"]
+    return {"workload": f"grid{side}x{side}_stiff", "vertices": n, "blocks": info["blocks"],
+            "steps": f"{warm}-{scene.steps - 1}", "ms_per_step": sum(ms) / len(ms),
+            "vertex_steps_per_s": n * len(ms) / (sum(ms) / 1e3), "cg_iterations_mean": float(np.mean(its)),
+            "cg_iterations_max": int(max(its)), "cg": "relative residual 1e-4, max 2000, fp64 dots, fused persistent",
+            "roofline": {"bound": "hbm", "kernel": "grid_cg_fused", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": GRID_CG_TRAFFIC.get(side),
+                         "algorithmic_bytes_per_launch": alg, "avg_launch_ms": cg_ms,
+                         "cg_iterations_per_launch": cg_it}}
 
 
 def run_batched(args, dev: int, cpu_sample: bool = False):
@@ -282,7 +379,6 @@ def run_batched(args, dev: int, cpu_sample: bool = False):
     scenes = [every[k] for k in shards[env.rank]]
     opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
     cloths = [b3g.Cloth(sc.mesh, sc.cdef, device=dev).setup(sc, opts) for sc in scenes]
-    plain = [b3g.Cloth(sc.mesh, sc.cdef, device=dev).setup(sc, opts) for sc in scenes]
     rows = sum(c.n for c in cloths)
     dt = scenes[0].dt
     batch = b3g.Batch(max(1024, len(cloths)), device=dev)
@@ -302,24 +398,37 @@ def run_batched(args, dev: int, cpu_sample: bool = False):
         # the same per-cloth count as the persistent single-cloth solve
         cg_bytes.append(float(np.sum(40.0 * blocks + 73.0 * nrows + it * (40.0 * blocks + 146.0 * nrows))))
     launches = b3g.kernel_launch_count() - launches0
-    # the plain single-instance path, same cloths, same number of steps
     batched = replicas.aggregate_rate(rows * len(ms), sum(ms) / 1000.0)
-    plain_v = None
-    if not args.skip_plain:
-        for _ in range(args.warmup):
-            for c in plain:
-                c.step(dt)
-        pms = 0.0
-        for _ in range(args.batch_steps):
-            for c in plain:
-                pms += c.step(dt)["step_ms"]
-        plain_v = replicas.aggregate_rate(rows * args.batch_steps, pms / 1000.0)
-    for c in cloths + plain:
+    for c in cloths:
         c.close()
     batch.close()
+    # the plain single-instance path on the same cloths, the same steps from
+    # rest: each cloth alone, once with the per-iteration launches in a graph
+    # loop and once with the fused persistent CG; each cloth counts at the
+    # faster of the two
+    plain_v, plain_by = None, {}
+    if not args.skip_plain:
+        per = []
+        for strategy in ("launches", "fused"):
+            plain = [b3g.Cloth(sc.mesh, sc.cdef, device=dev).setup(sc, opts) for sc in scenes]
+            t = np.zeros(len(plain))
+            for k, c in enumerate(plain):
+                if strategy == "fused":
+                    c.set_cg_strategy(True, fused=True)
+                for _ in range(args.warmup):
+                    c.step(dt)
+                for _ in range(args.batch_steps):
+                    t[k] += c.step(dt)["step_ms"]
+                c.close()
+            per.append(t)
+            plain_by[strategy] = replicas.aggregate_rate(rows * args.batch_steps, float(t.sum()) / 1000.0)
+        best = np.minimum(per[0], per[1])
+        plain_v = replicas.aggregate_rate(rows * args.batch_steps, float(best.sum()) / 1000.0)
     return {"cloths": int(replicas.sum_over_ranks(len(scenes))), "vertices": int(replicas.sum_over_ranks(rows)),
             "vertex_steps_per_s": batched,
             "ms_per_step": sum(ms) / len(ms), "plain_vertex_steps_per_s": plain_v,
+            "plain_by_strategy": plain_by,
+            "plain": "each cloth alone, at the faster of per-iteration launches and the fused persistent CG",
             "speedup_vs_plain": batched / plain_v if plain_v else None, "cg_iterations_mean": float(np.mean(iters)),
             "schedule": {"cluster": sched["cluster"],
                          "split_size_classes": [k for k, v in enumerate(sched["split_class"]) if v]},
@@ -565,7 +674,10 @@ def run_colliders(args, dev: int, cpu_sample: bool):
 def run_serving(args, dev: int):
     from bounce_b200 import serving
 
-    return serving.run_poisson(rate=2000.0, seconds=args.serve_seconds, budget_bytes=150 * 10**9, device=dev)
+    # the offered load exceeds one GPU's capacity: the stream is served for its
+    # 30 s and a 5 s drain, and requests still queued then are reported
+    return serving.run_poisson(rate=2000.0, seconds=args.serve_seconds, budget_bytes=150 * 10**9, device=dev,
+                               drain_limit_s=5.0)
 
 
 def _reference_worker(job):
@@ -659,6 +771,28 @@ def cpu_batch_sample(count: int, every: int = 8, steps: int = 2, procs: int = 0)
                       f"(one per host core); slowest process {slowest:.2f} s"}
 
 
+def summary(line: dict) -> dict:
+    """The section headlines, repeated compactly at the end of the line."""
+    def g(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict):
+                return None
+            d = d.get(k)
+        return round(d, 4) if isinstance(d, float) else d
+
+    b, s, st = line.get("batched"), line.get("serving"), line.get("stiff1024")
+    return {
+        "headline_vertex_steps_per_s": g(line, "value"), "headline_e2e": g(line, "e2e", "value"),
+        "headline_frac": g(line, "roofline", "frac"), "headline_fp64_rel_dv_error": g(line, "fp64", "rel_dv_error"),
+        "batched_vertex_steps_per_s": g(b, "vertex_steps_per_s"), "batched_speedup_vs_plain": g(b, "speedup_vs_plain"),
+        "batched_frac": g(b, "roofline", "frac"),
+        "serving_vertex_steps_per_s": g(s, "vertex_steps_per_s"), "serving_tick_p50_ms": g(s, "p50_step_ms"),
+        "serving_tick_p99_ms": g(s, "p99_step_ms"), "serving_busy": g(s, "device_busy_fraction"),
+        "serving_seconds_offered": g(s, "seconds_offered"),
+        "stiff1024_vertex_steps_per_s": g(st, "vertex_steps_per_s"), "stiff1024_frac": g(st, "roofline", "frac"),
+    }
+
+
 def host_cpu():
     try:
         with open("/proc/cpuinfo") as f:
@@ -714,6 +848,7 @@ def main():
     batched = None if args.skip_batch else run_batched(args, local, rank == 0 and world == 1
                                                          and not args.no_cpu_baseline)
     served = None if args.skip_serve else run_serving(args, local)
+    stiff = None if args.skip_stiff else run_stiff(args, local)
     soft = None if args.skip_softbody else run_softbody(args, local, rank == 0 and world == 1
                                                          and not args.no_cpu_baseline)
     selfc = None if args.skip_self else run_self_collision(args, local, rank == 0 and world == 1
@@ -754,12 +889,15 @@ def main():
         "roofline": r["roofline"],
         "kernel_ms": r["kernel_ms"],
         "cpu_baseline": base,
+        "fp64": r["fp64"],
         "batched": batched,
         "serving": served,
+        "stiff1024": stiff,
         "softbody": soft,
         "self_collision": selfc,
         "colliders": colliders,
     }
+    line["summary"] = summary(line)
     print(json.dumps(line))
 
 

@@ -158,6 +158,10 @@ def lib() -> C.CDLL:
             "b3g_particle_get_mass": [vp, u32, C.POINTER(f32)],
             "b3g_particle_apply_force": [vp, u32, vp],
             "b3g_particle_apply_translation": [vp, u32, vp],
+            "b3g_particle_set_radius": [vp, u32, f32],
+            "b3g_particle_get_radius": [vp, u32, C.POINTER(f32)],
+            "b3g_particle_set_friction": [vp, u32, f32],
+            "b3g_particle_get_friction": [vp, u32, C.POINTER(f32)],
             "b3g_cloth_set_types": [vp, vp],
             "b3g_cloth_apply_forces": [vp, vp],
             "b3g_cloth_apply_translations": [vp, vp],
@@ -318,6 +322,22 @@ class Particle:
     def apply_translation(self, t) -> None:
         t3 = _f3(t)
         check(lib().b3g_particle_apply_translation(self.cloth.h, self.vertex, _ptr(t3)), "apply_translation")
+
+    def set_radius(self, r: float) -> None:
+        check(lib().b3g_particle_set_radius(self.cloth.h, self.vertex, r), "set_radius")
+
+    def get_radius(self) -> float:
+        out = C.c_float(0.0)
+        check(lib().b3g_particle_get_radius(self.cloth.h, self.vertex, C.byref(out)), "get_radius")
+        return float(out.value)
+
+    def set_friction(self, f: float) -> None:
+        check(lib().b3g_particle_set_friction(self.cloth.h, self.vertex, f), "set_friction")
+
+    def get_friction(self) -> float:
+        out = C.c_float(0.0)
+        check(lib().b3g_particle_get_friction(self.cloth.h, self.vertex, C.byref(out)), "get_friction")
+        return float(out.value)
 
 
 class Cloth:

@@ -341,6 +341,7 @@ b3g_status layout_cloth(b3g_cloth* c)
     add((size_t)nmouse * 16 + 16); add((size_t)nmouse * 32 + 32);  // mouse forces
     for (int k = 0; k < 13; ++k) add(vec);  // x v fext y mx b dv r p s pinv z p2
     add((size_t)n * 4); add(n);             // mass, type
+    add((size_t)n * 4); add((size_t)n * 4); // particle radius, friction
     add(vec); add(vec);                     // fat lo / hi
     const size_t nn = (size_t)kMaxSpheres * n;
     add(nn); add(nn); add(nn * 4); add(nn * 12); add(nn * 12); add(nn * 12); add(nn * 12); add(nn * 12);
@@ -392,6 +393,9 @@ b3g_status layout_cloth(b3g_cloth* c)
             im->hi[(size_t)q * n + i] = (x + r) + 0.2f;
         }
     im->types.assign(n, (uint8_t)B3G_DYNAMIC);
+    // every particle starts with the cloth's thickness and friction (cloth.cpp:116-117)
+    im->radius.assign(n, def->thickness);
+    im->friction.assign(n, def->friction);
     c->images.reset(im);
     return B3G_OK;
 }
@@ -444,6 +448,8 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     d.p2 = A.take<float>(3 * (size_t)n);
     float* mass = A.take<float>(n);
     d.type = A.take<uint8_t>(n);
+    d.p_radius = A.take<float>(n);
+    d.p_friction = A.take<float>(n);
     d.fat_lo = A.take<float>(3 * (size_t)n);
     d.fat_hi = A.take<float>(3 * (size_t)n);
     d.c_exists = A.take<uint8_t>(nn);
@@ -509,6 +515,8 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     up(d.x, im.x.data(), vec);
     up(mass, T.mass.data(), (size_t)n * 4);
     up(d.type, im.types.data(), n);
+    up(d.p_radius, im.radius.data(), (size_t)n * 4);
+    up(d.p_friction, im.friction.data(), (size_t)n * 4);
     up(d.fat_lo, im.lo.data(), vec);
     up(d.fat_hi, im.hi.data(), vec);
     if (e != cudaSuccess) return from_cuda(e);
@@ -753,7 +761,7 @@ namespace {
 // Every per-particle device array of a cloth, on the host (SoA planes).
 struct ParticleState {
     uint32_t n = 0, nsph = 0;
-    std::vector<float> x, v, fext, y, mx, lo, hi, mass;
+    std::vector<float> x, v, fext, y, mx, lo, hi, mass, radius, friction;
     std::vector<uint8_t> type, c_exists, c_active;
     std::vector<uint32_t> c_key;
     std::vector<float> c_normal, c_t1, c_t2, c_imp, c_point;
@@ -780,6 +788,8 @@ b3g_status download_state(b3g_cloth* c, ParticleState& s)
     B3G_TRY(get(s.hi, d.fat_hi, 3 * n));
     B3G_TRY(get(s.mass, d.mass, n));
     B3G_TRY(get(s.type, d.type, n));
+    B3G_TRY(get(s.radius, d.p_radius, n));
+    B3G_TRY(get(s.friction, d.p_friction, n));
     B3G_TRY(get(s.c_exists, d.c_exists, nn));
     B3G_TRY(get(s.c_active, d.c_active, nn));
     B3G_TRY(get(s.c_key, d.c_key, nn));
@@ -810,6 +820,8 @@ b3g_status upload_state(b3g_cloth* c, const ParticleState& s)
     B3G_TRY(put(d.fat_hi, s.hi, 3 * n));
     B3G_TRY(put(const_cast<float*>(d.mass), s.mass, n));
     B3G_TRY(put(d.type, s.type, n));
+    B3G_TRY(put(d.p_radius, s.radius, n));
+    B3G_TRY(put(d.p_friction, s.friction, n));
     B3G_TRY(put(d.c_exists, s.c_exists, nn));
     B3G_TRY(put(d.c_active, s.c_active, nn));
     B3G_TRY(put(d.c_key, s.c_key, nn));
@@ -854,6 +866,8 @@ ParticleState remap(const ParticleState& s, const std::vector<uint32_t>& keep)
     planes(s.hi, r.hi, n0, n1, 1);
     column(s.mass, r.mass, 1);
     column(s.type, r.type, 1);
+    column(s.radius, r.radius, 1);
+    column(s.friction, r.friction, 1);
     column(s.c_exists, r.c_exists, s.nsph);
     column(s.c_active, r.c_active, s.nsph);
     column(s.c_key, r.c_key, s.nsph);
@@ -932,11 +946,10 @@ b3g_status b3g_cloth_create_particle(b3g_cloth* c, const b3g_particle_def* def, 
     for (int q = 0; q < 3; ++q)
         if (!std::isfinite(def->position[q]) || !std::isfinite(def->velocity[q]) || !std::isfinite(def->force[q]))
             return B3G_ERR_INVALID_ARGUMENT;
-    if (!(def->mass >= 0.0f) || !std::isfinite(def->mass) || !(def->radius >= 0.0f)) return B3G_ERR_INVALID_ARGUMENT;
-    const bool dynamic = def->mass != 0.0f;
-    // a created dynamic particle meets colliders with the cloth's thickness and friction
-    if (dynamic && (def->radius != c->in_def.thickness || def->friction != c->in_def.friction))
+    if (!(def->mass >= 0.0f) || !std::isfinite(def->mass) || !(def->radius >= 0.0f) || !std::isfinite(def->radius) ||
+        !(def->friction >= 0.0f) || !std::isfinite(def->friction))
         return B3G_ERR_INVALID_ARGUMENT;
+    const bool dynamic = def->mass != 0.0f;
     cudaSetDevice(c->device);
     b3g_status st = flush_ops(c);
     if (st != B3G_OK) return st;
@@ -958,6 +971,8 @@ b3g_status b3g_cloth_create_particle(b3g_cloth* c, const b3g_particle_def* def, 
         r.hi[q * (size_t)n1 + i] = (p + def->radius) + 0.2f;
     }
     r.mass[i] = dynamic ? def->mass : 1.0f;
+    r.radius[i] = def->radius;
+    r.friction[i] = def->friction;
     r.type[i] = (uint8_t)(dynamic ? B3G_DYNAMIC : B3G_STATIC);
     const uint32_t old_extra = c->n_extra;
     c->n_extra += 1;
@@ -1087,6 +1102,43 @@ b3g_status b3g_particle_apply_translation(b3g_cloth* c, uint32_t vertex, const f
 {
     if (!t) return B3G_ERR_INVALID_ARGUMENT;
     return push_op(c, vertex, OP_APPLY_TRANSLATION, t);
+}
+
+b3g_status b3g_particle_set_radius(b3g_cloth* c, uint32_t vertex, float radius)
+{
+    if (!(radius >= 0.0f) || !std::isfinite(radius)) return B3G_ERR_INVALID_ARGUMENT;
+    const float a[3] = {radius, 0.0f, 0.0f};
+    return push_op(c, vertex, OP_SET_RADIUS, a);
+}
+
+b3g_status b3g_particle_set_friction(b3g_cloth* c, uint32_t vertex, float friction)
+{
+    if (!(friction >= 0.0f) || !std::isfinite(friction)) return B3G_ERR_INVALID_ARGUMENT;
+    const float a[3] = {friction, 0.0f, 0.0f};
+    return push_op(c, vertex, OP_SET_FRICTION, a);
+}
+
+// One float of a per-particle plane, after the queued edits.
+static b3g_status read_scalar(const b3g_cloth* cc, uint32_t vertex, const float* plane, float* out)
+{
+    b3g_cloth* c = const_cast<b3g_cloth*>(cc);
+    if (!valid(c) || vertex >= c->dev.n || !out) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    b3g_status s = flush_ops(c);
+    if (s != B3G_OK) return s;
+    B3G_TRY(cudaMemcpyAsync(out, plane + vertex, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    return B3G_OK;
+}
+
+b3g_status b3g_particle_get_radius(const b3g_cloth* c, uint32_t vertex, float* radius)
+{
+    return valid(c) ? read_scalar(c, vertex, c->dev.p_radius, radius) : B3G_ERR_INVALID_ARGUMENT;
+}
+
+b3g_status b3g_particle_get_friction(const b3g_cloth* c, uint32_t vertex, float* friction)
+{
+    return valid(c) ? read_scalar(c, vertex, c->dev.p_friction, friction) : B3G_ERR_INVALID_ARGUMENT;
 }
 
 static b3g_status read_vertex(const b3g_cloth* cc, uint32_t vertex, const float* planes, float out[3])

@@ -94,7 +94,8 @@ struct ClothDev {
     uint32_t nmouse;
 
     float k_stretch, k_shear, k_damp;
-    float thickness, friction;  // particle radius and friction (b3ClothDef)
+    float thickness, friction;  // the triangles' radius and friction (b3ClothDef, cloth.cpp:136-137)
+    float *p_radius, *p_friction;  // per particle (b3Particle::m_radius, m_friction), n each
 
     float *x, *v, *fext, *y, *mx;
     const float* mass;
@@ -189,7 +190,15 @@ struct ParticleOp {
     uint32_t vertex, kind;
     float a[3];
 };
-enum { OP_SET_TYPE = 0, OP_SET_POSITION = 1, OP_SET_VELOCITY = 2, OP_APPLY_FORCE = 3, OP_APPLY_TRANSLATION = 4 };
+enum {
+    OP_SET_TYPE = 0,
+    OP_SET_POSITION = 1,
+    OP_SET_VELOCITY = 2,
+    OP_APPLY_FORCE = 3,
+    OP_APPLY_TRANSLATION = 4,
+    OP_SET_RADIUS = 5,
+    OP_SET_FRICTION = 6
+};
 cudaError_t launch_particle_ops(const ClothDev& c, const ParticleOp* ops, uint32_t count, cudaStream_t st);
 cudaError_t launch_set_types(const ClothDev& c, const uint8_t* types, cudaStream_t st);
 cudaError_t launch_add_vectors(const ClothDev& c, float* dst_planes, const float* src_xyz, int only_dynamic,

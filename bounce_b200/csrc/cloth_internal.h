@@ -35,6 +35,7 @@ struct HostImages {
     std::vector<float4> sp;
     std::vector<float> x, lo, hi;
     std::vector<uint8_t> types;
+    std::vector<float> radius, friction;
     std::vector<uint4> mouse_v;
     std::vector<float4> mouse_par;
 };

@@ -689,7 +689,7 @@ __global__ void k_contacts_update(const __grid_constant__ ClothDev one, const __
             c.c_active[q] = 0;
             continue;
         }
-        const float radius = sp.radius + c.thickness;
+        const float radius = sp.radius + c.p_radius[i];
         f3 normal;
         if (sp.kind == 0) {
             // b3SphereShape::TestSphere (sphere_shape.cpp:71-95)
@@ -777,7 +777,7 @@ __global__ void k_hull_contacts_update(const __grid_constant__ ClothDev one, con
             c.c_active[q] = 0;
             continue;
         }
-        const float radius = sp.radius + c.thickness;
+        const float radius = sp.radius + c.p_radius[i];
         f3 normal, P;
         if (!hull::test_sphere(sp.hull, sp.nhv, sp.hull + 3 * sp.nhv, sp.nhf, radius, xi, normal, P)) {
             c.c_active[q] = 0;
@@ -828,7 +828,7 @@ __device__ float position_iteration(const ClothDev& c, uint32_t i, f3& pos, cons
         const SphereDev& sp = c.sph[s];
         const f3 nA = ld3(c.c_normal, nn, s * n + i);
         const f3 cB = sp.kind == 0 ? mk(sp.cx, sp.cy, sp.cz) : ld3(c.c_point, nn, s * n + i);
-        const float separation = dot(cB - pos, nA) - c.thickness - sp.radius;
+        const float separation = dot(cB - pos, nA) - c.p_radius[i] - sp.radius;
         min_sep = min_sep < separation ? min_sep : separation;
         const float Cv = kBaumgarte * (separation + kLinearSlop);
         float C = Cv < 0.0f ? Cv : 0.0f;
@@ -881,7 +881,7 @@ __global__ void k_finalize(const __grid_constant__ ClothDev one, const __grid_co
                 tm_yx[a] = -det * k12;
                 tm_xy[a] = -det * k12;
                 tm_yy[a] = det * k11;
-                fr[a] = sqrtf(c.friction * c.sph[s].friction);
+                fr[a] = sqrtf(c.p_friction[i] * c.sph[s].friction);
                 ni[a] = c.c_imp[q];
                 tix[a] = c.c_imp[nn + q];
                 tiy[a] = c.c_imp[2 * nn + q];
@@ -985,7 +985,7 @@ __device__ void move_proxy_dev(const ClothDev& c, uint32_t i, f3 disp)
     const f3 x = ld3(c.x, n, i);
     float lo[3], hi[3];
     load_fat(c, i, lo, hi);
-    const float r = c.thickness;
+    const float r = c.p_radius[i];
     float tlo[3] = {x.x - r, x.y - r, x.z - r}, thi[3] = {x.x + r, x.y + r, x.z + r};
     bool contains = true;
     for (int d = 0; d < 3; ++d)
@@ -1168,6 +1168,13 @@ __global__ void k_particle_ops(ClothDev c, const ParticleOp* ops, uint32_t count
                 break;
             case OP_APPLY_TRANSLATION:  // particle.h:269-272
                 st3(c.y, n, i, ld3(c.y, n, i) + a);
+                break;
+            case OP_SET_RADIUS:  // particle.h:240-245: the radius, then Synchronize(0)
+                c.p_radius[i] = op.a[0];
+                move_proxy_dev(c, i, zero3());
+                break;
+            case OP_SET_FRICTION:  // particle.h:252-255
+                c.p_friction[i] = op.a[0];
                 break;
         }
     }

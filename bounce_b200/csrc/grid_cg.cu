@@ -27,6 +27,7 @@ namespace {
 constexpr int kMaxBlock = 512;
 constexpr int kMaxWarps = kMaxBlock / 32;
 constexpr int kPrefetch = 16;  // partials per lane loaded together (up to 512 CTAs)
+constexpr int kPrefetchFused = 6;  // the fused form's 32-byte partials: up to 192 CTAs
 constexpr uint64_t kSpinLimit = 1ull << 26;
 constexpr uint32_t kStatusTimeout = 7;
 
@@ -134,11 +135,10 @@ __device__ bool grid_sync(GridBarrier* b, uint32_t nblocks, uint32_t& epoch)
 // the same partials in the same order (lane l takes CTAs l, l + 32, ... in
 // order, then a fixed shuffle tree), so all agree without another barrier.
 // A lane's partials are loaded together before they are summed.
-template <int DOT, int NV>
-__device__ bool grid_total(typename DotT<DOT>::T (&v)[NV], typename DotT<DOT>::T* part, GridBarrier* bar,
-                           uint32_t nblocks, uint32_t& epoch)
+template <class D, int NV, int PF = kPrefetch>
+__device__ bool grid_total_of(typename D::T (&v)[NV], typename D::T* part, GridBarrier* bar, uint32_t nblocks,
+                              uint32_t& epoch)
 {
-    typedef DotT<DOT> D;
     typedef typename D::T T;
     __shared__ T wsum[NV][kMaxWarps];
     __shared__ T tot[NV];
@@ -163,17 +163,17 @@ __device__ bool grid_total(typename DotT<DOT>::T (&v)[NV], typename DotT<DOT>::T
     if (warp == 0) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
-            T buf[kPrefetch];
+            T buf[PF];
 #pragma unroll
-            for (int m = 0; m < kPrefetch; ++m) {
+            for (int m = 0; m < PF; ++m) {
                 const uint32_t b = lane + 32u * m;
                 buf[m] = b < nblocks ? D::load(part + b * NV + k) : D::zero();
             }
             T a = D::zero();
 #pragma unroll
-            for (int m = 0; m < kPrefetch; ++m)
+            for (int m = 0; m < PF; ++m)
                 if (lane + 32u * m < nblocks) a = D::combine(a, buf[m]);
-            for (uint32_t b = lane + 32u * kPrefetch; b < nblocks; b += 32) a = D::combine(a, D::load(part + b * NV + k));
+            for (uint32_t b = lane + 32u * PF; b < nblocks; b += 32) a = D::combine(a, D::load(part + b * NV + k));
             for (int off = 16; off > 0; off >>= 1) a = D::combine(a, D::shfl(a, off));
             if (lane == 0) tot[k] = a;
         }
@@ -182,6 +182,13 @@ __device__ bool grid_total(typename DotT<DOT>::T (&v)[NV], typename DotT<DOT>::T
 #pragma unroll
     for (int k = 0; k < NV; ++k) v[k] = tot[k];
     return true;
+}
+
+template <int DOT, int NV>
+__device__ __forceinline__ bool grid_total(typename DotT<DOT>::T (&v)[NV], typename DotT<DOT>::T* part,
+                                           GridBarrier* bar, uint32_t nblocks, uint32_t& epoch)
+{
+    return grid_total_of<DotT<DOT>, NV>(v, part, bar, nblocks, epoch);
 }
 
 // The row of a one-row thread, kept in registers for the whole solve: its
@@ -451,6 +458,43 @@ __device__ __forceinline__ f3 rec_direction(const Rec& q, float alpha, float bet
     return hadamard(rn, q.sp) + beta * q.p;
 }
 
+// The four sums of a fused pass, reduced together: p.s and r.z in the
+// solve's dot precision (they give alpha and the exact delta, as the
+// reference's float32 b3Dot would), s.z and s.P^-1 s always in FP64.  The
+// latter two only enter the expanded next delta, whose terms cancel; summed
+// in FP32 their rounding would be magnified into beta.
+template <int DOT>
+struct FusedSums {
+    typedef DotT<DOT> P;
+    struct T {
+        typename P::T ps, rz;
+        double sz, sps;
+    };
+    static __device__ T zero() { return T{P::zero(), P::zero(), 0.0, 0.0}; }
+    static __device__ T combine(T a, T b)
+    {
+        return T{P::combine(a.ps, b.ps), P::combine(a.rz, b.rz), a.sz + b.sz, a.sps + b.sps};
+    }
+    static __device__ T shfl(T a, int off)
+    {
+        return T{P::shfl(a.ps, off), P::shfl(a.rz, off), __shfl_down_sync(0xffffffffu, a.sz, off),
+                 __shfl_down_sync(0xffffffffu, a.sps, off)};
+    }
+    static __device__ T load(const T* p) { return T{P::load(&p->ps), P::load(&p->rz), __ldcg(&p->sz), __ldcg(&p->sps)}; }
+    static __device__ double dot64(f3 a, f3 b)
+    {
+        return (double)a.x * (double)b.x + (double)a.y * (double)b.y + (double)a.z * (double)b.z;
+    }
+    static __device__ void add(T& acc, f3 p, f3 s, f3 z, f3 r, f3 sp)
+    {
+        acc.ps = P::add_term(acc.ps, p, s);
+        acc.rz = P::add_term(acc.rz, r, z);
+        acc.sz += dot64(s, z);
+        acc.sps += dot64(s, hadamard(s, sp));
+    }
+};
+static_assert(sizeof(FusedSums<1>::T) <= 32, "fused partials: 32 bytes per CTA and parity");
+
 // The scalars of one pass from its four sums.  Returns false when the true
 // delta of the iterate (r.z) already meets the stop rule: the pass is then
 // discarded.  DOT 0 and 1 round every scalar to float, as the reference's
@@ -486,8 +530,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
     const uint32_t nb = gridDim.x;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t first_row = blockIdx.x * blockDim.x + threadIdx.x;
-    T* part0 = reinterpret_cast<T*>(c.partials);
-    T* part1 = part0 + 4 * nb;
+    typedef FusedSums<DOT> F;
+    typedef typename F::T FT;
+    T* part_init = reinterpret_cast<T*>(c.partials);
+    FT* part0 = reinterpret_cast<FT*>(c.partials);
+    FT* part1 = part0 + nb;
     const uint32_t max_iter = sc->max_iter;
     uint32_t epoch = 0;
 
@@ -539,7 +586,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
         v2[1] = D::add_term(v2[1], rv, zv);
         if (ONE_ROW) break;
     }
-    if (!grid_total<DOT, 2>(v2, part0, bar, nb, epoch)) goto timeout;
+    if (!grid_total<DOT, 2>(v2, part_init, bar, nb, epoch)) goto timeout;
     {
         double b_delta = D::value(v2[0]), delta = D::value(v2[1]);
         if (DOT != 2) {
@@ -556,7 +603,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
             const bool first = it == 0;
             const float4* rin = (it & 1u) ? rec1 : rec0;
             float4* rout = (it & 1u) ? rec0 : rec1;
-            T v4[4] = {D::zero(), D::zero(), D::zero(), D::zero()};
+            FT v4[1] = {F::zero()};
             if (ONE_ROW) {
                 if (act) {
                     f3 z;
@@ -581,10 +628,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
                     }
                     s = Si ? acc : zero3();
                     st_rec(rout, first_row, r, s, p, sp);
-                    v4[0] = D::add_term(v4[0], p, s);
-                    v4[1] = D::add_term(v4[1], s, z);
-                    v4[2] = D::add_term(v4[2], s, hadamard(s, sp));
-                    v4[3] = D::add_term(v4[3], r, z);
+                    F::add(v4[0], p, s, z, r, sp);
                 }
             } else {
                 for (uint32_t row = first_row; row < n; row += stride) {
@@ -615,17 +659,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
                     }
                     const f3 sv = dyn(c, row) ? acc : zero3();
                     st_rec(rout, row, rv, sv, pv, own.sp);
-                    v4[0] = D::add_term(v4[0], pv, sv);
-                    v4[1] = D::add_term(v4[1], sv, z);
-                    v4[2] = D::add_term(v4[2], sv, hadamard(sv, own.sp));
-                    v4[3] = D::add_term(v4[3], rv, z);
+                    F::add(v4[0], pv, sv, z, rv, own.sp);
                 }
             }
-            if (!grid_total<DOT, 4>(v4, (it & 1u) ? part0 : part1, bar, nb, epoch)) goto timeout;
+            if (!grid_total_of<F, 1, kPrefetchFused>(v4, (it & 1u) ? part0 : part1, bar, nb, epoch)) goto timeout;
             double dn = 0.0, dt = 0.0;
             float a1 = 0.0f, b1 = 0.0f;
-            const bool accept = fused_scalars<DOT>(sc, D::value(v4[0]), D::value(v4[1]), D::value(v4[2]),
-                                                   D::value(v4[3]), b_delta, a1, b1, dn, dt);
+            const bool accept = fused_scalars<DOT>(sc, D::value(v4[0].ps), v4[0].sz, v4[0].sps, D::value(v4[0].rz),
+                                                   b_delta, a1, b1, dn, dt);
             if (!accept) {
                 // the iterate already meets the stop rule: the reference stops
                 // before this pass; its x is the current one

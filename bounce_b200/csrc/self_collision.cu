@@ -135,7 +135,7 @@ __device__ bool contact_update(const ClothDev& c, uint32_t p, uint4 tv, float4& 
     f3 N = cross(B - A, C - A);
     const float len = normalize(N);
     if (len == 0.0f) return false;
-    const float total = c.thickness + c.thickness;  // particle radius + triangle radius
+    const float total = c.p_radius[p] + c.thickness;  // particle radius + triangle radius
     const f3 P1 = ld3(c.x, n, p);
     const float distance = dot(N, P1 - A);
     if (distance < -total) return false;
@@ -272,7 +272,7 @@ __device__ void body_velocity(const ClothDev& c, uint32_t i, const int* order, i
         float det = k11 * k22 - k12 * k12;
         if (det != 0.0f) det = 1.0f / det;
         const float tm_xx = det * k22, tm_yx = -det * k12, tm_xy = -det * k12, tm_yy = det * k11;
-        const float fr = sqrtf(c.friction * c.sph[sidx].friction);
+        const float fr = sqrtf(c.p_friction[i] * c.sph[sidx].friction);
         float ni = c.c_imp[q], tix = c.c_imp[nn + q], tiy = c.c_imp[2 * nn + q];
         const f3 nrm = ld3(c.c_normal, nn, q), t1 = ld3(c.c_t1, nn, q), t2 = ld3(c.c_t2, nn, q);
         {
@@ -329,7 +329,7 @@ __device__ float body_position(const ClothDev& c, uint32_t i, const int* order, 
         const SphereDev& sp = c.sph[sidx];
         const f3 nA = ld3(c.c_normal, nn, sidx * n + i);
         const f3 cB = sp.kind == 0 ? mk(sp.cx, sp.cy, sp.cz) : ld3(c.c_point, nn, sidx * n + i);
-        const float separation = dot(cB - pos, nA) - c.thickness - sp.radius;
+        const float separation = dot(cB - pos, nA) - c.p_radius[i] - sp.radius;
         min_sep = min_sep < separation ? min_sep : separation;
         const float Cv = kBaum * (separation + kSlop);
         float C = Cv < 0.0f ? Cv : 0.0f;
@@ -357,8 +357,8 @@ __device__ void tri_init(const ClothDev& c, TriCon& x, uint2 key, float4 w, floa
     const uint4 tv = c.tri[key.y];
     x.ia = key.x; x.ib = tv.x; x.ic = tv.y; x.id = tv.z;
     x.mA = inv_mass(c, x.ia); x.mB = inv_mass(c, x.ib); x.mC = inv_mass(c, x.ic); x.mD = inv_mass(c, x.id);
-    x.radius_a = c.thickness;
-    x.radius_t = c.thickness;
+    x.radius_a = c.p_radius[x.ia];
+    x.radius_t = c.thickness;  // the triangle's radius (cloth.cpp:136)
     x.wB = w.x; x.wC = w.y; x.wD = w.z;
     const f3 xA = ld3(c.x, n, x.ia), xB = ld3(c.x, n, x.ib), xC = ld3(c.x, n, x.ic), xD = ld3(c.x, n, x.id);
     const f3 cB = (x.wB * xB + x.wC * xC) + x.wD * xD;
@@ -367,7 +367,7 @@ __device__ void tri_init(const ClothDev& c, TriCon& x, uint2 key, float4 w, floa
     x.nx = nrm.x; x.ny = nrm.y; x.nz = nrm.z;
     const float K = ((x.mA + x.mB * x.wB * x.wB) + x.mC * x.wC * x.wC) + x.mD * x.wD * x.wD;
     x.normal_mass = K > 0.0f ? 1.0f / K : 0.0f;
-    x.friction = sqrtf(c.friction * c.friction);  // b3MixFriction(particle, triangle)
+    x.friction = sqrtf(c.p_friction[x.ia] * c.friction);  // b3MixFriction(particle, triangle)
     const f3 t1 = perp(nrm), t2 = cross(t1, nrm);
     x.t1x = t1.x; x.t1y = t1.y; x.t1z = t1.z;
     x.t2x = t2.x; x.t2y = t2.y; x.t2z = t2.z;

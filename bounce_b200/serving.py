@@ -71,7 +71,8 @@ def run_poisson(rate: float = 2000.0, seconds: float = 30.0, side_lo: int = 8, s
         "requests": nreq, "completed": int(st["completed"]), "rejected": int(st["rejected"]),
         "seconds_offered": seconds, "wall_s": wall, "ticks": int(st["ticks"]),
         "vertex_steps": int(st["vertex_steps"]), "vertex_steps_per_s": st["vertex_steps"] / wall,
-        "device_busy_s": st["busy_ms"] / 1000.0,
+        "device_busy_s": st["busy_ms"] / 1000.0, "device_busy_fraction": st["busy_ms"] / 1000.0 / wall,
+        "unfinished": nreq - int(st["completed"]) - int(st["rejected"]),
         "p50_step_ms": st["p50_step_ms"], "p99_step_ms": st["p99_step_ms"], "max_step_ms": st["max_step_ms"],
         "p50_request_s": float(np.percentile(lat, 50)), "p99_request_s": float(np.percentile(lat, 99)),
         "peak_active": int(st["peak_active"]), "peak_bytes": int(st["peak_bytes"]),

@@ -133,9 +133,8 @@ b3g_status b3g_cloth_clear_colliders(b3g_cloth* cloth);
 /* ---- created particles and mouse forces ------------------------------------ */
 
 /* b3ParticleDef (include/bounce/cloth/particle.h:38-60).  mass 0 makes a
- * static particle (of mass 1, particle.cpp:34-39).  A created dynamic
- * particle must use the cloth's thickness and friction as its radius and
- * friction (colliders see every particle with those). */
+ * static particle (of mass 1, particle.cpp:34-39).  radius and friction are
+ * the particle's own (b3g_particle_set_radius). */
 typedef struct {
     float position[3];
     float velocity[3];
@@ -181,6 +180,20 @@ b3g_status b3g_particle_get_velocity(const b3g_cloth* cloth, uint32_t vertex, fl
 b3g_status b3g_particle_get_mass(const b3g_cloth* cloth, uint32_t vertex, float* mass);
 b3g_status b3g_particle_apply_force(b3g_cloth* cloth, uint32_t vertex, const float force[3]);
 b3g_status b3g_particle_apply_translation(b3g_cloth* cloth, uint32_t vertex, const float translation[3]);
+/* b3Particle::SetRadius / GetRadius, SetFriction / GetFriction (particle.h:
+ * 93-102, 240-260).  A particle starts with the cloth's thickness and
+ * friction.  The radius enters its body contacts (b3ParticleBodyContact::
+ * Update, cloth_particle_body_contact.cpp:24-47, and the position solve) and
+ * its proxy, which SetRadius moves (Synchronize(0)); the friction enters
+ * b3MixFriction with the shape's.  On a cloth created with thickness > 0 both
+ * also enter its particle-triangle contacts.  A cloth created with thickness
+ * 0 runs no particle-triangle contacts at all, even when a particle's radius
+ * is set above 0 (the reference would then test them).  Radius and friction
+ * must be finite and >= 0. */
+b3g_status b3g_particle_set_radius(b3g_cloth* cloth, uint32_t vertex, float radius);
+b3g_status b3g_particle_get_radius(const b3g_cloth* cloth, uint32_t vertex, float* radius);
+b3g_status b3g_particle_set_friction(b3g_cloth* cloth, uint32_t vertex, float friction);
+b3g_status b3g_particle_get_friction(const b3g_cloth* cloth, uint32_t vertex, float* friction);
 
 /* Whole-cloth forms of the particle calls: arrays of 3 * vertex_count floats
  * (xyz per vertex) or vertex_count types, host memory. */

@@ -51,6 +51,20 @@ public:
     {
         b3gCheck(b3g_particle_apply_translation(m_cloth, m_vertex, t), "ApplyTranslation");
     }
+    void SetRadius(float r) { b3gCheck(b3g_particle_set_radius(m_cloth, m_vertex, r), "SetRadius"); }
+    float GetRadius() const
+    {
+        float r;
+        b3gCheck(b3g_particle_get_radius(m_cloth, m_vertex, &r), "GetRadius");
+        return r;
+    }
+    void SetFriction(float f) { b3gCheck(b3g_particle_set_friction(m_cloth, m_vertex, f), "SetFriction"); }
+    float GetFriction() const
+    {
+        float f;
+        b3gCheck(b3g_particle_get_friction(m_cloth, m_vertex, &f), "GetFriction");
+        return f;
+    }
 
 private:
     b3g_cloth* m_cloth;

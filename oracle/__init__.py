@@ -30,15 +30,21 @@ _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 
 
+# Root of the reference's source tree (include/ and src/), read only by the
+# build of the reference library below; the environment variable
+# B3G_REFERENCE_DIR overrides the default.
+REFERENCE_DIR = os.environ.get("B3G_REFERENCE_DIR", "/root/reference")
+
+
 def build(port: bool = True, ref: bool = True) -> None:
     """Compile the checkers (the reference part needs its sources on disk)."""
     targets = []
     if port:
         targets.append("port")
-    if ref and os.path.isdir("/root/reference/src"):
+    if ref and os.path.isdir(os.path.join(REFERENCE_DIR, "src")):
         targets.append("ref")
     if targets:
-        subprocess.run(["make", "-s", "-C", HERE, "-j8"] + targets, check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "-j8", f"REF={REFERENCE_DIR}"] + targets, check=True)
 
 
 class _OcStepInfo(C.Structure):
@@ -62,6 +68,8 @@ def port_lib():
         L.oc_destroy.argtypes = [C.c_void_p]
         L.oc_set_gravity.argtypes = [C.c_void_p, _f32p]
         L.oc_set_type.argtypes = [C.c_void_p, C.c_uint32, C.c_int]
+        L.oc_set_radius.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.oc_set_friction.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
         L.oc_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_set_contacts.argtypes = [C.c_void_p, C.c_uint32, _u32p, _u32p, _f32p]
         L.oc_set_proxies.argtypes = [C.c_void_p, _f32p, _f32p]
@@ -126,6 +134,8 @@ def ref_lib():
         L.ref_cloth_destroy.argtypes = [C.c_void_p]
         L.ref_cloth_set_gravity.argtypes = [C.c_void_p, _f32p]
         L.ref_cloth_set_type.argtypes = [C.c_void_p, C.c_uint32, C.c_int]
+        L.ref_cloth_set_radius.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.ref_cloth_set_friction.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
         for name in ("ref_cloth_apply_force", "ref_cloth_apply_translation", "ref_cloth_set_position",
                      "ref_cloth_set_velocity"):
             getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, _f32p]
@@ -295,6 +305,12 @@ class PortCloth(_Base):
     def set_type(self, vertex, ty):
         self.L.oc_set_type(self.h, vertex, ty)
 
+    def set_radius(self, vertex, radius):
+        self.L.oc_set_radius(self.h, vertex, radius)
+
+    def set_friction(self, vertex, friction):
+        self.L.oc_set_friction(self.h, vertex, friction)
+
     def set_state(self, x=None, v=None, dv=None):
         arrs = [None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1) for a in (x, v, dv)]
         self.L.oc_set_state(self.h, *[None if a is None else a.ctypes.data for a in arrs])
@@ -414,6 +430,12 @@ class RefCloth(_Base):
 
     def set_type(self, vertex, ty):
         self.L.ref_cloth_set_type(self.h, vertex, ty)
+
+    def set_radius(self, vertex, radius):
+        self.L.ref_cloth_set_radius(self.h, vertex, radius)
+
+    def set_friction(self, vertex, friction):
+        self.L.ref_cloth_set_friction(self.h, vertex, friction)
 
     def apply_force(self, vertex, f):
         self.L.ref_cloth_apply_force(self.h, vertex, np.asarray(f, np.float32))

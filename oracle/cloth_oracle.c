@@ -633,6 +633,17 @@ void oc_set_type(oc_cloth* c, uint32_t i, int type)
     c->p_moved[i] = 1; /* TouchProxy */
 }
 
+/* b3Particle::SetRadius (particle.h:240-245): the new radius, then
+ * Synchronize(0), which moves the particle's proxy (particle.cpp:58-64). */
+void oc_set_radius(oc_cloth* c, uint32_t i, float radius)
+{
+    c->radius[i] = radius;
+    move_proxy(c, i, vzero());
+}
+
+/* b3Particle::SetFriction (particle.h:252-255) */
+void oc_set_friction(oc_cloth* c, uint32_t i, float friction) { c->friction[i] = friction; }
+
 /* b3Particle::ApplyForce / ApplyTranslation / SetPosition / SetVelocity (particle.h:205-271) */
 void oc_apply_force(oc_cloth* c, uint32_t i, const float* f)
 {

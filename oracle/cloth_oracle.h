@@ -68,6 +68,8 @@ void oc_set_contacts(oc_cloth* c, uint32_t count, const uint32_t* particle, cons
                      const float* impulses);
 void oc_set_proxies(oc_cloth* c, const float* lo, const float* hi);
 void oc_set_type(oc_cloth* c, uint32_t vertex, int type);
+void oc_set_radius(oc_cloth* c, uint32_t vertex, float radius);
+void oc_set_friction(oc_cloth* c, uint32_t vertex, float friction);
 void oc_apply_force(oc_cloth* c, uint32_t vertex, const float* f);
 void oc_apply_translation(oc_cloth* c, uint32_t vertex, const float* t);
 void oc_set_position(oc_cloth* c, uint32_t vertex, const float* x);

@@ -397,6 +397,16 @@ void ref_cloth_set_type(void* hp, uint32_t vertex, int type)
     particle_at((RefCloth*)hp, vertex)->SetType((b3ParticleType)type);
 }
 
+void ref_cloth_set_radius(void* hp, uint32_t vertex, float radius)
+{
+    particle_at((RefCloth*)hp, vertex)->SetRadius(radius);
+}
+
+void ref_cloth_set_friction(void* hp, uint32_t vertex, float friction)
+{
+    particle_at((RefCloth*)hp, vertex)->SetFriction(friction);
+}
+
 void ref_cloth_apply_force(void* hp, uint32_t vertex, const float* f)
 {
     particle_at((RefCloth*)hp, vertex)->ApplyForce(b3Vec3(f[0], f[1], f[2]));

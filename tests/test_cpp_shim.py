@@ -1,5 +1,8 @@
 """The C++ shim (include/b3g_cloth.hpp) compiles against the C ABI and links
-with libb3g.so; without a GPU it reports B3G_ERR_NO_DEVICE through b3gError."""
+with libb3g.so.  Without a GPU it reports B3G_ERR_NO_DEVICE through
+b3gError; on a GPU it steps a cloth through a mouse drag, and its final
+positions equal those of the same sequence run through the Python front-end
+(the same library calls, so bit for bit)."""
 import os
 import subprocess
 
@@ -32,6 +35,11 @@ int main() {
         c.DestroyParticle(mp);
         s = c.Step(1.0f / 60.0f, 8, 2);
         std::printf("stepped %u\n", s.iterations);
+        for (uint32_t i = 0; i < 3; ++i) {
+            float p[3];
+            c.GetParticle(i).GetPosition(p);
+            std::printf("%.9g %.9g %.9g\n", p[0], p[1], p[2]);
+        }
         return 0;
     } catch (const b3gError& e) {
         std::printf("status %d\n", (int)e.status);
@@ -41,17 +49,47 @@ int main() {
 '''
 
 
-def test_shim_compiles_and_runs(b3g, tmp_path):
+def _run_shim(b3g, tmp_path):
     src = tmp_path / "shim.cpp"
     src.write_text(PROG)
     exe = tmp_path / "shim"
     libdir = os.path.dirname(b3g.LIB_PATH)
     subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
                     "-L", libdir, "-lb3g", f"-Wl,-rpath,{libdir}"], check=True)
-    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    return subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+
+
+def test_shim_compiles_and_reports_no_device(b3g, tmp_path):
     import torch
 
     if torch.cuda.is_available():
-        assert r.returncode == 0, r.stdout + r.stderr
-    else:
-        assert r.returncode == 3, r.stdout + r.stderr
+        pytest.skip("a GPU is present: test_shim_steps_a_cloth_on_the_gpu runs the shim")
+    r = _run_shim(b3g, tmp_path)
+    assert r.returncode == 3, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_shim_steps_a_cloth_on_the_gpu(b3g, tmp_path):
+    import numpy as np
+
+    r = _run_shim(b3g, tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines = r.stdout.strip().splitlines()
+    assert lines[0].startswith("stepped")
+    shim_x = np.array([[float(t) for t in ln.split()] for ln in lines[1:4]], np.float32)
+    # the same sequence through the Python front-end
+    mesh = b3g.Mesh(np.array([[0, 0, 0], [1, 0, 0], [0, 0, 1]], np.float32), np.array([[2, 1, 0]], np.uint32))
+    cloth = b3g.Cloth(mesh, b3g.ClothDef(1.0, 1e4, 1e3, 0.0, 0.0, 0.05, 0.0, 0.3))
+    cloth.set_gravity((0.0, -9.8, 0.0))
+    cloth.particle(0).set_type(b3g.STATIC)
+    cloth.step(1.0 / 60.0, 8, 2)
+    mp = cloth.create_particle((0.3, 0.1, 0.3))
+    f = cloth.create_mouse_force(mp, 0, 0.3, 0.3, 0.4, 1000.0, 5.0)
+    cloth.step(1.0 / 60.0, 8, 2)
+    cloth.destroy_force(f)
+    cloth.destroy_particle(mp)
+    cloth.step(1.0 / 60.0, 8, 2)
+    x = cloth.positions()
+    cloth.close()
+    assert np.array_equal(shim_x, x), (shim_x, x)
+    assert not np.array_equal(x[1], mesh.vertices[1])  # it moved

@@ -121,6 +121,58 @@ def test_sphere_contacts_per_step(b3g, port):
     assert seen_active > 100  # the cloth did hit the sphere
 
 
+def test_particle_radius_and_friction_per_step(b3g, port):
+    """Per-particle radius (0-2 cm) and friction (0-1) on the sphere scene,
+    set through b3g_particle_set_radius / _set_friction before the first
+    step and again, for a third of the particles, at step 25 while the cloth
+    lies on the sphere: each step from the GPU's state matches the oracle
+    (CG iterations +-1, active contacts within 1%, x within 1e-4), and the
+    getters return what was set."""
+    scene = b3g.sphere_scene(32)
+    gpu, ora = _pair(b3g, port, scene)
+    n = scene.mesh.vertex_count
+
+    def mixed(seed, frac):
+        rng = np.random.default_rng(seed)
+        last = None
+        for i in range(n):
+            if rng.uniform() < frac:
+                r, f = float(rng.uniform(0.0, 0.02)), float(rng.uniform(0.0, 1.0))
+                gpu.particle(i).set_radius(r)
+                gpu.particle(i).set_friction(f)
+                ora.set_radius(i, r)
+                ora.set_friction(i, f)
+                last = (i, np.float32(r), np.float32(f))
+        return last
+
+    i, r, f = mixed(21, 1.0)
+    assert gpu.particle(i).get_radius() == r and gpu.particle(i).get_friction() == f
+    seen = 0
+    for step in range(50):
+        if step == 25:
+            mixed(22, 0.3)
+        st = gpu.state()
+        ora.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        g = gpu.step(scene.dt)
+        o = ora.step(scene.dt)
+        seen = max(seen, o["active_contacts"])
+        assert abs(g["iterations"] - o["iterations"]) <= 1, step
+        assert abs(int(g["active_contacts"]) - int(o["active_contacts"])) <= max(2, o["active_contacts"] // 100), step
+        assert rel_err(gpu.state()["x"], ora.state()["x"]) <= 1e-4, step
+    assert seen > 100
+
+
+def test_particle_radius_rejects_bad_values(b3g):
+    scene = b3g.plain_scene(8)
+    cloth = b3g.Cloth(scene.mesh, scene.cdef)
+    L = b3g.lib()
+    for bad in (-1.0, float("nan"), float("inf")):
+        assert L.b3g_particle_set_radius(cloth.h, 0, bad) == 1
+        assert L.b3g_particle_set_friction(cloth.h, 0, bad) == 1
+    assert L.b3g_particle_set_radius(cloth.h, 64, 0.1) == 1  # vertex out of range
+    cloth.close()
+
+
 def test_sphere_trajectory_bulk(b3g, port):
     """Free trajectories with contacts: whether a particle touches the sphere
     is a discrete test, so two correct solvers that round differently part

@@ -266,3 +266,42 @@ def test_ray_cast_single_matches_reference():
                 assert a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2])
                 hits += 1
     assert hits > 100
+
+
+def _mixed_radii(cloth, n, seed, frac=1.0):
+    """Per-particle radius (0..2 cm) and friction (0..1) for a random subset."""
+    rng = np.random.default_rng(seed)
+    for i in range(n):
+        if rng.uniform() < frac:
+            cloth.set_radius(i, float(rng.uniform(0.0, 0.02)))
+            cloth.set_friction(i, float(rng.uniform(0.0, 1.0)))
+
+
+def test_particle_radius_and_friction_match_reference():
+    """b3Particle::SetRadius / SetFriction (particle.h:240-255) on the sphere
+    scene: radii of 0-2 cm and frictions of 0-1 before the first step, and a
+    second set at step 25 while the cloth lies on the sphere (SetRadius moves
+    the proxy).  They enter the contact test, the position solve and the
+    friction mix; the restatement follows the reference bit for bit."""
+    scene = sphere_scene(16)
+    ref = oracle.RefCloth(scene.mesh, scene.cdef).setup(scene)
+    port = oracle.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    n = scene.mesh.vertex_count
+    _mixed_radii(ref, n, 11)
+    _mixed_radii(port, n, 11)
+    active = 0
+    for step in range(60):
+        if step == 25:
+            _mixed_radii(ref, n, 12, 0.3)
+            _mixed_radii(port, n, 12, 0.3)
+        assert ref.step(scene.dt)["iterations"] == port.step(scene.dt)["iterations"], step
+        sr, sp = ref.state(), port.state()
+        for q in ("x", "v", "dv"):
+            assert np.array_equal(sr[q], sp[q]), (step, q)
+        cr, cp = ref.contacts(), port.contacts()
+        assert cr["count"] == cp["count"], step
+        assert np.array_equal(cr["active"], cp["active"]), step
+        assert np.array_equal(cr["impulses"], cp["impulses"]), step
+        active = max(active, int(cr["active"].sum()))
+    assert active > 20
+    assert np.array_equal(ref.describe()["fat_aabb"], port.describe()["fat_aabb"])
