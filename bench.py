@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--side", type=int, default=256)
-    ap.add_argument("--cg", choices=["fused", "persistent"], default="fused",
+    ap.add_argument("--cg", choices=["fused", "persistent"], default="persistent",
                     help="the headline cloth's CG: one persistent launch with one grid reduction per "
                          "iteration (fused) or two")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -135,12 +135,12 @@ def peaks():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (read + write) of one persistent-CG launch on the 256x256 headline
-# cloth, from one ncu capture of that launch (dram__bytes_read.sum +
-# dram__bytes_write.sum).  The whole system stays in L2 after its first
-# touch, so the figure holds for any iteration count.  Other sizes have no
-# capture: traffic is reported as null.
-GRID_CG_TRAFFIC = {256: 36.53e6 + 0.04e6}
+# DRAM bytes (read + write) of one persistent-CG launch, by (cloth side, CG
+# form), from one ncu capture of that launch (dram__bytes_read.sum +
+# dram__bytes_write.sum).  At 256 x 256 the whole system stays in L2 after
+# its first touch, so the figure holds for any iteration count.  Sizes and
+# forms without a capture report null.
+GRID_CG_TRAFFIC = {(256, "persistent"): 36.53e6 + 0.04e6}
 
 
 def algorithmic_bytes(info: dict, kernel: str) -> float:
@@ -312,7 +312,7 @@ def run_ours(args, rank, world):
         "launches": launches, "clocks": clocks.summary(), "info": info,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                      "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": GRID_CG_TRAFFIC.get(args.side) if dom == "grid_cg" else None,
+                     "traffic": GRID_CG_TRAFFIC.get((args.side, args.cg)) if dom == "grid_cg" else None,
                      "traffic_source": "ncu capture of one launch at this size",
                      "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
                      "share": kern[dom][0] / total if total else None},
@@ -324,45 +324,55 @@ def run_stiff(args, dev: int):
     """The 1024 x 1024 study cloth (1,048,576 vertices, 2,093,058 triangles,
     no bending): stretch 1e5, damping 0.1, shear 1e3, the two corners of row
     0 pinned, no jitter, CG to relative residual 1e-4 (at most 2000
-    iterations) with FP64 dots in the fused persistent form.  Of its 50 steps
-    from rest, steps 3-49 are timed with CUDA events (the first three build
-    the step graph and load the modules).  Its system, 7.3 M blocks or 293 MB
-    of values and columns, is larger than L2, so every CG iteration streams
-    it from HBM.  The roofline is of the CG launch, from three more steps
-    launched kernel by kernel."""
+    iterations) with FP64 dots.  Of its 50 steps from rest, steps 3-49 are
+    timed with CUDA events (the first three build the step graph and load
+    the modules), once with each persistent CG form.  Its system, 7.3 M
+    blocks or 293 MB of values and columns, is larger than L2, so every CG
+    iteration streams it from HBM.  Each form's roofline is of its CG launch,
+    from three more steps launched kernel by kernel; the section reports the
+    faster form at its top level."""
     import bounce_b200 as b3g
 
     side = args.stiff_side
     scene = b3g.stiff_scene(side)
     opts = b3g.SolverOptions.relative(1e-4, 2000, b3g.DOT_F64)
-    cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene, opts)
-    cloth.set_cg_strategy(True, fused=True)
-    info = cloth.info()
-    warm = 3
-    for _ in range(warm):
-        cloth.step(scene.dt)
-    ms, its = [], []
-    for _ in range(warm, scene.steps):
-        st = cloth.step(scene.dt)
-        ms.append(st["step_ms"])
-        its.append(st["iterations"])
-    prof = [cloth.step_profiled(scene.dt) for _ in range(3)]
-    cloth.close()
-    cg_ms = sum(p["cg_spmv_ms"] for p in prof) / len(prof)
-    cg_it = sum(p["cg_iterations"] for p in prof) / len(prof)
-    alg = algorithmic_bytes(info, f"grid_cg:{cg_it}")
     peak, peak_kind = peaks()
-    achieved = alg / (cg_ms / 1e3) / 1e9
-    n = info["vertices"]
-    return {"workload": f"grid{side}x{side}_stiff", "vertices": n, "blocks": info["blocks"],
-            "steps": f"{warm}-{scene.steps - 1}", "ms_per_step": sum(ms) / len(ms),
-            "vertex_steps_per_s": n * len(ms) / (sum(ms) / 1e3), "cg_iterations_mean": float(np.mean(its)),
-            "cg_iterations_max": int(max(its)), "cg": "relative residual 1e-4, max 2000, fp64 dots, fused persistent",
-            "roofline": {"bound": "hbm", "kernel": "grid_cg_fused", "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": GRID_CG_TRAFFIC.get(side),
+    forms = {}
+    for form in ("persistent", "fused"):
+        cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene, opts)
+        cloth.set_cg_strategy(True, fused=form == "fused")
+        info = cloth.info()
+        warm = 3
+        for _ in range(warm):
+            cloth.step(scene.dt)
+        ms, its = [], []
+        for _ in range(warm, scene.steps):
+            st = cloth.step(scene.dt)
+            ms.append(st["step_ms"])
+            its.append(st["iterations"])
+        prof = [cloth.step_profiled(scene.dt) for _ in range(3)]
+        cloth.close()
+        cg_ms = sum(p["cg_spmv_ms"] for p in prof) / len(prof)
+        cg_it = sum(p["cg_iterations"] for p in prof) / len(prof)
+        alg = algorithmic_bytes(info, f"grid_cg:{cg_it}")
+        achieved = alg / (cg_ms / 1e3) / 1e9
+        n = info["vertices"]
+        forms[form] = {
+            "ms_per_step": sum(ms) / len(ms), "vertex_steps_per_s": n * len(ms) / (sum(ms) / 1e3),
+            "cg_iterations_mean": float(np.mean(its)), "cg_iterations_max": int(max(its)),
+            "us_per_cg_iteration": 1e3 * cg_ms / max(cg_it, 1.0),
+            "roofline": {"bound": "hbm", "kernel": "grid_cg" if form == "persistent" else "grid_cg_fused",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": GRID_CG_TRAFFIC.get((side, form)),
                          "algorithmic_bytes_per_launch": alg, "avg_launch_ms": cg_ms,
                          "cg_iterations_per_launch": cg_it}}
+    best = max(forms, key=lambda f: forms[f]["vertex_steps_per_s"])
+    out = {"workload": f"grid{side}x{side}_stiff", "vertices": info["vertices"], "blocks": info["blocks"],
+           "steps": f"3-{scene.steps - 1}", "cg": "relative residual 1e-4, max 2000, fp64 dots",
+           "cg_strategy": best}
+    out.update(forms[best])
+    out["by_strategy"] = forms
+    return out
 
 
 def run_batched(args, dev: int, cpu_sample: bool = False):
@@ -403,18 +413,18 @@ def run_batched(args, dev: int, cpu_sample: bool = False):
         c.close()
     batch.close()
     # the plain single-instance path on the same cloths, the same steps from
-    # rest: each cloth alone, once with the per-iteration launches in a graph
-    # loop and once with the fused persistent CG; each cloth counts at the
-    # faster of the two
+    # rest: each cloth alone with each CG form (per-iteration launches in a
+    # graph loop, the persistent CG, the fused persistent CG); each cloth
+    # counts at its fastest
     plain_v, plain_by = None, {}
     if not args.skip_plain:
         per = []
-        for strategy in ("launches", "fused"):
+        for strategy in ("launches", "persistent", "fused"):
             plain = [b3g.Cloth(sc.mesh, sc.cdef, device=dev).setup(sc, opts) for sc in scenes]
             t = np.zeros(len(plain))
             for k, c in enumerate(plain):
-                if strategy == "fused":
-                    c.set_cg_strategy(True, fused=True)
+                if strategy != "launches":
+                    c.set_cg_strategy(True, fused=strategy == "fused")
                 for _ in range(args.warmup):
                     c.step(dt)
                 for _ in range(args.batch_steps):
@@ -422,13 +432,13 @@ def run_batched(args, dev: int, cpu_sample: bool = False):
                 c.close()
             per.append(t)
             plain_by[strategy] = replicas.aggregate_rate(rows * args.batch_steps, float(t.sum()) / 1000.0)
-        best = np.minimum(per[0], per[1])
+        best = np.minimum(np.minimum(per[0], per[1]), per[2])
         plain_v = replicas.aggregate_rate(rows * args.batch_steps, float(best.sum()) / 1000.0)
     return {"cloths": int(replicas.sum_over_ranks(len(scenes))), "vertices": int(replicas.sum_over_ranks(rows)),
             "vertex_steps_per_s": batched,
             "ms_per_step": sum(ms) / len(ms), "plain_vertex_steps_per_s": plain_v,
             "plain_by_strategy": plain_by,
-            "plain": "each cloth alone, at the faster of per-iteration launches and the fused persistent CG",
+            "plain": "each cloth alone, at the fastest of its three CG forms",
             "speedup_vs_plain": batched / plain_v if plain_v else None, "cg_iterations_mean": float(np.mean(iters)),
             "schedule": {"cluster": sched["cluster"],
                          "split_size_classes": [k for k, v in enumerate(sched["split_class"]) if v]},

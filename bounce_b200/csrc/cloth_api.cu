@@ -13,6 +13,7 @@
 #include "topology.h"
 #include "cloth_internal.h"
 #include "grid_cg.cuh"
+#include "broadphase_order.h"
 
 using namespace b3g;
 
@@ -622,6 +623,27 @@ b3g_status b3g_cloth_set_solver(b3g_cloth* c, const b3g_solver_opts* o)
     return B3G_OK;
 }
 
+}  // extern "C"
+
+namespace b3g {
+
+void rank_colliders(SphereDev* sph, uint32_t count)
+{
+    float lo[kMaxSpheres][3], hi[kMaxSpheres][3];
+    uint32_t rank[kMaxSpheres];
+    for (uint32_t s = 0; s < count; ++s)
+        for (int q = 0; q < 3; ++q) {
+            lo[s][q] = sph[s].lo[q];
+            hi[s][q] = sph[s].hi[q];
+        }
+    query_report_ranks(lo, hi, count, rank);
+    for (uint32_t s = 0; s < count; ++s) sph[s].rank = rank[s];
+}
+
+}  // namespace b3g
+
+extern "C" {
+
 b3g_status b3g_cloth_add_static_sphere(b3g_cloth* c, const float center[3], float radius, float friction,
                                        uint32_t* shape_id)
 {
@@ -642,6 +664,7 @@ b3g_status b3g_cloth_add_static_sphere(b3g_cloth* c, const float center[3], floa
     }
     if (shape_id) *shape_id = c->dev.nsph;
     c->dev.nsph += 1;
+    rank_colliders(c->dev.sph, c->dev.nsph);
     destroy_graph(c);
     return B3G_OK;
 }
@@ -667,6 +690,7 @@ b3g_status b3g_cloth_add_static_capsule(b3g_cloth* c, const float a[3], const fl
     }
     if (shape_id) *shape_id = c->dev.nsph;
     c->dev.nsph += 1;
+    rank_colliders(c->dev.sph, c->dev.nsph);
     destroy_graph(c);
     return B3G_OK;
 }
@@ -729,6 +753,7 @@ b3g_status b3g_cloth_add_static_hull(b3g_cloth* c, const float* vertices, uint32
     }
     if (shape_id) *shape_id = c->dev.nsph;
     c->dev.nsph += 1;
+    rank_colliders(c->dev.sph, c->dev.nsph);
     destroy_graph(c);
     return B3G_OK;
 }

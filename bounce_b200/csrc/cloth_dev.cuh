@@ -70,7 +70,13 @@ struct SphereDev {
     float ax, ay, az, bx, by, bz;
     const float* hull;    // hull: nhv vertices (3 floats), then nhf planes (normal, offset)
     uint32_t nhv, nhf;
+    uint32_t rank;        // position among the shapes a world query reports (new contacts of one
+                          // step are listed in that order)
 };
+
+// Ranks the colliders sph[0..count) by the world broadphase's report order
+// (cloth_api.cu).
+void rank_colliders(SphereDev* sph, uint32_t count);
 
 struct ClothDev {
     uint32_t n, t, ns, nsph;

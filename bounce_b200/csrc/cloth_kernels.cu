@@ -1027,7 +1027,7 @@ __global__ void k_post(const __grid_constant__ ClothDev one, const __grid_consta
             if (!c.c_exists[q] && dyn && overlap(lo, hi, c.sph[s])) {
                 c.c_exists[q] = 1;
                 c.c_active[q] = 0;
-                c.c_key[q] = sc->step_index * kMaxSpheres + s;
+                c.c_key[q] = sc->step_index * kMaxSpheres + c.sph[s].rank;
                 c.c_imp[q] = 0.0f;
                 c.c_imp[nn + q] = 0.0f;
                 c.c_imp[2 * nn + q] = 0.0f;

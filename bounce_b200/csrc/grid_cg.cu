@@ -28,6 +28,7 @@ constexpr int kMaxBlock = 512;
 constexpr int kMaxWarps = kMaxBlock / 32;
 constexpr int kPrefetch = 16;  // partials per lane loaded together (up to 512 CTAs)
 constexpr int kPrefetchFused = 6;  // the fused form's 32-byte partials: up to 192 CTAs
+constexpr size_t kSmemLimit = 227 * 1024;  // dynamic shared memory of one CTA on sm_100
 constexpr uint64_t kSpinLimit = 1ull << 26;
 constexpr uint32_t kStatusTimeout = 7;
 
@@ -449,6 +450,14 @@ __device__ __forceinline__ void st_rec(float4* rec, uint32_t j, f3 r, f3 s, f3 p
 
 __device__ __forceinline__ f3 hadamard(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
 
+// Block k of a thread's row kept in shared memory, [slot][component][thread].
+__device__ __forceinline__ m3 smem_block(const float* sa, uint32_t k, uint32_t B, uint32_t tid)
+{
+    const uint32_t o = k * 9u * B + tid;
+    return m3{f3{sa[o], sa[o + B], sa[o + 2 * B]}, f3{sa[o + 3 * B], sa[o + 4 * B], sa[o + 5 * B]},
+              f3{sa[o + 6 * B], sa[o + 7 * B], sa[o + 8 * B]}};
+}
+
 // The direction of this pass at a vertex, from its record of the previous
 // pass: the owner evaluates exactly this for its own row.
 __device__ __forceinline__ f3 rec_direction(const Rec& q, float alpha, float beta, bool first)
@@ -458,29 +467,67 @@ __device__ __forceinline__ f3 rec_direction(const Rec& q, float alpha, float bet
     return hadamard(rn, q.sp) + beta * q.p;
 }
 
-// The four sums of a fused pass, reduced together: p.s and r.z in the
-// solve's dot precision (they give alpha and the exact delta, as the
-// reference's float32 b3Dot would), s.z and s.P^-1 s always in FP64.  The
-// latter two only enter the expanded next delta, whose terms cancel; summed
-// in FP32 their rounding would be magnified into beta.
+// The sums of a fused pass, reduced together: p.s and r.z in the solve's
+// dot precision (they give alpha and the exact delta, as the reference's
+// float32 b3Dot would), s.z and s.P^-1 s always in FP64.  Those two only
+// enter the expanded next delta, whose terms cancel; summed in FP32 their
+// rounding would be magnified into beta.  The expansion also needs r.z to
+// that accuracy: with FP32 dots an FP64 copy of it rides along (the
+// compensated and FP64 sums carry it already).  32 bytes per CTA in every
+// precision.
+template <int DOT>
+struct FusedStore {
+    typename DotT<DOT>::T ps, rz;
+    double sz, sps;
+};
+template <>
+struct FusedStore<0> {
+    float ps, rz;
+    double sz, sps, rz64;
+};
+
 template <int DOT>
 struct FusedSums {
     typedef DotT<DOT> P;
-    struct T {
-        typename P::T ps, rz;
-        double sz, sps;
-    };
-    static __device__ T zero() { return T{P::zero(), P::zero(), 0.0, 0.0}; }
-    static __device__ T combine(T a, T b)
+    typedef FusedStore<DOT> T;
+    static __device__ T zero()
     {
-        return T{P::combine(a.ps, b.ps), P::combine(a.rz, b.rz), a.sz + b.sz, a.sps + b.sps};
+        T a;
+        a.ps = P::zero();
+        a.rz = P::zero();
+        a.sz = 0.0;
+        a.sps = 0.0;
+        if constexpr (DOT == 0) a.rz64 = 0.0;
+        return a;
+    }
+    static __device__ T combine(T a, const T& b)
+    {
+        a.ps = P::combine(a.ps, b.ps);
+        a.rz = P::combine(a.rz, b.rz);
+        a.sz += b.sz;
+        a.sps += b.sps;
+        if constexpr (DOT == 0) a.rz64 += b.rz64;
+        return a;
     }
     static __device__ T shfl(T a, int off)
     {
-        return T{P::shfl(a.ps, off), P::shfl(a.rz, off), __shfl_down_sync(0xffffffffu, a.sz, off),
-                 __shfl_down_sync(0xffffffffu, a.sps, off)};
+        a.ps = P::shfl(a.ps, off);
+        a.rz = P::shfl(a.rz, off);
+        a.sz = __shfl_down_sync(0xffffffffu, a.sz, off);
+        a.sps = __shfl_down_sync(0xffffffffu, a.sps, off);
+        if constexpr (DOT == 0) a.rz64 = __shfl_down_sync(0xffffffffu, a.rz64, off);
+        return a;
     }
-    static __device__ T load(const T* p) { return T{P::load(&p->ps), P::load(&p->rz), __ldcg(&p->sz), __ldcg(&p->sps)}; }
+    static __device__ T load(const T* p)
+    {
+        T a;
+        a.ps = P::load(&p->ps);
+        a.rz = P::load(&p->rz);
+        a.sz = __ldcg(&p->sz);
+        a.sps = __ldcg(&p->sps);
+        if constexpr (DOT == 0) a.rz64 = __ldcg(&p->rz64);
+        return a;
+    }
     static __device__ double dot64(f3 a, f3 b)
     {
         return (double)a.x * (double)b.x + (double)a.y * (double)b.y + (double)a.z * (double)b.z;
@@ -491,9 +538,17 @@ struct FusedSums {
         acc.rz = P::add_term(acc.rz, r, z);
         acc.sz += dot64(s, z);
         acc.sps += dot64(s, hadamard(s, sp));
+        if constexpr (DOT == 0) acc.rz64 += dot64(r, z);
+    }
+    // r.z to FP64-like accuracy, for the expansion
+    static __device__ double rz_exact(const T& a)
+    {
+        if constexpr (DOT == 0) return a.rz64;
+        else return P::value(a.rz);
     }
 };
-static_assert(sizeof(FusedSums<1>::T) <= 32, "fused partials: 32 bytes per CTA and parity");
+static_assert(sizeof(FusedStore<0>) == 32 && sizeof(FusedStore<1>) == 32 && sizeof(FusedStore<2>) == 32,
+              "fused partials: 32 bytes per CTA and parity");
 
 // The scalars of one pass from its four sums.  Returns false when the true
 // delta of the iterate (r.z) already meets the stop rule: the pass is then
@@ -501,8 +556,8 @@ static_assert(sizeof(FusedSums<1>::T) <= 32, "fused partials: 32 bytes per CTA a
 // float32 b3Dot does.
 template <int DOT>
 __device__ __forceinline__ bool fused_scalars(const StepScalars* sc, double ps, double sz, double sps, double rz,
-                                              double b_delta, float& alpha, float& beta, double& delta_next,
-                                              double& delta_true)
+                                              double rz_exact, double b_delta, float& alpha, float& beta,
+                                              double& delta_next, double& delta_true)
 {
     if (DOT != 2) {
         ps = (double)(float)ps;
@@ -512,17 +567,22 @@ __device__ __forceinline__ bool fused_scalars(const StepScalars* sc, double ps, 
     if (cg_stop(sc, rz, b_delta)) return false;
     alpha = DOT == 2 ? (float)(rz / ps) : (float)rz / (float)ps;
     const double a = (double)alpha;
-    double dn = rz - 2.0 * a * sz + a * a * sps;
+    double dn = rz_exact - 2.0 * a * sz + a * a * sps;
     if (DOT != 2) dn = (double)(float)dn;
     delta_next = dn;
     beta = DOT == 2 ? (float)(dn / rz) : (float)dn / (float)rz;
     return true;
 }
 
-template <int DOT, bool ONE_ROW>
+// SMEM_A (one-row form only): the CTA's rows' blocks are copied into shared
+// memory at the start, [slot][component][thread], and every later product
+// reads them there; only the neighbours' records come from L2.
+template <int DOT, bool ONE_ROW, bool SMEM_A>
 __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_constant__ ClothDev c, GridBarrier* bar,
                                                              float4* rec0, float4* rec1)
 {
+    extern __shared__ float smem_a[];
+    const uint32_t B = blockDim.x, tid = threadIdx.x;
     typedef DotT<DOT> D;
     typedef typename D::T T;
     StepScalars* sc = c.sc;
@@ -543,6 +603,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
     RegRow rr;
     f3 x = zero3(), r = zero3(), s = zero3(), p = zero3(), sp = zero3();
     if (ONE_ROW && act) load_reg_row(c, first_row, rr);
+    if (SMEM_A && act) {
+        // the row's blocks into shared memory, once for the whole solve
+#pragma unroll 1
+        for (uint32_t k = 0; k < rr.deg; ++k) {
+            const uint32_t g = rr.base + 32u * k, o = k * 9u * B + tid;
+#pragma unroll
+            for (uint32_t q = 0; q < 9; ++q) smem_a[o + q * B] = c.vals[(size_t)q * c.E + g];
+        }
+    }
 
     // x0 = S m_x, r = S (b - A x0), b_delta, delta = r.S P^-1 r
     // (cloth_force_solver.cpp:90-100); record 0 holds r with s = p = 0.
@@ -556,7 +625,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
                 if ((uint32_t)k < rr.deg) {
                     const uint32_t col = rr.col[k];
                     const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
-                    ax = ax + block_at(c, rr.base + 32u * k) * xj;
+                    const m3 a = block_at(c, rr.base + 32u * k);
+                    ax = ax + a * xj;
                 }
             }
         } else {
@@ -617,11 +687,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
                         p = z + beta * p;
                     }
                     // s = S A p; slot 0 is the row's own diagonal block
-                    f3 acc = zero3() + block_at(c, rr.base) * p;
+                    f3 acc = zero3() + (SMEM_A ? smem_block(smem_a, 0, B, tid) : block_at(c, rr.base)) * p;
 #pragma unroll
                     for (int k = 1; k < kRegCols; ++k) {
                         if ((uint32_t)k < rr.deg) {
-                            const m3 a = block_at(c, rr.base + 32u * k);
+                            const m3 a = SMEM_A ? smem_block(smem_a, k, B, tid) : block_at(c, rr.base + 32u * k);
                             const Rec q = ld_rec(rin, rr.col[k]);
                             acc = acc + a * rec_direction(q, alpha, beta, first);
                         }
@@ -666,7 +736,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
             double dn = 0.0, dt = 0.0;
             float a1 = 0.0f, b1 = 0.0f;
             const bool accept = fused_scalars<DOT>(sc, D::value(v4[0].ps), v4[0].sz, v4[0].sps, D::value(v4[0].rz),
-                                                   b_delta, a1, b1, dn, dt);
+                                                   F::rz_exact(v4[0]), b_delta, a1, b1, dn, dt);
             if (!accept) {
                 // the iterate already meets the stop rule: the reference stops
                 // before this pass; its x is the current one
@@ -708,9 +778,10 @@ timeout:
 }
 
 template <int DOT>
-const void* fused_kernel(bool one_row)
+const void* fused_kernel(bool one_row, bool smem_a)
 {
-    return one_row ? (const void*)k_grid_cg_fused<DOT, true> : (const void*)k_grid_cg_fused<DOT, false>;
+    if (!one_row) return (const void*)k_grid_cg_fused<DOT, false, false>;
+    return smem_a ? (const void*)k_grid_cg_fused<DOT, true, true> : (const void*)k_grid_cg_fused<DOT, true, false>;
 }
 
 }  // namespace
@@ -727,7 +798,7 @@ GridCgShape grid_cg_shape(uint32_t n, int device, bool fused)
         g.blocks = (int)((n + g.threads - 1) / g.threads);
     } else {
         int per_sm = 1;
-        const void* fn = fused ? (const void*)k_grid_cg_fused<2, false> : (const void*)k_grid_cg<2, false>;
+        const void* fn = fused ? (const void*)k_grid_cg_fused<2, false, false> : (const void*)k_grid_cg<2, false>;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMaxBlock, 0) != cudaSuccess ||
             per_sm < 1) {
             cudaGetLastError();
@@ -777,7 +848,17 @@ cudaError_t launch_grid_cg_fused(const ClothDev& c, int dot, GridBarrier* bar, f
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const void* fn = dot == 2 ? fused_kernel<2>(one_row) : dot == 1 ? fused_kernel<1>(one_row) : fused_kernel<0>(one_row);
+    // the rows' blocks in shared memory when they fit beside the static
+    // shared memory of the reductions
+    const size_t smem = (size_t)c.max_deg * 9 * sizeof(float) * (size_t)g.threads;
+    const bool smem_a = one_row && smem + 4096 <= kSmemLimit;
+    const void* fn = dot == 2 ? fused_kernel<2>(one_row, smem_a)
+                   : dot == 1 ? fused_kernel<1>(one_row, smem_a) : fused_kernel<0>(one_row, smem_a);
+    if (smem_a) {
+        cudaError_t ea = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (ea != cudaSuccess) return ea;
+        cfg.dynamicSmemBytes = smem;
+    }
     float4* rec1 = rec + 3 * (size_t)c.n;
     void* args[4] = {const_cast<ClothDev*>(&c), &bar, &rec, &rec1};
     const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);

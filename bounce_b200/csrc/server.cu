@@ -161,6 +161,7 @@ b3g_status activate(b3g_server* s, Request* r)
             sp.hi[q] = (ctr[q] + sp.radius) + 0.2f;
         }
     }
+    rank_colliders(c->dev.sph, c->dev.nsph);
     return B3G_OK;
 }
 

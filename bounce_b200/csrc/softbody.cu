@@ -578,7 +578,7 @@ __global__ void k_sb_post(SoftDev d, float h)
         if (d.c_exists[q] || !node_overlap(d, i, d.hull[s])) continue;
         d.c_exists[q] = 1;
         d.c_active[q] = 0;
-        d.c_key[q] = d.step_index * kMaxSpheres + s;
+        d.c_key[q] = d.step_index * kMaxSpheres + d.hull[s].rank;
         d.c_imp[q] = 0.0f;
         d.c_imp[nn + q] = 0.0f;
         d.c_imp[2 * nn + q] = 0.0f;
@@ -1073,6 +1073,7 @@ b3g_status b3g_softbody_add_static_hull(b3g_softbody* b, const float* vertices, 
     d.c_imp = f + 12 * nn;
     if (shape_id) *shape_id = d.nhull;
     d.nhull += 1;
+    rank_colliders(d.hull, d.nhull);
     return B3G_OK;
 }
 

@@ -87,6 +87,8 @@ def port_lib():
         L.oc_describe.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_get_contacts.restype = C.c_uint32
         L.oc_get_contacts.argtypes = [C.c_void_p, _u8p, _u8p, _f32p]
+        L.oc_get_contact_list.restype = C.c_uint32
+        L.oc_get_contact_list.argtypes = [C.c_void_p, C.c_uint32] + [C.c_void_p] * 4
         L.oc_ray_cast_single.restype = C.c_int
         L.oc_ray_cast_single.argtypes = [C.c_void_p, _f32p, _f32p, C.POINTER(C.c_uint32), C.POINTER(C.c_float), _f32p]
         L.oc_get_tri_contacts.restype = C.c_uint32
@@ -153,6 +155,8 @@ def ref_lib():
         L.ref_cloth_describe.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_cloth_get_contacts.restype = C.c_uint32
         L.ref_cloth_get_contacts.argtypes = [C.c_void_p, _u8p, _u8p, _f32p]
+        L.ref_cloth_get_contact_list.restype = C.c_uint32
+        L.ref_cloth_get_contact_list.argtypes = [C.c_void_p, C.c_uint32] + [C.c_void_p] * 4
         L.ref_cloth_ray_cast_single.restype = C.c_int
         L.ref_cloth_ray_cast_single.argtypes = [C.c_void_p, _f32p, _f32p, C.POINTER(C.c_uint32), C.POINTER(C.c_float),
                                                 _f32p]
@@ -239,6 +243,18 @@ class _Base:
         imp = np.zeros(3 * self.n, np.float32)
         cnt = self._get_contacts(ex, ac, imp)
         return {"count": int(cnt), "exists": ex, "active": ac, "impulses": imp.reshape(-1, 3)}
+
+    def contact_list(self):
+        """Every body contact from the list's head: particle, shape, active,
+        impulses (normal, tangent x, tangent y)."""
+        fn = self._get_contact_list
+        m = int(fn(0, None, None, None, None))
+        part = np.zeros(max(m, 1), np.uint32)
+        shape = np.zeros(max(m, 1), np.uint32)
+        act = np.zeros(max(m, 1), np.uint8)
+        imp = np.zeros(3 * max(m, 1), np.float32)
+        fn(m, part.ctypes.data, shape.ctypes.data, act.ctypes.data, imp.ctypes.data)
+        return {"particle": part[:m], "shape": shape[:m], "active": act[:m], "impulses": imp.reshape(-1, 3)[:m]}
 
     def ray_cast_single(self, p1, p2):
         """b3Cloth::RayCastSingle: (triangle, fraction, normal) or None."""
@@ -398,6 +414,9 @@ class PortCloth(_Base):
     def _get_contacts(self, *a):
         return self.L.oc_get_contacts(self.h, *a)
 
+    def _get_contact_list(self, *a):
+        return self.L.oc_get_contact_list(self.h, *a)
+
     def _get_tri_contacts(self, *a):
         return self.L.oc_get_tri_contacts(self.h, *a)
 
@@ -496,6 +515,9 @@ class RefCloth(_Base):
     def _get_contacts(self, *a):
         return self.L.ref_cloth_get_contacts(self.h, *a)
 
+    def _get_contact_list(self, *a):
+        return self.L.ref_cloth_get_contact_list(self.h, *a)
+
     def _get_tri_contacts(self, *a):
         return self.L.ref_cloth_get_tri_contacts(self.h, *a)
 
@@ -592,6 +614,8 @@ def _sb_port():
         L.os_add_hull.argtypes = [C.c_void_p, _f32p, C.c_uint32, _f32p, C.c_uint32, C.c_float]
         L.os_get_contacts.restype = C.c_uint32
         L.os_get_contacts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.os_get_contact_list.restype = C.c_uint32
+        L.os_get_contact_list.argtypes = [C.c_void_p, C.c_uint32] + [C.c_void_p] * 4
         _sb_port_ready = True
     return L
 
@@ -623,6 +647,8 @@ def _sb_ref():
         L.ref_softbody_set_node_friction.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
         L.ref_softbody_get_contacts.restype = C.c_uint32
         L.ref_softbody_get_contacts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_softbody_get_contact_list.restype = C.c_uint32
+        L.ref_softbody_get_contact_list.argtypes = [C.c_void_p, C.c_uint32] + [C.c_void_p] * 4
         _sb_ref_ready = True
     return L
 
@@ -666,6 +692,18 @@ class _SoftBase:
         cnt = self._get_contacts(ex.ctypes.data, ac.ctypes.data, imp.ctypes.data)
         return {"count": int(cnt), "exists": ex, "active": ac, "impulses": imp.reshape(-1, 3)}
 
+    def contact_list(self):
+        """Every node-body contact from the list's head: node, hull, active,
+        impulses (normal, tangent x, tangent y)."""
+        fn = self._get_contact_list
+        m = int(fn(0, None, None, None, None))
+        node = np.zeros(max(m, 1), np.uint32)
+        shape = np.zeros(max(m, 1), np.uint32)
+        act = np.zeros(max(m, 1), np.uint8)
+        imp = np.zeros(3 * max(m, 1), np.float32)
+        fn(m, node.ctypes.data, shape.ctypes.data, act.ctypes.data, imp.ctypes.data)
+        return {"node": node[:m], "shape": shape[:m], "active": act[:m], "impulses": imp.reshape(-1, 3)[:m]}
+
     def element_data(self, e):
         K = np.zeros(144, np.float32)
         invE = np.zeros(9, np.float32)
@@ -689,6 +727,9 @@ class PortSoftBody(_SoftBase):
 
     def _get_contacts(self, *a):
         return self.L.os_get_contacts(self.h, *a)
+
+    def _get_contact_list(self, *a):
+        return self.L.os_get_contact_list(self.h, *a)
 
     def __init__(self, vertices, tets, density, E, nu, c_yield, c_creep, c_max):
         self.L = _sb_port()
@@ -785,6 +826,9 @@ class RefSoftBody(_SoftBase):
 
     def _get_contacts(self, *a):
         return self.L.ref_softbody_get_contacts(self.h, *a)
+
+    def _get_contact_list(self, *a):
+        return self.L.ref_softbody_get_contact_list(self.h, *a)
 
     def __init__(self, vertices, tets, density, E, nu, c_yield, c_creep, c_max):
         self.L = _sb_ref()

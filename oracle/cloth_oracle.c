@@ -6,6 +6,7 @@
  * vec3.h, mat33.h, vec2.h, mat22.h), which is what makes the results
  * bit-identical to the compiled reference in reference mode.
  */
+#include "world_order.h"
 #include "cloth_oracle.h"
 
 #include <float.h>
@@ -1969,10 +1970,19 @@ static void find_new_body_contacts(oc_cloth* c)
     uint8_t* has = (uint8_t*)calloc((size_t)c->n * c->nsphere, 1);
     for (uint32_t q = 0; q < c->ncontact; ++q)
         has[(size_t)c->contacts[q].particle * c->nsphere + c->contacts[q].shape] = 1;
+    /* the world query reports the shapes in its tree's order */
+    float wlo[WO_MAX][3], whi[WO_MAX][3];
+    uint32_t report[WO_MAX];
+    for (uint32_t s = 0; s < c->nsphere && s < WO_MAX; ++s) {
+        wlo[s][0] = c->spheres[s].fat_lo.x; wlo[s][1] = c->spheres[s].fat_lo.y; wlo[s][2] = c->spheres[s].fat_lo.z;
+        whi[s][0] = c->spheres[s].fat_hi.x; whi[s][1] = c->spheres[s].fat_hi.y; whi[s][2] = c->spheres[s].fat_hi.z;
+    }
+    world_report_order(wlo, whi, c->nsphere, report);
     for (uint32_t k = 0; k < c->n; ++k) {
         uint32_t i = c->order[k];
         if (c->type[i] != OC_DYNAMIC) continue;
-        for (uint32_t s = 0; s < c->nsphere; ++s) {
+        for (uint32_t r = 0; r < c->nsphere; ++r) {
+            const uint32_t s = report[r];
             const sphere_t* sp = c->spheres + s;
             if (!aabb_overlap(c->fat_lo[i], c->fat_hi[i], sp->fat_lo, sp->fat_hi)) continue;
             if (has[(size_t)i * c->nsphere + s]) continue;
@@ -2614,6 +2624,24 @@ uint32_t oc_get_contacts(const oc_cloth* c, uint8_t* exists, uint8_t* active, fl
             impulses[3 * i + 1] = k->tangent_impulse.x;
             impulses[3 * i + 2] = k->tangent_impulse.y;
         }
+    }
+    return c->ncontact;
+}
+
+/* The body-contact list from its head: particle, shape, active flag and
+ * impulses; at most `cap` written, the count returned. */
+uint32_t oc_get_contact_list(const oc_cloth* c, uint32_t cap, uint32_t* particle, uint32_t* shape, uint8_t* active,
+                             float* impulses)
+{
+    uint32_t k = 0;
+    for (uint32_t q = c->ncontact; q-- > 0 && k < cap; ++k) {
+        const contact_t* ct = c->contacts + q;
+        particle[k] = ct->particle;
+        shape[k] = ct->shape;
+        active[k] = (uint8_t)(ct->active != 0);
+        impulses[3 * k] = ct->normal_impulse;
+        impulses[3 * k + 1] = ct->tangent_impulse.x;
+        impulses[3 * k + 2] = ct->tangent_impulse.y;
     }
     return c->ncontact;
 }

@@ -90,6 +90,8 @@ void oc_get_state(const oc_cloth* c, float* x, float* v, float* dv, float* mass,
 float oc_energy(const oc_cloth* c);
 uint32_t oc_describe(const oc_cloth* c, float* tri_rest, float* fat_aabb, float* force_desc);
 uint32_t oc_get_contacts(const oc_cloth* c, uint8_t* exists, uint8_t* active, float* impulses);
+uint32_t oc_get_contact_list(const oc_cloth* c, uint32_t cap, uint32_t* particle, uint32_t* shape, uint8_t* active,
+                             float* impulses);
 int oc_ray_cast_single(const oc_cloth* c, const float* p1, const float* p2, uint32_t* triangle, float* fraction,
                        float* normal);
 uint32_t oc_get_tri_contacts(const oc_cloth* c, uint32_t* pt, uint8_t* active, float* w, float* impulses);

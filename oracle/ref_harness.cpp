@@ -125,6 +125,7 @@ struct RefCloth {
     std::vector<b3CapsuleShape*> capsule_protos;
     std::vector<b3HullShape*> hull_protos;
     std::vector<b3QHull*> hulls;  // the hulls the shapes point to
+    std::vector<const b3Shape*> shapes;  // the world's shapes, in creation order
     // Particles made with b3Cloth::CreateParticle, addressed after the mesh
     // vertices (index vertexCount + k), and mouse forces by id - 1 (null once
     // destroyed).
@@ -447,7 +448,7 @@ void ref_cloth_add_sphere(void* hp, const float* center, float radius, float fri
     b3ShapeDef sd;
     sd.shape = sphere;
     sd.friction = friction;
-    body->CreateShape(sd);
+    h->shapes.push_back(body->CreateShape(sd));
 }
 
 // A static body at the origin carrying one capsule shape, segment a-b.
@@ -469,7 +470,7 @@ void ref_cloth_add_capsule(void* hp, const float* a, const float* b, float radiu
     b3ShapeDef sd;
     sd.shape = cap;
     sd.friction = friction;
-    body->CreateShape(sd);
+    h->shapes.push_back(body->CreateShape(sd));
 }
 
 // A static body at the origin with a b3HullShape: the hull b3QHull::Set
@@ -498,7 +499,7 @@ uint32_t ref_cloth_add_hull(void* hp, const float* points, uint32_t count, float
     b3ShapeDef sd;
     sd.shape = shape;
     sd.friction = friction;
-    body->CreateShape(sd);
+    h->shapes.push_back(body->CreateShape(sd));
     for (uint32_t i = 0; i < hull->vertexCount; ++i) put3(vertices + 3 * i, hull->vertices[i]);
     for (uint32_t i = 0; i < hull->faceCount; ++i) {
         put3(planes + 4 * i, hull->planes[i].normal);
@@ -685,6 +686,28 @@ uint32_t ref_cloth_get_contacts(void* hp, uint8_t* exists, uint8_t* active, floa
             impulses[3 * vtx + 1] = c->m_tangentImpulse.x;
             impulses[3 * vtx + 2] = c->m_tangentImpulse.y;
         }
+    }
+    return count;
+}
+
+// The particle-body contact list from its head: particle, shape (creation
+// index), active flag, impulses; at most `cap` written, the count returned.
+uint32_t ref_cloth_get_contact_list(void* hp, uint32_t cap, uint32_t* particle, uint32_t* shape, uint8_t* active,
+                                    float* impulses)
+{
+    RefCloth* h = (RefCloth*)hp;
+    uint32_t count = 0;
+    for (b3ParticleBodyContact* c = h->cloth->m_contactManager.m_particleBodyContactList.m_head; c;
+         c = c->m_next, ++count) {
+        if (count >= cap) continue;
+        particle[count] = c->m_p1->m_vertex;
+        uint32_t s = 0;
+        while (s < h->shapes.size() && h->shapes[s] != c->m_s2) ++s;
+        shape[count] = s;
+        active[count] = c->m_active ? 1 : 0;
+        impulses[3 * count] = c->m_normalImpulse;
+        impulses[3 * count + 1] = c->m_tangentImpulse.x;
+        impulses[3 * count + 2] = c->m_tangentImpulse.y;
     }
     return count;
 }

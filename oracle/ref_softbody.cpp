@@ -40,6 +40,7 @@ struct RefSoftBody {
     b3World* world = nullptr;
     std::vector<b3QHull*> hulls;
     std::vector<b3HullShape*> protos;
+    std::vector<const b3Shape*> shapes;  // the world's shapes, in creation order
 };
 
 }  // namespace
@@ -113,7 +114,7 @@ uint32_t ref_softbody_add_hull(void* p, const float* points, uint32_t count, flo
     b3ShapeDef sd;
     sd.shape = shape;
     sd.friction = friction;
-    body->CreateShape(sd);
+    h->shapes.push_back(body->CreateShape(sd));
     for (uint32_t i = 0; i < hull->vertexCount; ++i) {
         vertices[3 * i] = hull->vertices[i].x;
         vertices[3 * i + 1] = hull->vertices[i].y;
@@ -156,6 +157,27 @@ uint32_t ref_softbody_get_contacts(void* p, uint8_t* exists, uint8_t* active, fl
         impulses[3 * v] = c->m_normalImpulse;
         impulses[3 * v + 1] = c->m_tangentImpulse.x;
         impulses[3 * v + 2] = c->m_tangentImpulse.y;
+    }
+    return count;
+}
+
+// The node-body contact list from its head: node, hull (creation index),
+// active flag, impulses; at most `cap` written, the count returned.
+uint32_t ref_softbody_get_contact_list(void* p, uint32_t cap, uint32_t* node, uint32_t* shape, uint8_t* active,
+                                       float* impulses)
+{
+    RefSoftBody* h = static_cast<RefSoftBody*>(p);
+    uint32_t count = 0;
+    for (b3NodeBodyContact* c = h->body->m_contactManager.m_nodeBodyContactList.m_head; c; c = c->m_next, ++count) {
+        if (count >= cap) continue;
+        node[count] = c->m_n1->m_vertex;
+        uint32_t s = 0;
+        while (s < h->shapes.size() && h->shapes[s] != c->m_s2) ++s;
+        shape[count] = s;
+        active[count] = c->m_active ? 1 : 0;
+        impulses[3 * count] = c->m_normalImpulse;
+        impulses[3 * count + 1] = c->m_tangentImpulse.x;
+        impulses[3 * count + 2] = c->m_tangentImpulse.y;
     }
     return count;
 }

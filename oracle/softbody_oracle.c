@@ -13,6 +13,7 @@
  * Sparse rows follow b3SparseMat33 (include/bounce/sparse/sparse_mat33.h):
  * a new block goes to the front of its row list, a copy reverses a row,
  * products and sums walk the list from its head. */
+#include "world_order.h"
 #include "softbody_oracle.h"
 
 #include <float.h>
@@ -494,12 +495,22 @@ static void sb_update_contacts(os_body* b)
 }
 
 /* FindNewBodyContacts + AddNSPair (softbody_contact_manager.cpp:44-107):
- * dynamic nodes in index order, each against every overlapping shape. */
+ * dynamic nodes in index order, each against every overlapping shape in the
+ * world query's report order. */
 static void sb_find_new_contacts(os_body* b)
 {
+    /* the world query reports the hulls in its tree's order */
+    float wlo[WO_MAX][3], whi[WO_MAX][3];
+    uint32_t report[WO_MAX];
+    for (uint32_t k = 0; k < b->nhull; ++k) {
+        wlo[k][0] = b->hulls[k].lo.x; wlo[k][1] = b->hulls[k].lo.y; wlo[k][2] = b->hulls[k].lo.z;
+        whi[k][0] = b->hulls[k].hi.x; whi[k][1] = b->hulls[k].hi.y; whi[k][2] = b->hulls[k].hi.z;
+    }
+    world_report_order(wlo, whi, b->nhull, report);
     for (uint32_t i = 0; i < b->n; ++i) {
         if (b->type[i] != 2) continue;
-        for (uint32_t sh = 0; sh < b->nhull; ++sh) {
+        for (uint32_t r = 0; r < b->nhull; ++r) {
+            const uint32_t sh = report[r];
             if (!sb_overlap(b->fat_lo[i], b->fat_hi[i], b->hulls[sh].lo, b->hulls[sh].hi)) continue;
             int exists = 0;
             for (uint32_t q = 0; q < b->ncontact && !exists; ++q)
@@ -878,6 +889,25 @@ uint32_t os_get_contacts(const os_body* b, uint8_t* exists, uint8_t* active, flo
         impulses[3 * c->node] = c->normal_impulse;
         impulses[3 * c->node + 1] = c->ti_x;
         impulses[3 * c->node + 2] = c->ti_y;
+    }
+    return b->ncontact;
+}
+
+/* The contact list from its head: per contact its node, hull, active flag
+ * and impulses (normal, tangent x, tangent y); at most `cap` are written,
+ * the count is returned. */
+uint32_t os_get_contact_list(const os_body* b, uint32_t cap, uint32_t* node, uint32_t* shape, uint8_t* active,
+                             float* impulses)
+{
+    uint32_t k = 0;
+    for (uint32_t q = b->ncontact; q-- > 0 && k < cap; ++k) {
+        const os_contact* c = b->contacts + q;
+        node[k] = c->node;
+        shape[k] = c->shape;
+        active[k] = (uint8_t)(c->active != 0);
+        impulses[3 * k] = c->normal_impulse;
+        impulses[3 * k + 1] = c->ti_x;
+        impulses[3 * k + 2] = c->ti_y;
     }
     return b->ncontact;
 }

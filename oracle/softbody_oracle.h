@@ -62,5 +62,7 @@ void os_set_node_radius(os_body* b, uint32_t i, float radius);
 void os_set_node_friction(os_body* b, uint32_t i, float friction);
 int os_add_hull(os_body* b, const float* vertices, uint32_t nv, const float* planes, uint32_t nf, float friction);
 uint32_t os_get_contacts(const os_body* b, uint8_t* exists, uint8_t* active, float* impulses);
+uint32_t os_get_contact_list(const os_body* b, uint32_t cap, uint32_t* node, uint32_t* shape, uint8_t* active,
+                             float* impulses);
 
 #endif

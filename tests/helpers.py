@@ -23,6 +23,32 @@ def rel_err(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
 
 
+def oracle_floor_step(port, scene, ora, dt, stop_rule, tol, max_iter, dress=None):
+    """Positions after one step of clones of the oracle `ora` -- its whole
+    state: positions, velocities, CG warm start, body contacts with their
+    impulses and the particles' proxies -- with compensated and with FP64
+    dots.  Against `ora`'s own step they measure how far the same algorithm
+    moves under different rounding alone; a truncated CG (the reference's
+    20-iteration rule) is sensitive at some steps.  `dress(clone)` applies
+    per-particle settings; call before `ora` steps."""
+    st = ora.state()
+    ca = ora.contacts()
+    fat = ora.describe()["fat_aabb"]
+    live = np.nonzero(ca["exists"])[0]
+    out = []
+    for dot in (1, 2):
+        c = port.PortCloth(scene.mesh, scene.cdef).setup(scene)
+        if dress:
+            dress(c)
+        c.set_solver(stop_rule, tol, max_iter, dot)
+        c.set_state(x=st["x"], v=st["v"], dv=st["dv"])
+        c.set_contacts(live, np.zeros(live.size, np.uint32), ca["impulses"][live])
+        c.set_proxies(fat[:, :3], fat[:, 3:])
+        c.step(dt)
+        out.append(c.state()["x"])
+    return out
+
+
 def device_system(sysd, device="cuda:0"):
     """Copy an exported block-CSR system to device tensors (uint32 as int32 bits)."""
     import torch

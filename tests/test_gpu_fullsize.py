@@ -103,8 +103,9 @@ def test_batch512_sample_matches_oracle(b3g, port):
 
 def test_headline_in_contact_one_step(b3g, port):
     """The headline cloth draped on the sphere, at the benchmark's own setting
-    (CG to relative residual 1e-4, FP64 dots, the fused persistent CG).  After
-    30 steps of fall, some 25,000 particles touch the sphere.  The oracle is
+    (CG to relative residual 1e-4, FP64 dots, the persistent CG).  After 20
+    steps of fall, within the benchmark's timed steps, over 10,000 particles
+    touch the sphere.  The oracle is
     given the GPU's whole state: positions, velocities, the CG warm start,
     the body-contact list with its impulses and the particles' fat AABBs.
     Then both take one step.
@@ -118,8 +119,8 @@ def test_headline_in_contact_one_step(b3g, port):
     scene = b3g.sphere_scene(256)
     opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
     gpu = b3g.Cloth(scene.mesh, scene.cdef).setup(scene, opts)
-    gpu.set_cg_strategy(True, fused=True)
-    for _ in range(30):
+    gpu.set_cg_strategy(True)
+    for _ in range(20):
         gpu.step(scene.dt)
     st = gpu.state()
     gc = gpu.contacts()
@@ -134,7 +135,7 @@ def test_headline_in_contact_one_step(b3g, port):
 
     g = gpu.step(scene.dt)
     o = ora.step(scene.dt)
-    assert o["active_contacts"] > 20000, o["active_contacts"]
+    assert o["active_contacts"] > 10000, o["active_contacts"]
     assert g["active_contacts"] == o["active_contacts"], (g["active_contacts"], o["active_contacts"])
     assert abs(g["iterations"] - o["iterations"]) <= 1, (g["iterations"], o["iterations"])
     gs, os_ = gpu.state(), ora.state()

@@ -263,3 +263,54 @@ def test_softbody_hull_arguments(b3g):
     assert e.value.status == 8
     body.step(scene.dt)
     assert body.contacts()["exists"].size == 4 * n
+
+
+def test_softbody_coplanar_hulls_contact_order(b3g, port):
+    """A block landing on three overlapping hulls whose tops lie in one plane,
+    so that nodes over the overlaps rest on two or three hulls at once.  A
+    node's contacts are solved in the list order Bounce gives them, which the
+    world query's tree decides; per step from the GPU's state, positions,
+    velocities and each (hull, node) contact's impulses match the oracle,
+    which matches the reference's own list bit for bit
+    (test_softbody_overlapping_hulls_match_live_reference)."""
+    from bounce_b200.meshes import SoftBodyDef, SoftBodyScene, block_softbody_mesh
+
+    verts, tets = block_softbody_mesh(4, 3, 3, 0.5)
+    sdef = SoftBodyDef(density=0.2, E=1000.0, nu=0.33, c_yield=0.1, c_creep=0.5, c_max=1.0)
+    scene = SoftBodyScene(verts, tets, sdef, np.full(len(verts), 0.2, np.float32), np.zeros(0, np.uint32))
+    boxes = [((-3.0, -1.5, -3.0), (3.0, -0.9, 3.0)), ((-1.2, -1.4, -1.0), (0.3, -0.9, 1.0)),
+             ((-0.3, -1.3, -1.0), (1.2, -0.9, 1.0))]
+    gpu = b3g.SoftBody(verts, tets, sdef).setup(scene)
+    ora = port.PortSoftBody(verts, tets, sdef.density, sdef.E, sdef.nu, sdef.c_yield, sdef.c_creep,
+                            sdef.c_max).setup(scene)
+    for lo, hi in boxes:
+        c, h = (np.add(lo, hi) / 2.0), (np.subtract(hi, lo) / 2.0)
+        hv, hp = _box(tuple(c), tuple(h))
+        for b in (gpu, ora):
+            b.add_hull(hv, hp, 0.4)
+    for b in (gpu, ora):
+        for i in range(len(verts)):
+            b.set_node_radius(i, 0.05)
+            b.set_node_friction(i, 0.3)
+    n = len(verts)
+    vscale = float(np.linalg.norm(scene.gravity)) * scene.dt
+    multi = 0
+    for step in range(60):
+        _sync(gpu, ora)
+        gpu.step(scene.dt)
+        ora.step(scene.dt)
+        gs, os_ = gpu.state(), ora.state()
+        assert rel_err(gs["x"], os_["x"]) <= 1e-4, step
+        assert float(np.abs(gs["v"] - os_["v"]).max()) <= 1e-4 * max(float(np.abs(os_["v"]).max()), vscale), step
+        gc, ol = gpu.contacts(), ora.contact_list()
+        oimp = np.zeros((3 * n, 3), np.float32)
+        oact = np.zeros(3 * n, np.uint8)
+        slot = ol["shape"].astype(np.int64) * n + ol["node"].astype(np.int64)
+        oimp[slot] = ol["impulses"]
+        oact[slot] = ol["active"]
+        both = (gc["active"] != 0) & (oact != 0)
+        scale = max(float(np.abs(oimp).max()), 1e-6)
+        assert float(np.abs(gc["impulses"][both] - oimp[both]).max(initial=0.0)) <= 1e-3 * scale, step
+        nodes = np.nonzero(oact)[0] % n
+        multi = max(multi, int((np.bincount(nodes, minlength=n) >= 2).sum()) if nodes.size else 0)
+    assert multi > 0

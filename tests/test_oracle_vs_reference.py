@@ -282,7 +282,10 @@ def test_particle_radius_and_friction_match_reference():
     scene: radii of 0-2 cm and frictions of 0-1 before the first step, and a
     second set at step 25 while the cloth lies on the sphere (SetRadius moves
     the proxy).  They enter the contact test, the position solve and the
-    friction mix; the restatement follows the reference bit for bit."""
+    friction mix; the restatement follows the reference bit for bit.  Both
+    step without the self-collision pass, as the GPU does for a cloth created
+    with thickness 0; the reference's full Step would turn some
+    particle-triangle contacts active here from step 12 on."""
     scene = sphere_scene(16)
     ref = oracle.RefCloth(scene.mesh, scene.cdef).setup(scene)
     port = oracle.PortCloth(scene.mesh, scene.cdef).setup(scene)
@@ -305,3 +308,32 @@ def test_particle_radius_and_friction_match_reference():
         active = max(active, int(cr["active"].sum()))
     assert active > 20
     assert np.array_equal(ref.describe()["fat_aabb"], port.describe()["fat_aabb"])
+
+
+def test_overlapping_colliders_match_reference():
+    """A cloth draping over a sphere, a capsule lying across its top and a box
+    hull whose top is level with both, so that particles touch two or three
+    shapes at once.  A particle's contacts are in the list order the world
+    query's tree gives; the restatement derives that order from the
+    broadphase tree, and its whole contact list (particle, shape, active,
+    impulses, in order) matches the reference bit for bit."""
+    scene = sphere_scene(16)
+    ref = oracle.RefCloth(scene.mesh, scene.cdef).setup(scene)
+    port = oracle.PortCloth(scene.mesh, scene.cdef).setup(scene)
+    for o in (ref, port):
+        o.add_capsule((-0.6, -0.25, 0.0), (0.6, -0.25, 0.0), 0.05, 0.5)
+    box = np.array([(x, y, z) for x in (-0.7, -0.15) for y in (-0.6, -0.2) for z in (-0.4, 0.4)], np.float32)
+    hv, hp = ref.add_hull_from_points(box, 0.2)
+    port.add_hull(hv, hp, 0.2)
+    multi = 0
+    for step in range(60):
+        assert ref.step(scene.dt)["iterations"] == port.step(scene.dt)["iterations"], step
+        sr, sp = ref.state(), port.state()
+        for q in ("x", "v", "dv"):
+            assert np.array_equal(sr[q], sp[q]), (step, q)
+        lr, lp = ref.contact_list(), port.contact_list()
+        for q in ("particle", "shape", "active", "impulses"):
+            assert np.array_equal(lr[q], lp[q]), (step, q)
+        act = lr["particle"][lr["active"] != 0]
+        multi = max(multi, int((np.bincount(act, minlength=scene.mesh.vertex_count) >= 2).sum()) if act.size else 0)
+    assert multi > 0

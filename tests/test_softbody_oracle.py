@@ -116,3 +116,47 @@ def test_softbody_hull_contacts_match_golden(port):
             for q in ("exists", "active", "impulses"):
                 assert np.array_equal(c[q], d[f"contact_{q}_{k}"]), (k, q)
     assert int(d["contact_active_150"].sum()) > 10
+
+
+def _box_points(lo, hi):
+    return np.array([(x, y, z) for x in (lo[0], hi[0]) for y in (lo[1], hi[1]) for z in (lo[2], hi[2])], np.float32)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built")
+def test_softbody_overlapping_hulls_match_live_reference():
+    """A block landing on three overlapping hulls (a ground slab and two
+    boxes whose tops lie in the slab's top plane, overlapping each other).  A node
+    touching several hulls has its contacts in the world query's report
+    order, which the restatement derives from the broadphase tree; positions,
+    velocities and every contact's state and impulses match the reference
+    bit for bit."""
+    from bounce_b200.meshes import SoftBodyDef, SoftBodyScene, block_softbody_mesh
+
+    verts, tets = block_softbody_mesh(4, 3, 3, 0.5)
+    sdef = SoftBodyDef(density=0.2, E=1000.0, nu=0.33, c_yield=0.1, c_creep=0.5, c_max=1.0)
+    scene = SoftBodyScene(verts, tets, sdef, np.full(len(verts), 0.2, np.float32), np.zeros(0, np.uint32))
+    # the three tops lie in one plane: nodes over the overlaps rest on two or
+    # three hulls at once
+    boxes = [((-3.0, -1.5, -3.0), (3.0, -0.9, 3.0)), ((-1.2, -1.4, -1.0), (0.3, -0.9, 1.0)),
+             ((-0.3, -1.3, -1.0), (1.2, -0.9, 1.0))]
+    port = _make(oracle.PortSoftBody, scene)
+    ref = _make(oracle.RefSoftBody, scene)
+    for lo, hi in boxes:
+        hv, hp = ref.add_hull_from_points(_box_points(lo, hi), 0.4)
+        port.add_hull(hv, hp, 0.4)
+    for b in (port, ref):
+        for i in range(len(verts)):
+            b.set_node_radius(i, 0.05)
+            b.set_node_friction(i, 0.3)
+    multi = 0
+    for k in range(60):
+        a, b = port.step(scene.dt), ref.step(scene.dt)
+        assert a["iterations"] == b["iterations"], k
+        sa, sb = port.state(), ref.state()
+        assert np.array_equal(sa["x"], sb["x"]) and np.array_equal(sa["v"], sb["v"]), k
+        la, lb = port.contact_list(), ref.contact_list()
+        for q in ("node", "shape", "active", "impulses"):
+            assert np.array_equal(la[q], lb[q]), (k, q)
+        nodes = lb["node"][lb["active"] != 0]
+        multi = max(multi, int((np.bincount(nodes, minlength=len(verts)) >= 2).sum()) if nodes.size else 0)
+    assert multi > 0  # some node had two or more active hull contacts at once
