@@ -54,6 +54,27 @@ __device__ __forceinline__ m3 block_at(const ClothDev& c, uint32_t idx)
               f3{v[6 * E + idx], v[7 * E + idx], v[8 * E + idx]}};
 }
 
+// Block k of a thread's row kept in shared memory, [slot][component][thread].
+__device__ __forceinline__ m3 smem_block(const float* sa, uint32_t k, uint32_t B, uint32_t tid)
+{
+    const uint32_t o = k * 9u * B + tid;
+    return m3{f3{sa[o], sa[o + B], sa[o + 2 * B]}, f3{sa[o + 3 * B], sa[o + 4 * B], sa[o + 5 * B]},
+              f3{sa[o + 6 * B], sa[o + 7 * B], sa[o + 8 * B]}};
+}
+
+// Copies the blocks of a one-row thread's row into its shared-memory column
+// (once per solve; only the thread itself reads them later).
+__device__ __forceinline__ void stage_row_blocks(const ClothDev& c, uint32_t base, uint32_t deg, float* sa,
+                                                 uint32_t B, uint32_t tid)
+{
+#pragma unroll 1
+    for (uint32_t k = 0; k < deg; ++k) {
+        const uint32_t g = base + 32u * k, o = k * 9u * B + tid;
+#pragma unroll
+        for (uint32_t q = 0; q < 9; ++q) sa[o + q * B] = c.vals[(size_t)q * c.E + g];
+    }
+}
+
 // Row `row` of s = A p, where the direction p = z + beta p_old is formed on
 // the fly from the neighbours' z = S P^-1 r and previous direction (first
 // iteration: p = z).  That is the same float expression the owner of each
@@ -210,15 +231,18 @@ __device__ __forceinline__ void load_reg_row(const ClothDev& c, uint32_t row, Re
 
 // row_times_direction with the row's columns already in registers: every
 // load of the row (blocks, neighbours' z and p_old) is issued at once.
+// SMEM_A: the row's blocks come from the thread's shared-memory column.
+template <bool SMEM_A>
 __device__ __forceinline__ f3 reg_row_times_direction(const ClothDev& c, const RegRow& rr, const float* z,
-                                                      const float* pold, float beta, bool first)
+                                                      const float* pold, float beta, bool first, const float* sa,
+                                                      uint32_t B, uint32_t tid)
 {
     const uint32_t n = c.n;
     f3 acc = zero3();
 #pragma unroll
     for (int k = 0; k < kRegCols; ++k) {
         if ((uint32_t)k < rr.deg) {
-            const m3 a = block_at(c, rr.base + 32u * k);
+            const m3 a = SMEM_A ? smem_block(sa, (uint32_t)k, B, tid) : block_at(c, rr.base + 32u * k);
             const uint32_t j = rr.col[k];
             const f3 zj = ld3_l2(z, n, j);
             const f3 pj = first ? zj : zj + beta * ld3_l2(pold, n, j);
@@ -237,9 +261,14 @@ __device__ __forceinline__ f3 reg_row_times_direction(const ClothDev& c, const R
 // thread owns at most one row of at most kRegCols blocks and keeps its
 // columns and its x, r, z, p and P^-1 in registers for the whole solve;
 // only what neighbours read (z, p) and the solution go to memory.
-template <int DOT, bool ONE_ROW>
+// SMEM_A (one-row form only): the CTA's rows' blocks are copied into shared
+// memory at the start, [slot][component][thread], and every later product
+// reads them there; only the neighbours' z and p come from L2.
+template <int DOT, bool ONE_ROW, bool SMEM_A>
 __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ ClothDev c, GridBarrier* bar)
 {
+    extern __shared__ float smem_a[];
+    const uint32_t B = blockDim.x, tid = threadIdx.x;
     typedef DotT<DOT> D;
     typedef typename D::T T;
     StepScalars* sc = c.sc;
@@ -258,6 +287,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ C
     RegRow rr;
     f3 x = zero3(), r = zero3(), z = zero3(), pv = zero3(), p = zero3();
     if (ONE_ROW && act) load_reg_row(c, first_row, rr);
+    if (SMEM_A && act) stage_row_blocks(c, rr.base, rr.deg, smem_a, B, tid);
 
     // x0 = S m_x, r = S (b - A x0), z = S P^-1 r (cloth_force_solver.cpp:90-100)
     T v2[2] = {D::zero(), D::zero()};
@@ -323,7 +353,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ C
             if (ONE_ROW) {
                 if (act) {
                     p = first ? z : z + beta * p;
-                    const f3 ap = reg_row_times_direction(c, rr, c.z, pold, beta, first);
+                    const f3 ap = reg_row_times_direction<SMEM_A>(c, rr, c.z, pold, beta, first, smem_a, B, tid);
                     s = Si ? ap : zero3();
                     st3(pnew, n, first_row, p);
                     v1[0] = D::add_term(v1[0], p, s);
@@ -397,9 +427,10 @@ timeout:
 }
 
 template <int DOT>
-const void* grid_kernel(bool one_row)
+const void* grid_kernel(bool one_row, bool smem_a)
 {
-    return one_row ? (const void*)k_grid_cg<DOT, true> : (const void*)k_grid_cg<DOT, false>;
+    if (!one_row) return (const void*)k_grid_cg<DOT, false, false>;
+    return smem_a ? (const void*)k_grid_cg<DOT, true, true> : (const void*)k_grid_cg<DOT, true, false>;
 }
 
 // ---------------------------------------------------------------------------
@@ -450,13 +481,7 @@ __device__ __forceinline__ void st_rec(float4* rec, uint32_t j, f3 r, f3 s, f3 p
 
 __device__ __forceinline__ f3 hadamard(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
 
-// Block k of a thread's row kept in shared memory, [slot][component][thread].
-__device__ __forceinline__ m3 smem_block(const float* sa, uint32_t k, uint32_t B, uint32_t tid)
-{
-    const uint32_t o = k * 9u * B + tid;
-    return m3{f3{sa[o], sa[o + B], sa[o + 2 * B]}, f3{sa[o + 3 * B], sa[o + 4 * B], sa[o + 5 * B]},
-              f3{sa[o + 6 * B], sa[o + 7 * B], sa[o + 8 * B]}};
-}
+
 
 // The direction of this pass at a vertex, from its record of the previous
 // pass: the owner evaluates exactly this for its own row.
@@ -603,15 +628,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
     RegRow rr;
     f3 x = zero3(), r = zero3(), s = zero3(), p = zero3(), sp = zero3();
     if (ONE_ROW && act) load_reg_row(c, first_row, rr);
-    if (SMEM_A && act) {
-        // the row's blocks into shared memory, once for the whole solve
-#pragma unroll 1
-        for (uint32_t k = 0; k < rr.deg; ++k) {
-            const uint32_t g = rr.base + 32u * k, o = k * 9u * B + tid;
-#pragma unroll
-            for (uint32_t q = 0; q < 9; ++q) smem_a[o + q * B] = c.vals[(size_t)q * c.E + g];
-        }
-    }
+    if (SMEM_A && act) stage_row_blocks(c, rr.base, rr.deg, smem_a, B, tid);
 
     // x0 = S m_x, r = S (b - A x0), b_delta, delta = r.S P^-1 r
     // (cloth_force_solver.cpp:90-100); record 0 holds r with s = p = 0.
@@ -798,7 +815,7 @@ GridCgShape grid_cg_shape(uint32_t n, int device, bool fused)
         g.blocks = (int)((n + g.threads - 1) / g.threads);
     } else {
         int per_sm = 1;
-        const void* fn = fused ? (const void*)k_grid_cg_fused<2, false, false> : (const void*)k_grid_cg<2, false>;
+        const void* fn = fused ? (const void*)k_grid_cg_fused<2, false, false> : (const void*)k_grid_cg<2, false, false>;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMaxBlock, 0) != cudaSuccess ||
             per_sm < 1) {
             cudaGetLastError();
@@ -826,7 +843,17 @@ cudaError_t launch_grid_cg(const ClothDev& c, int dot, GridBarrier* bar, cudaStr
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const void* fn = dot == 2 ? grid_kernel<2>(one_row) : dot == 1 ? grid_kernel<1>(one_row) : grid_kernel<0>(one_row);
+    // the rows' blocks in shared memory when they fit beside the static
+    // shared memory of the reductions
+    const size_t smem = (size_t)c.max_deg * 9 * sizeof(float) * (size_t)g.threads;
+    const bool smem_a = one_row && smem + 4096 <= kSmemLimit;
+    const void* fn = dot == 2 ? grid_kernel<2>(one_row, smem_a)
+                   : dot == 1 ? grid_kernel<1>(one_row, smem_a) : grid_kernel<0>(one_row, smem_a);
+    if (smem_a) {
+        cudaError_t ea = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (ea != cudaSuccess) return ea;
+        cfg.dynamicSmemBytes = smem;
+    }
     void* args[2] = {const_cast<ClothDev*>(&c), &bar};
     const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     count_launches(1);

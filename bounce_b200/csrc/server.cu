@@ -309,7 +309,8 @@ b3g_status b3g_server_tick(b3g_server* s, double now, b3g_server_tick_info* info
     std::vector<Request*> newly;
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        while (!s->ready.empty() && s->active.size() < s->cfg.max_active) {
+        // the slot limit counts the cloths admitted in this tick too
+        while (!s->ready.empty() && s->active.size() + newly.size() < s->cfg.max_active) {
             Request* r = s->ready.begin()->second;
             if (s->used + r->bytes > s->cfg.hbm_budget_bytes) break;
             s->ready.erase(s->ready.begin());

@@ -24,7 +24,7 @@ def rel_err(a, b):
 
 
 def oracle_floor_step(port, scene, ora, dt, stop_rule, tol, max_iter, dress=None):
-    """Positions after one step of clones of the oracle `ora` -- its whole
+    """Positions and velocities after one step of clones of the oracle `ora` -- its whole
     state: positions, velocities, CG warm start, body contacts with their
     impulses and the particles' proxies -- with compensated and with FP64
     dots.  Against `ora`'s own step they measure how far the same algorithm
@@ -45,7 +45,8 @@ def oracle_floor_step(port, scene, ora, dt, stop_rule, tol, max_iter, dress=None
         c.set_contacts(live, np.zeros(live.size, np.uint32), ca["impulses"][live])
         c.set_proxies(fat[:, :3], fat[:, 3:])
         c.step(dt)
-        out.append(c.state()["x"])
+        cs = c.state()
+        out.append({"x": cs["x"], "v": cs["v"]})
     return out
 
 

@@ -7,7 +7,7 @@ import sys
 import numpy as np
 import pytest
 
-from helpers import rel_err, system_blocks
+from helpers import oracle_floor_step, rel_err, system_blocks
 
 pytestmark = pytest.mark.gpu
 
@@ -113,7 +113,11 @@ def test_headline_in_contact_one_step(b3g, port):
        same positions, so the active contacts handed to the solver agree
        exactly.
      - CG iterations agree within +-1, positions within 1e-4 relative.
-     - Velocities agree within 1e-4 of the largest velocity.
+     - Velocities: at a 1e-4 stop two correct solvers whose dots round
+       differently part by about 2e-4 of the largest velocity.  The bound is
+       twice the oracle's own spread, measured by stepping clones of its whole
+       state with compensated and with FP64 dots, or 1e-4 where that is
+       larger.
      - The contacts alive after the step agree within 0.1%: a particle whose
        new fat AABB lies within rounding of the sphere's proxy may differ."""
     scene = b3g.sphere_scene(256)
@@ -133,6 +137,7 @@ def test_headline_in_contact_one_step(b3g, port):
     ora.set_proxies(lo, hi)
     assert ora.contacts()["count"] == live.size
 
+    clones = oracle_floor_step(port, scene, ora, scene.dt, opts.stop_rule, opts.tolerance, opts.max_iterations)
     g = gpu.step(scene.dt)
     o = ora.step(scene.dt)
     assert o["active_contacts"] > 10000, o["active_contacts"]
@@ -141,10 +146,11 @@ def test_headline_in_contact_one_step(b3g, port):
     gs, os_ = gpu.state(), ora.state()
     ex = rel_err(gs["x"], os_["x"])
     ev = rel_err(gs["v"], os_["v"])
+    floor_v = max(rel_err(c["v"], os_["v"]) for c in clones)
     print(f"in contact: {o['active_contacts']} active, iterations {g['iterations']}/{o['iterations']}, "
-          f"x rel {ex:.2e}, v rel {ev:.2e}")
+          f"x rel {ex:.2e}, v rel {ev:.2e}, oracle's own v spread {floor_v:.2e}")
     assert ex <= 1e-4, ex
-    assert ev <= 1e-4, ev
+    assert ev <= max(1e-4, 2.0 * floor_v), (ev, floor_v)
     ge = gpu.contacts()["exists"].astype(bool)
     oe = ora.contacts()["exists"].astype(bool)
     assert np.count_nonzero(ge != oe) <= max(2, oe.sum() // 1000), np.count_nonzero(ge != oe)

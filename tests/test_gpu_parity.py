@@ -272,7 +272,7 @@ def test_fused_cg_reference_rule_per_step(b3g, port, maker, dot):
         g = gpu.step(scene.dt)
         o = ora.step(scene.dt)
         xo = ora.state()["x"]
-        floor = max(rel_err(xc, xo) for xc in clones)
+        floor = max(rel_err(c["x"], xo) for c in clones)
         assert abs(g["iterations"] - o["iterations"]) <= 1, (step, g["iterations"], o["iterations"])
         err = rel_err(gpu.state()["x"], xo)
         assert err <= max(2e-4, 2.0 * floor), (step, err, floor)

@@ -76,6 +76,21 @@ def test_admission_respects_the_budget(b3g):
     assert st["p99_step_ms"] >= st["p50_step_ms"] > 0
 
 
+def test_admission_respects_the_slot_limit(b3g):
+    """More prepared requests than slots, all admissible by memory: one tick
+    admits at most max_active of them, and every request still completes."""
+    scenes = [b3g.plain_scene(16, seed=60 + k) for k in range(12)]
+    srv = b3g.Server(budget_bytes=1 << 34, max_active=4)
+    ids = [srv.submit_scene(sc, steps=3) for sc in scenes]
+    _wait_prepared(srv, ids)
+    t = srv.tick(0.0)
+    assert t["active"] <= 4 and t["admitted"] <= 4, t
+    srv.drain()
+    st = srv.stats()
+    assert st["completed"] == len(scenes)
+    assert st["peak_active"] <= 4
+
+
 def test_oversized_request_is_rejected(b3g):
     srv = b3g.Server(budget_bytes=1 << 20, max_active=4)
     rid = srv.submit_scene(b3g.plain_scene(64), steps=1)
