@@ -72,6 +72,16 @@ def port_lib():
         L.oc_set_friction.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
         L.oc_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_set_contacts.argtypes = [C.c_void_p, C.c_uint32, _u32p, _u32p, _f32p]
+        L.oc_add_body.restype = C.c_int
+        L.oc_add_body.argtypes = [C.c_void_p, _f32p]
+        L.oc_set_body.argtypes = [C.c_void_p, C.c_uint32, _f32p]
+        L.oc_get_body.argtypes = [C.c_void_p, C.c_uint32, _f32p]
+        L.oc_add_body_shape.restype = C.c_int
+        L.oc_add_body_shape.argtypes = [C.c_void_p, C.c_uint32, C.c_int, _f32p, C.c_uint32, C.c_uint32, C.c_float,
+                                        C.c_float]
+        L.oc_set_shape_proxy.argtypes = [C.c_void_p, C.c_uint32, _f32p, _f32p]
+        L.oc_set_report_order.argtypes = [C.c_void_p, _u32p, C.c_uint32]
+        L.oc_get_shape_proxy.argtypes = [C.c_void_p, C.c_uint32, _f32p, _f32p]
         L.oc_set_proxies.argtypes = [C.c_void_p, _f32p, _f32p]
         for name in ("oc_apply_force", "oc_apply_translation", "oc_set_position", "oc_set_velocity"):
             getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, _f32p]
@@ -137,6 +147,19 @@ def ref_lib():
         L.ref_cloth_set_gravity.argtypes = [C.c_void_p, _f32p]
         L.ref_cloth_set_type.argtypes = [C.c_void_p, C.c_uint32, C.c_int]
         L.ref_cloth_set_radius.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
+        L.ref_cloth_add_body.restype = C.c_uint32
+        L.ref_cloth_add_body.argtypes = [C.c_void_p, C.c_int, _f32p, _f32p, _f32p, _f32p]
+        L.ref_cloth_add_body_shape.restype = C.c_uint32
+        L.ref_cloth_add_body_shape.argtypes = [C.c_void_p, C.c_uint32, C.c_int, _f32p, C.c_float, C.c_float, C.c_float]
+        L.ref_cloth_add_body_hull.restype = C.c_uint32
+        L.ref_cloth_add_body_hull.argtypes = [C.c_void_p, C.c_uint32, _f32p, C.c_uint32, C.c_float, C.c_float, _f32p,
+                                              _f32p, C.POINTER(C.c_uint32)]
+        L.ref_cloth_get_body.argtypes = [C.c_void_p, C.c_uint32, _f32p]
+        L.ref_cloth_get_shape_proxy.argtypes = [C.c_void_p, C.c_uint32, _f32p, _f32p]
+        L.ref_world_step.argtypes = [C.c_void_p, C.c_float, C.c_uint32, C.c_uint32]
+        L.ref_world_report_order.restype = C.c_uint32
+        L.ref_world_report_order.argtypes = [C.c_void_p, _u32p]
+        L.ref_world_set_gravity.argtypes = [C.c_void_p, _f32p]
         L.ref_cloth_set_friction.argtypes = [C.c_void_p, C.c_uint32, C.c_float]
         for name in ("ref_cloth_apply_force", "ref_cloth_apply_translation", "ref_cloth_set_position",
                      "ref_cloth_set_velocity"):
@@ -341,6 +364,36 @@ class PortCloth(_Base):
         self.L.oc_set_contacts(self.h, p.size, p if p.size else np.zeros(1, np.uint32),
                                s if s.size else np.zeros(1, np.uint32), imp if imp.size else np.zeros(3, np.float32))
 
+    def add_body(self, desc):
+        """A body (55-float state, as RefCloth.body() returns) for body shapes."""
+        return int(self.L.oc_add_body(self.h, np.ascontiguousarray(desc, np.float32)))
+
+    def set_body(self, body, desc):
+        self.L.oc_set_body(self.h, body, np.ascontiguousarray(desc, np.float32))
+
+    def body(self, body):
+        d = np.zeros(55, np.float32)
+        self.L.oc_get_body(self.h, body, d)
+        return d
+
+    def add_body_shape(self, body, kind, geom, radius, friction, nv=0, nf=0):
+        """kind 0 sphere (centre), 1 capsule (ends), 2 hull (vertices then
+        planes); geometry in the body's frame."""
+        g = np.ascontiguousarray(geom, np.float32).reshape(-1)
+        return int(self.L.oc_add_body_shape(self.h, body, kind, g, nv, nf, radius, friction))
+
+    def set_report_order(self, order):
+        o = np.ascontiguousarray(order, np.uint32)
+        self.L.oc_set_report_order(self.h, o if o.size else np.zeros(1, np.uint32), o.size)
+
+    def set_shape_proxy(self, shape, lo, hi):
+        self.L.oc_set_shape_proxy(self.h, shape, np.asarray(lo, np.float32), np.asarray(hi, np.float32))
+
+    def shape_proxy(self, shape):
+        lo, hi = np.zeros(3, np.float32), np.zeros(3, np.float32)
+        self.L.oc_get_shape_proxy(self.h, shape, lo, hi)
+        return lo, hi
+
     def set_proxies(self, lo, hi):
         """Overwrite the particles' fat AABBs (n x 3 each)."""
         self.L.oc_set_proxies(self.h, np.ascontiguousarray(lo, np.float32).reshape(-1),
@@ -455,6 +508,47 @@ class RefCloth(_Base):
 
     def set_friction(self, vertex, friction):
         self.L.ref_cloth_set_friction(self.h, vertex, friction)
+
+    def add_body(self, type_, position, orientation=(0.0, 0.0, 0.0, 1.0), velocity=(0.0, 0.0, 0.0),
+                 angular_velocity=(0.0, 0.0, 0.0)):
+        f = lambda a: np.asarray(a, np.float32)
+        return int(self.L.ref_cloth_add_body(self.h, type_, f(position), f(orientation), f(velocity),
+                                             f(angular_velocity)))
+
+    def add_body_shape(self, body, kind, geom, radius, density, friction):
+        return int(self.L.ref_cloth_add_body_shape(self.h, body, kind, np.asarray(geom, np.float32), radius, density,
+                                                   friction))
+
+    def add_body_hull(self, body, points, density, friction):
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1)
+        verts = np.zeros(3 * 256, np.float32)
+        planes = np.zeros(4 * 256, np.float32)
+        nf = C.c_uint32(0)
+        nv = self.L.ref_cloth_add_body_hull(self.h, body, pts, pts.size // 3, density, friction, verts, planes,
+                                            C.byref(nf))
+        return verts[:3 * nv].reshape(-1, 3).copy(), planes[:4 * nf.value].reshape(-1, 4).copy()
+
+    def body(self, body):
+        d = np.zeros(55, np.float32)
+        self.L.ref_cloth_get_body(self.h, body, d)
+        return d
+
+    def shape_proxy(self, shape):
+        lo, hi = np.zeros(3, np.float32), np.zeros(3, np.float32)
+        self.L.ref_cloth_get_shape_proxy(self.h, shape, lo, hi)
+        return lo, hi
+
+    def report_order(self):
+        """The world's shapes in its query's report order."""
+        o = np.zeros(64, np.uint32)
+        m = self.L.ref_world_report_order(self.h, o)
+        return o[:m].copy()
+
+    def world_step(self, dt, velocity_iterations=8, position_iterations=2):
+        self.L.ref_world_step(self.h, dt, velocity_iterations, position_iterations)
+
+    def set_world_gravity(self, g):
+        self.L.ref_world_set_gravity(self.h, np.asarray(g, np.float32))
 
     def apply_force(self, vertex, f):
         self.L.ref_cloth_apply_force(self.h, vertex, np.asarray(f, np.float32))

@@ -158,8 +158,32 @@ typedef struct {
 
 enum { SHAPE_SPHERE = 0, SHAPE_CAPSULE = 1, SHAPE_HULL = 2 };
 
+/* b3Quat (include/bounce/common/math/quat.h) */
+typedef struct { float x, y, z, w; } quat;
+
+/* The state of a b3Body a collider belongs to (include/bounce/dynamics/
+ * body.h): type (0 static, 1 kinematic, 2 dynamic), transform m_xf, sweep
+ * (local center, world centers and orientations at the start and end of
+ * the world step), velocities, inverse mass, local and world inverse
+ * inertia.  The caller's world owns it; the cloth step reads it and, as the
+ * reference's contact solver does, writes velocities, the sweep's end state
+ * and the synchronised transform back. */
+typedef struct {
+    int type;
+    m33 R;
+    v3 p;
+    v3 lc, c0, c;
+    quat q0, q;
+    v3 v, w;
+    float im;
+    m33 ii, wii;
+} body_t;
+
 typedef struct {
     int kind;
+    int body;          /* -1: a static shape given in the world frame, whose body sits at the
+                          sphere's centre (spheres) or the origin (others); else the index of a
+                          body, with the geometry below in that body's frame */
     v3 center;         /* sphere */
     v3 a, b;           /* capsule segment, world frame (the body at the origin) */
     v3* hv;            /* hull: vertices and face planes (normal, offset), world frame (body at the origin) */
@@ -214,6 +238,10 @@ struct oc_cloth {
     v3 gravity;
     sphere_t* spheres;
     uint32_t nsphere;
+    body_t* bodies;
+    uint32_t nbody;
+    uint32_t report[WO_MAX]; /* shapes in a world query's report order, when given */
+    int has_report;
 
     /* body-contact list stored tail first: element [ncontact-1] is the list head */
     contact_t* contacts;
@@ -479,7 +507,7 @@ void oc_destroy(oc_cloth* c)
     for (uint32_t k = 0; k < c->nsphere; ++k) {
         free(c->spheres[k].hv); free(c->spheres[k].hn); free(c->spheres[k].ho);
     }
-    free(c->forces); free(c->spheres); free(c->contacts);
+    free(c->forces); free(c->spheres); free(c->contacts); free(c->bodies);
     lrows_free(c->dfdx, c->n);
     lrows_free(c->dfdv, c->n);
     free(c->a_rowptr); free(c->a_cols); free(c->a_vals);
@@ -681,6 +709,7 @@ int oc_add_sphere(oc_cloth* c, const float* center, float radius, float friction
     sphere_t* s = c->spheres + c->nsphere;
     memset(s, 0, sizeof(*s));
     s->kind = SHAPE_SPHERE;
+    s->body = -1;
     s->center = V(center[0], center[1], center[2]);
     s->radius = radius;
     s->friction = friction;
@@ -700,6 +729,7 @@ int oc_add_capsule(oc_cloth* c, const float* a, const float* b, float radius, fl
     sphere_t* s = c->spheres + c->nsphere;
     memset(s, 0, sizeof(*s));
     s->kind = SHAPE_CAPSULE;
+    s->body = -1;
     s->a = V(a[0], a[1], a[2]);
     s->b = V(b[0], b[1], b[2]);
     s->radius = radius;
@@ -735,6 +765,7 @@ int oc_add_hull(oc_cloth* c, const float* vertices, uint32_t nv, const float* pl
     sphere_t* s = c->spheres + c->nsphere;
     memset(s, 0, sizeof(*s));
     s->kind = SHAPE_HULL;
+    s->body = -1;
     s->radius = 0.0f;
     s->friction = friction;
     s->nhv = nv;
@@ -1938,6 +1969,361 @@ static void contact_update(oc_cloth* c, contact_t* k)
     k->tangent2 = vcross(k->tangent1, k->normal1);
 }
 
+/* ------------------------------------------------------------------------ */
+/* colliders on bodies: transforms, shape tests, the body API               */
+/* ------------------------------------------------------------------------ */
+
+/* b3Mul / b3MulT of a matrix, a transform, a quaternion (mat33.h:129-160,
+ * transform.h:74-110, quat.h:225-238), in the reference's float order. */
+static inline v3 mmul_t(m33 a, v3 v) { return V(vdot(a.x, v), vdot(a.y, v), vdot(a.z, v)); }
+static inline v3 xmul(m33 R, v3 p, v3 v) { return vadd(mmul(R, v), p); }
+static inline v3 xmul_t(m33 R, v3 p, v3 v) { return mmul_t(R, vsub(v, p)); }
+static inline m33 mmul3(m33 a, m33 b) { return M3(mmul(a, b.x), mmul(a, b.y), mmul(a, b.z)); }
+static inline m33 mtrans(m33 a) { return M3(V(a.x.x, a.y.x, a.z.x), V(a.x.y, a.y.y, a.z.y), V(a.x.z, a.y.z, a.z.z)); }
+static inline quat Qt(float x, float y, float z, float w) { quat q = {x, y, z, w}; return q; }
+static inline quat qmul(quat a, quat b) /* quat.h:172-180 */
+{
+    return Qt(a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y, a.w * b.y + a.y * b.w + a.z * b.x - a.x * b.z,
+              a.w * b.z + a.z * b.w + a.x * b.y - a.y * b.x, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z);
+}
+static inline void qnormalize(quat* q) /* b3Quat::Normalize (quat.h:88-100) */
+{
+    float length = sqrtf(q->x * q->x + q->y * q->y + q->z * q->z + q->w * q->w);
+    if (length > kEps) {
+        float s = 1.0f / length;
+        q->x *= s; q->y *= s; q->z *= s; q->w *= s;
+    }
+}
+static inline m33 qmat(quat q) /* b3QuatMat33 (quat.h:306-318) */
+{
+    float x = q.x, y = q.y, z = q.z, w = q.w;
+    float x2 = x + x, y2 = y + y, z2 = z + z;
+    float xx = x * x2, xy = x * y2, xz = x * z2;
+    float yy = y * y2, yz = y * z2, zz = z * z2;
+    float wx = w * x2, wy = w * y2, wz = w * z2;
+    return M3(V(1.0f - (yy + zz), xy + wz, xz - wy), V(xy - wz, 1.0f - (xx + zz), yz + wx),
+              V(xz + wy, yz - wx, 1.0f - (xx + yy)));
+}
+static inline v3 qrot(quat q, v3 v) /* b3Mul(b3Quat, b3Vec3) (quat.h:225-232) */
+{
+    v3 qv = V(q.x, q.y, q.z);
+    v3 t = vscale(2.0f, vcross(qv, v));
+    return vadd(vadd(v, vscale(q.w, t)), vcross(qv, t));
+}
+static inline quat qderiv(quat q, v3 w) /* b3Derivative (time_step.h:105-109) */
+{
+    return qmul(Qt(0.5f * w.x, 0.5f * w.y, 0.5f * w.z, 0.0f), q);
+}
+
+/* The body a shape sits on; a world-frame shape's implicit static body. */
+static body_t shape_body(const oc_cloth* c, const sphere_t* sp)
+{
+    if (sp->body >= 0) return c->bodies[sp->body];
+    body_t b;
+    memset(&b, 0, sizeof(b));
+    b.R = mident();
+    b.p = sp->kind == SHAPE_SPHERE ? sp->center : vzero();
+    b.c0 = b.c = b.p;
+    b.q0 = b.q = Qt(0.0f, 0.0f, 0.0f, 1.0f);
+    return b;
+}
+
+/* b3Shape::ComputeAABB with a transform (sphere_shape.cpp:53-59,
+ * capsule_shape.cpp:130-137, hull_shape.cpp:162-166 with b3AABB3::Set). */
+static void shape_aabb(const sphere_t* sp, m33 R, v3 p, v3* lo, v3* hi)
+{
+    v3 r = V(sp->radius, sp->radius, sp->radius);
+    if (sp->kind == SHAPE_SPHERE) {
+        v3 ctr = xmul(R, p, sp->center);
+        *lo = vsub(ctr, r);
+        *hi = vadd(ctr, r);
+    } else if (sp->kind == SHAPE_CAPSULE) {
+        v3 c1 = xmul(R, p, sp->a), c2 = xmul(R, p, sp->b);
+        *lo = vsub(vmin(c1, c2), r);
+        *hi = vadd(vmax(c1, c2), r);
+    } else {
+        v3 l = xmul(R, p, sp->hv[0]), h = l;
+        for (uint32_t i = 1; i < sp->nhv; ++i) {
+            v3 w = xmul(R, p, sp->hv[i]);
+            l = vmin(l, w);
+            h = vmax(h, w);
+        }
+        *lo = vsub(l, r);
+        *hi = vadd(h, r);
+    }
+}
+
+/* b3GJK (gjk.cpp:579-740) between a hull on a body (transform R, p) and a
+ * point in the world frame: supports in the hull's frame
+ * (b3MulT(xf1.rotation, -d)), vertices mapped by b3Mul(xf1, v). */
+static float gjk_hull_point_xf(const sphere_t* h, m33 R, v3 p, v3 Q, v3* p1, v3* p2)
+{
+    gjk_simplex s;
+    memset(&s, 0, sizeof(s));
+    s.v[0].point1 = xmul(R, p, h->hv[0]);
+    s.v[0].point2 = xf_mul(Q);
+    s.v[0].point = vsub(s.v[0].point2, s.v[0].point1);
+    s.v[0].weight = 1.0f;
+    s.count = 1;
+    uint32_t save1[4], save2[4], saveCount = 0;
+    const v3 origin = vzero();
+    uint32_t iter = 0;
+    while (iter < 20) {
+        saveCount = s.count;
+        for (uint32_t i = 0; i < saveCount; ++i) {
+            save1[i] = s.v[i].index1;
+            save2[i] = s.v[i].index2;
+        }
+        if (s.count == 2) gsolve2(&s, origin);
+        else if (s.count == 3) gsolve3(&s, origin);
+        else if (s.count == 4) gsolve4(&s, origin);
+        if (s.count == 4) break;
+        (void)gclosest(&s);
+        v3 d = gsearch(&s, origin);
+        if (vdot(d, d) < kEps * kEps) break;
+        gjk_vertex* vx = s.v + s.count;
+        v3 dl = mmul_t(R, vneg(d));
+        uint32_t best = 0;
+        float bestp = vdot(dl, h->hv[0]);
+        for (uint32_t i = 1; i < h->nhv; ++i) {
+            float pr = vdot(dl, h->hv[i]);
+            if (pr > bestp) {
+                best = i;
+                bestp = pr;
+            }
+        }
+        vx->index1 = best;
+        vx->point1 = xmul(R, p, h->hv[best]);
+        vx->index2 = 0;
+        vx->point2 = xf_mul(Q);
+        vx->point = vsub(vx->point2, vx->point1);
+        ++iter;
+        int duplicate = 0;
+        for (uint32_t i = 0; i < saveCount; ++i)
+            if (vx->index1 == save1[i] && vx->index2 == save2[i]) {
+                duplicate = 1;
+                break;
+            }
+        if (duplicate) break;
+        ++s.count;
+    }
+    gwitness(&s, p1, p2);
+    return vlength(vsub(*p1, *p2));
+}
+
+/* b3ParticleBodyContact::Update (cloth_particle_body_contact.cpp:24-47) for a
+ * shape on a body: TestSphere with the body's transform m_xf, the contact
+ * point stored in the body's frame (GetLocalPoint). */
+static void contact_update_body(oc_cloth* c, contact_t* k)
+{
+    const sphere_t* sp = c->spheres + k->shape;
+    const body_t* bd = c->bodies + sp->body;
+    m33 R = bd->R;
+    v3 p = bd->p;
+    uint32_t i = k->particle;
+    float radius = sp->radius + c->radius[i];
+    v3 Q = c->x[i];
+    v3 normal, point;
+    if (sp->kind == SHAPE_SPHERE) {
+        v3 center = xmul(R, p, sp->center);
+        float rr = radius * radius;
+        v3 d = vsub(Q, center);
+        float dd = vdot(d, d);
+        if (!(dd <= rr)) {
+            k->active = 0;
+            return;
+        }
+        float d_len = sqrtf(dd);
+        normal = V(0.0f, 1.0f, 0.0f);
+        if (d_len > kEps) normal = vdiv(d, d_len);
+        point = center;
+    } else if (sp->kind == SHAPE_HULL) {
+        v3 c1, c2;
+        float distance = gjk_hull_point_xf(sp, R, p, Q, &c1, &c2);
+        float total = sp->radius + c->radius[i];
+        if (distance > total) {
+            k->active = 0;
+            return;
+        }
+        if (distance > 0.0f) {
+            normal = vdiv(vsub(c2, c1), distance);
+            point = c1;
+        } else {
+            v3 support = xmul_t(R, p, Q);
+            uint32_t maxIndex = ~0u;
+            float maxSeparation = -FLT_MAX;
+            for (uint32_t f = 0; f < sp->nhf; ++f) {
+                float separation = vdot(sp->hn[f], support) - sp->ho[f];
+                if (separation > total) {
+                    k->active = 0;
+                    return;
+                }
+                if (separation > maxSeparation) {
+                    maxIndex = f;
+                    maxSeparation = separation;
+                }
+            }
+            v3 pn = mmul(R, sp->hn[maxIndex]);
+            float po = sp->ho[maxIndex] + vdot(pn, p);
+            float fraction = vdot(pn, Q) - po;
+            point = vsub(Q, vscale(fraction, pn));
+            normal = pn;
+        }
+    } else {
+        v3 A = xmul(R, p, sp->a), B = xmul(R, p, sp->b);
+        v3 AB = vsub(B, A);
+        float u = vdot(vsub(B, Q), AB);
+        float v = vdot(vsub(Q, A), AB);
+        if (v <= 0.0f || u <= 0.0f) {
+            v3 P = v <= 0.0f ? A : B;
+            v3 d = vsub(Q, P);
+            float dd = vdot(d, d);
+            if (dd > radius * radius) {
+                k->active = 0;
+                return;
+            }
+            normal = V(0.0f, 1.0f, 0.0f);
+            float len = sqrtf(dd);
+            if (len > kEps) normal = vdiv(d, len);
+            point = P;
+        } else {
+            float ss = vdot(AB, AB);
+            v3 P;
+            if (ss < kLinearSlop * kLinearSlop) P = A;
+            else P = vdiv(vadd(vscale(u, A), vscale(v, B)), ss);
+            v3 d = vsub(Q, P);
+            float dd = vdot(d, d);
+            if (dd > radius * radius) {
+                k->active = 0;
+                return;
+            }
+            v3 QA = vsub(A, Q);
+            v3 e = vcross(AB, QA);
+            v3 nn = vcross(AB, e);
+            if (vdot(nn, QA) < 0.0f) nn = vneg(nn);
+            float len = sqrtf(nn.x * nn.x + nn.y * nn.y + nn.z * nn.z);
+            if (len > kEps) {
+                float s1 = 1.0f / len;
+                nn = V(nn.x * s1, nn.y * s1, nn.z * s1);
+            }
+            normal = vneg(nn);
+            point = P;
+        }
+    }
+    k->active = 1;
+    k->normal1 = vneg(normal);
+    k->local_point2 = xmul_t(R, p, point);
+    k->tangent1 = vperp(k->normal1);
+    k->tangent2 = vcross(k->tangent1, k->normal1);
+}
+
+/* Body state as 55 floats: type, R (9, column-major), p, local center,
+ * world center 0, world center, orientation 0 (x y z w), orientation,
+ * linear and angular velocity, inverse mass, local inverse inertia (9),
+ * world inverse inertia (9). */
+static void body_read(body_t* b, const float* d)
+{
+    b->type = (int)d[0];
+    b->R = M3(V(d[1], d[2], d[3]), V(d[4], d[5], d[6]), V(d[7], d[8], d[9]));
+    b->p = V(d[10], d[11], d[12]);
+    b->lc = V(d[13], d[14], d[15]);
+    b->c0 = V(d[16], d[17], d[18]);
+    b->c = V(d[19], d[20], d[21]);
+    b->q0 = Qt(d[22], d[23], d[24], d[25]);
+    b->q = Qt(d[26], d[27], d[28], d[29]);
+    b->v = V(d[30], d[31], d[32]);
+    b->w = V(d[33], d[34], d[35]);
+    b->im = d[36];
+    b->ii = M3(V(d[37], d[38], d[39]), V(d[40], d[41], d[42]), V(d[43], d[44], d[45]));
+    b->wii = M3(V(d[46], d[47], d[48]), V(d[49], d[50], d[51]), V(d[52], d[53], d[54]));
+}
+
+static void put_v3(float* o, v3 v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; }
+
+static void body_write(const body_t* b, float* d)
+{
+    d[0] = (float)b->type;
+    put_v3(d + 1, b->R.x); put_v3(d + 4, b->R.y); put_v3(d + 7, b->R.z);
+    put_v3(d + 10, b->p); put_v3(d + 13, b->lc); put_v3(d + 16, b->c0); put_v3(d + 19, b->c);
+    d[22] = b->q0.x; d[23] = b->q0.y; d[24] = b->q0.z; d[25] = b->q0.w;
+    d[26] = b->q.x; d[27] = b->q.y; d[28] = b->q.z; d[29] = b->q.w;
+    put_v3(d + 30, b->v); put_v3(d + 33, b->w);
+    d[36] = b->im;
+    put_v3(d + 37, b->ii.x); put_v3(d + 40, b->ii.y); put_v3(d + 43, b->ii.z);
+    put_v3(d + 46, b->wii.x); put_v3(d + 49, b->wii.y); put_v3(d + 52, b->wii.z);
+}
+
+int oc_add_body(oc_cloth* c, const float* desc)
+{
+    c->bodies = (body_t*)realloc(c->bodies, (c->nbody + 1) * sizeof(body_t));
+    body_read(c->bodies + c->nbody, desc);
+    return (int)c->nbody++;
+}
+
+void oc_set_body(oc_cloth* c, uint32_t body, const float* desc) { body_read(c->bodies + body, desc); }
+void oc_get_body(const oc_cloth* c, uint32_t body, float* desc) { body_write(c->bodies + body, desc); }
+
+/* A shape on a body, its geometry in the body's frame (b3Body::CreateShape):
+ * sphere: centre (3 floats); capsule: the segment's ends (6); hull: nv
+ * vertices then nf planes (normal, offset).  Its proxy in the world
+ * broadphase starts as ComputeAABB(m_xf) fattened (broad_phase.cpp:78-90). */
+int oc_add_body_shape(oc_cloth* c, uint32_t body, int kind, const float* geom, uint32_t nv, uint32_t nf,
+                      float radius, float friction)
+{
+    c->spheres = (sphere_t*)realloc(c->spheres, (c->nsphere + 1) * sizeof(sphere_t));
+    sphere_t* s = c->spheres + c->nsphere;
+    memset(s, 0, sizeof(*s));
+    s->kind = kind;
+    s->body = (int)body;
+    s->radius = radius;
+    s->friction = friction;
+    if (kind == SHAPE_SPHERE) {
+        s->center = V(geom[0], geom[1], geom[2]);
+    } else if (kind == SHAPE_CAPSULE) {
+        s->a = V(geom[0], geom[1], geom[2]);
+        s->b = V(geom[3], geom[4], geom[5]);
+    } else {
+        s->nhv = nv;
+        s->nhf = nf;
+        s->hv = (v3*)malloc((nv ? nv : 1) * sizeof(v3));
+        s->hn = (v3*)malloc((nf ? nf : 1) * sizeof(v3));
+        s->ho = (float*)malloc((nf ? nf : 1) * sizeof(float));
+        for (uint32_t i = 0; i < nv; ++i) s->hv[i] = V(geom[3 * i], geom[3 * i + 1], geom[3 * i + 2]);
+        const float* pl = geom + 3 * (size_t)nv;
+        for (uint32_t i = 0; i < nf; ++i) {
+            s->hn[i] = V(pl[4 * i], pl[4 * i + 1], pl[4 * i + 2]);
+            s->ho[i] = pl[4 * i + 3];
+        }
+    }
+    const body_t* b = c->bodies + body;
+    v3 lo, hi, ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
+    shape_aabb(s, b->R, b->p, &lo, &hi);
+    s->fat_lo = vsub(lo, ext);
+    s->fat_hi = vadd(hi, ext);
+    return (int)c->nsphere++;
+}
+
+/* The order in which the caller's world query reports the shapes (its
+ * dynamic tree's order), replacing the one derived from inserting the
+ * proxies in creation order; count 0 returns to the derived one. */
+void oc_set_report_order(oc_cloth* c, const uint32_t* order, uint32_t count)
+{
+    c->has_report = count > 0;
+    for (uint32_t s = 0; s < count && s < WO_MAX; ++s) c->report[s] = order[s];
+}
+
+void oc_set_shape_proxy(oc_cloth* c, uint32_t shape, const float* lo, const float* hi)
+{
+    c->spheres[shape].fat_lo = V(lo[0], lo[1], lo[2]);
+    c->spheres[shape].fat_hi = V(hi[0], hi[1], hi[2]);
+}
+
+void oc_get_shape_proxy(const oc_cloth* c, uint32_t shape, float* lo, float* hi)
+{
+    put_v3(lo, c->spheres[shape].fat_lo);
+    put_v3(hi, c->spheres[shape].fat_hi);
+}
+
 /* UpdateBodyContacts (cloth_contact_manager.cpp:277-315). */
 static void update_body_contacts(oc_cloth* c)
 {
@@ -1947,10 +2333,13 @@ static void update_body_contacts(oc_cloth* c)
     for (uint32_t q = n; q-- > 0;) {
         contact_t* k = c->contacts + q;
         keep[q] = 0;
-        if (c->type[k->particle] != OC_DYNAMIC) continue; /* the body is static too */
         const sphere_t* sp = c->spheres + k->shape;
+        /* neither side dynamic: the pair must not collide */
+        const int body_dynamic = sp->body >= 0 && c->bodies[sp->body].type == 2;
+        if (c->type[k->particle] != OC_DYNAMIC && !body_dynamic) continue;
         if (!aabb_overlap(c->fat_lo[k->particle], c->fat_hi[k->particle], sp->fat_lo, sp->fat_hi)) continue;
-        contact_update(c, k);
+        if (sp->body >= 0) contact_update_body(c, k);
+        else contact_update(c, k);
         keep[q] = 1;
     }
     uint32_t w = 0;
@@ -1978,6 +2367,8 @@ static void find_new_body_contacts(oc_cloth* c)
         whi[s][0] = c->spheres[s].fat_hi.x; whi[s][1] = c->spheres[s].fat_hi.y; whi[s][2] = c->spheres[s].fat_hi.z;
     }
     world_report_order(wlo, whi, c->nsphere, report);
+    if (c->has_report)
+        for (uint32_t s = 0; s < c->nsphere && s < WO_MAX; ++s) report[s] = c->report[s];
     for (uint32_t k = 0; k < c->n; ++k) {
         uint32_t i = c->order[k];
         if (c->type[i] != OC_DYNAMIC) continue;
@@ -2462,6 +2853,318 @@ static void solve_contacts(oc_cloth* c, float h, uint32_t vel_iters, uint32_t po
     free(tc);
 }
 
+/* b3BroadPhase::MoveProxy (broad_phase.cpp:99-149) on a shape's proxy in the
+ * world broadphase. */
+static void move_shape_proxy(sphere_t* sp, v3 lo, v3 hi, v3 displacement)
+{
+    v3 flo = sp->fat_lo, fhi = sp->fat_hi;
+    int contains = flo.x <= lo.x && lo.x <= fhi.x && flo.y <= lo.y && lo.y <= fhi.y && flo.z <= lo.z &&
+                   lo.z <= fhi.z && flo.x <= hi.x && hi.x <= fhi.x && flo.y <= hi.y && hi.y <= fhi.y &&
+                   flo.z <= hi.z && hi.z <= fhi.z;
+    if (contains) return;
+    v3 ext = V(kAabbExtension, kAabbExtension, kAabbExtension);
+    lo = vsub(lo, ext);
+    hi = vadd(hi, ext);
+    v3 d = vscale(kAabbMultiplier, displacement);
+    if (d.x < 0.0f) lo.x += d.x; else hi.x += d.x;
+    if (d.y < 0.0f) lo.y += d.y; else hi.y += d.y;
+    if (d.z < 0.0f) lo.z += d.z; else hi.z += d.z;
+    sp->fat_lo = lo;
+    sp->fat_hi = hi;
+}
+
+/* b3Sweep::GetTransform (transform.h:224-234) */
+static void sweep_xf(const body_t* b, float t, m33* R, v3* p)
+{
+    v3 cc = vadd(vscale(1.0f - t, b->c0), vscale(t, b->c));
+    quat q0 = b->q0, q1 = b->q;
+    quat q = Qt((1.0f - t) * q0.x + t * q1.x, (1.0f - t) * q0.y + t * q1.y, (1.0f - t) * q0.z + t * q1.z,
+                (1.0f - t) * q0.w + t * q1.w);
+    qnormalize(&q);
+    *R = qmat(q);
+    *p = vsub(cc, qrot(q, b->lc));
+}
+
+/* After the position solve, each non-static body with an active contact
+ * (cloth_solver.cpp:167-181): SynchronizeTransform (body.cpp:176-179), the
+ * world inverse inertia (b3RotateToFrame, time_step.h:86-89) and
+ * SynchronizeShapes (body.cpp:181-202) for its shapes. */
+static void sync_body(oc_cloth* c, uint32_t body)
+{
+    body_t* b = c->bodies + body;
+    if (b->type == 0) return;
+    sweep_xf(b, 1.0f, &b->R, &b->p);
+    b->wii = mmul3(mmul3(b->R, b->ii), mtrans(b->R));
+    m33 R1;
+    v3 p1;
+    sweep_xf(b, 0.0f, &R1, &p1);
+    v3 disp = vsub(b->p, p1);
+    for (uint32_t s = 0; s < c->nsphere; ++s) {
+        sphere_t* sp = c->spheres + s;
+        if (sp->body != (int)body) continue;
+        v3 lo1, hi1, lo2, hi2;
+        shape_aabb(sp, R1, p1, &lo1, &hi1);
+        shape_aabb(sp, b->R, b->p, &lo2, &hi2);
+        move_shape_proxy(sp, vmin(lo1, lo2), vmax(hi1, hi2), disp);
+    }
+}
+
+typedef struct {
+    uint32_t index;
+    int body;  /* -1: an implicit static body */
+    float mA, mB, friction, normal_mass;
+    m33 iA, iB;
+    float tm_xx, tm_xy, tm_yx, tm_yy;
+    v3 normal, tangent1, tangent2, point, rA, rB;
+    float normal_impulse;
+    v2 tangent_impulse;
+    float radius_a, radius_b;
+    v3 lcB, normal_a, lpA, lpB;
+    body_t fixed;  /* the implicit static body */
+    contact_t* src;
+} gbc_t;
+
+static inline body_t* gbody(oc_cloth* c, gbc_t* x) { return x->body >= 0 ? c->bodies + x->body : &x->fixed; }
+
+/* b3Body::SetLinearVelocity / SetAngularVelocity (body.h) skip static bodies */
+static inline void set_body_velocity(body_t* b, v3 v, v3 w)
+{
+    if (b->type == 0) return;
+    b->v = v;
+    b->w = w;
+}
+
+/* The contact part of b3ClothSolver::Solve (cloth_solver.cpp:103-182) with
+ * b3ClothContactSolver's body-contact functions in full
+ * (cloth_contact_solver.cpp:54-177, 264-307, 388-472, 598-718): body
+ * velocities and sweeps are read and written per contact, in list order. */
+static void solve_contacts_bodies(oc_cloth* c, float h, uint32_t vel_iters, uint32_t pos_iters, v3* pos,
+                                  v3* vel, uint32_t* nactive, uint32_t* ntactive)
+{
+    uint32_t nt = 0;
+    for (uint32_t q = c->ntc; q-- > 0;) nt += c->tcs[q].active != 0;
+    *ntactive = nt;
+    tc_t* tc = (tc_t*)calloc(nt + 1, sizeof(tc_t));
+    {
+        uint32_t w = 0;
+        for (uint32_t q = c->ntc; q-- > 0;)
+            if (c->tcs[q].active) tc_init(c, tc + w++, c->tcs + q, pos);
+    }
+    uint32_t na = 0;
+    for (uint32_t q = c->ncontact; q-- > 0;) na += c->contacts[q].active != 0;
+    *nactive = na;
+    gbc_t* bc = (gbc_t*)calloc(na + 1, sizeof(gbc_t));
+    uint32_t w = 0;
+    for (uint32_t q = c->ncontact; q-- > 0;) {
+        contact_t* k = c->contacts + q;
+        if (!k->active) continue;
+        gbc_t* x = bc + w++;
+        const sphere_t* sp = c->spheres + k->shape;
+        uint32_t i = k->particle;
+        x->src = k;
+        x->body = sp->body;
+        x->fixed = shape_body(c, sp);
+        const body_t* b = gbody(c, x);
+        x->index = c->solver_of_vertex[i];
+        x->mA = c->type[i] == OC_STATIC ? 0.0f : c->inv_mass[i];
+        x->mB = b->im;
+        x->iA = mzero();
+        x->iB = b->wii;
+        x->friction = sqrtf(c->friction[i] * sp->friction);
+        x->radius_a = c->radius[i];
+        x->radius_b = sp->radius;
+        x->lcB = b->lc;
+        x->normal_a = k->normal1;
+        x->lpA = vzero();
+        x->lpB = k->local_point2;
+    }
+    for (uint32_t q = 0; q < na; ++q) {
+        gbc_t* x = bc + q;
+        const body_t* b = gbody(c, x);
+        float mA = x->mA, mB = x->mB;
+        m33 iA = x->iA, iB = x->iB;
+        v3 xA = pos[x->index], xB = b->c;
+        m33 RA = qmat(Qt(0.0f, 0.0f, 0.0f, 1.0f));
+        v3 pA = vsub(xA, mmul(RA, vzero()));
+        m33 RB = qmat(b->q);
+        v3 pB = vsub(xB, mmul(RB, x->lcB));
+        /* b3ParticleBodyContactWorldPoint::Initialize (cloth_particle_body_contact.cpp:49-62) */
+        v3 nA = x->src->normal1;
+        v3 cA = xmul(RA, pA, x->lpA);
+        v3 cB = xmul(RB, pB, x->lpB);
+        v3 wA = vadd(cA, vscale(x->radius_a, nA));
+        v3 wB = vsub(cB, vscale(x->radius_b, nA));
+        x->point = vscale(0.5f, vadd(wA, wB));
+        x->normal = nA;
+        x->tangent1 = x->src->tangent1;
+        x->tangent2 = x->src->tangent2;
+        x->rA = vsub(x->point, xA);
+        x->rB = vsub(x->point, xB);
+        x->normal_impulse = x->src->normal_impulse;
+        x->tangent_impulse = x->src->tangent_impulse;
+        {
+            v3 rnA = vcross(x->rA, x->normal), rnB = vcross(x->rB, x->normal);
+            float K = mA + mB + vdot(mmul(iA, rnA), rnA) + vdot(mmul(iB, rnB), rnB);
+            x->normal_mass = K > 0.0f ? 1.0f / K : 0.0f;
+        }
+        {
+            v3 rn1A = vcross(x->rA, x->tangent1), rn1B = vcross(x->rB, x->tangent1);
+            v3 rn2A = vcross(x->rA, x->tangent2), rn2B = vcross(x->rB, x->tangent2);
+            float k11 = mA + mB + vdot(mmul(iA, rn1A), rn1A) + vdot(mmul(iB, rn1B), rn1B);
+            float k12 = vdot(mmul(iA, rn1A), rn2A) + vdot(mmul(iB, rn1B), rn2B);
+            float k22 = mA + mB + vdot(mmul(iA, rn2A), rn2A) + vdot(mmul(iB, rn2B), rn2B);
+            float det = k11 * k22 - k12 * k12;
+            if (det != 0.0f) det = 1.0f / det;
+            x->tm_xx = det * k22;
+            x->tm_yx = -det * k12;
+            x->tm_xy = -det * k12;
+            x->tm_yy = det * k11;
+        }
+    }
+    /* WarmStartBodyContactConstraints (:264-307) */
+    for (uint32_t q = 0; q < na; ++q) {
+        gbc_t* x = bc + q;
+        body_t* b = gbody(c, x);
+        v3 vA = vel[x->index], vB = b->v, wA = vzero(), wB = b->w;
+        float mA = x->mA, mB = x->mB;
+        v3 P = vscale(x->normal_impulse, x->normal);
+        vA = vsub(vA, vscale(mA, P));
+        wA = vsub(wA, mmul(x->iA, vcross(x->rA, P)));
+        vB = vadd(vB, vscale(mB, P));
+        wB = vadd(wB, mmul(x->iB, vcross(x->rB, P)));
+        v3 P1 = vscale(x->tangent_impulse.x, x->tangent1);
+        v3 P2 = vscale(x->tangent_impulse.y, x->tangent2);
+        vA = vsub(vA, vscale(mA, vadd(P1, P2)));
+        wA = vsub(wA, mmul(x->iA, vcross(x->rA, vadd(P1, P2))));
+        vB = vadd(vB, vscale(mB, vadd(P1, P2)));
+        wB = vadd(wB, mmul(x->iB, vcross(x->rB, vadd(P1, P2))));
+        vel[x->index] = vA;
+        set_body_velocity(b, vB, wB);
+    }
+    for (uint32_t q = 0; q < nt; ++q) tc_warm_start(tc + q, vel);
+    /* SolveBodyContactVelocityConstraints (:388-472), then the triangle contacts */
+    for (uint32_t it = 0; it < vel_iters; ++it) {
+        for (uint32_t q = 0; q < na; ++q) {
+            gbc_t* x = bc + q;
+            body_t* b = gbody(c, x);
+            v3 vA = vel[x->index], vB = b->v, wA = vzero(), wB = b->w;
+            float mA = x->mA, mB = x->mB;
+            m33 iA = x->iA, iB = x->iB;
+            v3 rA = x->rA, rB = x->rB;
+            {
+                v3 dv = vsub(vsub(vadd(vB, vcross(wB, rB)), vA), vcross(wA, rA));
+                float Cdot = vdot(x->normal, dv);
+                float impulse = x->normal_mass * (-Cdot + 0.0f);
+                float old = x->normal_impulse;
+                float ni = old + impulse;
+                x->normal_impulse = ni > 0.0f ? ni : 0.0f;
+                impulse = x->normal_impulse - old;
+                v3 P = vscale(impulse, x->normal);
+                vA = vsub(vA, vscale(mA, P));
+                wA = vsub(wA, mmul(iA, vcross(rA, P)));
+                vB = vadd(vB, vscale(mB, P));
+                wB = vadd(wB, mmul(iB, vcross(rB, P)));
+            }
+            {
+                v3 dv = vsub(vsub(vadd(vB, vcross(wB, rB)), vA), vcross(wA, rA));
+                v2 Cdot = W(vdot(dv, x->tangent1), vdot(dv, x->tangent2));
+                v2 nc = W(-Cdot.x, -Cdot.y);
+                v2 impulse = W(nc.x * x->tm_xx + nc.y * x->tm_yx, nc.x * x->tm_xy + nc.y * x->tm_yy);
+                v2 old = x->tangent_impulse;
+                x->tangent_impulse.x += impulse.x;
+                x->tangent_impulse.y += impulse.y;
+                float maxImpulse = x->friction * x->normal_impulse;
+                v2 ti = x->tangent_impulse;
+                if (ti.x * ti.x + ti.y * ti.y > maxImpulse * maxImpulse) {
+                    float sl = sqrtf(ti.x * ti.x + ti.y * ti.y);
+                    if (sl > kEps) {
+                        ti.x /= sl;
+                        ti.y /= sl;
+                    }
+                    ti.x *= maxImpulse;
+                    ti.y *= maxImpulse;
+                    x->tangent_impulse = ti;
+                }
+                impulse = W(x->tangent_impulse.x - old.x, x->tangent_impulse.y - old.y);
+                v3 P1 = vscale(impulse.x, x->tangent1);
+                v3 P2 = vscale(impulse.y, x->tangent2);
+                v3 P = vadd(P1, P2);
+                vA = vsub(vA, vscale(mA, P));
+                wA = vsub(wA, mmul(iA, vcross(rA, P)));
+                vB = vadd(vB, vscale(mB, P));
+                wB = vadd(wB, mmul(iB, vcross(rB, P)));
+            }
+            vel[x->index] = vA;
+            set_body_velocity(b, vB, wB);
+        }
+        for (uint32_t q = 0; q < nt; ++q) tc_solve_velocity(tc + q, vel);
+    }
+    for (uint32_t q = 0; q < na; ++q) {
+        bc[q].src->normal_impulse = bc[q].normal_impulse;
+        bc[q].src->tangent_impulse = bc[q].tangent_impulse;
+    }
+    for (uint32_t q = 0; q < nt; ++q) {
+        tc[q].src->normal_impulse = tc[q].normalImpulse;
+        tc[q].src->tangent_impulse1 = tc[q].tangentImpulse1;
+        tc[q].src->tangent_impulse2 = tc[q].tangentImpulse2;
+    }
+    for (uint32_t k = 0; k < c->n; ++k) pos[k] = vadd(pos[k], vscale(h, vel[k]));
+    /* SolveBodyContactPositionConstraints (:620-718) */
+    for (uint32_t it = 0; it < pos_iters; ++it) {
+        float minSeparation = 0.0f;
+        for (uint32_t q = 0; q < na; ++q) {
+            gbc_t* x = bc + q;
+            body_t* b = gbody(c, x);
+            float mA = x->mA, mB = x->mB;
+            m33 iA = x->iA, iB = x->iB;
+            v3 cA = pos[x->index];
+            quat qA = Qt(0.0f, 0.0f, 0.0f, 1.0f);
+            v3 cB = b->c;
+            quat qB = b->q;
+            m33 RA = qmat(qA);
+            v3 pA = vsub(cA, mmul(RA, vzero()));
+            m33 RB = qmat(qB);
+            v3 pB = vsub(cB, mmul(RB, x->lcB));
+            v3 nA = x->normal_a;
+            v3 wcA = xmul(RA, pA, x->lpA);
+            v3 wcB = xmul(RB, pB, x->lpB);
+            v3 point = wcB;
+            float separation = vdot(vsub(wcB, wcA), nA) - x->radius_a - x->radius_b;
+            minSeparation = minSeparation < separation ? minSeparation : separation;
+            float Cv = kBaumgarte * (separation + kLinearSlop);
+            float C = Cv < 0.0f ? Cv : 0.0f;
+            C = -kMaxLinearCorrection > C ? -kMaxLinearCorrection : C;
+            v3 rA = vsub(point, cA), rB = vsub(point, cB);
+            v3 rnA = vcross(rA, nA), rnB = vcross(rB, nA);
+            float K = mA + mB + vdot(rnA, mmul(iA, rnA)) + vdot(rnB, mmul(iB, rnB));
+            float impulse = K > 0.0f ? -C / K : 0.0f;
+            v3 P = vscale(impulse, nA);
+            cA = vsub(cA, vscale(mA, P));
+            quat dA = qderiv(qA, mmul(iA, vcross(rA, P)));
+            qA = Qt(qA.x - dA.x, qA.y - dA.y, qA.z - dA.z, qA.w - dA.w);
+            qnormalize(&qA);
+            cB = vadd(cB, vscale(mB, P));
+            quat dB = qderiv(qB, mmul(iB, vcross(rB, P)));
+            qB = Qt(qB.x + dB.x, qB.y + dB.y, qB.z + dB.z, qB.w + dB.w);
+            qnormalize(&qB);
+            pos[x->index] = cA;
+            b->c = cB;
+            b->q = qB;
+        }
+        float minTri = 0.0f;
+        for (uint32_t q = 0; q < nt; ++q) {
+            float sep = tc_solve_position(tc + q, pos);
+            minTri = minTri < sep ? minTri : sep;
+        }
+        if (minSeparation >= -3.0f * kLinearSlop && minTri >= -3.0f * kLinearSlop) break;
+    }
+    /* synchronize the bodies of the active contacts (cloth_solver.cpp:167-181) */
+    for (uint32_t q = 0; q < na; ++q)
+        if (bc[q].body >= 0) sync_body(c, (uint32_t)bc[q].body);
+    free(bc);
+    free(tc);
+}
+
 /* ------------------------------------------------------------------------ */
 /* step                                                                      */
 /* ------------------------------------------------------------------------ */
@@ -2498,7 +3201,9 @@ void oc_step(oc_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, oc_s
             pos[k] = vadd(c->sx[k], c->sy[k]);
             c->mx[i] = c->dvsol[k];
         }
-        solve_contacts(c, h, vel_iters, pos_iters, pos, vel, &local.active_contacts, &local.active_tri_contacts);
+        if (c->nbody) solve_contacts_bodies(c, h, vel_iters, pos_iters, pos, vel, &local.active_contacts,
+                                            &local.active_tri_contacts);
+        else solve_contacts(c, h, vel_iters, pos_iters, pos, vel, &local.active_contacts, &local.active_tri_contacts);
         for (uint32_t k = 0; k < n; ++k) {
             uint32_t i = c->order[k];
             c->x[i] = pos[k];

@@ -67,6 +67,16 @@ void oc_set_state(oc_cloth* c, const float* x, const float* v, const float* dv);
 void oc_set_contacts(oc_cloth* c, uint32_t count, const uint32_t* particle, const uint32_t* shape,
                      const float* impulses);
 void oc_set_proxies(oc_cloth* c, const float* lo, const float* hi);
+/* Colliders on bodies: body state as 55 floats (see body_read); shapes with
+ * geometry in the body's frame; the shapes' world-broadphase proxies. */
+int oc_add_body(oc_cloth* c, const float* desc);
+void oc_set_body(oc_cloth* c, uint32_t body, const float* desc);
+void oc_get_body(const oc_cloth* c, uint32_t body, float* desc);
+int oc_add_body_shape(oc_cloth* c, uint32_t body, int kind, const float* geom, uint32_t nv, uint32_t nf,
+                      float radius, float friction);
+void oc_set_shape_proxy(oc_cloth* c, uint32_t shape, const float* lo, const float* hi);
+void oc_set_report_order(oc_cloth* c, const uint32_t* order, uint32_t count);
+void oc_get_shape_proxy(const oc_cloth* c, uint32_t shape, float* lo, float* hi);
 void oc_set_type(oc_cloth* c, uint32_t vertex, int type);
 void oc_set_radius(oc_cloth* c, uint32_t vertex, float radius);
 void oc_set_friction(oc_cloth* c, uint32_t vertex, float friction);

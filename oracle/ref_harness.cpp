@@ -126,6 +126,7 @@ struct RefCloth {
     std::vector<b3HullShape*> hull_protos;
     std::vector<b3QHull*> hulls;  // the hulls the shapes point to
     std::vector<const b3Shape*> shapes;  // the world's shapes, in creation order
+    std::vector<b3Body*> bodies;         // bodies made by ref_cloth_add_body
     // Particles made with b3Cloth::CreateParticle, addressed after the mesh
     // vertices (index vertexCount + k), and mouse forces by id - 1 (null once
     // destroyed).
@@ -449,6 +450,154 @@ void ref_cloth_add_sphere(void* hp, const float* center, float radius, float fri
     sd.shape = sphere;
     sd.friction = friction;
     h->shapes.push_back(body->CreateShape(sd));
+}
+
+// A body of any type (b3BodyDef: type 0 static, 1 kinematic, 2 dynamic,
+// position, orientation x y z w, linear and angular velocity) in the cloth's
+// world; shapes are added to it with the calls below.  Returns its index.
+uint32_t ref_cloth_add_body(void* hp, int type, const float* position, const float* orientation,
+                            const float* velocity, const float* angular_velocity)
+{
+    RefCloth* h = (RefCloth*)hp;
+    if (!h->world) {
+        h->world = new b3World();
+        h->cloth->SetWorld(h->world);
+    }
+    b3BodyDef bd;
+    bd.type = (b3BodyType)type;
+    bd.position.Set(position[0], position[1], position[2]);
+    bd.orientation.Set(orientation[0], orientation[1], orientation[2], orientation[3]);
+    bd.linearVelocity.Set(velocity[0], velocity[1], velocity[2]);
+    bd.angularVelocity.Set(angular_velocity[0], angular_velocity[1], angular_velocity[2]);
+    h->bodies.push_back(h->world->CreateBody(bd));
+    return (uint32_t)h->bodies.size() - 1;
+}
+
+// A shape on one of those bodies, its geometry in the body's frame, with
+// density (the body's mass follows, b3Body::ResetMass) and friction.
+// kind 0 sphere (centre, radius), 1 capsule (a, b, radius); returns the
+// shape's index among the world's shapes.
+uint32_t ref_cloth_add_body_shape(void* hp, uint32_t body, int kind, const float* geom, float radius, float density,
+                                  float friction)
+{
+    RefCloth* h = (RefCloth*)hp;
+    b3ShapeDef sd;
+    sd.density = density;
+    sd.friction = friction;
+    if (kind == 0) {
+        b3SphereShape* sphere = new b3SphereShape();
+        sphere->m_center.Set(geom[0], geom[1], geom[2]);
+        sphere->m_radius = radius;
+        h->sphere_protos.push_back(sphere);
+        sd.shape = sphere;
+    } else {
+        b3CapsuleShape* cap = new b3CapsuleShape();
+        cap->m_centers[0].Set(geom[0], geom[1], geom[2]);
+        cap->m_centers[1].Set(geom[3], geom[4], geom[5]);
+        cap->m_radius = radius;
+        h->capsule_protos.push_back(cap);
+        sd.shape = cap;
+    }
+    h->shapes.push_back(h->bodies[body]->CreateShape(sd));
+    return (uint32_t)h->shapes.size() - 1;
+}
+
+// A hull (the reference's quickhull of `points`) on one of those bodies;
+// writes its vertices and planes like ref_cloth_add_hull.
+uint32_t ref_cloth_add_body_hull(void* hp, uint32_t body, const float* points, uint32_t count, float density,
+                                 float friction, float* vertices, float* planes, uint32_t* face_count)
+{
+    RefCloth* h = (RefCloth*)hp;
+    std::vector<b3Vec3> pts(count);
+    for (uint32_t i = 0; i < count; ++i) pts[i].Set(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
+    b3QHull* hull = new b3QHull();
+    hull->Set(sizeof(b3Vec3), pts.data(), count);
+    h->hulls.push_back(hull);
+    b3HullShape* shape = new b3HullShape();
+    shape->m_hull = hull;
+    h->hull_protos.push_back(shape);
+    b3ShapeDef sd;
+    sd.shape = shape;
+    sd.density = density;
+    sd.friction = friction;
+    h->shapes.push_back(h->bodies[body]->CreateShape(sd));
+    for (uint32_t i = 0; i < hull->vertexCount; ++i) put3(vertices + 3 * i, hull->vertices[i]);
+    for (uint32_t i = 0; i < hull->faceCount; ++i) {
+        put3(planes + 4 * i, hull->planes[i].normal);
+        planes[4 * i + 3] = hull->planes[i].offset;
+    }
+    *face_count = hull->faceCount;
+    return hull->vertexCount;
+}
+
+// A body's state as 55 floats: type, m_xf (rotation column-major, position),
+// m_sweep (local center, world center 0, world center, orientation 0,
+// orientation), velocities, inverse mass, local and world inverse inertia.
+void ref_cloth_get_body(void* hp, uint32_t body, float* d)
+{
+    const b3Body* b = ((RefCloth*)hp)->bodies[body];
+    d[0] = (float)b->m_type;
+    put3(d + 1, b->m_xf.rotation.x); put3(d + 4, b->m_xf.rotation.y); put3(d + 7, b->m_xf.rotation.z);
+    put3(d + 10, b->m_xf.position);
+    put3(d + 13, b->m_sweep.localCenter); put3(d + 16, b->m_sweep.worldCenter0); put3(d + 19, b->m_sweep.worldCenter);
+    const b3Quat& q0 = b->m_sweep.orientation0;
+    const b3Quat& q = b->m_sweep.orientation;
+    d[22] = q0.x; d[23] = q0.y; d[24] = q0.z; d[25] = q0.w;
+    d[26] = q.x; d[27] = q.y; d[28] = q.z; d[29] = q.w;
+    put3(d + 30, b->m_linearVelocity); put3(d + 33, b->m_angularVelocity);
+    d[36] = b->m_invMass;
+    put3(d + 37, b->m_invI.x); put3(d + 40, b->m_invI.y); put3(d + 43, b->m_invI.z);
+    put3(d + 46, b->m_worldInvI.x); put3(d + 49, b->m_worldInvI.y); put3(d + 52, b->m_worldInvI.z);
+}
+
+// A shape's proxy in the world broadphase (b3Shape::GetAABB).
+void ref_cloth_get_shape_proxy(void* hp, uint32_t shape, float* lo, float* hi)
+{
+    const b3AABB3& a = ((RefCloth*)hp)->shapes[shape]->GetAABB();
+    put3(lo, a.m_lower);
+    put3(hi, a.m_upper);
+}
+
+// The world's shapes in the order a query over everything reports them (its
+// dynamic tree's order, b3World::QueryAABB, world.cpp:464-470); returns the
+// count written.
+struct ReportAll : public b3QueryListener {
+    RefCloth* h;
+    std::vector<uint32_t> out;
+    bool ReportShape(b3Shape* s) override
+    {
+        uint32_t k = 0;
+        while (k < h->shapes.size() && h->shapes[k] != s) ++k;
+        out.push_back(k);
+        return true;
+    }
+};
+
+uint32_t ref_world_report_order(void* hp, uint32_t* order)
+{
+    RefCloth* h = (RefCloth*)hp;
+    if (!h->world) return 0;
+    ReportAll all;
+    all.h = h;
+    b3AABB3 box;
+    box.m_lower.Set(-1e30f, -1e30f, -1e30f);
+    box.m_upper.Set(1e30f, 1e30f, 1e30f);
+    h->world->QueryAABB(&all, box);
+    for (size_t k = 0; k < all.out.size(); ++k) order[k] = all.out[k];
+    return (uint32_t)all.out.size();
+}
+
+// b3World::Step of the cloth's world (rigid bodies only).
+void ref_world_step(void* hp, float dt, uint32_t velocity_iterations, uint32_t position_iterations)
+{
+    RefCloth* h = (RefCloth*)hp;
+    if (h->world) h->world->Step(dt, velocity_iterations, position_iterations);
+}
+
+void ref_world_set_gravity(void* hp, const float* g)
+{
+    RefCloth* h = (RefCloth*)hp;
+    if (h->world) h->world->SetGravity(b3Vec3(g[0], g[1], g[2]));
 }
 
 // A static body at the origin carrying one capsule shape, segment a-b.
