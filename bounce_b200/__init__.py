@@ -84,6 +84,45 @@ class MouseForceDefC(C.Structure):
                 ("w4", C.c_float), ("mouse", C.c_float), ("damping", C.c_float)]
 
 
+class BodyStateC(C.Structure):
+    """b3g_body_state: a rigid body's transform, sweep, velocities and mass
+    (b3Body, include/bounce/dynamics/body.h)."""
+    _fields_ = [("type", C.c_int32), ("rotation", C.c_float * 9), ("position", C.c_float * 3),
+                ("local_center", C.c_float * 3), ("world_center0", C.c_float * 3), ("world_center", C.c_float * 3),
+                ("orientation0", C.c_float * 4), ("orientation", C.c_float * 4), ("linear_velocity", C.c_float * 3),
+                ("angular_velocity", C.c_float * 3), ("inv_mass", C.c_float), ("inv_inertia", C.c_float * 9),
+                ("world_inv_inertia", C.c_float * 9)]
+
+
+def body_state_from_array(a) -> BodyStateC:
+    """A body state from its 55 floats: type, rotation (9, column-major),
+    position, local centre, world centre 0 and 1, orientation 0 and 1 (x y z
+    w), linear and angular velocity, inverse mass, inverse inertia (9) and
+    world inverse inertia (9)."""
+    a = np.asarray(a, np.float32).reshape(-1)
+    if a.size != 55:
+        raise ValueError("a body state has 55 floats")
+    b = BodyStateC()
+    b.type = int(a[0])
+    k = 1
+    for name, t in BodyStateC._fields_[1:]:
+        m = getattr(t, "_length_", 1)
+        if m == 1:
+            setattr(b, name, float(a[k]))
+        else:
+            getattr(b, name)[:] = [float(u) for u in a[k:k + m]]
+        k += m
+    return b
+
+
+def body_state_to_array(b: BodyStateC) -> np.ndarray:
+    out = [float(b.type)]
+    for name, t in BodyStateC._fields_[1:]:
+        v = getattr(b, name)
+        out.extend([v] if getattr(t, "_length_", 1) == 1 else list(v))
+    return np.asarray(out, np.float32)
+
+
 class ClothInfoC(C.Structure):
     _fields_ = [(k, C.c_uint32) for k in ("vertices", "triangles", "springs", "blocks", "sell_entries",
                                            "max_degree")]
@@ -178,6 +217,15 @@ def lib() -> C.CDLL:
             "b3g_cloth_ray_cast": [vp, vp, vp, f32, u32, C.POINTER(f32), vp, C.POINTER(i32)],
             "b3g_cloth_get_self_stats": [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)],
             "b3g_cloth_last_stats": [vp, C.POINTER(StepStatsC)],
+            "b3g_cloth_add_body": [vp, C.POINTER(BodyStateC), C.POINTER(u32)],
+            "b3g_cloth_set_body": [vp, u32, C.POINTER(BodyStateC)],
+            "b3g_cloth_get_body": [vp, u32, C.POINTER(BodyStateC)],
+            "b3g_cloth_add_body_sphere": [vp, u32, vp, f32, f32, C.POINTER(u32)],
+            "b3g_cloth_add_body_capsule": [vp, u32, vp, vp, f32, f32, C.POINTER(u32)],
+            "b3g_cloth_add_body_hull": [vp, u32, vp, u32, vp, u32, f32, C.POINTER(u32)],
+            "b3g_cloth_set_shape_proxy": [vp, u32, vp, vp],
+            "b3g_cloth_get_shape_proxy": [vp, u32, vp, vp],
+            "b3g_cloth_set_report_order": [vp, vp, u32],
             "b3g_cloth_read_system": [vp, C.POINTER(u32), vp, vp, vp, vp, vp, vp],
             "b3g_cloth_step_profiled": [vp, f32, u32, u32, C.POINTER(PhaseTimesC), C.POINTER(StepStatsC)],
             "b3g_cloth_get_info": [vp, C.POINTER(ClothInfoC)],
@@ -438,6 +486,66 @@ class Cloth:
     def clear_colliders(self) -> None:
         check(lib().b3g_cloth_clear_colliders(self.h), "clear_colliders")
         self.nsph = 0
+
+    # ---- colliders on bodies (b3Cloth::SetWorld with b3Body) ----
+
+    def add_body(self, state) -> int:
+        """A body for body colliders; `state` is a BodyStateC or its 55
+        floats (body_state_from_array)."""
+        b = state if isinstance(state, BodyStateC) else body_state_from_array(state)
+        bid = C.c_uint32(0)
+        check(lib().b3g_cloth_add_body(self.h, C.byref(b), C.byref(bid)), "add_body")
+        return bid.value
+
+    def set_body(self, body: int, state) -> None:
+        b = state if isinstance(state, BodyStateC) else body_state_from_array(state)
+        check(lib().b3g_cloth_set_body(self.h, body, C.byref(b)), "set_body")
+
+    def body(self, body: int) -> np.ndarray:
+        """The body's state as 55 floats, after the cloth's contact solve and
+        synchronisation changed it."""
+        b = BodyStateC()
+        check(lib().b3g_cloth_get_body(self.h, body, C.byref(b)), "get_body")
+        return body_state_to_array(b)
+
+    def add_body_sphere(self, body: int, center, radius: float, friction: float) -> int:
+        sid = C.c_uint32(0)
+        c3 = _f3(center)
+        check(lib().b3g_cloth_add_body_sphere(self.h, body, _ptr(c3), radius, friction, C.byref(sid)),
+              "add_body_sphere")
+        self.nsph += 1
+        return sid.value
+
+    def add_body_capsule(self, body: int, a, b, radius: float, friction: float) -> int:
+        sid = C.c_uint32(0)
+        a3, b3 = _f3(a), _f3(b)
+        check(lib().b3g_cloth_add_body_capsule(self.h, body, _ptr(a3), _ptr(b3), radius, friction, C.byref(sid)),
+              "add_body_capsule")
+        self.nsph += 1
+        return sid.value
+
+    def add_body_hull(self, body: int, vertices, planes, friction: float) -> int:
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        p = np.ascontiguousarray(planes, np.float32).reshape(-1, 4)
+        sid = C.c_uint32(0)
+        check(lib().b3g_cloth_add_body_hull(self.h, body, _ptr(v), len(v), _ptr(p), len(p), friction,
+                                            C.byref(sid)), "add_body_hull")
+        self.nsph += 1
+        return sid.value
+
+    def set_shape_proxy(self, shape: int, lo, hi) -> None:
+        a, b = _f3(lo), _f3(hi)
+        check(lib().b3g_cloth_set_shape_proxy(self.h, shape, _ptr(a), _ptr(b)), "set_shape_proxy")
+
+    def shape_proxy(self, shape: int):
+        lo, hi = np.zeros(3, np.float32), np.zeros(3, np.float32)
+        check(lib().b3g_cloth_get_shape_proxy(self.h, shape, _ptr(lo), _ptr(hi)), "get_shape_proxy")
+        return lo, hi
+
+    def set_report_order(self, order) -> None:
+        """The world query's report order of the colliders (empty: derived)."""
+        o = np.ascontiguousarray(order, np.uint32).reshape(-1)
+        check(lib().b3g_cloth_set_report_order(self.h, _ptr(o) if o.size else None, o.size), "set_report_order")
 
     def particle(self, i: int) -> Particle:
         return Particle(self, i)

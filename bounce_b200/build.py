@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libb3g.so")
 SOURCES = ["cloth_kernels.cu", "cloth_api.cu", "mpcg_solve.cu", "batch_cg.cu", "batch_api.cu", "server.cu", "grid_cg.cu",
-           "softbody.cu", "self_collision.cu", "topology.cpp", "softbody_prep.cpp", "broadphase_order.cpp"]
+           "softbody.cu", "self_collision.cu", "bodies.cu", "topology.cpp", "softbody_prep.cpp", "broadphase_order.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-warn-spills"]
 

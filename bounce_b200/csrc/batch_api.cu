@@ -195,7 +195,8 @@ b3g_status check_list(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count)
     for (uint32_t k = 0; k < count; ++k)
         if (!cloths[k] || cloths[k]->dev.n == 0 || cloths[k]->device != b->device) return B3G_ERR_INVALID_ARGUMENT;
     for (uint32_t k = 0; k < count; ++k)
-        if (cloths[k]->self) return B3G_ERR_UNSUPPORTED;  // self-collision runs on single cloths only
+        // self-collision and body colliders run on single cloths only
+        if (cloths[k]->self || cloths[k]->dev.nbody) return B3G_ERR_UNSUPPORTED;
     return B3G_OK;
 }
 

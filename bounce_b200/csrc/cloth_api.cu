@@ -1,6 +1,7 @@
 // C ABI of libb3g.so (include/b3g.h): cloth handles, device memory, the
 // per-step CUDA graph, particle edits and state transfers.
 #include <algorithm>
+#include <cstddef>
 #include <cstdio>
 #include <cmath>
 #include <cstring>
@@ -216,6 +217,28 @@ b3g_status launch_step_plain(b3g_cloth* c, uint32_t pos_iters)
     B3G_TRY(launch_finalize(c->dev, st));
     for (uint32_t k = 1; k < pos_iters && k < (uint32_t)kMaxPosIters; ++k)
         B3G_TRY(launch_contact_position(c->dev, k, st));
+    B3G_TRY(launch_post(c->dev, st));
+    return B3G_OK;
+}
+
+// A step of a cloth with body colliders, launched without a graph: the
+// contact update, assembly and CG as in any step, then the force solver's
+// state update and the body-contact solve in list order on one block
+// (bodies.cu), then the proxy sync and the new contacts.
+b3g_status launch_step_bodies(b3g_cloth* c)
+{
+    const int dot = (int)c->opts.dot;
+    cudaStream_t st = c->stream;
+    cudaGraphConditionalHandle none = 0;
+    B3G_TRY(launch_contacts_update(c->dev, st));
+    B3G_TRY(launch_assemble(c->dev, c->assemble_block, st));
+    if (persistent_cg(c)) {
+        B3G_TRY(launch_persistent_cg(c, dot, st));
+    } else {
+        B3G_TRY(launch_cg_init(c->dev, dot, none, 0, st));
+        for (uint32_t k = 0; k < c->opts.max_iterations; ++k) B3G_TRY(launch_cg_iteration(c->dev, dot, none, 0, st));
+    }
+    B3G_TRY(launch_body_solve(c->dev, c->body_scratch, st));
     B3G_TRY(launch_post(c->dev, st));
     return B3G_OK;
 }
@@ -583,6 +606,8 @@ b3g_status destroy_cloth(b3g_cloth* c)
     c->hull_bufs.clear();
     if (c->ray_buf) cudaFree(c->ray_buf);
     if (c->cg_rec) cudaFree(c->cg_rec);
+    if (c->body_buf) cudaFree(c->body_buf);
+    body_scratch_free(c->body_scratch);
     destroy_graph(c);
     if (c->arena.base && c->owns_arena) cudaFree(c->arena.base);
     if (c->d_ops) cudaFree(c->d_ops);
@@ -664,6 +689,7 @@ b3g_status b3g_cloth_add_static_sphere(b3g_cloth* c, const float center[3], floa
     }
     if (shape_id) *shape_id = c->dev.nsph;
     c->dev.nsph += 1;
+    c->report_fixed = false;
     rank_colliders(c->dev.sph, c->dev.nsph);
     destroy_graph(c);
     return B3G_OK;
@@ -690,22 +716,21 @@ b3g_status b3g_cloth_add_static_capsule(b3g_cloth* c, const float a[3], const fl
     }
     if (shape_id) *shape_id = c->dev.nsph;
     c->dev.nsph += 1;
+    c->report_fixed = false;
     rank_colliders(c->dev.sph, c->dev.nsph);
     destroy_graph(c);
     return B3G_OK;
 }
 
-b3g_status b3g_cloth_add_static_hull(b3g_cloth* c, const float* vertices, uint32_t vertex_count,
-                                     const float* planes, uint32_t face_count, float friction, uint32_t* shape_id)
+}  // extern "C"
+
+namespace {
+
+// Copies a hull's vertices and planes to the device (kept until the
+// colliders are cleared).
+b3g_status upload_hull(b3g_cloth* c, const float* vertices, uint32_t vertex_count, const float* planes,
+                       uint32_t face_count, float** out)
 {
-    if (!valid(c) || !vertices || !planes || vertex_count == 0 || face_count == 0 || vertex_count > 4096 ||
-        face_count > 4096 || !(friction >= 0.0f))
-        return B3G_ERR_INVALID_ARGUMENT;
-    for (uint32_t k = 0; k < 3 * vertex_count; ++k)
-        if (!std::isfinite(vertices[k])) return B3G_ERR_INVALID_ARGUMENT;
-    for (uint32_t k = 0; k < 4 * face_count; ++k)
-        if (!std::isfinite(planes[k])) return B3G_ERR_INVALID_ARGUMENT;
-    if (c->dev.nsph >= (uint32_t)kMaxSpheres) return B3G_ERR_CAPACITY;
     cudaSetDevice(c->device);
     const size_t nf = 3 * (size_t)vertex_count + 4 * (size_t)face_count;
     std::vector<float> img(nf);
@@ -720,6 +745,36 @@ b3g_status b3g_cloth_add_static_hull(b3g_cloth* c, const float* vertices, uint32
         return from_cuda(e);
     }
     c->hull_bufs.push_back(d);
+    *out = d;
+    return B3G_OK;
+}
+
+bool hull_args_ok(const float* vertices, uint32_t vertex_count, const float* planes, uint32_t face_count,
+                  float friction)
+{
+    if (!vertices || !planes || vertex_count == 0 || face_count == 0 || vertex_count > 4096 || face_count > 4096 ||
+        !(friction >= 0.0f))
+        return false;
+    for (uint32_t k = 0; k < 3 * vertex_count; ++k)
+        if (!std::isfinite(vertices[k])) return false;
+    for (uint32_t k = 0; k < 4 * face_count; ++k)
+        if (!std::isfinite(planes[k])) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+b3g_status b3g_cloth_add_static_hull(b3g_cloth* c, const float* vertices, uint32_t vertex_count,
+                                     const float* planes, uint32_t face_count, float friction, uint32_t* shape_id)
+{
+    if (!valid(c) || !hull_args_ok(vertices, vertex_count, planes, face_count, friction))
+        return B3G_ERR_INVALID_ARGUMENT;
+    if (c->dev.nsph >= (uint32_t)kMaxSpheres) return B3G_ERR_CAPACITY;
+    float* d = nullptr;
+    const b3g_status us = upload_hull(c, vertices, vertex_count, planes, face_count, &d);
+    if (us != B3G_OK) return us;
     SphereDev& s = c->dev.sph[c->dev.nsph];
     s = SphereDev{};
     s.kind = 2;
@@ -753,6 +808,7 @@ b3g_status b3g_cloth_add_static_hull(b3g_cloth* c, const float* vertices, uint32
     }
     if (shape_id) *shape_id = c->dev.nsph;
     c->dev.nsph += 1;
+    c->report_fixed = false;
     rank_colliders(c->dev.sph, c->dev.nsph);
     destroy_graph(c);
     return B3G_OK;
@@ -771,7 +827,264 @@ b3g_status b3g_cloth_clear_colliders(b3g_cloth* c)
     B3G_TRY(launch_clear_contacts(c->dev, c->stream));
     B3G_TRY(cudaStreamSynchronize(c->stream));
     c->dev.nsph = 0;
+    c->dev.nbody = 0;
+    c->report_fixed = false;
     free_hulls(c);
+    destroy_graph(c);
+    return B3G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// colliders on bodies (b3Cloth::SetWorld with b3Body)
+// ---------------------------------------------------------------------------
+
+}  // extern "C"
+
+namespace {
+
+constexpr uint32_t kMaxBodies = kMaxSpheres;  // a body matters to the cloth only through a collider
+
+bool body_ok(const b3g_body_state& b)
+{
+    if (b.type < 0 || b.type > 2) return false;
+    const float* f = b.rotation;
+    const size_t nf = (sizeof(b3g_body_state) - offsetof(b3g_body_state, rotation)) / sizeof(float);
+    for (size_t k = 0; k < nf; ++k)
+        if (!std::isfinite(f[k])) return false;
+    return true;
+}
+
+// The bodies' and the body shapes' proxies' device buffer, made on first use.
+b3g_status ensure_body_buf(b3g_cloth* c)
+{
+    if (c->body_buf) return B3G_OK;
+    cudaSetDevice(c->device);
+    const size_t bytes = kMaxBodies * sizeof(b3g_body_state) + 6 * kMaxSpheres * sizeof(float);
+    B3G_TRY(cudaMalloc(&c->body_buf, bytes));
+    B3G_TRY(cudaMemsetAsync(c->body_buf, 0, bytes, c->stream));
+    c->dev.bodies = (b3g_body_state*)c->body_buf;
+    c->dev.shape_fat = (float*)((char*)c->body_buf + kMaxBodies * sizeof(b3g_body_state));
+    return B3G_OK;
+}
+
+// b3Mul(xf, v) on the host, in the device's float order
+void xf_point(const float R[9], const float p[3], const float v[3], float out[3])
+{
+    for (int q = 0; q < 3; ++q) out[q] = ((v[0] * R[q] + v[1] * R[3 + q]) + v[2] * R[6 + q]) + p[q];
+}
+
+// b3Shape::ComputeAABB(m_xf) of a body shape, fattened by B3_AABB_EXTENSION
+// (b3BroadPhase::CreateProxy, broad_phase.cpp:78-82).
+void body_shape_proxy(const SphereDev& s, const float* hull_host, const b3g_body_state& b, float lo[3], float hi[3])
+{
+    float l[3], h[3];
+    if (s.kind == 0) {
+        const float ctr[3] = {s.cx, s.cy, s.cz};
+        float w[3];
+        xf_point(b.rotation, b.position, ctr, w);
+        for (int q = 0; q < 3; ++q) l[q] = h[q] = w[q];
+    } else if (s.kind == 1) {
+        const float A[3] = {s.ax, s.ay, s.az}, B[3] = {s.bx, s.by, s.bz};
+        float wa[3], wb[3];
+        xf_point(b.rotation, b.position, A, wa);
+        xf_point(b.rotation, b.position, B, wb);
+        for (int q = 0; q < 3; ++q) {
+            l[q] = wa[q] < wb[q] ? wa[q] : wb[q];
+            h[q] = wa[q] > wb[q] ? wa[q] : wb[q];
+        }
+    } else {
+        for (uint32_t k = 0; k < s.nhv; ++k) {
+            float w[3];
+            xf_point(b.rotation, b.position, hull_host + 3 * k, w);
+            for (int q = 0; q < 3; ++q) {
+                l[q] = k == 0 || w[q] < l[q] ? w[q] : l[q];
+                h[q] = k == 0 || w[q] > h[q] ? w[q] : h[q];
+            }
+        }
+    }
+    for (int q = 0; q < 3; ++q) {
+        lo[q] = (l[q] - s.radius) - 0.2f;
+        hi[q] = (h[q] + s.radius) + 0.2f;
+    }
+}
+
+b3g_status read_body(const b3g_cloth* c, uint32_t id, b3g_body_state* out)
+{
+    cudaSetDevice(c->device);
+    B3G_TRY(cudaMemcpyAsync(out, c->dev.bodies + id, sizeof(b3g_body_state), cudaMemcpyDeviceToHost, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    return B3G_OK;
+}
+
+// Installs collider `s` on body `body_id`: its proxy from the body's
+// current transform, host and device copies.
+b3g_status add_body_shape(b3g_cloth* c, uint32_t body_id, SphereDev s, const float* hull_host, uint32_t* shape_id)
+{
+    b3g_body_state b;
+    b3g_status st = read_body(c, body_id, &b);
+    if (st != B3G_OK) return st;
+    s.body1 = body_id + 1;
+    body_shape_proxy(s, hull_host, b, s.lo, s.hi);
+    const uint32_t id = c->dev.nsph;
+    const float fat[6] = {s.lo[0], s.lo[1], s.lo[2], s.hi[0], s.hi[1], s.hi[2]};
+    B3G_TRY(cudaMemcpyAsync(c->dev.shape_fat + 6 * id, fat, sizeof(fat), cudaMemcpyHostToDevice, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    c->dev.sph[id] = s;
+    c->dev.nsph += 1;
+    c->report_fixed = false;
+    rank_colliders(c->dev.sph, c->dev.nsph);
+    destroy_graph(c);
+    if (shape_id) *shape_id = id;
+    return B3G_OK;
+}
+
+bool body_target(const b3g_cloth* c, uint32_t body_id) { return valid(c) && body_id < c->dev.nbody; }
+
+}  // namespace
+
+extern "C" {
+
+b3g_status b3g_cloth_add_body(b3g_cloth* c, const b3g_body_state* state, uint32_t* body_id)
+{
+    if (!valid(c) || !state || !body_ok(*state)) return B3G_ERR_INVALID_ARGUMENT;
+    if (c->self || !c->owns_stream) return B3G_ERR_UNSUPPORTED;  // single cloths without self-collision
+    if (c->dev.nbody >= kMaxBodies) return B3G_ERR_CAPACITY;
+    b3g_status s = ensure_body_buf(c);
+    if (s != B3G_OK) return s;
+    B3G_TRY(cudaMemcpyAsync(c->dev.bodies + c->dev.nbody, state, sizeof(b3g_body_state), cudaMemcpyHostToDevice,
+                            c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    if (body_id) *body_id = c->dev.nbody;
+    c->dev.nbody += 1;
+    destroy_graph(c);
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_set_body(b3g_cloth* c, uint32_t body_id, const b3g_body_state* state)
+{
+    if (!valid(c) || !state || body_id >= c->dev.nbody || !body_ok(*state)) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    B3G_TRY(cudaMemcpyAsync(c->dev.bodies + body_id, state, sizeof(b3g_body_state), cudaMemcpyHostToDevice,
+                            c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_get_body(const b3g_cloth* c, uint32_t body_id, b3g_body_state* state)
+{
+    if (!valid(c) || !state || body_id >= c->dev.nbody) return B3G_ERR_INVALID_ARGUMENT;
+    return read_body(c, body_id, state);
+}
+
+b3g_status b3g_cloth_add_body_sphere(b3g_cloth* c, uint32_t body_id, const float center[3], float radius,
+                                     float friction, uint32_t* shape_id)
+{
+    if (!body_target(c, body_id) || !center || !(radius > 0.0f) || !(friction >= 0.0f))
+        return B3G_ERR_INVALID_ARGUMENT;
+    for (int q = 0; q < 3; ++q)
+        if (!std::isfinite(center[q])) return B3G_ERR_INVALID_ARGUMENT;
+    if (c->dev.nsph >= (uint32_t)kMaxSpheres) return B3G_ERR_CAPACITY;
+    SphereDev s{};
+    s.kind = 0;
+    s.cx = center[0], s.cy = center[1], s.cz = center[2];
+    s.radius = radius;
+    s.friction = friction;
+    return add_body_shape(c, body_id, s, nullptr, shape_id);
+}
+
+b3g_status b3g_cloth_add_body_capsule(b3g_cloth* c, uint32_t body_id, const float a[3], const float b[3],
+                                      float radius, float friction, uint32_t* shape_id)
+{
+    if (!body_target(c, body_id) || !a || !b || !(radius > 0.0f) || !(friction >= 0.0f))
+        return B3G_ERR_INVALID_ARGUMENT;
+    for (int q = 0; q < 3; ++q)
+        if (!std::isfinite(a[q]) || !std::isfinite(b[q])) return B3G_ERR_INVALID_ARGUMENT;
+    if (c->dev.nsph >= (uint32_t)kMaxSpheres) return B3G_ERR_CAPACITY;
+    SphereDev s{};
+    s.kind = 1;
+    s.ax = a[0], s.ay = a[1], s.az = a[2];
+    s.bx = b[0], s.by = b[1], s.bz = b[2];
+    s.radius = radius;
+    s.friction = friction;
+    return add_body_shape(c, body_id, s, nullptr, shape_id);
+}
+
+b3g_status b3g_cloth_add_body_hull(b3g_cloth* c, uint32_t body_id, const float* vertices, uint32_t vertex_count,
+                                   const float* planes, uint32_t face_count, float friction, uint32_t* shape_id)
+{
+    if (!body_target(c, body_id) || !hull_args_ok(vertices, vertex_count, planes, face_count, friction))
+        return B3G_ERR_INVALID_ARGUMENT;
+    if (c->dev.nsph >= (uint32_t)kMaxSpheres) return B3G_ERR_CAPACITY;
+    float* d = nullptr;
+    const b3g_status us = upload_hull(c, vertices, vertex_count, planes, face_count, &d);
+    if (us != B3G_OK) return us;
+    SphereDev s{};
+    s.kind = 2;
+    s.radius = 0.0f;  // B3_HULL_RADIUS
+    s.friction = friction;
+    s.hull = d;
+    s.nhv = vertex_count;
+    s.nhf = face_count;
+    return add_body_shape(c, body_id, s, vertices, shape_id);
+}
+
+b3g_status b3g_cloth_set_shape_proxy(b3g_cloth* c, uint32_t shape_id, const float lo[3], const float hi[3])
+{
+    if (!valid(c) || !lo || !hi || shape_id >= c->dev.nsph || !c->dev.sph[shape_id].body1)
+        return B3G_ERR_INVALID_ARGUMENT;
+    for (int q = 0; q < 3; ++q)
+        if (!std::isfinite(lo[q]) || !std::isfinite(hi[q]) || !(lo[q] <= hi[q])) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    const float fat[6] = {lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]};
+    B3G_TRY(cudaMemcpyAsync(c->dev.shape_fat + 6 * shape_id, fat, sizeof(fat), cudaMemcpyHostToDevice, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    SphereDev& s = c->dev.sph[shape_id];
+    for (int q = 0; q < 3; ++q) {
+        s.lo[q] = lo[q];
+        s.hi[q] = hi[q];
+    }
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_get_shape_proxy(const b3g_cloth* c, uint32_t shape_id, float lo[3], float hi[3])
+{
+    if (!valid(c) || !lo || !hi || shape_id >= c->dev.nsph) return B3G_ERR_INVALID_ARGUMENT;
+    const SphereDev& s = c->dev.sph[shape_id];
+    if (!s.body1) {
+        for (int q = 0; q < 3; ++q) {
+            lo[q] = s.lo[q];
+            hi[q] = s.hi[q];
+        }
+        return B3G_OK;
+    }
+    cudaSetDevice(c->device);
+    float fat[6];
+    B3G_TRY(cudaMemcpyAsync(fat, c->dev.shape_fat + 6 * shape_id, sizeof(fat), cudaMemcpyDeviceToHost, c->stream));
+    B3G_TRY(cudaStreamSynchronize(c->stream));
+    for (int q = 0; q < 3; ++q) {
+        lo[q] = fat[q];
+        hi[q] = fat[3 + q];
+    }
+    return B3G_OK;
+}
+
+b3g_status b3g_cloth_set_report_order(b3g_cloth* c, const uint32_t* order, uint32_t count)
+{
+    if (!valid(c) || (count && !order)) return B3G_ERR_INVALID_ARGUMENT;
+    const uint32_t m = c->dev.nsph;
+    if (count == 0) {
+        c->report_fixed = false;
+        rank_colliders(c->dev.sph, m);
+        return B3G_OK;
+    }
+    if (count != m) return B3G_ERR_INVALID_ARGUMENT;
+    bool seen[kMaxSpheres] = {};
+    for (uint32_t r = 0; r < count; ++r) {
+        if (order[r] >= m || seen[order[r]]) return B3G_ERR_INVALID_ARGUMENT;
+        seen[order[r]] = true;
+    }
+    for (uint32_t r = 0; r < count; ++r) c->dev.sph[order[r]].rank = r;
+    c->report_fixed = true;
     destroy_graph(c);
     return B3G_OK;
 }
@@ -931,6 +1244,9 @@ b3g_status relayout(b3g_cloth* c, const ParticleState& s, uint32_t old_extra, st
     }
     c->dev.nsph = old_dev.nsph;
     std::memcpy(c->dev.sph, old_dev.sph, sizeof(old_dev.sph));
+    c->dev.bodies = old_dev.bodies;
+    c->dev.shape_fat = old_dev.shape_fat;
+    c->dev.nbody = old_dev.nbody;
     // the host copy of the masses follows the state (created particles carry their own)
     for (uint32_t i = 0; i < s.n && i < c->topo.mass.size(); ++i) c->topo.mass[i] = s.mass[i];
     char* base = nullptr;
@@ -1277,6 +1593,8 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
     B3G_TRY(cudaEventRecord(c->ev0, st));
     if (c->self) {
         if ((s = launch_step_self(c, dt)) != B3G_OK) return s;
+    } else if (dt > 0.0f && c->dev.nbody) {
+        if ((s = launch_step_bodies(c)) != B3G_OK) return s;
     } else if (dt > 0.0f) {
         if (c->graph_ok && (!c->exec || c->graph_dot != (int)c->opts.dot || c->graph_pos_iters != pos_iters ||
                             c->graph_nsph != c->dev.nsph || c->graph_strategy != c->cg_strategy)) {
@@ -1305,7 +1623,7 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
     L.active_contacts = h->active_contacts;
     L.contacts = h->contacts;
     L.step_ms = ms;
-    if (dt > 0.0f && !c->self && c->graph_ok && c->exec) {
+    if (dt > 0.0f && !c->self && !c->dev.nbody && c->graph_ok && c->exec) {
         // kernel nodes the graph ran: [contacts_update] assemble cg_init,
         // 3 per CG iteration, finalize, [contact_position x (pos_iters - 1)], post
         const uint64_t ns = c->dev.nsph ? 1 : 0;

@@ -23,6 +23,8 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/b3g.h"
+
 namespace b3g {
 
 constexpr int kMaxSpheres = 4;
@@ -72,6 +74,9 @@ struct SphereDev {
     uint32_t nhv, nhf;
     uint32_t rank;        // position among the shapes a world query reports (new contacts of one
                           // step are listed in that order)
+    uint32_t body1;       // 0: a static shape in the world frame (as above); else 1 + the index of
+                          // the body it sits on, its geometry (centre, segment, hull) in that
+                          // body's frame and its proxy in ClothDev::shape_fat
 };
 
 // Ranks the colliders sph[0..count) by the world broadphase's report order
@@ -120,6 +125,9 @@ struct ClothDev {
     float* c_imp;               // normal, tangent x, tangent y
     float* c_point;             // capsules: the shape point of the contact (3 planes of nsph * n)
     SphereDev sph[kMaxSpheres];
+    b3g_body_state* bodies;     // the bodies of body colliders (device copies), nbody of them
+    float* shape_fat;           // per collider its world-broadphase proxy (lo xyz, hi xyz); body shapes only
+    uint32_t nbody;
 
     StepScalars* sc;
     GridBarrier* bar;           // persistent-CG grid barrier

@@ -42,6 +42,13 @@ struct HostImages {
 
 }  // namespace b3g
 
+namespace b3g {
+// The body-contact solve of a cloth with body colliders (bodies.cu).
+struct BodyScratch;
+void body_scratch_free(BodyScratch* s);
+cudaError_t launch_body_solve(const ClothDev& c, BodyScratch*& s, cudaStream_t st);
+}  // namespace b3g
+
 struct b3g_cloth {
     int device = 0;
     cudaStream_t stream = nullptr, body_stream = nullptr;
@@ -95,6 +102,9 @@ struct b3g_cloth {
     b3g::SelfState* self = nullptr;           // particle-triangle contacts (thickness > 0)
     std::vector<void*> hull_bufs;             // device copies of the hull colliders' data
     void* ray_buf = nullptr;                  // ray cast scratch (key and result)
+    void* body_buf = nullptr;                 // body colliders: the bodies, then the shapes' proxies
+    b3g::BodyScratch* body_scratch = nullptr; // the body-contact solve's sort and constraint scratch
+    bool report_fixed = false;                // collider ranks given by b3g_cloth_set_report_order
 };
 
 

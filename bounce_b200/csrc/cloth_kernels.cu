@@ -25,6 +25,7 @@
 #include "cg_common.cuh"
 #include "cloth_dev.cuh"
 #include "hull_gjk.cuh"
+#include "bodies.cuh"
 #include "self_collision.cuh"
 #include "sell_spmv.cuh"
 #include "vec.cuh"
@@ -658,6 +659,37 @@ __device__ __forceinline__ bool overlap(const float* lo, const float* hi, const 
            hi[2] >= s.lo[2];
 }
 
+// The overlap of a particle's proxy with collider s: body shapes keep their
+// proxy in device memory (the caller's world and the step's body sync move it).
+__device__ __forceinline__ bool overlap_shape(const ClothDev& c, uint32_t s, const float* lo, const float* hi)
+{
+    const SphereDev& sp = c.sph[s];
+    if (!sp.body1) return overlap(lo, hi, sp);
+    const float* f = c.shape_fat + 6 * s;
+    return lo[0] <= f[3] && lo[1] <= f[4] && lo[2] <= f[5] && hi[0] >= f[0] && hi[1] >= f[1] && hi[2] >= f[2];
+}
+
+// A pair of a non-dynamic particle and a collider whose body is not dynamic
+// does not collide (cloth_contact_manager.cpp:286-298).
+__device__ __forceinline__ bool body_dynamic(const ClothDev& c, uint32_t s)
+{
+    return c.sph[s].body1 && c.bodies[c.sph[s].body1 - 1].type == 2;
+}
+
+// TestSphere of a collider on a body, with the body's transform m_xf; the
+// contact keeps its shape point in the body's frame (GetLocalPoint).
+__device__ __forceinline__ bool body_contact(const ClothDev& c, uint32_t s, uint32_t q, uint32_t nn, f3 xi,
+                                             float radius, f3& normal)
+{
+    const SphereDev& sp = c.sph[s];
+    m3 R;
+    f3 p, point;
+    body::body_xf(c.bodies[sp.body1 - 1], R, p);
+    if (!body::test_sphere(sp, R, p, xi, radius, normal, point)) return false;
+    st3(c.c_point, nn, q, body::xmult(R, p, point));
+    return true;
+}
+
 __device__ __forceinline__ void load_fat(const ClothDev& c, uint32_t i, float* lo, float* hi)
 {
     const uint32_t n = c.n;
@@ -684,14 +716,19 @@ __global__ void k_contacts_update(const __grid_constant__ ClothDev one, const __
         const uint32_t q = s * n + i;
         if (!c.c_exists[q] || c.sph[s].kind == 2) continue;  // hulls: k_hull_contacts_update
         const SphereDev& sp = c.sph[s];
-        if (!is_dynamic(c, i) || !overlap(lo, hi, sp)) {
+        if ((!is_dynamic(c, i) && !body_dynamic(c, s)) || !overlap_shape(c, s, lo, hi)) {
             c.c_exists[q] = 0;
             c.c_active[q] = 0;
             continue;
         }
         const float radius = sp.radius + c.p_radius[i];
         f3 normal;
-        if (sp.kind == 0) {
+        if (sp.body1) {
+            if (!body_contact(c, s, q, nn, xi, radius, normal)) {
+                c.c_active[q] = 0;
+                continue;
+            }
+        } else if (sp.kind == 0) {
             // b3SphereShape::TestSphere (sphere_shape.cpp:71-95)
             const float rr = radius * radius;
             const f3 d = xi - mk(sp.cx, sp.cy, sp.cz);
@@ -772,18 +809,26 @@ __global__ void k_hull_contacts_update(const __grid_constant__ ClothDev one, con
         const uint32_t q = s * n + i;
         const SphereDev& sp = c.sph[s];
         if (sp.kind != 2 || !c.c_exists[q]) continue;
-        if (!is_dynamic(c, i) || !overlap(lo, hi, sp)) {
+        if ((!is_dynamic(c, i) && !body_dynamic(c, s)) || !overlap_shape(c, s, lo, hi)) {
             c.c_exists[q] = 0;
             c.c_active[q] = 0;
             continue;
         }
         const float radius = sp.radius + c.p_radius[i];
         f3 normal, P;
-        if (!hull::test_sphere(sp.hull, sp.nhv, sp.hull + 3 * sp.nhv, sp.nhf, radius, xi, normal, P)) {
-            c.c_active[q] = 0;
-            continue;
+        if (sp.body1) {
+            if (!body_contact(c, s, q, nn, xi, radius, normal)) {
+                c.c_active[q] = 0;
+                continue;
+            }
+        } else {
+            if (!hull::test_sphere(sp.hull, sp.nhv, sp.hull + 3 * sp.nhv, sp.nhf, radius, mident(), zero3(), xi,
+                                   normal, P)) {
+                c.c_active[q] = 0;
+                continue;
+            }
+            st3(c.c_point, nn, q, hull::xf_mult(P));  // body->GetLocalPoint
         }
-        st3(c.c_point, nn, q, hull::xf_mult(P));  // body->GetLocalPoint
         const f3 n1 = mk(-normal.x, -normal.y, -normal.z);
         const f3 t1 = perp(n1);
         const f3 t2 = cross(t1, n1);
@@ -1024,7 +1069,7 @@ __global__ void k_post(const __grid_constant__ ClothDev one, const __grid_consta
         const bool dyn = is_dynamic(c, i);
         for (uint32_t s = 0; s < c.nsph; ++s) {
             const uint32_t q = s * n + i;
-            if (!c.c_exists[q] && dyn && overlap(lo, hi, c.sph[s])) {
+            if (!c.c_exists[q] && dyn && overlap_shape(c, s, lo, hi)) {
                 c.c_exists[q] = 1;
                 c.c_active[q] = 0;
                 c.c_key[q] = sc->step_index * kMaxSpheres + c.sph[s].rank;

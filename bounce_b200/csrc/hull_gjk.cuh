@@ -257,12 +257,18 @@ __device__ __forceinline__ void witness(const Simplex& s, f3& p1, f3& p2)
     }
 }
 
-// b3GJK between the hull (vertices hv[0, nv)) and the point Q; returns the
-// distance and the witness points (p1 on the hull).
-__device__ __noinline__ float gjk(const float* hv, uint32_t nv, f3 Q, f3& p1, f3& p2)
+// b3Mul(xf, v) and b3MulT(xf.rotation, v) for the hull's body transform
+// (rotation R, column-major, position p); with the identity and the origin
+// they are the static forms above, bit for bit.
+__device__ __forceinline__ f3 xr_mul(const m3& R, f3 p, f3 v) { return ((v.x * R.x + v.y * R.y) + v.z * R.z) + p; }
+__device__ __forceinline__ f3 r_mult(const m3& R, f3 v) { return mk(dot(R.x, v), dot(R.y, v), dot(R.z, v)); }
+
+// b3GJK between the hull (vertices hv[0, nv), in its body's frame R, p) and
+// the point Q; returns the distance and the witness points (p1 on the hull).
+__device__ __noinline__ float gjk(const float* hv, uint32_t nv, const m3 R, const f3 P, f3 Q, f3& p1, f3& p2)
 {
     Simplex s;
-    s.v[0].p1 = xf_mul(mk(hv[0], hv[1], hv[2]));
+    s.v[0].p1 = xr_mul(R, P, mk(hv[0], hv[1], hv[2]));
     s.v[0].p2 = xf_mul(Q);
     s.v[0].p = s.v[0].p2 - s.v[0].p1;
     s.v[0].w = 1.0f;
@@ -285,7 +291,7 @@ __device__ __noinline__ float gjk(const float* hv, uint32_t nv, f3 Q, f3& p1, f3
         const f3 d = search(s);
         if (dot(d, d) < FLT_EPSILON * FLT_EPSILON) break;
         // the hull's support vertex in -d (b3GJKProxy::GetSupportIndex)
-        const f3 dl = xf_mult(neg(d));
+        const f3 dl = r_mult(R, neg(d));
         uint32_t best = 0;
         float bestp = dot(dl, mk(hv[0], hv[1], hv[2]));
         for (uint32_t i = 1; i < nv; ++i) {
@@ -297,7 +303,7 @@ __device__ __noinline__ float gjk(const float* hv, uint32_t nv, f3 Q, f3& p1, f3
         }
         Vtx& x = s.v[s.n];
         x.i1 = best;
-        x.p1 = xf_mul(mk(hv[3 * best], hv[3 * best + 1], hv[3 * best + 2]));
+        x.p1 = xr_mul(R, P, mk(hv[3 * best], hv[3 * best + 1], hv[3 * best + 2]));
         x.p2 = xf_mul(Q);
         x.p = x.p2 - x.p1;
         ++iter;
@@ -316,19 +322,20 @@ __device__ __noinline__ float gjk(const float* hv, uint32_t nv, f3 Q, f3& p1, f3
 }
 
 // b3HullShape::TestSphere for a particle at Q of radius r against the hull
-// (vertices, then planes as normal xyz + offset).  false: no contact.
+// (vertices, then planes as normal xyz + offset, in its body's frame R, P).
+// false: no contact.
 __device__ __forceinline__ bool test_sphere(const float* hv, uint32_t nv, const float* hp, uint32_t nf, float radius,
-                                            f3 Q, f3& normal, f3& point)
+                                            const m3& R, f3 P, f3 Q, f3& normal, f3& point)
 {
     f3 c1, c2;
-    const float distance = gjk(hv, nv, Q, c1, c2);
+    const float distance = gjk(hv, nv, R, P, Q, c1, c2);
     if (distance > radius) return false;
     if (distance > 0.0f) {
         normal = (c2 - c1) / distance;
         point = c1;
         return true;
     }
-    const f3 support = xf_mult(Q);
+    const f3 support = r_mult(R, Q - P);
     uint32_t best = 0;
     float best_sep = -FLT_MAX;
     for (uint32_t f = 0; f < nf; ++f) {
@@ -341,8 +348,8 @@ __device__ __forceinline__ bool test_sphere(const float* hv, uint32_t nv, const 
     }
     // b3Mul(xf, plane) and b3ClosestPointOnPlane (geometry.h:77-100)
     const f3 n0 = mk(hp[4 * best], hp[4 * best + 1], hp[4 * best + 2]);
-    const f3 n = (n0.x * mk(1.0f, 0.0f, 0.0f) + n0.y * mk(0.0f, 1.0f, 0.0f)) + n0.z * mk(0.0f, 0.0f, 1.0f);
-    const float off = hp[4 * best + 3] + dot(n, zero3());
+    const f3 n = (n0.x * R.x + n0.y * R.y) + n0.z * R.z;
+    const float off = hp[4 * best + 3] + dot(n, P);
     const float fraction = dot(n, Q) - off;
     point = Q - fraction * n;
     normal = n;

@@ -410,7 +410,8 @@ __global__ void k_sb_contacts_update(SoftDev d)
             continue;
         }
         f3 normal, P;
-        if (!hull::test_sphere(sp.hull, sp.nhv, sp.hull + 3 * sp.nhv, sp.nhf, sp.radius + d.radius[i], xi, normal, P)) {
+        if (!hull::test_sphere(sp.hull, sp.nhv, sp.hull + 3 * sp.nhv, sp.nhf, sp.radius + d.radius[i], mident(), zero3(),
+                               xi, normal, P)) {
             d.c_active[q] = 0;
             continue;
         }

@@ -130,6 +130,61 @@ b3g_status b3g_cloth_add_static_hull(b3g_cloth* cloth, const float* vertices, ui
                                      const float* planes, uint32_t face_count, float friction, uint32_t* shape_id);
 b3g_status b3g_cloth_clear_colliders(b3g_cloth* cloth);
 
+/* ---- colliders on bodies -------------------------------------------------- */
+
+/* Colliders on rigid bodies of any type, for a cloth in a world whose bodies
+ * move (b3Cloth::SetWorld with b3Body, include/bounce/dynamics/body.h).  The
+ * caller's world keeps stepping the bodies; before each cloth step the caller
+ * gives the cloth every body's state and every body shape's broadphase proxy
+ * as its world has them, and after the step reads them back: the cloth's
+ * contact solver changes dynamic bodies' velocities and sweeps
+ * (cloth_contact_solver.cpp:264-307, 388-472, 620-718) and synchronises the
+ * transform, world inverse inertia and proxies of every non-static body it
+ * touched (cloth_solver.cpp:165-181).  A cloth with any body collider solves
+ * its body contacts in one ordered pass over its contact list on the GPU,
+ * as the reference does: correct for any body type, and serial.  Not with
+ * self-collision (thickness > 0), in a batch or in a server. */
+typedef struct {
+    int32_t type;                 /* b3BodyType: 0 static, 1 kinematic, 2 dynamic */
+    float rotation[9];            /* m_xf.rotation, column-major */
+    float position[3];            /* m_xf.position */
+    float local_center[3];        /* m_sweep.localCenter */
+    float world_center0[3];       /* m_sweep.worldCenter0 */
+    float world_center[3];        /* m_sweep.worldCenter */
+    float orientation0[4];        /* m_sweep.orientation0, x y z w */
+    float orientation[4];         /* m_sweep.orientation */
+    float linear_velocity[3];
+    float angular_velocity[3];
+    float inv_mass;               /* m_invMass */
+    float inv_inertia[9];         /* m_invI, body frame, column-major */
+    float world_inv_inertia[9];   /* m_worldInvI */
+} b3g_body_state;
+
+b3g_status b3g_cloth_add_body(b3g_cloth* cloth, const b3g_body_state* state, uint32_t* body_id);
+b3g_status b3g_cloth_set_body(b3g_cloth* cloth, uint32_t body_id, const b3g_body_state* state);
+b3g_status b3g_cloth_get_body(const b3g_cloth* cloth, uint32_t body_id, b3g_body_state* state);
+/* Shapes on a body, geometry in the body's frame (b3SphereShape,
+ * b3CapsuleShape, b3HullShape); each takes a collider slot (shape_id, shared
+ * with the static colliders) and starts with the proxy
+ * ComputeAABB(m_xf) fattened by B3_AABB_EXTENSION. */
+b3g_status b3g_cloth_add_body_sphere(b3g_cloth* cloth, uint32_t body_id, const float center[3], float radius,
+                                     float friction, uint32_t* shape_id);
+b3g_status b3g_cloth_add_body_capsule(b3g_cloth* cloth, uint32_t body_id, const float a[3], const float b[3],
+                                      float radius, float friction, uint32_t* shape_id);
+b3g_status b3g_cloth_add_body_hull(b3g_cloth* cloth, uint32_t body_id, const float* vertices, uint32_t vertex_count,
+                                   const float* planes, uint32_t face_count, float friction, uint32_t* shape_id);
+/* A body shape's proxy in the caller's world broadphase (b3Shape::GetAABB). */
+b3g_status b3g_cloth_set_shape_proxy(b3g_cloth* cloth, uint32_t shape_id, const float lo[3], const float hi[3]);
+b3g_status b3g_cloth_get_shape_proxy(const b3g_cloth* cloth, uint32_t shape_id, float lo[3], float hi[3]);
+/* The order in which the caller's world query reports the colliders
+ * (b3World::QueryAABB walks its dynamic tree): a particle's new contacts with
+ * several colliders in one step enter the contact list in that order.  By
+ * default the order is derived from the colliders' proxies inserted into a
+ * tree in creation order, which is the world's own while its proxies have
+ * not moved; with moving bodies give the world's order before each step.
+ * count 0 returns to the derived order. */
+b3g_status b3g_cloth_set_report_order(b3g_cloth* cloth, const uint32_t* order, uint32_t count);
+
 /* ---- created particles and mouse forces ------------------------------------ */
 
 /* b3ParticleDef (include/bounce/cloth/particle.h:38-60).  mass 0 makes a
