@@ -136,11 +136,33 @@ def peaks():
 
 
 # DRAM bytes (read + write) of one persistent-CG launch, by (cloth side, CG
-# form), from one ncu capture of that launch (dram__bytes_read.sum +
-# dram__bytes_write.sum).  At 256 x 256 the whole system stays in L2 after
-# its first touch, so the figure holds for any iteration count.  Sizes and
-# forms without a capture report null.
-GRID_CG_TRAFFIC = {(256, "persistent"): 36.53e6 + 0.04e6}
+# form): (bytes of one captured launch, that launch's CG iterations), from
+# one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum).
+# * 256 x 256: the whole system stays in L2 after its first touch, so the
+#   figure holds for any iteration count (None).
+# * 1024 x 1024: the 293 MB system streams from HBM once at the start (A x0)
+#   and once per iteration, so the traffic scales with 1 + iterations (the
+#   captured launch, the third step from rest, ran 10 iterations).
+# Sizes and forms without a capture report null.
+GRID_CG_TRAFFIC = {
+    (256, "persistent"): (36.53e6 + 0.04e6, None),
+    (1024, "persistent"): (4107670528 + 631533568, 10),
+    (1024, "fused"): (3919580160 + 676790272, 10),
+}
+# DRAM bytes over algorithmic bytes of the batched CG launch (512 cloths):
+# 19.46 GB of DRAM traffic against 20.48 GB algorithmic (the average of the
+# run's two timed launches; the captured launch is the second).
+BATCH_CG_TRAFFIC_RATIO = (16734817024 + 2720797440) / 20483036026.0
+
+
+def grid_cg_traffic(side: int, form: str, iterations: float):
+    """DRAM bytes of one persistent-CG launch of `iterations` CG iterations,
+    from the captured launch of the same size and form (null without one)."""
+    cap = GRID_CG_TRAFFIC.get((side, form))
+    if cap is None:
+        return None
+    bytes_, its = cap
+    return bytes_ if its is None else bytes_ * (1.0 + iterations) / (1.0 + its)
 
 
 def algorithmic_bytes(info: dict, kernel: str) -> float:
@@ -312,7 +334,8 @@ def run_ours(args, rank, world):
         "launches": launches, "clocks": clocks.summary(), "info": info,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                      "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": GRID_CG_TRAFFIC.get((args.side, args.cg)) if dom == "grid_cg" else None,
+                     "traffic": (grid_cg_traffic(args.side, args.cg, it_total / len(prof))
+                                 if dom == "grid_cg" else None),
                      "traffic_source": "ncu capture of one launch at this size",
                      "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
                      "share": kern[dom][0] / total if total else None},
@@ -343,8 +366,7 @@ def run_stiff(args, dev: int):
         cloth.set_cg_strategy(True, fused=form == "fused")
         info = cloth.info()
         warm = 3
-        for _ in range(warm):
-            cloth.step(scene.dt)
+        warm_its = [int(cloth.step(scene.dt)["iterations"]) for _ in range(warm)]
         ms, its = [], []
         for _ in range(warm, scene.steps):
             st = cloth.step(scene.dt)
@@ -360,10 +382,13 @@ def run_stiff(args, dev: int):
         forms[form] = {
             "ms_per_step": sum(ms) / len(ms), "vertex_steps_per_s": n * len(ms) / (sum(ms) / 1e3),
             "cg_iterations_mean": float(np.mean(its)), "cg_iterations_max": int(max(its)),
+            "warmup_cg_iterations": warm_its,
             "us_per_cg_iteration": 1e3 * cg_ms / max(cg_it, 1.0),
             "roofline": {"bound": "hbm", "kernel": "grid_cg" if form == "persistent" else "grid_cg_fused",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": GRID_CG_TRAFFIC.get((side, form)),
+                         "frac": achieved / peak, "traffic": grid_cg_traffic(side, form, cg_it),
+                         "dram_frac": (grid_cg_traffic(side, form, cg_it) / (cg_ms / 1e3) / 1e9 / peak
+                                       if grid_cg_traffic(side, form, cg_it) else None),
                          "algorithmic_bytes_per_launch": alg, "avg_launch_ms": cg_ms,
                          "cg_iterations_per_launch": cg_it}}
     best = max(forms, key=lambda f: forms[f]["vertex_steps_per_s"])
@@ -447,6 +472,10 @@ def run_batched(args, dev: int, cpu_sample: bool = False):
                          "peak": peaks()[0], "peak_kind": peaks()[1], "unit": "GB/s",
                          "frac": sum(cg_bytes) / (sum(cg_ms) / 1e3) / 1e9 / peaks()[0],
                          "algorithmic_bytes_per_launch": sum(cg_bytes) / len(cg_bytes),
+                         "traffic": BATCH_CG_TRAFFIC_RATIO * sum(cg_bytes) / len(cg_bytes),
+                         "traffic_source": "DRAM/algorithmic ratio of one captured 512-cloth launch",
+                         "dram_frac": (BATCH_CG_TRAFFIC_RATIO * sum(cg_bytes) / (sum(cg_ms) / 1e3) / 1e9
+                                       / peaks()[0]),
                          "avg_launch_ms": sum(cg_ms) / len(cg_ms), "share": sum(cg_ms) / sum(ms)},
             "l2": "inputs larger than L2 (about 1 GB of resident cloth state)",
             "cpu_baseline": cpu_batch_sample(args.batch_count) if cpu_sample else None}
@@ -844,10 +873,11 @@ def main():
         soft = None if args.skip_softbody else run_softbody(args, local, False)
         selfc = None if args.skip_self else run_self_collision(args, local, False)
         colliders = None if args.skip_colliders else run_colliders(args, local, False)
+        stiff = None if args.skip_stiff else run_stiff(args, local)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "note": "headline skipped (--skip-single)",
                               "batched": batched, "serving": served, "softbody": soft, "self_collision": selfc,
-                              "colliders": colliders}))
+                              "colliders": colliders, "stiff1024": stiff}))
         if world > 1:
             import torch
 

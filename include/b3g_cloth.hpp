@@ -99,6 +99,53 @@ public:
         return id;
     }
     void ClearColliders() { b3gCheck(b3g_cloth_clear_colliders(m_cloth), "ClearColliders"); }
+    // SetWorld(world) with moving bodies: the cloth's copy of a b3Body, the
+    // shapes on it (body frame), and the state exchange around each Step
+    uint32_t AddBody(const b3g_body_state& b)
+    {
+        uint32_t id;
+        b3gCheck(b3g_cloth_add_body(m_cloth, &b, &id), "AddBody");
+        return id;
+    }
+    void SetBody(uint32_t id, const b3g_body_state& b) { b3gCheck(b3g_cloth_set_body(m_cloth, id, &b), "SetBody"); }
+    b3g_body_state GetBody(uint32_t id) const
+    {
+        b3g_body_state b;
+        b3gCheck(b3g_cloth_get_body(m_cloth, id, &b), "GetBody");
+        return b;
+    }
+    uint32_t AddBodySphere(uint32_t body, const float c[3], float radius, float friction)
+    {
+        uint32_t id;
+        b3gCheck(b3g_cloth_add_body_sphere(m_cloth, body, c, radius, friction, &id), "AddBodySphere");
+        return id;
+    }
+    uint32_t AddBodyCapsule(uint32_t body, const float a[3], const float b[3], float radius, float friction)
+    {
+        uint32_t id;
+        b3gCheck(b3g_cloth_add_body_capsule(m_cloth, body, a, b, radius, friction, &id), "AddBodyCapsule");
+        return id;
+    }
+    uint32_t AddBodyHull(uint32_t body, const float* vertices, uint32_t vertexCount, const float* planes,
+                         uint32_t faceCount, float friction)
+    {
+        uint32_t id;
+        b3gCheck(b3g_cloth_add_body_hull(m_cloth, body, vertices, vertexCount, planes, faceCount, friction, &id),
+                 "AddBodyHull");
+        return id;
+    }
+    void SetShapeProxy(uint32_t shape, const float lo[3], const float hi[3])
+    {
+        b3gCheck(b3g_cloth_set_shape_proxy(m_cloth, shape, lo, hi), "SetShapeProxy");
+    }
+    void GetShapeProxy(uint32_t shape, float lo[3], float hi[3]) const
+    {
+        b3gCheck(b3g_cloth_get_shape_proxy(m_cloth, shape, lo, hi), "GetShapeProxy");
+    }
+    void SetReportOrder(const uint32_t* order, uint32_t count)
+    {
+        b3gCheck(b3g_cloth_set_report_order(m_cloth, order, count), "SetReportOrder");
+    }
     void SetSolver(const b3g_solver_opts& o) { b3gCheck(b3g_cloth_set_solver(m_cloth, &o), "SetSolver"); }
     b3gParticle GetParticle(uint32_t i) { return b3gParticle(m_cloth, i); }
     // b3Cloth::CreateParticle / DestroyParticle (cloth.cpp:307-351): a particle

@@ -1,8 +1,9 @@
 """The C++ shim (include/b3g_cloth.hpp) compiles against the C ABI and links
 with libb3g.so.  Without a GPU it reports B3G_ERR_NO_DEVICE through
-b3gError; on a GPU it steps a cloth through a mouse drag, and its final
-positions equal those of the same sequence run through the Python front-end
-(the same library calls, so bit for bit)."""
+b3gError; on a GPU it steps a cloth through a mouse drag and onto a
+kinematic sphere body, and its final positions equal those of the same
+sequence run through the Python front-end (the same library calls, so bit
+for bit)."""
 import os
 import subprocess
 
@@ -34,7 +35,24 @@ int main() {
         c.DestroyForce(f);
         c.DestroyParticle(mp);
         s = c.Step(1.0f / 60.0f, 8, 2);
-        std::printf("stepped %u\n", s.iterations);
+        // a kinematic sphere body rising under the triangle (SetWorld with a b3Body)
+        b3g_body_state b = {};
+        b.type = 1;
+        b.rotation[0] = b.rotation[4] = b.rotation[8] = 1.0f;
+        b.position[0] = b.world_center0[0] = b.world_center[0] = 0.3f;
+        b.position[1] = b.world_center0[1] = b.world_center[1] = -0.3f;
+        b.position[2] = b.world_center0[2] = b.world_center[2] = 0.3f;
+        b.orientation0[3] = b.orientation[3] = 1.0f;
+        b.linear_velocity[1] = 1.0f;
+        uint32_t body = c.AddBody(b);
+        float zero[3] = {0.0f, 0.0f, 0.0f};
+        uint32_t shape = c.AddBodySphere(body, zero, 0.25f, 0.3f);
+        float lo[3], hi[3];
+        c.GetShapeProxy(shape, lo, hi);
+        c.SetShapeProxy(shape, lo, hi);
+        s = c.Step(1.0f / 60.0f, 8, 2);
+        b3g_body_state after = c.GetBody(body);
+        std::printf("stepped %u body %.9g\n", s.iterations, after.position[1]);
         for (uint32_t i = 0; i < 3; ++i) {
             float p[3];
             c.GetParticle(i).GetPosition(p);
@@ -89,6 +107,17 @@ def test_shim_steps_a_cloth_on_the_gpu(b3g, tmp_path):
     cloth.destroy_force(f)
     cloth.destroy_particle(mp)
     cloth.step(1.0 / 60.0, 8, 2)
+    body = np.zeros(55, np.float32)
+    body[0] = 1.0
+    body[[1, 5, 9]] = 1.0
+    for k in (10, 16, 19):
+        body[k:k + 3] = (0.3, -0.3, 0.3)
+    body[25] = body[29] = 1.0
+    body[31] = 1.0
+    bid = cloth.add_body(body)
+    cloth.add_body_sphere(bid, (0.0, 0.0, 0.0), 0.25, 0.3)
+    cloth.step(1.0 / 60.0, 8, 2)
+    assert float(lines[0].split()[-1]) == float(cloth.body(bid)[11])
     x = cloth.positions()
     cloth.close()
     assert np.array_equal(shim_x, x), (shim_x, x)
