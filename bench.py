@@ -492,19 +492,24 @@ def run_softbody(args, dev: int, cpu_sample: bool):
 
     side = args.softbody_side
     scene = b3g.pinned_block_scene(side, side, side, spacing=1.0 / side)
-    body = b3g.SoftBody(scene.vertices, scene.tets, scene.sdef, device=dev).setup(scene)
-    for _ in range(args.warmup):
-        body.step(scene.dt)
-    launches0 = b3g.kernel_launch_count()
-    ms, iters = [], []
-    for _ in range(args.softbody_steps):
-        s = body.step(scene.dt)
-        ms.append(s["step_ms"])
-        iters.append(s["iterations"])
-    launches = b3g.kernel_launch_count() - launches0
-    nnz = body.block_count()
-    body.close()
     n, t = len(scene.vertices), len(scene.tets)
+    by = {}
+    for form in ("launches", "persistent", "fused"):
+        body = b3g.SoftBody(scene.vertices, scene.tets, scene.sdef, device=dev).setup(scene)
+        body.set_cg_strategy(form != "launches", fused=form == "fused")
+        for _ in range(args.warmup):
+            body.step(scene.dt)
+        launches0 = b3g.kernel_launch_count()
+        ms, iters = [], []
+        for _ in range(args.softbody_steps):
+            s = body.step(scene.dt)
+            ms.append(s["step_ms"])
+            iters.append(s["iterations"])
+        launches = b3g.kernel_launch_count() - launches0
+        nnz = body.block_count()
+        body.close()
+        by[form] = {"ms_per_step": sum(ms) / len(ms), "node_steps_per_s": n * len(ms) / (sum(ms) / 1e3),
+                    "cg_iterations_mean": float(np.mean(iters)), "gpu_launches": launches, "steps": len(ms)}
     # algorithmic bytes of one step (FP32): the element kernel reads an
     # element's vertices, rest frame, Ke, B, P and state and writes R, q, eps,
     # f0, f_plastic (1,512 B); the assembly reads R, Ke, f0, f_plastic and the
@@ -512,17 +517,19 @@ def run_softbody(args, dev: int, cpu_sample: bool):
     # the column, the gathered x and the value written (52 B); each CG
     # iteration moves 40 B per block and 164 B per row, the CG start 40 B per
     # block and 100 B per row; the integration 48 B per node.
-    it = float(np.mean(iters))
-    step_bytes = 1512.0 * t + 708.0 * t + 41.0 * n + 52.0 * nnz + (40.0 * nnz + 100.0 * n) + \
-        it * (40.0 * nnz + 164.0 * n) + 48.0 * n
-    achieved = step_bytes / (sum(ms) / len(ms) / 1e3) / 1e9
+    for form, f in by.items():
+        it = f["cg_iterations_mean"]
+        step_bytes = 1512.0 * t + 708.0 * t + 41.0 * n + 52.0 * nnz + (40.0 * nnz + 100.0 * n) + \
+            it * (40.0 * nnz + 164.0 * n) + 48.0 * n
+        achieved = step_bytes / (f["ms_per_step"] / 1e3) / 1e9
+        f["roofline"] = {"bound": "hbm", "kernel": "whole step", "achieved": achieved, "peak": peaks()[0],
+                         "peak_kind": peaks()[1], "unit": "GB/s", "frac": achieved / peaks()[0],
+                         "algorithmic_bytes_per_step": step_bytes}
     out = {"workload": f"block{side}x{side}x{side}_pinned", "nodes": n, "tetrahedra": t, "blocks": nnz,
-           "node_steps_per_s": n * len(ms) / (sum(ms) / 1e3), "ms_per_step": sum(ms) / len(ms),
-           "cg_iterations_mean": it, "cg": "reference rule (20 iterations, f32 dots)",
-           "gpu_launches": launches, "steps": len(ms),
-           "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": achieved, "peak": peaks()[0],
-                        "peak_kind": peaks()[1], "unit": "GB/s", "frac": achieved / peaks()[0],
-                        "algorithmic_bytes_per_step": step_bytes}}
+           "cg": "reference rule (20 iterations, f32 dots)",
+           "cg_strategy": "persistent cooperative launch (the default)"}
+    out.update(by["persistent"])
+    out["by_strategy"] = by
     if cpu_sample:
         import oracle
 
@@ -829,6 +836,9 @@ def summary(line: dict) -> dict:
         "serving_tick_p99_ms": g(s, "p99_step_ms"), "serving_busy": g(s, "device_busy_fraction"),
         "serving_seconds_offered": g(s, "seconds_offered"),
         "stiff1024_vertex_steps_per_s": g(st, "vertex_steps_per_s"), "stiff1024_frac": g(st, "roofline", "frac"),
+        "stiff1024_dram_frac": g(st, "roofline", "dram_frac"), "batched_dram_frac": g(b, "roofline", "dram_frac"),
+        "softbody_node_steps_per_s": g(line.get("softbody"), "node_steps_per_s"),
+        "softbody_frac": g(line.get("softbody"), "roofline", "frac"),
     }
 
 

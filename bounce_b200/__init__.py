@@ -259,6 +259,7 @@ def lib() -> C.CDLL:
             "b3g_softbody_set_velocity": [vp, u32, vp],
             "b3g_softbody_set_position": [vp, u32, vp],
             "b3g_softbody_set_solver": [vp, C.POINTER(SolverOptsC)],
+            "b3g_softbody_set_cg_strategy": [vp, i32],
             "b3g_softbody_step": [vp, f32, u32, u32, C.POINTER(StepStatsC)],
             "b3g_softbody_read_state": [vp, vp, vp],
             "b3g_softbody_write_state": [vp, vp, vp],
@@ -920,6 +921,13 @@ class SoftBody:
     def set_solver(self, o: SolverOptions) -> None:
         c = SolverOptsC(o.stop_rule, o.tolerance, o.max_iterations, o.dot)
         check(lib().b3g_softbody_set_solver(self.h, C.byref(c)), "softbody_set_solver")
+
+    def set_cg_strategy(self, persistent: bool, fused: bool = False) -> None:
+        """True (the default): the MPCG as one persistent cooperative launch
+        (fused: one grid reduction per iteration); False: three launches per
+        CG iteration."""
+        code = 0 if not persistent else 2 if fused else 1
+        check(lib().b3g_softbody_set_cg_strategy(self.h, code), "softbody_set_cg_strategy")
 
     def add_hull(self, vertices, planes, friction: float) -> int:
         """A static convex hull the nodes collide with: vertices (n, 3) and

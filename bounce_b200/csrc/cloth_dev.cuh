@@ -128,6 +128,11 @@ struct ClothDev {
     b3g_body_state* bodies;     // the bodies of body colliders (device copies), nbody of them
     float* shape_fat;           // per collider its world-broadphase proxy (lo xyz, hi xyz); body shapes only
     uint32_t nbody;
+    // the soft body's MPCG mode of the persistent CG (a soft body's system
+    // viewed as a ClothDev): x0 unfiltered, b_delta with diag(A), which
+    // cg_diag holds (3 planes); 0 for cloths
+    uint32_t cg_soft;
+    const float* cg_diag;
 
     StepScalars* sc;
     GridBarrier* bar;           // persistent-CG grid barrier

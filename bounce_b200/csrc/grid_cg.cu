@@ -289,7 +289,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ C
     if (ONE_ROW && act) load_reg_row(c, first_row, rr);
     if (SMEM_A && act) stage_row_blocks(c, rr.base, rr.deg, smem_a, B, tid);
 
-    // x0 = S m_x, r = S (b - A x0), z = S P^-1 r (cloth_force_solver.cpp:90-100)
+    // x0 = S m_x, r = S (b - A x0), z = S P^-1 r (cloth_force_solver.cpp:90-100);
+    // the soft body's MPCG (cg_soft) starts from x0 on every row and takes
+    // b_delta = Sb . diag(A) Sb (softbody_force_solver.cpp:93-127)
     T v2[2] = {D::zero(), D::zero()};
     for (uint32_t row = first_row; row < n; row += stride) {
         const bool Sr = dyn(c, row);
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ C
             for (int k = 0; k < kRegCols; ++k) {
                 if ((uint32_t)k < rr.deg) {
                     const uint32_t col = rr.col[k];
-                    const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
+                    const f3 xj = (c.cg_soft || dyn(c, col)) ? ld3(c.mx, n, col) : zero3();
                     ax = ax + block_at(c, rr.base + 32u * k) * xj;
                 }
             }
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ C
             for (uint32_t k = 0; k < deg; ++k) {
                 const uint32_t idx = base + 32u * k;
                 const uint32_t col = c.cols[idx];
-                const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
+                const f3 xj = (c.cg_soft || dyn(c, col)) ? ld3(c.mx, n, col) : zero3();
                 ax = ax + block_at(c, idx) * xj;
             }
         }
@@ -318,7 +320,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ C
         const f3 rv = Sr ? bi - ax : zero3();
         const f3 zv = Sr ? mk(rv.x * pvr.x, rv.y * pvr.y, rv.z * pvr.z) : zero3();
         const f3 bh = Sr ? bi : zero3();
-        const f3 x0 = Sr ? ld3(c.mx, n, row) : zero3();
+        const f3 x0 = (c.cg_soft || Sr) ? ld3(c.mx, n, row) : zero3();
         st3(c.z, n, row, zv);
         if (ONE_ROW) {
             Si = Sr, x = x0, r = rv, z = zv, pv = pvr;
@@ -326,7 +328,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg(const __grid_constant__ C
             st3(c.dv, n, row, x0);
             st3(c.r, n, row, rv);
         }
-        v2[0] = D::add_term(v2[0], bh, mk(bh.x * pvr.x, bh.y * pvr.y, bh.z * pvr.z));
+        const f3 w = c.cg_soft ? ld3(c.cg_diag, n, row) : pvr;
+        v2[0] = D::add_term(v2[0], bh, mk(bh.x * w.x, bh.y * w.y, bh.z * w.z));
         v2[1] = D::add_term(v2[1], rv, zv);
         if (ONE_ROW) break;
     }
@@ -641,7 +644,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
             for (int k = 0; k < kRegCols; ++k) {
                 if ((uint32_t)k < rr.deg) {
                     const uint32_t col = rr.col[k];
-                    const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
+                    const f3 xj = (c.cg_soft || dyn(c, col)) ? ld3(c.mx, n, col) : zero3();
                     const m3 a = block_at(c, rr.base + 32u * k);
                     ax = ax + a * xj;
                 }
@@ -652,7 +655,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
             for (uint32_t k = 0; k < deg; ++k) {
                 const uint32_t idx = base + 32u * k;
                 const uint32_t col = c.cols[idx];
-                const f3 xj = dyn(c, col) ? ld3(c.mx, n, col) : zero3();
+                const f3 xj = (c.cg_soft || dyn(c, col)) ? ld3(c.mx, n, col) : zero3();
                 ax = ax + block_at(c, idx) * xj;
             }
         }
@@ -662,14 +665,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_grid_cg_fused(const __grid_consta
         const f3 spr = Sr ? pvr : zero3();
         const f3 zv = hadamard(rv, spr);
         const f3 bh = Sr ? bi : zero3();
-        const f3 x0 = Sr ? ld3(c.mx, n, row) : zero3();
+        const f3 x0 = (c.cg_soft || Sr) ? ld3(c.mx, n, row) : zero3();
         st_rec(rec0, row, rv, zero3(), zero3(), spr);
         if (ONE_ROW) {
             Si = Sr, x = x0, r = rv, sp = spr;
         } else {
             st3(c.dv, n, row, x0);
         }
-        v2[0] = D::add_term(v2[0], bh, mk(bh.x * pvr.x, bh.y * pvr.y, bh.z * pvr.z));
+        const f3 w = c.cg_soft ? ld3(c.cg_diag, n, row) : pvr;
+        v2[0] = D::add_term(v2[0], bh, mk(bh.x * w.x, bh.y * w.y, bh.z * w.z));
         v2[1] = D::add_term(v2[1], rv, zv);
         if (ONE_ROW) break;
     }

@@ -30,10 +30,13 @@ GridCgShape grid_cg_shape(uint32_t n, int device, bool fused);
 // Cooperative launch over the current device, shaped by grid_cg_shape():
 // two grid reductions per iteration.
 cudaError_t launch_grid_cg(const ClothDev& c, int dot, GridBarrier* bar, cudaStream_t st);
-// The fused form, one grid reduction per iteration.  `rec`: device scratch
+// The fused form, one grid reduction per iteration; slot 0 of every row must
+// hold the row's diagonal block (it multiplies the row's own direction,
+// formed in registers).  `rec`: device scratch
 // of grid_cg_fused_rec_bytes(n) bytes, 16-byte aligned (the per-vertex
 // records of two consecutive iterations).
 cudaError_t launch_grid_cg_fused(const ClothDev& c, int dot, GridBarrier* bar, float4* rec, cudaStream_t st);
 inline size_t grid_cg_fused_rec_bytes(uint32_t n) { return 2 * 3 * sizeof(float4) * (size_t)n; }
+
 
 }  // namespace b3g

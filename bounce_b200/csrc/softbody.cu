@@ -27,6 +27,7 @@
 
 #include "../../include/b3g.h"
 #include "cloth_dev.cuh"
+#include "grid_cg.cuh"
 #include "mpcg_solve.cuh"
 #include "hull_gjk.cuh"
 #include "softbody_prep.h"
@@ -65,6 +66,21 @@ struct SoftDev {
     int* min_sep;                   // per position iteration, order-preserving ints
     uint32_t* active_count;
     uint32_t vel_iters, pos_iters;
+
+    // The system again in the cloth's SELL-32 layout for the persistent CG
+    // (null until the first persistent solve): slot k of row r at
+    // sell_off[r / 32] + 32 k + r % 32 of each of the 9 value planes; slot 0
+    // is the diagonal block, as in the cloth's layout (the fused CG relies on
+    // it), the other slots follow in the row list's order; b, x0 (= v), P^-1
+    // and diag(A) as 3 planes of n.
+    // The rows are reordered by degree there (sell_inv: node -> row), so
+    // that every slice holds rows of one width; sb_type is the node types in
+    // that order.
+    float* sell_vals;
+    const uint32_t *sell_off, *sell_inv;
+    uint32_t sell_E;
+    float *sb_b, *sb_x0, *sb_pinv, *sb_diag;
+    uint8_t* sb_type;
 };
 
 namespace {
@@ -330,6 +346,20 @@ __global__ void __launch_bounds__(32 * kAsmWarps, 8) k_sb_assemble(SoftDev d, fl
             if (slot == dg) a = (M + h * diag3(cd)) + hh * acc;
             else a = mzero() + hh * acc;
             stm(vals + 9 * slot, a);
+            if (d.sell_vals) {
+                // the SELL copy keeps the diagonal block in slot 0, then the rest in order
+                const uint32_t ri = d.sell_inv[i];
+                const uint32_t ss = slot == dg ? 0u : slot < dg ? slot + 1u : slot;
+                float* sv = d.sell_vals + d.sell_off[ri >> 5] + 32u * ss + (ri & 31u);
+                const size_t E = d.sell_E;
+                sv[0] = a.x.x, sv[E] = a.x.y, sv[2 * E] = a.x.z;
+                sv[3 * E] = a.y.x, sv[4 * E] = a.y.y, sv[5 * E] = a.y.z;
+                sv[6 * E] = a.z.x, sv[7 * E] = a.z.y, sv[8 * E] = a.z.z;
+                if (slot == dg) {
+                    st3(d.sb_pinv, d.n, ri, mk(1.0f / a.x.x, 1.0f / a.y.y, 1.0f / a.z.z));
+                    st3(d.sb_diag, d.n, ri, mk(a.x.x, a.y.y, a.z.z));
+                }
+            }
         }
     }
     if (lane == 0) {
@@ -338,8 +368,15 @@ __global__ void __launch_bounds__(32 * kAsmWarps, 8) k_sb_assemble(SoftDev d, fl
         f3 fe = ldv(d.f, i);
         if (dyn) fe = fe + m * mk(d.gx, d.gy, d.gz);
         const f3 mv = zero3() + M * ldv(d.v, i);
-        stv(d.b, i, mv - h * ((kp + f0n) - (fp + fe)));
+        const f3 bi = mv - h * ((kp + f0n) - (fp + fe));
+        stv(d.b, i, bi);
         d.S[i] = dyn ? 1.0f : 0.0f;
+        if (d.sell_vals) {
+            const uint32_t ri = d.sell_inv[i];
+            st3(d.sb_b, d.n, ri, bi);
+            st3(d.sb_x0, d.n, ri, ldv(d.v, i));
+            d.sb_type[ri] = d.type[i];
+        }
     }
 }
 
@@ -641,6 +678,14 @@ __global__ void k_sb_node_op(SoftDev d, uint32_t i, int op, float a, float b, fl
 constexpr uint32_t kBlock = 256;
 inline uint32_t blocks_for(uint32_t n) { return (n + kBlock - 1) / kBlock; }
 
+// The solution's planes, in row order, back to xyz per node, where the
+// integration and the contact solve read it.
+__global__ void k_sb_from_planes(const float* dv, const uint32_t* inv, float* xsol, uint32_t n)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        stv(xsol, i, ld3(dv, n, inv[i]));
+}
+
 }  // namespace
 
 }  // namespace b3g
@@ -662,6 +707,12 @@ struct b3g_softbody {
     void* cbuf = nullptr;                 // node radius, friction, proxies, position-iteration words
     void* slots = nullptr;                // contact slots for kMaxSpheres hulls
     std::vector<void*> hull_bufs;         // device copies of the hulls' vertices and planes
+    bool persistent = true;               // the MPCG as one persistent launch (else three launches per iteration)
+    void* pcg = nullptr;                  // its SELL copy of the system, vectors, partials and grid barrier
+    b3g::ClothDev view{};                 // the system as the persistent CG sees it
+    b3g::GridBarrier* bar = nullptr;
+    float4* rec = nullptr;                // the fused form's per-row records
+    bool fused = false;                   // one grid reduction per CG iteration
 };
 
 namespace {
@@ -679,6 +730,138 @@ b3g_status cuda_status(cudaError_t e)
     } while (0)
 
 bool ok(const b3g_softbody* b) { return b && b->dev.n > 0; }
+
+// The soft body's system in the cloth's SELL-32 layout, for the persistent
+// CG: the pattern built from the row lists on the host once, the buffers
+// (values, the solve's vectors as planes, partials, grid barrier) made on
+// first use.  The assembly then writes the values there as well.
+b3g_status ensure_sell(b3g_softbody* b)
+{
+    if (b->pcg) return B3G_OK;
+    const uint32_t n = b->dev.n;
+    const uint32_t nslices = (n + 31) / 32;
+    // rows by degree, widest first, node order within a degree
+    std::vector<uint32_t> perm(n), inv(n);
+    for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+    auto degree = [&](uint32_t i) { return b->rowptr[i + 1] - b->rowptr[i]; };
+    std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) { return degree(x) > degree(y); });
+    for (uint32_t r = 0; r < n; ++r) inv[perm[r]] = r;
+    std::vector<uint32_t> off(nslices + 1, 0);
+    std::vector<uint8_t> deg(n);
+    uint32_t max_deg = 0;
+    for (uint32_t q = 0; q < nslices; ++q) {
+        uint32_t w = 0;
+        for (uint32_t r = 32 * q; r < std::min(n, 32 * q + 32); ++r) {
+            const uint32_t d = degree(perm[r]);
+            deg[r] = (uint8_t)d;
+            w = std::max(w, d);
+        }
+        max_deg = std::max(max_deg, w);
+        off[q + 1] = off[q] + 32 * w;
+    }
+    const uint32_t E = off[nslices];
+    std::vector<uint32_t> cols(E);
+    for (uint32_t r = 0; r < n; ++r) {
+        const uint32_t i = perm[r];
+        const uint32_t width = (off[r / 32 + 1] - off[r / 32]) / 32;  // the slice's widest row
+        const uint32_t dg = b->diag[i] - b->rowptr[i];
+        for (uint32_t k = 0; k < width; ++k) cols[off[r / 32] + 32 * k + (r & 31)] = r;  // padding
+        for (uint32_t k = 0; k < deg[r]; ++k) {
+            const uint32_t ss = k == dg ? 0u : k < dg ? k + 1u : k;  // the diagonal block first
+            cols[off[r / 32] + 32 * ss + (r & 31)] = inv[b->cols[b->rowptr[i] + k]];
+        }
+    }
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t plane = al(3 * (size_t)n * sizeof(float));
+    const size_t bytes = al((nslices + 1) * 4) + al(n) + al((size_t)E * 4) + al((size_t)E * 36) + 10 * plane +
+                         al(kGridCgPartialBytes) + al(sizeof(GridBarrier)) + al((size_t)n * 4) + al(n) +
+                         al(grid_cg_fused_rec_bytes(n));
+    SB_TRY(cudaMalloc(&b->pcg, bytes));
+    char* q = static_cast<char*>(b->pcg);
+    auto take = [&](size_t x) {
+        char* r = q;
+        q += al(x);
+        return r;
+    };
+    uint32_t* d_off = (uint32_t*)take((nslices + 1) * 4);
+    uint8_t* d_deg = (uint8_t*)take(n);
+    uint32_t* d_cols = (uint32_t*)take((size_t)E * 4);
+    float* d_vals = (float*)take((size_t)E * 36);
+    float* planes[10];
+    for (float*& f : planes) f = (float*)take(3 * (size_t)n * sizeof(float));
+    void* partials = take(kGridCgPartialBytes);
+    GridBarrier* bar = (GridBarrier*)take(sizeof(GridBarrier));
+    uint32_t* d_inv = (uint32_t*)take((size_t)n * 4);
+    uint8_t* d_type = (uint8_t*)take(n);
+    b->rec = (float4*)take(grid_cg_fused_rec_bytes(n));
+    cudaStream_t s = b->stream;
+    SB_TRY(cudaMemcpyAsync(d_inv, inv.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    SB_TRY(cudaMemcpyAsync(d_off, off.data(), (nslices + 1) * 4, cudaMemcpyHostToDevice, s));
+    SB_TRY(cudaMemcpyAsync(d_deg, deg.data(), n, cudaMemcpyHostToDevice, s));
+    SB_TRY(cudaMemcpyAsync(d_cols, cols.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
+    SB_TRY(cudaMemsetAsync(d_vals, 0, (size_t)E * 36, s));
+    SB_TRY(cudaStreamSynchronize(s));  // the host vectors go out of scope
+    SoftDev& d = b->dev;
+    d.sell_vals = d_vals;
+    d.sell_off = d_off;
+    d.sell_inv = d_inv;
+    d.sb_type = d_type;
+    d.sell_E = E;
+    d.sb_b = planes[0];
+    d.sb_x0 = planes[1];
+    d.sb_pinv = planes[2];
+    d.sb_diag = planes[3];
+    ClothDev& v = b->view;
+    v = ClothDev{};
+    v.n = n;
+    v.nslices = nslices;
+    v.max_deg = max_deg;
+    v.E = E;
+    v.slice_off = d_off;
+    v.row_deg = d_deg;
+    v.cols = d_cols;
+    v.vals = d_vals;
+    v.b = planes[0];
+    v.mx = planes[1];
+    v.pinv = planes[2];
+    v.cg_diag = planes[3];
+    v.dv = planes[4];
+    v.r = planes[5];
+    v.p = planes[6];
+    v.p2 = planes[7];
+    v.s = planes[8];
+    v.z = planes[9];
+    v.type = d_type;
+    v.sc = b->cs.sc;
+    v.partials = partials;
+    v.cg_soft = 1;
+    b->bar = bar;
+    return B3G_OK;
+}
+
+// The soft body's MPCG (softbody_force_solver.cpp:93-164) as the cloth's
+// persistent cooperative CG in its soft body mode, on the SELL copy of the
+// system the assembly just wrote.
+b3g_status persistent_cg(b3g_softbody* b, cudaStream_t s, StepScalars* h)
+{
+    const ClothDev& v = b->view;
+    StepScalars init;
+    std::memset(&init, 0, sizeof(init));
+    init.max_iter = b->opts.max_iterations;
+    init.stop_rule = (int)b->opts.stop_rule;
+    init.tol = b->opts.tolerance;
+    init.dot = (int)b->opts.dot;
+    SB_TRY(cudaMemcpyAsync(v.sc, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+    SB_TRY(cudaMemsetAsync(b->bar, 0, sizeof(GridBarrier), s));
+    SB_TRY(b->fused ? launch_grid_cg_fused(v, (int)b->opts.dot, b->bar, b->rec, s)
+                    : launch_grid_cg(v, (int)b->opts.dot, b->bar, s));
+    k_sb_from_planes<<<blocks_for(v.n), kBlock, 0, s>>>(v.dv, b->dev.sell_inv, b->cs.x, v.n);
+    count_launches(1);
+    SB_TRY(cudaGetLastError());
+    SB_TRY(cudaMemcpyAsync(h, v.sc, sizeof(StepScalars), cudaMemcpyDeviceToHost, s));
+    SB_TRY(cudaStreamSynchronize(s));
+    return B3G_OK;
+}
 
 b3g_status node_op(b3g_softbody* b, uint32_t i, int op, float x, float y, float z)
 {
@@ -874,9 +1057,20 @@ b3g_status b3g_softbody_destroy(b3g_softbody* b)
     if (b->arena) cudaFree(b->arena);
     if (b->cbuf) cudaFree(b->cbuf);
     if (b->slots) cudaFree(b->slots);
+    if (b->pcg) cudaFree(b->pcg);
     for (void* p : b->hull_bufs) cudaFree(p);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
+    return B3G_OK;
+}
+
+b3g_status b3g_softbody_set_cg_strategy(b3g_softbody* b, b3g_cg_strategy strategy)
+{
+    if (!ok(b) || (strategy != B3G_CG_LAUNCHES && strategy != B3G_CG_PERSISTENT &&
+                   strategy != B3G_CG_PERSISTENT_FUSED))
+        return B3G_ERR_INVALID_ARGUMENT;
+    b->persistent = strategy != B3G_CG_LAUNCHES;
+    b->fused = strategy == B3G_CG_PERSISTENT_FUSED;
     return B3G_OK;
 }
 
@@ -952,11 +1146,15 @@ b3g_status b3g_softbody_step(b3g_softbody* b, float dt, uint32_t velocity_iterat
     StepScalars h;
     std::memset(&h, 0, sizeof(h));
     if (dt > 0.0f) {
+        if (b->persistent) {
+            const b3g_status es = ensure_sell(b);
+            if (es != B3G_OK) return es;
+        }
         k_sb_elements<<<blocks_for(d.t), kBlock, 0, s>>>(d, dt, 1.0f / dt);
         k_sb_assemble<<<(d.n + kAsmWarps - 1) / kAsmWarps, 32 * kAsmWarps, 0, s>>>(d, dt);
         count_launches(2);
         SB_TRY(cudaGetLastError());
-        const b3g_status r = csr_run(b->cs, &b->opts, s, &h);
+        const b3g_status r = b->persistent ? persistent_cg(b, s, &h) : csr_run(b->cs, &b->opts, s, &h);
         if (r != B3G_OK) return r;
         if (d.nhull) {
             k_sb_contact_solve<<<blocks_for(d.n), kBlock, 0, s>>>(d, dt);

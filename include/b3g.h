@@ -569,6 +569,14 @@ b3g_status b3g_softbody_set_velocity(b3g_softbody* body, uint32_t node, const fl
 b3g_status b3g_softbody_set_position(b3g_softbody* body, uint32_t node, const float* position);
 /* Default: the reference's MPCG (20 iterations, FLT_EPSILON^2, FP32 dots). */
 b3g_status b3g_softbody_set_solver(b3g_softbody* body, const b3g_solver_opts* opts);
+/* How the MPCG runs: B3G_CG_PERSISTENT (the default) is one cooperative
+ * launch per solve with two grid reductions per iteration, on a copy of the
+ * system in the cloth's SELL-32 layout with its rows ordered by degree;
+ * B3G_CG_PERSISTENT_FUSED the same with one grid reduction per iteration;
+ * B3G_CG_LAUNCHES three launches per iteration on the block-CSR system.
+ * All solve the same system by the same rule; their dot products sum in
+ * different orders. */
+b3g_status b3g_softbody_set_cg_strategy(b3g_softbody* body, b3g_cg_strategy strategy);
 /* b3SoftBody::Step (softbody.cpp:700-735) without a world.  stats->delta0 is
  * r.P^-1 r at the CG start, b_delta the soft body's delta_0 (Sb . diag(A) Sb).
  * At most B3G_MAX_POSITION_ITERATIONS position iterations. */

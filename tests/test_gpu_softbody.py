@@ -55,13 +55,17 @@ def test_softbody_system_bit_exact(b3g, port):
         ora.step(scene.dt)
 
 
+@pytest.mark.parametrize("form", ["persistent", "fused", "launches"])
 @pytest.mark.parametrize("dot", [0, 2])
-def test_softbody_step_matches_oracle(b3g, port, dot):
+def test_softbody_step_matches_oracle(b3g, port, dot, form):
     """Each step starts the oracle from the GPU's state (positions,
-    velocities, element rotations and plastic strains)."""
+    velocities, element rotations and plastic strains); the MPCG as one
+    persistent launch (two grid reductions per iteration, or one) and as
+    three launches per iteration."""
     scene = b3g.pinned_block_scene(5, 4, 3, spacing=0.5)
     opts = b3g.SolverOptions.reference() if dot == 0 else b3g.SolverOptions.relative(1e-5, 200, dot)
     gpu, ora = _pair(b3g, port, scene, opts)
+    gpu.set_cg_strategy(form != "launches", fused=form == "fused")
     gpu.set_node_type(3, 1)
     ora.set_type(3, 1)
     gpu.set_velocity(3, [0.2, 0.0, 0.0])
@@ -107,6 +111,32 @@ def test_softbody_against_reference_golden(b3g, port):
     print("soft body drift against the reference (m) at the kept steps:", drift)
     assert drift[0] <= 1e-5
     assert max(drift) <= 1e-2
+
+
+def test_softbody_persistent_cg_large_block(b3g, port):
+    """The persistent MPCG on a block with more rows than the GPU has
+    threads in one pass of one-row CTAs (several rows per thread), at a
+    relative stop: one step from identical state against the oracle and
+    against the three-launch form."""
+    scene = b3g.pinned_block_scene(48, 48, 48, spacing=1.0 / 48)
+    opts = b3g.SolverOptions.relative(1e-5, 400, 2)
+    gpu, ora = _pair(b3g, port, scene, opts)
+    other = b3g.SoftBody(scene.vertices, scene.tets, scene.sdef).setup(scene, opts)
+    other.set_cg_strategy(False)
+    for _ in range(3):
+        gpu.step(scene.dt)
+    st, el = gpu.state(), gpu.elements()
+    _sync(gpu, ora)
+    other.write_state(st["x"], st["v"])
+    other.write_elements(el["q"], el["eps"])
+    g = gpu.step(scene.dt)
+    o = ora.step(scene.dt)
+    h = other.step(scene.dt)
+    assert abs(g["iterations"] - o["iterations"]) <= 1, (g["iterations"], o["iterations"])
+    assert abs(g["iterations"] - h["iterations"]) <= 1, (g["iterations"], h["iterations"])
+    assert rel_err(gpu.state()["x"], ora.state()["x"]) <= 1e-4
+    assert rel_err(gpu.state()["v"], ora.state()["v"]) <= 1e-3
+    assert rel_err(gpu.state()["x"], other.state()["x"]) <= 1e-4
 
 
 def test_softbody_free_fall_matches_oracle_bulk(b3g, port):
