@@ -288,17 +288,12 @@ b3g_status b3g_batch_get_schedule(const b3g_batch* b, b3g_batch_schedule* s)
 
 }  // extern "C"
 
-b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, float dt, uint32_t vel_iters,
-                           uint32_t pos_iters, b3g_step_stats* per_cloth, b3g_batch_stats* stats, bool use_graph)
+// Waits for the cloths' queued edits and earlier work: the edits go first,
+// on the batch's stream; earlier work on the cloths' own streams is waited
+// for once per distinct stream (a server's cloths share one).
+static b3g_status sync_inputs(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, cudaStream_t st)
 {
-    b3g_status s = check_list(b, cloths, count);
-    if (s != B3G_OK) return s;
-    if (!(dt > 0.0f) || pos_iters > (uint32_t)kMaxPosIters) return B3G_ERR_INVALID_ARGUMENT;
-    cudaSetDevice(b->device);
-    cudaStream_t st = b->stream;
-    // queued particle edits go first, on the batch's stream; earlier work on
-    // the cloths' own streams is waited for once per distinct stream (a
-    // server's cloths share one)
+    b3g_status s;
     std::vector<cudaStream_t> waited;
     for (uint32_t k = 0; k < count; ++k) {
         if (!cloths[k]->pending.empty() && (s = flush_ops_on(cloths[k], st)) != B3G_OK) return s;
@@ -309,24 +304,92 @@ b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t coun
         }
     }
     B3G_TRY(cudaStreamSynchronize(st));
-    if (!use_graph) {
-        destroy_graph(b);
-        plan(b, cloths, count);
-        for (uint32_t k = 0; k < count; ++k) fill_step_scalars(cloths[k], dt, vel_iters, pos_iters, b->h_stage + k);
-        B3G_TRY(cudaEventRecord(b->ev0, st));
-        uint32_t kern = 0;
-        if ((s = enqueue(b, count, pos_iters, st, &kern)) != B3G_OK) return s;
-        B3G_TRY(cudaEventRecord(b->ev1, st));
-        B3G_TRY(cudaStreamSynchronize(st));
+    return B3G_OK;
+}
+
+// One step of the cloths, launched without a graph; returns once the work
+// is queued.  batch_step_finish waits for it and collects the statistics.
+b3g_status batch_step_launch(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, float dt, uint32_t vel_iters,
+                             uint32_t pos_iters)
+{
+    b3g_status s = check_list(b, cloths, count);
+    if (s != B3G_OK) return s;
+    if (!(dt > 0.0f) || pos_iters > (uint32_t)kMaxPosIters) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    cudaStream_t st = b->stream;
+    if ((s = sync_inputs(b, cloths, count, st)) != B3G_OK) return s;
+    destroy_graph(b);
+    plan(b, cloths, count);
+    for (uint32_t k = 0; k < count; ++k) fill_step_scalars(cloths[k], dt, vel_iters, pos_iters, b->h_stage + k);
+    B3G_TRY(cudaEventRecord(b->ev0, st));
+    uint32_t kern = 0;
+    if ((s = enqueue(b, count, pos_iters, st, &kern)) != B3G_OK) return s;
+    B3G_TRY(cudaEventRecord(b->ev1, st));
+    return B3G_OK;
+}
+
+// The statistics of the step just run, per cloth and for the batch.
+static b3g_status collect(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, b3g_step_stats* per_cloth,
+                          b3g_batch_stats* stats)
+{
+    float ms = 0.0f, cg_ms = 0.0f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    if (cudaEventElapsedTime(&cg_ms, b->ev_cg0, b->ev_cg1) != cudaSuccess) {
+        cudaGetLastError();
+        cg_ms = 0.0f;
     }
+    uint32_t it_total = 0, it_max = 0, status = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        const StepScalars& h = b->h_stage[k];
+        record_stats(cloths[k], h, ms, true);
+        if (per_cloth) per_cloth[k] = cloths[k]->last;
+        it_total += h.iter;
+        it_max = std::max(it_max, h.iter);
+        if (h.status) status = h.status;
+    }
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->count = count;
+        stats->rows = b->total_rows;
+        stats->step_ms = ms;
+        stats->cg_ms = cg_ms;
+        stats->cg_iterations_total = it_total;
+        stats->cg_iterations_max = it_max;
+        stats->tasks = b->ntasks;
+    }
+    return status ? (b3g_status)status : B3G_OK;
+}
+
+b3g_status batch_step_finish(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, b3g_step_stats* per_cloth,
+                             b3g_batch_stats* stats)
+{
+    cudaSetDevice(b->device);
+    B3G_TRY(cudaStreamSynchronize(b->stream));
+    return collect(b, cloths, count, per_cloth, stats);
+}
+
+b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, float dt, uint32_t vel_iters,
+                           uint32_t pos_iters, b3g_step_stats* per_cloth, b3g_batch_stats* stats, bool use_graph)
+{
+    if (!use_graph) {
+        b3g_status s = batch_step_launch(b, cloths, count, dt, vel_iters, pos_iters);
+        if (s != B3G_OK) return s;
+        return batch_step_finish(b, cloths, count, per_cloth, stats);
+    }
+    b3g_status s = check_list(b, cloths, count);
+    if (s != B3G_OK) return s;
+    if (!(dt > 0.0f) || pos_iters > (uint32_t)kMaxPosIters) return B3G_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    cudaStream_t st = b->stream;
+    if ((s = sync_inputs(b, cloths, count, st)) != B3G_OK) return s;
     uint32_t hulls_now = 0;
     for (uint32_t k = 0; k < count; ++k)
         for (uint32_t q = 0; q < cloths[k]->dev.nsph; ++q) hulls_now |= cloths[k]->dev.sph[q].kind == 2 ? 1u : 0u;
-    bool same = !use_graph || (b->exec && b->graph_pi == pos_iters && b->graph_sched == b->sched_version &&
+    bool same = (b->exec && b->graph_pi == pos_iters && b->graph_sched == b->sched_version &&
                 b->graph_hulls == hulls_now &&
                 b->graph_list.size() == count && std::equal(b->graph_list.begin(), b->graph_list.end(), cloths));
     // a cloth laid out again (particles or forces created) has new sizes and buffers
-    for (uint32_t k = 0; same && use_graph && k < count; ++k) same = b->graph_layouts[k] == cloths[k]->layout_version;
+    for (uint32_t k = 0; same && k < count; ++k) same = b->graph_layouts[k] == cloths[k]->layout_version;
     if (!same) {
         destroy_graph(b);
         plan(b, cloths, count);
@@ -354,44 +417,17 @@ b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t coun
         b->graph_sched = b->sched_version;
         b->graph_hulls = hulls_now;
         b->graph_kernels = kern;
-    } else if (use_graph) {
+    } else {
         // descriptors may have changed (colliders added): refresh the pinned copy the graph uploads
         for (uint32_t k = 0; k < count; ++k) b->h_descs[k] = cloths[k]->dev;
     }
-    if (use_graph) {
-        for (uint32_t k = 0; k < count; ++k) fill_step_scalars(cloths[k], dt, vel_iters, pos_iters, b->h_stage + k);
-        B3G_TRY(cudaEventRecord(b->ev0, st));
-        B3G_TRY(cudaGraphLaunch(b->exec, st));
-        B3G_TRY(cudaEventRecord(b->ev1, st));
-        B3G_TRY(cudaStreamSynchronize(st));
-        count_launches(b->graph_kernels);
-    }
-    float ms = 0.0f, cg_ms = 0.0f;
-    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-    if (cudaEventElapsedTime(&cg_ms, b->ev_cg0, b->ev_cg1) != cudaSuccess) {
-        cudaGetLastError();
-        cg_ms = 0.0f;
-    }
-    uint32_t it_total = 0, it_max = 0, status = 0;
-    for (uint32_t k = 0; k < count; ++k) {
-        const StepScalars& h = b->h_stage[k];
-        record_stats(cloths[k], h, ms, true);
-        if (per_cloth) per_cloth[k] = cloths[k]->last;
-        it_total += h.iter;
-        it_max = std::max(it_max, h.iter);
-        if (h.status) status = h.status;
-    }
-    if (stats) {
-        std::memset(stats, 0, sizeof(*stats));
-        stats->count = count;
-        stats->rows = b->total_rows;
-        stats->step_ms = ms;
-        stats->cg_ms = cg_ms;
-        stats->cg_iterations_total = it_total;
-        stats->cg_iterations_max = it_max;
-        stats->tasks = b->ntasks;
-    }
-    return status ? (b3g_status)status : B3G_OK;
+    for (uint32_t k = 0; k < count; ++k) fill_step_scalars(cloths[k], dt, vel_iters, pos_iters, b->h_stage + k);
+    B3G_TRY(cudaEventRecord(b->ev0, st));
+    B3G_TRY(cudaGraphLaunch(b->exec, st));
+    B3G_TRY(cudaEventRecord(b->ev1, st));
+    B3G_TRY(cudaStreamSynchronize(st));
+    count_launches(b->graph_kernels);
+    return collect(b, cloths, count, per_cloth, stats);
 }
 
 extern "C" {

@@ -429,7 +429,8 @@ b3g_status layout_cloth(b3g_cloth* c)
 // cloth gets its own stream and events and the call waits for the uploads;
 // otherwise it uses `st` and the host images stay alive until
 // finish_upload() after the caller has synchronised `st`.
-b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, cudaStream_t st, bool own_stream)
+b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, cudaStream_t st, bool own_stream,
+                         UploadStage* stage)
 {
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return from_cuda(e);
@@ -520,7 +521,20 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     }
     const HostImages& im = *c->images;
     auto up = [&](void* dst, const void* src, size_t b) {
-        if (e == cudaSuccess && b) e = cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess || !b) return;
+        if (stage && stage->used + b > stage->size && stage->used && b <= stage->size) {
+            // the staging buffer is full: wait for the copies queued from it
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return;
+            stage->used = 0;
+        }
+        if (stage && stage->used + b <= stage->size) {
+            char* p = stage->base + stage->used;
+            std::memcpy(p, src, b);
+            stage->used += (b + 255) & ~size_t(255);
+            e = cudaMemcpyAsync(dst, p, b, cudaMemcpyHostToDevice, st);
+        } else {
+            e = cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, st);
+        }
     };
     e = cudaMemsetAsync(A.base, 0, A.size, st);
     up(slice_off, T.slice_off.data(), T.slice_off.size() * 4);

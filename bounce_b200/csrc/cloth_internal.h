@@ -113,7 +113,17 @@ void fill_step_scalars(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_
 void record_stats(b3g_cloth* c, const b3g::StepScalars& h, float ms, bool solved);
 b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3g_cloth** out);
 b3g_status layout_cloth(b3g_cloth* c);
-b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, cudaStream_t st, bool own_stream);
+// Page-locked staging for a cloth's uploads: each upload is copied into the
+// staging buffer on the host and from there to the device asynchronously.
+// When the buffer is full the upload stream is waited for and the buffer
+// starts over; an upload larger than the buffer goes straight from its host
+// array.
+struct UploadStage {
+    char* base = nullptr;
+    size_t size = 0, used = 0;
+};
+b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, cudaStream_t st, bool own_stream,
+                         UploadStage* stage = nullptr);
 void finish_upload(b3g_cloth* c);
 b3g_status destroy_cloth(b3g_cloth* c);
 
@@ -131,3 +141,10 @@ void self_stats(const b3g_cloth* c, uint32_t* contacts, uint32_t* active, uint32
 }  // namespace b3g
 b3g_status batch_step_impl(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, float dt, uint32_t vel_iters,
                            uint32_t pos_iters, b3g_step_stats* per_cloth, b3g_batch_stats* stats, bool use_graph);
+// The same step without a graph in two halves: launch returns once the work
+// is queued on the batch's stream, finish waits for it and collects the
+// statistics.  The cloths must not change in between.
+b3g_status batch_step_launch(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, float dt, uint32_t vel_iters,
+                             uint32_t pos_iters);
+b3g_status batch_step_finish(b3g_batch* b, b3g_cloth* const* cloths, uint32_t count, b3g_step_stats* per_cloth,
+                             b3g_batch_stats* stats);

@@ -11,6 +11,9 @@
 // server, so a request's result does not depend on which others share its
 // ticks.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -77,6 +80,11 @@ struct b3g_server {
     bool stop = false;
 
     std::map<uint64_t, Request*> ready;      // prepared, awaiting admission (arrival order)
+    // Workers prepare ahead only while fewer than this many requests wait
+    // prepared: the free slots plus a margin, set by each tick.  Preparing
+    // further ahead than admission can follow only takes cores from the tick.
+    size_t prep_limit = 0;
+    UploadStage stage;                       // page-locked staging of the activations' uploads
     std::vector<Request*> active;
     std::unordered_map<uint64_t, Request*> all;
     uint64_t next_id = 1;
@@ -92,13 +100,19 @@ struct b3g_server {
 
 namespace {
 
+// Requests prepared beyond the free slots, so that the next ticks' admissions
+// do not wait for the topology workers.
+constexpr size_t kPrepMargin = 512;
+// Page-locked staging of the admitted cloths' uploads (reused every tick).
+constexpr size_t kStageBytes = 256ull << 20;
+
 void worker_main(b3g_server* s)
 {
     for (;;) {
         Request* r = nullptr;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            s->cv.wait(lk, [&] { return s->stop || !s->prep.empty(); });
+            s->cv.wait(lk, [&] { return s->stop || (!s->prep.empty() && s->ready.size() < s->prep_limit); });
             if (s->stop && s->prep.empty()) return;
             r = s->prep.front();
             s->prep.pop_front();
@@ -138,12 +152,19 @@ b3g_status activate(b3g_server* s, Request* r)
     b3g_cloth* c = r->cloth;
     cudaError_t e = cudaMallocFromPoolAsync((void**)&r->arena, r->bytes, s->pool, s->stream);
     if (e != cudaSuccess) return from_cuda(e);
-    b3g_status st = realize_cloth(c, s->device, r->arena, false, s->stream, false);
+    b3g_status st = realize_cloth(c, s->device, r->arena, false, s->stream, false, &s->stage);
     if (st != B3G_OK) return st;
     c->opts = s->cfg.solver;
     std::memcpy(c->gravity, r->gravity, sizeof(c->gravity));
     if (!r->types.empty()) {
-        e = cudaMemcpyAsync(c->d_stage_u8, r->types.data(), c->dev.n, cudaMemcpyHostToDevice, s->stream);
+        const void* src = r->types.data();
+        if (s->stage.used + c->dev.n <= s->stage.size) {
+            char* p = s->stage.base + s->stage.used;
+            std::memcpy(p, src, c->dev.n);
+            s->stage.used += ((size_t)c->dev.n + 255) & ~size_t(255);
+            src = p;
+        }
+        e = cudaMemcpyAsync(c->d_stage_u8, src, c->dev.n, cudaMemcpyHostToDevice, s->stream);
         if (e == cudaSuccess) e = launch_set_types(c->dev, c->d_stage_u8, s->stream);
         if (e != cudaSuccess) return from_cuda(e);
     }
@@ -224,6 +245,22 @@ b3g_status b3g_server_create(int device, const b3g_server_config* cfg, b3g_serve
         uint64_t keep = UINT64_MAX;  // keep freed blocks for reuse instead of returning them to the driver
         e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
+    if (e == cudaSuccess && cfg->hbm_budget_bytes) {
+        // reserve the budget in the pool up front: a block freed to the pool
+        // stays with it, and later arenas are carved from it instead of each
+        // growing the pool while requests wait
+        void* all = nullptr;
+        if (cudaMallocFromPoolAsync(&all, cfg->hbm_budget_bytes, s->pool, s->stream) == cudaSuccess) {
+            cudaFreeAsync(all, s->stream);
+            cudaStreamSynchronize(s->stream);
+        }
+        cudaGetLastError();  // a budget above the free memory leaves the pool to grow on demand
+    }
+    if (e == cudaSuccess) {
+        s->stage.size = kStageBytes;
+        e = cudaMallocHost(&s->stage.base, s->stage.size);
+        if (e != cudaSuccess) s->stage = UploadStage{};
+    }
     if (e != cudaSuccess) {
         b3g_server_destroy(s);
         return from_cuda(e);
@@ -239,7 +276,10 @@ b3g_status b3g_server_create(int device, const b3g_server_config* cfg, b3g_serve
         b3g_server_destroy(s);
         return st;
     }
-    const uint32_t nw = cfg->host_threads ? cfg->host_threads : std::max(1u, std::thread::hardware_concurrency());
+    // one core stays with the thread that ticks
+    const uint32_t hw = std::thread::hardware_concurrency();
+    const uint32_t nw = cfg->host_threads ? cfg->host_threads : std::max(1u, hw > 1 ? hw - 1 : 1u);
+    s->prep_limit = (size_t)cfg->max_active + kPrepMargin;
     for (uint32_t k = 0; k < nw; ++k) s->workers.emplace_back(worker_main, s);
     *out = s;
     return B3G_OK;
@@ -266,6 +306,7 @@ b3g_status b3g_server_destroy(b3g_server* s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->batch) b3g_batch_destroy(s->batch);
     if (s->pool) cudaMemPoolDestroy(s->pool);
+    if (s->stage.base) cudaFreeHost(s->stage.base);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return B3G_OK;
@@ -304,7 +345,35 @@ b3g_status b3g_server_tick(b3g_server* s, double now, b3g_server_tick_info* info
 {
     if (!s) return B3G_ERR_INVALID_ARGUMENT;
     cudaSetDevice(s->device);
+    // B3G_TRACE_SERVER=1: each tick's host phases to stderr
+    static const bool trace = std::getenv("B3G_TRACE_SERVER") != nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto ms_since = [](std::chrono::steady_clock::time_point a) {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+    };
+    double t_activate = 0.0, t_wait = 0.0, t_retire = 0.0;
     b3g_server_tick_info ti{};
+    // The active cloths' step goes to the device first; requests admitted
+    // meanwhile are brought onto the device while it runs and join from the
+    // next tick on.  A request's steps are the same whichever tick it joins.
+    std::vector<b3g_cloth*> cl(s->active.size());
+    uint64_t rows = 0;
+    for (size_t k = 0; k < cl.size(); ++k) {
+        cl[k] = s->active[k]->cloth;
+        rows += cl[k]->dev.n;
+    }
+    if (!cl.empty()) {
+        const b3g_status st = batch_step_launch(s->batch, cl.data(), (uint32_t)cl.size(), s->cfg.dt,
+                                                s->cfg.velocity_iterations, s->cfg.position_iterations);
+        if (st != B3G_OK) return st;
+    }
+    // the last tick's uploads are done (the launch above waited for the
+    // server stream); the staging buffer starts over
+    if (s->stage.used) {
+        cudaError_t e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) return from_cuda(e);
+        s->stage.used = 0;
+    }
     // admission in arrival order while memory and slots allow
     std::vector<Request*> newly;
     {
@@ -319,6 +388,8 @@ b3g_status b3g_server_tick(b3g_server* s, double now, b3g_server_tick_info* info
         }
         ti.queued = (uint32_t)(s->prep.size() + s->ready.size());
     }
+    const auto ta = std::chrono::steady_clock::now();
+    std::vector<Request*> joined;
     for (Request* r : newly) {
         b3g_status st = activate(s, r);
         if (st != B3G_OK) {
@@ -336,24 +407,17 @@ b3g_status b3g_server_tick(b3g_server* s, double now, b3g_server_tick_info* info
         }
         r->state = R_ACTIVE;
         r->admitted = now;
-        s->active.push_back(r);
+        joined.push_back(r);
         s->admitted += 1;
         ti.admitted += 1;
     }
+    t_activate = ms_since(ta);
     s->peak_used = std::max(s->peak_used, s->used);
-    s->peak_active = std::max<uint32_t>(s->peak_active, (uint32_t)s->active.size());
-    if (!s->active.empty()) {
-        std::vector<b3g_cloth*> cl(s->active.size());
-        uint64_t rows = 0;
-        for (size_t k = 0; k < cl.size(); ++k) {
-            cl[k] = s->active[k]->cloth;
-            rows += cl[k]->dev.n;
-        }
+    if (!cl.empty()) {
         b3g_batch_stats bs{};
-        b3g_status st = batch_step_impl(s->batch, cl.data(), (uint32_t)cl.size(), s->cfg.dt, s->cfg.velocity_iterations,
-                                        s->cfg.position_iterations, nullptr, &bs, false);
-        for (Request* r : newly)
-            if (r->cloth) finish_upload(r->cloth);
+        const auto tw = std::chrono::steady_clock::now();
+        const b3g_status st = batch_step_finish(s->batch, cl.data(), (uint32_t)cl.size(), nullptr, &bs);
+        t_wait = ms_since(tw);
         if (st != B3G_OK && st != B3G_ERR_NUMERICAL) return st;
         ti.stepped = (uint32_t)cl.size();
         ti.rows = (uint32_t)rows;
@@ -373,11 +437,32 @@ b3g_status b3g_server_tick(b3g_server* s, double now, b3g_server_tick_info* info
                 still.push_back(r);
             }
         }
-        retire(s, done, now);
+        const auto tr = std::chrono::steady_clock::now();
+        retire(s, done, now);  // waits for the server stream, so the new cloths' uploads are done too
+        t_retire = ms_since(tr);
         s->active.swap(still);
     }
+    if (!joined.empty()) {
+        cudaError_t e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) return from_cuda(e);
+        for (Request* r : joined) {
+            finish_upload(r->cloth);
+            s->active.push_back(r);
+        }
+    }
+    s->peak_active = std::max<uint32_t>(s->peak_active, (uint32_t)s->active.size());
+    if (trace)
+        std::fprintf(stderr, "tick %llu: stepped %zu admitted %zu | activate %.1f ms, wait %.1f ms (device %.1f), "
+                             "retire %.1f ms, total %.1f ms\n",
+                     (unsigned long long)s->ticks, cl.size(), joined.size(), t_activate, t_wait, ti.tick_ms, t_retire,
+                     ms_since(t0));
     ti.active = (uint32_t)s->active.size();
     ti.bytes_used = s->used;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->prep_limit = (s->cfg.max_active - std::min<size_t>(s->active.size(), s->cfg.max_active)) + kPrepMargin;
+    }
+    s->cv.notify_all();
     if (info) *info = ti;
     return B3G_OK;
 }

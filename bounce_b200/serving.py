@@ -14,7 +14,7 @@ from .meshes import ClothDef, grid_mesh
 def run_poisson(rate: float = 2000.0, seconds: float = 30.0, side_lo: int = 8, side_hi: int = 256,
                 steps_lo: int = 1, steps_hi: int = 60, sphere_fraction: float = 0.25,
                 budget_bytes: int = 150 * 10**9, max_active: int = 16384, seed: int = 7, device: int = 0,
-                drain_limit_s: float = 120.0, cluster: int = 8, split_classes=tuple(range(11, 20))) -> dict:
+                drain_limit_s: float = 120.0, cluster: int = 4, split_classes=tuple(range(9, 20))) -> dict:
     """Run the stream in real time; returns throughput and latency figures."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, size=int(rate * seconds * 1.5) + 16)
@@ -28,7 +28,9 @@ def run_poisson(rate: float = 2000.0, seconds: float = 30.0, side_lo: int = 8, s
     for s in np.unique(sides):  # one jittered grid per size, built before the clock starts
         meshes[int(s)] = grid_mesh(int(s), 1.0, 1e-3, seed + int(s))
     cdef = ClothDef(density=1.0, streching=1e4, shearing=1e3, damping=0.05, friction=0.3)
-    # split-instance for cloths of 2048 vertices and more, block-per-instance below
+    # split-instance over clusters of 4 CTAs for cloths of 512 vertices and
+    # more, block-per-instance below (the fastest of the schedules tried on
+    # this stream: clusters of 1, 4 and 8, splits from 2^9 or 2^11)
     srv = Server(budget_bytes=budget_bytes, max_active=max_active,
                  solver=SolverOptions.relative(1e-4, 200, DOT_F64), cluster=cluster, split_classes=split_classes,
                  device=device)
