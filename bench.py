@@ -145,7 +145,7 @@ def peaks():
 #   captured launch, the third step from rest, ran 10 iterations).
 # Sizes and forms without a capture report null.
 GRID_CG_TRAFFIC = {
-    (256, "persistent"): (36.53e6 + 0.04e6, None),
+    (256, "persistent"): (36536320 + 8448000, None),
     (1024, "persistent"): (4107670528 + 631533568, 10),
     (1024, "fused"): (3919580160 + 676790272, 10),
 }
