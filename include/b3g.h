@@ -406,12 +406,12 @@ b3g_status b3g_mpcg_solve(uint32_t n, const uint32_t* rowptr, const uint32_t* co
  *    loads the library holds it until the process exits.  Larger systems
  *    return B3G_ERR_CAPACITY.
  *  - The first call on each device looks the array's device address up
- *    (cudaGetSymbolAddress) and keeps it for the life of the process; make
- *    that first call before any stream capture.  A cudaDeviceReset after it
- *    is not supported (the library's module, and the array with it, may come
- *    back at another address).
- *  - Like b3g_mpcg_solve, it waits for its work to finish before it returns:
- *    the iteration count and residual are read back to the host.
+ *    (cudaGetSymbolAddress) and keeps it for the life of the process.  A
+ *    cudaDeviceReset after it is not supported (the library's module, and
+ *    the array with it, may come back at another address).
+ *  - Like b3g_mpcg_solve, it is synchronous: it waits for its work to
+ *    finish before it returns (the iteration count and residual are read
+ *    back to the host), so neither can be captured into a CUDA graph.
  *  - All calls share the one array: calls whose work overlaps on the GPU
  *    (other streams, other host threads) race and corrupt each other.  Each
  *    call clears the CG scalars it needs zeroed; other scratch contents are
