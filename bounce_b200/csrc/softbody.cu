@@ -274,7 +274,7 @@ constexpr uint32_t kMaxRowSlots = 128;  // slot ids are 7 bits wide
 
 __global__ void __launch_bounds__(32 * kAsmWarps, 8) k_sb_assemble(SoftDev d, float h)
 {
-    __shared__ float sX[kAsmWarps][32 * 4 * 9];   // element blocks of one chunk
+    __shared__ __align__(16) float sX[kAsmWarps][32 * 4 * 9];   // element blocks of one chunk
     __shared__ uint8_t sSlot[kAsmWarps][32 * 4];
     __shared__ float sF[kAsmWarps][32 * 6];       // f0 and f_plastic terms of one chunk
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
@@ -308,11 +308,24 @@ __global__ void __launch_bounds__(32 * kAsmWarps, 8) k_sb_assemble(SoftDev d, fl
                 const uint32_t li = meta & 3u;
                 const m3 R = ldm(d.R + 9 * (size_t)e);
                 const m3 RT = transpose(R);
-                const float* Ke = d.Ke + 144 * (size_t)e;
+                // Ke is symmetric and stored so: a block below the diagonal
+                // is the exact transpose of the one above it.  So the node's
+                // blocks Ke(li, j) are the transposes of Ke(j, li), j != li,
+                // which lie together, 144 bytes from 36 li on: nine 16-byte
+                // loads instead of four scattered 36-byte blocks.
+                // They are staged in the lane's own 36 floats of X and
+                // replaced there by the products, block by block.
+                const float4* K4 = reinterpret_cast<const float4*>(d.Ke + 144 * (size_t)e + 36 * li);
+                float4* X4 = reinterpret_cast<float4*>(X + 36 * lane);
+#pragma unroll 3
+                for (int q = 0; q < 9; ++q) X4[q] = K4[q];
 #pragma unroll
                 for (uint32_t j = 0; j < 4; ++j) {
                     SL[4 * lane + j] = (uint8_t)((meta >> (4 + 7 * j)) & 127u);
-                    stm(X + 9 * (4 * lane + j), mmul(mmul(R, ldm(Ke + 9 * (li + 4 * j))), RT));
+                    float* xb = X + 36 * lane + 9 * j;
+                    // Ke(li, j): Ke(j, li) itself on the diagonal, else its transpose
+                    if (j == li) stm(xb, mmul(mmul(R, ldm(xb)), RT));
+                    else stm(xb, mmul(mmul(R, transpose(ldm(xb))), RT));
                 }
                 if (g == 0) {
                     const f3 a = ldv(d.f0s + 12 * (size_t)e, li), b = ldv(d.fps + 12 * (size_t)e, li);
