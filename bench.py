@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--batch-count", type=int, default=512)
-    ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--serve-seconds", type=float, default=30.0)
     ap.add_argument("--skip-batch", action="store_true")
     ap.add_argument("--skip-serve", action="store_true")
@@ -402,8 +402,9 @@ def run_stiff(args, dev: int):
 
 def run_batched(args, dev: int, cpu_sample: bool = False):
     """Many cloths of uneven sizes per launch: 512 cloths, side U{16..128},
-    stretch log-U[1e3, 1e5], shear log-U[1e2, 1e4], row 0 pinned; against the
-    plain one-cloth-at-a-time GPU path on the same cloths."""
+    stretch log-U[1e3, 1e5], shear log-U[1e2, 1e4], row 0 pinned, 100 steps
+    (`--batch-steps`), each step one launch of the batch's CUDA graph; against
+    the plain one-cloth-at-a-time GPU path on the same cloths and steps."""
     import bounce_b200 as b3g
 
     # weak scaling over ranks: the job holds batch_count cloths per rank, and
