@@ -113,6 +113,8 @@ def main():
     ap.add_argument("--cap", type=int, default=2000)
     ap.add_argument("--workers", type=int, default=min(8, os.cpu_count() or 1))
     ap.add_argument("--json", default="")
+    ap.add_argument("--cg", choices=["persistent", "fused"], default="persistent",
+                    help="the persistent CG with two grid reductions per iteration, or one (fused)")
     args = ap.parse_args()
     checks = sorted({int(s) for s in args.check.split(",") if s})
 
@@ -129,13 +131,13 @@ def main():
     cloths = {}
     for dot in (0, 1, 2):
         c = b3g.Cloth(scene.mesh, scene.cdef).setup(scene, b3g.SolverOptions.relative(1e-4, args.cap, dot))
-        c.set_cg_strategy(True)
+        c.set_cg_strategy(True, fused=args.cg == "fused")
         cloths[dot] = c
     build_s = time.perf_counter() - t0
     n = cloths[2].n
 
     traj = {NAMES[d]: [] for d in cloths}
-    pending = []  # (variant, step, system path, gpu dv, true residual)
+    pending = []  # (variant, step, system path, gpu dv, true residual, the CG's own residual)
     same = {}     # step -> system path of the FP64-dot trajectory
     for step in range(1, args.steps + 1):
         for dot, c in cloths.items():
@@ -151,7 +153,7 @@ def main():
                 path = os.path.join(tmp, f"sys_{NAMES[dot]}_{step}.npz")
                 np.savez(path, **sysd)
                 dv = c.state()["dv"].astype(np.float64)
-                pending.append((NAMES[dot], step, path, dv, true_residual(sysd, dv)))
+                pending.append((NAMES[dot], step, path, dv, true_residual(sysd, dv), rec["cg_residual"]))
                 if dot == 2:
                     same[step] = (path, sysd)
         print(f"step {step}: " + ", ".join(f"{NAMES[d]} {traj[NAMES[d]][-1]['iterations']} it" for d in cloths),
@@ -166,7 +168,7 @@ def main():
             same_gpu[(step, NAMES[dot])] = (x.astype(np.float64), it, st, true_residual(sysd, x.astype(np.float64)))
 
     # FP64 CPU solves (and the reference's sequential FP32 dots) in parallel
-    paths = sorted({p for _, _, p, _, _ in pending})
+    paths = sorted({p for _, _, p, _, _, _ in pending})
     f64 = {p: (x, it, s) for p, x, it, s in pool.map(_solve_job, [(p, 1e-10) for p in paths])}
     seq = {p: (x, it, s) for p, x, it, s in
            pool.map(_seq_f32_job, [(same[s][0], 1e-4, args.cap) for s in sorted(same)])}
@@ -174,12 +176,13 @@ def main():
 
     h = dt
     checks_out = []
-    for name, step, path, dv, tres in pending:
+    for name, step, path, dv, tres, cres in pending:
         x64 = f64[path][0]
         err = np.abs(dv - x64)
         checks_out.append({"variant": name, "step": step, "dv_rel_err": float(np.linalg.norm(dv - x64) /
                                                                               max(np.linalg.norm(x64), 1e-300)),
                            "position_err_m": float(h * err.max()), "true_residual": tres,
+                           "cg_residual": cres, "cg_over_true": cres / tres if tres > 0 else None,
                            "f64_iterations": f64[path][1], "f64_solve_s": f64[path][2]})
     same_out = []
     for step, (path, sysd) in same.items():
@@ -206,7 +209,7 @@ def main():
                          "steps_at_cap": int((it >= args.cap).sum()),
                          "cg_residual_max": float(max(r["cg_residual"] for r in recs)),
                          "final_position_diff_vs_fp64_dots_m": drift.get(name, 0.0)}
-    result = {"workload": f"grid{args.side}_stiff", "vertices": n, "steps": args.steps, "checks": checks,
+    result = {"workload": f"grid{args.side}_stiff", "cg": args.cg, "vertices": n, "steps": args.steps, "checks": checks,
               "cap": args.cap, "build_s": build_s, "summary": summary, "trajectory_checks": checks_out,
               "same_system": same_out, "per_step": traj}
     print(json.dumps({k: result[k] for k in ("workload", "vertices", "summary")}, indent=1))
