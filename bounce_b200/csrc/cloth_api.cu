@@ -373,6 +373,7 @@ b3g_status layout_cloth(b3g_cloth* c)
     add(sizeof(GridBarrier));
     add(std::max((size_t)d.grid * 32, kGridCgPartialBytes));
     add(vec); add(n);                       // staging
+    add(T.E); add(n);                       // the assembly's first-touch order and its length
     c->arena.size = bytes + 256;
 
     HostImages* im = new (std::nothrow) HostImages();
@@ -490,6 +491,8 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     d.partials = A.take<char>(std::max((size_t)d.grid * 32, kGridCgPartialBytes));
     c->d_stage = A.take<float>(3 * (size_t)n);
     c->d_stage_u8 = A.take<uint8_t>(n);
+    d.asm_touch = A.take<uint8_t>(T.E);
+    d.asm_ntouch = A.take<uint8_t>(n);
     if (A.used > A.size) return B3G_ERR_CUDA;  // sizing bug guard
     d.slice_off = slice_off;
     d.row_deg = row_deg;
@@ -1638,11 +1641,14 @@ b3g_status b3g_cloth_step(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t p
     L.contacts = h->contacts;
     L.step_ms = ms;
     if (dt > 0.0f && !c->self && !c->dev.nbody && c->graph_ok && c->exec) {
-        // kernel nodes the graph ran: [contacts_update] assemble cg_init,
-        // 3 per CG iteration, finalize, [contact_position x (pos_iters - 1)], post
+        // kernel nodes the graph ran: [contacts_update, hull contacts update]
+        // assemble (two passes), cg_init, 3 per CG iteration (or the one
+        // persistent CG), finalize, [contact_position x (pos_iters - 1)], post
         const uint64_t ns = c->dev.nsph ? 1 : 0;
+        uint64_t hulls = 0;
+        for (uint32_t q = 0; q < c->dev.nsph; ++q) hulls |= c->dev.sph[q].kind == 2 ? 1u : 0u;
         const uint64_t cg = persistent_cg(c) ? 1 : 1 + 3ull * L.iterations;
-        count_launches(ns + 1 + cg + 1 + (ns && pos_iters > 1 ? pos_iters - 1 : 0) + 1);
+        count_launches(ns + hulls + 2 + cg + 1 + (ns && pos_iters > 1 ? pos_iters - 1 : 0) + 1);
     }
     if (stats) *stats = L;
     if (dt > 0.0f && h->status != 0) return (b3g_status)h->status;

@@ -116,6 +116,10 @@ struct ClothDev {
     float *fat_lo, *fat_hi;
 
     // contacts, [sphere][vertex]
+    // the assembly's first pass hands the second each row's dfdx first-touch
+    // order (slot ids at the row's SELL positions) and its length
+    uint8_t *asm_touch, *asm_ntouch;
+
     uint8_t* c_exists;
     uint8_t* c_active;
     uint32_t* c_key;            // creation key: step index * kMaxSpheres + sphere
@@ -180,10 +184,10 @@ cudaError_t launch_ray_cast(const ClothDev& c, const RayQuery& q, cudaStream_t s
 // The result kernel alone, for a key already in q.best (one triangle).
 cudaError_t launch_ray_result(const ClothDev& c, const RayQuery& q, cudaStream_t st);
 
-// Host launchers (cloth_kernels.cu).  The assembly kernel needs
+// Host launchers (cloth_kernels.cu).  The assembly's two kernels need
 // assemble_smem_bytes() of dynamic shared memory; a block size <= 0 asks for
 // assemble_block_for() of the rows' widest degree.
-size_t assemble_smem_bytes(const ClothDev& c, int block);
+size_t assemble_smem_bytes(uint32_t max_deg, int block);
 int assemble_block_for(uint32_t max_deg, bool multi);
 cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st);
 cudaError_t launch_assemble(const ClothDev& c, int block, cudaStream_t st);

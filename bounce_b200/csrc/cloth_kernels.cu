@@ -128,8 +128,20 @@ __device__ __forceinline__ float ord_dec(int i) { return __int_as_float(i >= 0 ?
 // assembly
 // ---------------------------------------------------------------------------
 
-// Per-thread accumulators for one row in shared memory, laid out
-// [(slot * 18 + component) * B + thread] so that lanes never conflict.
+// The assembly runs in two passes over each row's incidences, so that a row
+// needs one 3x3 accumulator per slot in shared memory instead of two (twice
+// the resident rows):
+//   kPassK  the forces and dfdx: the row's force goes to b and its dfdx
+//           blocks to A's storage, with the order of the slots' first touch;
+//   kPassD  dfdv, then A = (M - h dfdv) - h^2 dfdx and b from the stored
+//           parts.
+// Each sum still runs over the row's elements in the reference's order, so
+// A and b are the same floats as with both accumulators at once.
+constexpr int kPassK = 0, kPassD = 1;
+
+// Per-thread accumulators for one row in shared memory, one block per slot,
+// laid out [(slot * 9 + component) * B + thread] so that lanes never
+// conflict.
 struct RowAcc {
     float* base;
     uint8_t* touch;   // dfdx first-touch order, [k * B + thread]
@@ -140,79 +152,65 @@ struct RowAcc {
     __device__ void clear(int deg)
     {
         for (int k = 0; k < deg; ++k)
-            for (int q = 0; q < 18; ++q) base[(k * 18 + q) * B + tid] = 0.0f;
+            for (int q = 0; q < 9; ++q) base[(k * 9 + q) * B + tid] = 0.0f;
         touched = 0ull;
         ntouch = 0;
     }
+    __device__ void mark(int slot)
+    {
+        if (!(touched & (1ull << slot))) {
+            touched |= 1ull << slot;
+            touch[ntouch * B + tid] = (uint8_t)slot;
+            ++ntouch;
+        }
+    }
+    __device__ void add(int slot, const m3& m)
+    {
+        float* p = base + (slot * 9) * B + tid;
+        p[0 * B] += m.x.x; p[1 * B] += m.x.y; p[2 * B] += m.x.z;
+        p[3 * B] += m.y.x; p[4 * B] += m.y.y; p[5 * B] += m.y.z;
+        p[6 * B] += m.z.x; p[7 * B] += m.z.y; p[8 * B] += m.z.z;
+    }
+    // dfdx: the first touch of a slot is recorded
     __device__ void addK(int slot, const m3& m)
     {
-        if (!(touched & (1ull << slot))) {
-            touched |= 1ull << slot;
-            touch[ntouch * B + tid] = (uint8_t)slot;
-            ++ntouch;
-        }
-        float* p = base + (slot * 18) * B + tid;
-        p[0 * B] += m.x.x; p[1 * B] += m.x.y; p[2 * B] += m.x.z;
-        p[3 * B] += m.y.x; p[4 * B] += m.y.y; p[5 * B] += m.y.z;
-        p[6 * B] += m.z.x; p[7 * B] += m.z.y; p[8 * B] += m.z.z;
+        mark(slot);
+        add(slot, m);
     }
-    __device__ void addD(int slot, const m3& m)
+    __device__ m3 get(int slot) const
     {
-        float* p = base + (slot * 18 + 9) * B + tid;
-        p[0 * B] += m.x.x; p[1 * B] += m.x.y; p[2 * B] += m.x.z;
-        p[3 * B] += m.y.x; p[4 * B] += m.y.y; p[5 * B] += m.y.z;
-        p[6 * B] += m.z.x; p[7 * B] += m.z.y; p[8 * B] += m.z.z;
-    }
-    __device__ m3 getK(int slot) const
-    {
-        const float* p = base + (slot * 18) * B + tid;
+        const float* p = base + (slot * 9) * B + tid;
         return m3{f3{p[0], p[B], p[2 * B]}, f3{p[3 * B], p[4 * B], p[5 * B]}, f3{p[6 * B], p[7 * B], p[8 * B]}};
     }
-    // the slot's dfdx accumulator, marking its first touch
     __device__ m3 touchK(int slot)
     {
-        if (!(touched & (1ull << slot))) {
-            touched |= 1ull << slot;
-            touch[ntouch * B + tid] = (uint8_t)slot;
-            ++ntouch;
-        }
-        return getK(slot);
+        mark(slot);
+        return get(slot);
     }
-    __device__ void setK(int slot, const m3& m)
+    __device__ void set(int slot, const m3& m)
     {
-        float* p = base + (slot * 18) * B + tid;
+        float* p = base + (slot * 9) * B + tid;
         p[0 * B] = m.x.x; p[1 * B] = m.x.y; p[2 * B] = m.x.z;
         p[3 * B] = m.y.x; p[4 * B] = m.y.y; p[5 * B] = m.y.z;
         p[6 * B] = m.z.x; p[7 * B] = m.z.y; p[8 * B] = m.z.z;
     }
-    __device__ void setD(int slot, const m3& m)
+    // reuse of a slot's area once its block of A is stored: two vectors
+    __device__ void set6(int slot, const f3& a, const f3& b)
     {
-        float* p = base + (slot * 18 + 9) * B + tid;
-        p[0 * B] = m.x.x; p[1 * B] = m.x.y; p[2 * B] = m.x.z;
-        p[3 * B] = m.y.x; p[4 * B] = m.y.y; p[5 * B] = m.y.z;
-        p[6 * B] = m.z.x; p[7 * B] = m.z.y; p[8 * B] = m.z.z;
-    }
-    // reuse of a slot's dfdv area after A is stored: v and y of its column
-    __device__ void setD6(int slot, const f3& a, const f3& b)
-    {
-        float* p = base + (slot * 18 + 9) * B + tid;
+        float* p = base + (slot * 9) * B + tid;
         p[0] = a.x; p[B] = a.y; p[2 * B] = a.z;
         p[3 * B] = b.x; p[4 * B] = b.y; p[5 * B] = b.z;
     }
-    __device__ void getD6(int slot, f3& a, f3& b) const
+    __device__ void get6(int slot, f3& a, f3& b) const
     {
-        const float* p = base + (slot * 18 + 9) * B + tid;
+        const float* p = base + (slot * 9) * B + tid;
         a = f3{p[0], p[B], p[2 * B]};
         b = f3{p[3 * B], p[4 * B], p[5 * B]};
-    }
-    __device__ m3 getD(int slot) const
-    {
-        const float* p = base + (slot * 18 + 9) * B + tid;
-        return m3{f3{p[0], p[B], p[2 * B]}, f3{p[3 * B], p[4 * B], p[5 * B]}, f3{p[6 * B], p[7 * B], p[8 * B]}};
     }
 };
 
 // b3SpringForce::Apply (spring_force.cpp:53-120) restricted to one end.
+template <int PASS>
 __device__ void spring_row(const ClothDev& c, RowAcc& acc, uint32_t sid, int end, int slot_self, int slot_other,
                            f3& f_row)
 {
@@ -220,9 +218,17 @@ __device__ void spring_row(const ClothDev& c, RowAcc& acc, uint32_t sid, int end
     const float4 par = c.spr_par[sid];
     const float L0 = par.x, ks = par.y, kd = par.z;
     const uint32_t n = c.n;
-    const f3 x1 = ld3(c.x, n, pr.x), x2 = ld3(c.x, n, pr.y);
-    const f3 v1 = ld3(c.v, n, pr.x), v2 = ld3(c.v, n, pr.y);
     const m3 I = mident();
+    if (PASS == kPassD) {
+        if (kd > 0.0f) {
+            const m3 K11 = -kd * I;
+            const m3 K12 = -1.0f * K11;
+            acc.add(slot_self, K11);
+            acc.add(slot_other, K12);
+        }
+        return;
+    }
+    const f3 x1 = ld3(c.x, n, pr.x), x2 = ld3(c.x, n, pr.y);
     f3 mf = zero3();
     if (ks > 0.0f) {
         const f3 dx = x1 - x2;
@@ -242,12 +248,9 @@ __device__ void spring_row(const ClothDev& c, RowAcc& acc, uint32_t sid, int end
         }
     }
     if (kd > 0.0f) {
+        const f3 v1 = ld3(c.v, n, pr.x), v2 = ld3(c.v, n, pr.y);
         const f3 dv = v1 - v2;
         mf = mf + (-kd) * dv;
-        const m3 K11 = -kd * I;
-        const m3 K12 = -1.0f * K11;
-        acc.addD(slot_self, K11);
-        acc.addD(slot_other, K12);
     }
     f_row = end == 0 ? f_row + mf : f_row - mf;
 }
@@ -257,6 +260,7 @@ __device__ void spring_row(const ClothDev& c, RowAcc& acc, uint32_t sid, int end
 // C = |x1 - (w2 x2 + w3 x3 + w4 x4)|, dC/dx = (n, -w2 n, -w3 n, -w4 n), and
 // no second-derivative term.  The row's blocks are added for the force's
 // vertices in order.
+template <int PASS>
 __device__ void mouse_row(const ClothDev& c, RowAcc& acc, uint32_t m, int role, const int slot[4], f3& f_row)
 {
     const uint4 mv = c.mouse_v[m];
@@ -272,23 +276,26 @@ __device__ void mouse_row(const ClothDev& c, RowAcc& acc, uint32_t m, int role, 
         const f3 nrm = d / len;
         const f3 dC[4] = {nrm, (-w2) * nrm, (-w3) * nrm, (-w4) * nrm};
         const f3 dCr = role == 0 ? dC[0] : role == 1 ? dC[1] : role == 2 ? dC[2] : dC[3];
-        if (km > 0.0f) {
+        if (PASS == kPassK && km > 0.0f) {
             const float C = len;
             mf = mf + (-km * C) * dCr;
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc.addK(slot[j], -km * outer(dCr, dC[j]));
         }
         if (kd > 0.0f) {
-            const f3 vs[4] = {ld3(c.v, n, mv.x), ld3(c.v, n, mv.y), ld3(c.v, n, mv.z), ld3(c.v, n, mv.w)};
-            float dCdt = 0.0f;
+            if (PASS == kPassK) {
+                const f3 vs[4] = {ld3(c.v, n, mv.x), ld3(c.v, n, mv.y), ld3(c.v, n, mv.z), ld3(c.v, n, mv.w)};
+                float dCdt = 0.0f;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) dCdt += dot(dC[i], vs[i]);
-            mf = mf + (-kd * dCdt) * dCr;
+                for (int i = 0; i < 4; ++i) dCdt += dot(dC[i], vs[i]);
+                mf = mf + (-kd * dCdt) * dCr;
+            } else {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc.addD(slot[j], -kd * outer(dCr, dC[j]));
+                for (int j = 0; j < 4; ++j) acc.add(slot[j], -kd * outer(dCr, dC[j]));
+            }
         }
     }
-    f_row = f_row + mf;
+    if (PASS == kPassK) f_row = f_row + mf;
 }
 
 // Element `cn` of a 3-array held in registers (a select, not local memory).
@@ -307,6 +314,7 @@ __device__ __forceinline__ T corner(int cn, const T& a0, const T& a1, const T& a
 // (shear_force.cpp:142-207, strech_force.cpp:151-325); here every factor is
 // computed first, then each slot's accumulators are read once, the present
 // terms added in the same order, and written back once.
+template <int PASS>
 __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn, const int slot[3], f3& f_row)
 {
     const uint4 tv = c.tri[t];
@@ -315,7 +323,8 @@ __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn,
     const float du1 = rs.x, dv1 = rs.y, du2 = rs.z, dv2 = rs.w, inv_det = rs2.x, alpha = rs2.y;
     const uint32_t n = c.n;
     const f3 x1 = ld3(c.x, n, tv.x), x2 = ld3(c.x, n, tv.y), x3 = ld3(c.x, n, tv.z);
-    const f3 vs[3] = {ld3(c.v, n, tv.x), ld3(c.v, n, tv.y), ld3(c.v, n, tv.z)};
+    f3 vs[3] = {zero3(), zero3(), zero3()};
+    if (PASS == kPassK) vs[0] = ld3(c.v, n, tv.x), vs[1] = ld3(c.v, n, tv.y), vs[2] = ld3(c.v, n, tv.z);
     const f3 dx1 = x2 - x1, dx2 = x3 - x1;
     const f3 wu = inv_det * (dv2 * dx1 - dv1 * dx2);
     const f3 wv = inv_det * ((-du2) * dx1 + du1 * dx2);
@@ -331,7 +340,7 @@ __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn,
 #pragma unroll
     for (int i = 0; i < 3; ++i) dCs[i] = alpha * (dwudx[i] * wv + dwvdx[i] * wu);
     const f3 dCsc = corner(cn, dCs[0], dCs[1], dCs[2]);
-    if (sh) {
+    if (PASS == kPassK && sh) {
         f3 fe = zero3();
         if (shK) {
             const float C = alpha * dot(wu, wv);
@@ -375,40 +384,42 @@ __device__ void triangle_row(const ClothDev& c, RowAcc& acc, uint32_t t, int cn,
 #pragma unroll
             for (int j = 0; j < 3; ++j) kfac[d][j] = alpha * inv_len * dwc * dw[j];
             P[d] = I - outer(nw, nw);
-            if (K_on[d]) fe = fe + (-ks * Cst[d]) * dCstc[d];
-            if (D_on[d]) {
-                float dCdt = 0.0f;
+            if (PASS == kPassK) {
+                if (K_on[d]) fe = fe + (-ks * Cst[d]) * dCstc[d];
+                if (D_on[d]) {
+                    float dCdt = 0.0f;
 #pragma unroll
-                for (int i = 0; i < 3; ++i) dCdt += dot(dCst[d][i], vs[i]);
-                fe = fe + (-kd * dCdt) * dCstc[d];
+                    for (int i = 0; i < 3; ++i) dCdt += dot(dCst[d][i], vs[i]);
+                    fe = fe + (-kd * dCdt) * dCstc[d];
+                }
             }
         }
-        if (st) f_row = f_row + fe;
+        if (PASS == kPassK && st) f_row = f_row + fe;
     }
 
     // per slot, in the reference's order: shear, stretch u, stretch v
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        if (shK || K_on[0] || K_on[1]) {
+        if (PASS == kPassK && (shK || K_on[0] || K_on[1])) {
             m3 k = acc.touchK(slot[j]);
             if (shK) k = k + -ks_sh * outer(dCsc, dCs[j]);
 #pragma unroll
             for (int d = 0; d < 2; ++d)
                 if (K_on[d]) k = k + -ks * (outer(dCstc[d], dCst[d][j]) + Cst[d] * (kfac[d][j] * P[d]));
-            acc.setK(slot[j], k);
+            acc.set(slot[j], k);
         }
-        if (shD || D_on[0] || D_on[1]) {
-            m3 dm = acc.getD(slot[j]);
+        if (PASS == kPassD && (shD || D_on[0] || D_on[1])) {
+            m3 dm = acc.get(slot[j]);
             if (shD) dm = dm + -kd * outer(dCsc, dCs[j]);
 #pragma unroll
             for (int d = 0; d < 2; ++d)
                 if (D_on[d]) dm = dm + -kd * outer(dCstc[d], dCst[d][j]);
-            acc.setD(slot[j], dm);
+            acc.set(slot[j], dm);
         }
     }
 }
 
-template <bool MULTI>
+template <bool MULTI, int PASS>
 __global__ void __launch_bounds__(256) k_assemble(const __grid_constant__ ClothDev one,
                                                   const __grid_constant__ RowSpan span)
 {
@@ -426,17 +437,19 @@ __global__ void __launch_bounds__(256) k_assemble(const __grid_constant__ ClothD
 
     RowAcc acc;
     acc.base = smem;
-    acc.touch = reinterpret_cast<uint8_t*>(smem + (size_t)max_deg * 18 * B);
+    acc.touch = reinterpret_cast<uint8_t*>(smem + (size_t)max_deg * 9 * B);
     acc.B = B;
     acc.tid = tid;
     const int deg = c.row_deg[row];
     acc.clear(deg);
 
     // sf = f_ext (+ m g for dynamic particles), cloth_force_solver.cpp:172-180
-    f3 f = ld3(c.fext, n, row);
     const float m = c.mass[row];
-    const bool dyn = is_dynamic(c, row);
-    if (dyn) f = f + m * mk(sc->gx, sc->gy, sc->gz);
+    f3 f = zero3();
+    if (PASS == kPassK) {
+        f = ld3(c.fext, n, row);
+        if (is_dynamic(c, row)) f = f + m * mk(sc->gx, sc->gy, sc->gz);
+    }
 
     // the next incidence entry is loaded while the current element is computed
     const uint32_t e_end = c.inc_ptr[row + 1];
@@ -455,32 +468,31 @@ __global__ void __launch_bounds__(256) k_assemble(const __grid_constant__ ClothD
             // mouse force: role in bits 0-1, the four slots 7 bits each from bit 4
             const int ms[4] = {(int)((meta >> 4) & 0x7fu), (int)((meta >> 11) & 0x7fu), (int)((meta >> 18) & 0x7fu),
                                (int)((meta >> 25) & 0x7fu)};
-            mouse_row(c, acc, el & 0x3fffffffu, cn, ms, f);
+            mouse_row<PASS>(c, acc, el & 0x3fffffffu, cn, ms, f);
         } else if (el & 0x80000000u) {
             // springs: slot of p1 in s0, of p2 in s1; cn = end
-            spring_row(c, acc, el & 0x7fffffffu, cn, cn == 0 ? s0 : s1, cn == 0 ? s1 : s0, f);
+            spring_row<PASS>(c, acc, el & 0x7fffffffu, cn, cn == 0 ? s0 : s1, cn == 0 ? s1 : s0, f);
         } else {
             const int slots[3] = {s0, s1, s2};
-            triangle_row(c, acc, el, cn, slots, f);
+            triangle_row<PASS>(c, acc, el, cn, slots, f);
         }
     }
 
-    // A = (M - h dfdv) - h^2 dfdx, one row (cloth_force_solver.cpp:198)
     const uint32_t base = row_base(c, row);
-    m3 diag = mzero();
-    for (int k = 0; k < deg; ++k) {
-        const m3 M = k == 0 ? m3{f3{m, 0.0f, 0.0f}, f3{0.0f, m, 0.0f}, f3{0.0f, 0.0f, m}} : mzero();
-        const m3 a = (M - h * acc.getD(k)) - hh * acc.getK(k);
-        if (k == 0) diag = a;
-        store_block(c, base + 32u * k, a);
+    if (PASS == kPassK) {
+        // dfdx into A's storage, the first-touch order beside it, the force into b
+        for (int k = 0; k < deg; ++k) store_block(c, base + 32u * k, acc.get(k));
+        for (int q = 0; q < acc.ntouch; ++q) c.asm_touch[base + 32u * q] = acc.touch[q * B + tid];
+        c.asm_ntouch[row] = (uint8_t)acc.ntouch;
+        st3(c.b, n, row, f);
+        return;
     }
-    // Jacobi preconditioner (cloth_force_solver.cpp:70-88)
-    st3(c.pinv, n, row, mk(1.0f / diag.x.x, 1.0f / diag.y.y, 1.0f / diag.z.z));
 
-    // b = h (f + h dfdx v + dfdx y), dfdx summed in its row-list order
-    // (reverse first touch, sparse_mat33.h:264-282).  The v and y of every
-    // slot's column are gathered first, with independent loads, into the
-    // slot's dfdv accumulator (no longer needed once A is stored).
+    // A = (M - h dfdv) - h^2 dfdx, one row (cloth_force_solver.cpp:198).
+    // Each slot's dfdx block is read back, and its products with the v and y
+    // of the slot's column (for b) go to the slot's accumulator once its
+    // block of A is stored.  The column loads are issued 8 slots at a time.
+    m3 diag = mzero();
     for (int k0 = 0; k0 < deg; k0 += 8) {
         uint32_t cl[8];
 #pragma unroll
@@ -488,21 +500,31 @@ __global__ void __launch_bounds__(256) k_assemble(const __grid_constant__ ClothD
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             if (k0 + k < deg) {
+                const int s = k0 + k;
+                const m3 K = load_block(c, base + 32u * s);
+                const m3 M = s == 0 ? m3{f3{m, 0.0f, 0.0f}, f3{0.0f, m, 0.0f}, f3{0.0f, 0.0f, m}} : mzero();
+                const m3 a = (M - h * acc.get(s)) - hh * K;
+                if (s == 0) diag = a;
+                store_block(c, base + 32u * s, a);
                 const f3 vj = ld3(c.v, n, cl[k]), yj = ld3(c.y, n, cl[k]);
-                acc.setD6(k0 + k, vj, yj);
+                acc.set6(s, K * vj, K * yj);
             }
         }
     }
+    // Jacobi preconditioner (cloth_force_solver.cpp:70-88)
+    st3(c.pinv, n, row, mk(1.0f / diag.x.x, 1.0f / diag.y.y, 1.0f / diag.z.z));
+
+    // b = h (f + h dfdx v + dfdx y), dfdx summed in its row-list order
+    // (reverse first touch, sparse_mat33.h:264-282)
     f3 t1 = zero3(), t2 = zero3();
-    for (int q = acc.ntouch - 1; q >= 0; --q) {
-        const int k = acc.touch[q * B + tid];
-        const m3 K = acc.getK(k);
-        f3 vj, yj;
-        acc.getD6(k, vj, yj);
-        t1 = t1 + K * vj;
-        t2 = t2 + K * yj;
+    for (int q = (int)c.asm_ntouch[row] - 1; q >= 0; --q) {
+        const int k = c.asm_touch[base + 32u * q];
+        f3 kv, ky;
+        acc.get6(k, kv, ky);
+        t1 = t1 + kv;
+        t2 = t2 + ky;
     }
-    st3(c.b, n, row, h * ((f + h * t1) + t2));
+    st3(c.b, n, row, h * ((ld3(c.b, n, row) + h * t1) + t2));
 }
 
 // ---------------------------------------------------------------------------
@@ -1274,9 +1296,9 @@ inline uint32_t blocks_for(uint32_t n, uint32_t b) { return (n + b - 1) / b; }
 // launchers
 // ---------------------------------------------------------------------------
 
-size_t assemble_smem_bytes(const ClothDev& c, int block)
+size_t assemble_smem_bytes(uint32_t max_deg, int block)
 {
-    return (size_t)c.max_deg * 18 * sizeof(float) * block + (size_t)c.max_deg * block;
+    return (size_t)max_deg * 9 * sizeof(float) * block + (size_t)max_deg * block;
 }
 
 // Every launch raises the kernel's dynamic shared memory limit to the same
@@ -1284,7 +1306,7 @@ size_t assemble_smem_bytes(const ClothDev& c, int block)
 // under one another.
 constexpr size_t kAssembleSmemLimit = 227 * 1024;
 
-// The assembly keeps a row's accumulators in shared memory (73 bytes per
+// The assembly keeps a row's accumulators in shared memory (37 bytes per
 // slot), so shared memory bounds how many rows an SM holds.  Of the block
 // sizes 32..256 take the one with the most resident rows per SM (the
 // smaller on ties, for a finer tail), from the occupancy calculator.
@@ -1294,10 +1316,10 @@ int assemble_block_for(uint32_t max_deg, bool multi)
     if (max_deg > 255) max_deg = 255;
     std::atomic<int>& slot = cache[multi ? 1 : 0][max_deg];
     if (const int known = slot.load(std::memory_order_relaxed)) return known;
-    const void* fn = multi ? (const void*)k_assemble<true> : (const void*)k_assemble<false>;
+    const void* fn = multi ? (const void*)k_assemble<true, kPassK> : (const void*)k_assemble<false, kPassK>;
     int best = 32, best_rows = 0;
     for (int b = 32; b <= 256; b += 32) {
-        const size_t smem = (size_t)max_deg * 73 * b;
+        const size_t smem = assemble_smem_bytes(max_deg, b);
         if (smem > kAssembleSmemLimit) break;
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAssembleSmemLimit) !=
             cudaSuccess) {
@@ -1351,16 +1373,20 @@ cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// The assembly's two passes (forces and dfdx, then dfdv, A and b).
 cudaError_t launch_assemble(const ClothDev& c, int block, cudaStream_t st)
 {
     if (block <= 0) block = assemble_block_for(c.max_deg, false);
-    const size_t smem = assemble_smem_bytes(c, block);
+    const size_t smem = assemble_smem_bytes(c.max_deg, block);
     if (smem > kAssembleSmemLimit) return cudaErrorInvalidValue;
-    cudaError_t e =
-        cudaFuncSetAttribute(k_assemble<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAssembleSmemLimit);
-    if (e != cudaSuccess) return e;
-    k_assemble<false><<<blocks_for(c.n, block), block, smem, st>>>(c, kNoSpan);
-    count_launches(1);
+    for (const void* fn : {(const void*)k_assemble<false, kPassK>, (const void*)k_assemble<false, kPassD>}) {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)kAssembleSmemLimit);
+        if (e != cudaSuccess) return e;
+    }
+    k_assemble<false, kPassK><<<blocks_for(c.n, block), block, smem, st>>>(c, kNoSpan);
+    k_assemble<false, kPassD><<<blocks_for(c.n, block), block, smem, st>>>(c, kNoSpan);
+    count_launches(2);
     return cudaGetLastError();
 }
 
@@ -1451,13 +1477,16 @@ cudaError_t launch_span_assemble(const RowSpan& sp, int block, cudaStream_t st)
 {
     if (!sp.total) return cudaSuccess;
     if (block <= 0) block = assemble_block_for(sp.max_deg, true);
-    const size_t smem = (size_t)sp.max_deg * 18 * sizeof(float) * block + (size_t)sp.max_deg * block;
+    const size_t smem = assemble_smem_bytes(sp.max_deg, block);
     if (smem > kAssembleSmemLimit) return cudaErrorInvalidValue;
-    cudaError_t e =
-        cudaFuncSetAttribute(k_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAssembleSmemLimit);
-    if (e != cudaSuccess) return e;
-    k_assemble<true><<<blocks_for(sp.total, block), block, smem, st>>>(g_unused_one, sp);
-    count_launches(1);
+    for (const void* fn : {(const void*)k_assemble<true, kPassK>, (const void*)k_assemble<true, kPassD>}) {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)kAssembleSmemLimit);
+        if (e != cudaSuccess) return e;
+    }
+    k_assemble<true, kPassK><<<blocks_for(sp.total, block), block, smem, st>>>(g_unused_one, sp);
+    k_assemble<true, kPassD><<<blocks_for(sp.total, block), block, smem, st>>>(g_unused_one, sp);
+    count_launches(2);
     return cudaGetLastError();
 }
 
