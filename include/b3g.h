@@ -492,7 +492,7 @@ typedef struct {
     float gravity[3];
     b3g_solver_opts solver;          /* max_iterations 0: relative 1e-4, at most 200, FP64 dots */
     b3g_batch_schedule schedule;     /* cluster 0: block-per-instance */
-    uint32_t host_threads;           /* topology worker threads, 0: one per core */
+    uint32_t host_threads;           /* topology worker threads, 0: one per core but one */
 } b3g_server_config;
 
 typedef struct {
@@ -525,7 +525,9 @@ b3g_status b3g_server_destroy(b3g_server* server);
 b3g_status b3g_server_submit(b3g_server* server, const b3g_mesh_desc* mesh, const b3g_cloth_def* def,
                              const uint8_t* types, const float* spheres, uint32_t sphere_count, uint32_t steps,
                              double arrival, uint64_t* request_id);
-/* Admit what fits, step every active cloth once, retire finished requests. */
+/* Step every active cloth once; while the device runs the step, admit what
+ * fits the budget and the slots (admitted requests step from the next tick
+ * on); then retire finished requests. */
 b3g_status b3g_server_tick(b3g_server* server, double now, b3g_server_tick_info* info);
 b3g_status b3g_server_poll(b3g_server* server, uint64_t request_id, b3g_request_info* info);
 /* Final positions (3 floats per vertex) of a finished request. */
