@@ -76,8 +76,11 @@ def test_trajectory_drift_plain(b3g, port):
     chaotic once the cloth folds (about step 55): the oracle against itself
     with FP64 instead of FP32 CG dots -- the same algorithm, another rounding --
     drifts apart by centimetres there.  The GPU trajectory must stay within
-    1e-4 m of the oracle before that, and its bulk motion (centroid, kinetic
-    energy) must agree after it."""
+    1e-4 m of the oracle before that; after it the GPU's largest drift must
+    stay within ten times the oracle's own (measured on a B200: 0.026 m
+    against 0.005 m at step 100; chaotic separation grows by such factors
+    from any change of rounding), and its bulk motion (centroid, kinetic
+    energy) must agree."""
     scene = b3g.plain_scene(32)
     gpu, ora = _pair(b3g, port, scene)
     floor = port.PortCloth(scene.mesh, scene.cdef).setup(scene)
@@ -94,6 +97,7 @@ def test_trajectory_drift_plain(b3g, port):
           "| oracle f32 vs f64 dots:", noise[0], noise[9], noise[49], noise[99])
     assert drift[0] <= 1e-6
     assert max(drift[:50]) <= 1e-4
+    assert max(drift[50:]) <= 10.0 * max(noise[50:]) + 1e-3, (max(drift[50:]), max(noise[50:]))
     g, o = gpu.state(), ora.state()
     assert abs(g["x"][:, 1].mean() - o["x"][:, 1].mean()) <= 0.02 * abs(o["x"][:, 1].mean())
     assert abs(gpu.energy() - ora.energy()) <= 0.1 * ora.energy()
