@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--cg", choices=["fused", "persistent"], default="persistent",
                     help="the headline cloth's CG: one persistent launch with one grid reduction per "
                          "iteration (fused) or two")
+    ap.add_argument("--assembly", choices=["records", "rows"], default="records",
+                    help="how every cloth's system is assembled: each element evaluated once into a record "
+                         "(records) or recomputed by each of its rows in two passes (rows); same floats")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--batch-count", type=int, default=512)
@@ -242,6 +245,7 @@ def run_ours(args, rank, world):
     cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene, opts)
     # the whole solve in one persistent cooperative launch
     cloth.set_cg_strategy(True, fused=args.cg == "fused")
+    cloth.set_assembly(args.assembly)
     info = cloth.info()
     n = info["vertices"]
     # L2 flush buffer (> 126 MB L2), written between timed steps
@@ -327,6 +331,12 @@ def run_ours(args, rank, world):
     alg = algorithmic_bytes(info, dom if dom != "grid_cg" else f"grid_cg:{it_total / len(prof)}")
     peak, peak_kind = peaks()
     achieved = alg / (avg_ms / 1000.0) / 1e9
+    # the assembly (both of its launches) against the same roofline
+    asm_ms = kern["assemble"][0] / kern["assemble"][1]
+    asm_alg = algorithmic_bytes(info, "assemble")
+    assembly = {"form": cloth.assembly(), "ms": asm_ms, "algorithmic_bytes": asm_alg,
+                "achieved": asm_alg / (asm_ms / 1000.0) / 1e9,
+                "frac": asm_alg / (asm_ms / 1000.0) / 1e9 / peak, "unit": "GB/s"}
     cloth.close()
     return {
         "value": value, "ms_per_step": 1000.0 * dev_s / args.steps, "wall_s": wall, "e2e": e2e, "fp64": fp64,
@@ -340,6 +350,7 @@ def run_ours(args, rank, world):
                      "algorithmic_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
                      "share": kern[dom][0] / total if total else None},
         "kernel_ms": {k: v[0] / v[1] for k, v in kern.items()},
+        "assembly": assembly,
     }
 
 
@@ -364,6 +375,7 @@ def run_stiff(args, dev: int):
     for form in ("persistent", "fused"):
         cloth = b3g.Cloth(scene.mesh, scene.cdef, device=dev).setup(scene, opts)
         cloth.set_cg_strategy(True, fused=form == "fused")
+        cloth.set_assembly(args.assembly)
         info = cloth.info()
         warm = 3
         warm_its = [int(cloth.step(scene.dt)["iterations"]) for _ in range(warm)]
@@ -415,6 +427,8 @@ def run_batched(args, dev: int, cpu_sample: bool = False):
     scenes = [every[k] for k in shards[env.rank]]
     opts = b3g.SolverOptions.relative(1e-4, 200, b3g.DOT_F64)
     cloths = [b3g.Cloth(sc.mesh, sc.cdef, device=dev).setup(sc, opts) for sc in scenes]
+    for c in cloths:
+        c.set_assembly(args.assembly)
     rows = sum(c.n for c in cloths)
     dt = scenes[0].dt
     batch = b3g.Batch(max(1024, len(cloths)), device=dev)
@@ -449,6 +463,7 @@ def run_batched(args, dev: int, cpu_sample: bool = False):
             plain = [b3g.Cloth(sc.mesh, sc.cdef, device=dev).setup(sc, opts) for sc in scenes]
             t = np.zeros(len(plain))
             for k, c in enumerate(plain):
+                c.set_assembly(args.assembly)
                 if strategy != "launches":
                     c.set_cg_strategy(True, fused=strategy == "fused")
                 for _ in range(args.warmup):
@@ -831,6 +846,7 @@ def summary(line: dict) -> dict:
     return {
         "headline_vertex_steps_per_s": g(line, "value"), "headline_e2e": g(line, "e2e", "value"),
         "headline_frac": g(line, "roofline", "frac"), "headline_fp64_rel_dv_error": g(line, "fp64", "rel_dv_error"),
+        "assembly_ms": g(line, "assembly", "ms"), "assembly_frac": g(line, "assembly", "frac"),
         "batched_vertex_steps_per_s": g(b, "vertex_steps_per_s"), "batched_speedup_vs_plain": g(b, "speedup_vs_plain"),
         "batched_frac": g(b, "roofline", "frac"),
         "serving_vertex_steps_per_s": g(s, "vertex_steps_per_s"), "serving_tick_p50_ms": g(s, "p50_step_ms"),
@@ -939,6 +955,7 @@ def main():
         "gpu_launches": r["launches"],
         "roofline": r["roofline"],
         "kernel_ms": r["kernel_ms"],
+        "assembly": r["assembly"],
         "cpu_baseline": base,
         "fp64": r["fp64"],
         "batched": batched,

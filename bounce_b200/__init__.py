@@ -230,6 +230,8 @@ def lib() -> C.CDLL:
             "b3g_cloth_step_profiled": [vp, f32, u32, u32, C.POINTER(PhaseTimesC), C.POINTER(StepStatsC)],
             "b3g_cloth_get_info": [vp, C.POINTER(ClothInfoC)],
             "b3g_cloth_set_cg_strategy": [vp, i32],
+            "b3g_cloth_set_assembly": [vp, i32],
+            "b3g_cloth_get_assembly": [vp],
             "b3g_debug_cg_barrier_timeout": [vp, u32, C.POINTER(i32)],
             "b3g_mpcg_solve": [u32, vp, vp, vp, vp, vp, vp, C.POINTER(SolverOptsC), vp, C.POINTER(u32),
                                C.POINTER(StepStatsC), vp],
@@ -585,6 +587,19 @@ class Cloth:
         cooperative launch (fused: one grid reduction per iteration)."""
         code = 0 if not persistent else 2 if fused else 1
         check(lib().b3g_cloth_set_cg_strategy(self.h, code), "set_cg_strategy")
+
+    def set_assembly(self, form: str) -> None:
+        """'records': every element evaluated once a step, each block summed
+        from its own term list (the default where the layout allows it);
+        'rows': each row recomputes its incident elements in two passes.
+        Both give the same floats."""
+        code = {"records": 0, "rows": 1}[form]
+        check(lib().b3g_cloth_set_assembly(self.h, code), "set_assembly")
+
+    def assembly(self) -> str:
+        """The assembly form in use ('rows' where the layout does not allow
+        the records)."""
+        return "records" if lib().b3g_cloth_get_assembly(self.h) == 0 else "rows"
 
     def info(self) -> dict:
         i = ClothInfoC()

@@ -374,6 +374,12 @@ b3g_status layout_cloth(b3g_cloth* c)
     add(std::max((size_t)d.grid * 32, kGridCgPartialBytes));
     add(vec); add(n);                       // staging
     add(T.E); add(n);                       // the assembly's first-touch order and its length
+    if (T.slot_terms) {                     // slot-major assembly: term lists and element records
+        add((size_t)T.E / 32 * 4 + 4); add((size_t)T.E * 4); add(T.terms.size() * 4 + 4);
+        add((size_t)t * 240); add((size_t)ns * 48 + 48); add((size_t)nmouse * 80 + 80);
+        add((size_t)T.E * 24);
+    }
+    d.slot_asm = T.slot_terms && !c->row_assembly ? 1u : 0u;
     c->arena.size = bytes + 256;
 
     HostImages* im = new (std::nothrow) HostImages();
@@ -493,6 +499,22 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     c->d_stage_u8 = A.take<uint8_t>(n);
     d.asm_touch = A.take<uint8_t>(T.E);
     d.asm_ntouch = A.take<uint8_t>(n);
+    uint32_t *term_qk = nullptr, *term_slot = nullptr, *terms = nullptr;
+    d.term_qk = d.term_slot = d.terms = nullptr;
+    d.tri_rec = d.spr_rec = d.mouse_rec = nullptr;
+    d.asm_kv = nullptr;
+    if (T.slot_terms) {
+        term_qk = A.take<uint32_t>(T.E / 32 + 1);
+        term_slot = A.take<uint32_t>(T.E);
+        terms = A.take<uint32_t>(T.terms.size() + 1);
+        d.tri_rec = A.take<float4>((size_t)t * 15);
+        d.spr_rec = A.take<float4>((size_t)ns * 3 + 3);
+        d.mouse_rec = A.take<float4>((size_t)d.nmouse * 5 + 5);
+        d.asm_kv = A.take<float>((size_t)T.E * 6);
+        d.term_qk = term_qk;
+        d.term_slot = term_slot;
+        d.terms = terms;
+    }
     if (A.used > A.size) return B3G_ERR_CUDA;  // sizing bug guard
     d.slice_off = slice_off;
     d.row_deg = row_deg;
@@ -546,6 +568,11 @@ b3g_status realize_cloth(b3g_cloth* c, int device, char* base, bool owns_arena, 
     up(inc_ptr, T.inc_ptr.data(), (n + 1) * 4);
     up(inc_elem, T.inc_elem.data(), T.inc_elem.size() * 4);
     up(inc_meta, T.inc_meta.data(), T.inc_meta.size() * 4);
+    if (T.slot_terms) {
+        up(term_qk, T.term_qk.data(), T.term_qk.size() * 4);
+        up(term_slot, T.term_slot.data(), (size_t)T.E * 4);
+        up(terms, T.terms.data(), T.terms.size() * 4);
+    }
     up(tri, im.tri.data(), (size_t)t * 16);
     up(tri_rest, im.rest.data(), (size_t)t * 16);
     up(tri_rest2, im.rest2.data(), (size_t)t * 8);
@@ -1792,6 +1819,23 @@ b3g_status b3g_cloth_set_cg_strategy(b3g_cloth* c, b3g_cg_strategy s)
     if (!c->owns_stream) return B3G_OK;  // batch and server cloths run their own CG
     cudaSetDevice(c->device);
     return ensure_cg_rec(c);
+}
+
+b3g_status b3g_cloth_set_assembly(b3g_cloth* c, b3g_assembly form)
+{
+    if (!valid(c) || (form != B3G_ASSEMBLY_ELEMENT_RECORDS && form != B3G_ASSEMBLY_ROWS))
+        return B3G_ERR_INVALID_ARGUMENT;
+    c->row_assembly = form == B3G_ASSEMBLY_ROWS;
+    c->dev.slot_asm = c->topo.slot_terms && !c->row_assembly ? 1u : 0u;
+    cudaSetDevice(c->device);
+    destroy_graph(c);
+    c->layout_version += 1;  // batches holding the cloth capture their step again
+    return B3G_OK;
+}
+
+b3g_assembly b3g_cloth_get_assembly(const b3g_cloth* c)
+{
+    return valid(c) && c->dev.slot_asm ? B3G_ASSEMBLY_ELEMENT_RECORDS : B3G_ASSEMBLY_ROWS;
 }
 
 b3g_status b3g_cloth_get_info(const b3g_cloth* c, b3g_cloth_info* info)

@@ -14,9 +14,11 @@
 //  * per-vertex incidence lists (CSR) of the elements touching the vertex, in
 //    the order Bounce applies its forces (force list = reverse creation order,
 //    src/bounce/cloth/cloth.cpp:353-358), each with the SELL slots of the
-//    element's vertices inside the vertex's row.  Assembly is row-centric:
-//    one thread owns one row, recomputes each incident element and
-//    accumulates only its own row -- no atomics, no colouring, deterministic.
+//    element's vertices inside the vertex's row.  Assembly is row-owned:
+//    one thread owns one row and accumulates only its own row -- no atomics,
+//    no colouring, deterministic.  By default every element is evaluated
+//    once a step into a record and each block of the row is summed from its
+//    own term list; the other form recomputes each incident element per row.
 #pragma once
 
 #include <cstdint>
@@ -115,11 +117,21 @@ struct ClothDev {
     float *z, *p2;              // S P^-1 r and the second direction buffer (persistent CG)
     float *fat_lo, *fat_hi;
 
-    // contacts, [sphere][vertex]
     // the assembly's first pass hands the second each row's dfdx first-touch
     // order (slot ids at the row's SELL positions) and its length
     uint8_t *asm_touch, *asm_ntouch;
+    // slot-major assembly (slot_asm != 0, the default where the layout
+    // allows it): per-element records written once a step by
+    // k_elem_records (planes of float4: 15 a triangle, 3 a spring, 5 a
+    // mouse force), the per-block term lists (topology.h) read by
+    // k_assemble_blocks, and each block's dfdx products with its column's v
+    // and y (6 planes of E floats) that k_assemble_rhs sums into b
+    uint32_t slot_asm;
+    const uint32_t *term_qk, *term_slot, *terms;
+    float4 *tri_rec, *spr_rec, *mouse_rec;
+    float* asm_kv;
 
+    // contacts, [sphere][vertex]
     uint8_t* c_exists;
     uint8_t* c_active;
     uint32_t* c_key;            // creation key: step index * kMaxSpheres + sphere
@@ -159,6 +171,9 @@ struct RowSpan {
     const uint32_t* prefix;     // device array of count + 1 row offsets
     uint32_t count, total, max_deg;
     uint32_t hulls;             // nonzero when some cloth has a hull collider
+    uint32_t slot_asm;          // nonzero when every cloth has the slot-major assembly
+    const uint32_t* eprefix;    // device array of count + 1 element offsets (triangles, springs, mouse forces)
+    uint32_t etotal;
 };
 
 cudaError_t launch_span_contacts_update(const RowSpan& sp, cudaStream_t st);

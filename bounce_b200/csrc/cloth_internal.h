@@ -60,6 +60,7 @@ struct b3g_cloth {
     b3g_solver_opts opts{B3G_STOP_REFERENCE, 0.0f, 20u, B3G_DOT_F32};
     uint32_t step_index = 0;
     int assemble_block = 0;  // threads per assembly block; 0: chosen at launch for occupancy
+    bool row_assembly = false;  // the row-centric assembly even where the slot-major one applies
 
     // pinned staging
     b3g::StepScalars* h_sc = nullptr;

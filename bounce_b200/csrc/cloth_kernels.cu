@@ -28,6 +28,7 @@
 #include "bodies.cuh"
 #include "self_collision.cuh"
 #include "sell_spmv.cuh"
+#include "topology.h"
 #include "vec.cuh"
 
 namespace b3g {
@@ -82,9 +83,36 @@ __device__ __forceinline__ bool is_dynamic(const ClothDev& c, uint32_t i) { retu
 // one cloth or many: thread -> (cloth, row)
 // ---------------------------------------------------------------------------
 
+// The entry k of prefix sums with prefix[k] <= g < prefix[k + 1] (binary search).
+__device__ __forceinline__ uint32_t span_find(const uint32_t* prefix, uint32_t count, uint32_t g)
+{
+    uint32_t lo = 0, hi = count;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(prefix + mid) <= g) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The same for every lane of a warp whose g are consecutive: lane 0 searches
+// and the lanes whose g fall in its entry take its answer; a lane past the
+// entry's end (the warp straddles two cloths) searches on its own.  Every
+// lane of the warp must call it, converged (kernel entry).
+__device__ __forceinline__ uint32_t span_find_warp(const uint32_t* prefix, uint32_t count, uint32_t total,
+                                                   uint32_t g)
+{
+    const uint32_t g0 = __shfl_sync(0xffffffffu, g, 0);
+    uint32_t k0 = 0;
+    if ((threadIdx.x & 31u) == 0u) k0 = span_find(prefix, count, g0 < total ? g0 : total - 1u);
+    k0 = __shfl_sync(0xffffffffu, k0, 0);
+    if (g < total && !(__ldg(prefix + k0) <= g && g < __ldg(prefix + k0 + 1))) k0 = span_find(prefix, count, g);
+    return k0;
+}
+
 // Single-cloth launches read the cloth from the kernel parameter; launches
 // over many cloths find the cloth of global thread g in the span's prefix sums
-// of row counts (prefix[k] <= g < prefix[k + 1]).
+// of row counts (prefix[k] <= g < prefix[k + 1]), one search per warp.
 template <bool MULTI>
 __device__ __forceinline__ bool resolve(const ClothDev& one, const RowSpan& sp, uint32_t g, const ClothDev*& c,
                                         uint32_t& row)
@@ -94,15 +122,10 @@ __device__ __forceinline__ bool resolve(const ClothDev& one, const RowSpan& sp, 
         row = g;
         return g < one.n;
     }
+    const uint32_t k = span_find_warp(sp.prefix, sp.count, sp.total, g);
     if (g >= sp.total) return false;
-    uint32_t lo = 0, hi = sp.count;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(sp.prefix + mid) <= g) lo = mid;
-        else hi = mid;
-    }
-    c = sp.descs + lo;
-    row = g - __ldg(sp.prefix + lo);
+    c = sp.descs + k;
+    row = g - __ldg(sp.prefix + k);
     return true;
 }
 
@@ -524,6 +547,464 @@ __global__ void __launch_bounds__(256) k_assemble(const __grid_constant__ ClothD
         t1 = t1 + kv;
         t2 = t2 + ky;
     }
+    st3(c.b, n, row, h * ((ld3(c.b, n, row) + h * t1) + t2));
+}
+
+// ---------------------------------------------------------------------------
+// slot-major assembly
+// ---------------------------------------------------------------------------
+//
+// The row-centric kernel above evaluates each triangle once per corner and
+// pass (six times a step), one thread per row.  The slot-major form runs
+// three launches:
+//   k_elem_records     one thread per element: its per-corner constraint
+//                      gradients, stretch projectors, force scalars and
+//                      liveness flags go to a record (each element once);
+//   k_assemble_blocks  one thread per block of A (row, slot): the terms of
+//                      the elements that couple the row to the slot's column
+//                      (the block's term list, topology.h), in the row's
+//                      force-list order, into a dfdx and a dfdv sum held in
+//                      registers; it stores the block of A and the dfdx
+//                      block's products with the column's v and y.  The
+//                      diagonal block's thread also sums the row's force
+//                      from the records in force-list order (into b) and
+//                      notes the order in which the row's dfdx blocks are
+//                      first touched (as the row-centric first pass does);
+//   k_assemble_rhs     one thread per row: b = h (f + h dfdx v + dfdx y) with
+//                      the products summed in reverse first-touch order, and
+//                      P^-1.
+// Each block's sums see the same terms in the same order as the row-centric
+// sums, every term is the same float expression, and b's dfdx products are
+// summed in reverse first-touch order as before, so A, b and P^-1 are the
+// same floats.  (A spring whose two ends are one particle would add its two
+// dfdv terms to the diagonal in the other order at its second end: -kd and
+// kd in either order sum to +0, so even that case agrees.)  A warp of
+// k_assemble_blocks holds one slot of 32 consecutive rows, which on a
+// regular mesh share their term pattern; walking a row's blocks in
+// first-touch order instead (which follows which springs happen to be
+// stretched) left 13 of 32 lanes active.
+//
+// Records are planes of float4: component j of element e at rec[j * count + e],
+// so the record writes of a warp and the reads of neighbouring rows'
+// elements are coalesced.
+//
+// Triangle record, 15 components:
+//   3k, 3k+1, 3k+2 (corner k): (dC_shear_k, dwu_k), (dC_u_k, dwv_k), (dC_v_k, 0)
+//   9-11  the stretch projectors P_u = I - n_u n_u^T, P_v (symmetric: xx xy xz yy yz zz each)
+//   12    (alpha / |wu|, alpha / |wv|, C_u, C_v)
+//   13    (flags, -ks_shear C_shear, -kd dC_shear/dt, 0)
+//   14    (-ks C_u, -ks C_v, -kd dC_u/dt, -kd dC_v/dt)
+// Spring record, 3: (force on p1, K live), (K11: xx xy xz yy), (yz zz, kd, 0).
+// Mouse force record, 5: (dC_k, ·) for k = 0..3 with flags, -km C, -kd dC/dt
+// and km in the w of 0..3, then (kd, 0, 0, 0).
+enum : uint32_t {
+    kTriShear = 1u, kTriShearK = 2u, kTriShearD = 4u, kTriStretch = 8u,
+    kTriKu = 16u, kTriKv = 32u, kTriDu = 64u, kTriDv = 128u
+};
+
+__device__ __forceinline__ float4 f4(f3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+__device__ __forceinline__ f3 xyz(float4 a) { return f3{a.x, a.y, a.z}; }
+// symmetric 3x3 from (xx xy xz yy) (yz zz)
+__device__ __forceinline__ m3 sym3(float xx, float xy, float xz, float yy, float yz, float zz)
+{
+    return m3{f3{xx, xy, xz}, f3{xy, yy, yz}, f3{xz, yz, zz}};
+}
+// component j of a record whose component 0 is at r, in planes of `count`
+__device__ __forceinline__ float4 rec(const float4* r, uint32_t count, int j) { return __ldg(r + (size_t)j * count); }
+
+// b3ShearForce::Apply and b3StrechForce::Apply (shear_force.cpp:57-212,
+// strech_force.cpp:59-329) up to the per-block products, in the same
+// expressions as triangle_row.
+__device__ void tri_record(const ClothDev& c, uint32_t t)
+{
+    const uint4 tv = c.tri[t];
+    const float4 rs = c.tri_rest[t];
+    const float2 rs2 = c.tri_rest2[t];
+    const float du1 = rs.x, dv1 = rs.y, du2 = rs.z, dv2 = rs.w, inv_det = rs2.x, alpha = rs2.y;
+    const uint32_t n = c.n;
+    const f3 x1 = ld3(c.x, n, tv.x), x2 = ld3(c.x, n, tv.y), x3 = ld3(c.x, n, tv.z);
+    const f3 vs[3] = {ld3(c.v, n, tv.x), ld3(c.v, n, tv.y), ld3(c.v, n, tv.z)};
+    const f3 dx1 = x2 - x1, dx2 = x3 - x1;
+    const f3 wu = inv_det * (dv2 * dx1 - dv1 * dx2);
+    const f3 wv = inv_det * ((-du2) * dx1 + du1 * dx2);
+    const float dwudx[3] = {inv_det * (dv1 - dv2), inv_det * dv2, -inv_det * dv1};
+    const float dwvdx[3] = {inv_det * (du2 - du1), -inv_det * du2, inv_det * du1};
+    const float kd = c.k_damp;
+
+    const float ks_sh = c.k_shear;
+    const bool sh = ks_sh > 0.0f, shK = sh && ks_sh > 0.0f, shD = sh && kd > 0.0f;
+    f3 dCs[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) dCs[i] = alpha * (dwudx[i] * wv + dwvdx[i] * wu);
+    uint32_t flags = (sh ? kTriShear : 0u) | (shK ? kTriShearK : 0u) | (shD ? kTriShearD : 0u);
+    float fKs = 0.0f, fDs = 0.0f;
+    if (shK) {
+        const float C = alpha * dot(wu, wv);
+        fKs = -ks_sh * C;
+    }
+    if (shD) {
+        float dCdt = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) dCdt += dot(dCs[i], vs[i]);
+        fDs = -kd * dCdt;
+    }
+
+    const float ks = c.k_stretch;
+    const bool st = ks > 0.0f;
+    if (st) flags |= kTriStretch;
+    const m3 I = mident();
+    f3 dCst[2][3];
+    float ai[2], Cst[2], fK[2] = {0.0f, 0.0f}, fD[2] = {0.0f, 0.0f};
+    m3 P[2];
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+        const f3 w = d == 0 ? wu : wv;
+        const float len = d == 0 ? length(wu) : length(wv);
+        const float dw[3] = {d == 0 ? dwudx[0] : dwvdx[0], d == 0 ? dwudx[1] : dwvdx[1],
+                             d == 0 ? dwudx[2] : dwvdx[2]};
+        const bool live = st && len > 0.0f;
+        const float inv_len = 1.0f / len;
+        const f3 nw = inv_len * w;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) dCst[d][i] = (alpha * dw[i]) * nw;
+        const bool Kon = live && ks > 0.0f && len > 1.0f, Don = live && kd > 0.0f;
+        Cst[d] = alpha * (len - 1.0f);
+        ai[d] = alpha * inv_len;
+        P[d] = I - outer(nw, nw);
+        if (Kon) {
+            flags |= d == 0 ? kTriKu : kTriKv;
+            fK[d] = -ks * Cst[d];
+        }
+        if (Don) {
+            flags |= d == 0 ? kTriDu : kTriDv;
+            float dCdt = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) dCdt += dot(dCst[d][i], vs[i]);
+            fD[d] = -kd * dCdt;
+        }
+    }
+
+    float4* r = c.tri_rec + t;
+    const size_t T = c.t;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        r[(3 * k) * T] = f4(dCs[k], dwudx[k]);
+        r[(3 * k + 1) * T] = f4(dCst[0][k], dwvdx[k]);
+        r[(3 * k + 2) * T] = f4(dCst[1][k], 0.0f);
+    }
+    r[9 * T] = make_float4(P[0].x.x, P[0].x.y, P[0].x.z, P[0].y.y);
+    r[10 * T] = make_float4(P[0].y.z, P[0].z.z, P[1].x.x, P[1].x.y);
+    r[11 * T] = make_float4(P[1].x.z, P[1].y.y, P[1].y.z, P[1].z.z);
+    r[12 * T] = make_float4(ai[0], ai[1], Cst[0], Cst[1]);
+    r[13 * T] = make_float4(__uint_as_float(flags), fKs, fDs, 0.0f);
+    r[14 * T] = make_float4(fK[0], fK[1], fD[0], fD[1]);
+}
+
+// b3SpringForce::Apply (spring_force.cpp:53-120), the expressions of spring_row.
+__device__ void spring_record(const ClothDev& c, uint32_t sid)
+{
+    const uint2 pr = c.spr[sid];
+    const float4 par = c.spr_par[sid];
+    const float L0 = par.x, ks = par.y, kd = par.z;
+    const uint32_t n = c.n;
+    const m3 I = mident();
+    f3 mf = zero3();
+    m3 K11 = mzero();
+    uint32_t live = 0u;
+    if (ks > 0.0f) {
+        const f3 x1 = ld3(c.x, n, pr.x), x2 = ld3(c.x, n, pr.y);
+        const f3 dx = x1 - x2;
+        const float L = length(dx);
+        if (L > L0) {
+            const f3 dCdx = dx / L;
+            mf = mf + (-ks * (L - L0)) * dCdx;
+            K11 = -ks * (outer(dx, dx) + (1.0f - L0 / L) * (I - outer(dx, dx)));
+            live = 1u;
+        }
+    }
+    if (kd > 0.0f) {
+        const f3 v1 = ld3(c.v, n, pr.x), v2 = ld3(c.v, n, pr.y);
+        const f3 dv = v1 - v2;
+        mf = mf + (-kd) * dv;
+    }
+    float4* r = c.spr_rec + sid;
+    const size_t S = c.ns;
+    r[0] = f4(mf, __uint_as_float(live));
+    r[S] = make_float4(K11.x.x, K11.x.y, K11.x.z, K11.y.y);
+    r[2 * S] = make_float4(K11.y.z, K11.z.z, kd, 0.0f);
+}
+
+// b3MouseForce::Apply (mouse_force.cpp:63-227), the expressions of mouse_row.
+__device__ void mouse_record(const ClothDev& c, uint32_t m)
+{
+    const uint4 mv = c.mouse_v[m];
+    const float4 pa = c.mouse_par[2 * m], pb = c.mouse_par[2 * m + 1];
+    const float w2 = pa.x, w3 = pa.y, w4 = pa.z, km = pa.w, kd = pb.x;
+    const uint32_t n = c.n;
+    const f3 x1 = ld3(c.x, n, mv.x), x2 = ld3(c.x, n, mv.y), x3 = ld3(c.x, n, mv.z), x4 = ld3(c.x, n, mv.w);
+    const f3 c2 = (w2 * x2 + w3 * x3) + w4 * x4;
+    const f3 d = x1 - c2;
+    const float len = length(d);
+    f3 dC[4] = {zero3(), zero3(), zero3(), zero3()};
+    float fK = 0.0f, fD = 0.0f;
+    uint32_t flags = 0u;
+    if (len > 0.0f) {
+        const f3 nrm = d / len;
+        dC[0] = nrm;
+        dC[1] = (-w2) * nrm;
+        dC[2] = (-w3) * nrm;
+        dC[3] = (-w4) * nrm;
+        flags = 1u;
+        if (km > 0.0f) {
+            flags |= 2u;
+            const float C = len;
+            fK = -km * C;
+        }
+        if (kd > 0.0f) {
+            flags |= 4u;
+            const f3 vs[4] = {ld3(c.v, n, mv.x), ld3(c.v, n, mv.y), ld3(c.v, n, mv.z), ld3(c.v, n, mv.w)};
+            float dCdt = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) dCdt += dot(dC[i], vs[i]);
+            fD = -kd * dCdt;
+        }
+    }
+    float4* r = c.mouse_rec + m;
+    const size_t M = c.nmouse;
+    r[0] = f4(dC[0], __uint_as_float(flags));
+    r[M] = f4(dC[1], fK);
+    r[2 * M] = f4(dC[2], fD);
+    r[3 * M] = f4(dC[3], km);
+    r[4 * M] = make_float4(kd, 0.0f, 0.0f, 0.0f);
+}
+
+// The element of global thread g of a launch over one cloth's or many
+// cloths' elements: triangles, then springs, then mouse forces.
+template <bool MULTI>
+__device__ __forceinline__ bool resolve_elem(const ClothDev& one, const RowSpan& sp, uint32_t g, const ClothDev*& c,
+                                             uint32_t& e)
+{
+    if (!MULTI) {
+        c = &one;
+        e = g;
+        return g < one.t + one.ns + one.nmouse;
+    }
+    const uint32_t k = span_find_warp(sp.eprefix, sp.count, sp.etotal, g);
+    if (g >= sp.etotal) return false;
+    c = sp.descs + k;
+    e = g - __ldg(sp.eprefix + k);
+    return true;
+}
+
+// Every element's record, one thread per element.
+template <bool MULTI>
+__global__ void __launch_bounds__(256) k_elem_records(const __grid_constant__ ClothDev one,
+                                                      const __grid_constant__ RowSpan span)
+{
+    const ClothDev* cp;
+    uint32_t e;
+    if (!resolve_elem<MULTI>(one, span, blockIdx.x * blockDim.x + threadIdx.x, cp, e)) return;
+    const ClothDev& c = *cp;
+    if (e < c.t) tri_record(c, e);
+    else if (e < c.t + c.ns) spring_record(c, e - c.t);
+    else mouse_record(c, e - c.t - c.ns);
+}
+
+// Adds one element term (code: kind, row corner, column corner, id) to a
+// block's dfdx (K) and dfdv (D) sums, in triangle_row / spring_row /
+// mouse_row's order and expressions.
+__device__ __forceinline__ void slot_term(const ClothDev& c, uint32_t code, m3& K, m3& D)
+{
+    const uint32_t id = code & ((1u << kTermIdBits) - 1u);
+    const int cr = (int)((code >> 28) & 3u), cj = (int)((code >> 26) & 3u);
+    const uint32_t kind = code >> 30;
+    if (kind == 0u) {
+        const float4* r = c.tri_rec + id;
+        const uint32_t T = c.t;
+        const uint32_t flags = __float_as_uint(rec(r, T, 13).x);
+        const float4 a0 = rec(r, T, 3 * cr), a1 = rec(r, T, 3 * cr + 1), a2 = rec(r, T, 3 * cr + 2);
+        const float4 b0 = rec(r, T, 3 * cj), b1 = rec(r, T, 3 * cj + 1), b2 = rec(r, T, 3 * cj + 2);
+        const f3 sc = xyz(a0), sj = xyz(b0), uc = xyz(a1), uj = xyz(b1), vc = xyz(a2), vj = xyz(b2);
+        const float kd = c.k_damp;
+        if (flags & kTriShearK) K = K + -c.k_shear * outer(sc, sj);
+        if (flags & (kTriKu | kTriKv)) {
+            const float ks = c.k_stretch;
+            const float4 p0 = rec(r, T, 9), p1 = rec(r, T, 10), p2 = rec(r, T, 11), q = rec(r, T, 12);
+            if (flags & kTriKu) {
+                const float kf = (q.x * a0.w) * b0.w;
+                K = K + -ks * (outer(uc, uj) + q.z * (kf * sym3(p0.x, p0.y, p0.z, p0.w, p1.x, p1.y)));
+            }
+            if (flags & kTriKv) {
+                const float kf = (q.y * a1.w) * b1.w;
+                K = K + -ks * (outer(vc, vj) + q.w * (kf * sym3(p1.z, p1.w, p2.x, p2.y, p2.z, p2.w)));
+            }
+        }
+        if (flags & kTriShearD) D = D + -kd * outer(sc, sj);
+        if (flags & kTriDu) D = D + -kd * outer(uc, uj);
+        if (flags & kTriDv) D = D + -kd * outer(vc, vj);
+    } else if (kind == 2u) {
+        const float4* r = c.spr_rec + id;
+        const uint32_t S = c.ns;
+        const float4 r1 = rec(r, S, 1), r2 = rec(r, S, 2);
+        if (__float_as_uint(rec(r, S, 0).w)) {
+            const m3 K11 = sym3(r1.x, r1.y, r1.z, r1.w, r2.x, r2.y);
+            K = K + (cj == cr ? K11 : -1.0f * K11);
+        }
+        const float kd = r2.z;
+        if (kd > 0.0f) {
+            const m3 D11 = -kd * mident();
+            D = D + (cj == cr ? D11 : -1.0f * D11);
+        }
+    } else {
+        const float4* r = c.mouse_rec + id;
+        const uint32_t M = c.nmouse;
+        const uint32_t flags = __float_as_uint(rec(r, M, 0).w);
+        const f3 a = xyz(rec(r, M, cr)), b = xyz(rec(r, M, cj));
+        if ((flags & 3u) == 3u) K = K + -rec(r, M, 3).w * outer(a, b);
+        if ((flags & 5u) == 5u) D = D + -rec(r, M, 4).x * outer(a, b);
+    }
+}
+
+// The row's force from the element records in force-list order
+// (cloth_force_solver.cpp:172-180, the forces' Apply), stored in b, and the
+// order in which its dfdx blocks are first touched, stored as the row-centric
+// first pass stores it (slot ids at the row's SELL positions, and the count).
+__device__ void row_force(const ClothDev& c, uint32_t row, uint32_t base)
+{
+    const StepScalars* sc = c.sc;
+    const uint32_t n = c.n;
+    const float m = c.mass[row];
+    f3 f = ld3(c.fext, n, row);
+    if (is_dynamic(c, row)) f = f + m * mk(sc->gx, sc->gy, sc->gz);
+    uint32_t touched = 0u, ntouch = 0u;
+    auto mark = [&](uint32_t s) {
+        if (!((touched >> s) & 1u)) {
+            touched |= 1u << s;
+            c.asm_touch[base + 32u * ntouch] = (uint8_t)s;
+            ++ntouch;
+        }
+    };
+    const uint32_t T = c.t, S = c.ns, M = c.nmouse;
+    const uint32_t e_end = c.inc_ptr[row + 1];
+    for (uint32_t e = c.inc_ptr[row]; e < e_end; ++e) {
+        const uint32_t el = c.inc_elem[e], meta = c.inc_meta[e];
+        const int cn = (int)(meta & 3u);
+        if ((el & 0xc0000000u) == 0xc0000000u) {
+            const float4* r = c.mouse_rec + (el & 0x3fffffffu);
+            const float4 a = rec(r, M, cn), r0 = rec(r, M, 0), r1 = rec(r, M, 1), r2 = rec(r, M, 2);
+            const uint32_t flags = __float_as_uint(r0.w);
+            f3 mf = zero3();
+            if (flags & 1u) {
+                if (flags & 2u) mf = mf + r1.w * xyz(a);
+                if (flags & 4u) mf = mf + r2.w * xyz(a);
+            }
+            f = f + mf;
+            if ((flags & 3u) == 3u) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) mark((meta >> (4 + 7 * q)) & 0x7fu);
+            }
+        } else if (el & 0x80000000u) {
+            const float4 r0 = rec(c.spr_rec + (el & 0x7fffffffu), S, 0);
+            const f3 mf = xyz(r0);
+            f = cn == 0 ? f + mf : f - mf;
+            if (__float_as_uint(r0.w)) {
+                mark((meta >> 8) & 0xffu);
+                mark((meta >> 16) & 0xffu);
+            }
+        } else {
+            const float4* r = c.tri_rec + el;
+            const float4 g0 = rec(r, T, 3 * cn), g1 = rec(r, T, 3 * cn + 1), g2 = rec(r, T, 3 * cn + 2);
+            const float4 s13 = rec(r, T, 13), s14 = rec(r, T, 14);
+            const uint32_t flags = __float_as_uint(s13.x);
+            if (flags & kTriShear) {
+                f3 fe = zero3();
+                if (flags & kTriShearK) fe = fe + s13.y * xyz(g0);
+                if (flags & kTriShearD) fe = fe + s13.z * xyz(g0);
+                f = f + fe;
+            }
+            f3 fe = zero3();
+            if (flags & kTriKu) fe = fe + s14.x * xyz(g1);
+            if (flags & kTriDu) fe = fe + s14.z * xyz(g1);
+            if (flags & kTriKv) fe = fe + s14.y * xyz(g2);
+            if (flags & kTriDv) fe = fe + s14.w * xyz(g2);
+            if (flags & kTriStretch) f = f + fe;
+            if (flags & (kTriShearK | kTriKu | kTriKv)) {
+                mark((meta >> 8) & 0xffu);
+                mark((meta >> 16) & 0xffu);
+                mark((meta >> 24) & 0xffu);
+            }
+        }
+    }
+    c.asm_ntouch[row] = (uint8_t)ntouch;
+    st3(c.b, n, row, f);
+}
+
+// One block of A per thread: thread (row, slot k) with k = blockIdx.y, so a
+// warp handles the same slot of 32 consecutive rows (the same term pattern
+// on a regular mesh): its term codes and its stores are coalesced SELL
+// words.  Besides the block of A (cloth_force_solver.cpp:198) it stores its
+// dfdx products with the column's v and y, which k_assemble_rhs sums in the
+// row's order.
+template <bool MULTI>
+__global__ void __launch_bounds__(128) k_assemble_blocks(const __grid_constant__ ClothDev one,
+                                                         const __grid_constant__ RowSpan span)
+{
+    const ClothDev* cp;
+    uint32_t row;
+    if (!resolve<MULTI>(one, span, blockIdx.x * blockDim.x + threadIdx.x, cp, row)) return;
+    const ClothDev& c = *cp;
+    const uint32_t k = blockIdx.y;
+    if (k >= c.row_deg[row]) return;
+    const float h = c.sc->dt;
+    const float hh = h * h;
+    const uint32_t base = row_base(c, row);
+    const uint32_t idx = base + 32u * k;
+    const uint32_t col = c.cols[idx];
+    const uint32_t cnt = c.term_slot[idx];
+    const uint32_t* tp = c.terms + c.term_qk[(base >> 5) + k] + (row & 31u);
+    m3 K = mzero(), D = mzero();
+    uint32_t code_next = cnt ? __ldg(tp) : 0u;
+    for (uint32_t q = 0; q < cnt; ++q) {
+        const uint32_t code = code_next;
+        if (q + 1 < cnt) code_next = __ldg(tp + 32u * (q + 1));
+        slot_term(c, code, K, D);
+    }
+    const float m = k == 0 ? c.mass[row] : 0.0f;
+    const m3 M = k == 0 ? m3{f3{m, 0.0f, 0.0f}, f3{0.0f, m, 0.0f}, f3{0.0f, 0.0f, m}} : mzero();
+    store_block(c, idx, (M - h * D) - hh * K);
+    const f3 kv = K * ld3(c.v, c.n, col), ky = K * ld3(c.y, c.n, col);
+    float* qv = c.asm_kv;
+    const uint32_t E = c.E;
+    qv[idx] = kv.x; qv[E + idx] = kv.y; qv[2 * E + idx] = kv.z;
+    qv[3 * E + idx] = ky.x; qv[4 * E + idx] = ky.y; qv[5 * E + idx] = ky.z;
+    if (k == 0) row_force(c, row, base);
+}
+
+// One row per thread: b = h (f + h dfdx v + dfdx y) with the blocks' dfdx
+// products summed in reverse first-touch order (the dfdx row list order,
+// sparse_mat33.h:264-282), and the Jacobi preconditioner from the diagonal
+// block (cloth_force_solver.cpp:70-88, 172-204).
+template <bool MULTI>
+__global__ void __launch_bounds__(256) k_assemble_rhs(const __grid_constant__ ClothDev one,
+                                                      const __grid_constant__ RowSpan span)
+{
+    const ClothDev* cp;
+    uint32_t row;
+    if (!resolve<MULTI>(one, span, blockIdx.x * blockDim.x + threadIdx.x, cp, row)) return;
+    const ClothDev& c = *cp;
+    const float h = c.sc->dt;
+    const uint32_t n = c.n;
+    const uint32_t base = row_base(c, row);
+    const float* q = c.asm_kv;
+    const uint32_t E = c.E;
+    f3 t1 = zero3(), t2 = zero3();
+    for (int i = (int)c.asm_ntouch[row] - 1; i >= 0; --i) {
+        const uint32_t idx = base + 32u * c.asm_touch[base + 32u * i];
+        t1 = t1 + f3{q[idx], q[E + idx], q[2 * E + idx]};
+        t2 = t2 + f3{q[3 * E + idx], q[4 * E + idx], q[5 * E + idx]};
+    }
+    const float* v = c.vals;
+    st3(c.pinv, n, row, mk(1.0f / v[base], 1.0f / v[4 * E + base], 1.0f / v[8 * E + base]));
     st3(c.b, n, row, h * ((ld3(c.b, n, row) + h * t1) + t2));
 }
 
@@ -1373,9 +1854,21 @@ cudaError_t launch_contacts_update(const ClothDev& c, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// The assembly's two passes (forces and dfdx, then dfdv, A and b).
+constexpr int kRecordBlock = 256, kSlotBlock = 128;
+
+// The assembly: the element records and the slot-major rows where the
+// cloth's layout has them, else the row-centric two passes (forces and dfdx,
+// then dfdv, A and b).
 cudaError_t launch_assemble(const ClothDev& c, int block, cudaStream_t st)
 {
+    if (c.slot_asm) {
+        k_elem_records<false><<<blocks_for(c.t + c.ns + c.nmouse, kRecordBlock), kRecordBlock, 0, st>>>(c,
+                                                                                                   kNoSpan);
+        k_assemble_blocks<false><<<dim3(blocks_for(c.n, kSlotBlock), c.max_deg), kSlotBlock, 0, st>>>(c, kNoSpan);
+        k_assemble_rhs<false><<<blocks_for(c.n, kRecordBlock), kRecordBlock, 0, st>>>(c, kNoSpan);
+        count_launches(3);
+        return cudaGetLastError();
+    }
     if (block <= 0) block = assemble_block_for(c.max_deg, false);
     const size_t smem = assemble_smem_bytes(c.max_deg, block);
     if (smem > kAssembleSmemLimit) return cudaErrorInvalidValue;
@@ -1476,6 +1969,14 @@ cudaError_t launch_span_contacts_update(const RowSpan& sp, cudaStream_t st)
 cudaError_t launch_span_assemble(const RowSpan& sp, int block, cudaStream_t st)
 {
     if (!sp.total) return cudaSuccess;
+    if (sp.slot_asm) {
+        k_elem_records<true><<<blocks_for(sp.etotal, kRecordBlock), kRecordBlock, 0, st>>>(g_unused_one, sp);
+        k_assemble_blocks<true><<<dim3(blocks_for(sp.total, kSlotBlock), sp.max_deg), kSlotBlock, 0, st>>>(
+            g_unused_one, sp);
+        k_assemble_rhs<true><<<blocks_for(sp.total, kRecordBlock), kRecordBlock, 0, st>>>(g_unused_one, sp);
+        count_launches(3);
+        return cudaGetLastError();
+    }
     if (block <= 0) block = assemble_block_for(sp.max_deg, true);
     const size_t smem = assemble_smem_bytes(sp.max_deg, block);
     if (smem > kAssembleSmemLimit) return cudaErrorInvalidValue;

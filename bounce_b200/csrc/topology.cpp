@@ -246,7 +246,63 @@ int build_topology(uint32_t n, const float* X, uint32_t t, const uint32_t* tris,
         }
         c.inc_ptr[i + 1] = (uint32_t)c.inc_elem.size();
     }
+    build_slot_terms(&c);
     return kOk;
+}
+
+void build_slot_terms(ClothTopology* out)
+{
+    ClothTopology& c = *out;
+    c.slot_terms = false;
+    c.term_qk.clear();
+    c.term_slot.clear();
+    c.terms.clear();
+    const uint64_t id_limit = 1ull << kTermIdBits;
+    if (c.max_deg > kSlotMajorMaxDeg || c.t >= id_limit || c.ns >= id_limit) return;
+    c.term_qk.assign(c.E / 32, 0);
+    c.term_slot.assign(c.E, 0);
+    // per lane of the slice, per slot: the block's terms in the order the
+    // row's dfdx accumulation adds them: per element (force-list order) its
+    // vertices in element order
+    std::vector<std::vector<uint32_t>> per(32 * kSlotMajorMaxDeg);
+    for (uint32_t q = 0; q < c.nslices; ++q) {
+        for (auto& v : per) v.clear();
+        const uint32_t r0 = 32 * q, r1 = std::min(c.n, r0 + 32);
+        for (uint32_t i = r0; i < r1; ++i) {
+            auto slot_list = [&](uint32_t k) -> std::vector<uint32_t>& { return per[(i - r0) * kSlotMajorMaxDeg + k]; };
+            for (uint32_t e = c.inc_ptr[i]; e < c.inc_ptr[i + 1]; ++e) {
+                const uint32_t el = c.inc_elem[e], meta = c.inc_meta[e], cn = meta & 3u;
+                if ((el & (kIncSpring | kIncMouse)) == (kIncSpring | kIncMouse)) {
+                    const uint32_t id = el & ~(kIncSpring | kIncMouse);
+                    if (id >= id_limit) return;
+                    for (uint32_t v = 0; v < 4; ++v)
+                        slot_list((meta >> (4 + 7 * v)) & 0x7fu).push_back(kTermKindMouse | cn << 28 | v << 26 | id);
+                } else if (el & kIncSpring) {
+                    const uint32_t id = el & ~kIncSpring;
+                    for (uint32_t v = 0; v < 2; ++v)
+                        slot_list((meta >> (8 + 8 * v)) & 0xffu).push_back(kTermKindSpring | cn << 28 | v << 26 | id);
+                } else {
+                    for (uint32_t v = 0; v < 3; ++v) slot_list((meta >> (8 + 8 * v)) & 0xffu).push_back(cn << 28 | v << 26 | el);
+                }
+            }
+        }
+        // slot k of the slice: term j of lane l at term_qk[.] + 32 j + l
+        const uint32_t width = (c.slice_off[q + 1] - c.slice_off[q]) / 32;
+        for (uint32_t k = 0; k < width; ++k) {
+            size_t w = 0;
+            for (uint32_t l = 0; l < r1 - r0; ++l) w = std::max(w, per[l * kSlotMajorMaxDeg + k].size());
+            if (w > 255 || c.terms.size() + 32 * w >= (1ull << 32)) return;
+            const size_t base = c.terms.size();
+            c.term_qk[c.slice_off[q] / 32 + k] = (uint32_t)base;
+            c.terms.resize(base + 32 * w, 0u);
+            for (uint32_t l = 0; l < r1 - r0; ++l) {
+                const auto& v = per[l * kSlotMajorMaxDeg + k];
+                for (size_t j = 0; j < v.size(); ++j) c.terms[base + 32 * j + l] = v[j];
+                c.term_slot[c.slice_off[q] + 32 * k + l] = (uint32_t)v.size();
+            }
+        }
+    }
+    c.slot_terms = true;
 }
 
 }  // namespace b3g

@@ -43,7 +43,26 @@ struct ClothTopology {
     std::vector<uint32_t> sell_cols;         // E
     // incidence in force-list order
     std::vector<uint32_t> inc_ptr, inc_elem, inc_meta;
+    // Slot-major assembly: for every row and every slot of the row, the
+    // element terms that add to that block, in the order the reference adds
+    // them (the row's force-list order).  A term code holds the element kind
+    // (bits 30-31: 0 triangle, 2 spring, 3 mouse force), the row's corner of
+    // the element (bits 28-29), the corner of the slot's column (bits 26-27)
+    // and the element id (bits 0-25).  The codes are laid out like the matrix:
+    // term j of the block at SELL position slice_off[q] + 32 k + lane sits at
+    // term_qk[slice_off[q] / 32 + k] + 32 j + lane, so a warp reading term j
+    // of one slot of its 32 rows reads 32 consecutive words; term_slot holds
+    // each block's term count.  Built only when every row has at most
+    // kSlotMajorMaxDeg slots and every code fits (slot_terms).
+    bool slot_terms = false;
+    std::vector<uint32_t> term_qk;           // E / 32
+    std::vector<uint32_t> term_slot;         // E
+    std::vector<uint32_t> terms;
 };
+
+constexpr uint32_t kSlotMajorMaxDeg = 16;
+constexpr uint32_t kTermKindSpring = 2u << 30, kTermKindMouse = 3u << 30;
+constexpr uint32_t kTermIdBits = 26;
 
 // Returns 0 on success, else a b3g_status (degenerate mesh, unsupported degree).
 // n_extra created particles follow the n mesh vertices (masses left to the
@@ -51,6 +70,10 @@ struct ClothTopology {
 int build_topology(uint32_t n, const float* vertices, uint32_t t, const uint32_t* tris, uint32_t nsew,
                    const uint32_t* sewing, const float* def8, ClothTopology* out, uint32_t n_extra = 0,
                    const MouseForceDesc* mice = nullptr, uint32_t nmice = 0);
+
+// Fills the slot-major term lists of a built topology (build_topology calls
+// it); leaves slot_terms false when the layout does not fit them.
+void build_slot_terms(ClothTopology* out);
 
 // Bending pairs of b3FindSharedEdges (cloth.cpp:40-94): for every triangle i,
 // each edge (a -> b), every later triangle holding (b -> a); the pair is the

@@ -285,6 +285,24 @@ b3g_status b3g_cloth_step(b3g_cloth* cloth, float dt, uint32_t velocity_iteratio
  * device buffer of 96 bytes per vertex, allocated when the strategy is set. */
 typedef enum { B3G_CG_LAUNCHES = 0, B3G_CG_PERSISTENT = 1, B3G_CG_PERSISTENT_FUSED = 2 } b3g_cg_strategy;
 b3g_status b3g_cloth_set_cg_strategy(b3g_cloth* cloth, b3g_cg_strategy strategy);
+
+/* How one cloth's system (b3ClothForceSolver::Solve's forces, Jacobians, A,
+ * b and P^-1, cloth_force_solver.cpp:142-204) is assembled on the GPU; both
+ * forms give the same floats.  ELEMENT_RECORDS (the default where the layout
+ * allows it: rows of at most 16 blocks, under 2^26 triangles and springs):
+ * every element evaluated once a step into a record, then each block of A
+ * summed from the terms of the elements that couple its row and column, in
+ * the reference's order.  ROWS: each row recomputes its incident elements,
+ * in two passes.  The records and term lists take about 240 bytes a
+ * triangle, 48 a spring and 4 a block term of the cloth's arena.
+ * b3g_cloth_get_assembly returns the form in use (ROWS where the layout
+ * does not allow the records).  A batch (and a server) assembles with the
+ * records when every cloth it steps has them and their records take at
+ * most 64 MB, so that they stay in L2 between the launch that writes them
+ * and the launches that read them; otherwise row by row. */
+typedef enum { B3G_ASSEMBLY_ELEMENT_RECORDS = 0, B3G_ASSEMBLY_ROWS = 1 } b3g_assembly;
+b3g_status b3g_cloth_set_assembly(b3g_cloth* cloth, b3g_assembly form);
+b3g_assembly b3g_cloth_get_assembly(const b3g_cloth* cloth);
 /* Diagnostic of the bounded waits: runs the persistent CG once with a grid
  * barrier that can never complete and a wait limit of spin_limit polls;
  * *result receives the solve status (B3G_ERR_TIMEOUT when the limit works).
