@@ -36,6 +36,8 @@ def test_invalid_arguments_without_device(b3g):
     assert L.b3g_cloth_create(None, None, 0, C.byref(h)) == 1
     assert L.b3g_cloth_destroy(None) == 1
     assert L.b3g_cloth_step(None, 0.01, 8, 2, None) == 1
+    assert L.b3g_cloth_set_assembly(None, 0) == 1
+    assert L.b3g_cloth_get_assembly(None) == 1  # B3G_ASSEMBLY_ROWS for no cloth
 
 
 @pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES", None) is not None and
