@@ -299,7 +299,7 @@ uint64_t b3g_kernel_launch_count(void) { return kernel_launches(); }
 
 // Host half of cloth creation: validates the mesh, builds the topology and the
 // device images, sizes the arena.  Touches no CUDA state; thread-safe.
-b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3g_cloth** out)
+b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3g_cloth** out, bool records)
 {
     if (!mesh || !def || !out || !mesh->vertices || !mesh->triangles || mesh->vertex_count == 0 ||
         mesh->triangle_count == 0 || (mesh->sewing_line_count && !mesh->sewing_lines))
@@ -313,6 +313,7 @@ b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3
     if (mesh->sewing_line_count)
         c->in_sewing.assign(mesh->sewing_lines, mesh->sewing_lines + 4 * (size_t)mesh->sewing_line_count);
     c->in_def = *def;
+    c->lean_layout = !records;
     const b3g_status s = layout_cloth(c);
     if (s != B3G_OK) {
         delete c;
@@ -334,7 +335,7 @@ b3g_status layout_cloth(b3g_cloth* c)
     ClothTopology topo;
     int rc = build_topology(n_mesh, c->in_vertices.data(), (uint32_t)(c->in_tris.size() / 3), c->in_tris.data(),
                             (uint32_t)(c->in_sewing.size() / 4), c->in_sewing.empty() ? nullptr : c->in_sewing.data(),
-                            d8, &topo, c->n_extra, c->mice.data(), (uint32_t)c->mice.size());
+                            d8, &topo, c->n_extra, c->mice.data(), (uint32_t)c->mice.size(), !c->lean_layout);
     if (rc != 0) return (b3g_status)rc;
     c->topo = std::move(topo);
     const ClothTopology& T = c->topo;

@@ -61,6 +61,7 @@ struct b3g_cloth {
     uint32_t step_index = 0;
     int assemble_block = 0;  // threads per assembly block; 0: chosen at launch for occupancy
     bool row_assembly = false;  // the row-centric assembly even where the slot-major one applies
+    bool lean_layout = false;   // laid out without the slot-major assembly's records (server cloths)
 
     // pinned staging
     b3g::StepScalars* h_sc = nullptr;
@@ -112,7 +113,10 @@ struct b3g_cloth {
 b3g_status flush_ops_on(b3g_cloth* c, cudaStream_t st);
 void fill_step_scalars(b3g_cloth* c, float dt, uint32_t vel_iters, uint32_t pos_iters, b3g::StepScalars* h);
 void record_stats(b3g_cloth* c, const b3g::StepScalars& h, float ms, bool solved);
-b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3g_cloth** out);
+// records = false lays the cloth out without the slot-major assembly's
+// records and term lists (it then assembles row by row).
+b3g_status prepare_cloth(const b3g_mesh_desc* mesh, const b3g_cloth_def* def, b3g_cloth** out,
+                         bool records = true);
 b3g_status layout_cloth(b3g_cloth* c);
 // Page-locked staging for a cloth's uploads: each upload is copied into the
 // staging buffer on the host and from there to the device asynchronously.

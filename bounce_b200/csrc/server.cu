@@ -120,7 +120,10 @@ void worker_main(b3g_server* s)
         b3g_mesh_desc m{(uint32_t)(r->verts.size() / 3), r->verts.data(), (uint32_t)(r->tris.size() / 3),
                         r->tris.data(), 0, nullptr};
         b3g_cloth* c = nullptr;
-        b3g_status st = prepare_cloth(&m, &r->def, &c);
+        // the server's batches assemble row by row (their records would not
+        // stay in L2), so its cloths are laid out without the records: the
+        // HBM budget then admits more of them
+        b3g_status st = prepare_cloth(&m, &r->def, &c, false);
         std::lock_guard<std::mutex> lk(s->mu);
         if (st != B3G_OK) {
             r->status = st;

@@ -58,7 +58,7 @@ void bending_pairs(uint32_t t, const uint32_t* tris, std::vector<uint32_t>* pair
 
 int build_topology(uint32_t n, const float* X, uint32_t t, const uint32_t* tris, uint32_t nsew,
                    const uint32_t* sewing, const float* def, ClothTopology* out, uint32_t n_extra,
-                   const MouseForceDesc* mice, uint32_t nmice)
+                   const MouseForceDesc* mice, uint32_t nmice, bool slot_terms)
 {
     ClothTopology& c = *out;
     c.n_mesh = n;
@@ -246,7 +246,8 @@ int build_topology(uint32_t n, const float* X, uint32_t t, const uint32_t* tris,
         }
         c.inc_ptr[i + 1] = (uint32_t)c.inc_elem.size();
     }
-    build_slot_terms(&c);
+    if (slot_terms) build_slot_terms(&c);
+    else c.slot_terms = false;
     return kOk;
 }
 

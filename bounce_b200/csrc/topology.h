@@ -67,9 +67,10 @@ constexpr uint32_t kTermIdBits = 26;
 // Returns 0 on success, else a b3g_status (degenerate mesh, unsupported degree).
 // n_extra created particles follow the n mesh vertices (masses left to the
 // caller, 1 each here); `mice` holds the mouse forces in creation order.
+// slot_terms: also build the slot-major assembly's term lists.
 int build_topology(uint32_t n, const float* vertices, uint32_t t, const uint32_t* tris, uint32_t nsew,
                    const uint32_t* sewing, const float* def8, ClothTopology* out, uint32_t n_extra = 0,
-                   const MouseForceDesc* mice = nullptr, uint32_t nmice = 0);
+                   const MouseForceDesc* mice = nullptr, uint32_t nmice = 0, bool slot_terms = true);
 
 // Fills the slot-major term lists of a built topology (build_topology calls
 // it); leaves slot_terms false when the layout does not fit them.

@@ -299,7 +299,9 @@ b3g_status b3g_cloth_set_cg_strategy(b3g_cloth* cloth, b3g_cg_strategy strategy)
  * does not allow the records).  A batch (and a server) assembles with the
  * records when every cloth it steps has them and their records take at
  * most 64 MB, so that they stay in L2 between the launch that writes them
- * and the launches that read them; otherwise row by row. */
+ * and the launches that read them; otherwise row by row.  A server lays its
+ * cloths out without the records (row by row), which leaves more of its HBM
+ * budget for cloths. */
 typedef enum { B3G_ASSEMBLY_ELEMENT_RECORDS = 0, B3G_ASSEMBLY_ROWS = 1 } b3g_assembly;
 b3g_status b3g_cloth_set_assembly(b3g_cloth* cloth, b3g_assembly form);
 b3g_assembly b3g_cloth_get_assembly(const b3g_cloth* cloth);
